@@ -1,0 +1,384 @@
+#!/usr/bin/env python3
+"""AMG-PCG time-to-1e-8 on the 128³ heterogeneous-diffusion system, B200.
+
+Workload (one "step" = one full solve from x0 = 0 to a relative residual
+of 1e-8, checked in FP64):
+  3-D 7-point finite-volume diffusion on a 128³ grid, permeability
+  κ = exp(g), g a seeded Gaussian random field (σ = 3, correlation length 8
+  cells), harmonic-mean face transmissibilities, Dirichlet faces; b ~ U(-1,1).
+  Hierarchy: hypre_default_config(agg_trunc_factor=0.2) with l1-Jacobi
+  (HMIS θ=0.5, aggressive HMIS on level 1, extended+i interpolation),
+  V(1,1).  Solver: conjugate gradients preconditioned by one AMG cycle.
+  `value` = mean time of the mixed-precision solve (FP32 hierarchy and
+  cycle, FP64 outer residual / products / dots / updates); the FP64-cycle
+  solve is timed beside it.  Inputs stay in HBM; the finest matrix alone
+  (175 MB) exceeds the 126 MB L2, so no L2 flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+--impl reference times the reference's CPU solve (the oracle restatement of
+Draugr.jl's cycle inside a textbook PCG, all host cores) on the same
+system and hierarchy structure.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "draugr.jl_b200"))
+
+METRIC = ("AMG-PCG time-to-1e-8 (s) at 128³, mixed vs FP64 on B200; V-cycle HBM GB/s")
+TOL = 1e-8
+MAXITER = 500
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=128, help="grid side (128 = the quoted workload)")
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(n, seed):
+    from draugr import problems
+    import draugr
+
+    A = problems.heterogeneous_diffusion_3d(n, sigma=3.0, corr_len=8.0, seed=seed)
+    b = problems.rhs(A.shape[0], seed + 1)
+    cfg = draugr.hypre_default_config(agg_trunc_factor=0.2, smoother=draugr.L1JacobiSmootherType(),
+                                      seed=seed)
+    return A, b, cfg
+
+
+def workload_config(n, A, h=None, setup_s=None):
+    d = {"workload": f"3D 7-point heterogeneous diffusion {n}^3 (kappa=exp(g), sigma=3, "
+                     "corr. length 8), hypre_default_config(agg_trunc_factor=0.2) + l1-Jacobi "
+                     "V(1,1), AMG-PCG to 1e-8 from x0=0",
+         "n": int(A.shape[0]), "nnz": int(A.nnz), "tol": TOL,
+         "l2": "inputs larger than L2 (finest matrix alone 175 MB > 126 MB); no flush"}
+    if h is not None:
+        nl = h.nlevels
+        rows = [int(h.level_info(l)[0]) for l in range(nl)] + [int(h.level_info(-1)[0])]
+        nnzs = [int(h.level_info(l)[1]) for l in range(nl)]
+        d.update(levels=nl + 1, level_rows=rows, level_nnz=nnzs,
+                 operator_complexity=round(sum(nnzs) / nnzs[0], 3) if nnzs else None)
+    if setup_s is not None:
+        d["setup_s_cpu"] = round(setup_s, 3)
+    return d
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(name):
+    """Per-launch DRAM bytes of a kernel from a committed ncu summary line
+    'traffic_bytes_per_launch <name> <bytes>' under profiles/, else None."""
+    for f in sorted((ROOT / "profiles").glob("*.md")):
+        for line in f.read_text().splitlines():
+            parts = line.strip().strip("`").split()
+            if len(parts) == 3 and parts[0] == "traffic_bytes_per_launch" and parts[1] == name:
+                return float(parts[2])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = pathlib.Path(f"/tmp/draugr_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}", "--format=csv,noheader",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1].split()[0]))
+                smax.append(float(f[2].split()[0]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        self.path.unlink(missing_ok=True)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if args.impl == "ours":
+            import torch
+
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+# --------------------------------------------------------------------- ours
+def run_ours(args, world, rank, local):
+    import torch
+
+    import draugr
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    A, b, cfg = workload(args.n, args.seed)
+    n = A.shape[0]
+    t0 = time.time()
+    h = draugr.amg_setup(A, cfg)
+    setup_s = time.time() - t0
+    stream = torch.cuda.current_stream()
+    h.set_stream(stream)
+    bd = torch.tensor(b, dtype=torch.float64, device=dev)
+    xd = torch.zeros(n, dtype=torch.float64, device=dev)
+    bnorm = np.linalg.norm(b)
+
+    def solve(mode):
+        xd.zero_()
+        return draugr.pcg(xd, bd, h, cfg, tol=TOL, maxiter=MAXITER, precision=mode)
+
+    def timed(mode, steps):
+        times, its = [], []
+        for _ in range(steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            xd.zero_()
+            e0.record(stream)
+            _, it, _ = draugr.pcg(xd, bd, h, cfg, tol=TOL, maxiter=MAXITER, precision=mode)
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1) / 1e3)
+            its.append(it)
+        return times, its
+
+    res = {}
+    for mode in ("fp64", "mixed"):
+        for _ in range(args.warmup):
+            solve(mode)
+        torch.cuda.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        if mode == "mixed":
+            launches0 = draugr.load().draugr_b200_kernel_launches()
+            with ClockSampler(local) as cs:
+                times, its = timed(mode, args.steps)
+            launches = draugr.load().draugr_b200_kernel_launches() - launches0
+            clocks = cs.summary()
+        else:
+            times, its = timed(mode, args.steps)
+        torch.cuda.synchronize()
+        barrier(world)
+        x = xd.cpu().numpy()
+        rr = float(np.linalg.norm(b - A @ x) / bnorm)
+        res[mode] = {"time_s": max_over_ranks(float(np.mean(times)), world),
+                     "time_s_min": float(np.min(times)), "iterations": int(its[-1]),
+                     "relres_fp64_verified": rr}
+        if rr >= TOL:
+            raise SystemExit(f"{mode} solve did not reach {TOL}: {rr}")
+
+    # end-to-end through the C ABI with host buffers: H2D of x0 and b, D2H of x
+    xh = np.zeros(n)
+    e2e_times = []
+    for k in range(args.warmup + args.steps):
+        xh[:] = 0.0
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        draugr.pcg(xh, b, h, cfg, tol=TOL, maxiter=MAXITER, precision="mixed")
+        e1.record(stream)
+        e1.synchronize()
+        if k >= args.warmup:
+            e2e_times.append(e0.elapsed_time(e1) / 1e3)
+    e2e = {"value": max_over_ranks(float(np.mean(e2e_times)), world), "unit": "s",
+           "h2d_bytes_per_step": 2 * n * 8, "d2h_bytes_per_step": n * 8,
+           "path": "draugr_b200_pcg (C ABI, host x/b)"}
+
+    # roofline of the dominant kernels: finest-level Jacobi sweep and SpMV
+    nnz = A.nnz
+    kern = {}
+    for name, op, prec, byts in (
+            ("l1_jacobi_fp64_level1", 2, 0, 12 * nnz + 4 * (n + 1) + 32 * n),
+            ("l1_jacobi_fp32_level1", 2, 1, 8 * nnz + 4 * (n + 1) + 16 * n),
+            ("spmv_fp64_level1", 0, 0, 12 * nnz + 4 * (n + 1) + 16 * n),
+            ("spmv_fp32_level1", 0, 1, 8 * nnz + 4 * (n + 1) + 8 * n)):
+        ms = h.time_level_op(0, op, prec, reps=50)
+        kern[name] = {"bytes": int(byts), "ms": ms, "GBps": byts / (ms * 1e-3) / 1e9}
+    peak, peak_kind = peaks()
+    dom = kern["l1_jacobi_fp64_level1"]
+    roofline = {"bound": "hbm", "kernel": "l1_jacobi_fp64_level1 (k_csr_rows<8>, EpJacobi)",
+                "achieved": round(dom["GBps"], 1), "peak": peak, "unit": "GB/s",
+                "frac": round(dom["GBps"] / peak, 3),
+                "traffic": profiled_traffic("l1_jacobi_fp64_level1"),
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                else "fallback 6.65 TB/s",
+                "algorithmic_bytes_per_launch": dom["bytes"],
+                "timing": "CUDA events on the hierarchy's stream, 50 launches after 3 warm-up, "
+                          "run after the timed solves",
+                "kernels": {k: {kk: (round(vv, 4) if isinstance(vv, float) else vv)
+                                for kk, vv in v.items()} for k, v in kern.items()}}
+
+    out = {"metric": METRIC, "value": res["mixed"]["time_s"], "unit": "s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": res["mixed"]["time_s"] * 1e3, "higher_is_better": False,
+           "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32 (hierarchy, cycle) + f64 (outer residual, A-products, dots, updates)",
+           "data": "synthetic (seeded log-normal permeability field, b ~ U(-1,1))",
+           "config": dict(workload_config(args.n, A, h, setup_s),
+                          parallelism=f"replicas x{world}" if world > 1 else "1 GPU"),
+           "fp64": res["fp64"], "mixed": res["mixed"],
+           "speedup_mixed_vs_fp64": res["fp64"]["time_s"] / res["mixed"]["time_s"],
+           "e2e": e2e, "roofline": roofline, "clocks": clocks, "gpu_launches": int(launches)}
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(h, b, cfg)
+    h.set_stream(None)
+    return out
+
+
+def cpu_solve_time(h, b, cfg, reps=1):
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+
+    O = oracle.OracleHierarchy(h)
+    n = len(b)
+    ts = []
+    its = 0
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        x, its, rel = O.pcg(np.zeros(n), b, cfg.pre_smoothing_steps, cfg.post_smoothing_steps,
+                            cfg.cycle_type == "W", TOL, MAXITER)
+        ts.append(time.perf_counter() - t0)
+    return float(np.mean(ts)), its
+
+
+def cpu_baseline(h, b, cfg):
+    t, its = cpu_solve_time(h, b, cfg)
+    return {"value": t, "unit": "s", "cores": os.cpu_count(), "kind": "port",
+            "iterations": its,
+            "sample": "one full AMG-PCG solve (FP64 cycle) of the same system and hierarchy "
+                      "to 1e-8, oracle restatement of the reference's CPU kernels, OpenMP "
+                      "static/64-row chunks on all host threads"}
+
+
+# --------------------------------------------------------------- reference
+def run_reference(args, world, rank):
+    import draugr
+
+    if rank != 0:
+        return None
+    A, b, cfg = workload(args.n, args.seed)
+    h = draugr.amg_setup(A, cfg, on_device=False)   # structure only (shared input)
+    times = []
+    its = 0
+    for k in range(args.warmup + args.steps):
+        t, its = cpu_solve_time(h, b, cfg)
+        if k >= args.warmup:
+            times.append(t)
+    v = float(np.mean(times))
+    sample = ("full AMG-PCG solve per step (FP64 cycle), oracle restatement of Draugr.jl's "
+              "CPU kernels (Julia is not available), OpenMP on all host threads")
+    return {"metric": METRIC, "impl": "reference", "value": v, "unit": "s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded log-normal permeability field, b ~ U(-1,1))",
+            "config": dict(workload_config(args.n, A, h), parallelism="CPU"),
+            "iterations": its,
+            "cpu_baseline": {"value": v, "unit": "s", "cores": os.cpu_count(), "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_init(args)
+    if args.impl == "reference":
+        out = run_reference(args, world, rank)
+    else:
+        out = run_ours(args, world, rank, local)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0 and out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

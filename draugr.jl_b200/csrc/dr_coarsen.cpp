@@ -1,0 +1,579 @@
+// Strength of connection and coarsening (CPU setup phase).
+//
+// These routines produce the C/F splitting or aggregates that define the
+// hierarchy structure.  They follow the sequential algorithms of Draugr.jl
+// step by step (same visiting orders, same tie-breaking), so that for the
+// same random measures the same splitting results:
+//   strength         src/strength.jl:24-76 (absolute), :78-150 (signed),
+//                    :183-218 (max row sum)
+//   aggregation      src/coarsening.jl:14-171
+//   PMIS             src/coarsening.jl:202-289
+//   HMIS             src/coarsening.jl:330-404, RS first pass :406-573,
+//                    PMIS on undecided :575-630
+//   aggressive CF    src/coarsening.jl:990-1112
+// The reference draws PMIS/HMIS measures from an unseeded global generator;
+// here they come from a seeded generator (Config::seed).
+#include <algorithm>
+#include <cmath>
+#include <limits>
+#include <numeric>
+
+#include "dr_host.h"
+
+namespace dr {
+
+static const double kEps = std::numeric_limits<double>::epsilon();
+
+double rng_uniform(uint64_t& s) {
+  // splitmix64 step, 53 random bits mapped to [0, 1).
+  s += 0x9E3779B97F4A7C15ULL;
+  uint64_t z = s;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  z ^= z >> 31;
+  return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+void validate_csr(const CSR& A, const char* what) {
+  if (A.n < 0 || A.m < 0) fail(std::string(what) + ": negative dimension");
+  if ((int64_t)A.rp.size() != (int64_t)A.n + 1)
+    fail(std::string(what) + ": rowptr must have n+1 entries");
+  if (A.rp[0] != 0) fail(std::string(what) + ": rowptr must start at the index base");
+  for (int i = 0; i < A.n; ++i)
+    if (A.rp[i + 1] < A.rp[i]) fail(std::string(what) + ": rowptr is not monotone at row " + std::to_string(i + 1));
+  if ((int64_t)A.rp[A.n] != A.nnz())
+    fail(std::string(what) + ": rowptr[n+1]-base must equal nnz");
+  if (A.v.size() != A.ci.size()) fail(std::string(what) + ": colval and nzval lengths differ");
+  for (int64_t k = 0; k < A.nnz(); ++k)
+    if (A.ci[k] < 0 || A.ci[k] >= A.m)
+      fail(std::string(what) + ": column index out of range at entry " + std::to_string(k + 1));
+}
+
+// --------------------------------------------------------------- strength
+std::vector<uint8_t> strength_absolute(const CSR& A, double theta) {
+  std::vector<uint8_t> s(A.nnz(), 0);
+#pragma omp parallel for schedule(static, 1024)
+  for (int i = 0; i < A.n; ++i) {
+    double mx = 0.0;
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
+      if (A.ci[k] != i) mx = std::max(mx, std::fabs(A.v[k]));
+    double thr = theta * mx;
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
+      s[k] = (A.ci[k] != i) ? (std::fabs(A.v[k]) >= thr) : 0;
+  }
+  return s;
+}
+
+static inline double sgn(double x) { return x > 0 ? 1.0 : (x < 0 ? -1.0 : 0.0); }
+
+std::vector<uint8_t> strength_signed(const CSR& A, double theta) {
+  std::vector<uint8_t> s(A.nnz(), 0);
+#pragma omp parallel for schedule(static, 1024)
+  for (int i = 0; i < A.n; ++i) {
+    double aii = 0.0;
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
+      if (A.ci[k] == i) { aii = A.v[k]; break; }
+    double ds = sgn(aii);
+    if (ds == 0) ds = 1.0;
+    double mx = 0.0;
+    bool has = false;
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
+      if (A.ci[k] != i && sgn(A.v[k]) != ds) { mx = std::max(mx, std::fabs(A.v[k])); has = true; }
+    if (has) {
+      double thr = theta * mx;
+      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
+        s[k] = (A.ci[k] != i && sgn(A.v[k]) != ds) ? (std::fabs(A.v[k]) >= thr) : 0;
+    } else {
+      double mo = 0.0;
+      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
+        if (A.ci[k] != i) mo = std::max(mo, std::fabs(A.v[k]));
+      double thr = theta * mo;
+      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
+        s[k] = (A.ci[k] != i) ? (std::fabs(A.v[k]) >= thr) : 0;
+    }
+  }
+  return s;
+}
+
+CSR apply_max_row_sum(const CSR& A, double threshold) {
+  CSR W = A;
+  for (int i = 0; i < A.n; ++i) {
+    double diag = 0.0, rs = 0.0;
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+      rs += A.v[k];
+      if (A.ci[k] == i) diag = A.v[k];
+    }
+    double ad = std::fabs(diag);
+    if (ad < kEps) continue;
+    if (std::fabs(rs) > ad * threshold && threshold < 1.0)
+      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
+        if (A.ci[k] != i) W.v[k] = 0.0;
+  }
+  return W;
+}
+
+// ------------------------------------------------------------ union-find
+static int find_root(std::vector<int>& parent, int i) {
+  while (parent[i] != i) {
+    parent[i] = parent[parent[i]];
+    i = parent[i];
+  }
+  return i;
+}
+static void union_roots(std::vector<int>& parent, int a, int b) {
+  int ra = find_root(parent, a), rb = find_root(parent, b);
+  if (ra != rb) parent[rb] = ra;
+}
+
+// ------------------------------------------------------------ aggregation
+void coarsen_aggregation(const CSR& A, double theta, std::vector<int>& agg, int& nc) {
+  const int n = A.n;
+  agg.assign(n, 0);
+  if (n <= 1) {
+    for (int i = 0; i < n; ++i) agg[i] = 0;
+    nc = n;
+    return;
+  }
+  std::vector<uint8_t> st = strength_absolute(A, theta);
+  // aggregate ids are 1-based during construction (0 = unassigned)
+  std::vector<int> a(n, 0);
+  int ncoarse = 0;
+  std::vector<int> scount(n, 0);
+  for (int i = 0; i < n; ++i)
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
+      if (A.ci[k] != i && st[k]) scount[i]++;
+  // Phase 1: distance-2 MIS seeds in decreasing strong-count order (ties by
+  // ascending index, as sortperm(...; rev=true) keeps equal keys in order).
+  std::vector<int> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int x, int y) { return scount[x] > scount[y]; });
+  std::vector<int8_t> state(n, 0);
+  for (int idx = 0; idx < n; ++idx) {
+    int i = order[idx];
+    if (state[i] != 0) continue;
+    bool can_seed = true;
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+      int j = A.ci[k];
+      if (j != i && st[k] && (state[j] == 1 || state[j] == -1)) { can_seed = false; break; }
+    }
+    if (!can_seed) continue;
+    state[i] = 1;
+    ++ncoarse;
+    a[i] = ncoarse;
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+      int j = A.ci[k];
+      if (j != i && st[k] && state[j] == 0) {
+        state[j] = -1;
+        a[j] = ncoarse;
+        for (int k2 = A.rp[j]; k2 < A.rp[j + 1]; ++k2) {
+          int q = A.ci[k2];
+          if (q != j && st[k2] && state[q] == 0) state[q] = -2;
+        }
+      }
+    }
+  }
+  // Phase 2: attach leftovers to the strongest aggregated neighbour.
+  for (int i = 0; i < n; ++i) {
+    if (a[i] != 0) continue;
+    int best = 0;
+    double bv = 0.0;
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+      int j = A.ci[k];
+      if (j != i && st[k] && a[j] != 0 && std::fabs(A.v[k]) > bv) { bv = std::fabs(A.v[k]); best = a[j]; }
+    }
+    if (best == 0)
+      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+        int j = A.ci[k];
+        if (j != i && a[j] != 0 && std::fabs(A.v[k]) > bv) { bv = std::fabs(A.v[k]); best = a[j]; }
+      }
+    if (best != 0) a[i] = best;
+    else { ++ncoarse; a[i] = ncoarse; }
+  }
+  // Phase 3: merge singleton aggregates into their strongest neighbour.
+  std::vector<int> size(ncoarse + 1, 0);
+  for (int i = 0; i < n; ++i) size[a[i]]++;
+  std::vector<int> mm(ncoarse + 1);
+  std::iota(mm.begin(), mm.end(), 0);
+  for (int i = 0; i < n; ++i) {
+    int my = find_root(mm, a[i]);
+    if (size[my] > 1) continue;
+    int tgt = 0;
+    double bv = 0.0;
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+      int j = A.ci[k];
+      if (j == i) continue;
+      int jr = find_root(mm, a[j]);
+      if (jr != my && std::fabs(A.v[k]) > bv) { bv = std::fabs(A.v[k]); tgt = jr; }
+    }
+    if (tgt != 0) {
+      int om = size[my], ot = size[tgt];
+      union_roots(mm, tgt, my);
+      int nr = find_root(mm, tgt);
+      size[nr] = om + ot;
+    }
+  }
+  std::vector<int> nid(ncoarse + 1, 0);
+  int cnt = 0;
+  for (int i = 1; i <= ncoarse; ++i) {
+    int r = find_root(mm, i);
+    if (nid[r] == 0) nid[r] = ++cnt;
+    nid[i] = nid[r];
+  }
+  for (int i = 0; i < n; ++i) agg[i] = nid[find_root(mm, a[i])] - 1;  // 0-based
+  nc = cnt;
+}
+
+// ------------------------------------------------------------ helpers
+static std::vector<int> strong_transpose_count(const CSR& A, const std::vector<uint8_t>& st) {
+  std::vector<int> c(A.n, 0);
+  for (int i = 0; i < A.n; ++i)
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
+      if (A.ci[k] != i && st[k]) c[A.ci[k]]++;
+  return c;
+}
+
+static void strong_transpose_adj(const CSR& A, const std::vector<uint8_t>& st,
+                                 std::vector<int>& off, std::vector<int>& src) {
+  const int n = A.n;
+  off.assign(n + 1, 0);
+  for (int i = 0; i < n; ++i)
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
+      if (A.ci[k] != i && st[k]) off[A.ci[k] + 1]++;
+  for (int j = 0; j < n; ++j) off[j + 1] += off[j];
+  src.assign(off[n], 0);
+  std::vector<int> pos(off.begin(), off.end() - 1);
+  for (int i = 0; i < n; ++i)
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
+      if (A.ci[k] != i && st[k]) src[pos[A.ci[k]]++] = i;
+}
+
+static bool has_strong_nbr(const CSR& A, const std::vector<uint8_t>& st, int i) {
+  for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
+    if (A.ci[k] != i && st[k]) return true;
+  return false;
+}
+
+static void build_cmap(const std::vector<int>& cf, std::vector<int>& cmap, int& nc) {
+  const int n = (int)cf.size();
+  cmap.assign(n, -1);
+  nc = 0;
+  for (int i = 0; i < n; ++i)
+    if (cf[i] == 1) cmap[i] = nc++;
+}
+
+// ------------------------------------------------------------ PMIS
+void coarsen_pmis(const CSR& A, double theta, uint64_t& rng, std::vector<int>& cf,
+                  std::vector<int>& cmap, int& nc) {
+  const int n = A.n;
+  if (n <= 1) {
+    cf.assign(n, 1);
+    build_cmap(cf, cmap, nc);
+    return;
+  }
+  std::vector<uint8_t> st = strength_absolute(A, theta);
+  std::vector<int> stc = strong_transpose_count(A, st);
+  std::vector<double> meas(n);
+  for (int i = 0; i < n; ++i) meas[i] = (double)stc[i] + rng_uniform(rng);
+  cf.assign(n, 0);
+  for (int i = 0; i < n; ++i)
+    if (!has_strong_nbr(A, st, i) && stc[i] == 0) cf[i] = 1;
+  for (int it = 0; it <= n; ++it) {
+    bool all_decided = true;
+    for (int i = 0; i < n; ++i) {
+      if (cf[i] != 0) continue;
+      all_decided = false;
+      bool is_max = true;
+      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+        int j = A.ci[k];
+        if (st[k] && j != i && cf[j] != -1 && meas[j] > meas[i]) { is_max = false; break; }
+      }
+      if (is_max) cf[i] = 1;
+    }
+    for (int i = 0; i < n; ++i) {
+      if (cf[i] != 0) continue;
+      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
+        if (st[k] && cf[A.ci[k]] == 1) { cf[i] = -1; break; }
+    }
+    if (all_decided) break;
+  }
+  for (int i = 0; i < n; ++i)
+    if (cf[i] == 0) cf[i] = 1;
+  build_cmap(cf, cmap, nc);
+}
+
+// ------------------------------------------------------------ RS first pass
+// Bucket lists keyed by the measure lambda; insertion at the head.
+namespace {
+struct Buckets {
+  std::vector<int> head, next, prev;
+  std::vector<int>& lam;
+  Buckets(int n, int maxl, std::vector<int>& l)
+      : head(std::max(maxl + 1, 1), -1), next(n, -1), prev(n, -1), lam(l) {}
+  void insert(int i) {
+    int k = lam[i];
+    if (k >= (int)head.size()) head.resize(k + 1, -1);
+    int oh = head[k];
+    head[k] = i;
+    next[i] = oh;
+    prev[i] = -1;
+    if (oh != -1) prev[oh] = i;
+  }
+  void remove(int i) {
+    int k = lam[i];
+    int p = prev[i], nx = next[i];
+    if (p != -1) next[p] = nx;
+    else head[k] = nx;
+    if (nx != -1) prev[nx] = p;
+    next[i] = -1;
+    prev[i] = -1;
+  }
+  void update(int i, int nl) {
+    remove(i);
+    lam[i] = nl;
+    insert(i);
+  }
+};
+}  // namespace
+
+static std::vector<int> rs_first_pass(const CSR& A, const std::vector<uint8_t>& st, bool use_zpt) {
+  const int n = A.n;
+  const int f_pnt = use_zpt ? -2 : -1;
+  std::vector<int> lam = strong_transpose_count(A, st);
+  std::vector<int> st_off, st_src;
+  strong_transpose_adj(A, st, st_off, st_src);
+  std::vector<int> cf(n, 0);
+  for (int i = 0; i < n; ++i)
+    if (!has_strong_nbr(A, st, i) && lam[i] == 0) cf[i] = 1;
+  for (int i = 0; i < n; ++i) {
+    if (cf[i] != 0) continue;
+    if (lam[i] == 0) {
+      cf[i] = f_pnt;
+      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+        int j = A.ci[k];
+        if (j != i && st[k] && cf[j] == 0) lam[j]++;
+      }
+    }
+  }
+  int maxl = 0;
+  for (int i = 0; i < n; ++i)
+    if (cf[i] == 0) maxl = std::max(maxl, lam[i]);
+  Buckets B(n, maxl, lam);
+  for (int i = 0; i < n; ++i)
+    if (cf[i] == 0) B.insert(i);
+  int top = maxl;
+  for (;;) {
+    while (top >= 0 && B.head[top] == -1) --top;
+    if (top < 0) break;
+    int best = B.head[top];
+    if (best == -1) break;
+    B.remove(best);
+    cf[best] = 1;
+    for (int idx = st_off[best]; idx < st_off[best + 1]; ++idx) {
+      int j = st_src[idx];
+      if (cf[j] != 0) continue;
+      B.remove(j);
+      cf[j] = -1;
+      for (int k2 = A.rp[j]; k2 < A.rp[j + 1]; ++k2) {
+        int q = A.ci[k2];
+        if (q != j && st[k2] && cf[q] == 0) {
+          int nv = lam[q] + 1;
+          B.update(q, nv);
+          if (nv > top) top = nv;
+        }
+      }
+    }
+    for (int k = A.rp[best]; k < A.rp[best + 1]; ++k) {
+      int j = A.ci[k];
+      if (j != best && st[k] && cf[j] == 0) {
+        int nv = std::max(0, lam[j] - 1);
+        B.update(j, nv);
+        if (nv == 0) {
+          B.remove(j);
+          cf[j] = f_pnt;
+          for (int k2 = A.rp[j]; k2 < A.rp[j + 1]; ++k2) {
+            int q = A.ci[k2];
+            if (q != j && st[k2] && cf[q] == 0) {
+              int nv2 = lam[q] + 1;
+              B.update(q, nv2);
+              if (nv2 > top) top = nv2;
+            }
+          }
+        }
+      }
+    }
+  }
+  return cf;
+}
+
+static void pmis_on_undecided(std::vector<int>& cf, const CSR& A, const std::vector<uint8_t>& st,
+                              const std::vector<double>& meas) {
+  const int n = A.n;
+  for (int it = 0; it <= n; ++it) {
+    bool all_decided = true;
+    for (int i = 0; i < n; ++i) {
+      if (cf[i] != 0) continue;
+      all_decided = false;
+      if (meas[i] < 1.0) { cf[i] = -1; continue; }
+      bool is_max = true;
+      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+        int j = A.ci[k];
+        if (j != i && st[k] && cf[j] != -1 && meas[j] > meas[i]) { is_max = false; break; }
+      }
+      if (is_max) cf[i] = 1;
+    }
+    for (int i = 0; i < n; ++i) {
+      if (cf[i] != 0) continue;
+      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
+        if (st[k] && cf[A.ci[k]] == 1) { cf[i] = -1; break; }
+    }
+    if (all_decided) break;
+  }
+  for (int i = 0; i < n; ++i)
+    if (cf[i] == 0) cf[i] = -1;
+}
+
+void coarsen_hmis(const CSR& A, double theta, uint64_t& rng, std::vector<int>& cf,
+                  std::vector<int>& cmap, int& nc) {
+  const int n = A.n;
+  if (n <= 1) {
+    cf.assign(n, 1);
+    build_cmap(cf, cmap, nc);
+    return;
+  }
+  std::vector<uint8_t> st = strength_absolute(A, theta);
+  cf = rs_first_pass(A, st, true);
+  std::vector<int> stc = strong_transpose_count(A, st);
+  std::vector<double> meas(n);
+  for (int i = 0; i < n; ++i) meas[i] = (double)stc[i] + rng_uniform(rng);
+  for (int i = 0; i < n; ++i) {
+    if (cf[i] == -2) {
+      if (meas[i] >= 1.0 || has_strong_nbr(A, st, i)) cf[i] = 0;
+      else cf[i] = -1;
+    }
+  }
+  pmis_on_undecided(cf, A, st, meas);
+  build_cmap(cf, cmap, nc);
+}
+
+static void ensure_fine_have_coarse_neighbor(std::vector<int>& cf, const CSR& A,
+                                             const std::vector<uint8_t>& st) {
+  bool changed = true;
+  while (changed) {
+    changed = false;
+    for (int i = 0; i < A.n; ++i) {
+      if (cf[i] != -1) continue;
+      bool has_c = false;
+      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+        int j = A.ci[k];
+        if (j != i && st[k] && cf[j] == 1) { has_c = true; break; }
+      }
+      if (!has_c) { cf[i] = 1; changed = true; }
+    }
+  }
+}
+
+void coarsen_aggressive_cf(const CSR& A_in, double theta, bool base_hmis, const Config& cfg,
+                           uint64_t& rng, std::vector<int>& cf, std::vector<int>& cmap,
+                           int& nc) {
+  const int n = A_in.n;
+  if (n <= 1) {
+    cf.assign(n, 1);
+    build_cmap(cf, cmap, nc);
+    return;
+  }
+  CSR Aw;
+  const CSR* Ap = &A_in;
+  if (cfg.max_row_sum < 1.0) {
+    Aw = apply_max_row_sum(A_in, cfg.max_row_sum);
+    Ap = &Aw;
+  }
+  const CSR& A = *Ap;
+  std::vector<int> cf1, cm1;
+  int nc1 = 0;
+  if (base_hmis) coarsen_hmis(A, theta, rng, cf1, cm1, nc1);
+  else coarsen_pmis(A, theta, rng, cf1, cm1, nc1);
+  std::vector<uint8_t> st = strength_absolute(A, theta);
+
+  // C-points of the first pass and their local numbering.
+  std::vector<int> cidx, clocal(n, -1);
+  for (int i = 0; i < n; ++i)
+    if (cf1[i] == 1) { clocal[i] = (int)cidx.size(); cidx.push_back(i); }
+  const int m = (int)cidx.size();
+
+  // Distance-2 graph among C-points: N(a) collects, over every node i with a
+  // in its strong C-neighbour list cn(i), the other members of cn(i), plus i
+  // itself when i is a C-point; and cn(node(a)) itself.
+  std::vector<int> st_off, st_src;
+  strong_transpose_adj(A, st, st_off, st_src);
+  std::vector<int> noff(m + 1, 0);
+  std::vector<std::vector<int>> nbr_chunks;
+  std::vector<int> ncount(m, 0);
+  std::vector<int> nflat;
+  {
+    // two passes (count, fill) over a, each with a per-thread marker array
+    std::vector<std::vector<int>> rows(m);
+#pragma omp parallel
+    {
+      std::vector<int> mark(m, -1);
+      std::vector<int> buf;
+#pragma omp for schedule(dynamic, 256)
+      for (int a = 0; a < m; ++a) {
+        buf.clear();
+        int node = cidx[a];
+        auto add = [&](int b) {
+          if (b != a && mark[b] != a) { mark[b] = a; buf.push_back(b); }
+        };
+        // cn(node): strong C neighbours of node(a) (a -> them via "i is C")
+        for (int k = A.rp[node]; k < A.rp[node + 1]; ++k) {
+          int j = A.ci[k];
+          if (j != node && st[k] && cf1[j] == 1) add(clocal[j]);
+        }
+        // every i that has node(a) as a strong neighbour
+        for (int t = st_off[node]; t < st_off[node + 1]; ++t) {
+          int i = st_src[t];
+          if (cf1[i] == 1) add(clocal[i]);
+          for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+            int j = A.ci[k];
+            if (j != i && st[k] && cf1[j] == 1) add(clocal[j]);
+          }
+        }
+        rows[a] = buf;
+      }
+    }
+    for (int a = 0; a < m; ++a) noff[a + 1] = noff[a] + (int)rows[a].size();
+    nflat.resize(noff[m]);
+    for (int a = 0; a < m; ++a) std::copy(rows[a].begin(), rows[a].end(), nflat.begin() + noff[a]);
+  }
+  std::vector<double> cmeas(m);
+  for (int a = 0; a < m; ++a) cmeas[a] = (double)(noff[a + 1] - noff[a]) + rng_uniform(rng);
+  std::vector<int> cf2(m, 0);
+  for (int it = 0; it <= m; ++it) {
+    bool all_decided = true;
+    for (int a = 0; a < m; ++a) {
+      if (cf2[a] != 0) continue;
+      all_decided = false;
+      bool is_max = true;
+      for (int t = noff[a]; t < noff[a + 1]; ++t) {
+        int b = nflat[t];
+        if (cf2[b] != -1 && cmeas[b] > cmeas[a]) { is_max = false; break; }
+      }
+      if (is_max) cf2[a] = 1;
+    }
+    for (int a = 0; a < m; ++a) {
+      if (cf2[a] != 0) continue;
+      for (int t = noff[a]; t < noff[a + 1]; ++t)
+        if (cf2[nflat[t]] == 1) { cf2[a] = -1; break; }
+    }
+    if (all_decided) break;
+  }
+  for (int a = 0; a < m; ++a)
+    if (cf2[a] == 0) cf2[a] = 1;
+  cf = cf1;
+  for (int a = 0; a < m; ++a)
+    if (cf2[a] == -1) cf[cidx[a]] = -1;
+  ensure_fine_have_coarse_neighbor(cf, A, st);
+  build_cmap(cf, cmap, nc);
+}
+
+}  // namespace dr

@@ -1,0 +1,870 @@
+// Device hierarchy, V/W cycle, stationary AMG solve, AMG-preconditioned CG
+// and the numeric resetup (sm_100a).
+//
+// Reference behaviour reproduced here (Draugr.jl):
+//   amg_cycle! / _vcycle_descend!  src/cycle.jl:12-28, :63-99
+//   amg_solve!                     src/cycle.jl:110-160
+//   amg_resetup! (partial)         src/resetup.jl:20-45, :95-158
+//   preconditioner_apply!          src/preconditioner.jl:76-80 (x zeroed, one cycle)
+// Differences in form, not in result: the Jacobi ping-pong of
+// src/smoothers.jl:103-124 swaps buffer pointers instead of copying back;
+// the first Jacobi step from a zero iterate (every coarse level, and the
+// finest level inside PCG) needs no product with A, so it is evaluated
+// inside the residual kernel that follows it; restriction uses Pᵀ stored
+// with values in transpose-map order, so no index indirection is needed.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "dr_device.h"
+#include "dr_kernels.cuh"
+
+namespace dr {
+
+using namespace kern;
+
+// Kernels launched by this library (host-side count; a CUDA graph adds the
+// number of kernels captured in it on every launch).
+static std::atomic<long long> g_launches{0};
+long long kernel_launches() { return g_launches.load(); }
+static inline void counted() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+void cuda_check(cudaError_t e, const char* what, const char* file, int line) {
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    char buf[512];
+    std::snprintf(buf, sizeof buf, "CUDA error %d (%s) in %s at %s:%d", (int)e, cudaGetErrorString(e),
+                  what, file, line);
+    fail(buf);
+  }
+}
+
+namespace {
+
+int pick_G(long long nnz, int n) {
+  if (n <= 0) return 1;
+  double avg = (double)nnz / (double)n;
+  int G = 1;
+  while (G < 32 && G < avg * 0.75) G *= 2;
+  return G;
+}
+
+template <typename TA, class XL, class EP, bool DOT, class Fin>
+void launch_rows_impl(cudaStream_t st, int max_grid, int G, int n, const int* rp, const int* ci,
+                      const TA* av, XL xl, EP ep, double* partials, unsigned* ticket, Fin fin) {
+  if (n <= 0) {
+    if constexpr (DOT) {
+      // an empty reduction still has to deliver its (zero) result
+      counted();
+      k_dot<double, double, Fin><<<1, kBlock, 0, st>>>(0, nullptr, nullptr, partials, ticket, fin);
+    }
+    return;
+  }
+  const long long thr = (long long)n * G;
+  const int grid = (int)std::max<long long>(1, std::min<long long>((thr + kBlock - 1) / kBlock, max_grid));
+  counted();
+  switch (G) {
+#define DR_CASE(g)                                                                              \
+  case g:                                                                                       \
+    k_csr_rows<g, TA, XL, EP, DOT, Fin><<<grid, kBlock, 0, st>>>(n, rp, ci, av, xl, ep, partials, \
+                                                                 ticket, fin);                   \
+    break;
+    DR_CASE(1) DR_CASE(2) DR_CASE(4) DR_CASE(8) DR_CASE(16) DR_CASE(32)
+#undef DR_CASE
+    default: fail("bad lanes-per-row");
+  }
+  DR_CK(cudaGetLastError());
+}
+
+template <typename TA, class XL, class EP>
+void launch_rows(cudaStream_t st, int max_grid, const DevMat& M, const TA* av, XL xl, EP ep) {
+  launch_rows_impl<TA, XL, EP, false, FinStore>(st, max_grid, M.G, M.n, M.rp, M.ci, av, xl, ep, nullptr,
+                                                nullptr, FinStore{nullptr});
+}
+
+template <typename TA, class XL, class EP, class Fin>
+void launch_rows_dot(cudaStream_t st, int max_grid, const DevMat& M, const TA* av, XL xl, EP ep,
+                     double* partials, unsigned* ticket, Fin fin) {
+  launch_rows_impl<TA, XL, EP, true, Fin>(st, max_grid, M.G, M.n, M.rp, M.ci, av, xl, ep, partials,
+                                          ticket, fin);
+}
+
+int grid1d(long long n, int max_grid) {
+  return (int)std::max<long long>(1, std::min<long long>((n + kBlock - 1) / kBlock, max_grid));
+}
+
+// Finalizer writing the same total to two places (r·z and its "old" copy).
+struct FinStore2 {
+  double* a;
+  double* b;
+  __device__ void operator()(double s) const {
+    *a = s;
+    *b = s;
+  }
+};
+
+// ticket slots
+enum : int { TK_DOT = 0, TK_RES = 1, TK_PQ = 2, TK_UPD = 3, TK_RZ = 4, TK_N = 8 };
+// scalar slots
+enum : int { SC_BB = 0, SC_RR = 1, SC_RZ = 2, SC_RZOLD = 3, SC_PQ = 4, SC_TMP = 5, SC_N = 8 };
+
+}  // namespace
+
+template <typename T>
+T* DevHier::alloc(size_t n) {
+  void* p = nullptr;
+  size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+  DR_CK(cudaMalloc(&p, bytes));
+  allocs_.push_back(p);
+  bytes_ += bytes;
+  return (T*)p;
+}
+
+template <typename T>
+static void h2d(T* d, const std::vector<T>& h, cudaStream_t st) {
+  if (!h.empty()) DR_CK(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+}
+
+DevHier::DevHier(const HostHierarchy& H, int device) {
+  device_ = device;
+  DR_CK(cudaSetDevice(device));
+  DR_CK(cudaDeviceGetAttribute(&nsm_, cudaDevAttrMultiProcessorCount, device));
+  max_grid_ = nsm_ * 8;
+  DR_CK(cudaStreamCreateWithFlags(&own_st_, cudaStreamNonBlocking));
+  st_ = own_st_;
+  own_stream_ = true;
+  DR_CK(cudaEventCreateWithFlags(&ev_[0], cudaEventDisableTiming));
+  DR_CK(cudaEventCreateWithFlags(&ev_[1], cudaEventDisableTiming));
+  try {
+    const int nl = (int)H.levels.size();
+    n0_ = nl ? H.levels[0].A.n : H.nc;
+    nnz0_ = nl ? H.levels[0].A.nnz() : H.coarse.nnz();
+    L_.resize(nl);
+    auto up_csr = [&](DevMat& M, int n, int m, const std::vector<int>& rp, const std::vector<int>& ci,
+                      const std::vector<double>* v) {
+      M.n = n;
+      M.m = m;
+      M.nnz = (long long)ci.size();
+      M.rp = alloc<int>(rp.size());
+      M.ci = alloc<int>(ci.size());
+      h2d(M.rp, rp, st_);
+      h2d(M.ci, ci, st_);
+      M.v = alloc<double>(ci.size());
+      if (v) h2d(M.v, *v, st_);
+      M.G = pick_G(M.nnz, n);
+    };
+    for (int l = 0; l < nl; ++l) {
+      const HostLevel& h = H.levels[l];
+      DevLevel& d = L_[l];
+      up_csr(d.A, h.A.n, h.A.m, h.A.rp, h.A.ci, &h.A.v);
+      up_csr(d.P, h.P.nf, h.P.nc, h.P.rp, h.P.ci, &h.P.v);
+      up_csr(d.R, h.P.nc, h.P.nf, h.T.off, h.T.rows, &h.Rv);
+      d.smoother = h.smoother;
+      d.omega = h.omega;
+      d.invd = alloc<double>(h.A.n);
+      h2d(d.invd, h.invdiag, st_);
+      d.ncolors = h.num_colors;
+      d.color_off = h.color_off;
+      if (h.num_colors > 0) {
+        d.color_order = alloc<int>(h.color_order.size());
+        h2d(d.color_order, h.color_order, st_);
+      }
+      d.has_rap = h.has_rap_map;
+      if (d.has_rap) {
+        up_csr(d.AP, h.A.n, h.P.nc, h.ap_rp, h.ap_ci, nullptr);
+        d.AP.G = 8;
+      }
+      const int n = h.A.n;
+      if (l > 0) {
+        d.v64.xa = alloc<double>(n);
+        d.v64.b = alloc<double>(n);
+      }
+      d.v64.xb = alloc<double>(n);
+      d.v64.r = alloc<double>(n);
+    }
+    nc_ = H.nc;
+    up_csr(C_, H.coarse.n, H.coarse.m, H.coarse.rp, H.coarse.ci, &H.coarse.v);
+    cdense_ = alloc<double>((size_t)nc_ * nc_);
+    clu_ = alloc<double>((size_t)nc_ * nc_);
+    cpiv_ = alloc<int>(nc_);
+    info_ = alloc<int>(1);
+    h2d(cdense_, H.coarse_dense, st_);
+    h2d(clu_, H.coarse_lu, st_);
+    h2d(cpiv_, H.coarse_piv, st_);
+    cb64_ = alloc<double>(nc_);
+    cx64_ = alloc<double>(nc_);
+    partials_ = alloc<double>(max_grid_ + 32);
+    tickets_ = alloc<unsigned>(TK_N);
+    DR_CK(cudaMemsetAsync(tickets_, 0, TK_N * sizeof(unsigned), st_));
+    scal_ = alloc<double>(SC_N);
+    DR_CK(cudaMemsetAsync(scal_, 0, SC_N * sizeof(double), st_));
+    DR_CK(cudaMallocHost(&hscal_, SC_N * sizeof(double)));
+    xd_ = alloc<double>(n0_);
+    bd_ = alloc<double>(n0_);
+    if ((size_t)nc_ * sizeof(double) > 48 * 1024) {
+      size_t need = (size_t)nc_ * sizeof(double);
+      if (need > 200 * 1024) fail("coarsest level too large for the on-chip LU solve (n_c = " + std::to_string(nc_) + ")");
+      DR_CK(cudaFuncSetAttribute(k_lu_solve<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+      DR_CK(cudaFuncSetAttribute(k_lu_solve<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+    }
+    DR_CK(cudaStreamSynchronize(st_));
+  } catch (...) {
+    for (void* p : allocs_) cudaFree(p);
+    allocs_.clear();
+    if (hscal_) cudaFreeHost(hscal_);
+    cudaEventDestroy(ev_[0]);
+    cudaEventDestroy(ev_[1]);
+    cudaStreamDestroy(own_st_);
+    throw;
+  }
+}
+
+DevHier::~DevHier() {
+  cudaSetDevice(device_);
+  if (st_) cudaStreamSynchronize(st_);
+  graphs_clear();
+  for (void* p : allocs_) cudaFree(p);
+  if (hscal_) cudaFreeHost(hscal_);
+  cudaEventDestroy(ev_[0]);
+  cudaEventDestroy(ev_[1]);
+  if (own_stream_ && own_st_) cudaStreamDestroy(own_st_);
+}
+
+void DevHier::set_stream(cudaStream_t s) {
+  DR_CK(cudaStreamSynchronize(st_));
+  st_ = s ? s : own_st_;
+  graphs_clear();
+}
+
+void DevHier::graphs_clear() {
+  for (int i = 0; i < 2; ++i)
+    if (pg_.g1[i]) { cudaGraphExecDestroy(pg_.g1[i]); pg_.g1[i] = nullptr; }
+  if (pg_.g2) { cudaGraphExecDestroy(pg_.g2); pg_.g2 = nullptr; }
+  pg_.valid = false;
+}
+
+// ------------------------------------------------------------ typed accessors
+template <> LevelVecs<double>& DevHier::vecs<double>(int l) { return L_[l].v64; }
+template <> LevelVecs<float>& DevHier::vecs<float>(int l) { return L_[l].v32; }
+template <> double* DevHier::coarse_b<double>() { return cb64_; }
+template <> float* DevHier::coarse_b<float>() { return cb32_; }
+template <> double* DevHier::coarse_x<double>() { return cx64_; }
+template <> float* DevHier::coarse_x<float>() { return cx32_; }
+template <> const double* DevHier::mval<double>(const DevMat& M) const { return M.v; }
+template <> const float* DevHier::mval<float>(const DevMat& M) const { return M.v32; }
+template <> const double* DevHier::invd<double>(const DevLevel& L) const { return L.invd; }
+template <> const float* DevHier::invd<float>(const DevLevel& L) const { return L.invd32; }
+
+// ------------------------------------------------------------ FP32 copies
+void DevHier::ensure_fp32() {
+  if (fp32_) return;
+  graphs_clear();
+  for (auto& d : L_) {
+    d.A.v32 = alloc<float>(d.A.nnz);
+    d.P.v32 = alloc<float>(d.P.nnz);
+    d.R.v32 = alloc<float>(d.R.nnz);
+    d.invd32 = alloc<float>(d.A.n);
+    const int n = d.A.n;
+    d.v32.xa = alloc<float>(n);
+    d.v32.xb = alloc<float>(n);
+    d.v32.b = alloc<float>(n);
+    d.v32.r = alloc<float>(n);
+  }
+  cb32_ = alloc<float>(nc_);
+  cx32_ = alloc<float>(nc_);
+  fp32_ = true;
+  refresh_fp32();
+}
+
+void DevHier::refresh_fp32() {
+  if (!fp32_) return;
+  for (auto& d : L_) {
+    counted();
+    k_convert<double, float><<<grid1d(d.A.nnz, max_grid_), kBlock, 0, st_>>>(d.A.nnz, d.A.v, d.A.v32);
+    counted();
+    k_convert<double, float><<<grid1d(d.P.nnz, max_grid_), kBlock, 0, st_>>>(d.P.nnz, d.P.v, d.P.v32);
+    counted();
+    k_convert<double, float><<<grid1d(d.R.nnz, max_grid_), kBlock, 0, st_>>>(d.R.nnz, d.R.v, d.R.v32);
+    counted();
+    k_convert<double, float><<<grid1d(d.A.n, max_grid_), kBlock, 0, st_>>>(d.A.n, d.invd, d.invd32);
+  }
+  DR_CK(cudaGetLastError());
+}
+
+// ------------------------------------------------------------ cycle pieces
+template <typename T>
+T* DevHier::smooth(int l, T* x, const T* b, int steps, T* ext) {
+  DevLevel& L = L_[l];
+  LevelVecs<T>& V = vecs<T>(l);
+  const DevMat& A = L.A;
+  const T om = (T)L.omega;
+  if (L.smoother == SmootherKind::Jacobi || L.smoother == SmootherKind::L1Jacobi) {
+    for (int s = 0; s < steps; ++s) {
+      T* dst = (l == 0) ? (x == V.xb ? ext : V.xb) : (x == V.xa ? V.xb : V.xa);
+      launch_rows(st_, max_grid_, A, mval<T>(A), XPlain<T>{x},
+                  EpJacobi<T>{x, b, invd<T>(L), dst, om, nullptr});
+      x = dst;
+    }
+  } else {
+    for (int s = 0; s < steps; ++s)
+      for (int c = 0; c < L.ncolors; ++c) {
+        const int off = L.color_off[c];
+        const int cnt = L.color_off[c + 1] - off;
+        if (cnt == 0) continue;
+        const int grid = (int)std::max<long long>(1, std::min<long long>(((long long)cnt * A.G + kBlock - 1) / kBlock, max_grid_));
+        counted();
+        switch (A.G) {
+#define DR_CASE(g)                                                                                  \
+  case g:                                                                                           \
+    k_gs_color<g, T><<<grid, kBlock, 0, st_>>>(cnt, L.color_order + off, A.rp, A.ci, mval<T>(A), b, \
+                                               invd<T>(L), x);                                      \
+    break;
+          DR_CASE(1) DR_CASE(2) DR_CASE(4) DR_CASE(8) DR_CASE(16) DR_CASE(32)
+#undef DR_CASE
+        }
+        DR_CK(cudaGetLastError());
+      }
+  }
+  return x;
+}
+
+template <typename T>
+void DevHier::residual(int l, const T* x, const T* b, T* r, double* rr_dst) {
+  const DevMat& A = l < nlevels() ? L_[l].A : C_;
+  if (rr_dst)
+    launch_rows_dot(st_, max_grid_, A, mval<T>(A), XPlain<T>{x}, EpResidual<T>{b, r}, partials_,
+                    tickets_ + TK_RES, FinStore{rr_dst});
+  else
+    launch_rows(st_, max_grid_, A, mval<T>(A), XPlain<T>{x}, EpResidual<T>{b, r});
+}
+
+template <typename T>
+void DevHier::coarse_solve(const T* b, T* x) {
+  int threads = 32;
+  while (threads < nc_ && threads < 1024) threads *= 2;
+  counted();
+  k_lu_solve<T><<<1, threads, (size_t)std::max(nc_, 1) * sizeof(double), st_>>>(nc_, clu_, cpiv_, b, x);
+  DR_CK(cudaGetLastError());
+}
+
+template <typename T>
+T* DevHier::cycle_level(int l, T* x, const T* b, bool x_zero, const CycleOpts& o, T* ext) {
+  DevLevel& L = L_[l];
+  LevelVecs<T>& V = vecs<T>(l);
+  const DevMat& A = L.A;
+  const T om = (T)L.omega;
+  const bool jac = (L.smoother == SmootherKind::Jacobi || L.smoother == SmootherKind::L1Jacobi);
+  bool have_r = false;
+  // pre-smoothing
+  if (x_zero && jac && o.pre >= 1) {
+    if (o.pre == 1) {
+      launch_rows(st_, max_grid_, A, mval<T>(A), XZeroJacobi<T>{b, invd<T>(L), om},
+                  EpZeroJacobiResidual<T>{b, invd<T>(L), x, V.r, om});
+      have_r = true;
+    } else {
+      counted();
+      k_scale_jacobi_zero<T><<<grid1d(A.n, max_grid_), kBlock, 0, st_>>>(A.n, b, invd<T>(L), om, x);
+      DR_CK(cudaGetLastError());
+      x = smooth<T>(l, x, b, o.pre - 1, ext);
+    }
+  } else {
+    if (x_zero) {
+      counted();
+      k_fill<T><<<grid1d(A.n, max_grid_), kBlock, 0, st_>>>(A.n, T(0), x);
+      DR_CK(cudaGetLastError());
+    }
+    x = smooth<T>(l, x, b, o.pre, ext);
+  }
+  if (!have_r) residual<T>(l, x, b, V.r, nullptr);
+  // restriction  b_{l+1} = Pᵀ r
+  const bool last = (l + 1 == nlevels());
+  T* bn = last ? coarse_b<T>() : vecs<T>(l + 1).b;
+  launch_rows(st_, max_grid_, L.R, mval<T>(L.R), XPlain<T>{V.r}, EpStore<T>{bn});
+  // coarse-grid correction
+  T* xn;
+  if (!last) {
+    xn = vecs<T>(l + 1).xa;
+    xn = cycle_level<T>(l + 1, xn, bn, true, o, nullptr);
+    if (o.w) xn = cycle_level<T>(l + 1, xn, bn, false, o, nullptr);
+  } else {
+    xn = coarse_x<T>();
+    coarse_solve<T>(bn, xn);
+  }
+  // prolongation and correction  x += P xc
+  launch_rows(st_, max_grid_, L.P, mval<T>(L.P), XPlain<T>{xn}, EpAddTo<T>{x});
+  // post-smoothing
+  x = smooth<T>(l, x, b, o.post, ext);
+  return x;
+}
+
+void DevHier::cycle(double* x, const double* b, const CycleOpts& o) {
+  if (L_.empty()) {
+    coarse_solve<double>(b, x);
+    return;
+  }
+  double* xo = cycle_level<double>(0, x, b, false, o, x);
+  if (xo != x) DR_CK(cudaMemcpyAsync(x, xo, (size_t)n0_ * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+}
+
+double DevHier::dot_host(const double* a, const double* b, int n) {
+  counted();
+  k_dot<double, double, FinStore><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, a, b, partials_, tickets_ + TK_DOT,
+                                                                           FinStore{scal_ + SC_TMP});
+  DR_CK(cudaGetLastError());
+  DR_CK(cudaMemcpyAsync(hscal_ + SC_TMP, scal_ + SC_TMP, sizeof(double), cudaMemcpyDeviceToHost, st_));
+  DR_CK(cudaStreamSynchronize(st_));
+  return hscal_[SC_TMP];
+}
+
+int DevHier::solve(double* x, const double* b, const CycleOpts& o, double tol, int maxiter, int verbose,
+                   double* relres) {
+  const double bnorm = std::sqrt(dot_host(b, b, n0_));
+  if (bnorm == 0.0) {
+    counted();
+    k_fill<double><<<grid1d(n0_, max_grid_), kBlock, 0, st_>>>(n0_, 0.0, x);
+    DR_CK(cudaStreamSynchronize(st_));
+    if (relres) *relres = 0.0;
+    return 0;
+  }
+  if (L_.empty()) {
+    coarse_solve<double>(b, x);
+    DR_CK(cudaStreamSynchronize(st_));
+    if (relres) *relres = NAN;
+    return 1;
+  }
+  double* r = L_[0].v64.r;
+  double rel = 1.0;
+  for (int it = 1; it <= maxiter; ++it) {
+    cycle(x, b, o);
+    residual<double>(0, x, b, r, scal_ + SC_RR);
+    DR_CK(cudaMemcpyAsync(hscal_ + SC_RR, scal_ + SC_RR, sizeof(double), cudaMemcpyDeviceToHost, st_));
+    DR_CK(cudaStreamSynchronize(st_));
+    const double rnorm = std::sqrt(hscal_[SC_RR]);
+    rel = rnorm / bnorm;
+    if (verbose >= 2) std::printf("  AMG iter %4d: residual norm = %.6e, relative = %.6e\n", it, rnorm, rel);
+    if (rel < tol) {
+      if (verbose >= 1) std::printf("AMG solve converged: %d iterations, final residual %.2e\n", it, rel);
+      if (relres) *relres = rel;
+      return it;
+    }
+  }
+  if (verbose >= 1) std::printf("AMG solve did NOT converge: %d iterations, final residual %.2e\n", maxiter, rel);
+  if (relres) *relres = rel;
+  return maxiter;
+}
+
+// ------------------------------------------------------------ PCG
+// Preconditioned conjugate gradients around one AMG cycle per iteration
+// (x of the cycle zeroed, as preconditioner_apply! does,
+// src/preconditioner.jl:76-80).  Outer vectors, products with A and dot
+// products are FP64; with `mixed` the cycle runs on FP32 copies of the
+// hierarchy values and vectors.  Per iteration:
+//   K1  q = A p,  p = z + β p_old (on the fly),  p·q       (one pass over A)
+//   K2  x += α p, r -= α q, r·r (and the FP32 copy of r)    (one vector pass)
+//   M   z = M r                                              (the cycle)
+//   D   r·z                                                  (one vector pass)
+// K1+K2 and M+D are captured once as CUDA graphs; the host reads r·r of
+// iteration k while the preconditioner of iteration k runs.
+int DevHier::pcg(double* x, const double* b, const CycleOpts& o, double tol, int maxiter, bool mixed,
+                 double* relres, int verbose) {
+  if (mixed) ensure_fp32();
+  if (!pr_) {
+    pr_ = alloc<double>(n0_);
+    pp_[0] = alloc<double>(n0_);
+    pp_[1] = alloc<double>(n0_);
+    pq_ = alloc<double>(n0_);
+    pz_ = alloc<double>(n0_);
+  }
+  if (mixed && !pr32_) {
+    pr32_ = alloc<float>(n0_);
+    pz32_ = alloc<float>(n0_);
+  }
+  if (pg_.valid && (pg_.mixed != mixed || pg_.o.pre != o.pre || pg_.o.post != o.post || pg_.o.w != o.w))
+    graphs_clear();
+  const DevMat& A = L_.empty() ? C_ : L_[0].A;
+  const int n = n0_;
+  double* X = xd_;
+  if (x != X) DR_CK(cudaMemcpyAsync(X, x, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+  // r = b - A x, r·r ;  b·b
+  residual<double>(0, X, b, pr_, scal_ + SC_RR);
+  counted();
+  k_dot<double, double, FinStore><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, b, b, partials_, tickets_ + TK_DOT,
+                                                                           FinStore{scal_ + SC_BB});
+  DR_CK(cudaGetLastError());
+  DR_CK(cudaMemcpyAsync(hscal_, scal_, 2 * sizeof(double), cudaMemcpyDeviceToHost, st_));
+  DR_CK(cudaStreamSynchronize(st_));
+  const double bnorm = std::sqrt(hscal_[SC_BB]);
+  if (bnorm == 0.0) {
+    counted();
+    k_fill<double><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, 0.0, x);
+    DR_CK(cudaStreamSynchronize(st_));
+    if (relres) *relres = 0.0;
+    return 0;
+  }
+  double rel = std::sqrt(hscal_[SC_RR]) / bnorm;
+  if (rel < tol) {
+    if (x != X) DR_CK(cudaMemcpyAsync(x, X, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+    DR_CK(cudaStreamSynchronize(st_));
+    if (relres) *relres = rel;
+    return 0;
+  }
+  // z = M r (the cycle writes where it ends; the location is the same for
+  // every application with the same options)
+  void* zptr = nullptr;
+  auto precond = [&](bool rz_first) {
+    if (mixed) {
+      if (L_.empty()) {
+        counted();
+        k_convert<double, float><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, pr_, pr32_);
+        coarse_solve<float>(pr32_, pz32_);
+        zptr = pz32_;
+      } else {
+        zptr = cycle_level<float>(0, pz32_, pr32_, true, o, pz32_);
+      }
+      counted();
+      if (rz_first)
+        k_dot<double, float, FinStore2><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(
+            n, pr_, (const float*)zptr, partials_, tickets_ + TK_RZ, FinStore2{scal_ + SC_RZ, scal_ + SC_RZOLD});
+      else
+        k_dot<double, float, FinShift><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(
+            n, pr_, (const float*)zptr, partials_, tickets_ + TK_RZ, FinShift{scal_ + SC_RZ, scal_ + SC_RZOLD});
+    } else {
+      if (L_.empty()) {
+        coarse_solve<double>(pr_, pz_);
+        zptr = pz_;
+      } else {
+        zptr = cycle_level<double>(0, pz_, pr_, true, o, pz_);
+      }
+      counted();
+      if (rz_first)
+        k_dot<double, double, FinStore2><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(
+            n, pr_, (const double*)zptr, partials_, tickets_ + TK_RZ, FinStore2{scal_ + SC_RZ, scal_ + SC_RZOLD});
+      else
+        k_dot<double, double, FinShift><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(
+            n, pr_, (const double*)zptr, partials_, tickets_ + TK_RZ, FinShift{scal_ + SC_RZ, scal_ + SC_RZOLD});
+    }
+    DR_CK(cudaGetLastError());
+  };
+  if (mixed) {
+    counted();
+    k_convert<double, float><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, pr_, pr32_);
+  }
+  precond(true);
+  counted();
+  k_fill<double><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, 0.0, pp_[0]);
+  DR_CK(cudaGetLastError());
+  auto k1k2 = [&](int par) {
+    double* pold = pp_[par];
+    double* pnew = pp_[par ^ 1];
+    if (mixed) {
+      XPcgDir<float> dir{(const float*)zptr, pold, scal_ + SC_RZ, 0};
+      launch_rows_dot(st_, max_grid_, A, A.v, dir, EpPcgDir<float>{dir, pnew, pq_}, partials_,
+                      tickets_ + TK_PQ, FinStore{scal_ + SC_PQ});
+      counted();
+      k_pcg_update<float><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, X, pr_, pnew, pq_, scal_ + SC_RZ,
+                                                                    scal_ + SC_PQ, pr32_, partials_,
+                                                                    tickets_ + TK_UPD, FinStore{scal_ + SC_RR});
+    } else {
+      XPcgDir<double> dir{(const double*)zptr, pold, scal_ + SC_RZ, 0};
+      launch_rows_dot(st_, max_grid_, A, A.v, dir, EpPcgDir<double>{dir, pnew, pq_}, partials_,
+                      tickets_ + TK_PQ, FinStore{scal_ + SC_PQ});
+      counted();
+      k_pcg_update<float><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, X, pr_, pnew, pq_, scal_ + SC_RZ,
+                                                                    scal_ + SC_PQ, nullptr, partials_,
+                                                                    tickets_ + TK_UPD, FinStore{scal_ + SC_RR});
+    }
+    DR_CK(cudaGetLastError());
+    DR_CK(cudaMemcpyAsync(hscal_ + SC_RR, scal_ + SC_RR, sizeof(double), cudaMemcpyDeviceToHost, st_));
+  };
+  // capture the iteration graphs once per option set
+  if (!pg_.valid) {
+    for (int par = 0; par < 2; ++par) {
+      cudaGraph_t g;
+      const long long c0 = g_launches.load();
+      DR_CK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+      k1k2(par);
+      DR_CK(cudaStreamEndCapture(st_, &g));
+      pg_.n1[par] = g_launches.load() - c0;
+      g_launches.fetch_sub(pg_.n1[par]);
+      DR_CK(cudaGraphInstantiate(&pg_.g1[par], g, 0));
+      cudaGraphDestroy(g);
+    }
+    cudaGraph_t g;
+    const long long c0 = g_launches.load();
+    DR_CK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+    precond(false);
+    DR_CK(cudaStreamEndCapture(st_, &g));
+    pg_.n2 = g_launches.load() - c0;
+    g_launches.fetch_sub(pg_.n2);
+    DR_CK(cudaGraphInstantiate(&pg_.g2, g, 0));
+    cudaGraphDestroy(g);
+    pg_.valid = true;
+    pg_.mixed = mixed;
+    pg_.o = o;
+  }
+  int it = 1;
+  for (; it <= maxiter; ++it) {
+    const int par = (it - 1) & 1;
+    DR_CK(cudaGraphLaunch(pg_.g1[par], st_));
+    g_launches.fetch_add(pg_.n1[par]);
+    DR_CK(cudaEventRecord(ev_[par], st_));
+    const bool more = it < maxiter;
+    if (more) {
+      DR_CK(cudaGraphLaunch(pg_.g2, st_));
+      g_launches.fetch_add(pg_.n2);
+    }
+    DR_CK(cudaEventSynchronize(ev_[par]));
+    rel = std::sqrt(hscal_[SC_RR]) / bnorm;
+    if (verbose >= 2) std::printf("  PCG iter %4d: relative residual = %.6e\n", it, rel);
+    if (rel < tol || !more) break;
+  }
+  if (it > maxiter) it = maxiter;
+  if (x != X) DR_CK(cudaMemcpyAsync(x, X, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+  DR_CK(cudaStreamSynchronize(st_));
+  if (verbose >= 1)
+    std::printf("AMG-PCG (%s cycle) %s: %d iterations, final residual %.2e\n", mixed ? "FP32" : "FP64",
+                rel < tol ? "converged" : "did NOT converge", it, rel);
+  if (relres) *relres = rel;
+  return it;
+}
+
+// ------------------------------------------------------------ resetup
+void DevHier::resetup_values(const double* v_dev) {
+  const int nl = nlevels();
+  for (int l = 0; l < nl; ++l)
+    if (!L_[l].has_rap)
+      fail("partial resetup needs the Galerkin maps; set up the hierarchy with allow_partial_resetup=1");
+  graphs_clear();
+  if (nl == 0) {
+    DR_CK(cudaMemcpyAsync(C_.v, v_dev, (size_t)C_.nnz * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+  } else {
+    DR_CK(cudaMemcpyAsync(L_[0].A.v, v_dev, (size_t)L_[0].A.nnz * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+  }
+  auto upd_invd = [&](DevLevel& d) {
+    counted();
+    if (d.smoother == SmootherKind::L1Jacobi || d.smoother == SmootherKind::L1ColoredGS)
+      k_l1_invdiag<<<grid1d(d.A.n, max_grid_), kBlock, 0, st_>>>(d.A.n, d.A.rp, d.A.v, d.invd);
+    else
+      k_invdiag<<<grid1d(d.A.n, max_grid_), kBlock, 0, st_>>>(d.A.n, d.A.rp, d.A.ci, d.A.v, d.invd);
+    DR_CK(cudaGetLastError());
+  };
+  if (nl > 0) upd_invd(L_[0]);
+  for (int l = 0; l < nl; ++l) {
+    DevLevel& d = L_[l];
+    DevMat& next = (l + 1 < nl) ? L_[l + 1].A : C_;
+    {
+      const int grid = std::max(1, std::min((d.A.n + (kBlock / 8) - 1) / (kBlock / 8), max_grid_));
+      counted();
+      k_spgemm_rows<8, 120><<<grid, kBlock, 0, st_>>>(d.AP.n, d.AP.rp, d.AP.ci, d.AP.v, d.A.rp, d.A.ci,
+                                                      d.A.v, d.P.rp, d.P.ci, d.P.v);
+      DR_CK(cudaGetLastError());
+    }
+    {
+      const int grid = std::max(1, std::min((next.n + (kBlock / 32) - 1) / (kBlock / 32), max_grid_));
+      counted();
+      k_spgemm_rows<32, 500><<<grid, kBlock, 0, st_>>>(next.n, next.rp, next.ci, next.v, d.R.rp, d.R.ci,
+                                                       d.R.v, d.AP.rp, d.AP.ci, d.AP.v);
+      DR_CK(cudaGetLastError());
+    }
+    if (l + 1 < nl) upd_invd(L_[l + 1]);
+  }
+  // coarsest dense matrix and its LU
+  DR_CK(cudaMemsetAsync(cdense_, 0, (size_t)nc_ * nc_ * sizeof(double), st_));
+  counted();
+  k_csr_to_dense<<<grid1d(nc_, max_grid_), kBlock, 0, st_>>>(nc_, C_.rp, C_.ci, C_.v, cdense_);
+  DR_CK(cudaMemcpyAsync(clu_, cdense_, (size_t)nc_ * nc_ * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+  int threads = 32;
+  while (threads < nc_ && threads < 1024) threads *= 2;
+  counted();
+  k_lu_factor<<<1, threads, 0, st_>>>(nc_, clu_, cpiv_, info_);
+  DR_CK(cudaGetLastError());
+  refresh_fp32();
+  int info = 0;
+  DR_CK(cudaMemcpyAsync(&info, info_, sizeof(int), cudaMemcpyDeviceToHost, st_));
+  DR_CK(cudaStreamSynchronize(st_));
+  if (info != 0) fail("SingularException(" + std::to_string(info) + ")");
+}
+
+// ------------------------------------------------------------ level ops
+void DevHier::level_op(int lvl, int op, bool fp32, const double* in1, const double* in2, double* out,
+                       int steps) {
+  const int nl = nlevels();
+  if (op != 5 && (lvl < 0 || lvl >= nl)) fail("level index out of range");
+  if (fp32) ensure_fp32();
+  const int n = op == 5 ? nc_ : L_[lvl].A.n;
+  const int ncn = op == 5 ? nc_ : (lvl + 1 < nl ? L_[lvl + 1].A.n : nc_);
+  auto run = [&](auto tag) {
+    using T = decltype(tag);
+    LevelVecs<T>& V = vecs<T>(op == 5 ? 0 : lvl);
+    auto to_t = [&](const double* s, T* d, int m) {
+      counted();
+      k_convert<double, T><<<grid1d(m, max_grid_), kBlock, 0, st_>>>(m, s, d);
+    };
+    auto from_t = [&](const T* s, double* d, int m) {
+      counted();
+      k_convert<T, double><<<grid1d(m, max_grid_), kBlock, 0, st_>>>(m, s, d);
+    };
+    // staging buffers in T: use level vectors (xa may be null at level 0)
+    T* bufA = V.xb;
+    T* bufB = V.r;
+    switch (op) {
+      case 0: {  // y = A x
+        to_t(in1, bufA, n);
+        const DevMat& A = L_[lvl].A;
+        launch_rows(st_, max_grid_, A, mval<T>(A), XPlain<T>{bufA}, EpStore<T>{bufB});
+        from_t(bufB, out, n);
+        break;
+      }
+      case 1: {  // r = b - A x   (third buffer: level rhs, or the PCG z at level 0)
+        T* tb = lvl > 0 ? V.b : nullptr;
+        if (!tb) {
+          if constexpr (sizeof(T) == 8) { if (!pz_) pz_ = alloc<double>(n0_); tb = (T*)pz_; }
+          else { if (!pz32_) pz32_ = alloc<float>(n0_); tb = (T*)pz32_; }
+        }
+        to_t(in1, bufA, n);
+        to_t(in2, tb, n);
+        residual<T>(lvl, bufA, tb, bufB, nullptr);
+        from_t(bufB, out, n);
+        break;
+      }
+      case 2: {  // smoothing sweeps from x with rhs b (lvl >= 1: xa/b; lvl 0: xb + z)
+        T* tb;
+        T* x0;
+        T* ext;
+        if (lvl > 0) {
+          tb = V.b;
+          x0 = V.xa;
+          ext = nullptr;
+        } else {
+          if constexpr (sizeof(T) == 8) { if (!pz_) pz_ = alloc<double>(n0_); tb = (T*)pz_; }
+          else { if (!pz32_) pz32_ = alloc<float>(n0_); tb = (T*)pz32_; }
+          x0 = V.r;   // caller-side x
+          ext = V.r;
+        }
+        to_t(in1, x0, n);
+        to_t(in2, tb, n);
+        T* xr = smooth<T>(lvl, x0, tb, steps, ext);
+        from_t(xr, out, n);
+        break;
+      }
+      case 3: {  // bc = Pᵀ r
+        to_t(in1, bufB, n);
+        T* bc = (lvl + 1 < nl) ? vecs<T>(lvl + 1).b : coarse_b<T>();
+        launch_rows(st_, max_grid_, L_[lvl].R, mval<T>(L_[lvl].R), XPlain<T>{bufB}, EpStore<T>{bc});
+        from_t(bc, out, ncn);
+        break;
+      }
+      case 4: {  // x += P xc
+        T* xc = (lvl + 1 < nl) ? vecs<T>(lvl + 1).b : coarse_b<T>();
+        to_t(in1, bufA, n);
+        to_t(in2, xc, ncn);
+        launch_rows(st_, max_grid_, L_[lvl].P, mval<T>(L_[lvl].P), XPlain<T>{xc}, EpAddTo<T>{bufA});
+        from_t(bufA, out, n);
+        break;
+      }
+      case 5: {  // coarsest solve
+        to_t(in1, coarse_b<T>(), nc_);
+        coarse_solve<T>(coarse_b<T>(), coarse_x<T>());
+        from_t(coarse_x<T>(), out, nc_);
+        break;
+      }
+      case 6: {  // first Jacobi step from zero fused with the residual: out = [x1, r]
+        const DevLevel& L = L_[lvl];
+        T* tb;
+        if (lvl > 0) tb = V.b;
+        else {
+          if constexpr (sizeof(T) == 8) { if (!pz_) pz_ = alloc<double>(n0_); tb = (T*)pz_; }
+          else { if (!pz32_) pz32_ = alloc<float>(n0_); tb = (T*)pz32_; }
+        }
+        to_t(in1, tb, n);
+        const T om = (T)L.omega;
+        launch_rows(st_, max_grid_, L.A, mval<T>(L.A), XZeroJacobi<T>{tb, invd<T>(L), om},
+                    EpZeroJacobiResidual<T>{tb, invd<T>(L), bufA, bufB, om});
+        from_t(bufA, out, n);
+        from_t(bufB, out + n, n);
+        break;
+      }
+      default:
+        fail("unknown level op");
+    }
+    DR_CK(cudaGetLastError());
+  };
+  if (fp32) run(float());
+  else run(double());
+  DR_CK(cudaStreamSynchronize(st_));
+}
+
+float DevHier::time_level_op(int lvl, int op, bool fp32, int reps) {
+  if (lvl < 0 || lvl >= nlevels()) fail("level index out of range");
+  if (fp32) ensure_fp32();
+  cudaEvent_t e0, e1;
+  DR_CK(cudaEventCreate(&e0));
+  DR_CK(cudaEventCreate(&e1));
+  float ms = 0.f;
+  auto run = [&](auto tag) {
+    using T = decltype(tag);
+    DevLevel& L = L_[lvl];
+    LevelVecs<T>& V = vecs<T>(lvl);
+    const int n = L.A.n;
+    T* x0 = lvl > 0 ? V.xa : V.r;
+    T* x1 = V.xb;
+    T* b = lvl > 0 ? V.b : V.r;
+    counted();
+    k_fill<T><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, T(1), x0);
+    if (lvl > 0) {
+      counted();
+      k_fill<T><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, T(1), b);
+    }
+    const T om = (T)L.omega;
+    auto once = [&]() {
+      if (op == 2)
+        launch_rows(st_, max_grid_, L.A, mval<T>(L.A), XPlain<T>{x0}, EpJacobi<T>{x0, b, invd<T>(L), x1, om, nullptr});
+      else
+        launch_rows(st_, max_grid_, L.A, mval<T>(L.A), XPlain<T>{x0}, EpStore<T>{x1});
+    };
+    for (int w = 0; w < 3; ++w) once();
+    DR_CK(cudaEventRecord(e0, st_));
+    for (int r = 0; r < reps; ++r) once();
+    DR_CK(cudaEventRecord(e1, st_));
+    DR_CK(cudaEventSynchronize(e1));
+    DR_CK(cudaEventElapsedTime(&ms, e0, e1));
+  };
+  if (fp32) run(float());
+  else run(double());
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return ms / reps;
+}
+
+void DevHier::export_values(int lvl, const std::string& what, std::vector<double>& out) const {
+  const double* src = nullptr;
+  long long n = 0;
+  if (lvl == -1) {
+    if (what == "C_nzval") { src = C_.v; n = C_.nnz; }
+    else if (what == "C_lu") { src = clu_; n = (long long)nc_ * nc_; }
+    else if (what == "C_dense") { src = cdense_; n = (long long)nc_ * nc_; }
+  } else {
+    const DevLevel& d = L_.at(lvl);
+    if (what == "A_nzval") { src = d.A.v; n = d.A.nnz; }
+    else if (what == "P_nzval") { src = d.P.v; n = d.P.nnz; }
+    else if (what == "invdiag") { src = d.invd; n = d.A.n; }
+    else if (what == "AP_nzval" && d.has_rap) { src = d.AP.v; n = d.AP.nnz; }
+  }
+  if (!src) fail("unknown device export: " + what);
+  out.resize(n);
+  DR_CK(cudaMemcpyAsync(out.data(), src, n * sizeof(double), cudaMemcpyDeviceToHost, st_));
+  DR_CK(cudaStreamSynchronize(st_));
+}
+
+void DevHier::export_piv(std::vector<int>& out) const {
+  out.resize(nc_);
+  DR_CK(cudaMemcpyAsync(out.data(), cpiv_, (size_t)nc_ * sizeof(int), cudaMemcpyDeviceToHost, st_));
+  DR_CK(cudaStreamSynchronize(st_));
+}
+
+}  // namespace dr

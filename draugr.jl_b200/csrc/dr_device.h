@@ -1,0 +1,171 @@
+// Device-resident hierarchy and the solve / resetup drivers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "dr_host.h"
+
+namespace dr {
+
+void cuda_check(cudaError_t e, const char* what, const char* file, int line);
+long long kernel_launches();
+#define DR_CK(x) ::dr::cuda_check((x), #x, __FILE__, __LINE__)
+
+// Sparse matrix on the device: CSR pattern, FP64 values and (after the first
+// mixed-precision use) an FP32 copy of the values.  G = lanes per row used by
+// the row kernels.
+struct DevMat {
+  int n = 0, m = 0;
+  long long nnz = 0;
+  int* rp = nullptr;
+  int* ci = nullptr;
+  double* v = nullptr;
+  float* v32 = nullptr;
+  int G = 8;
+};
+
+template <typename T>
+struct LevelVecs {
+  T* xa = nullptr;  // iterate (levels >= 1) ...
+  T* xb = nullptr;  // ... and its Jacobi ping-pong partner (level 0: partner of the caller's x)
+  T* b = nullptr;   // right-hand side (levels >= 1: written by the restriction above)
+  T* r = nullptr;   // residual
+};
+
+struct DevLevel {
+  DevMat A, P, R;            // R = Pᵀ stored as the transpose map with values
+  SmootherKind smoother = SmootherKind::Jacobi;
+  double omega = 2.0 / 3.0;
+  double* invd = nullptr;
+  float* invd32 = nullptr;
+  int ncolors = 0;
+  std::vector<int> color_off;  // host copy, num_colors+1
+  int* color_order = nullptr;
+  bool has_rap = false;
+  DevMat AP;                 // pattern and values of A·P (partial resetup)
+  LevelVecs<double> v64;
+  LevelVecs<float> v32;
+};
+
+struct CycleOpts {
+  int pre = 1;
+  int post = 1;
+  bool w = false;
+};
+
+// Per-launch timing of the dominant kernels, filled when enabled.
+struct KernelClock {
+  bool enabled = false;
+  std::vector<cudaEvent_t> ev;  // pairs (start, stop)
+  std::vector<int> tag;         // 0 = finest-level smoother sweep
+};
+
+class DevHier {
+ public:
+  DevHier(const HostHierarchy& H, int device);
+  ~DevHier();
+  DevHier(const DevHier&) = delete;
+  DevHier& operator=(const DevHier&) = delete;
+
+  int n0() const { return n0_; }
+  int nlevels() const { return (int)L_.size(); }
+  cudaStream_t stream() const { return st_; }
+  // Run on the caller's stream (nullptr: back to the library's own stream).
+  void set_stream(cudaStream_t s);
+  size_t device_bytes() const { return bytes_; }
+
+  // Solve phase (device pointers, length n0).
+  void cycle(double* x, const double* b, const CycleOpts& o);
+  int solve(double* x, const double* b, const CycleOpts& o, double tol, int maxiter, int verbose,
+            double* relres);
+  int pcg(double* x, const double* b, const CycleOpts& o, double tol, int maxiter, bool mixed,
+          double* relres, int verbose);
+
+  // Numeric resetup on the fixed structure; values of the finest matrix on
+  // the device (nnz0 entries).
+  void resetup_values(const double* v_dev);
+
+  // Single operations on one level for kernel-level parity tests (device
+  // pointers; precision 0 = FP64, 1 = FP32 buffers converted in/out).
+  void level_op(int lvl, int op, bool fp32, const double* in1, const double* in2, double* out,
+                int steps);
+  float time_level_op(int lvl, int op, bool fp32, int reps);
+
+  // Export device values (after a GPU resetup) into host vectors.
+  void export_values(int lvl, const std::string& what, std::vector<double>& out) const;
+  void export_piv(std::vector<int>& out) const;
+
+  // Scratch host-pointer helpers
+  double* xbuf() { return xd_; }
+  double* bbuf() { return bd_; }
+
+ private:
+  template <typename T> LevelVecs<T>& vecs(int l);
+  template <typename T> T* coarse_b();
+  template <typename T> T* coarse_x();
+  template <typename T> const T* mval(const DevMat& M) const;
+  template <typename T> const T* invd(const DevLevel& L) const;
+
+  template <typename T>
+  T* cycle_level(int l, T* x, const T* b, bool x_zero, const CycleOpts& o, T* ext_partner);
+  template <typename T>
+  T* smooth(int l, T* x, const T* b, int steps, T* ext_partner);
+  template <typename T>
+  void residual(int l, const T* x, const T* b, T* r, double* rr_dst);
+  template <typename T>
+  void coarse_solve(const T* b, T* x);
+
+  void ensure_fp32();
+  void refresh_fp32();
+  void graphs_clear();
+  double dot_host(const double* a, const double* b, int n);
+
+  int device_ = 0;
+  cudaStream_t st_ = nullptr;       // stream in use
+  cudaStream_t own_st_ = nullptr;   // stream created by the library
+  bool own_stream_ = false;
+  int n0_ = 0;
+  long long nnz0_ = 0;
+  int nsm_ = 148;
+  int max_grid_ = 148 * 8;
+  std::vector<DevLevel> L_;
+  DevMat C_;                 // coarsest CSR (pattern + values)
+  int nc_ = 0;
+  double* cdense_ = nullptr;
+  double* clu_ = nullptr;
+  int* cpiv_ = nullptr;
+  int* info_ = nullptr;
+  double *cb64_ = nullptr, *cx64_ = nullptr;
+  float *cb32_ = nullptr, *cx32_ = nullptr;
+  bool fp32_ = false;
+  // reductions: partial sums, tickets, scalars
+  double* partials_ = nullptr;
+  unsigned* tickets_ = nullptr;
+  double* scal_ = nullptr;     // [0] bb [1] rr [2] rz [3] rz_old [4] pq [5] tmp
+  double* hscal_ = nullptr;    // pinned host mirror
+  // host-pointer staging and PCG workspace
+  double *xd_ = nullptr, *bd_ = nullptr;
+  double *pr_ = nullptr, *pp_[2] = {nullptr, nullptr}, *pq_ = nullptr, *pz_ = nullptr;
+  float *pr32_ = nullptr, *pz32_ = nullptr;
+  double *tin1_ = nullptr, *tin2_ = nullptr, *tout_ = nullptr;  // level_op staging
+  size_t bytes_ = 0;
+  std::vector<void*> allocs_;
+  template <typename T> T* alloc(size_t n);
+  // CUDA graphs of the PCG iteration, keyed by (mixed, parity)
+  struct PcgGraphs {
+    bool valid = false;
+    bool mixed = false;
+    CycleOpts o;
+    cudaGraphExec_t g1[2] = {nullptr, nullptr};  // direction + update
+    cudaGraphExec_t g2 = nullptr;                // preconditioner + r·z
+    long long n1[2] = {0, 0}, n2 = 0;            // kernels per graph
+  } pg_;
+  cudaEvent_t ev_[2] = {nullptr, nullptr};
+
+  friend struct DevHierAccess;
+};
+
+}  // namespace dr

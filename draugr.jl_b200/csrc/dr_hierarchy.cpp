@@ -1,0 +1,484 @@
+// Galerkin product structure, smoother data, coarsest LU and the level loop
+// of the CPU setup phase.
+//
+//   transpose map        src/prolongation.jl:767-800
+//   coarse sparsity      src/galerkin.jl:11-183 (the pattern of P^T A P:
+//                        sorted unique columns per coarse row); here built
+//                        row by row through A*P instead of from sorted triples
+//   colouring            src/smoothers.jl:136-195
+//   smoother diagonals   src/smoothers.jl:47-63, :816-827
+//   coarse solver        src/setup.jl:177-209, :495-516, :526-534
+//   level loop           src/setup.jl:123-166, θ fallback :219-237,
+//                        coarsen+P :256-327
+#include <omp.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <limits>
+#include <numeric>
+#include <sstream>
+
+#include "dr_host.h"
+
+namespace dr {
+
+static const double kEps = std::numeric_limits<double>::epsilon();
+
+TransposeMap build_transpose_map(const Prolong& P) {
+  TransposeMap T;
+  T.off.assign(P.nc + 1, 0);
+  for (int64_t k = 0; k < P.nnz(); ++k) T.off[P.ci[k] + 1]++;
+  for (int j = 0; j < P.nc; ++j) T.off[j + 1] += T.off[j];
+  T.rows.resize(P.nnz());
+  T.pnz.resize(P.nnz());
+  std::vector<int> pos(T.off.begin(), T.off.end() - 1);
+  for (int i = 0; i < P.nf; ++i)
+    for (int k = P.rp[i]; k < P.rp[i + 1]; ++k) {
+      int J = P.ci[k];
+      T.rows[pos[J]] = i;
+      T.pnz[pos[J]] = k;
+      pos[J]++;
+    }
+  return T;
+}
+
+void symbolic_ap(const CSR& A, const Prolong& P, std::vector<int>& ap_rp, std::vector<int>& ap_ci) {
+  const int n = A.n, nc = P.nc;
+  ap_rp.assign(n + 1, 0);
+#pragma omp parallel
+  {
+    std::vector<int> mark(nc, -1);
+#pragma omp for schedule(static, 2048)
+    for (int i = 0; i < n; ++i) {
+      int cnt = 0;
+      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+        int j = A.ci[k];
+        for (int p = P.rp[j]; p < P.rp[j + 1]; ++p) {
+          int J = P.ci[p];
+          if (mark[J] != i) { mark[J] = i; ++cnt; }
+        }
+      }
+      ap_rp[i + 1] = cnt;
+    }
+  }
+  for (int i = 0; i < n; ++i) ap_rp[i + 1] += ap_rp[i];
+  ap_ci.resize(ap_rp[n]);
+#pragma omp parallel
+  {
+    std::vector<int> mark(nc, -1);
+#pragma omp for schedule(static, 2048)
+    for (int i = 0; i < n; ++i) {
+      int w = ap_rp[i];
+      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+        int j = A.ci[k];
+        for (int p = P.rp[j]; p < P.rp[j + 1]; ++p) {
+          int J = P.ci[p];
+          if (mark[J] != i) { mark[J] = i; ap_ci[w++] = J; }
+        }
+      }
+      std::sort(ap_ci.begin() + ap_rp[i], ap_ci.begin() + ap_rp[i + 1]);
+    }
+  }
+}
+
+void symbolic_ptap(const TransposeMap& T, int nc, const std::vector<int>& ap_rp,
+                   const std::vector<int>& ap_ci, std::vector<int>& c_rp, std::vector<int>& c_ci) {
+  c_rp.assign(nc + 1, 0);
+#pragma omp parallel
+  {
+    std::vector<int> mark(nc, -1);
+#pragma omp for schedule(dynamic, 256)
+    for (int I = 0; I < nc; ++I) {
+      int cnt = 0;
+      for (int t = T.off[I]; t < T.off[I + 1]; ++t) {
+        int i = T.rows[t];
+        for (int q = ap_rp[i]; q < ap_rp[i + 1]; ++q) {
+          int J = ap_ci[q];
+          if (mark[J] != I) { mark[J] = I; ++cnt; }
+        }
+      }
+      c_rp[I + 1] = cnt;
+    }
+  }
+  for (int I = 0; I < nc; ++I) c_rp[I + 1] += c_rp[I];
+  c_ci.resize(c_rp[nc]);
+#pragma omp parallel
+  {
+    std::vector<int> mark(nc, -1);
+#pragma omp for schedule(dynamic, 256)
+    for (int I = 0; I < nc; ++I) {
+      int w = c_rp[I];
+      for (int t = T.off[I]; t < T.off[I + 1]; ++t) {
+        int i = T.rows[t];
+        for (int q = ap_rp[i]; q < ap_rp[i + 1]; ++q) {
+          int J = ap_ci[q];
+          if (mark[J] != I) { mark[J] = I; c_ci[w++] = J; }
+        }
+      }
+      std::sort(c_ci.begin() + c_rp[I], c_ci.begin() + c_rp[I + 1]);
+    }
+  }
+}
+
+void numeric_ap(const CSR& A, const Prolong& P, const std::vector<int>& ap_rp,
+                const std::vector<int>& ap_ci, std::vector<double>& ap_v) {
+  const int n = A.n, nc = P.nc;
+  ap_v.assign(ap_ci.size(), 0.0);
+#pragma omp parallel
+  {
+    std::vector<double> acc(nc, 0.0);
+#pragma omp for schedule(static, 2048)
+    for (int i = 0; i < n; ++i) {
+      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+        const double a = A.v[k];
+        const int j = A.ci[k];
+        for (int p = P.rp[j]; p < P.rp[j + 1]; ++p) {
+          const double prod = a * P.v[p];
+          acc[P.ci[p]] = acc[P.ci[p]] + prod;
+        }
+      }
+      for (int q = ap_rp[i]; q < ap_rp[i + 1]; ++q) {
+        ap_v[q] = acc[ap_ci[q]];
+        acc[ap_ci[q]] = 0.0;
+      }
+    }
+  }
+}
+
+void numeric_ptap(const TransposeMap& T, const std::vector<double>& Rv, const std::vector<int>& ap_rp,
+                  const std::vector<int>& ap_ci, const std::vector<double>& ap_v,
+                  const std::vector<int>& c_rp, const std::vector<int>& c_ci, std::vector<double>& c_v) {
+  const int nc = (int)T.off.size() - 1;
+  c_v.assign(c_ci.size(), 0.0);
+#pragma omp parallel
+  {
+    std::vector<double> acc(nc, 0.0);
+#pragma omp for schedule(dynamic, 256)
+    for (int I = 0; I < nc; ++I) {
+      for (int t = T.off[I]; t < T.off[I + 1]; ++t) {
+        const double p = Rv[t];
+        const int i = T.rows[t];
+        for (int q = ap_rp[i]; q < ap_rp[i + 1]; ++q) {
+          const double prod = p * ap_v[q];
+          acc[ap_ci[q]] = acc[ap_ci[q]] + prod;
+        }
+      }
+      for (int q = c_rp[I]; q < c_rp[I + 1]; ++q) {
+        c_v[q] = acc[c_ci[q]];
+        acc[c_ci[q]] = 0.0;
+      }
+    }
+  }
+}
+
+void greedy_coloring(const CSR& A, std::vector<int>& colors, int& num_colors) {
+  const int n = A.n;
+  colors.assign(n, 0);
+  num_colors = 0;
+  std::vector<int> stamp(8, -1);
+  for (int i = 0; i < n; ++i) {
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+      int j = A.ci[k];
+      if (j != i && colors[j] > 0) {
+        int c = colors[j];
+        if (c >= (int)stamp.size()) stamp.resize(2 * c + 2, -1);
+        stamp[c] = i;
+      }
+    }
+    int c = 1;
+    while (c < (int)stamp.size() && stamp[c] == i) ++c;
+    colors[i] = c;
+    num_colors = std::max(num_colors, c);
+  }
+}
+
+void color_order_from(const std::vector<int>& colors, int num_colors, std::vector<int>& off,
+                      std::vector<int>& order) {
+  // Counting sort of the rows by colour, ascending row index within a colour
+  // (src/smoothers.jl:168-195); off[c-1] .. off[c] holds colour c.
+  const int n = (int)colors.size();
+  std::vector<int> cnt(num_colors + 1, 0);
+  for (int i = 0; i < n; ++i) cnt[colors[i]]++;
+  off.assign(num_colors + 1, 0);
+  for (int c = 1; c <= num_colors; ++c) off[c] = off[c - 1] + cnt[c];
+  order.resize(n);
+  std::vector<int> pos(off.begin(), off.end() - 1);
+  for (int i = 0; i < n; ++i) order[pos[colors[i] - 1]++] = i;
+}
+
+void inverse_diagonal(const CSR& A, std::vector<double>& invd) {
+  invd.resize(A.n);
+#pragma omp parallel for schedule(static, 4096)
+  for (int i = 0; i < A.n; ++i) {
+    double d = 0.0, rn = 0.0;
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+      rn += std::fabs(A.v[k]);
+      if (A.ci[k] == i) d = A.v[k];
+    }
+    double thr = kEps * std::max(1.0, rn);
+    invd[i] = std::fabs(d) > thr ? 1.0 / d : 0.0;
+  }
+}
+
+void l1_inverse_diagonal(const CSR& A, std::vector<double>& invd) {
+  invd.resize(A.n);
+#pragma omp parallel for schedule(static, 4096)
+  for (int i = 0; i < A.n; ++i) {
+    double l1 = 0.0;
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) l1 += std::fabs(A.v[k]);
+    invd[i] = l1 > kEps ? 1.0 / l1 : 0.0;
+  }
+}
+
+void csr_to_dense(const CSR& A, std::vector<double>& M) {
+  const int n = A.n;
+  M.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i)
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) M[(size_t)A.ci[k] * n + i] = A.v[k];
+}
+
+// Unblocked LU with partial pivoting, column-major (LAPACK dgetf2 order:
+// pivot = first row of maximum magnitude, column scaled by the reciprocal
+// of the pivot, rank-1 update of the trailing matrix).  A zero pivot is an
+// error, as Julia's lu(A) throws SingularException for it.
+void dense_lu(int n, std::vector<double>& a, std::vector<int>& piv) {
+  piv.resize(n);
+  for (int j = 0; j < n; ++j) {
+    int p = j;
+    double mx = std::fabs(a[(size_t)j * n + j]);
+    for (int i = j + 1; i < n; ++i) {
+      double v = std::fabs(a[(size_t)j * n + i]);
+      if (v > mx) { mx = v; p = i; }
+    }
+    piv[j] = p;
+    if (a[(size_t)j * n + p] == 0.0) fail("SingularException(" + std::to_string(j + 1) + ")");
+    if (p != j)
+      for (int c = 0; c < n; ++c) std::swap(a[(size_t)c * n + j], a[(size_t)c * n + p]);
+    const double r = 1.0 / a[(size_t)j * n + j];
+    for (int i = j + 1; i < n; ++i) a[(size_t)j * n + i] = a[(size_t)j * n + i] * r;
+    for (int c = j + 1; c < n; ++c) {
+      const double t = a[(size_t)c * n + j];
+      for (int i = j + 1; i < n; ++i) {
+        const double prod = a[(size_t)j * n + i] * t;
+        a[(size_t)c * n + i] = a[(size_t)c * n + i] - prod;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------ level loop
+namespace {
+
+bool uses_cf(CoarsenKind k) {
+  return k == CoarsenKind::PMIS || k == CoarsenKind::HMIS || k == CoarsenKind::RS;
+}
+
+void coarsen_and_build_p(const CSR& A, const Coarsening& alg, const Config& cfg, uint64_t& rng,
+                         Prolong& P, int& nc) {
+  std::vector<int> cf, cmap;
+  switch (alg.kind) {
+    case CoarsenKind::PMIS:
+    case CoarsenKind::HMIS: {
+      CSR Aw;
+      const CSR* Ap = &A;
+      if (cfg.max_row_sum < 1.0) { Aw = apply_max_row_sum(A, cfg.max_row_sum); Ap = &Aw; }
+      if (alg.kind == CoarsenKind::PMIS) coarsen_pmis(*Ap, alg.theta, rng, cf, cmap, nc);
+      else coarsen_hmis(*Ap, alg.theta, rng, cf, cmap, nc);
+      P = build_interpolation(A, cf, cmap, nc, alg.interp, alg.theta);
+      if (alg.interp.trunc_factor > 0) P = truncate_interpolation(P, alg.interp.trunc_factor);
+      return;
+    }
+    case CoarsenKind::RS:
+      fail("RS coarsening is not supported by the B200 build (use hmis, pmis, aggressive_hmis, "
+           "aggressive_pmis, aggregation or smoothed_aggregation)");
+    case CoarsenKind::AggressivePMIS:
+    case CoarsenKind::AggressiveHMIS: {
+      coarsen_aggressive_cf(A, alg.theta, alg.kind == CoarsenKind::AggressiveHMIS, cfg, rng, cf,
+                            cmap, nc);
+      P = build_interpolation(A, cf, cmap, nc, alg.interp, alg.theta);
+      if (alg.interp.trunc_factor > 0) P = truncate_interpolation(P, alg.interp.trunc_factor);
+      return;
+    }
+    case CoarsenKind::Aggregation:
+    case CoarsenKind::SmoothedAggregation: {
+      std::vector<int> agg;
+      if (cfg.max_row_sum < 1.0) coarsen_aggregation(apply_max_row_sum(A, cfg.max_row_sum), alg.theta, agg, nc);
+      else coarsen_aggregation(A, alg.theta, agg, nc);
+      P = build_aggregation_prolongation(A.n, agg, nc);
+      if (alg.kind == CoarsenKind::SmoothedAggregation) P = smooth_prolongation(A, P, alg.sa_omega);
+      if (alg.filtering) P = filter_prolongation(P, alg.filter_tol);
+      return;
+    }
+  }
+}
+
+void coarsen_with_fallback(const CSR& A, const Coarsening& alg, const Config& cfg, uint64_t& rng,
+                           Prolong& P, int& nc) {
+  const int n = A.n;
+  coarsen_and_build_p(A, alg, cfg, rng, P, nc);
+  if (nc < 0.8 * n || n <= cfg.max_coarse_size) return;
+  for (int attempt = 1; attempt <= 3; ++attempt) {
+    Coarsening red = alg;
+    red.theta = alg.theta * std::pow(0.5, attempt);
+    Prolong P2;
+    int nc2 = 0;
+    coarsen_and_build_p(A, red, cfg, rng, P2, nc2);
+    if (nc2 < nc) { P = std::move(P2); nc = nc2; }
+    if (nc < 0.8 * n) break;
+  }
+}
+
+void build_smoother(HostLevel& L, const Config& cfg) {
+  L.smoother = cfg.smoother;
+  L.omega = cfg.jacobi_omega;
+  switch (cfg.smoother) {
+    case SmootherKind::Jacobi:
+      inverse_diagonal(L.A, L.invdiag);
+      break;
+    case SmootherKind::L1Jacobi:
+      l1_inverse_diagonal(L.A, L.invdiag);
+      break;
+    case SmootherKind::ColoredGS:
+      greedy_coloring(L.A, L.colors, L.num_colors);
+      color_order_from(L.colors, L.num_colors, L.color_off, L.color_order);
+      inverse_diagonal(L.A, L.invdiag);
+      break;
+    case SmootherKind::L1ColoredGS:
+      greedy_coloring(L.A, L.colors, L.num_colors);
+      color_order_from(L.colors, L.num_colors, L.color_off, L.color_order);
+      l1_inverse_diagonal(L.A, L.invdiag);
+      break;
+    default:
+      fail("smoother \"" + smoother_name(cfg.smoother) +
+           "\" is not supported by the B200 build (use jacobi, l1_jacobi, colored_gs or "
+           "l1_colored_gs)");
+  }
+}
+
+}  // namespace
+
+void build_hierarchy(const CSR& A_in, const Config& cfg, bool allow_partial_resetup, HostHierarchy& H) {
+  auto t0 = std::chrono::steady_clock::now();
+  validate_csr(A_in, "matrix");
+  if (A_in.n != A_in.m) fail("matrix must be square");
+  // Check the smoother before any work, so an unsupported choice fails fast.
+  switch (cfg.smoother) {
+    case SmootherKind::Jacobi: case SmootherKind::L1Jacobi:
+    case SmootherKind::ColoredGS: case SmootherKind::L1ColoredGS: break;
+    default:
+      fail("smoother \"" + smoother_name(cfg.smoother) +
+           "\" is not supported by the B200 build (use jacobi, l1_jacobi, colored_gs or "
+           "l1_colored_gs)");
+  }
+  H = HostHierarchy();
+  H.cfg = cfg;
+  H.allow_partial_resetup = allow_partial_resetup;
+  uint64_t rng = cfg.seed;
+  CSR cur = A_in;
+  for (int lvl = 1; lvl <= cfg.max_levels - 1; ++lvl) {
+    const int n = cur.n;
+    if (n <= cfg.max_coarse_size) break;
+    const Coarsening& alg = lvl <= cfg.initial_coarsening_levels ? cfg.initial_coarsening : cfg.coarsening;
+    Prolong P;
+    int nc = 0;
+    coarsen_with_fallback(cur, alg, cfg, rng, P, nc);
+    if (nc >= n) break;
+    if (nc == 0) break;
+    HostLevel L;
+    L.T = build_transpose_map(P);
+    L.Rv.resize(P.nnz());
+    for (size_t k = 0; k < L.T.pnz.size(); ++k) L.Rv[k] = P.v[L.T.pnz[k]];
+    std::vector<int> ap_rp, ap_ci;
+    symbolic_ap(cur, P, ap_rp, ap_ci);
+    std::vector<double> ap_v;
+    numeric_ap(cur, P, ap_rp, ap_ci, ap_v);
+    CSR next;
+    next.n = next.m = nc;
+    symbolic_ptap(L.T, nc, ap_rp, ap_ci, next.rp, next.ci);
+    numeric_ptap(L.T, L.Rv, ap_rp, ap_ci, ap_v, next.rp, next.ci, next.v);
+    if (allow_partial_resetup) {
+      L.has_rap_map = true;
+      L.ap_rp = std::move(ap_rp);
+      L.ap_ci = std::move(ap_ci);
+    }
+    L.A = std::move(cur);
+    L.P = std::move(P);
+    build_smoother(L, cfg);
+    H.levels.push_back(std::move(L));
+    cur = std::move(next);
+  }
+  H.coarse = std::move(cur);
+  H.nc = H.coarse.n;
+  csr_to_dense(H.coarse, H.coarse_dense);
+  H.coarse_lu = H.coarse_dense;
+  dense_lu(H.nc, H.coarse_lu, H.coarse_piv);
+  H.setup_seconds =
+      std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+std::string hierarchy_summary(const HostHierarchy& H, int n_finest) {
+  // Layout of _print_hierarchy_info, src/setup.jl:405-473.
+  std::ostringstream o;
+  char buf[256];
+  const Config& c = H.cfg;
+  int nl = (int)H.levels.size();
+  o << "+=============================================================================+\n";
+  o << "                         AMG Hierarchy Summary                                  \n";
+  o << "+=============================================================================+\n";
+  std::snprintf(buf, sizeof buf, "  Setup time:      %.4f s\n", H.setup_seconds); o << buf;
+  o << "  Levels:          " << nl + 1 << " (" << nl << " AMG + 1 coarse direct)\n";
+  o << "  Cycle type:      " << (c.cycle_w ? "W" : "V") << "-cycle\n";
+  o << "  Backend:         CUDA (sm_100a)\n";
+  o << "  Coarse solve:    " << (c.coarse_solve_on_cpu ? "CPU (forced)" : "default") << "\n";
+  o << "  Strength:        " << (c.strength == StrengthKind::Absolute ? "AbsoluteStrength" : "SignedStrength") << "\n";
+  o << "  Coarsening:      " << coarsening_name(c.coarsening) << "\n";
+  if (c.initial_coarsening_levels > 0)
+    o << "  Initial coars.:  " << coarsening_name(c.initial_coarsening) << " (first "
+      << c.initial_coarsening_levels << " levels)\n";
+  o << "  Smoother:        " << smoother_name(c.smoother) << "\n";
+  if (c.smoother == SmootherKind::Jacobi || c.smoother == SmootherKind::L1Jacobi) {
+    std::snprintf(buf, sizeof buf, "    omega = %.3f\n", c.jacobi_omega); o << buf;
+  }
+  std::snprintf(buf, sizeof buf, "  Pre-smooth:      %d steps, Post-smooth: %d steps\n",
+                c.pre_smoothing_steps, c.post_smoothing_steps); o << buf;
+  o << "+-------+----------+-----------+---------+------------------------------------+\n";
+  o << "  Level     Rows        NNZ      Ratio    Smoother                              \n";
+  o << "+-------+----------+-----------+---------+------------------------------------+\n";
+  int64_t tot_nnz = 0, tot_rows = 0;
+  for (int i = 0; i < nl; ++i) {
+    const auto& L = H.levels[i];
+    tot_nnz += L.A.nnz();
+    tot_rows += L.A.n;
+    if (i == 0)
+      std::snprintf(buf, sizeof buf, "  %5d   %7d    %8lld        -   %s\n", i + 1, L.A.n,
+                    (long long)L.A.nnz(), smoother_name(L.smoother).c_str());
+    else
+      std::snprintf(buf, sizeof buf, "  %5d   %7d    %8lld    %5.3f   %s\n", i + 1, L.A.n,
+                    (long long)L.A.nnz(), (double)L.A.n / H.levels[i - 1].A.n,
+                    smoother_name(L.smoother).c_str());
+    o << buf;
+  }
+  int64_t cnz = 0;
+  for (double v : H.coarse_dense) cnz += (v != 0.0);
+  tot_nnz += cnz;
+  tot_rows += H.nc;
+  if (nl > 0)
+    std::snprintf(buf, sizeof buf, "  %5d   %7d    %8lld    %5.3f   %s\n", nl + 1, H.nc, (long long)cnz,
+                  (double)H.nc / H.levels[nl - 1].A.n, "Direct (LU)");
+  else
+    std::snprintf(buf, sizeof buf, "  %5d   %7d    %8lld         -   %s\n", nl + 1, H.nc, (long long)cnz,
+                  "Direct (LU)");
+  o << buf;
+  o << "+=============================================================================+\n";
+  if (nl > 0) {
+    std::snprintf(buf, sizeof buf, "  Operator complexity: %.3f\n",
+                  (double)tot_nnz / (double)H.levels[0].A.nnz()); o << buf;
+    std::snprintf(buf, sizeof buf, "  Grid complexity:     %.3f\n", (double)tot_rows / n_finest); o << buf;
+  }
+  o << "+=============================================================================+\n";
+  return o.str();
+}
+
+}  // namespace dr

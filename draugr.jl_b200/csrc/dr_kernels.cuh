@@ -1,0 +1,509 @@
+// sm_100a kernels of the AMG solve and resetup hot path.
+//
+// Row kernels use a group of G lanes per CSR row (G a power of two chosen
+// per matrix from its mean row length): the G lanes read G consecutive
+// (column, value) pairs per step, so a warp streams 32 consecutive entries
+// of the value and index arrays, and the group sum is a fixed shuffle tree.
+// Rows are walked with a warp-uniform grid-stride loop so every lane of a
+// warp takes part in every shuffle.  Epilogue functors fuse what follows the
+// product in the reference (residual, Jacobi update, prolongation add,
+// Gauss-Seidel update, dot products) into the same pass.
+//
+// Dot products are deterministic: a fixed grid writes one partial per block,
+// and the last block to finish (atomic ticket) sums the partials in index
+// order; results do not depend on block scheduling.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace dr {
+namespace kern {
+
+constexpr int kBlock = 256;
+
+// ------------------------------------------------------------ reductions
+// Sum `v` over the block; result valid in thread 0.
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double ws[32];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();  // ws may still be read by a previous call
+  if (l == 0) ws[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    v = (l < nw) ? ws[l] : 0.0;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  }
+  return v;
+}
+
+// Finalizers applied by the last block to the grand total.
+struct FinStore {
+  double* dst;
+  __device__ void operator()(double s) const { *dst = s; }
+};
+// Shift: old <- current, current <- s (used for r.z in PCG).
+struct FinShift {
+  double* cur;
+  double* old;
+  __device__ void operator()(double s) const {
+    *old = *cur;
+    *cur = s;
+  }
+};
+
+// Each block contributes `v`; the last block sums all partials in order and
+// applies `fin`.  `ticket` must be zero on entry and is zero again on exit.
+template <class Fin>
+__device__ __forceinline__ void grid_sum_finalize(double v, double* partials, unsigned* ticket,
+                                                  Fin fin) {
+  __shared__ bool am_last;
+  v = block_sum(v);
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = v;
+    __threadfence();
+    unsigned t = atomicAdd(ticket, 1u);
+    am_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (am_last) {
+    __threadfence();
+    double s = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) s += __ldcg(partials + i);
+    s = block_sum(s);
+    if (threadIdx.x == 0) {
+      fin(s);
+      *ticket = 0u;
+    }
+  }
+}
+
+// ------------------------------------------------------------ operand loaders
+template <typename T>
+struct XPlain {
+  const T* __restrict__ x;
+  __device__ __forceinline__ T operator()(int j) const { return __ldg(x + j); }
+};
+
+// First weighted-Jacobi step from a zero guess: x1_j = 0 + (ω·invd_j)·(b_j - 0)
+// (src/smoothers.jl:78-94 with x = 0), evaluated where it is consumed.
+template <typename T>
+struct XZeroJacobi {
+  const T* __restrict__ b;
+  const T* __restrict__ invd;
+  T omega;
+  __device__ __forceinline__ T operator()(int j) const { return (omega * __ldg(invd + j)) * __ldg(b + j); }
+};
+
+// PCG search direction on the fly: p_j = z_j + β·p_old_j.
+template <typename TZ>
+struct XPcgDir {
+  const TZ* __restrict__ z;
+  const double* __restrict__ pold;
+  const double* __restrict__ scal;  // [rz, rz_old]
+  int first;
+  __device__ __forceinline__ double operator()(int j) const {
+    double zj = (double)__ldg(z + j);
+    if (first) return zj;
+    double beta = __ldg(scal) / __ldg(scal + 1);
+    return zj + beta * __ldg(pold + j);
+  }
+};
+
+// ------------------------------------------------------------ epilogues
+template <typename T>
+struct EpStore {  // y = A x
+  using acc_t = T;
+  T* __restrict__ y;
+  __device__ __forceinline__ double operator()(int i, T s) const { y[i] = s; return 0.0; }
+};
+
+template <typename T>
+struct EpResidual {  // r = b - A x            (src/cycle.jl:32-43)
+  using acc_t = T;
+  const T* __restrict__ b;
+  T* __restrict__ r;
+  __device__ __forceinline__ double operator()(int i, T s) const {
+    T ri = __ldg(b + i) - s;
+    r[i] = ri;
+    return (double)ri * (double)ri;
+  }
+};
+
+template <typename T>
+struct EpJacobi {  // xn = x + ω·invd·(b - A x)  (src/smoothers.jl:78-94)
+  using acc_t = T;
+  const T* __restrict__ x;
+  const T* __restrict__ b;
+  const T* __restrict__ invd;
+  T* __restrict__ xn;
+  T omega;
+  const double* __restrict__ w;  // optional: returns w_i·xn_i for a fused dot
+  __device__ __forceinline__ double operator()(int i, T s) const {
+    T ri = __ldg(b + i) - s;
+    T v = __ldg(x + i) + (omega * __ldg(invd + i)) * ri;
+    xn[i] = v;
+    return w ? __ldg(w + i) * (double)v : 0.0;
+  }
+};
+
+template <typename T>
+struct EpZeroJacobiResidual {  // x1 = ω·invd·b ; r = b - A x1
+  using acc_t = T;
+  const T* __restrict__ b;
+  const T* __restrict__ invd;
+  T* __restrict__ x1;
+  T* __restrict__ r;
+  T omega;
+  __device__ __forceinline__ double operator()(int i, T s) const {
+    T bi = __ldg(b + i);
+    x1[i] = (omega * __ldg(invd + i)) * bi;
+    r[i] = bi - s;
+    return 0.0;
+  }
+};
+
+template <typename T>
+struct EpAddTo {  // x += P xc               (src/prolongation.jl:742-760)
+  using acc_t = T;
+  T* __restrict__ x;
+  __device__ __forceinline__ double operator()(int i, T s) const { x[i] += s; return 0.0; }
+};
+
+template <typename T>
+struct EpPcgDir {  // q = A p, p_new = z + β p_old, returns p_new·q
+  using acc_t = double;
+  XPcgDir<T> dir;
+  double* __restrict__ pnew;
+  double* __restrict__ q;
+  __device__ __forceinline__ double operator()(int i, double s) const {
+    double pi = dir(i);
+    pnew[i] = pi;
+    q[i] = s;
+    return pi * s;
+  }
+};
+
+// ------------------------------------------------------------ row kernel
+template <int G, typename TA, class XL, class EP, bool DOT, class Fin>
+__global__ void __launch_bounds__(kBlock)
+k_csr_rows(int n, const int* __restrict__ rp, const int* __restrict__ ci, const TA* __restrict__ av,
+           XL xl, EP ep, double* partials, unsigned* ticket, Fin fin) {
+  using acc_t = typename EP::acc_t;
+  constexpr int RPW = 32 / G;
+  const int lane = threadIdx.x & (G - 1);
+  const int g = (threadIdx.x & 31) / G;
+  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  double dacc = 0.0;
+  for (long long base = warp * RPW; base < n; base += nwarps * RPW) {
+    const int row = (int)(base + g);
+    const bool valid = row < n;
+    int s = 0, e = 0;
+    if (valid) {
+      s = __ldg(rp + row);
+      e = __ldg(rp + row + 1);
+    }
+    acc_t sum = acc_t(0);
+    for (int k = s + lane; k < e; k += G) sum += (acc_t)__ldg(av + k) * (acc_t)xl(__ldg(ci + k));
+#pragma unroll
+    for (int off = G >> 1; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+    if (valid && lane == 0) dacc += ep(row, sum);
+  }
+  if constexpr (DOT) grid_sum_finalize(dacc, partials, ticket, fin);
+}
+
+// Gauss-Seidel update of one colour: rows taken from `order`.
+// x_i += invd_i·(b_i - A_i x)                 (src/smoothers.jl:203-217)
+template <int G, typename T>
+__global__ void __launch_bounds__(kBlock)
+k_gs_color(int cnt, const int* __restrict__ order, const int* __restrict__ rp,
+           const int* __restrict__ ci, const T* __restrict__ av, const T* __restrict__ b,
+           const T* __restrict__ invd, T* x) {
+  constexpr int RPW = 32 / G;
+  const int lane = threadIdx.x & (G - 1);
+  const int g = (threadIdx.x & 31) / G;
+  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long base = warp * RPW; base < cnt; base += nwarps * RPW) {
+    const int idx = (int)(base + g);
+    const bool valid = idx < cnt;
+    int row = 0, s = 0, e = 0;
+    if (valid) {
+      row = __ldg(order + idx);
+      s = __ldg(rp + row);
+      e = __ldg(rp + row + 1);
+    }
+    T sum = T(0);
+    // x of the same colour is never a neighbour, so plain loads are safe
+    for (int k = s + lane; k < e; k += G) sum += __ldg(av + k) * x[__ldg(ci + k)];
+#pragma unroll
+    for (int off = G >> 1; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+    if (valid && lane == 0) x[row] += __ldg(invd + row) * (__ldg(b + row) - sum);
+  }
+}
+
+// ------------------------------------------------------------ vector kernels
+template <typename T>
+__global__ void k_scale_jacobi_zero(int n, const T* __restrict__ b, const T* __restrict__ invd,
+                                    T omega, T* __restrict__ x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    x[i] = (omega * invd[i]) * b[i];
+}
+
+template <typename T>
+__global__ void k_fill(long long n, T v, T* __restrict__ x) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    x[i] = v;
+}
+
+template <typename TS, typename TD>
+__global__ void k_convert(long long n, const TS* __restrict__ s, TD* __restrict__ d) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    d[i] = (TD)s[i];
+}
+
+// dot(a, b) with deterministic finalize
+template <typename TA, typename TB, class Fin>
+__global__ void __launch_bounds__(kBlock)
+k_dot(int n, const TA* __restrict__ a, const TB* __restrict__ b, double* partials, unsigned* ticket,
+      Fin fin) {
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    s += (double)a[i] * (double)b[i];
+  grid_sum_finalize(s, partials, ticket, fin);
+}
+
+// x += α p ; r -= α q ; rr = r·r ; optional r32 copy.  α = rz / pq.
+template <typename TR32>
+__global__ void __launch_bounds__(kBlock)
+k_pcg_update(int n, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
+             const double* __restrict__ q, const double* __restrict__ rz, const double* __restrict__ pq,
+             TR32* __restrict__ r32, double* partials, unsigned* ticket, FinStore fin) {
+  const double alpha = __ldg(rz) / __ldg(pq);
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    x[i] += alpha * p[i];
+    double ri = r[i] - alpha * q[i];
+    r[i] = ri;
+    if (r32) r32[i] = (TR32)ri;
+    s += ri * ri;
+  }
+  grid_sum_finalize(s, partials, ticket, fin);
+}
+
+// ------------------------------------------------------------ coarsest level
+// Solve with getrf-style factors (column-major LU, 0-based pivots) in one
+// block: row interchanges, unit-lower forward substitution and upper back
+// substitution in the column-oriented (axpy) order of LAPACK dgetrs/dtrsv,
+// without contraction, so the result equals a sequential CPU solve bit for
+// bit.  Input and output in T, arithmetic in double.
+template <typename T>
+__global__ void k_lu_solve(int n, const double* __restrict__ lu, const int* __restrict__ piv,
+                           const T* __restrict__ bin, T* __restrict__ xout) {
+  extern __shared__ double y[];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = (double)bin[i];
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int j = 0; j < n; ++j) {
+      int p = piv[j];
+      if (p != j) {
+        double t = y[j];
+        y[j] = y[p];
+        y[p] = t;
+      }
+    }
+  __syncthreads();
+  for (int j = 0; j < n; ++j) {
+    const double yj = y[j];
+    if (yj != 0.0)
+      for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x)
+        y[i] = __dsub_rn(y[i], __dmul_rn(yj, lu[(size_t)j * n + i]));
+    __syncthreads();
+  }
+  for (int j = n - 1; j >= 0; --j) {
+    if (threadIdx.x == 0 && y[j] != 0.0) y[j] = __ddiv_rn(y[j], lu[(size_t)j * n + j]);
+    __syncthreads();
+    const double yj = y[j];
+    if (yj != 0.0)
+      for (int i = threadIdx.x; i < j; i += blockDim.x)
+        y[i] = __dsub_rn(y[i], __dmul_rn(yj, lu[(size_t)j * n + i]));
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) xout[i] = (T)y[i];
+}
+
+// In-place unblocked LU with partial pivoting (dgetf2 order) of a
+// column-major n x n matrix in one block.  info = 0 or the 1-based index of
+// the first zero pivot (factorisation stops there).
+__global__ void k_lu_factor(int n, double* __restrict__ a, int* __restrict__ piv, int* info) {
+  __shared__ double sv[1024];
+  __shared__ int si[1024];
+  __shared__ int sp;
+  if (threadIdx.x == 0) *info = 0;
+  for (int j = 0; j < n; ++j) {
+    // pivot search: first index of the maximum magnitude in column j
+    double best = -1.0;
+    int bi = n;
+    for (int i = j + threadIdx.x; i < n; i += blockDim.x) {
+      double v = fabs(a[(size_t)j * n + i]);
+      if (v > best) { best = v; bi = i; }
+    }
+    sv[threadIdx.x] = best;
+    si[threadIdx.x] = bi;
+    __syncthreads();
+    for (int s = blockDim.x >> 1; s > 0; s >>= 1) {
+      if (threadIdx.x < s) {
+        double v2 = sv[threadIdx.x + s];
+        int i2 = si[threadIdx.x + s];
+        if (v2 > sv[threadIdx.x] || (v2 == sv[threadIdx.x] && i2 < si[threadIdx.x])) {
+          sv[threadIdx.x] = v2;
+          si[threadIdx.x] = i2;
+        }
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      sp = si[0];
+      piv[j] = sp;
+    }
+    __syncthreads();
+    const int p = sp;
+    if (a[(size_t)j * n + p] == 0.0) {
+      if (threadIdx.x == 0) *info = j + 1;
+      return;
+    }
+    if (p != j)
+      for (int c = threadIdx.x; c < n; c += blockDim.x) {
+        double t = a[(size_t)c * n + j];
+        a[(size_t)c * n + j] = a[(size_t)c * n + p];
+        a[(size_t)c * n + p] = t;
+      }
+    __syncthreads();
+    const double r = __drcp_rn(a[(size_t)j * n + j]);
+    for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x)
+      a[(size_t)j * n + i] = __dmul_rn(a[(size_t)j * n + i], r);
+    __syncthreads();
+    const int m = n - j - 1;
+    for (long long t = threadIdx.x; t < (long long)m * m; t += blockDim.x) {
+      const int c = j + 1 + (int)(t / m);
+      const int i = j + 1 + (int)(t % m);
+      a[(size_t)c * n + i] =
+          __dsub_rn(a[(size_t)c * n + i], __dmul_rn(a[(size_t)j * n + i], a[(size_t)c * n + j]));
+    }
+    __syncthreads();
+  }
+}
+
+// Scatter CSR values into a zeroed column-major dense matrix.
+__global__ void k_csr_to_dense(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                               const double* __restrict__ v, double* __restrict__ M) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    for (int k = rp[i]; k < rp[i + 1]; ++k) M[(size_t)ci[k] * n + i] = v[k];
+}
+
+// ------------------------------------------------------------ smoother diagonals
+// src/smoothers.jl:47-63: 1/a_ii, or 0 if |a_ii| <= eps·max(1, Σ|a_ij|)
+__global__ void k_invdiag(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                          const double* __restrict__ v, double* __restrict__ invd) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double d = 0.0, rn = 0.0;
+    for (int k = rp[i]; k < rp[i + 1]; ++k) {
+      rn = __dadd_rn(rn, fabs(v[k]));
+      if (ci[k] == i) d = v[k];
+    }
+    const double thr = 2.220446049250313e-16 * fmax(1.0, rn);
+    invd[i] = fabs(d) > thr ? __drcp_rn(d) : 0.0;
+  }
+}
+
+// src/smoothers.jl:816-827: 1/Σ|a_ij|, or 0 if the sum is <= eps
+__global__ void k_l1_invdiag(int n, const int* __restrict__ rp, const double* __restrict__ v,
+                             double* __restrict__ invd) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double l1 = 0.0;
+    for (int k = rp[i]; k < rp[i + 1]; ++k) l1 = __dadd_rn(l1, fabs(v[k]));
+    invd[i] = l1 > 2.220446049250313e-16 ? __drcp_rn(l1) : 0.0;
+  }
+}
+
+// ------------------------------------------------------------ Galerkin product
+// One output row per group of G lanes:  out_I = Σ_k s_Ik · B_{j_k}  on the
+// fixed sorted pattern of out_I.  Phase 1 (A·P): s = A, B = P.  Phase 2
+// (Pᵀ·(AP)): s = R = Pᵀ in transpose-map order, B = A·P.  The k loop is
+// sequential and each B row holds a column at most once, so every output
+// entry accumulates its terms in (k, B-entry) order with no two lanes
+// touching the same entry in one step: the sum is deterministic and equal to
+// a sequential CPU loop in that order (products and sums rounded
+// separately).  Output positions are found by binary search in the pattern
+// row, staged in shared memory when it fits.
+template <int G, int CAP>
+__global__ void __launch_bounds__(kBlock)
+k_spgemm_rows(int nrows, const int* __restrict__ out_rp, const int* __restrict__ out_ci,
+              double* __restrict__ out_v, const int* __restrict__ s_rp, const int* __restrict__ s_ci,
+              const double* __restrict__ s_v, const int* __restrict__ b_rp,
+              const int* __restrict__ b_ci, const double* __restrict__ b_v) {
+  constexpr int GPB = kBlock / G;  // groups per block
+  __shared__ int scol[GPB][CAP];
+  __shared__ double sacc[GPB][CAP];
+  const int lane = threadIdx.x & (G - 1);
+  const int gl = threadIdx.x / G;
+  const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
+  const long long ngroups = (long long)gridDim.x * GPB;
+  for (long long I0 = (long long)blockIdx.x * GPB + gl; I0 < nrows; I0 += ngroups) {
+    const int I = (int)I0;
+    const int os = out_rp[I], oe = out_rp[I + 1];
+    const int m = oe - os;
+    const bool fits = m <= CAP;
+    if (fits) {
+      for (int t = lane; t < m; t += G) {
+        scol[gl][t] = out_ci[os + t];
+        sacc[gl][t] = 0.0;
+      }
+    } else {
+      for (int t = lane; t < m; t += G) out_v[os + t] = 0.0;
+    }
+    __syncwarp(gmask);
+    const int ss = s_rp[I], se = s_rp[I + 1];
+    for (int k = ss; k < se; ++k) {
+      const int j = s_ci[k];
+      const double sv = s_v[k];
+      const int bs = b_rp[j], be = b_rp[j + 1];
+      for (int t = bs + lane; t < be; t += G) {
+        const int J = b_ci[t];
+        const double prod = __dmul_rn(sv, b_v[t]);
+        int lo = 0, hi = m - 1, pos = -1;
+        if (fits) {
+          while (lo <= hi) {
+            int mid = (lo + hi) >> 1;
+            int c = scol[gl][mid];
+            if (c == J) { pos = mid; break; }
+            if (c < J) lo = mid + 1; else hi = mid - 1;
+          }
+          if (pos >= 0) sacc[gl][pos] = __dadd_rn(sacc[gl][pos], prod);
+        } else {
+          while (lo <= hi) {
+            int mid = (lo + hi) >> 1;
+            int c = out_ci[os + mid];
+            if (c == J) { pos = mid; break; }
+            if (c < J) lo = mid + 1; else hi = mid - 1;
+          }
+          if (pos >= 0) out_v[os + pos] = __dadd_rn(out_v[os + pos], prod);
+        }
+      }
+      __syncwarp(gmask);
+    }
+    if (fits)
+      for (int t = lane; t < m; t += G) out_v[os + t] = sacc[gl][t];
+    __syncwarp(gmask);
+  }
+}
+
+}  // namespace kern
+}  // namespace dr

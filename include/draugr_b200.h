@@ -1,0 +1,105 @@
+/*
+ * draugr_b200.h - extensions of the B200 AMG library beyond the reference
+ * C API (draugr_amg.h).  All functions return -1 on error and set
+ * draugr_amg_last_error().  "Device pointers" are CUDA device addresses on
+ * the device that was current when the hierarchy was set up.
+ */
+#ifndef DRAUGR_B200_H
+#define DRAUGR_B200_H
+
+#include <stdint.h>
+
+#include "draugr_amg.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Hierarchy structure only, built on the CPU with nothing sent to a GPU
+ * (inspection and export; no counterpart in the reference, whose setup
+ * always produces a solver).  A later device call uploads it. */
+int32_t draugr_b200_setup_host(int32_t n, int32_t nnz, const int32_t *rowptr,
+                               const int32_t *colval, const double *nzval, int32_t config_handle,
+                               int32_t index_base, int32_t allow_partial_resetup);
+
+/* Number of AMG levels (the coarsest dense level not counted), as
+ * length(hierarchy.levels) in src/types.jl:457-467. */
+int32_t draugr_b200_num_levels(int32_t handle);
+
+/* Sizes of level lvl (0-based): info[0] n, [1] nnz(A), [2] n_coarse,
+ * [3] nnz(P), [4] smoother kind, [5] colours, [6] nnz(A*P) or -1.
+ * lvl = -1: the coarsest level, info[0] n_c, [1] nnz of its CSR. */
+int32_t draugr_b200_level_info(int32_t handle, int32_t lvl, int64_t *info);
+
+/* Copy one array of level lvl (0-based indices) into out.  Integer arrays
+ * (int32): A_rowptr A_colval P_rowptr P_colval T_offsets T_rows T_pnz
+ * colors color_order color_offsets AP_rowptr AP_colval, and for lvl = -1
+ * C_rowptr C_colval C_piv.  Double arrays: A_nzval P_nzval R_nzval invdiag
+ * AP_nzval, and for lvl = -1 C_nzval C_dense C_lu.  Values come from the
+ * device when the hierarchy lives there (so they reflect resetups).
+ * out = NULL returns the element count.  Returns the element count. */
+int64_t draugr_b200_export(int32_t handle, int32_t lvl, const char *what, void *out,
+                           int64_t capacity_elems);
+
+/* Hierarchy summary in the layout of the reference's verbose setup print
+ * (src/setup.jl:405-473).  Valid until the next call. */
+const char *draugr_b200_summary(int32_t handle);
+
+/* Device memory held by the hierarchy, in bytes (0 if host-only). */
+int64_t draugr_b200_device_bytes(int32_t handle);
+
+/* Solve / cycle on device vectors (no host copies).  Same semantics as
+ * draugr_amg_solve / draugr_amg_cycle. */
+int32_t draugr_b200_solve_device(int32_t handle, int32_t n, double *x_dev, const double *b_dev,
+                                 int32_t config_handle, double tol, int32_t maxiter);
+int32_t draugr_b200_cycle_device(int32_t handle, int32_t n, double *x_dev, const double *b_dev,
+                                 int32_t config_handle);
+
+/* Partial resetup from new values of the finest matrix already on the
+ * device (same pattern as at setup), nnz entries. */
+int32_t draugr_b200_resetup_values_device(int32_t handle, int64_t nnz, const double *nzval_dev);
+
+/* Conjugate gradients preconditioned by one AMG cycle per iteration, until
+ * ||b - A x|| / ||b|| < tol.  precision 0: FP64 cycle.  precision 1: cycle
+ * on FP32 copies of the hierarchy with FP64 outer residual, products with A,
+ * dot products and updates.  x holds the initial guess.  relres (may be
+ * NULL) receives the final relative residual.  Returns iterations or -1.
+ * The reference has no Krylov solver of its own (it hands amg_cycle! to
+ * LinearSolve.jl through ldiv!, src/preconditioner.jl:76-102). */
+int32_t draugr_b200_pcg(int32_t handle, int32_t n, double *x, const double *b,
+                        int32_t config_handle, double tol, int32_t maxiter, int32_t precision,
+                        double *relres);
+int32_t draugr_b200_pcg_device(int32_t handle, int32_t n, double *x_dev, const double *b_dev,
+                               int32_t config_handle, double tol, int32_t maxiter,
+                               int32_t precision, double *relres);
+
+/* One operation on one level, host arrays in and out (kernel-level checks).
+ * op 0: y = A x (in1 = x)            op 1: r = b - A x (in1 = x, in2 = b)
+ * op 2: `steps` smoother sweeps from x (in1) for rhs b (in2)
+ * op 3: b_c = Pᵀ r (in1 = r)         op 4: x + P x_c (in1 = x, in2 = x_c)
+ * op 5: coarsest solve (in1 = b_c; lvl ignored)
+ * op 6: first Jacobi step from zero fused with the residual (in1 = b);
+ *       out holds x1 then r (2n values)
+ * precision 0 = FP64, 1 = FP32 kernels (inputs rounded to FP32). */
+int32_t draugr_b200_level_op(int32_t handle, int32_t lvl, int32_t op, int32_t precision,
+                             const double *in1, const double *in2, double *out, int32_t steps);
+
+/* Mean device time of `reps` launches of a level kernel (op 2: one Jacobi
+ * sweep, op 0: SpMV), measured with CUDA events on the hierarchy's stream. */
+int32_t draugr_b200_time_level_op(int32_t handle, int32_t lvl, int32_t op, int32_t precision,
+                                  int32_t reps, float *ms_per_launch);
+
+/* Run this hierarchy's work on the caller's CUDA stream (a cudaStream_t;
+ * NULL returns to the library's own non-blocking stream).  Entry points
+ * still return only after their work on that stream is complete. */
+int32_t draugr_b200_set_stream(int32_t handle, void *stream);
+
+/* Number of CUDA kernels this library has launched in the process so far
+ * (each launch of a captured CUDA graph adds the kernels it contains). */
+int64_t draugr_b200_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DRAUGR_B200_H */

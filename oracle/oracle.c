@@ -1,0 +1,613 @@
+/*
+ * ORACLE — test infrastructure, not part of the product.
+ *
+ * A plain-C restatement of the arithmetic of Draugr.jl's AMG solve phase and
+ * numeric resetup, used only by the tests, by __graft_entry__.smoke() and by
+ * bench.py's CPU-baseline / reference arms to check and to time against.  It
+ * follows the reference's loops in order (sums accumulated left to right,
+ * products rounded separately), so for a given hierarchy it reproduces what
+ * the reference computes on its CPU backend up to the order of dot-product
+ * reductions.  Each function cites the reference routine it restates
+ * (paths relative to the Draugr.jl repository).
+ *
+ * The reference is Julia and cannot run here; this restatement is pinned
+ * against the reference's own test assertions (tests/test_oracle_pins.py):
+ * restriction = explicit Pᵀr, Galerkin = explicit PᵀAP, Jacobi invdiag 0.5,
+ * l1 invdiag 0.25, colouring validity, convergence thresholds.
+ *
+ * Row loops run under OpenMP with a static schedule in chunks of 64 rows,
+ * as the reference's KernelAbstractions CPU(static=true) backend with
+ * workgroup size 64 (src/Draugr.jl:10, src/setup.jl:48).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define CHUNK 64
+
+/* ------------------------------------------------------------------ types */
+typedef struct {
+  int n, nc;
+  const int *A_rp, *A_ci;
+  double *A_v;
+  const int *P_rp, *P_ci;
+  const double *P_v;
+  const int *T_off, *T_rows, *T_pnz;
+  int smoother; /* 0 jacobi, 1 colored_gs, 5 l1_jacobi, 6 l1_colored_gs */
+  double omega;
+  double *invd;
+  int ncolors;
+  const int *color_off, *color_order;
+  double *r, *xc, *bc, *tmp;
+  /* Galerkin restriction map (orc_coarse_sparsity) for the resetup */
+  const int64_t *nz_off;
+  const int *tpi, *tai, *tpj;
+} olevel;
+
+typedef struct {
+  int nlevels;
+  olevel *lv;
+  int nc;
+  double *dense; /* column-major nc x nc */
+  double *lu;
+  int *piv;
+  double *cx, *cb;
+  double *solve_r;
+  double *coarse_v; /* values of the coarsest CSR when nlevels == 0 */
+  const int *coarse_rp, *coarse_ci;
+} ohier;
+
+/* ------------------------------------------------------ CSR kernels */
+/* y = A x : csr_mul_kernel!, src/csr_matrix.jl:150-159 */
+void orc_spmv(int n, const int *rp, const int *ci, const double *v, const double *x, double *y) {
+#pragma omp parallel for schedule(static, CHUNK)
+  for (int i = 0; i < n; ++i) {
+    double s = 0.0;
+    for (int k = rp[i]; k < rp[i + 1]; ++k) s += v[k] * x[ci[k]];
+    y[i] = s;
+  }
+}
+
+/* r = b - A x : residual_kernel!, src/cycle.jl:32-43 */
+void orc_residual(int n, const int *rp, const int *ci, const double *v, const double *x,
+                  const double *b, double *r) {
+#pragma omp parallel for schedule(static, CHUNK)
+  for (int i = 0; i < n; ++i) {
+    double ax = 0.0;
+    for (int k = rp[i]; k < rp[i + 1]; ++k) ax += v[k] * x[ci[k]];
+    r[i] = b[i] - ax;
+  }
+}
+
+/* invdiag_kernel!, src/smoothers.jl:47-63 */
+void orc_invdiag(int n, const int *rp, const int *ci, const double *v, double *invd) {
+#pragma omp parallel for schedule(static, CHUNK)
+  for (int i = 0; i < n; ++i) {
+    double d = 0.0, rn = 0.0;
+    for (int k = rp[i]; k < rp[i + 1]; ++k) {
+      rn += fabs(v[k]);
+      if (ci[k] == i) d = v[k];
+    }
+    double thr = 2.220446049250313e-16 * (rn > 1.0 ? rn : 1.0);
+    invd[i] = fabs(d) > thr ? 1.0 / d : 0.0;
+  }
+}
+
+/* l1_invdiag_kernel!, src/smoothers.jl:816-827 */
+void orc_l1_invdiag(int n, const int *rp, const double *v, double *invd) {
+#pragma omp parallel for schedule(static, CHUNK)
+  for (int i = 0; i < n; ++i) {
+    double l1 = 0.0;
+    for (int k = rp[i]; k < rp[i + 1]; ++k) l1 += fabs(v[k]);
+    invd[i] = l1 > 2.220446049250313e-16 ? 1.0 / l1 : 0.0;
+  }
+}
+
+/* smooth!(::JacobiSmoother / ::L1JacobiSmoother): jacobi_kernel! with the
+ * tmp/x ping-pong and the copy back on odd step counts,
+ * src/smoothers.jl:78-124, :835-854 */
+void orc_jacobi(int n, const int *rp, const int *ci, const double *v, const double *invd,
+                double omega, double *x, const double *b, int steps, double *tmp) {
+  double *src = x, *dst = tmp;
+  for (int s = 0; s < steps; ++s) {
+#pragma omp parallel for schedule(static, CHUNK)
+    for (int i = 0; i < n; ++i) {
+      double ri = b[i];
+      for (int k = rp[i]; k < rp[i + 1]; ++k) ri -= v[k] * src[ci[k]];
+      dst[i] = src[i] + omega * invd[i] * ri;
+    }
+    double *t = src;
+    src = dst;
+    dst = t;
+  }
+  if (steps & 1) memcpy(x, tmp, (size_t)n * sizeof(double));
+}
+
+/* greedy_coloring, src/smoothers.jl:136-159; returns the number of colours */
+int orc_greedy_coloring(int n, const int *rp, const int *ci, int *colors) {
+  int ncol = 0;
+  int cap = 64;
+  int *stamp = (int *)malloc(sizeof(int) * cap);
+  for (int c = 0; c < cap; ++c) stamp[c] = -1;
+  for (int i = 0; i < n; ++i) colors[i] = 0;
+  for (int i = 0; i < n; ++i) {
+    for (int k = rp[i]; k < rp[i + 1]; ++k) {
+      int j = ci[k];
+      if (j != i && colors[j] > 0) {
+        int c = colors[j];
+        if (c >= cap) {
+          int nc2 = 2 * c + 2;
+          stamp = (int *)realloc(stamp, sizeof(int) * nc2);
+          for (int t = cap; t < nc2; ++t) stamp[t] = -1;
+          cap = nc2;
+        }
+        stamp[c] = i;
+      }
+    }
+    int c = 1;
+    while (c < cap && stamp[c] == i) ++c;
+    colors[i] = c;
+    if (c > ncol) ncol = c;
+  }
+  free(stamp);
+  return ncol;
+}
+
+/* colour-sorted node order, src/smoothers.jl:168-195 (0-based offsets) */
+void orc_color_order(int n, const int *colors, int ncol, int *off, int *order) {
+  for (int c = 0; c <= ncol; ++c) off[c] = 0;
+  for (int i = 0; i < n; ++i) off[colors[i]]++;
+  /* off[c] holds the count of colour c (1-based); prefix to starts */
+  int acc = 0;
+  for (int c = 1; c <= ncol; ++c) {
+    int cnt = off[c];
+    off[c] = acc + cnt;
+    acc += cnt;
+  }
+  off[0] = 0;
+  int *pos = (int *)malloc(sizeof(int) * (ncol + 1));
+  for (int c = 1; c <= ncol; ++c) pos[c] = off[c - 1];
+  for (int i = 0; i < n; ++i) order[pos[colors[i]]++] = i;
+  free(pos);
+}
+
+/* smooth!(::ColoredGaussSeidelSmoother) / L1 variant: gs_color_kernel! per
+ * colour in ascending colour order, src/smoothers.jl:203-241, :296-313 */
+void orc_gs(int n, const int *rp, const int *ci, const double *v, const double *invd, int ncol,
+            const int *off, const int *order, double *x, const double *b, int steps) {
+  (void)n;
+  for (int s = 0; s < steps; ++s)
+    for (int c = 0; c < ncol; ++c) {
+      int st = off[c], cnt = off[c + 1] - off[c];
+#pragma omp parallel for schedule(static, CHUNK)
+      for (int t = 0; t < cnt; ++t) {
+        int i = order[st + t];
+        double ri = b[i];
+        for (int k = rp[i]; k < rp[i + 1]; ++k) ri -= v[k] * x[ci[k]];
+        x[i] += invd[i] * ri;
+      }
+    }
+}
+
+/* build_transpose_map, src/prolongation.jl:767-800 */
+void orc_transpose_map(int nf, int nc, const int *prp, const int *pci, int *off, int *rows,
+                       int *pnz) {
+  for (int j = 0; j <= nc; ++j) off[j] = 0;
+  for (int i = 0; i < nf; ++i)
+    for (int k = prp[i]; k < prp[i + 1]; ++k) off[pci[k] + 1]++;
+  for (int j = 0; j < nc; ++j) off[j + 1] += off[j];
+  int *pos = (int *)malloc(sizeof(int) * (nc > 0 ? nc : 1));
+  for (int j = 0; j < nc; ++j) pos[j] = off[j];
+  for (int i = 0; i < nf; ++i)
+    for (int k = prp[i]; k < prp[i + 1]; ++k) {
+      int J = pci[k];
+      rows[pos[J]] = i;
+      pnz[pos[J]] = k;
+      pos[J]++;
+    }
+  free(pos);
+}
+
+/* restrict_kernel!, src/prolongation.jl:805-827 */
+void orc_restrict(int nc, const int *off, const int *rows, const int *pnz, const double *pv,
+                  const double *r, double *bc) {
+#pragma omp parallel for schedule(static, CHUNK)
+  for (int J = 0; J < nc; ++J) {
+    double acc = 0.0;
+    for (int k = off[J]; k < off[J + 1]; ++k) acc += pv[pnz[k]] * r[rows[k]];
+    bc[J] = acc;
+  }
+}
+
+/* prolongate_kernel!, src/prolongation.jl:742-760 (x updated per entry) */
+void orc_prolongate(int nf, const int *prp, const int *pci, const double *pv, const double *xc,
+                    double *x) {
+#pragma omp parallel for schedule(static, CHUNK)
+  for (int i = 0; i < nf; ++i)
+    for (int k = prp[i]; k < prp[i + 1]; ++k) x[i] += pv[k] * xc[pci[k]];
+}
+
+/* ------------------------------------------------------ Galerkin product */
+/* compute_coarse_sparsity, src/galerkin.jl:11-183: triples in the loop
+ * order (fine row i, P entry of i, A entry, P entry of j), counting sort by
+ * coarse row, sorted unique columns per coarse row, values accumulated in
+ * triple order, and the RestrictionMap with triples grouped by destination
+ * in stable order.  Call once with c_rp only (other outputs NULL) to get
+ * the sizes: returns ntriples, writes c_rp (nc+1).  Call again with all
+ * outputs allocated. */
+static int cmp_int(const void *a, const void *b) {
+  int x = *(const int *)a, y = *(const int *)b;
+  return (x > y) - (x < y);
+}
+
+int64_t orc_coarse_sparsity(int nf, int nc, const int *arp, const int *aci, const double *av,
+                            const int *prp, const int *pci, const double *pv, int *c_rp,
+                            int *c_ci, double *c_v, int64_t *nz_off, int *tpi, int *tai, int *tpj) {
+  int64_t nt = 0;
+  for (int i = 0; i < nf; ++i)
+    for (int a = prp[i]; a < prp[i + 1]; ++a)
+      for (int k = arp[i]; k < arp[i + 1]; ++k) {
+        int j = aci[k];
+        nt += prp[j + 1] - prp[j];
+      }
+  int *rI = (int *)malloc(sizeof(int) * (nt ? nt : 1));
+  int *rJ = (int *)malloc(sizeof(int) * (nt ? nt : 1));
+  int *rpi = (int *)malloc(sizeof(int) * (nt ? nt : 1));
+  int *rai = (int *)malloc(sizeof(int) * (nt ? nt : 1));
+  int *rpj = (int *)malloc(sizeof(int) * (nt ? nt : 1));
+  int64_t t = 0;
+  for (int i = 0; i < nf; ++i)
+    for (int a = prp[i]; a < prp[i + 1]; ++a) {
+      int I = pci[a];
+      for (int k = arp[i]; k < arp[i + 1]; ++k) {
+        int j = aci[k];
+        for (int b = prp[j]; b < prp[j + 1]; ++b) {
+          rI[t] = I;
+          rJ[t] = pci[b];
+          rpi[t] = a;
+          rai[t] = k;
+          rpj[t] = b;
+          ++t;
+        }
+      }
+    }
+  /* counting sort by coarse row */
+  int64_t *rtmp = (int64_t *)calloc((size_t)nc + 1, sizeof(int64_t));
+  for (int64_t s = 0; s < nt; ++s) rtmp[rI[s] + 1]++;
+  for (int r = 0; r < nc; ++r) rtmp[r + 1] += rtmp[r];
+  int64_t *perm = (int64_t *)malloc(sizeof(int64_t) * (nt ? nt : 1));
+  int64_t *pos = (int64_t *)malloc(sizeof(int64_t) * ((size_t)nc + 1));
+  for (int r = 0; r < nc; ++r) pos[r] = rtmp[r];
+  for (int64_t s = 0; s < nt; ++s) perm[pos[rI[s]]++] = s;
+  /* unique sorted columns per row */
+  int *buf = (int *)malloc(sizeof(int) * (nt ? nt : 1));
+  c_rp[0] = 0;
+  for (int r = 0; r < nc; ++r) {
+    int64_t rs = rtmp[r], re = rtmp[r + 1];
+    int len = (int)(re - rs);
+    int nu = 0;
+    if (len > 0) {
+      for (int64_t k = rs; k < re; ++k) buf[k - rs] = rJ[perm[k]];
+      qsort(buf, len, sizeof(int), cmp_int);
+      nu = 1;
+      for (int k = 1; k < len; ++k)
+        if (buf[k] != buf[k - 1]) ++nu;
+    }
+    c_rp[r + 1] = c_rp[r] + nu;
+  }
+  if (c_ci) {
+    int *rci = (int *)malloc(sizeof(int) * (nt ? nt : 1));
+    for (int r = 0; r < nc; ++r) {
+      int64_t rs = rtmp[r], re = rtmp[r + 1];
+      int len = (int)(re - rs);
+      if (len == 0) continue;
+      for (int64_t k = rs; k < re; ++k) buf[k - rs] = rJ[perm[k]];
+      qsort(buf, len, sizeof(int), cmp_int);
+      int p = c_rp[r];
+      c_ci[p] = buf[0];
+      for (int k = 1; k < len; ++k)
+        if (buf[k] != buf[k - 1]) c_ci[++p] = buf[k];
+      int lo0 = c_rp[r], hi0 = c_rp[r + 1] - 1;
+      for (int64_t k = rs; k < re; ++k) {
+        int64_t s = perm[k];
+        int J = rJ[s], lo = lo0, hi = hi0, at = -1;
+        while (lo <= hi) {
+          int mid = (lo + hi) >> 1;
+          if (c_ci[mid] == J) { at = mid; break; }
+          if (c_ci[mid] < J) lo = mid + 1; else hi = mid - 1;
+        }
+        rci[s] = at;
+      }
+    }
+    for (int k = 0; k < c_rp[nc]; ++k) c_v[k] = 0.0;
+    /* values in row order, triples of a row in generation order */
+    for (int r = 0; r < nc; ++r)
+      for (int64_t k = rtmp[r]; k < rtmp[r + 1]; ++k) {
+        int64_t s = perm[k];
+        c_v[rci[s]] += pv[rpi[s]] * av[rai[s]] * pv[rpj[s]];
+      }
+    /* restriction map: stable grouping by destination */
+    int nnzc = c_rp[nc];
+    for (int k = 0; k <= nnzc; ++k) nz_off[k] = 0;
+    for (int64_t s = 0; s < nt; ++s) nz_off[rci[s] + 1]++;
+    for (int k = 0; k < nnzc; ++k) nz_off[k + 1] += nz_off[k];
+    int64_t *wp = (int64_t *)malloc(sizeof(int64_t) * (nnzc ? nnzc : 1));
+    for (int k = 0; k < nnzc; ++k) wp[k] = nz_off[k];
+    for (int64_t s = 0; s < nt; ++s) {
+      int64_t q = wp[rci[s]]++;
+      tpi[q] = rpi[s];
+      tai[q] = rai[s];
+      tpj[q] = rpj[s];
+    }
+    free(wp);
+    free(rci);
+  }
+  free(buf);
+  free(pos);
+  free(perm);
+  free(rtmp);
+  free(rI);
+  free(rJ);
+  free(rpi);
+  free(rai);
+  free(rpj);
+  return nt;
+}
+
+/* galerkin_nz_kernel!, src/galerkin.jl:194-222 */
+void orc_galerkin(int nnzc, const int64_t *nz_off, const int *tpi, const int *tai, const int *tpj,
+                  const double *pv, const double *av, double *cv) {
+#pragma omp parallel for schedule(static, CHUNK)
+  for (int k = 0; k < nnzc; ++k) {
+    double acc = 0.0;
+    for (int64_t t = nz_off[k]; t < nz_off[k + 1]; ++t) acc += pv[tpi[t]] * av[tai[t]] * pv[tpj[t]];
+    cv[k] = acc;
+  }
+}
+
+/* _recompute_coarsest_dense!, src/resetup.jl:123-158 (column-major M) */
+void orc_coarsest_dense(int nf, int nc, const int *arp, const int *aci, const double *av,
+                        const int *prp, const int *pci, const double *pv, double *M) {
+  memset(M, 0, sizeof(double) * (size_t)nc * nc);
+  for (int i = 0; i < nf; ++i)
+    for (int a = prp[i]; a < prp[i + 1]; ++a) {
+      int I = pci[a];
+      double p_i = pv[a];
+      for (int k = arp[i]; k < arp[i + 1]; ++k) {
+        int j = aci[k];
+        double aij = av[k];
+        for (int b = prp[j]; b < prp[j + 1]; ++b) M[(size_t)pci[b] * nc + I] += p_i * aij * pv[b];
+      }
+    }
+}
+
+/* _csr_to_dense!, src/setup.jl:495-516 (later entries of a row overwrite) */
+void orc_csr_to_dense(int n, const int *rp, const int *ci, const double *v, double *M) {
+  memset(M, 0, sizeof(double) * (size_t)n * n);
+  for (int i = 0; i < n; ++i)
+    for (int k = rp[i]; k < rp[i + 1]; ++k) M[(size_t)ci[k] * n + i] = v[k];
+}
+
+/* ------------------------------------------------------ coarsest LU */
+/* lu(M) for the coarsest level (src/setup.jl:526-534, src/resetup.jl:44):
+ * LAPACK dgetf2 semantics — pivot = first row of largest magnitude, column
+ * scaled by the reciprocal of the pivot, rank-1 update.  Returns 0 or the
+ * 1-based index of the first zero pivot (Julia raises SingularException). */
+int orc_lu_factor(int n, double *a, int *piv) {
+  for (int j = 0; j < n; ++j) {
+    int p = j;
+    double mx = fabs(a[(size_t)j * n + j]);
+    for (int i = j + 1; i < n; ++i)
+      if (fabs(a[(size_t)j * n + i]) > mx) { mx = fabs(a[(size_t)j * n + i]); p = i; }
+    piv[j] = p;
+    if (a[(size_t)j * n + p] == 0.0) return j + 1;
+    if (p != j)
+      for (int c = 0; c < n; ++c) {
+        double t = a[(size_t)c * n + j];
+        a[(size_t)c * n + j] = a[(size_t)c * n + p];
+        a[(size_t)c * n + p] = t;
+      }
+    double r = 1.0 / a[(size_t)j * n + j];
+    for (int i = j + 1; i < n; ++i) a[(size_t)j * n + i] *= r;
+    for (int c = j + 1; c < n; ++c) {
+      double t = a[(size_t)c * n + j];
+      for (int i = j + 1; i < n; ++i) a[(size_t)c * n + i] -= a[(size_t)j * n + i] * t;
+    }
+  }
+  return 0;
+}
+
+/* ldiv!(x, F, b) with dgetrs semantics: row interchanges, then the
+ * column-oriented unit-lower and upper triangular solves of dtrsv. */
+void orc_lu_solve(int n, const double *lu, const int *piv, double *y) {
+  for (int j = 0; j < n; ++j)
+    if (piv[j] != j) {
+      double t = y[j];
+      y[j] = y[piv[j]];
+      y[piv[j]] = t;
+    }
+  for (int j = 0; j < n; ++j)
+    if (y[j] != 0.0)
+      for (int i = j + 1; i < n; ++i) y[i] -= y[j] * lu[(size_t)j * n + i];
+  for (int j = n - 1; j >= 0; --j)
+    if (y[j] != 0.0) {
+      y[j] /= lu[(size_t)j * n + j];
+      double t = y[j];
+      for (int i = 0; i < j; ++i) y[i] -= t * lu[(size_t)j * n + i];
+    }
+}
+
+/* ------------------------------------------------------ cycle and solve */
+static void smooth(olevel *L, double *x, const double *b, int steps) {
+  if (steps <= 0) return;
+  if (L->smoother == 0 || L->smoother == 5)
+    orc_jacobi(L->n, L->A_rp, L->A_ci, L->A_v, L->invd, L->omega, x, b, steps, L->tmp);
+  else
+    orc_gs(L->n, L->A_rp, L->A_ci, L->A_v, L->invd, L->ncolors, L->color_off, L->color_order, x, b,
+           steps);
+}
+
+/* _vcycle_descend!, src/cycle.jl:63-99 */
+static void vcycle(ohier *h, int lvl, double *x, const double *b, int pre, int post, int w) {
+  olevel *L = &h->lv[lvl];
+  smooth(L, x, b, pre);
+  orc_residual(L->n, L->A_rp, L->A_ci, L->A_v, x, b, L->r);
+  orc_restrict(L->nc, L->T_off, L->T_rows, L->T_pnz, L->P_v, L->r, L->bc);
+  memset(L->xc, 0, sizeof(double) * (size_t)L->nc);
+  if (lvl + 1 < h->nlevels) {
+    int nr = w ? 2 : 1;
+    for (int t = 0; t < nr; ++t) vcycle(h, lvl + 1, L->xc, L->bc, pre, post, w);
+  } else {
+    memcpy(h->cb, L->bc, sizeof(double) * (size_t)h->nc);
+    memcpy(h->cx, h->cb, sizeof(double) * (size_t)h->nc);
+    orc_lu_solve(h->nc, h->lu, h->piv, h->cx);
+    memcpy(L->xc, h->cx, sizeof(double) * (size_t)h->nc);
+  }
+  orc_prolongate(L->n, L->P_rp, L->P_ci, L->P_v, L->xc, x);
+  smooth(L, x, b, post);
+}
+
+/* amg_cycle!, src/cycle.jl:12-28 */
+void orc_cycle(ohier *h, double *x, const double *b, int pre, int post, int w) {
+  if (h->nlevels == 0) {
+    memcpy(h->cx, b, sizeof(double) * (size_t)h->nc);
+    orc_lu_solve(h->nc, h->lu, h->piv, h->cx);
+    memcpy(x, h->cx, sizeof(double) * (size_t)h->nc);
+    return;
+  }
+  vcycle(h, 0, x, b, pre, post, w);
+}
+
+static double dot(int n, const double *a, const double *b) {
+  double s = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : s)
+  for (int i = 0; i < n; ++i) s += a[i] * b[i];
+  return s;
+}
+
+/* amg_solve!, src/cycle.jl:110-160; returns iterations, relres[0] final */
+int orc_solve(ohier *h, double *x, const double *b, int pre, int post, int w, double tol,
+              int maxiter, double *relres) {
+  int n = h->nlevels ? h->lv[0].n : h->nc;
+  double bnorm = sqrt(dot(n, b, b));
+  if (bnorm == 0.0) {
+    memset(x, 0, sizeof(double) * (size_t)n);
+    if (relres) *relres = 0.0;
+    return 0;
+  }
+  if (h->nlevels == 0) {
+    orc_cycle(h, x, b, pre, post, w);
+    if (relres) *relres = NAN;
+    return 1;
+  }
+  olevel *L = &h->lv[0];
+  double rel = 1.0;
+  for (int it = 1; it <= maxiter; ++it) {
+    orc_cycle(h, x, b, pre, post, w);
+    orc_residual(n, L->A_rp, L->A_ci, L->A_v, x, b, h->solve_r);
+    rel = sqrt(dot(n, h->solve_r, h->solve_r)) / bnorm;
+    if (rel < tol) {
+      if (relres) *relres = rel;
+      return it;
+    }
+  }
+  if (relres) *relres = rel;
+  return maxiter;
+}
+
+/* Textbook preconditioned CG around amg_cycle! with a zeroed iterate per
+ * application (preconditioner_apply!, src/preconditioner.jl:76-80).  The
+ * reference has no CG of its own; this is the standard algorithm.
+ * work: 4n doubles (r, z, p, q). */
+int orc_pcg(ohier *h, double *x, const double *b, int pre, int post, int w, double tol,
+            int maxiter, double *relres, double *work) {
+  int n = h->nlevels ? h->lv[0].n : h->nc;
+  const int *rp = h->nlevels ? h->lv[0].A_rp : h->coarse_rp;
+  const int *ci = h->nlevels ? h->lv[0].A_ci : h->coarse_ci;
+  const double *v = h->nlevels ? h->lv[0].A_v : h->coarse_v;
+  double *r = work, *z = work + n, *p = work + 2 * (size_t)n, *q = work + 3 * (size_t)n;
+  orc_residual(n, rp, ci, v, x, b, r);
+  double bnorm = sqrt(dot(n, b, b));
+  if (bnorm == 0.0) {
+    memset(x, 0, sizeof(double) * (size_t)n);
+    if (relres) *relres = 0.0;
+    return 0;
+  }
+  double rel = sqrt(dot(n, r, r)) / bnorm;
+  if (rel < tol) {
+    if (relres) *relres = rel;
+    return 0;
+  }
+  memset(z, 0, sizeof(double) * (size_t)n);
+  orc_cycle(h, z, r, pre, post, w);
+  memcpy(p, z, sizeof(double) * (size_t)n);
+  double rz = dot(n, r, z);
+  int it;
+  for (it = 1; it <= maxiter; ++it) {
+    orc_spmv(n, rp, ci, v, p, q);
+    double alpha = rz / dot(n, p, q);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+      x[i] += alpha * p[i];
+      r[i] -= alpha * q[i];
+    }
+    rel = sqrt(dot(n, r, r)) / bnorm;
+    if (rel < tol || it == maxiter) break;
+    memset(z, 0, sizeof(double) * (size_t)n);
+    orc_cycle(h, z, r, pre, post, w);
+    double rzn = dot(n, r, z);
+    double beta = rzn / rz;
+    rz = rzn;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
+  }
+  if (it > maxiter) it = maxiter;
+  if (relres) *relres = rel;
+  return it;
+}
+
+/* ------------------------------------------------------ resetup */
+/* amg_resetup!(partial=true), src/resetup.jl:20-45: new finest values,
+ * smoother diagonals, Galerkin products through the restriction maps, the
+ * coarsest dense product (src/resetup.jl:123-158) and its LU.  coarse_rp /
+ * coarse_ci / coarse_v describe the coarsest CSR when nlevels == 0.
+ * Returns 0 or the LU's zero-pivot index. */
+static void upd_invd(olevel *L) {
+  if (L->smoother == 5 || L->smoother == 6) orc_l1_invdiag(L->n, L->A_rp, L->A_v, L->invd);
+  else orc_invdiag(L->n, L->A_rp, L->A_ci, L->A_v, L->invd);
+}
+
+int orc_resetup(ohier *h, const double *v0, int64_t nnz0) {
+  if (h->nlevels == 0) {
+    memcpy(h->coarse_v, v0, sizeof(double) * (size_t)nnz0);
+    orc_csr_to_dense(h->nc, h->coarse_rp, h->coarse_ci, h->coarse_v, h->dense);
+  } else {
+    memcpy(h->lv[0].A_v, v0, sizeof(double) * (size_t)nnz0);
+    upd_invd(&h->lv[0]);
+    for (int l = 0; l + 1 < h->nlevels; ++l) {
+      olevel *L = &h->lv[l], *N = &h->lv[l + 1];
+      int nnzc = N->A_rp[N->n];
+      orc_galerkin(nnzc, L->nz_off, L->tpi, L->tai, L->tpj, L->P_v, L->A_v, N->A_v);
+      upd_invd(N);
+    }
+    olevel *last = &h->lv[h->nlevels - 1];
+    orc_coarsest_dense(last->n, h->nc, last->A_rp, last->A_ci, last->A_v, last->P_rp, last->P_ci,
+                       last->P_v, h->dense);
+  }
+  memcpy(h->lu, h->dense, sizeof(double) * (size_t)h->nc * h->nc);
+  return orc_lu_factor(h->nc, h->lu, h->piv);
+}
+
+/* ------------------------------------------------------ setup pieces */
+/* absolute_strength_kernel!, src/strength.jl:38-76 */
+void orc_strength_abs(int n, const int *rp, const int *ci, const double *v, double theta,
+                      uint8_t *s) {
+  for (int i = 0; i < n; ++i) {
+    double mx = 0.0;
+    for (int k = rp[i]; k < rp[i + 1]; ++k)
+      if (ci[k] != i && fabs(v[k]) > mx) mx = fabs(v[k]);
+    double thr = theta * mx;
+    for (int k = rp[i]; k < rp[i + 1]; ++k) s[k] = (ci[k] != i) ? (fabs(v[k]) >= thr) : 0;
+  }
+}

@@ -1,0 +1,313 @@
+"""ORACLE — test infrastructure, not part of the product.
+
+ctypes harness around liboracle.so (oracle.c), the CPU restatement of
+Draugr.jl's solve-phase arithmetic.  Only tests/, __graft_entry__.smoke()
+and bench.py's CPU-baseline / reference arms use it, as the checker or as
+the timed CPU reference; the library in draugr.jl_b200/ never calls it.
+
+OracleHierarchy takes the hierarchy *structure* a product hierarchy exports
+(A, P, transpose map, colours of every level and the coarsest LU) — the
+shared input of both sides — and runs the reference's cycle, stationary
+solve, a textbook PCG and the reference's triple-map Galerkin resetup on it.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import pathlib
+import subprocess
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle.so"
+_lib = None
+
+
+def build() -> pathlib.Path:
+    subprocess.run(["make", "-C", str(HERE)], check=True, capture_output=True)
+    return LIB_PATH
+
+
+def load() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        _lib = C.CDLL(str(LIB_PATH))
+        _declare(_lib)
+    return _lib
+
+
+P = C.c_void_p
+i32, i64, f64 = C.c_int, C.c_int64, C.c_double
+
+
+class OLevel(C.Structure):
+    _fields_ = [("n", i32), ("nc", i32), ("A_rp", P), ("A_ci", P), ("A_v", P), ("P_rp", P),
+                ("P_ci", P), ("P_v", P), ("T_off", P), ("T_rows", P), ("T_pnz", P),
+                ("smoother", i32), ("omega", f64), ("invd", P), ("ncolors", i32),
+                ("color_off", P), ("color_order", P), ("r", P), ("xc", P), ("bc", P),
+                ("tmp", P), ("nz_off", P), ("tpi", P), ("tai", P), ("tpj", P)]
+
+
+class OHier(C.Structure):
+    _fields_ = [("nlevels", i32), ("lv", C.POINTER(OLevel)), ("nc", i32), ("dense", P),
+                ("lu", P), ("piv", P), ("cx", P), ("cb", P), ("solve_r", P), ("coarse_v", P),
+                ("coarse_rp", P), ("coarse_ci", P)]
+
+
+def _declare(lib):
+    sig = {
+        "orc_spmv": (None, [i32, P, P, P, P, P]),
+        "orc_residual": (None, [i32, P, P, P, P, P, P]),
+        "orc_invdiag": (None, [i32, P, P, P, P]),
+        "orc_l1_invdiag": (None, [i32, P, P, P]),
+        "orc_jacobi": (None, [i32, P, P, P, P, f64, P, P, i32, P]),
+        "orc_greedy_coloring": (i32, [i32, P, P, P]),
+        "orc_color_order": (None, [i32, P, i32, P, P]),
+        "orc_gs": (None, [i32, P, P, P, P, i32, P, P, P, P, i32]),
+        "orc_transpose_map": (None, [i32, i32, P, P, P, P, P]),
+        "orc_restrict": (None, [i32, P, P, P, P, P, P]),
+        "orc_prolongate": (None, [i32, P, P, P, P, P]),
+        "orc_coarse_sparsity": (i64, [i32, i32, P, P, P, P, P, P, P, P, P, P, P, P, P]),
+        "orc_galerkin": (None, [i32, P, P, P, P, P, P, P]),
+        "orc_coarsest_dense": (None, [i32, i32, P, P, P, P, P, P, P]),
+        "orc_csr_to_dense": (None, [i32, P, P, P, P]),
+        "orc_lu_factor": (i32, [i32, P, P]),
+        "orc_lu_solve": (None, [i32, P, P, P]),
+        "orc_cycle": (None, [C.POINTER(OHier), P, P, i32, i32, i32]),
+        "orc_solve": (i32, [C.POINTER(OHier), P, P, i32, i32, i32, f64, i32, P]),
+        "orc_pcg": (i32, [C.POINTER(OHier), P, P, i32, i32, i32, f64, i32, P, P]),
+        "orc_resetup": (i32, [C.POINTER(OHier), P, i64]),
+        "orc_strength_abs": (None, [i32, P, P, P, f64, P]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+def ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+# ---------------------------------------------------------------- array-level helpers
+def csr_parts(A):
+    A = A.tocsr()
+    return (A.shape[0], np.ascontiguousarray(A.indptr, np.int32),
+            np.ascontiguousarray(A.indices, np.int32), np.ascontiguousarray(A.data, np.float64))
+
+
+def spmv(n, rp, ci, v, x):
+    y = np.zeros(n)
+    load().orc_spmv(n, ptr(rp), ptr(ci), ptr(v), ptr(np.ascontiguousarray(x, np.float64)), ptr(y))
+    return y
+
+
+def residual(n, rp, ci, v, x, b):
+    r = np.zeros(n)
+    load().orc_residual(n, ptr(rp), ptr(ci), ptr(v), ptr(np.ascontiguousarray(x, np.float64)),
+                        ptr(np.ascontiguousarray(b, np.float64)), ptr(r))
+    return r
+
+
+def invdiag(n, rp, ci, v, l1=False):
+    d = np.zeros(n)
+    if l1:
+        load().orc_l1_invdiag(n, ptr(rp), ptr(v), ptr(d))
+    else:
+        load().orc_invdiag(n, ptr(rp), ptr(ci), ptr(v), ptr(d))
+    return d
+
+
+def jacobi(n, rp, ci, v, invd, omega, x, b, steps):
+    x = np.array(x, dtype=np.float64)
+    tmp = np.zeros(n)
+    load().orc_jacobi(n, ptr(rp), ptr(ci), ptr(v), ptr(invd), omega, ptr(x),
+                      ptr(np.ascontiguousarray(b, np.float64)), steps, ptr(tmp))
+    return x
+
+
+def greedy_coloring(n, rp, ci):
+    colors = np.zeros(n, np.int32)
+    nc = load().orc_greedy_coloring(n, ptr(rp), ptr(ci), ptr(colors))
+    off = np.zeros(nc + 1, np.int32)
+    order = np.zeros(n, np.int32)
+    load().orc_color_order(n, ptr(colors), nc, ptr(off), ptr(order))
+    return colors, nc, off, order
+
+
+def gs(n, rp, ci, v, invd, ncol, off, order, x, b, steps):
+    x = np.array(x, dtype=np.float64)
+    load().orc_gs(n, ptr(rp), ptr(ci), ptr(v), ptr(invd), ncol, ptr(off), ptr(order), ptr(x),
+                  ptr(np.ascontiguousarray(b, np.float64)), steps)
+    return x
+
+
+def transpose_map(nf, nc, prp, pci):
+    nnz = int(prp[nf])
+    off = np.zeros(nc + 1, np.int32)
+    rows = np.zeros(nnz, np.int32)
+    pnz = np.zeros(nnz, np.int32)
+    load().orc_transpose_map(nf, nc, ptr(prp), ptr(pci), ptr(off), ptr(rows), ptr(pnz))
+    return off, rows, pnz
+
+
+def restrict(nc, off, rows, pnz, pv, r):
+    bc = np.zeros(nc)
+    load().orc_restrict(nc, ptr(off), ptr(rows), ptr(pnz), ptr(pv),
+                        ptr(np.ascontiguousarray(r, np.float64)), ptr(bc))
+    return bc
+
+
+def prolongate(nf, prp, pci, pv, xc, x):
+    x = np.array(x, dtype=np.float64)
+    load().orc_prolongate(nf, ptr(prp), ptr(pci), ptr(pv), ptr(np.ascontiguousarray(xc, np.float64)),
+                          ptr(x))
+    return x
+
+
+def coarse_sparsity(nf, nc, arp, aci, av, prp, pci, pv):
+    """compute_coarse_sparsity: (c_rp, c_ci, c_v, nz_off, tpi, tai, tpj)."""
+    lib = load()
+    c_rp = np.zeros(nc + 1, np.int32)
+    nt = lib.orc_coarse_sparsity(nf, nc, ptr(arp), ptr(aci), ptr(av), ptr(prp), ptr(pci), ptr(pv),
+                                 ptr(c_rp), None, None, None, None, None, None)
+    nnzc = int(c_rp[nc])
+    c_ci = np.zeros(nnzc, np.int32)
+    c_v = np.zeros(nnzc)
+    nz_off = np.zeros(nnzc + 1, np.int64)
+    tpi = np.zeros(max(nt, 1), np.int32)
+    tai = np.zeros(max(nt, 1), np.int32)
+    tpj = np.zeros(max(nt, 1), np.int32)
+    lib.orc_coarse_sparsity(nf, nc, ptr(arp), ptr(aci), ptr(av), ptr(prp), ptr(pci), ptr(pv),
+                            ptr(c_rp), ptr(c_ci), ptr(c_v), ptr(nz_off), ptr(tpi), ptr(tai), ptr(tpj))
+    return c_rp, c_ci, c_v, nz_off, tpi, tai, tpj
+
+
+def lu_factor(M):
+    """Column-major LU of a dense matrix: (lu as an n x n array, piv, info)."""
+    n = M.shape[0]
+    a = np.ascontiguousarray(np.asarray(M, dtype=np.float64).T).ravel()  # column-major
+    piv = np.zeros(n, np.int32)
+    info = load().orc_lu_factor(n, ptr(a), ptr(piv))
+    return a.reshape(n, n).T, piv, info
+
+
+def strength_abs(n, rp, ci, v, theta):
+    s = np.zeros(len(ci), np.uint8)
+    load().orc_strength_abs(n, ptr(rp), ptr(ci), ptr(v), theta, ptr(s))
+    return s
+
+
+# ---------------------------------------------------------------- hierarchy mirror
+SMOOTHER_KIND = {0: "jacobi", 1: "colored_gs", 5: "l1_jacobi", 6: "l1_colored_gs"}
+
+
+class OracleHierarchy:
+    """The reference's solve phase on the structure of a product hierarchy.
+
+    `h` is a draugr.Hierarchy (possibly host-only).  Level values are copied;
+    with with_rmaps=True each level also gets the reference's Galerkin
+    RestrictionMap (built by the oracle from that level's A and P) so that
+    resetup() can run the reference's triple-map product.
+    """
+
+    def __init__(self, h, with_rmaps: bool = False):
+        self._keep = []
+        nl = h.nlevels
+        self.nlevels = nl
+        levels = (OLevel * max(nl, 1))()
+        self.levels_np = []
+        for l in range(nl):
+            info = h.level_info(l)
+            n, nc = int(info[0]), int(info[2])
+            d = dict(
+                A_rp=h.export(l, "A_rowptr"), A_ci=h.export(l, "A_colval"),
+                A_v=h.export(l, "A_nzval").copy(), P_rp=h.export(l, "P_rowptr"),
+                P_ci=h.export(l, "P_colval"), P_v=h.export(l, "P_nzval"),
+                T_off=h.export(l, "T_offsets"), T_rows=h.export(l, "T_rows"),
+                T_pnz=h.export(l, "T_pnz"), invd=h.export(l, "invdiag").copy(),
+                color_off=h.export(l, "color_offsets"), color_order=h.export(l, "color_order"),
+                r=np.zeros(n), xc=np.zeros(nc), bc=np.zeros(nc), tmp=np.zeros(n))
+            sk = int(info[4])
+            if sk not in SMOOTHER_KIND:
+                raise ValueError(f"smoother kind {sk} has no oracle")
+            omega = float(h.export(l, "omega")[0])
+            L = levels[l]
+            L.n, L.nc, L.smoother, L.omega = n, nc, sk, omega
+            L.ncolors = int(info[5])
+            for k in ("A_rp", "A_ci", "A_v", "P_rp", "P_ci", "P_v", "T_off", "T_rows", "T_pnz",
+                      "invd", "color_off", "color_order", "r", "xc", "bc", "tmp"):
+                setattr(L, k, ptr(d[k]))
+            self.levels_np.append(d)
+        self.nc = int(h.level_info(-1)[0])
+        self.coarse_rp = h.export(-1, "C_rowptr")
+        self.coarse_ci = h.export(-1, "C_colval")
+        self.coarse_v = h.export(-1, "C_nzval").copy()
+        self.dense = np.zeros(self.nc * self.nc)
+        load().orc_csr_to_dense(self.nc, ptr(self.coarse_rp), ptr(self.coarse_ci),
+                                ptr(self.coarse_v), ptr(self.dense))
+        self.lu = self.dense.copy()
+        self.piv = np.zeros(self.nc, np.int32)
+        info = load().orc_lu_factor(self.nc, ptr(self.lu), ptr(self.piv))
+        if info:
+            raise ZeroDivisionError(f"SingularException({info})")
+        self.cx = np.zeros(self.nc)
+        self.cb = np.zeros(self.nc)
+        n0 = int(h.level_info(0)[0]) if nl else self.nc
+        self.n = n0
+        self.solve_r = np.zeros(n0)
+        if with_rmaps:
+            for l in range(nl - 1):
+                d = self.levels_np[l]
+                nf, ncl = levels[l].n, levels[l].nc
+                c_rp, c_ci, c_v, nz_off, tpi, tai, tpj = coarse_sparsity(
+                    nf, ncl, d["A_rp"], d["A_ci"], d["A_v"], d["P_rp"], d["P_ci"], d["P_v"])
+                d.update(nz_off=nz_off, tpi=tpi, tai=tai, tpj=tpj, c_rp=c_rp, c_ci=c_ci)
+                L = levels[l]
+                L.nz_off, L.tpi, L.tai, L.tpj = ptr(nz_off), ptr(tpi), ptr(tai), ptr(tpj)
+        H = OHier()
+        H.nlevels = nl
+        H.lv = C.cast(levels, C.POINTER(OLevel))
+        H.nc = self.nc
+        H.dense, H.lu, H.piv = ptr(self.dense), ptr(self.lu), ptr(self.piv)
+        H.cx, H.cb, H.solve_r = ptr(self.cx), ptr(self.cb), ptr(self.solve_r)
+        H.coarse_v, H.coarse_rp, H.coarse_ci = (ptr(self.coarse_v), ptr(self.coarse_rp),
+                                                ptr(self.coarse_ci))
+        self._levels = levels
+        self.H = H
+
+    # solve phase -------------------------------------------------------
+    def cycle(self, x, b, pre=1, post=1, w=False):
+        x = np.array(x, dtype=np.float64)
+        b = np.ascontiguousarray(b, np.float64)
+        load().orc_cycle(C.byref(self.H), ptr(x), ptr(b), pre, post, int(w))
+        return x
+
+    def solve(self, x, b, pre=1, post=1, w=False, tol=1e-10, maxiter=100):
+        x = np.array(x, dtype=np.float64)
+        b = np.ascontiguousarray(b, np.float64)
+        rel = C.c_double(0)
+        it = load().orc_solve(C.byref(self.H), ptr(x), ptr(b), pre, post, int(w), tol, maxiter,
+                              C.byref(rel))
+        return x, it, rel.value
+
+    def pcg(self, x, b, pre=1, post=1, w=False, tol=1e-8, maxiter=500):
+        x = np.array(x, dtype=np.float64)
+        b = np.ascontiguousarray(b, np.float64)
+        work = np.zeros(4 * self.n)
+        rel = C.c_double(0)
+        it = load().orc_pcg(C.byref(self.H), ptr(x), ptr(b), pre, post, int(w), tol, maxiter,
+                            C.byref(rel), ptr(work))
+        return x, it, rel.value
+
+    def resetup(self, new_values):
+        v = np.ascontiguousarray(new_values, np.float64)
+        info = load().orc_resetup(C.byref(self.H), ptr(v), len(v))
+        if info:
+            raise ZeroDivisionError(f"SingularException({info})")
+
+    def level_values(self, l):
+        return self.levels_np[l]["A_v"]

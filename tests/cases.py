@@ -1,0 +1,22 @@
+"""Shared small parity cases: (matrix factory, AMGConfig), one per
+coarsening / smoother family on the hot path."""
+
+import draugr
+from draugr import problems
+
+CASES = {
+    "aggregation_jacobi": (lambda: problems.poisson2d(24),
+                           draugr.AMGConfig(coarsening=draugr.AggregationCoarsening(0.25),
+                                            smoother=draugr.JacobiSmootherType())),
+    "hypre_l1jacobi": (lambda: problems.heterogeneous_diffusion_3d(12, seed=3),
+                       draugr.hypre_default_config(agg_trunc_factor=0.2,
+                                                   smoother=draugr.L1JacobiSmootherType())),
+    "default_hmis_l1gs": (lambda: problems.poisson2d(20), draugr.AMGConfig()),
+    "pmis_direct_gs": (lambda: problems.poisson3d(10),
+                       draugr.AMGConfig(coarsening=draugr.PMISCoarsening(0.25),
+                                        smoother=draugr.ColoredGaussSeidelType())),
+    "aniso27_hmis": (lambda: problems.anisotropic_27pt(9, 1e-3),
+                     draugr.AMGConfig(coarsening=draugr.HMISCoarsening(
+                         0.25, draugr.ExtendedIInterpolation(0.2)),
+                         smoother=draugr.L1JacobiSmootherType())),
+}

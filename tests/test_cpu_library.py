@@ -1,0 +1,199 @@
+"""CPU tests of the library: it loads, exports every symbol its headers
+declare, parses configurations like the reference, reports errors like the
+reference, and its CPU-built hierarchy structure equals the oracle's
+restatement of the reference's structure routines (bit for bit)."""
+
+import re
+
+import numpy as np
+import pytest
+
+import draugr
+import oracle
+from conftest import ROOT
+from draugr import problems
+from draugr._lib import SIGNATURES, check
+
+HEADERS = [ROOT / "include" / "draugr_amg.h", ROOT / "include" / "draugr_b200.h"]
+
+
+def declared_functions():
+    names = set()
+    for h in HEADERS:
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        for m in re.finditer(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\(", text):
+            name = m.group(1)
+            if name.startswith(("draugr_", "init_julia", "shutdown_julia")):
+                names.add(name)
+    return names
+
+
+def test_library_exports_every_declared_symbol(lib):
+    names = declared_functions()
+    assert "draugr_amg_setup" in names and "draugr_b200_pcg" in names
+    for name in names:
+        assert hasattr(lib, name), name
+    # the ctypes signature table covers the same set
+    assert names == set(SIGNATURES)
+
+
+def test_config_defaults_and_errors(lib):
+    h = lib.draugr_amg_config_from_json(None)
+    assert h > 0
+    assert lib.draugr_amg_config_from_json(b"{}") > h
+    # string values are case-insensitive, numbers may be strings, unknown keys ignored
+    ok = lib.draugr_amg_config_from_json(
+        b'{"coarsening": "AGGREGATION", "theta": "0.25", "smoother": {"type": "Jacobi", '
+        b'"omega": "0.5"}, "cycle": "W", "max_levels": 10.0, "whatever": [1, 2]}')
+    assert ok > 0
+    bad = lib.draugr_amg_config_from_json(b'{"coarsening": "nope"}')
+    assert bad == -1
+    msg = draugr.last_error()
+    assert 'Unknown coarsening: "nope"' in msg and "aggregation" in msg
+    assert lib.draugr_amg_config_from_json(b'{"smoother": 3}') == -1
+    assert lib.draugr_amg_config_from_json(b'{"cycle": "x"}') == -1
+    assert lib.draugr_amg_config_from_json(b"{not json") == -1
+    assert lib.draugr_amg_config_free(ok) == 0
+    assert lib.draugr_amg_config_free(ok) == -1
+    assert "Invalid config handle" in draugr.last_error()
+
+
+def test_invalid_handles(lib):
+    x = np.zeros(4)
+    b = np.ones(4)
+    p = lambda a: a.ctypes.data_as(draugr._lib.C.c_void_p)
+    cfg = draugr.config_handle(None)
+    assert lib.draugr_amg_solve(9999, 4, p(x), p(b), cfg, 1e-8, 10) == -1
+    assert len(draugr.last_error()) > 0
+    assert lib.draugr_amg_cycle(9999, 4, p(x), p(b), cfg) == -1
+    assert lib.draugr_amg_free(9999) == -1
+    rp = np.array([0, 1], np.int32)
+    ci = np.array([0], np.int32)
+    v = np.array([1.0])
+    assert lib.draugr_amg_resetup(9999, 1, 1, p(rp), p(ci), p(v), cfg, 0, 1, 1) == -1
+
+
+def test_index_base_and_validation(lib):
+    A = problems.poisson1d(200)
+    n, rp, ci, v = oracle.csr_parts(A)
+    p = lambda a: a.ctypes.data_as(draugr._lib.C.c_void_p)
+    cfg = draugr.config_handle(draugr.AMGConfig(coarsening=draugr.AggregationCoarsening()))
+    h0 = lib.draugr_b200_setup_host(n, len(ci), p(rp), p(ci), p(v), cfg, 0, 1)
+    rp1, ci1 = rp + 1, ci + 1
+    h1 = lib.draugr_b200_setup_host(n, len(ci), p(rp1), p(ci1), p(v), cfg, 1, 1)
+    assert h0 > 0 and h1 > 0
+    H0, H1 = draugr.Hierarchy(h0, n, None), draugr.Hierarchy(h1, n, None)
+    for what in ("A_rowptr", "A_colval", "P_colval", "T_rows"):
+        assert np.array_equal(H0.export(0, what), H1.export(0, what))
+    assert lib.draugr_b200_setup_host(n, len(ci), p(rp), p(ci), p(v), cfg, 2, 1) == -1
+    assert "index_base must be 0 or 1" in draugr.last_error()
+    bad = ci.copy()
+    bad[3] = n + 5
+    assert lib.draugr_b200_setup_host(n, len(ci), p(rp), p(bad), p(v), cfg, 0, 1) == -1
+    assert "column index out of range" in draugr.last_error()
+    # unsupported smoother fails with a clear message
+    cfg2 = draugr.config_handle(draugr.AMGConfig(smoother=draugr.ILU0SmootherType()))
+    assert lib.draugr_b200_setup_host(n, len(ci), p(rp), p(ci), p(v), cfg2, 0, 1) == -1
+    assert "not supported" in draugr.last_error()
+
+
+from cases import CASES as CONFIGS  # noqa: E402
+
+
+@pytest.fixture(scope="module", params=sorted(CONFIGS))
+def host_case(request):
+    make, cfg = CONFIGS[request.param]
+    A = make()
+    h = draugr.amg_setup(A, cfg, on_device=False)
+    return request.param, A, cfg, h
+
+
+def test_structure_matches_oracle(host_case):
+    """Transpose maps, Galerkin sparsity (compute_coarse_sparsity), colours
+    and smoother diagonals equal the oracle's restatement exactly; setup
+    values of the coarse operators agree to 1e-12 (different summation
+    order than the reference's triple map)."""
+    name, A, cfg, h = host_case
+    nl = h.nlevels
+    assert nl >= 1
+    for l in range(nl):
+        info = h.level_info(l)
+        n, nc = int(info[0]), int(info[2])
+        arp, aci, av = h.export(l, "A_rowptr"), h.export(l, "A_colval"), h.export(l, "A_nzval")
+        prp, pci, pv = h.export(l, "P_rowptr"), h.export(l, "P_colval"), h.export(l, "P_nzval")
+        off, rows, pnz = oracle.transpose_map(n, nc, prp, pci)
+        assert np.array_equal(off, h.export(l, "T_offsets"))
+        assert np.array_equal(rows, h.export(l, "T_rows"))
+        assert np.array_equal(pnz, h.export(l, "T_pnz"))
+        c_rp, c_ci, c_v, *_ = oracle.coarse_sparsity(n, nc, arp, aci, av, prp, pci, pv)
+        if l + 1 < nl:
+            nrp, nci, nv = (h.export(l + 1, "A_rowptr"), h.export(l + 1, "A_colval"),
+                            h.export(l + 1, "A_nzval"))
+        else:
+            nrp, nci, nv = h.export(-1, "C_rowptr"), h.export(-1, "C_colval"), h.export(-1, "C_nzval")
+        assert np.array_equal(c_rp, nrp), f"level {l}: coarse rowptr differs"
+        assert np.array_equal(c_ci, nci), f"level {l}: coarse colval differs"
+        scale = np.abs(c_v).max()
+        assert np.abs(c_v - nv).max() <= 1e-12 * scale
+        kind = int(info[4])
+        inv = oracle.invdiag(n, arp, aci, av, l1=kind in (5, 6))
+        assert np.array_equal(inv, h.export(l, "invdiag"))
+        if kind in (1, 6):
+            colors, ncol, coff, order = oracle.greedy_coloring(n, arp, aci)
+            assert ncol == int(info[5])
+            assert np.array_equal(colors, h.export(l, "colors"))
+            assert np.array_equal(coff, h.export(l, "color_offsets"))
+            assert np.array_equal(order, h.export(l, "color_order"))
+            # no two neighbours share a colour (test/runtests.jl:549-566)
+            rr = np.repeat(np.arange(n), np.diff(arp))
+            off_diag = rr != aci
+            assert not np.any(colors[rr[off_diag]] == colors[aci[off_diag]])
+    # coarsest LU equals the oracle's getf2
+    nc = int(h.level_info(-1)[0])
+    lu, piv, info = oracle.lu_factor(h.export(-1, "C_dense").reshape(nc, nc).T)
+    assert info == 0
+    assert np.array_equal(piv, h.export(-1, "C_piv"))
+    assert np.array_equal(lu.T.reshape(-1), h.export(-1, "C_lu"))
+
+
+def test_prolongation_properties(host_case):
+    """Every fine row interpolates from at least one coarse point; C-point
+    rows are unit rows; P columns are in range and sorted per row."""
+    name, A, cfg, h = host_case
+    for l in range(h.nlevels):
+        info = h.level_info(l)
+        prp, pci = h.export(l, "P_rowptr"), h.export(l, "P_colval")
+        assert np.all(np.diff(prp) >= 1)
+        assert pci.min() >= 0 and pci.max() < info[2]
+        for i in range(0, int(info[0]), max(1, int(info[0]) // 200)):
+            row = pci[prp[i]:prp[i + 1]]
+            assert np.all(np.diff(row) > 0)
+
+
+def test_hierarchy_summary(host_case):
+    name, A, cfg, h = host_case
+    s = h.summary()
+    assert "AMG Hierarchy Summary" in s and "Operator complexity" in s
+
+
+def test_allow_partial_resetup_false_has_no_maps():
+    A = problems.poisson2d(16)
+    h = draugr.amg_setup(A, draugr.AMGConfig(coarsening=draugr.AggregationCoarsening()),
+                         allow_partial_resetup=False, on_device=False)
+    for l in range(h.nlevels):
+        assert h.level_info(l)[6] == -1
+
+
+def test_setup_seed_determinism():
+    A = problems.heterogeneous_diffusion_3d(10, seed=5)
+    cfg = draugr.hypre_default_config(agg_trunc_factor=0.2, seed=7)
+    h1 = draugr.amg_setup(A, cfg, on_device=False)
+    h2 = draugr.amg_setup(A, cfg, on_device=False)
+    for l in range(h1.nlevels):
+        assert np.array_equal(h1.export(l, "P_colval"), h2.export(l, "P_colval"))
+        assert np.array_equal(h1.export(l, "P_nzval"), h2.export(l, "P_nzval"))
+
+
+def test_check_raises():
+    with pytest.raises(draugr.DraugrError):
+        check(-1, "x")

@@ -1,0 +1,191 @@
+"""Parity of the CUDA solve / resetup path with the oracle (the CPU
+restatement of Draugr.jl's arithmetic), on the same hierarchy structure,
+through the library's C ABI.
+
+Tolerances (normwise relative): FP64 kernels and cycles 1e-12; the coarsest
+LU solve is bit-exact (same operation order, no contraction); FP32 kernels
+1e-5; Galerkin resetup values 1e-12 per level against the reference's
+triple-map product.
+"""
+
+import numpy as np
+import pytest
+
+import draugr
+import oracle
+from cases import CASES
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL32 = 1e-5
+
+
+def rel(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / (nb if nb > 0 else 1.0)
+
+
+@pytest.fixture(scope="module", params=sorted(CASES))
+def case(request):
+    make, cfg = CASES[request.param]
+    A = make()
+    h = draugr.amg_setup(A, cfg)
+    O = oracle.OracleHierarchy(h, with_rmaps=True)
+    return request.param, A, cfg, h, O
+
+
+def _level_arrays(O, l):
+    d = O.levels_np[l]
+    L = O._levels[l]
+    return d, L
+
+
+def test_level_kernels(case):
+    name, A, cfg, h, O = case
+    rng = np.random.default_rng(11)
+    for l in range(h.nlevels):
+        d, L = _level_arrays(O, l)
+        n, nc = L.n, L.nc
+        x = rng.uniform(-1, 1, n)
+        b = rng.uniform(-1, 1, n)
+        xc = rng.uniform(-1, 1, nc)
+        ref = oracle.spmv(n, d["A_rp"], d["A_ci"], d["A_v"], x)
+        assert rel(h.level_op(l, 0, x), ref) < TOL64
+        assert rel(h.level_op(l, 0, x, precision=1), ref) < TOL32
+        ref = oracle.residual(n, d["A_rp"], d["A_ci"], d["A_v"], x, b)
+        assert rel(h.level_op(l, 1, x, b), ref) < TOL64
+        ref = oracle.restrict(nc, d["T_off"], d["T_rows"], d["T_pnz"], d["P_v"], x)
+        assert rel(h.level_op(l, 3, x), ref) < TOL64
+        assert rel(h.level_op(l, 3, x, precision=1), ref) < TOL32
+        ref = oracle.prolongate(n, d["P_rp"], d["P_ci"], d["P_v"], xc, x)
+        assert rel(h.level_op(l, 4, x, xc), ref) < TOL64
+        for steps in (1, 2, 3):
+            if L.smoother in (0, 5):
+                ref = oracle.jacobi(n, d["A_rp"], d["A_ci"], d["A_v"], d["invd"], L.omega, x, b, steps)
+            else:
+                ref = oracle.gs(n, d["A_rp"], d["A_ci"], d["A_v"], d["invd"], L.ncolors,
+                                d["color_off"], d["color_order"], x, b, steps)
+            assert rel(h.level_op(l, 2, x, b, steps=steps), ref) < TOL64, (l, steps)
+            assert rel(h.level_op(l, 2, x, b, steps=steps, precision=1), ref) < TOL32
+        if L.smoother in (0, 5):
+            x1 = oracle.jacobi(n, d["A_rp"], d["A_ci"], d["A_v"], d["invd"], L.omega,
+                               np.zeros(n), b, 1)
+            r1 = oracle.residual(n, d["A_rp"], d["A_ci"], d["A_v"], x1, b)
+            out = h.level_op(l, 6, b)
+            assert rel(out[:n], x1) < TOL64
+            assert rel(out[n:], r1) < TOL64
+
+
+def test_coarse_solve_bit_exact(case):
+    name, A, cfg, h, O = case
+    rng = np.random.default_rng(5)
+    bc = rng.uniform(-1, 1, O.nc)
+    y = bc.copy()
+    oracle.load().orc_lu_solve(O.nc, oracle.ptr(O.lu), oracle.ptr(O.piv), oracle.ptr(y))
+    assert np.array_equal(h.level_op(0, 5, bc), y)
+
+
+@pytest.mark.parametrize("wcycle", [False, True])
+def test_cycle(case, wcycle):
+    name, A, cfg, h, O = case
+    n = A.shape[0]
+    rng = np.random.default_rng(3)
+    b = rng.uniform(-1, 1, n)
+    x0 = rng.uniform(-1, 1, n)
+    c2 = draugr.AMGConfig(**{**cfg.__dict__, "cycle_type": "W" if wcycle else "V"})
+    ref = O.cycle(x0, b, cfg.pre_smoothing_steps, cfg.post_smoothing_steps, wcycle)
+    x = x0.copy()
+    draugr.amg_cycle(x, b, h, c2)
+    assert rel(x, ref) < TOL64
+    # zero initial guess (the path that fuses the first Jacobi step)
+    ref0 = O.cycle(np.zeros(n), b, cfg.pre_smoothing_steps, cfg.post_smoothing_steps, wcycle)
+    x = np.zeros(n)
+    draugr.amg_cycle(x, b, h, c2)
+    assert rel(x, ref0) < TOL64
+
+
+def test_cycle_more_smoothing(case):
+    name, A, cfg, h, O = case
+    n = A.shape[0]
+    b = np.random.default_rng(8).uniform(-1, 1, n)
+    c2 = draugr.AMGConfig(**{**cfg.__dict__, "pre_smoothing_steps": 2, "post_smoothing_steps": 3})
+    ref = O.cycle(np.zeros(n), b, 2, 3, False)
+    x = np.zeros(n)
+    draugr.amg_cycle(x, b, h, c2)
+    assert rel(x, ref) < TOL64
+
+
+def test_stationary_solve(case):
+    name, A, cfg, h, O = case
+    n = A.shape[0]
+    b = np.random.default_rng(1).uniform(-1, 1, n)
+    xr, itr, relr = O.solve(np.zeros(n), b, cfg.pre_smoothing_steps, cfg.post_smoothing_steps,
+                            False, 1e-8, 300)
+    x = np.zeros(n)
+    x, it = draugr.amg_solve(x, b, h, cfg, tol=1e-8, maxiter=300)
+    assert it == itr
+    assert rel(x, xr) < 1e-9
+    if it < 300:
+        assert np.linalg.norm(b - A @ x) / np.linalg.norm(b) < 1e-8
+
+
+def test_pcg_fp64_and_mixed(case):
+    name, A, cfg, h, O = case
+    n = A.shape[0]
+    b = np.random.default_rng(2).uniform(-1, 1, n)
+    xr, itr, relr = O.pcg(np.zeros(n), b, cfg.pre_smoothing_steps, cfg.post_smoothing_steps,
+                          False, 1e-8, 500)
+    x, it, rr = draugr.pcg(np.zeros(n), b, h, cfg, tol=1e-8, maxiter=500, precision="fp64")
+    if "gs" not in name:   # colored GS cycles are not symmetric: CG is not guaranteed
+        assert abs(it - itr) <= 1
+        assert rel(x, xr) < 1e-7
+        assert np.linalg.norm(b - A @ x) / np.linalg.norm(b) < 1e-8
+        xm, itm, rm = draugr.pcg(np.zeros(n), b, h, cfg, tol=1e-8, maxiter=500, precision="mixed")
+        assert np.linalg.norm(b - A @ xm) / np.linalg.norm(b) < 1e-8  # FP64-verified
+        assert itm <= int(1.25 * it) + 2
+
+
+def test_resetup_matches_reference_galerkin(case):
+    name, A, cfg, h, O = case
+    n = A.shape[0]
+    rng = np.random.default_rng(4)
+    dscale = rng.uniform(0.5, 2.0, n)
+    A2 = A.multiply(dscale[:, None]).multiply(dscale[None, :]).tocsr()  # D A D, same pattern
+    A2.sort_indices()
+    assert np.array_equal(A2.indices, A.indices)
+    draugr.amg_resetup(h, A2, cfg, partial=True)
+    O.resetup(A2.data)
+    for l in range(h.nlevels):
+        dev = h.export(l, "A_nzval")
+        ref = O.level_values(l)
+        assert rel(dev, ref) < TOL64, f"level {l}"
+        assert rel(h.export(l, "invdiag"), O.levels_np[l]["invd"]) < TOL64
+    nc = O.nc
+    assert rel(h.export(-1, "C_dense"), O.dense) < TOL64
+    # the resetup hierarchy solves the new system
+    b = rng.uniform(-1, 1, n)
+    x, it = draugr.amg_solve(np.zeros(n), b, h, cfg, tol=1e-8, maxiter=400)
+    if it < 400:
+        assert np.linalg.norm(b - A2 @ x) / np.linalg.norm(b) < 1e-8
+    # and the cycle after resetup still matches the oracle's
+    xr = O.cycle(np.zeros(n), b, cfg.pre_smoothing_steps, cfg.post_smoothing_steps, False)
+    x = np.zeros(n)
+    draugr.amg_cycle(x, b, h, cfg)
+    assert rel(x, xr) < 1e-11
+    assert nc > 0
+
+
+def test_device_pointer_entry_points(case):
+    torch = pytest.importorskip("torch")
+    name, A, cfg, h, O = case
+    n = A.shape[0]
+    b = np.random.default_rng(6).uniform(-1, 1, n)
+    xh, ith = draugr.amg_solve(np.zeros(n), b, h, cfg, tol=1e-8, maxiter=200)
+    xd = torch.zeros(n, dtype=torch.float64, device="cuda")
+    bd = torch.tensor(b, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    xd, itd = draugr.amg_solve(xd, bd, h, cfg, tol=1e-8, maxiter=200)
+    torch.cuda.synchronize()
+    assert itd == ith
+    assert np.array_equal(xd.cpu().numpy(), xh)
