@@ -51,6 +51,14 @@ def parse():
     ap.add_argument("--n", type=int, default=128, help="grid side (128 = the quoted workload)")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel-only", action="store_true",
+                    help="only time one level kernel (for profiling): --level --op --precision --reps")
+    ap.add_argument("--level", type=int, default=0)
+    ap.add_argument("--op", type=int, default=2, help="2 = smoother sweep, 0 = SpMV")
+    ap.add_argument("--precision", type=int, default=0)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--profile-solve", choices=["fp64", "mixed"], default=None,
+                    help="run exactly one PCG solve in this precision (for profiling)")
     return ap.parse_args()
 
 
@@ -364,8 +372,42 @@ def run_reference(args, world, rank):
             "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def run_kernel_only(args):
+    import torch
+
+    import draugr
+
+    torch.cuda.set_device(0)
+    A, b, cfg = workload(args.n, args.seed)
+    h = draugr.amg_setup(A, cfg)
+    ms = h.time_level_op(args.level, args.op, args.precision, reps=args.reps)
+    info = h.level_info(args.level)
+    return {"kernel_only": True, "level": args.level, "op": args.op, "precision": args.precision,
+            "rows": int(info[0]), "nnz": int(info[1]), "ms_per_launch": ms}
+
+
+def run_profile_solve(args):
+    import torch
+
+    import draugr
+
+    torch.cuda.set_device(0)
+    A, b, cfg = workload(args.n, args.seed)
+    h = draugr.amg_setup(A, cfg)
+    x = np.zeros(A.shape[0])
+    _, it, rel = draugr.pcg(x, b, h, cfg, tol=TOL, maxiter=MAXITER, precision=args.profile_solve)
+    return {"profile_solve": args.profile_solve, "iterations": it, "relres": rel,
+            "relres_fp64_verified": float(np.linalg.norm(b - A @ x) / np.linalg.norm(b))}
+
+
 def main():
     args = parse()
+    if args.profile_solve:
+        print(json.dumps(run_profile_solve(args)), flush=True)
+        return
+    if args.kernel_only:
+        print(json.dumps(run_kernel_only(args)), flush=True)
+        return
     world, rank, local = dist_init(args)
     if args.impl == "reference":
         out = run_reference(args, world, rank)

@@ -46,6 +46,7 @@ void cuda_check(cudaError_t e, const char* what, const char* file, int line) {
 
 namespace {
 
+// Lanes per row for the Gauss-Seidel colour kernel: about the mean row length.
 int pick_G(long long nnz, int n) {
   if (n <= 0) return 1;
   double avg = (double)nnz / (double)n;
@@ -54,9 +55,33 @@ int pick_G(long long nnz, int n) {
   return G;
 }
 
+// Greedy packing of consecutive rows into tiles of at most kBlock/G rows and
+// kTileCap nonzeros; a row longer than kTileCap is a tile of its own.
+std::vector<int> make_tiles(const std::vector<int>& rp, int n, int G) {
+  std::vector<int> tp;
+  tp.reserve(n / std::max(1, kBlock / G) + 2);
+  tp.push_back(0);
+  const int max_rows = kBlock / G;
+  int r = 0;
+  while (r < n) {
+    int rows = 0, nz = 0;
+    while (r < n && rows < max_rows) {
+      const int len = rp[r + 1] - rp[r];
+      if (rows > 0 && nz + len > kTileCap) break;
+      nz += len;
+      ++rows;
+      ++r;
+      if (len > kTileCap) break;
+    }
+    tp.push_back(r);
+  }
+  return tp;
+}
+
 template <typename TA, class XL, class EP, bool DOT, class Fin>
-void launch_rows_impl(cudaStream_t st, int max_grid, int G, int n, const int* rp, const int* ci,
-                      const TA* av, XL xl, EP ep, double* partials, unsigned* ticket, Fin fin) {
+void launch_rows_impl(cudaStream_t st, int max_grid, int G, int n, int ntiles, const int* tp,
+                      const int* rp, const int* ci, const TA* av, XL xl, EP ep, double* partials,
+                      unsigned* ticket, Fin fin) {
   if (n <= 0) {
     if constexpr (DOT) {
       // an empty reduction still has to deliver its (zero) result
@@ -65,14 +90,13 @@ void launch_rows_impl(cudaStream_t st, int max_grid, int G, int n, const int* rp
     }
     return;
   }
-  const long long thr = (long long)n * G;
-  const int grid = (int)std::max<long long>(1, std::min<long long>((thr + kBlock - 1) / kBlock, max_grid));
+  const int grid = std::max(1, std::min(ntiles, max_grid));
   counted();
   switch (G) {
-#define DR_CASE(g)                                                                              \
-  case g:                                                                                       \
-    k_csr_rows<g, TA, XL, EP, DOT, Fin><<<grid, kBlock, 0, st>>>(n, rp, ci, av, xl, ep, partials, \
-                                                                 ticket, fin);                   \
+#define DR_CASE(g)                                                                                \
+  case g:                                                                                         \
+    k_tile_rows<g, TA, XL, EP, DOT, Fin><<<grid, kBlock, 0, st>>>(ntiles, tp, rp, ci, av, xl, ep,   \
+                                                                  partials, ticket, fin);          \
     break;
     DR_CASE(1) DR_CASE(2) DR_CASE(4) DR_CASE(8) DR_CASE(16) DR_CASE(32)
 #undef DR_CASE
@@ -83,15 +107,15 @@ void launch_rows_impl(cudaStream_t st, int max_grid, int G, int n, const int* rp
 
 template <typename TA, class XL, class EP>
 void launch_rows(cudaStream_t st, int max_grid, const DevMat& M, const TA* av, XL xl, EP ep) {
-  launch_rows_impl<TA, XL, EP, false, FinStore>(st, max_grid, M.G, M.n, M.rp, M.ci, av, xl, ep, nullptr,
-                                                nullptr, FinStore{nullptr});
+  launch_rows_impl<TA, XL, EP, false, FinStore>(st, max_grid, M.G, M.n, M.ntiles, M.tp, M.rp, M.ci, av,
+                                                xl, ep, nullptr, nullptr, FinStore{nullptr});
 }
 
 template <typename TA, class XL, class EP, class Fin>
 void launch_rows_dot(cudaStream_t st, int max_grid, const DevMat& M, const TA* av, XL xl, EP ep,
                      double* partials, unsigned* ticket, Fin fin) {
-  launch_rows_impl<TA, XL, EP, true, Fin>(st, max_grid, M.G, M.n, M.rp, M.ci, av, xl, ep, partials,
-                                          ticket, fin);
+  launch_rows_impl<TA, XL, EP, true, Fin>(st, max_grid, M.G, M.n, M.ntiles, M.tp, M.rp, M.ci, av, xl,
+                                          ep, partials, ticket, fin);
 }
 
 int grid1d(long long n, int max_grid) {
@@ -156,7 +180,12 @@ DevHier::DevHier(const HostHierarchy& H, int device) {
       h2d(M.ci, ci, st_);
       M.v = alloc<double>(ci.size());
       if (v) h2d(M.v, *v, st_);
-      M.G = pick_G(M.nnz, n);
+      M.G = tile_lanes(M.nnz, n);
+      M.Ggs = pick_G(M.nnz, n);
+      std::vector<int> tiles = make_tiles(rp, n, M.G);
+      M.ntiles = (int)tiles.size() - 1;
+      M.tp = alloc<int>(tiles.size());
+      DR_CK(cudaMemcpy(M.tp, tiles.data(), tiles.size() * sizeof(int), cudaMemcpyHostToDevice));
     };
     for (int l = 0; l < nl; ++l) {
       const HostLevel& h = H.levels[l];
@@ -175,10 +204,7 @@ DevHier::DevHier(const HostHierarchy& H, int device) {
         h2d(d.color_order, h.color_order, st_);
       }
       d.has_rap = h.has_rap_map;
-      if (d.has_rap) {
-        up_csr(d.AP, h.A.n, h.P.nc, h.ap_rp, h.ap_ci, nullptr);
-        d.AP.G = 8;
-      }
+      if (d.has_rap) up_csr(d.AP, h.A.n, h.P.nc, h.ap_rp, h.ap_ci, nullptr);
       const int n = h.A.n;
       if (l > 0) {
         d.v64.xa = alloc<double>(n);
@@ -316,9 +342,9 @@ T* DevHier::smooth(int l, T* x, const T* b, int steps, T* ext) {
         const int off = L.color_off[c];
         const int cnt = L.color_off[c + 1] - off;
         if (cnt == 0) continue;
-        const int grid = (int)std::max<long long>(1, std::min<long long>(((long long)cnt * A.G + kBlock - 1) / kBlock, max_grid_));
+        const int grid = (int)std::max<long long>(1, std::min<long long>(((long long)cnt * A.Ggs + kBlock - 1) / kBlock, max_grid_));
         counted();
-        switch (A.G) {
+        switch (A.Ggs) {
 #define DR_CASE(g)                                                                                  \
   case g:                                                                                           \
     k_gs_color<g, T><<<grid, kBlock, 0, st_>>>(cnt, L.color_order + off, A.rp, A.ci, mval<T>(A), b, \

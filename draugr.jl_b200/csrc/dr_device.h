@@ -11,6 +11,19 @@
 namespace dr {
 
 void cuda_check(cudaError_t e, const char* what, const char* file, int line);
+
+// Lanes per row in the row phase of the tile kernel.  Rows of up to 32
+// entries get one lane, which sums the staged products in column order (the
+// reference's order, so those rows are reproduced bit for bit); longer rows
+// get a power of two of lanes with about 8 products each.
+inline int tile_lanes(long long nnz, int n) {
+  if (n <= 0) return 1;
+  const double avg = (double)nnz / (double)n;
+  if (avg <= 32.0) return 1;
+  int G = 2;
+  while (G < 32 && G * 8 < avg) G *= 2;
+  return G;
+}
 long long kernel_launches();
 #define DR_CK(x) ::dr::cuda_check((x), #x, __FILE__, __LINE__)
 
@@ -24,7 +37,10 @@ struct DevMat {
   int* ci = nullptr;
   double* v = nullptr;
   float* v32 = nullptr;
-  int G = 8;
+  int G = 1;          // lanes per row in the row phase of k_tile_rows
+  int Ggs = 8;        // lanes per row of the Gauss-Seidel colour kernel
+  int ntiles = 0;     // row tiles (see k_tile_rows)
+  int* tp = nullptr;  // tile row starts, ntiles+1
 };
 
 template <typename T>

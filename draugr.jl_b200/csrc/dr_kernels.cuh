@@ -96,7 +96,7 @@ struct XZeroJacobi {
   const T* __restrict__ b;
   const T* __restrict__ invd;
   T omega;
-  __device__ __forceinline__ T operator()(int j) const { return (omega * __ldg(invd + j)) * __ldg(b + j); }
+  __device__ __forceinline__ T operator()(int j) const;
 };
 
 // PCG search direction on the fly: p_j = z_j + β·p_old_j.
@@ -114,73 +114,105 @@ struct XPcgDir {
   }
 };
 
-// ------------------------------------------------------------ epilogues
+// ------------------------------------------------------------ rounding
+// Products and sums rounded separately (no contraction into FMA), as the
+// reference's Julia loops evaluate them.
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+
 template <typename T>
-struct EpStore {  // y = A x
+__device__ __forceinline__ T XZeroJacobi<T>::operator()(int j) const {
+  return mul_rn(mul_rn(omega, __ldg(invd + j)), __ldg(b + j));
+}
+
+// ------------------------------------------------------------ epilogues
+// A row of a row kernel is reduced as  acc = init(i) ± a_i1 x_1 ± a_i2 x_2 ...
+// (kSign = +1 adds the products, -1 subtracts them) and then apply(i, acc)
+// writes the row's results and returns its contribution to a fused dot
+// product.  With one lane per row the products are accumulated in column
+// order, exactly as the reference's loops do; with G > 1 lanes the products
+// are summed in a fixed tree first and then added to (subtracted from) init.
+template <typename T>
+struct EpStore {  // y = A x                                (csr_matrix.jl:150-159)
   using acc_t = T;
+  static constexpr int kSign = 1;
   T* __restrict__ y;
-  __device__ __forceinline__ double operator()(int i, T s) const { y[i] = s; return 0.0; }
+  __device__ __forceinline__ T init(int) const { return T(0); }
+  __device__ __forceinline__ double apply(int i, T v) const { y[i] = v; return 0.0; }
 };
 
 template <typename T>
-struct EpResidual {  // r = b - A x            (src/cycle.jl:32-43)
+struct EpResidual {  // Ax = Σ a x ; r = b - Ax                (cycle.jl:32-43)
   using acc_t = T;
+  static constexpr int kSign = 1;
   const T* __restrict__ b;
   T* __restrict__ r;
-  __device__ __forceinline__ double operator()(int i, T s) const {
-    T ri = __ldg(b + i) - s;
+  __device__ __forceinline__ T init(int) const { return T(0); }
+  __device__ __forceinline__ double apply(int i, T v) const {
+    T ri = sub_rn(__ldg(b + i), v);
     r[i] = ri;
     return (double)ri * (double)ri;
   }
 };
 
 template <typename T>
-struct EpJacobi {  // xn = x + ω·invd·(b - A x)  (src/smoothers.jl:78-94)
+struct EpJacobi {  // r = b - a x - ... ; xn = x + (ω·invd)·r   (smoothers.jl:78-94)
   using acc_t = T;
+  static constexpr int kSign = -1;
   const T* __restrict__ x;
   const T* __restrict__ b;
   const T* __restrict__ invd;
   T* __restrict__ xn;
   T omega;
   const double* __restrict__ w;  // optional: returns w_i·xn_i for a fused dot
-  __device__ __forceinline__ double operator()(int i, T s) const {
-    T ri = __ldg(b + i) - s;
-    T v = __ldg(x + i) + (omega * __ldg(invd + i)) * ri;
+  __device__ __forceinline__ T init(int i) const { return __ldg(b + i); }
+  __device__ __forceinline__ double apply(int i, T r) const {
+    T v = add_rn(__ldg(x + i), mul_rn(mul_rn(omega, __ldg(invd + i)), r));
     xn[i] = v;
     return w ? __ldg(w + i) * (double)v : 0.0;
   }
 };
 
 template <typename T>
-struct EpZeroJacobiResidual {  // x1 = ω·invd·b ; r = b - A x1
+struct EpZeroJacobiResidual {  // x1 = (ω·invd)·b ; r = b - A x1
   using acc_t = T;
+  static constexpr int kSign = 1;
   const T* __restrict__ b;
   const T* __restrict__ invd;
   T* __restrict__ x1;
   T* __restrict__ r;
   T omega;
-  __device__ __forceinline__ double operator()(int i, T s) const {
+  __device__ __forceinline__ T init(int) const { return T(0); }
+  __device__ __forceinline__ double apply(int i, T v) const {
     T bi = __ldg(b + i);
-    x1[i] = (omega * __ldg(invd + i)) * bi;
-    r[i] = bi - s;
+    x1[i] = mul_rn(mul_rn(omega, __ldg(invd + i)), bi);
+    r[i] = sub_rn(bi, v);
     return 0.0;
   }
 };
 
 template <typename T>
-struct EpAddTo {  // x += P xc               (src/prolongation.jl:742-760)
+struct EpAddTo {  // x += p xc, per entry                  (prolongation.jl:742-760)
   using acc_t = T;
+  static constexpr int kSign = 1;
   T* __restrict__ x;
-  __device__ __forceinline__ double operator()(int i, T s) const { x[i] += s; return 0.0; }
+  __device__ __forceinline__ T init(int i) const { return x[i]; }
+  __device__ __forceinline__ double apply(int i, T v) const { x[i] = v; return 0.0; }
 };
 
 template <typename T>
 struct EpPcgDir {  // q = A p, p_new = z + β p_old, returns p_new·q
   using acc_t = double;
+  static constexpr int kSign = 1;
   XPcgDir<T> dir;
   double* __restrict__ pnew;
   double* __restrict__ q;
-  __device__ __forceinline__ double operator()(int i, double s) const {
+  __device__ __forceinline__ double init(int) const { return 0.0; }
+  __device__ __forceinline__ double apply(int i, double s) const {
     double pi = dir(i);
     pnew[i] = pi;
     q[i] = s;
@@ -189,30 +221,88 @@ struct EpPcgDir {  // q = A p, p_new = z + β p_old, returns p_new·q
 };
 
 // ------------------------------------------------------------ row kernel
+// Rows are packed (on the host, once per matrix) into tiles of at most
+// kBlock/G consecutive rows holding at most kTileCap nonzeros.  A block
+// streams a tile's column and value arrays with consecutive threads on
+// consecutive entries (fully coalesced, many independent loads in flight),
+// stages the products a_ij·x_j in shared memory, then reduces the rows with
+// G lanes each and applies the fused epilogue.  A row longer than kTileCap
+// forms a tile of its own and is reduced by the whole block.
+constexpr int kTileCap = 2048;
+
 template <int G, typename TA, class XL, class EP, bool DOT, class Fin>
 __global__ void __launch_bounds__(kBlock)
-k_csr_rows(int n, const int* __restrict__ rp, const int* __restrict__ ci, const TA* __restrict__ av,
-           XL xl, EP ep, double* partials, unsigned* ticket, Fin fin) {
+k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ rp,
+            const int* __restrict__ ci, const TA* __restrict__ av, XL xl, EP ep, double* partials,
+            unsigned* ticket, Fin fin) {
   using acc_t = typename EP::acc_t;
-  constexpr int RPW = 32 / G;
+  __shared__ acc_t prod[kTileCap];
   const int lane = threadIdx.x & (G - 1);
-  const int g = (threadIdx.x & 31) / G;
-  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  const int grp = threadIdx.x / G;
   double dacc = 0.0;
-  for (long long base = warp * RPW; base < n; base += nwarps * RPW) {
-    const int row = (int)(base + g);
-    const bool valid = row < n;
-    int s = 0, e = 0;
-    if (valid) {
-      s = __ldg(rp + row);
-      e = __ldg(rp + row + 1);
-    }
-    acc_t sum = acc_t(0);
-    for (int k = s + lane; k < e; k += G) sum += (acc_t)__ldg(av + k) * (acc_t)xl(__ldg(ci + k));
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int r0 = __ldg(tp + t), r1 = __ldg(tp + t + 1);
+    const int s = __ldg(rp + r0), e = __ldg(rp + r1);
+    const int len = e - s;
+    if (len <= kTileCap) {
+      const int* cp = ci + s;
+      const TA* vp = av + s;
+#pragma unroll 4
+      for (int k = threadIdx.x; k < len; k += kBlock)
+        prod[k] = mul_rn((acc_t)__ldg(vp + k), (acc_t)xl(__ldg(cp + k)));
+      __syncthreads();
+      const int row = r0 + grp;
+      const bool valid = row < r1;
+      if constexpr (G == 1) {
+        if (valid) {
+          const int rs = __ldg(rp + row) - s, re = __ldg(rp + row + 1) - s;
+          acc_t a = ep.init(row);
+          for (int k = rs; k < re; ++k) {
+            if constexpr (EP::kSign > 0) a = add_rn(a, prod[k]);
+            else a = sub_rn(a, prod[k]);
+          }
+          dacc += ep.apply(row, a);
+        }
+      } else {
+        int rs = 0, re = 0;
+        if (valid) {
+          rs = __ldg(rp + row) - s;
+          re = __ldg(rp + row + 1) - s;
+        }
+        acc_t sum = acc_t(0);
+        for (int k = rs + lane; k < re; k += G) sum = add_rn(sum, prod[k]);
 #pragma unroll
-    for (int off = G >> 1; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
-    if (valid && lane == 0) dacc += ep(row, sum);
+        for (int off = G >> 1; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+        if (valid && lane == 0) {
+          acc_t a = ep.init(row);
+          if constexpr (EP::kSign > 0) a = add_rn(a, sum);
+          else a = sub_rn(a, sum);
+          dacc += ep.apply(row, a);
+        }
+      }
+      __syncthreads();
+    } else {
+      // a single row longer than the tile capacity
+      acc_t sum = acc_t(0);
+      for (int k = s + threadIdx.x; k < e; k += kBlock)
+        sum = add_rn(sum, mul_rn((acc_t)__ldg(av + k), (acc_t)xl(__ldg(ci + k))));
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+      if ((threadIdx.x & 31) == 0) prod[threadIdx.x >> 5] = sum;
+      __syncthreads();
+      if (threadIdx.x < 32) {
+        sum = threadIdx.x < (kBlock >> 5) ? prod[threadIdx.x] : acc_t(0);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+        if (threadIdx.x == 0) {
+          acc_t a = ep.init(r0);
+          if constexpr (EP::kSign > 0) a = add_rn(a, sum);
+          else a = sub_rn(a, sum);
+          dacc += ep.apply(r0, a);
+        }
+      }
+      __syncthreads();
+    }
   }
   if constexpr (DOT) grid_sum_finalize(dacc, partials, ticket, fin);
 }

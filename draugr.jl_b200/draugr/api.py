@@ -271,7 +271,7 @@ class Hierarchy:
         return _lib.check(_lib.load().draugr_b200_num_levels(self.handle), "num_levels")
 
     def level_info(self, lvl: int) -> np.ndarray:
-        info = np.zeros(8, dtype=np.int64)
+        info = np.zeros(10, dtype=np.int64)
         _lib.check(_lib.load().draugr_b200_level_info(self.handle, lvl, _ptr(info)), "level_info")
         return info
 

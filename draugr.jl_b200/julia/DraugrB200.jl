@@ -1,0 +1,292 @@
+"""
+    DraugrB200
+
+Julia front end of libdraugr_b200.so, keeping the names and argument meanings
+of Draugr.jl's AMG API (src/setup.jl, src/cycle.jl, src/resetup.jl,
+src/types.jl): `amg_setup`, `amg_solve!`, `amg_cycle!`, `amg_resetup!`,
+`AMGConfig`, `hypre_default_config`, plus `amg_pcg!` and an `ldiv!`
+preconditioner.  Every call is a `ccall` into the C ABI declared in
+include/draugr_amg.h and include/draugr_b200.h; setup builds the hierarchy
+structure on the CPU inside the library and the solve phase runs on the
+current CUDA device.  Vectors may be `Vector{Float64}` (copied to and from
+the device by the library) or any array whose `pointer` is a CUDA device
+pointer (`CuArray{Float64}` from CUDA.jl), which is passed straight through.
+"""
+module DraugrB200
+
+using LinearAlgebra
+using SparseArrays
+
+export AMGConfig, hypre_default_config, AMGHierarchy
+export amg_setup, amg_solve!, amg_cycle!, amg_resetup!, amg_pcg!
+export DraugrB200Preconditioner
+
+const libdraugr = get(ENV, "DRAUGR_B200_LIB", joinpath(@__DIR__, "..", "libdraugr_b200.so"))
+
+struct DraugrError <: Exception
+    msg::String
+end
+Base.showerror(io::IO, e::DraugrError) = print(io, "DraugrB200: ", e.msg)
+
+last_error() = unsafe_string(ccall((:draugr_amg_last_error, libdraugr), Cstring, ()))
+check(rc::Integer, what) = rc < 0 ? throw(DraugrError(string(what, ": ", last_error()))) : rc
+
+# ---------------------------------------------------------------- configuration
+# Type tags mirror src/types.jl; they are turned into the JSON accepted by
+# draugr_amg_config_from_json (same keys as src/cfunction_interface.jl).
+abstract type InterpolationType end
+struct DirectInterpolation <: InterpolationType
+    trunc_factor::Float64
+end
+DirectInterpolation() = DirectInterpolation(0.0)
+struct StandardInterpolation <: InterpolationType
+    trunc_factor::Float64
+end
+StandardInterpolation() = StandardInterpolation(0.0)
+struct ExtendedIInterpolation <: InterpolationType
+    trunc_factor::Float64
+    max_elements::Int
+    norm_p::Int
+    rescale::Bool
+end
+ExtendedIInterpolation() = ExtendedIInterpolation(0.0, 0, 1, false)
+ExtendedIInterpolation(tf::Real) = ExtendedIInterpolation(Float64(tf), 0, 1, false)
+
+abstract type CoarseningAlgorithm end
+struct AggregationCoarsening <: CoarseningAlgorithm
+    θ::Float64
+    filtering::Bool
+    filter_tol::Float64
+end
+AggregationCoarsening(θ::Real=0.25) = AggregationCoarsening(θ, false, 0.1)
+struct PMISCoarsening <: CoarseningAlgorithm
+    θ::Float64
+    interpolation::InterpolationType
+end
+PMISCoarsening(θ::Real=0.25) = PMISCoarsening(θ, DirectInterpolation())
+struct HMISCoarsening <: CoarseningAlgorithm
+    θ::Float64
+    interpolation::InterpolationType
+end
+HMISCoarsening(θ::Real=0.25) = HMISCoarsening(θ, DirectInterpolation())
+struct AggressiveCoarsening <: CoarseningAlgorithm
+    θ::Float64
+    base::Symbol
+    interpolation::InterpolationType
+end
+AggressiveCoarsening(θ::Real=0.25, base::Symbol=:pmis) = AggressiveCoarsening(θ, base, ExtendedIInterpolation())
+struct SmoothedAggregationCoarsening <: CoarseningAlgorithm
+    θ::Float64
+    ω::Float64
+end
+SmoothedAggregationCoarsening(θ::Real=0.25) = SmoothedAggregationCoarsening(θ, 2 / 3)
+
+abstract type SmootherType end
+for (T, name) in ((:JacobiSmootherType, "jacobi"), (:L1JacobiSmootherType, "l1_jacobi"),
+                  (:ColoredGaussSeidelType, "colored_gs"), (:L1ColoredGaussSeidelType, "l1_colored_gs"),
+                  (:SerialGaussSeidelType, "serial_gs"), (:L1SerialGaussSeidelType, "l1_serial_gs"),
+                  (:SPAI0SmootherType, "spai0"), (:SPAI1SmootherType, "spai1"),
+                  (:ChebyshevSmootherType, "chebyshev"), (:ILU0SmootherType, "ilu0"),
+                  (:SerialILU0SmootherType, "serial_ilu0"))
+    @eval begin
+        struct $T <: SmootherType end
+        smoother_name(::$T) = $name
+        export $T
+    end
+end
+export AggregationCoarsening, PMISCoarsening, HMISCoarsening, AggressiveCoarsening,
+       SmoothedAggregationCoarsening, DirectInterpolation, StandardInterpolation,
+       ExtendedIInterpolation
+
+jstr(x::AbstractString) = "\"" * replace(x, "\"" => "\\\"") * "\""
+jstr(x::Bool) = x ? "true" : "false"
+jstr(x::Real) = string(x)
+
+interp_json(i::DirectInterpolation) = "{\"type\":\"direct\",\"trunc_factor\":$(i.trunc_factor)}"
+interp_json(i::StandardInterpolation) = "{\"type\":\"standard\",\"trunc_factor\":$(i.trunc_factor)}"
+interp_json(i::ExtendedIInterpolation) =
+    "{\"type\":\"extended_i\",\"trunc_factor\":$(i.trunc_factor),\"max_elements\":$(i.max_elements)," *
+    "\"norm_p\":$(i.norm_p),\"rescale\":$(jstr(i.rescale))}"
+
+coarsening_json(c::AggregationCoarsening) = ("aggregation", c.θ, nothing,
+    ",\"aggregation_filtering\":$(jstr(c.filtering)),\"filter_tol\":$(c.filter_tol)")
+coarsening_json(c::SmoothedAggregationCoarsening) = ("smoothed_aggregation", c.θ, nothing, ",\"sa_omega\":$(c.ω)")
+coarsening_json(c::PMISCoarsening) = ("pmis", c.θ, c.interpolation, "")
+coarsening_json(c::HMISCoarsening) = ("hmis", c.θ, c.interpolation, "")
+coarsening_json(c::AggressiveCoarsening) = ("aggressive_" * String(c.base), c.θ, c.interpolation, "")
+
+"""
+    AMGConfig(; kwargs...)
+
+Same keywords and defaults as Draugr.jl's `AMGConfig` (src/types.jl:514-536),
+plus `seed` for the random PMIS/HMIS measures.
+"""
+struct AMGConfig
+    json::String
+    handle::Int32
+    pre_smoothing_steps::Int
+    post_smoothing_steps::Int
+end
+
+function AMGConfig(; coarsening::CoarseningAlgorithm=HMISCoarsening(0.5, ExtendedIInterpolation()),
+                   smoother::SmootherType=L1ColoredGaussSeidelType(), max_levels::Int=20,
+                   max_coarse_size::Int=50, pre_smoothing_steps::Int=1, post_smoothing_steps::Int=1,
+                   jacobi_omega::Float64=2.0 / 3.0, verbose::Union{Bool,Int}=0,
+                   initial_coarsening::CoarseningAlgorithm=coarsening,
+                   initial_coarsening_levels::Int=0, max_row_sum::Float64=1.0,
+                   cycle_type::Symbol=:V, coarse_solve_on_cpu::Bool=false,
+                   seed::Union{Nothing,Integer}=nothing)
+    @assert cycle_type in (:V, :W) "cycle_type must be :V or :W"
+    name, θ, ip, extra = coarsening_json(coarsening)
+    iname, iθ, iip, _ = coarsening_json(initial_coarsening)
+    js = "{\"coarsening\":$(jstr(name)),\"theta\":$(θ)" *
+         (ip === nothing ? "" : ",\"interpolation\":" * interp_json(ip)) * extra *
+         ",\"initial_coarsening\":$(jstr(iname)),\"initial_theta\":$(iθ)" *
+         (iip === nothing ? "" : ",\"initial_interpolation\":" * interp_json(iip)) *
+         ",\"smoother\":{\"type\":$(jstr(smoother_name(smoother))),\"omega\":$(jacobi_omega)}" *
+         ",\"max_levels\":$(max_levels),\"max_coarse_size\":$(max_coarse_size)" *
+         ",\"pre_smoothing_steps\":$(pre_smoothing_steps),\"post_smoothing_steps\":$(post_smoothing_steps)" *
+         ",\"verbose\":$(Int(verbose)),\"initial_coarsening_levels\":$(initial_coarsening_levels)" *
+         ",\"max_row_sum\":$(max_row_sum),\"cycle\":$(jstr(lowercase(String(cycle_type))))" *
+         ",\"coarse_solve_on_cpu\":$(jstr(coarse_solve_on_cpu))" *
+         (seed === nothing ? "" : ",\"seed\":$(seed)") * "}"
+    h = check(ccall((:draugr_amg_config_from_json, libdraugr), Int32, (Cstring,), js),
+              "draugr_amg_config_from_json")
+    return AMGConfig(js, h, pre_smoothing_steps, post_smoothing_steps)
+end
+
+"""hypre_default_config (src/types.jl:569-584)."""
+function hypre_default_config(; θ::Float64=0.5, agg_num_levels::Int=1,
+                              agg_trunc_factor::Float64=0.3, kwargs...)
+    interp = ExtendedIInterpolation(agg_trunc_factor)
+    return AMGConfig(; coarsening=HMISCoarsening(θ, interp),
+                     initial_coarsening=AggressiveCoarsening(θ, :hmis, interp),
+                     initial_coarsening_levels=agg_num_levels, kwargs...)
+end
+
+# ---------------------------------------------------------------- hierarchy
+mutable struct AMGHierarchy
+    handle::Int32
+    n::Int
+    function AMGHierarchy(h::Int32, n::Int)
+        H = new(h, n)
+        finalizer(H) do H
+            H.handle > 0 && ccall((:draugr_amg_free, libdraugr), Int32, (Int32,), H.handle)
+            H.handle = -1
+        end
+        return H
+    end
+end
+
+# CSR arrays (1-based Int32) of a SparseMatrixCSC, as csr_from_csc does.
+function csr_arrays(A::SparseMatrixCSC)
+    At = sparse(transpose(A))
+    return Int32.(At.colptr), Int32.(At.rowval), Vector{Float64}(At.nzval)
+end
+
+"""
+    amg_setup(A, config=AMGConfig(); allow_partial_resetup=true) -> AMGHierarchy
+"""
+function amg_setup(A::SparseMatrixCSC, config::AMGConfig=AMGConfig();
+                   allow_partial_resetup::Bool=true)
+    n = size(A, 1)
+    rp, cv, nz = csr_arrays(A)
+    h = check(ccall((:draugr_amg_setup, libdraugr), Int32,
+                    (Int32, Int32, Ptr{Int32}, Ptr{Int32}, Ptr{Float64}, Int32, Int32, Int32),
+                    n, length(nz), rp, cv, nz, config.handle, 1, allow_partial_resetup),
+              "amg_setup")
+    return AMGHierarchy(h, n)
+end
+
+"""
+    amg_resetup!(h, A, config; partial=true, allow_partial_resetup=true) -> h
+"""
+function amg_resetup!(h::AMGHierarchy, A::SparseMatrixCSC, config::AMGConfig=AMGConfig();
+                      partial::Bool=true, allow_partial_resetup::Bool=true)
+    rp, cv, nz = csr_arrays(A)
+    check(ccall((:draugr_amg_resetup, libdraugr), Int32,
+                (Int32, Int32, Int32, Ptr{Int32}, Ptr{Int32}, Ptr{Float64}, Int32, Int32, Int32, Int32),
+                h.handle, size(A, 1), length(nz), rp, cv, nz, config.handle, 1, partial,
+                allow_partial_resetup), "amg_resetup!")
+    return h
+end
+
+# Host vectors go through the host-pointer entry points; anything else is
+# taken to be device memory (e.g. CuArray) and its pointer passed as is.
+isdevice(x) = !(x isa Array)
+rawptr(x) = reinterpret(Ptr{Float64}, UInt(pointer(x)))
+
+"""
+    amg_cycle!(x, b, h, config) -> x
+"""
+function amg_cycle!(x::AbstractVector{Float64}, b::AbstractVector{Float64}, h::AMGHierarchy,
+                    config::AMGConfig=AMGConfig())
+    if isdevice(x)
+        check(ccall((:draugr_b200_cycle_device, libdraugr), Int32,
+                    (Int32, Int32, Ptr{Float64}, Ptr{Float64}, Int32),
+                    h.handle, length(x), rawptr(x), rawptr(b), config.handle), "amg_cycle!")
+    else
+        check(ccall((:draugr_amg_cycle, libdraugr), Int32,
+                    (Int32, Int32, Ptr{Float64}, Ptr{Float64}, Int32),
+                    h.handle, length(x), x, b, config.handle), "amg_cycle!")
+    end
+    return x
+end
+
+"""
+    amg_solve!(x, b, h, config; tol=1e-10, maxiter=100) -> (x, niter)
+"""
+function amg_solve!(x::AbstractVector{Float64}, b::AbstractVector{Float64}, h::AMGHierarchy,
+                    config::AMGConfig=AMGConfig(); tol::Real=1e-10, maxiter::Int=100)
+    it = if isdevice(x)
+        ccall((:draugr_b200_solve_device, libdraugr), Int32,
+              (Int32, Int32, Ptr{Float64}, Ptr{Float64}, Int32, Float64, Int32),
+              h.handle, length(x), rawptr(x), rawptr(b), config.handle, tol, maxiter)
+    else
+        ccall((:draugr_amg_solve, libdraugr), Int32,
+              (Int32, Int32, Ptr{Float64}, Ptr{Float64}, Int32, Float64, Int32),
+              h.handle, length(x), x, b, config.handle, tol, maxiter)
+    end
+    return x, Int(check(it, "amg_solve!"))
+end
+
+"""
+    amg_pcg!(x, b, h, config; tol=1e-8, maxiter=500, precision=:fp64) -> (x, niter, relres)
+
+Conjugate gradients preconditioned by one AMG cycle per iteration;
+`precision=:mixed` runs the cycle on FP32 copies of the hierarchy with the
+outer iteration in FP64.
+"""
+function amg_pcg!(x::AbstractVector{Float64}, b::AbstractVector{Float64}, h::AMGHierarchy,
+                  config::AMGConfig=AMGConfig(); tol::Real=1e-8, maxiter::Int=500,
+                  precision::Symbol=:fp64)
+    prec = precision === :mixed ? Int32(1) : Int32(0)
+    rel = Ref{Float64}(0.0)
+    fn = isdevice(x) ? :draugr_b200_pcg_device : :draugr_b200_pcg
+    px, pb = isdevice(x) ? (rawptr(x), rawptr(b)) : (pointer(x), pointer(b))
+    it = GC.@preserve x b ccall((fn, libdraugr), Int32,
+                                (Int32, Int32, Ptr{Float64}, Ptr{Float64}, Int32, Float64, Int32,
+                                 Int32, Ref{Float64}),
+                                h.handle, length(x), px, pb, config.handle, tol, maxiter, prec, rel)
+    return x, Int(check(it, "amg_pcg!")), rel[]
+end
+
+"""
+    DraugrB200Preconditioner(h, config)
+
+`ldiv!(x, P, b)` zeroes x and applies one cycle, like Draugr.jl's
+`preconditioner_apply!` (src/preconditioner.jl:76-80), for Krylov.jl or
+LinearSolve.jl.
+"""
+struct DraugrB200Preconditioner
+    h::AMGHierarchy
+    config::AMGConfig
+end
+
+function LinearAlgebra.ldiv!(x::AbstractVector{Float64}, P::DraugrB200Preconditioner,
+                             b::AbstractVector{Float64})
+    fill!(x, 0.0)
+    return amg_cycle!(x, b, P.h, P.config)
+end
+
+end # module

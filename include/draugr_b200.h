@@ -27,7 +27,9 @@ int32_t draugr_b200_setup_host(int32_t n, int32_t nnz, const int32_t *rowptr,
 int32_t draugr_b200_num_levels(int32_t handle);
 
 /* Sizes of level lvl (0-based): info[0] n, [1] nnz(A), [2] n_coarse,
- * [3] nnz(P), [4] smoother kind, [5] colours, [6] nnz(A*P) or -1.
+ * [3] nnz(P), [4] smoother kind, [5] colours, [6] nnz(A*P) or -1,
+ * [7] [8] [9] lanes per row of the row kernels for A, P and Pᵀ (1 = rows
+ * reduced sequentially in column order).  info must hold 10 values.
  * lvl = -1: the coarsest level, info[0] n_c, [1] nnz of its CSR. */
 int32_t draugr_b200_level_info(int32_t handle, int32_t lvl, int64_t *info);
 

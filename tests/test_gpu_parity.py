@@ -189,3 +189,72 @@ def test_device_pointer_entry_points(case):
     torch.cuda.synchronize()
     assert itd == ith
     assert np.array_equal(xd.cpu().numpy(), xh)
+
+
+@pytest.fixture(scope="module", params=sorted(CASES))
+def fresh_case(request):
+    """A hierarchy straight from setup (the resetup test above changes the
+    values of `case`; a GPU resetup's coarse values differ from the
+    reference's triple-map values in the last bits)."""
+    make, cfg = CASES[request.param]
+    A = make()
+    h = draugr.amg_setup(A, cfg)
+    return request.param, A, cfg, h, oracle.OracleHierarchy(h)
+
+
+def _single_lane(h, l):
+    info = h.level_info(l)
+    return int(info[7]) == 1, int(info[8]) == 1, int(info[9]) == 1
+
+
+def test_single_lane_rows_are_bit_exact(fresh_case):
+    """Rows reduced by one lane sum their products in column order, as the
+    reference does, so those kernels reproduce the oracle bit for bit."""
+    name, A, cfg, h, O = fresh_case
+    rng = np.random.default_rng(21)
+    checked = 0
+    for l in range(h.nlevels):
+        d, L = _level_arrays(O, l)
+        n, nc = L.n, L.nc
+        a1, p1, r1 = _single_lane(h, l)
+        x = rng.uniform(-1, 1, n)
+        b = rng.uniform(-1, 1, n)
+        xc = rng.uniform(-1, 1, nc)
+        if a1:
+            assert np.array_equal(h.level_op(l, 0, x), oracle.spmv(n, d["A_rp"], d["A_ci"], d["A_v"], x))
+            assert np.array_equal(h.level_op(l, 1, x, b),
+                                  oracle.residual(n, d["A_rp"], d["A_ci"], d["A_v"], x, b))
+            if L.smoother in (0, 5):
+                for steps in (1, 2):
+                    ref = oracle.jacobi(n, d["A_rp"], d["A_ci"], d["A_v"], d["invd"], L.omega, x, b, steps)
+                    assert np.array_equal(h.level_op(l, 2, x, b, steps=steps), ref)
+                x1 = oracle.jacobi(n, d["A_rp"], d["A_ci"], d["A_v"], d["invd"], L.omega,
+                                   np.zeros(n), b, 1)
+                r1v = oracle.residual(n, d["A_rp"], d["A_ci"], d["A_v"], x1, b)
+                out = h.level_op(l, 6, b)
+                assert np.array_equal(out[:n], x1) and np.array_equal(out[n:], r1v)
+            checked += 1
+        if r1:
+            ref = oracle.restrict(nc, d["T_off"], d["T_rows"], d["T_pnz"], d["P_v"], x)
+            assert np.array_equal(h.level_op(l, 3, x), ref)
+        if p1:
+            ref = oracle.prolongate(n, d["P_rp"], d["P_ci"], d["P_v"], xc, x)
+            assert np.array_equal(h.level_op(l, 4, x, xc), ref)
+    assert checked >= 1
+
+
+def test_cycle_bit_exact_when_all_rows_single_lane(fresh_case):
+    name, A, cfg, h, O = fresh_case
+    jac = all(int(h.level_info(l)[4]) in (0, 5) for l in range(h.nlevels))
+    single = all(all(_single_lane(h, l)) for l in range(h.nlevels))
+    if not (jac and single):
+        pytest.skip("hierarchy has multi-lane rows or Gauss-Seidel levels")
+    n = A.shape[0]
+    b = np.random.default_rng(9).uniform(-1, 1, n)
+    x0 = np.random.default_rng(10).uniform(-1, 1, n)
+    for w in (False, True):
+        c2 = draugr.AMGConfig(**{**cfg.__dict__, "cycle_type": "W" if w else "V"})
+        for start in (x0, np.zeros(n)):
+            x = start.copy()
+            draugr.amg_cycle(x, b, h, c2)
+            assert np.array_equal(x, O.cycle(start, b, 1, 1, w))

@@ -1,0 +1,192 @@
+"""Pins of the oracle (the CPU restatement of Draugr.jl's arithmetic) to the
+reference's own test assertions (test/runtests.jl), since the reference is
+Julia and cannot run here and ships no golden vectors.  Each test names the
+testset it restates.  Hierarchy structures come from the library's CPU setup
+(host-only, no GPU), as they do for the parity tests."""
+
+import numpy as np
+import scipy.sparse as sp
+
+import draugr
+import oracle
+from draugr import problems
+
+
+def parts(A):
+    return oracle.csr_parts(A)
+
+
+def explicit_P(h, l):
+    info = h.level_info(l)
+    return sp.csr_matrix((h.export(l, "P_nzval"), h.export(l, "P_colval"), h.export(l, "P_rowptr")),
+                         shape=(int(info[0]), int(info[2])))
+
+
+def agg_hierarchy(A, **kw):
+    cfg = draugr.AMGConfig(coarsening=draugr.AggregationCoarsening(0.25), max_coarse_size=2, **kw)
+    return draugr.amg_setup(A, cfg, on_device=False)
+
+
+def test_prolongation_and_restriction():
+    """testset "Prolongation" (:71-124): aggregation P has one unit entry per
+    row, P*ones = ones, restriction preserves the sum, the transpose map has
+    nc+1 offsets ending at nnz(P)+1, and restrict! equals the explicit Pᵀr
+    (atol 1e-12)."""
+    A = problems.poisson1d(10)
+    h = agg_hierarchy(A)
+    P = explicit_P(h, 0)
+    n, nc = P.shape
+    assert np.all(np.diff(P.indptr) == 1) and np.all(P.data == 1.0)
+    xf = oracle.prolongate(n, P.indptr.astype(np.int32), P.indices.astype(np.int32), P.data,
+                           np.ones(nc), np.zeros(n))
+    assert np.allclose(xf, 1.0)
+    off, rows, pnz = oracle.transpose_map(n, nc, P.indptr.astype(np.int32), P.indices.astype(np.int32))
+    assert len(off) == nc + 1 and off[0] == 0 and off[-1] == n
+    bc = oracle.restrict(nc, off, rows, pnz, P.data, np.ones(n))
+    assert np.isclose(bc.sum(), n)
+    r = np.random.default_rng(0).standard_normal(n)
+    bc = oracle.restrict(nc, off, rows, pnz, P.data, r)
+    assert np.allclose(bc, P.T @ r, atol=1e-12)
+
+
+def _galerkin_check(A, scale):
+    h = agg_hierarchy(A)
+    P = explicit_P(h, 0)
+    n, nc = P.shape
+    _, arp, aci, av = parts(A)
+    prp, pci = P.indptr.astype(np.int32), P.indices.astype(np.int32)
+    c_rp, c_ci, c_v, nz_off, tpi, tai, tpj = oracle.coarse_sparsity(n, nc, arp, aci, av, prp, pci, P.data)
+    Ac = sp.csr_matrix((c_v, c_ci, c_rp), shape=(nc, nc)).toarray()
+    assert np.allclose(Ac, (P.T @ A @ P).toarray(), atol=1e-12)
+    assert len(nz_off) == len(c_ci) + 1 and nz_off[0] == 0
+    assert np.all(np.diff(nz_off) >= 0)
+    # in-place resetup with scaled values
+    av2 = av * scale
+    cv2 = np.zeros(len(c_ci))
+    oracle.load().orc_galerkin(len(c_ci), oracle.ptr(nz_off), oracle.ptr(tpi), oracle.ptr(tai),
+                               oracle.ptr(tpj), oracle.ptr(P.data), oracle.ptr(av2), oracle.ptr(cv2))
+    Ac2 = sp.csr_matrix((cv2, c_ci, c_rp), shape=(nc, nc)).toarray()
+    A2 = sp.csr_matrix((av2, aci, arp), shape=(n, n))
+    assert np.allclose(Ac2, (P.T @ A2 @ P).toarray(), atol=1e-12)
+
+
+def test_galerkin_product():
+    """testsets "Galerkin Product" (:214-241), "contention-free kernel"
+    (:181-212) and "In-place Galerkin Resetup" (:243-270)."""
+    _galerkin_check(problems.poisson1d(10), 2.0)
+    _galerkin_check(problems.poisson1d(20), 3.0)
+
+
+def test_galerkin_multi_entry_p():
+    """testset with PMIS + standard interpolation (:1219-1252): several
+    entries per P row; the explicit PᵀAP agrees to 1e-10."""
+    A = problems.poisson2d(10)
+    cfg = draugr.AMGConfig(coarsening=draugr.PMISCoarsening(0.25, draugr.StandardInterpolation()),
+                           max_coarse_size=4)
+    h = draugr.amg_setup(A, cfg, on_device=False)
+    P = explicit_P(h, 0)
+    n, nc = P.shape
+    _, arp, aci, av = parts(A)
+    c_rp, c_ci, c_v, *_ = oracle.coarse_sparsity(n, nc, arp, aci, av, P.indptr.astype(np.int32),
+                                                 P.indices.astype(np.int32), P.data)
+    Ac = sp.csr_matrix((c_v, c_ci, c_rp), shape=(nc, nc)).toarray()
+    assert np.allclose(Ac, (P.T @ A @ P).toarray(), atol=1e-10)
+
+
+def test_jacobi_invdiag_and_smoothing():
+    """testset "Jacobi Smoother" (:272-284): invdiag ≡ 0.5 on the 1D
+    Laplacian; 10 steps reduce the residual."""
+    A = problems.poisson1d(10)
+    n, rp, ci, v = parts(A)
+    inv = oracle.invdiag(n, rp, ci, v)
+    assert np.allclose(inv, 0.5)
+    b = np.ones(n)
+    x = oracle.jacobi(n, rp, ci, v, inv, 2.0 / 3.0, np.zeros(n), b, 10)
+    assert np.linalg.norm(b - A @ x) < np.linalg.norm(b)
+
+
+def test_l1_invdiag():
+    """testset "L1 Colored GS Smoother - Build" (:607-617): interior row l1
+    norm 4 -> invdiag 0.25."""
+    A = problems.poisson1d(10)
+    n, rp, ci, v = parts(A)
+    inv = oracle.invdiag(n, rp, ci, v, l1=True)
+    assert np.isclose(inv[4], 0.25)
+
+
+def test_coloring():
+    """testsets "Graph Coloring" (:549-566) and "Colored GS Smoother" (:568-588)."""
+    A = problems.poisson1d(10)
+    n, rp, ci, v = parts(A)
+    colors, ncol, off, order = oracle.greedy_coloring(n, rp, ci)
+    assert len(colors) == 10 and np.all(colors > 0) and ncol >= 2
+    for i in range(n):
+        for k in range(rp[i], rp[i + 1]):
+            if ci[k] != i:
+                assert colors[i] != colors[ci[k]]
+    inv = oracle.invdiag(n, rp, ci, v)
+    b = np.ones(n)
+    x = oracle.gs(n, rp, ci, v, inv, ncol, off, order, np.zeros(n), b, 10)
+    assert np.linalg.norm(b - A @ x) < np.linalg.norm(b)
+
+
+def test_solve_thresholds_and_w_cycle():
+    """amg_solve! reaches 1e-8 in < 200 cycles (:332-415, :589-605) and the
+    W-cycle needs no more cycles than the V-cycle (:1828-1855)."""
+    A = problems.poisson2d(10)
+    b = np.random.default_rng(0).uniform(0, 1, 100)
+    for coars, smo in ((draugr.AggregationCoarsening(), draugr.L1ColoredGaussSeidelType()),
+                       (draugr.PMISCoarsening(), draugr.L1ColoredGaussSeidelType()),
+                       (draugr.AggressiveCoarsening(), draugr.L1ColoredGaussSeidelType()),
+                       (draugr.HMISCoarsening(0.5, draugr.ExtendedIInterpolation()),
+                        draugr.ColoredGaussSeidelType())):
+        cfg = draugr.AMGConfig(coarsening=coars, smoother=smo, max_coarse_size=10)
+        h = draugr.amg_setup(A, cfg, on_device=False)
+        O = oracle.OracleHierarchy(h)
+        x, it, rel = O.solve(np.zeros(100), b, tol=1e-8, maxiter=200)
+        assert it < 200 and rel < 1e-8
+        assert np.linalg.norm(b - A @ x) / np.linalg.norm(b) < 1e-8
+    A = problems.poisson2d(32)
+    b = np.random.default_rng(1).uniform(0, 1, A.shape[0])
+    h = draugr.amg_setup(A, draugr.AMGConfig(coarsening=draugr.AggregationCoarsening()),
+                         on_device=False)
+    O = oracle.OracleHierarchy(h)
+    _, itv, _ = O.solve(np.zeros(A.shape[0]), b, w=False, tol=1e-8, maxiter=300)
+    _, itw, _ = O.solve(np.zeros(A.shape[0]), b, w=True, tol=1e-8, maxiter=300)
+    assert itw <= itv
+
+
+def test_resetup_keeps_pattern_and_solves():
+    """testsets "AMG Resetup" (:392-415) and "Resetup Preserves Pattern"
+    (:417-434), on the oracle's partial resetup."""
+    A = problems.poisson2d(10)
+    cfg = draugr.AMGConfig(coarsening=draugr.AggregationCoarsening(), max_coarse_size=10)
+    h = draugr.amg_setup(A, cfg, on_device=False)
+    O = oracle.OracleHierarchy(h, with_rmaps=True)
+    pats = [(O.levels_np[l]["A_rp"].copy(), O.levels_np[l]["A_ci"].copy()) for l in range(O.nlevels)]
+    b = np.random.default_rng(2).uniform(0, 1, 100)
+    x1, _, r1 = O.solve(np.zeros(100), b, tol=1e-8, maxiter=200)
+    assert r1 < 1e-8
+    A2 = A * 2.0
+    O.resetup(A2.data)
+    for l, (rp, ci) in enumerate(pats):
+        assert np.array_equal(O.levels_np[l]["A_rp"], rp) and np.array_equal(O.levels_np[l]["A_ci"], ci)
+    x2, _, r2 = O.solve(np.zeros(100), b, tol=1e-8, maxiter=200)
+    assert np.linalg.norm(b - A2 @ x2) / np.linalg.norm(b) < 1e-8
+    assert not np.allclose(x1, x2, atol=1e-6)
+
+
+def test_lu_matches_numpy():
+    """The coarsest LU (getrf/getrs order) solves like a reference LU."""
+    rng = np.random.default_rng(3)
+    M = rng.standard_normal((17, 17)) + 17 * np.eye(17)
+    lu, piv, info = oracle.lu_factor(M)
+    assert info == 0
+    b = rng.standard_normal(17)
+    y = b.copy()
+    a = np.ascontiguousarray(lu.T).ravel()
+    oracle.load().orc_lu_solve(17, oracle.ptr(a), oracle.ptr(piv), oracle.ptr(y))
+    assert np.allclose(y, np.linalg.solve(M, b), atol=1e-12)
+    S = M.copy()
+    S[:, 3] = 0.0
+    assert oracle.lu_factor(S)[2] == 4  # SingularException(4)
