@@ -80,8 +80,8 @@ std::vector<int> make_tiles(const std::vector<int>& rp, int n, int G) {
 
 template <typename TA, class XL, class EP, bool DOT, class Fin>
 void launch_rows_impl(cudaStream_t st, int max_grid, int G, int n, int ntiles, const int* tp,
-                      const int* rp, const int* ci, const TA* av, XL xl, EP ep, double* partials,
-                      unsigned* ticket, Fin fin) {
+                      const int* ts, const int* rp, const int* ci, const TA* av, XL xl, EP ep,
+                      double* partials, unsigned* ticket, Fin fin) {
   if (n <= 0) {
     if constexpr (DOT) {
       // an empty reduction still has to deliver its (zero) result
@@ -95,8 +95,8 @@ void launch_rows_impl(cudaStream_t st, int max_grid, int G, int n, int ntiles, c
   switch (G) {
 #define DR_CASE(g)                                                                                \
   case g:                                                                                         \
-    k_tile_rows<g, TA, XL, EP, DOT, Fin><<<grid, kBlock, 0, st>>>(ntiles, tp, rp, ci, av, xl, ep,   \
-                                                                  partials, ticket, fin);          \
+    k_tile_rows<g, TA, XL, EP, DOT, Fin><<<grid, kBlock, 0, st>>>(ntiles, tp, ts, rp, ci, av, xl,   \
+                                                                  ep, partials, ticket, fin);      \
     break;
     DR_CASE(1) DR_CASE(2) DR_CASE(4) DR_CASE(8) DR_CASE(16) DR_CASE(32)
 #undef DR_CASE
@@ -107,15 +107,15 @@ void launch_rows_impl(cudaStream_t st, int max_grid, int G, int n, int ntiles, c
 
 template <typename TA, class XL, class EP>
 void launch_rows(cudaStream_t st, int max_grid, const DevMat& M, const TA* av, XL xl, EP ep) {
-  launch_rows_impl<TA, XL, EP, false, FinStore>(st, max_grid, M.G, M.n, M.ntiles, M.tp, M.rp, M.ci, av,
-                                                xl, ep, nullptr, nullptr, FinStore{nullptr});
+  launch_rows_impl<TA, XL, EP, false, FinStore>(st, max_grid, M.G, M.n, M.ntiles, M.tp, M.ts, M.rp, M.ci,
+                                                av, xl, ep, nullptr, nullptr, FinStore{nullptr});
 }
 
 template <typename TA, class XL, class EP, class Fin>
 void launch_rows_dot(cudaStream_t st, int max_grid, const DevMat& M, const TA* av, XL xl, EP ep,
                      double* partials, unsigned* ticket, Fin fin) {
-  launch_rows_impl<TA, XL, EP, true, Fin>(st, max_grid, M.G, M.n, M.ntiles, M.tp, M.rp, M.ci, av, xl,
-                                          ep, partials, ticket, fin);
+  launch_rows_impl<TA, XL, EP, true, Fin>(st, max_grid, M.G, M.n, M.ntiles, M.tp, M.ts, M.rp, M.ci, av,
+                                          xl, ep, partials, ticket, fin);
 }
 
 int grid1d(long long n, int max_grid) {
@@ -175,17 +175,23 @@ DevHier::DevHier(const HostHierarchy& H, int device) {
       M.m = m;
       M.nnz = (long long)ci.size();
       M.rp = alloc<int>(rp.size());
-      M.ci = alloc<int>(ci.size());
+      // column and value arrays carry 4 padding entries for the tile
+      // kernel's 128-bit loads
+      M.ci = alloc<int>(ci.size() + 4);
       h2d(M.rp, rp, st_);
       h2d(M.ci, ci, st_);
-      M.v = alloc<double>(ci.size());
+      M.v = alloc<double>(ci.size() + 4);
       if (v) h2d(M.v, *v, st_);
       M.G = tile_lanes(M.nnz, n);
       M.Ggs = pick_G(M.nnz, n);
       std::vector<int> tiles = make_tiles(rp, n, M.G);
+      std::vector<int> tstart(tiles.size());
+      for (size_t t = 0; t < tiles.size(); ++t) tstart[t] = rp[tiles[t]];
       M.ntiles = (int)tiles.size() - 1;
       M.tp = alloc<int>(tiles.size());
+      M.ts = alloc<int>(tiles.size());
       DR_CK(cudaMemcpy(M.tp, tiles.data(), tiles.size() * sizeof(int), cudaMemcpyHostToDevice));
+      DR_CK(cudaMemcpy(M.ts, tstart.data(), tstart.size() * sizeof(int), cudaMemcpyHostToDevice));
     };
     for (int l = 0; l < nl; ++l) {
       const HostLevel& h = H.levels[l];
@@ -291,9 +297,9 @@ void DevHier::ensure_fp32() {
   if (fp32_) return;
   graphs_clear();
   for (auto& d : L_) {
-    d.A.v32 = alloc<float>(d.A.nnz);
-    d.P.v32 = alloc<float>(d.P.nnz);
-    d.R.v32 = alloc<float>(d.R.nnz);
+    d.A.v32 = alloc<float>(d.A.nnz + 4);
+    d.P.v32 = alloc<float>(d.P.nnz + 4);
+    d.R.v32 = alloc<float>(d.R.nnz + 4);
     d.invd32 = alloc<float>(d.A.n);
     const int n = d.A.n;
     d.v32.xa = alloc<float>(n);

@@ -41,6 +41,7 @@ struct DevMat {
   int Ggs = 8;        // lanes per row of the Gauss-Seidel colour kernel
   int ntiles = 0;     // row tiles (see k_tile_rows)
   int* tp = nullptr;  // tile row starts, ntiles+1
+  int* ts = nullptr;  // tile nonzero starts, ntiles+1
 };
 
 template <typename T>

@@ -130,30 +130,36 @@ __device__ __forceinline__ T XZeroJacobi<T>::operator()(int j) const {
 }
 
 // ------------------------------------------------------------ epilogues
-// A row of a row kernel is reduced as  acc = init(i) ± a_i1 x_1 ± a_i2 x_2 ...
-// (kSign = +1 adds the products, -1 subtracts them) and then apply(i, acc)
-// writes the row's results and returns its contribution to a fused dot
-// product.  With one lane per row the products are accumulated in column
-// order, exactly as the reference's loops do; with G > 1 lanes the products
-// are summed in a fixed tree first and then added to (subtracted from) init.
+// A row of a row kernel is reduced as  acc = init ± a_i1 x_1 ± a_i2 x_2 ...
+// (kSign = +1 adds the products, -1 subtracts them) and then apply() writes
+// the row's results and returns its contribution to a fused dot product.
+// pre(i) loads the row's other operands; the tile kernel issues it before
+// its barrier so those loads overlap the streaming of the tile.  With one
+// lane per row the products are accumulated in column order, exactly as the
+// reference's loops do; with G > 1 lanes they are summed in a fixed tree
+// first and then added to (subtracted from) init.
 template <typename T>
 struct EpStore {  // y = A x                                (csr_matrix.jl:150-159)
   using acc_t = T;
   static constexpr int kSign = 1;
+  struct Pre {};
   T* __restrict__ y;
-  __device__ __forceinline__ T init(int) const { return T(0); }
-  __device__ __forceinline__ double apply(int i, T v) const { y[i] = v; return 0.0; }
+  __device__ __forceinline__ Pre pre(int) const { return {}; }
+  __device__ __forceinline__ T init(const Pre&) const { return T(0); }
+  __device__ __forceinline__ double apply(int i, T v, const Pre&) const { y[i] = v; return 0.0; }
 };
 
 template <typename T>
 struct EpResidual {  // Ax = Σ a x ; r = b - Ax                (cycle.jl:32-43)
   using acc_t = T;
   static constexpr int kSign = 1;
+  struct Pre { T b; };
   const T* __restrict__ b;
   T* __restrict__ r;
-  __device__ __forceinline__ T init(int) const { return T(0); }
-  __device__ __forceinline__ double apply(int i, T v) const {
-    T ri = sub_rn(__ldg(b + i), v);
+  __device__ __forceinline__ Pre pre(int i) const { return {__ldg(b + i)}; }
+  __device__ __forceinline__ T init(const Pre&) const { return T(0); }
+  __device__ __forceinline__ double apply(int i, T v, const Pre& p) const {
+    T ri = sub_rn(p.b, v);
     r[i] = ri;
     return (double)ri * (double)ri;
   }
@@ -163,17 +169,21 @@ template <typename T>
 struct EpJacobi {  // r = b - a x - ... ; xn = x + (ω·invd)·r   (smoothers.jl:78-94)
   using acc_t = T;
   static constexpr int kSign = -1;
+  struct Pre { T x, b, d; double w; };
   const T* __restrict__ x;
   const T* __restrict__ b;
   const T* __restrict__ invd;
   T* __restrict__ xn;
   T omega;
   const double* __restrict__ w;  // optional: returns w_i·xn_i for a fused dot
-  __device__ __forceinline__ T init(int i) const { return __ldg(b + i); }
-  __device__ __forceinline__ double apply(int i, T r) const {
-    T v = add_rn(__ldg(x + i), mul_rn(mul_rn(omega, __ldg(invd + i)), r));
+  __device__ __forceinline__ Pre pre(int i) const {
+    return {__ldg(x + i), __ldg(b + i), __ldg(invd + i), w ? __ldg(w + i) : 0.0};
+  }
+  __device__ __forceinline__ T init(const Pre& p) const { return p.b; }
+  __device__ __forceinline__ double apply(int i, T r, const Pre& p) const {
+    T v = add_rn(p.x, mul_rn(mul_rn(omega, p.d), r));
     xn[i] = v;
-    return w ? __ldg(w + i) * (double)v : 0.0;
+    return p.w * (double)v;
   }
 };
 
@@ -181,16 +191,17 @@ template <typename T>
 struct EpZeroJacobiResidual {  // x1 = (ω·invd)·b ; r = b - A x1
   using acc_t = T;
   static constexpr int kSign = 1;
+  struct Pre { T b, d; };
   const T* __restrict__ b;
   const T* __restrict__ invd;
   T* __restrict__ x1;
   T* __restrict__ r;
   T omega;
-  __device__ __forceinline__ T init(int) const { return T(0); }
-  __device__ __forceinline__ double apply(int i, T v) const {
-    T bi = __ldg(b + i);
-    x1[i] = mul_rn(mul_rn(omega, __ldg(invd + i)), bi);
-    r[i] = sub_rn(bi, v);
+  __device__ __forceinline__ Pre pre(int i) const { return {__ldg(b + i), __ldg(invd + i)}; }
+  __device__ __forceinline__ T init(const Pre&) const { return T(0); }
+  __device__ __forceinline__ double apply(int i, T v, const Pre& p) const {
+    x1[i] = mul_rn(mul_rn(omega, p.d), p.b);
+    r[i] = sub_rn(p.b, v);
     return 0.0;
   }
 };
@@ -199,85 +210,138 @@ template <typename T>
 struct EpAddTo {  // x += p xc, per entry                  (prolongation.jl:742-760)
   using acc_t = T;
   static constexpr int kSign = 1;
+  struct Pre { T x; };
   T* __restrict__ x;
-  __device__ __forceinline__ T init(int i) const { return x[i]; }
-  __device__ __forceinline__ double apply(int i, T v) const { x[i] = v; return 0.0; }
+  __device__ __forceinline__ Pre pre(int i) const { return {x[i]}; }
+  __device__ __forceinline__ T init(const Pre& p) const { return p.x; }
+  __device__ __forceinline__ double apply(int i, T v, const Pre&) const { x[i] = v; return 0.0; }
 };
 
 template <typename T>
 struct EpPcgDir {  // q = A p, p_new = z + β p_old, returns p_new·q
   using acc_t = double;
   static constexpr int kSign = 1;
+  struct Pre { double p; };
   XPcgDir<T> dir;
   double* __restrict__ pnew;
   double* __restrict__ q;
-  __device__ __forceinline__ double init(int) const { return 0.0; }
-  __device__ __forceinline__ double apply(int i, double s) const {
-    double pi = dir(i);
-    pnew[i] = pi;
+  __device__ __forceinline__ Pre pre(int i) const { return {dir(i)}; }
+  __device__ __forceinline__ double init(const Pre&) const { return 0.0; }
+  __device__ __forceinline__ double apply(int i, double s, const Pre& pr) const {
+    pnew[i] = pr.p;
     q[i] = s;
-    return pi * s;
+    return pr.p * s;
   }
 };
 
 // ------------------------------------------------------------ row kernel
 // Rows are packed (on the host, once per matrix) into tiles of at most
-// kBlock/G consecutive rows holding at most kTileCap nonzeros.  A block
-// streams a tile's column and value arrays with consecutive threads on
-// consecutive entries (fully coalesced, many independent loads in flight),
-// stages the products a_ij·x_j in shared memory, then reduces the rows with
-// G lanes each and applies the fused epilogue.  A row longer than kTileCap
-// forms a tile of its own and is reduced by the whole block.
-constexpr int kTileCap = 2048;
+// kBlock/G consecutive rows holding at most kTileCap nonzeros; tp[t] is the
+// first row and ts[t] the first nonzero of tile t.  Per tile a block
+//   1. loads the tile's columns and values four entries at a time with
+//      128-bit loads (the arrays are padded by four entries, and the first
+//      group is aligned down, so every vector load is aligned and in bounds),
+//      and, in the same round, the row pointers and epilogue operands of the
+//      row it will finish;
+//   2. gathers x for the valid entries and stages a_ij·x_j in shared memory;
+//   3. after a barrier reduces its row with G lanes and applies the epilogue.
+// A row longer than kTileCap forms a tile of its own and is reduced by the
+// whole block.
+constexpr int kTileCap = 2044;  // a tile's 4-entry groups (first aligned down) fit 2 per thread
+constexpr int kGroups = (kTileCap + 3 + 3) / 4;                 // 4-entry groups per tile
+constexpr int kGroupIters = (kGroups + kBlock - 1) / kBlock;     // per thread
+
+template <typename TA> struct Vec4;
+template <> struct Vec4<double> {
+  double2 a, b;
+  __device__ __forceinline__ void load(const double* p) {
+    a = __ldg(reinterpret_cast<const double2*>(p));
+    b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+  }
+  __device__ __forceinline__ double operator[](int j) const {
+    return j == 0 ? a.x : j == 1 ? a.y : j == 2 ? b.x : b.y;
+  }
+};
+template <> struct Vec4<float> {
+  float4 a;
+  __device__ __forceinline__ void load(const float* p) { a = __ldg(reinterpret_cast<const float4*>(p)); }
+  __device__ __forceinline__ float operator[](int j) const {
+    return j == 0 ? a.x : j == 1 ? a.y : j == 2 ? a.z : a.w;
+  }
+};
 
 template <int G, typename TA, class XL, class EP, bool DOT, class Fin>
 __global__ void __launch_bounds__(kBlock)
-k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ rp,
-            const int* __restrict__ ci, const TA* __restrict__ av, XL xl, EP ep, double* partials,
-            unsigned* ticket, Fin fin) {
+k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
+            const int* __restrict__ rp, const int* __restrict__ ci, const TA* __restrict__ av,
+            XL xl, EP ep, double* partials, unsigned* ticket, Fin fin) {
   using acc_t = typename EP::acc_t;
+  using Pre = typename EP::Pre;
   __shared__ acc_t prod[kTileCap];
   const int lane = threadIdx.x & (G - 1);
   const int grp = threadIdx.x / G;
   double dacc = 0.0;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int r0 = __ldg(tp + t), r1 = __ldg(tp + t + 1);
-    const int s = __ldg(rp + r0), e = __ldg(rp + r1);
+    const int s = __ldg(ts + t), e = __ldg(ts + t + 1);
     const int len = e - s;
     if (len <= kTileCap) {
-      const int* cp = ci + s;
-      const TA* vp = av + s;
-#pragma unroll 4
-      for (int k = threadIdx.x; k < len; k += kBlock)
-        prod[k] = mul_rn((acc_t)__ldg(vp + k), (acc_t)xl(__ldg(cp + k)));
-      __syncthreads();
+      // round 1: columns and values of the tile, row bounds and operands
+      const int sal = s & ~3;
+      const int ng = (e - sal + 3) >> 2;
+      int4 c[kGroupIters];
+      Vec4<TA> v[kGroupIters];
+#pragma unroll
+      for (int q = 0; q < kGroupIters; ++q) {
+        const int g = threadIdx.x + q * kBlock;
+        if (g < ng) {
+          c[q] = __ldg(reinterpret_cast<const int4*>(ci + sal) + g);
+          v[q].load(av + sal + 4 * g);
+        }
+      }
       const int row = r0 + grp;
       const bool valid = row < r1;
+      int rs = 0, re = 0;
+      Pre pr{};
+      if (valid) {
+        rs = __ldg(rp + row) - s;
+        re = __ldg(rp + row + 1) - s;
+        if (lane == 0) pr = ep.pre(row);
+      }
+      // round 2: gathers and products
+#pragma unroll
+      for (int q = 0; q < kGroupIters; ++q) {
+        const int g = threadIdx.x + q * kBlock;
+        if (g < ng) {
+          const int k0 = sal + 4 * g;
+          const int cc[4] = {c[q].x, c[q].y, c[q].z, c[q].w};
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int k = k0 + j;
+            if (k >= s && k < e) prod[k - s] = mul_rn((acc_t)v[q][j], (acc_t)xl(cc[j]));
+          }
+        }
+      }
+      __syncthreads();
       if constexpr (G == 1) {
         if (valid) {
-          const int rs = __ldg(rp + row) - s, re = __ldg(rp + row + 1) - s;
-          acc_t a = ep.init(row);
+          acc_t a = ep.init(pr);
           for (int k = rs; k < re; ++k) {
             if constexpr (EP::kSign > 0) a = add_rn(a, prod[k]);
             else a = sub_rn(a, prod[k]);
           }
-          dacc += ep.apply(row, a);
+          dacc += ep.apply(row, a, pr);
         }
       } else {
-        int rs = 0, re = 0;
-        if (valid) {
-          rs = __ldg(rp + row) - s;
-          re = __ldg(rp + row + 1) - s;
-        }
         acc_t sum = acc_t(0);
         for (int k = rs + lane; k < re; k += G) sum = add_rn(sum, prod[k]);
 #pragma unroll
         for (int off = G >> 1; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
         if (valid && lane == 0) {
-          acc_t a = ep.init(row);
+          acc_t a = ep.init(pr);
           if constexpr (EP::kSign > 0) a = add_rn(a, sum);
           else a = sub_rn(a, sum);
-          dacc += ep.apply(row, a);
+          dacc += ep.apply(row, a, pr);
         }
       }
       __syncthreads();
@@ -295,10 +359,11 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ rp,
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
         if (threadIdx.x == 0) {
-          acc_t a = ep.init(r0);
+          const Pre pr = ep.pre(r0);
+          acc_t a = ep.init(pr);
           if constexpr (EP::kSign > 0) a = add_rn(a, sum);
           else a = sub_rn(a, sum);
-          dacc += ep.apply(r0, a);
+          dacc += ep.apply(r0, a, pr);
         }
       }
       __syncthreads();
