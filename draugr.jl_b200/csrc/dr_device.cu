@@ -34,6 +34,11 @@ static std::atomic<long long> g_launches{0};
 long long kernel_launches() { return g_launches.load(); }
 static inline void counted() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
+// SM count of the device in use and a device flag the row kernels set when a
+// bounded wait gives up (checked after every solve / resetup).
+static int g_nsm = 148;
+static int* g_err = nullptr;
+
 void cuda_check(cudaError_t e, const char* what, const char* file, int line) {
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -90,13 +95,17 @@ void launch_rows_impl(cudaStream_t st, int max_grid, int G, int n, int ntiles, c
     }
     return;
   }
-  const int grid = std::max(1, std::min(ntiles, max_grid));
+  // resident blocks per SM: shared memory allows 4 (FP64 values) or 6 (FP32)
+  const int per_sm = sizeof(TA) == 8 ? 4 : 6;
+  const int grid = std::max(1, std::min({ntiles, max_grid, g_nsm * per_sm}));
+  const size_t smem = tile_smem_bytes<TA>();
   counted();
   switch (G) {
-#define DR_CASE(g)                                                                                \
-  case g:                                                                                         \
-    k_tile_rows<g, TA, XL, EP, DOT, Fin><<<grid, kBlock, 0, st>>>(ntiles, tp, ts, rp, ci, av, xl,   \
-                                                                  ep, partials, ticket, fin);      \
+#define DR_CASE(g)                                                                                 \
+  case g:                                                                                          \
+    k_tile_rows<g, TA, XL, EP, DOT, Fin><<<grid, kBlock, smem, st>>>(ntiles, tp, ts, rp, ci, av, xl, \
+                                                                     ep, partials, ticket, fin,    \
+                                                                     g_err);                       \
     break;
     DR_CASE(1) DR_CASE(2) DR_CASE(4) DR_CASE(8) DR_CASE(16) DR_CASE(32)
 #undef DR_CASE
@@ -159,6 +168,11 @@ DevHier::DevHier(const HostHierarchy& H, int device) {
   DR_CK(cudaSetDevice(device));
   DR_CK(cudaDeviceGetAttribute(&nsm_, cudaDevAttrMultiProcessorCount, device));
   max_grid_ = nsm_ * 8;
+  g_nsm = nsm_;
+  if (!g_err) {
+    DR_CK(cudaMalloc(&g_err, sizeof(int)));
+    DR_CK(cudaMemset(g_err, 0, sizeof(int)));
+  }
   DR_CK(cudaStreamCreateWithFlags(&own_st_, cudaStreamNonBlocking));
   st_ = own_st_;
   own_stream_ = true;
@@ -265,6 +279,19 @@ DevHier::~DevHier() {
   cudaEventDestroy(ev_[0]);
   cudaEventDestroy(ev_[1]);
   if (own_stream_ && own_st_) cudaStreamDestroy(own_st_);
+}
+
+// Raise if a row kernel reported a bounded wait that gave up (the flag is
+// cleared so the hierarchy stays usable).
+static void check_kernel_flag(cudaStream_t st) {
+  int e = 0;
+  DR_CK(cudaMemcpyAsync(&e, g_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  DR_CK(cudaStreamSynchronize(st));
+  if (e) {
+    DR_CK(cudaMemsetAsync(g_err, 0, sizeof(int), st));
+    DR_CK(cudaStreamSynchronize(st));
+    fail("a row kernel timed out waiting for its tile copy (results discarded)");
+  }
 }
 
 void DevHier::set_stream(cudaStream_t s) {
@@ -479,6 +506,7 @@ int DevHier::solve(double* x, const double* b, const CycleOpts& o, double tol, i
     const double rnorm = std::sqrt(hscal_[SC_RR]);
     rel = rnorm / bnorm;
     if (verbose >= 2) std::printf("  AMG iter %4d: residual norm = %.6e, relative = %.6e\n", it, rnorm, rel);
+    if (rel < tol || it == maxiter) check_kernel_flag(st_);
     if (rel < tol) {
       if (verbose >= 1) std::printf("AMG solve converged: %d iterations, final residual %.2e\n", it, rel);
       if (relres) *relres = rel;
@@ -657,7 +685,7 @@ int DevHier::pcg(double* x, const double* b, const CycleOpts& o, double tol, int
   }
   if (it > maxiter) it = maxiter;
   if (x != X) DR_CK(cudaMemcpyAsync(x, X, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st_));
-  DR_CK(cudaStreamSynchronize(st_));
+  check_kernel_flag(st_);
   if (verbose >= 1)
     std::printf("AMG-PCG (%s cycle) %s: %d iterations, final residual %.2e\n", mixed ? "FP32" : "FP64",
                 rel < tol ? "converged" : "did NOT converge", it, rel);
@@ -716,6 +744,7 @@ void DevHier::resetup_values(const double* v_dev) {
   k_lu_factor<<<1, threads, 0, st_>>>(nc_, clu_, cpiv_, info_);
   DR_CK(cudaGetLastError());
   refresh_fp32();
+  check_kernel_flag(st_);
   int info = 0;
   DR_CK(cudaMemcpyAsync(&info, info_, sizeof(int), cudaMemcpyDeviceToHost, st_));
   DR_CK(cudaStreamSynchronize(st_));
@@ -828,7 +857,7 @@ void DevHier::level_op(int lvl, int op, bool fp32, const double* in1, const doub
   };
   if (fp32) run(float());
   else run(double());
-  DR_CK(cudaStreamSynchronize(st_));
+  check_kernel_flag(st_);
 }
 
 float DevHier::time_level_op(int lvl, int op, bool fp32, int reps) {

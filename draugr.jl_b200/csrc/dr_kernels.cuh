@@ -234,109 +234,177 @@ struct EpPcgDir {  // q = A p, p_new = z + β p_old, returns p_new·q
   }
 };
 
+// ------------------------------------------------------------ TMA / mbarrier
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: gives up after `limit` polls (each poll itself blocks for a
+// hardware-defined time) and reports it; never spins forever.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int limit) {
+  for (int i = 0; i < limit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+// 1-D bulk copy global -> shared (TMA engine), completion counted on `bar`.
+// dst and src 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
 // ------------------------------------------------------------ row kernel
 // Rows are packed (on the host, once per matrix) into tiles of at most
 // kBlock/G consecutive rows holding at most kTileCap nonzeros; tp[t] is the
-// first row and ts[t] the first nonzero of tile t.  Per tile a block
-//   1. loads the tile's columns and values four entries at a time with
-//      128-bit loads (the arrays are padded by four entries, and the first
-//      group is aligned down, so every vector load is aligned and in bounds),
-//      and, in the same round, the row pointers and epilogue operands of the
-//      row it will finish;
-//   2. gathers x for the valid entries and stages a_ij·x_j in shared memory;
-//   3. after a barrier reduces its row with G lanes and applies the epilogue.
-// A row longer than kTileCap forms a tile of its own and is reduced by the
-// whole block.
-constexpr int kTileCap = 2044;  // a tile's 4-entry groups (first aligned down) fit 2 per thread
-constexpr int kGroups = (kTileCap + 3 + 3) / 4;                 // 4-entry groups per tile
-constexpr int kGroupIters = (kGroups + kBlock - 1) / kBlock;     // per thread
+// first row and ts[t] the first nonzero of tile t.  Each block walks the
+// tiles blockIdx.x, +gridDim.x, ... with two shared-memory stages: while it
+// reduces the rows of one tile, the TMA engine copies the column and value
+// arrays of the tile after next into the other stage (cp.async.bulk with an
+// mbarrier), so HBM streaming never waits on the SM.  The row phase reads
+// columns and values from shared memory, gathers x (an L2-resident vector)
+// and applies the fused epilogue, whose own operands are loaded before the
+// gathers.  The column / value arrays carry 4 padding entries so the
+// 16-byte-rounded copies stay in bounds.  A row longer than kTileCap forms a
+// tile of its own and is read straight from global memory by the whole block.
+constexpr int kTileCap = 2040;
+constexpr int kStageEntries = 2048;  // kTileCap + alignment slack, rounded to 16 bytes
+constexpr int kWaitLimit = 1 << 22;
 
-template <typename TA> struct Vec4;
-template <> struct Vec4<double> {
-  double2 a, b;
-  __device__ __forceinline__ void load(const double* p) {
-    a = __ldg(reinterpret_cast<const double2*>(p));
-    b = __ldg(reinterpret_cast<const double2*>(p) + 1);
-  }
-  __device__ __forceinline__ double operator[](int j) const {
-    return j == 0 ? a.x : j == 1 ? a.y : j == 2 ? b.x : b.y;
-  }
-};
-template <> struct Vec4<float> {
-  float4 a;
-  __device__ __forceinline__ void load(const float* p) { a = __ldg(reinterpret_cast<const float4*>(p)); }
-  __device__ __forceinline__ float operator[](int j) const {
-    return j == 0 ? a.x : j == 1 ? a.y : j == 2 ? a.z : a.w;
-  }
-};
+// Dynamic shared memory of k_tile_rows: two stages of columns and values
+// (48 KB for FP64 values, so no opt-in attribute is needed).
+template <typename TA>
+constexpr size_t tile_smem_bytes() {
+  return 2 * (size_t)kStageEntries * (sizeof(int) + sizeof(TA));
+}
 
 template <int G, typename TA, class XL, class EP, bool DOT, class Fin>
 __global__ void __launch_bounds__(kBlock)
 k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
             const int* __restrict__ rp, const int* __restrict__ ci, const TA* __restrict__ av,
-            XL xl, EP ep, double* partials, unsigned* ticket, Fin fin) {
+            XL xl, EP ep, double* partials, unsigned* ticket, Fin fin, int* err) {
   using acc_t = typename EP::acc_t;
   using Pre = typename EP::Pre;
-  __shared__ acc_t prod[kTileCap];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  // stage b: values at sv0 + b*kStageEntries, columns at sc0 + b*kStageEntries
+  TA* const sv0 = reinterpret_cast<TA*>(smem_raw);
+  int* const sc0 = reinterpret_cast<int*>(sv0 + 2 * kStageEntries);
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ acc_t red[32];
+
   const int lane = threadIdx.x & (G - 1);
   const int grp = threadIdx.x / G;
+  const int stride = gridDim.x;
+
+  auto issue = [&](int t, int b) {  // thread 0 only
+    const int s = __ldg(ts + t), e = __ldg(ts + t + 1);
+    if (e - s > kTileCap) {
+      mbar_arrive(bar + b);  // long row: nothing to stage
+      return;
+    }
+    const int sal = s & ~3;
+    const uint32_t cnt = (uint32_t)(e - sal);
+    const uint32_t cb = (cnt * 4u + 15u) & ~15u;
+    const uint32_t vb = (cnt * (uint32_t)sizeof(TA) + 15u) & ~15u;
+    mbar_expect_tx(bar + b, cb + vb);
+    bulk_g2s(sc0 + b * kStageEntries, ci + sal, cb, bar + b);
+    bulk_g2s(sv0 + b * kStageEntries, av + sal, vb, bar + b);
+  };
+
+  if (threadIdx.x == 0) {
+    mbar_init(bar + 0, 1);
+    mbar_init(bar + 1, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    if (blockIdx.x + stride < ntiles) issue(blockIdx.x + stride, 1);
+  }
+
   double dacc = 0.0;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+  int i = 0;
+  for (int t = blockIdx.x; t < ntiles; t += stride, ++i) {
+    const int b = i & 1;
+    const uint32_t parity = (uint32_t)((i >> 1) & 1);
     const int r0 = __ldg(tp + t), r1 = __ldg(tp + t + 1);
     const int s = __ldg(ts + t), e = __ldg(ts + t + 1);
     const int len = e - s;
+    // row bounds and epilogue operands, issued before waiting for the stage
+    const int row = r0 + grp;
+    const bool valid = (len <= kTileCap) && row < r1;
+    int rs = 0, re = 0;
+    Pre pr{};
+    if (valid) {
+      rs = __ldg(rp + row) - s;
+      re = __ldg(rp + row + 1) - s;
+      if (lane == 0) pr = ep.pre(row);
+    }
+    if (!mbar_wait_bounded(bar + b, parity, kWaitLimit)) {
+      if (threadIdx.x == 0) atomicExch(err, 1);
+      mbar_wait_bounded(bar + b, parity, kWaitLimit);
+    }
     if (len <= kTileCap) {
-      // round 1: columns and values of the tile, row bounds and operands
-      const int sal = s & ~3;
-      const int ng = (e - sal + 3) >> 2;
-      int4 c[kGroupIters];
-      Vec4<TA> v[kGroupIters];
-#pragma unroll
-      for (int q = 0; q < kGroupIters; ++q) {
-        const int g = threadIdx.x + q * kBlock;
-        if (g < ng) {
-          c[q] = __ldg(reinterpret_cast<const int4*>(ci + sal) + g);
-          v[q].load(av + sal + 4 * g);
-        }
-      }
-      const int row = r0 + grp;
-      const bool valid = row < r1;
-      int rs = 0, re = 0;
-      Pre pr{};
-      if (valid) {
-        rs = __ldg(rp + row) - s;
-        re = __ldg(rp + row + 1) - s;
-        if (lane == 0) pr = ep.pre(row);
-      }
-      // round 2: gathers and products
-#pragma unroll
-      for (int q = 0; q < kGroupIters; ++q) {
-        const int g = threadIdx.x + q * kBlock;
-        if (g < ng) {
-          const int k0 = sal + 4 * g;
-          const int cc[4] = {c[q].x, c[q].y, c[q].z, c[q].w};
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const int k = k0 + j;
-            if (k >= s && k < e) prod[k - s] = mul_rn((acc_t)v[q][j], (acc_t)xl(cc[j]));
-          }
-        }
-      }
-      __syncthreads();
+      const int off = s - (s & ~3);
+      const int* cs = sc0 + b * kStageEntries + off;
+      const TA* vs = sv0 + b * kStageEntries + off;
       if constexpr (G == 1) {
         if (valid) {
           acc_t a = ep.init(pr);
-          for (int k = rs; k < re; ++k) {
-            if constexpr (EP::kSign > 0) a = add_rn(a, prod[k]);
-            else a = sub_rn(a, prod[k]);
+          for (int k0 = rs; k0 < re; k0 += 8) {
+            acc_t p[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+              p[j] = (k0 + j < re) ? mul_rn((acc_t)vs[k0 + j], (acc_t)xl(cs[k0 + j])) : acc_t(0);
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+              if (k0 + j < re) {
+                if constexpr (EP::kSign > 0) a = add_rn(a, p[j]);
+                else a = sub_rn(a, p[j]);
+              }
           }
           dacc += ep.apply(row, a, pr);
         }
       } else {
         acc_t sum = acc_t(0);
-        for (int k = rs + lane; k < re; k += G) sum = add_rn(sum, prod[k]);
+        for (int k0 = rs + lane; k0 < re; k0 += 4 * G) {
+          acc_t p[4];
 #pragma unroll
-        for (int off = G >> 1; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+          for (int j = 0; j < 4; ++j) {
+            const int k = k0 + j * G;
+            p[j] = (k < re) ? mul_rn((acc_t)vs[k], (acc_t)xl(cs[k])) : acc_t(0);
+          }
+#pragma unroll
+          for (int j = 0; j < 4; ++j) sum = add_rn(sum, p[j]);
+        }
+#pragma unroll
+        for (int o = G >> 1; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
         if (valid && lane == 0) {
           acc_t a = ep.init(pr);
           if constexpr (EP::kSign > 0) a = add_rn(a, sum);
@@ -344,29 +412,32 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
           dacc += ep.apply(row, a, pr);
         }
       }
-      __syncthreads();
     } else {
-      // a single row longer than the tile capacity
+      // a single row longer than the tile capacity, from global memory
       acc_t sum = acc_t(0);
       for (int k = s + threadIdx.x; k < e; k += kBlock)
         sum = add_rn(sum, mul_rn((acc_t)__ldg(av + k), (acc_t)xl(__ldg(ci + k))));
 #pragma unroll
-      for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
-      if ((threadIdx.x & 31) == 0) prod[threadIdx.x >> 5] = sum;
+      for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sum;
       __syncthreads();
       if (threadIdx.x < 32) {
-        sum = threadIdx.x < (kBlock >> 5) ? prod[threadIdx.x] : acc_t(0);
+        sum = threadIdx.x < (kBlock >> 5) ? red[threadIdx.x] : acc_t(0);
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
         if (threadIdx.x == 0) {
-          const Pre pr = ep.pre(r0);
-          acc_t a = ep.init(pr);
+          const Pre p0 = ep.pre(r0);
+          acc_t a = ep.init(p0);
           if constexpr (EP::kSign > 0) a = add_rn(a, sum);
           else a = sub_rn(a, sum);
-          dacc += ep.apply(r0, a, pr);
+          dacc += ep.apply(r0, a, p0);
         }
       }
-      __syncthreads();
+    }
+    __syncthreads();  // stage b fully consumed
+    if (threadIdx.x == 0 && t + 2 * stride < ntiles) {
+      fence_proxy_async();
+      issue(t + 2 * stride, b);
     }
   }
   if constexpr (DOT) grid_sum_finalize(dacc, partials, ticket, fin);
