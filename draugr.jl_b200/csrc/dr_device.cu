@@ -96,7 +96,7 @@ void launch_rows_impl(cudaStream_t st, int max_grid, int G, int n, int ntiles, c
     return;
   }
   // resident blocks per SM: shared memory allows 4 (FP64 values) or 6 (FP32)
-  const int per_sm = sizeof(TA) == 8 ? 4 : 6;
+  const int per_sm = sizeof(TA) == 8 ? 4 : 7;
   const int grid = std::max(1, std::min({ntiles, max_grid, g_nsm * per_sm}));
   const size_t smem = tile_smem_bytes<TA>();
   counted();

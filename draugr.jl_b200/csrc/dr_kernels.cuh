@@ -293,12 +293,13 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 // gathers.  The column / value arrays carry 4 padding entries so the
 // 16-byte-rounded copies stay in bounds.  A row longer than kTileCap forms a
 // tile of its own and is read straight from global memory by the whole block.
-constexpr int kTileCap = 2040;
-constexpr int kStageEntries = 2048;  // kTileCap + alignment slack, rounded to 16 bytes
+constexpr int kTileCap = 2000;
+constexpr int kStageEntries = 2008;  // kTileCap + alignment slack, a multiple of 4 entries
 constexpr int kWaitLimit = 1 << 22;
 
 // Dynamic shared memory of k_tile_rows: two stages of columns and values
-// (48 KB for FP64 values, so no opt-in attribute is needed).
+// (47 KB for FP64 values; with the kernel's static shared memory it stays
+// under the 48 KB that needs no opt-in attribute).
 template <typename TA>
 constexpr size_t tile_smem_bytes() {
   return 2 * (size_t)kStageEntries * (sizeof(int) + sizeof(TA));
