@@ -84,6 +84,7 @@ def workload_config(n, A, h=None, setup_s=None):
         rows = [int(h.level_info(l)[0]) for l in range(nl)] + [int(h.level_info(-1)[0])]
         nnzs = [int(h.level_info(l)[1]) for l in range(nl)]
         d.update(levels=nl + 1, level_rows=rows, level_nnz=nnzs,
+                 level_nnzP=[int(h.level_info(l)[3]) for l in range(nl)],
                  operator_complexity=round(sum(nnzs) / nnzs[0], 3) if nnzs else None)
     if setup_s is not None:
         d["setup_s_cpu"] = round(setup_s, 3)
@@ -372,6 +373,42 @@ def run_reference(args, world, rank):
             "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+OPS = {0: "spmv", 2: "jacobi", 3: "restrict", 4: "prolong", 6: "zero_jacobi_residual"}
+
+
+def op_bytes(op, prec, n, nnz, nc, nnzp):
+    """Algorithmic bytes of one level kernel (each operand once, int32
+    indices; the formulas of the survey's measurement table, with V = 8 for
+    FP64 and 4 for FP32 values and vectors)."""
+    V = 8 if prec == 0 else 4
+    if op == 0:
+        return nnz * (4 + V) + 4 * (n + 1) + 2 * n * V
+    if op in (2, 6):
+        return nnz * (4 + V) + 4 * (n + 1) + 4 * n * V
+    if op == 3:
+        return nnzp * (4 + V) + 4 * (nc + 1) + n * V + nc * V
+    if op == 4:
+        return nnzp * (4 + V) + 4 * (n + 1) + nc * V + 2 * n * V
+    raise ValueError(op)
+
+
+def level_table(h, reps=20, precisions=(0, 1), ops=(2, 6, 3, 4)):
+    peak, _ = peaks()
+    rows = []
+    for l in range(h.nlevels):
+        info = h.level_info(l)
+        n, nnz, nc, nnzp, G = (int(info[0]), int(info[1]), int(info[2]), int(info[3]), int(info[7]))
+        for prec in precisions:
+            for op in ops:
+                ms = h.time_level_op(l, op, prec, reps=reps)
+                byts = op_bytes(op, prec, n, nnz, nc, nnzp)
+                rows.append({"level": l + 1, "op": OPS[op], "prec": "fp64" if prec == 0 else "fp32",
+                             "rows": n, "nnz": nnz, "nnzP": nnzp, "lanes": G, "us": round(ms * 1e3, 2),
+                             "GBps": round(byts / (ms * 1e-3) / 1e9, 1),
+                             "frac": round(byts / (ms * 1e-3) / 1e9 / peak, 3)})
+    return rows
+
+
 def run_kernel_only(args):
     import torch
 
@@ -380,6 +417,8 @@ def run_kernel_only(args):
     torch.cuda.set_device(0)
     A, b, cfg = workload(args.n, args.seed)
     h = draugr.amg_setup(A, cfg)
+    if args.level < 0:
+        return {"kernel_only": True, "levels": level_table(h, reps=max(args.reps, 10))}
     ms = h.time_level_op(args.level, args.op, args.precision, reps=args.reps)
     info = h.level_info(args.level)
     return {"kernel_only": True, "level": args.level, "op": args.op, "precision": args.precision,

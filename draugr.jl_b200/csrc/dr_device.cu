@@ -357,7 +357,7 @@ void DevHier::refresh_fp32() {
 
 // ------------------------------------------------------------ cycle pieces
 template <typename T>
-T* DevHier::smooth(int l, T* x, const T* b, int steps, T* ext) {
+T* DevHier::smooth(int l, T* x, const T* b, int steps, T* ext, const double* rz_w, bool rz_first) {
   DevLevel& L = L_[l];
   LevelVecs<T>& V = vecs<T>(l);
   const DevMat& A = L.A;
@@ -365,8 +365,18 @@ T* DevHier::smooth(int l, T* x, const T* b, int steps, T* ext) {
   if (L.smoother == SmootherKind::Jacobi || L.smoother == SmootherKind::L1Jacobi) {
     for (int s = 0; s < steps; ++s) {
       T* dst = (l == 0) ? (x == V.xb ? ext : V.xb) : (x == V.xa ? V.xb : V.xa);
-      launch_rows(st_, max_grid_, A, mval<T>(A), XPlain<T>{x},
-                  EpJacobi<T>{x, b, invd<T>(L), dst, om, nullptr});
+      if (rz_w && s == steps - 1) {
+        EpJacobi<T> ep{x, b, invd<T>(L), dst, om, rz_w};
+        if (rz_first)
+          launch_rows_dot(st_, max_grid_, A, mval<T>(A), XPlain<T>{x}, ep, partials_,
+                          tickets_ + TK_RZ, FinStore2{scal_ + SC_RZ, scal_ + SC_RZOLD});
+        else
+          launch_rows_dot(st_, max_grid_, A, mval<T>(A), XPlain<T>{x}, ep, partials_,
+                          tickets_ + TK_RZ, FinShift{scal_ + SC_RZ, scal_ + SC_RZOLD});
+      } else {
+        launch_rows(st_, max_grid_, A, mval<T>(A), XPlain<T>{x},
+                    EpJacobi<T>{x, b, invd<T>(L), dst, om, nullptr});
+      }
       x = dst;
     }
   } else {
@@ -406,13 +416,23 @@ template <typename T>
 void DevHier::coarse_solve(const T* b, T* x) {
   int threads = 32;
   while (threads < nc_ && threads < 1024) threads *= 2;
+  // stage the factors in shared memory when they fit in 40 KB (n_c <= 70)
+  const size_t ybytes = (size_t)((std::max(nc_, 1) + 1) & ~1) * sizeof(double);
+  const size_t lbytes = (size_t)nc_ * nc_ * sizeof(double);
+  const int staged = (ybytes + lbytes) <= 40 * 1024 ? 1 : 0;
   counted();
-  k_lu_solve<T><<<1, threads, (size_t)std::max(nc_, 1) * sizeof(double), st_>>>(nc_, clu_, cpiv_, b, x);
+  k_lu_solve<T><<<1, threads, ybytes + (staged ? lbytes : 0), st_>>>(nc_, clu_, cpiv_, b, x, staged);
   DR_CK(cudaGetLastError());
 }
 
+bool DevHier::fused_rz_ok(const CycleOpts& o) const {
+  return !L_.empty() && o.post >= 1 &&
+         (L_[0].smoother == SmootherKind::Jacobi || L_[0].smoother == SmootherKind::L1Jacobi);
+}
+
 template <typename T>
-T* DevHier::cycle_level(int l, T* x, const T* b, bool x_zero, const CycleOpts& o, T* ext) {
+T* DevHier::cycle_level(int l, T* x, const T* b, bool x_zero, const CycleOpts& o, T* ext,
+                        const double* rz_w, bool rz_first) {
   DevLevel& L = L_[l];
   LevelVecs<T>& V = vecs<T>(l);
   const DevMat& A = L.A;
@@ -457,7 +477,7 @@ T* DevHier::cycle_level(int l, T* x, const T* b, bool x_zero, const CycleOpts& o
   // prolongation and correction  x += P xc
   launch_rows(st_, max_grid_, L.P, mval<T>(L.P), XPlain<T>{xn}, EpAddTo<T>{x});
   // post-smoothing
-  x = smooth<T>(l, x, b, o.post, ext);
+  x = smooth<T>(l, x, b, o.post, ext, rz_w, rz_first);
   return x;
 }
 
@@ -576,6 +596,7 @@ int DevHier::pcg(double* x, const double* b, const CycleOpts& o, double tol, int
   // z = M r (the cycle writes where it ends; the location is the same for
   // every application with the same options)
   void* zptr = nullptr;
+  const bool fuse_rz = fused_rz_ok(o);
   auto precond = [&](bool rz_first) {
     if (mixed) {
       if (L_.empty()) {
@@ -584,29 +605,33 @@ int DevHier::pcg(double* x, const double* b, const CycleOpts& o, double tol, int
         coarse_solve<float>(pr32_, pz32_);
         zptr = pz32_;
       } else {
-        zptr = cycle_level<float>(0, pz32_, pr32_, true, o, pz32_);
+        zptr = cycle_level<float>(0, pz32_, pr32_, true, o, pz32_, fuse_rz ? pr_ : nullptr, rz_first);
       }
-      counted();
-      if (rz_first)
-        k_dot<double, float, FinStore2><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(
-            n, pr_, (const float*)zptr, partials_, tickets_ + TK_RZ, FinStore2{scal_ + SC_RZ, scal_ + SC_RZOLD});
-      else
-        k_dot<double, float, FinShift><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(
-            n, pr_, (const float*)zptr, partials_, tickets_ + TK_RZ, FinShift{scal_ + SC_RZ, scal_ + SC_RZOLD});
+      if (!fuse_rz) {
+        counted();
+        if (rz_first)
+          k_dot<double, float, FinStore2><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(
+              n, pr_, (const float*)zptr, partials_, tickets_ + TK_RZ, FinStore2{scal_ + SC_RZ, scal_ + SC_RZOLD});
+        else
+          k_dot<double, float, FinShift><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(
+              n, pr_, (const float*)zptr, partials_, tickets_ + TK_RZ, FinShift{scal_ + SC_RZ, scal_ + SC_RZOLD});
+      }
     } else {
       if (L_.empty()) {
         coarse_solve<double>(pr_, pz_);
         zptr = pz_;
       } else {
-        zptr = cycle_level<double>(0, pz_, pr_, true, o, pz_);
+        zptr = cycle_level<double>(0, pz_, pr_, true, o, pz_, fuse_rz ? pr_ : nullptr, rz_first);
       }
-      counted();
-      if (rz_first)
-        k_dot<double, double, FinStore2><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(
-            n, pr_, (const double*)zptr, partials_, tickets_ + TK_RZ, FinStore2{scal_ + SC_RZ, scal_ + SC_RZOLD});
-      else
-        k_dot<double, double, FinShift><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(
-            n, pr_, (const double*)zptr, partials_, tickets_ + TK_RZ, FinShift{scal_ + SC_RZ, scal_ + SC_RZOLD});
+      if (!fuse_rz) {
+        counted();
+        if (rz_first)
+          k_dot<double, double, FinStore2><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(
+              n, pr_, (const double*)zptr, partials_, tickets_ + TK_RZ, FinStore2{scal_ + SC_RZ, scal_ + SC_RZOLD});
+        else
+          k_dot<double, double, FinShift><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(
+              n, pr_, (const double*)zptr, partials_, tickets_ + TK_RZ, FinShift{scal_ + SC_RZ, scal_ + SC_RZOLD});
+      }
     }
     DR_CK(cudaGetLastError());
   };
@@ -622,7 +647,7 @@ int DevHier::pcg(double* x, const double* b, const CycleOpts& o, double tol, int
     double* pold = pp_[par];
     double* pnew = pp_[par ^ 1];
     if (mixed) {
-      XPcgDir<float> dir{(const float*)zptr, pold, scal_ + SC_RZ, 0};
+      XPcgDir<float> dir{(const float*)zptr, pold, scal_ + SC_RZ, 0.0};
       launch_rows_dot(st_, max_grid_, A, A.v, dir, EpPcgDir<float>{dir, pnew, pq_}, partials_,
                       tickets_ + TK_PQ, FinStore{scal_ + SC_PQ});
       counted();
@@ -630,7 +655,7 @@ int DevHier::pcg(double* x, const double* b, const CycleOpts& o, double tol, int
                                                                     scal_ + SC_PQ, pr32_, partials_,
                                                                     tickets_ + TK_UPD, FinStore{scal_ + SC_RR});
     } else {
-      XPcgDir<double> dir{(const double*)zptr, pold, scal_ + SC_RZ, 0};
+      XPcgDir<double> dir{(const double*)zptr, pold, scal_ + SC_RZ, 0.0};
       launch_rows_dot(st_, max_grid_, A, A.v, dir, EpPcgDir<double>{dir, pnew, pq_}, partials_,
                       tickets_ + TK_PQ, FinStore{scal_ + SC_PQ});
       counted();
@@ -862,6 +887,7 @@ void DevHier::level_op(int lvl, int op, bool fp32, const double* in1, const doub
 
 float DevHier::time_level_op(int lvl, int op, bool fp32, int reps) {
   if (lvl < 0 || lvl >= nlevels()) fail("level index out of range");
+  if (op != 0 && op != 2 && op != 3 && op != 4 && op != 6) fail("time_level_op: op must be 0, 2, 3, 4 or 6");
   if (fp32) ensure_fp32();
   cudaEvent_t e0, e1;
   DR_CK(cudaEventCreate(&e0));
@@ -871,22 +897,40 @@ float DevHier::time_level_op(int lvl, int op, bool fp32, int reps) {
     using T = decltype(tag);
     DevLevel& L = L_[lvl];
     LevelVecs<T>& V = vecs<T>(lvl);
-    const int n = L.A.n;
-    T* x0 = lvl > 0 ? V.xa : V.r;
+    const bool last = lvl + 1 == nlevels();
+    const int n = L.A.n, nc = L.P.m;
+    T* x0 = V.r;                                   // operand vectors of this level
     T* x1 = V.xb;
-    T* b = lvl > 0 ? V.b : V.r;
+    T* cvec = last ? coarse_b<T>() : vecs<T>(lvl + 1).b;   // coarse-size vector
+    if (!tout_) tout_ = alloc<double>(n0_);       // scratch output (second result of op 6)
+    T* x2 = reinterpret_cast<T*>(tout_);
     counted();
     k_fill<T><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, T(1), x0);
-    if (lvl > 0) {
-      counted();
-      k_fill<T><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, T(1), b);
-    }
+    counted();
+    k_fill<T><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, T(1), x1);
+    counted();
+    k_fill<T><<<grid1d(nc, max_grid_), kBlock, 0, st_>>>(nc, T(1), cvec);
     const T om = (T)L.omega;
     auto once = [&]() {
-      if (op == 2)
-        launch_rows(st_, max_grid_, L.A, mval<T>(L.A), XPlain<T>{x0}, EpJacobi<T>{x0, b, invd<T>(L), x1, om, nullptr});
-      else
-        launch_rows(st_, max_grid_, L.A, mval<T>(L.A), XPlain<T>{x0}, EpStore<T>{x1});
+      switch (op) {
+        case 0:
+          launch_rows(st_, max_grid_, L.A, mval<T>(L.A), XPlain<T>{x0}, EpStore<T>{x1});
+          break;
+        case 2:
+          launch_rows(st_, max_grid_, L.A, mval<T>(L.A), XPlain<T>{x0},
+                      EpJacobi<T>{x0, x0, invd<T>(L), x1, om, nullptr});
+          break;
+        case 3:
+          launch_rows(st_, max_grid_, L.R, mval<T>(L.R), XPlain<T>{x0}, EpStore<T>{cvec});
+          break;
+        case 4:
+          launch_rows(st_, max_grid_, L.P, mval<T>(L.P), XPlain<T>{cvec}, EpAddTo<T>{x1});
+          break;
+        case 6:
+          launch_rows(st_, max_grid_, L.A, mval<T>(L.A), XZeroJacobi<T>{x0, invd<T>(L), om},
+                      EpZeroJacobiResidual<T>{x0, invd<T>(L), x1, x2, om});
+          break;
+      }
     };
     for (int w = 0; w < 3; ++w) once();
     DR_CK(cudaEventRecord(e0, st_));
@@ -899,6 +943,7 @@ float DevHier::time_level_op(int lvl, int op, bool fp32, int reps) {
   else run(double());
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  check_kernel_flag(st_);
   return ms / reps;
 }
 

@@ -126,10 +126,16 @@ class DevHier {
   template <typename T> const T* mval(const DevMat& M) const;
   template <typename T> const T* invd(const DevLevel& L) const;
 
+  // rz_w: when set (finest level only), the last Jacobi sweep also forms
+  // r·z with r = rz_w and stores it like the PCG's r·z (rz_first: first
+  // application, else shift the previous value to "old").
   template <typename T>
-  T* cycle_level(int l, T* x, const T* b, bool x_zero, const CycleOpts& o, T* ext_partner);
+  T* cycle_level(int l, T* x, const T* b, bool x_zero, const CycleOpts& o, T* ext_partner,
+                 const double* rz_w = nullptr, bool rz_first = false);
   template <typename T>
-  T* smooth(int l, T* x, const T* b, int steps, T* ext_partner);
+  T* smooth(int l, T* x, const T* b, int steps, T* ext_partner, const double* rz_w = nullptr,
+            bool rz_first = false);
+  bool fused_rz_ok(const CycleOpts& o) const;
   template <typename T>
   void residual(int l, const T* x, const T* b, T* r, double* rr_dst);
   template <typename T>

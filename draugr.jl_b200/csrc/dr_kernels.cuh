@@ -99,20 +99,24 @@ struct XZeroJacobi {
   __device__ __forceinline__ T operator()(int j) const;
 };
 
-// PCG search direction on the fly: p_j = z_j + β·p_old_j.
+// PCG search direction on the fly: p_j = z_j + β·p_old_j, with
+// β = rz / rz_old read from device memory once per thread (bind()).
 template <typename TZ>
 struct XPcgDir {
   const TZ* __restrict__ z;
   const double* __restrict__ pold;
   const double* __restrict__ scal;  // [rz, rz_old]
-  int first;
+  double beta;
+  __device__ __forceinline__ void bind() { beta = __ldg(scal) / __ldg(scal + 1); }
   __device__ __forceinline__ double operator()(int j) const {
-    double zj = (double)__ldg(z + j);
-    if (first) return zj;
-    double beta = __ldg(scal) / __ldg(scal + 1);
-    return zj + beta * __ldg(pold + j);
+    return (double)__ldg(z + j) + beta * __ldg(pold + j);
   }
 };
+// Loaders without per-launch state.
+template <class XL>
+__device__ __forceinline__ void bind_loader(XL&) {}
+template <typename TZ>
+__device__ __forceinline__ void bind_loader(XPcgDir<TZ>& x) { x.bind(); }
 
 // ------------------------------------------------------------ rounding
 // Products and sums rounded separately (no contraction into FMA), as the
@@ -225,6 +229,7 @@ struct EpPcgDir {  // q = A p, p_new = z + β p_old, returns p_new·q
   XPcgDir<T> dir;
   double* __restrict__ pnew;
   double* __restrict__ q;
+  __device__ __forceinline__ void bind() { dir.bind(); }
   __device__ __forceinline__ Pre pre(int i) const { return {dir(i)}; }
   __device__ __forceinline__ double init(const Pre&) const { return 0.0; }
   __device__ __forceinline__ double apply(int i, double s, const Pre& pr) const {
@@ -305,6 +310,11 @@ constexpr size_t tile_smem_bytes() {
   return 2 * (size_t)kStageEntries * (sizeof(int) + sizeof(TA));
 }
 
+template <class EP>
+__device__ __forceinline__ void bind_epilogue(EP&) {}
+template <typename T>
+__device__ __forceinline__ void bind_epilogue(EpPcgDir<T>& e) { e.bind(); }
+
 template <int G, typename TA, class XL, class EP, bool DOT, class Fin>
 __global__ void __launch_bounds__(kBlock)
 k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
@@ -312,6 +322,8 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
             XL xl, EP ep, double* partials, unsigned* ticket, Fin fin, int* err) {
   using acc_t = typename EP::acc_t;
   using Pre = typename EP::Pre;
+  bind_loader(xl);
+  bind_epilogue(ep);
   extern __shared__ __align__(128) unsigned char smem_raw[];
   // stage b: values at sv0 + b*kStageEntries, columns at sc0 + b*kStageEntries
   TA* const sv0 = reinterpret_cast<TA*>(smem_raw);
@@ -533,8 +545,15 @@ k_pcg_update(int n, double* __restrict__ x, double* __restrict__ r, const double
 // bit.  Input and output in T, arithmetic in double.
 template <typename T>
 __global__ void k_lu_solve(int n, const double* __restrict__ lu, const int* __restrict__ piv,
-                           const T* __restrict__ bin, T* __restrict__ xout) {
-  extern __shared__ double y[];
+                           const T* __restrict__ bin, T* __restrict__ xout, int lu_in_smem) {
+  extern __shared__ double sh[];
+  double* y = sh;                            // n
+  const double* a = lu;                      // factors (global or staged)
+  if (lu_in_smem) {
+    double* s = sh + ((n + 1) & ~1);
+    for (int t = threadIdx.x; t < n * n; t += blockDim.x) s[t] = lu[t];
+    a = s;
+  }
   for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = (double)bin[i];
   __syncthreads();
   if (threadIdx.x == 0)
@@ -551,16 +570,16 @@ __global__ void k_lu_solve(int n, const double* __restrict__ lu, const int* __re
     const double yj = y[j];
     if (yj != 0.0)
       for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x)
-        y[i] = __dsub_rn(y[i], __dmul_rn(yj, lu[(size_t)j * n + i]));
+        y[i] = __dsub_rn(y[i], __dmul_rn(yj, a[(size_t)j * n + i]));
     __syncthreads();
   }
   for (int j = n - 1; j >= 0; --j) {
-    if (threadIdx.x == 0 && y[j] != 0.0) y[j] = __ddiv_rn(y[j], lu[(size_t)j * n + j]);
+    if (threadIdx.x == 0 && y[j] != 0.0) y[j] = __ddiv_rn(y[j], a[(size_t)j * n + j]);
     __syncthreads();
     const double yj = y[j];
     if (yj != 0.0)
       for (int i = threadIdx.x; i < j; i += blockDim.x)
-        y[i] = __dsub_rn(y[i], __dmul_rn(yj, lu[(size_t)j * n + i]));
+        y[i] = __dsub_rn(y[i], __dmul_rn(yj, a[(size_t)j * n + i]));
     __syncthreads();
   }
   for (int i = threadIdx.x; i < n; i += blockDim.x) xout[i] = (T)y[i];
