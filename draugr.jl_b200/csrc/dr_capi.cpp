@@ -312,9 +312,9 @@ int32_t draugr_b200_level_info(int32_t handle, int32_t lvl, int64_t* info) {
     info[4] = (int64_t)L.smoother;
     info[5] = L.num_colors;
     info[6] = L.has_rap_map ? (int64_t)L.ap_ci.size() : -1;
-    info[7] = tile_lanes(L.A.nnz(), L.A.n);
-    info[8] = tile_lanes(L.P.nnz(), L.P.nf);
-    info[9] = tile_lanes(L.P.nnz(), L.P.nc);
+    info[7] = rows_in_order(L.A.rp);
+    info[8] = rows_in_order(L.P.rp);
+    info[9] = rows_in_order(L.T.off);
     return 0;
   });
 }

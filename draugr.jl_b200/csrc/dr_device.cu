@@ -60,13 +60,13 @@ int pick_G(long long nnz, int n) {
   return G;
 }
 
-// Greedy packing of consecutive rows into tiles of at most kBlock/G rows and
+// Greedy packing of consecutive rows into tiles of at most kBlock rows and
 // kTileCap nonzeros; a row longer than kTileCap is a tile of its own.
-std::vector<int> make_tiles(const std::vector<int>& rp, int n, int G) {
+std::vector<int> make_tiles(const std::vector<int>& rp, int n) {
   std::vector<int> tp;
-  tp.reserve(n / std::max(1, kBlock / G) + 2);
+  tp.reserve(n / kBlock + 2);
   tp.push_back(0);
-  const int max_rows = kBlock / G;
+  const int max_rows = kBlock;
   int r = 0;
   while (r < n) {
     int rows = 0, nz = 0;
@@ -83,8 +83,10 @@ std::vector<int> make_tiles(const std::vector<int>& rp, int n, int G) {
   return tp;
 }
 
+static_assert(kTileCap == kRowTileCap, "host and device tile capacities differ");
+
 template <typename TA, class XL, class EP, bool DOT, class Fin>
-void launch_rows_impl(cudaStream_t st, int max_grid, int G, int n, int ntiles, const int* tp,
+void launch_rows_impl(cudaStream_t st, int max_grid, int n, int ntiles, const int* tp,
                       const int* ts, const int* rp, const int* ci, const TA* av, XL xl, EP ep,
                       double* partials, unsigned* ticket, Fin fin) {
   if (n <= 0) {
@@ -100,30 +102,21 @@ void launch_rows_impl(cudaStream_t st, int max_grid, int G, int n, int ntiles, c
   const int grid = std::max(1, std::min({ntiles, max_grid, g_nsm * per_sm}));
   const size_t smem = tile_smem_bytes<TA>();
   counted();
-  switch (G) {
-#define DR_CASE(g)                                                                                 \
-  case g:                                                                                          \
-    k_tile_rows<g, TA, XL, EP, DOT, Fin><<<grid, kBlock, smem, st>>>(ntiles, tp, ts, rp, ci, av, xl, \
-                                                                     ep, partials, ticket, fin,    \
-                                                                     g_err);                       \
-    break;
-    DR_CASE(1) DR_CASE(2) DR_CASE(4) DR_CASE(8) DR_CASE(16) DR_CASE(32)
-#undef DR_CASE
-    default: fail("bad lanes-per-row");
-  }
+  k_tile_rows<TA, XL, EP, DOT, Fin><<<grid, kBlock, smem, st>>>(ntiles, tp, ts, rp, ci, av, xl, ep,
+                                                                partials, ticket, fin, g_err);
   DR_CK(cudaGetLastError());
 }
 
 template <typename TA, class XL, class EP>
 void launch_rows(cudaStream_t st, int max_grid, const DevMat& M, const TA* av, XL xl, EP ep) {
-  launch_rows_impl<TA, XL, EP, false, FinStore>(st, max_grid, M.G, M.n, M.ntiles, M.tp, M.ts, M.rp, M.ci,
+  launch_rows_impl<TA, XL, EP, false, FinStore>(st, max_grid, M.n, M.ntiles, M.tp, M.ts, M.rp, M.ci,
                                                 av, xl, ep, nullptr, nullptr, FinStore{nullptr});
 }
 
 template <typename TA, class XL, class EP, class Fin>
 void launch_rows_dot(cudaStream_t st, int max_grid, const DevMat& M, const TA* av, XL xl, EP ep,
                      double* partials, unsigned* ticket, Fin fin) {
-  launch_rows_impl<TA, XL, EP, true, Fin>(st, max_grid, M.G, M.n, M.ntiles, M.tp, M.ts, M.rp, M.ci, av,
+  launch_rows_impl<TA, XL, EP, true, Fin>(st, max_grid, M.n, M.ntiles, M.tp, M.ts, M.rp, M.ci, av,
                                           xl, ep, partials, ticket, fin);
 }
 
@@ -196,9 +189,8 @@ DevHier::DevHier(const HostHierarchy& H, int device) {
       h2d(M.ci, ci, st_);
       M.v = alloc<double>(ci.size() + 4);
       if (v) h2d(M.v, *v, st_);
-      M.G = tile_lanes(M.nnz, n);
       M.Ggs = pick_G(M.nnz, n);
-      std::vector<int> tiles = make_tiles(rp, n, M.G);
+      std::vector<int> tiles = make_tiles(rp, n);
       std::vector<int> tstart(tiles.size());
       for (size_t t = 0; t < tiles.size(); ++t) tstart[t] = rp[tiles[t]];
       M.ntiles = (int)tiles.size() - 1;

@@ -11,25 +11,25 @@
 namespace dr {
 
 void cuda_check(cudaError_t e, const char* what, const char* file, int line);
-
-// Lanes per row in the row phase of the tile kernel.  Rows of up to 32
-// entries get one lane, which sums the staged products in column order (the
-// reference's order, so those rows are reproduced bit for bit); longer rows
-// get a power of two of lanes with about 8 products each.
-inline int tile_lanes(long long nnz, int n) {
-  if (n <= 0) return 1;
-  const double avg = (double)nnz / (double)n;
-  if (avg <= 32.0) return 1;
-  int G = 2;
-  while (G < 32 && G * 8 < avg) G *= 2;
-  return G;
-}
 long long kernel_launches();
 #define DR_CK(x) ::dr::cuda_check((x), #x, __FILE__, __LINE__)
 
+// Nonzeros per tile of the row kernel (k_tile_rows); rows longer than this
+// are reduced by a whole block in a fixed tree order instead of in column
+// order.
+constexpr int kRowTileCap = 2000;
+
+// 1 when every row of the CSR pattern is reduced in column order (the
+// reference's order, bit for bit), 0 if some row exceeds the tile capacity.
+inline int rows_in_order(const std::vector<int>& rp) {
+  for (size_t i = 0; i + 1 < rp.size(); ++i)
+    if (rp[i + 1] - rp[i] > kRowTileCap) return 0;
+  return 1;
+}
+
 // Sparse matrix on the device: CSR pattern, FP64 values and (after the first
-// mixed-precision use) an FP32 copy of the values.  G = lanes per row used by
-// the row kernels.
+// mixed-precision use) an FP32 copy of the values, plus the row tiling of
+// the row kernel.
 struct DevMat {
   int n = 0, m = 0;
   long long nnz = 0;
@@ -37,7 +37,6 @@ struct DevMat {
   int* ci = nullptr;
   double* v = nullptr;
   float* v32 = nullptr;
-  int G = 1;          // lanes per row in the row phase of k_tile_rows
   int Ggs = 8;        // lanes per row of the Gauss-Seidel colour kernel
   int ntiles = 0;     // row tiles (see k_tile_rows)
   int* tp = nullptr;  // tile row starts, ntiles+1

@@ -287,19 +287,25 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 
 // ------------------------------------------------------------ row kernel
 // Rows are packed (on the host, once per matrix) into tiles of at most
-// kBlock/G consecutive rows holding at most kTileCap nonzeros; tp[t] is the
+// kBlock consecutive rows holding at most kTileCap nonzeros; tp[t] is the
 // first row and ts[t] the first nonzero of tile t.  Each block walks the
 // tiles blockIdx.x, +gridDim.x, ... with two shared-memory stages: while it
-// reduces the rows of one tile, the TMA engine copies the column and value
-// arrays of the tile after next into the other stage (cp.async.bulk with an
-// mbarrier), so HBM streaming never waits on the SM.  The row phase reads
-// columns and values from shared memory, gathers x (an L2-resident vector)
-// and applies the fused epilogue, whose own operands are loaded before the
-// gathers.  The column / value arrays carry 4 padding entries so the
-// 16-byte-rounded copies stay in bounds.  A row longer than kTileCap forms a
-// tile of its own and is read straight from global memory by the whole block.
+// works on one tile, the TMA engine copies the column and value arrays of
+// the tile after next into the other stage (cp.async.bulk completing on an
+// mbarrier), so HBM streaming never waits on the SM.  Per tile:
+//   1. products: the block walks the tile's nonzeros flat (thread t takes
+//      entries t, t+256, ...), gathers x (an L2-resident vector) for up to
+//      eight entries at once and overwrites each staged value with a_ij·x_j;
+//   2. rows: thread t sums the products of row t of the tile in column order
+//      (the reference's order, products and sums rounded separately, so
+//      every row is reproduced bit for bit) and applies the fused epilogue,
+//      whose operands were loaded before waiting for the stage.
+// The column / value arrays carry 4 padding entries so the 16-byte-rounded
+// copies stay in bounds.  A row longer than kTileCap forms a tile of its own
+// and is reduced by the whole block straight from global memory.
 constexpr int kTileCap = 2000;
 constexpr int kStageEntries = 2008;  // kTileCap + alignment slack, a multiple of 4 entries
+constexpr int kProdIters = (kTileCap + kBlock - 1) / kBlock;
 constexpr int kWaitLimit = 1 << 22;
 
 // Dynamic shared memory of k_tile_rows: two stages of columns and values
@@ -315,12 +321,13 @@ __device__ __forceinline__ void bind_epilogue(EP&) {}
 template <typename T>
 __device__ __forceinline__ void bind_epilogue(EpPcgDir<T>& e) { e.bind(); }
 
-template <int G, typename TA, class XL, class EP, bool DOT, class Fin>
+template <typename TA, class XL, class EP, bool DOT, class Fin>
 __global__ void __launch_bounds__(kBlock)
 k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
             const int* __restrict__ rp, const int* __restrict__ ci, const TA* __restrict__ av,
             XL xl, EP ep, double* partials, unsigned* ticket, Fin fin, int* err) {
   using acc_t = typename EP::acc_t;
+  static_assert(sizeof(acc_t) == sizeof(TA), "products are stored over the staged values");
   using Pre = typename EP::Pre;
   bind_loader(xl);
   bind_epilogue(ep);
@@ -330,9 +337,6 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
   int* const sc0 = reinterpret_cast<int*>(sv0 + 2 * kStageEntries);
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ acc_t red[32];
-
-  const int lane = threadIdx.x & (G - 1);
-  const int grp = threadIdx.x / G;
   const int stride = gridDim.x;
 
   auto issue = [&](int t, int b) {  // thread 0 only
@@ -369,15 +373,15 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
     const int r0 = __ldg(tp + t), r1 = __ldg(tp + t + 1);
     const int s = __ldg(ts + t), e = __ldg(ts + t + 1);
     const int len = e - s;
-    // row bounds and epilogue operands, issued before waiting for the stage
-    const int row = r0 + grp;
+    // this thread's row: bounds and epilogue operands, before the wait
+    const int row = r0 + (int)threadIdx.x;
     const bool valid = (len <= kTileCap) && row < r1;
     int rs = 0, re = 0;
     Pre pr{};
     if (valid) {
       rs = __ldg(rp + row) - s;
       re = __ldg(rp + row + 1) - s;
-      if (lane == 0) pr = ep.pre(row);
+      pr = ep.pre(row);
     }
     if (!mbar_wait_bounded(bar + b, parity, kWaitLimit)) {
       if (threadIdx.x == 0) atomicExch(err, 1);
@@ -385,45 +389,29 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
     }
     if (len <= kTileCap) {
       const int off = s - (s & ~3);
+      TA* vs = sv0 + b * kStageEntries + off;
       const int* cs = sc0 + b * kStageEntries + off;
-      const TA* vs = sv0 + b * kStageEntries + off;
-      if constexpr (G == 1) {
-        if (valid) {
-          acc_t a = ep.init(pr);
-          for (int k0 = rs; k0 < re; k0 += 8) {
-            acc_t p[8];
+      // 1. products, flat over the tile
+      acc_t p[kProdIters];
 #pragma unroll
-            for (int j = 0; j < 8; ++j)
-              p[j] = (k0 + j < re) ? mul_rn((acc_t)vs[k0 + j], (acc_t)xl(cs[k0 + j])) : acc_t(0);
+      for (int j = 0; j < kProdIters; ++j) {
+        const int k = threadIdx.x + j * kBlock;
+        p[j] = (k < len) ? (acc_t)xl(cs[k]) : acc_t(0);
+      }
 #pragma unroll
-            for (int j = 0; j < 8; ++j)
-              if (k0 + j < re) {
-                if constexpr (EP::kSign > 0) a = add_rn(a, p[j]);
-                else a = sub_rn(a, p[j]);
-              }
-          }
-          dacc += ep.apply(row, a, pr);
+      for (int j = 0; j < kProdIters; ++j) {
+        const int k = threadIdx.x + j * kBlock;
+        if (k < len) vs[k] = (TA)mul_rn((acc_t)vs[k], p[j]);
+      }
+      __syncthreads();
+      // 2. rows, in column order
+      if (valid) {
+        acc_t a = ep.init(pr);
+        for (int k = rs; k < re; ++k) {
+          if constexpr (EP::kSign > 0) a = add_rn(a, (acc_t)vs[k]);
+          else a = sub_rn(a, (acc_t)vs[k]);
         }
-      } else {
-        acc_t sum = acc_t(0);
-        for (int k0 = rs + lane; k0 < re; k0 += 4 * G) {
-          acc_t p[4];
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const int k = k0 + j * G;
-            p[j] = (k < re) ? mul_rn((acc_t)vs[k], (acc_t)xl(cs[k])) : acc_t(0);
-          }
-#pragma unroll
-          for (int j = 0; j < 4; ++j) sum = add_rn(sum, p[j]);
-        }
-#pragma unroll
-        for (int o = G >> 1; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-        if (valid && lane == 0) {
-          acc_t a = ep.init(pr);
-          if constexpr (EP::kSign > 0) a = add_rn(a, sum);
-          else a = sub_rn(a, sum);
-          dacc += ep.apply(row, a, pr);
-        }
+        dacc += ep.apply(row, a, pr);
       }
     } else {
       // a single row longer than the tile capacity, from global memory

@@ -28,8 +28,9 @@ int32_t draugr_b200_num_levels(int32_t handle);
 
 /* Sizes of level lvl (0-based): info[0] n, [1] nnz(A), [2] n_coarse,
  * [3] nnz(P), [4] smoother kind, [5] colours, [6] nnz(A*P) or -1,
- * [7] [8] [9] lanes per row of the row kernels for A, P and Pᵀ (1 = rows
- * reduced sequentially in column order).  info must hold 10 values.
+ * [7] [8] [9] 1 if every row of A, P and Pᵀ is reduced by the row kernel
+ * in column order (the reference's summation order), 0 if some row is
+ * longer than the kernel's tile capacity.  info must hold 10 values.
  * lvl = -1: the coarsest level, info[0] n_c, [1] nnz of its CSR. */
 int32_t draugr_b200_level_info(int32_t handle, int32_t lvl, int64_t *info);
 

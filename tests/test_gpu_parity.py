@@ -203,6 +203,7 @@ def fresh_case(request):
 
 
 def _single_lane(h, l):
+    """(A, P, Pᵀ) rows all reduced in column order by the row kernel."""
     info = h.level_info(l)
     return int(info[7]) == 1, int(info[8]) == 1, int(info[9]) == 1
 
