@@ -60,13 +60,13 @@ int pick_G(long long nnz, int n) {
   return G;
 }
 
-// Greedy packing of consecutive rows into tiles of at most kBlock rows and
-// kTileCap nonzeros; a row longer than kTileCap is a tile of its own.
-std::vector<int> make_tiles(const std::vector<int>& rp, int n) {
+// Greedy packing of consecutive rows into tiles of at most kBlock/G rows
+// and kTileCap nonzeros; a row longer than kTileCap is a tile of its own.
+std::vector<int> make_tiles(const std::vector<int>& rp, int n, int G) {
   std::vector<int> tp;
-  tp.reserve(n / kBlock + 2);
+  tp.reserve(n / std::max(1, kBlock / G) + 2);
   tp.push_back(0);
-  const int max_rows = kBlock;
+  const int max_rows = kBlock / G;
   int r = 0;
   while (r < n) {
     int rows = 0, nz = 0;
@@ -85,10 +85,29 @@ std::vector<int> make_tiles(const std::vector<int>& rp, int n) {
 
 static_assert(kTileCap == kRowTileCap, "host and device tile capacities differ");
 
+// Form of the row kernel for a CSR pattern: flat products when row lengths
+// are very uneven (a long row among short ones), otherwise G lanes per row
+// with about six entries per lane (one lane up to 8 entries per row).
+void choose_row_form(const std::vector<int>& rp, int n, long long nnz, int& G, bool& flat) {
+  G = 1;
+  flat = false;
+  if (n <= 0) return;
+  int maxlen = 0;
+  for (int i = 0; i < n; ++i) maxlen = std::max(maxlen, rp[i + 1] - rp[i]);
+  const double avg = (double)nnz / (double)n;
+  if (maxlen > 64 && maxlen > 4.0 * avg) {
+    flat = true;
+    return;
+  }
+  if (avg <= 8.0) return;
+  G = 2;
+  while (G < 32 && G * 6 < avg) G *= 2;
+}
+
 template <typename TA, class XL, class EP, bool DOT, class Fin>
-void launch_rows_impl(cudaStream_t st, int max_grid, int n, int ntiles, const int* tp,
-                      const int* ts, const int* rp, const int* ci, const TA* av, XL xl, EP ep,
-                      double* partials, unsigned* ticket, Fin fin) {
+void launch_rows_impl(cudaStream_t st, int max_grid, int G, bool flat, int n, int ntiles,
+                      const int* tp, const int* ts, const int* rp, const int* ci, const TA* av,
+                      XL xl, EP ep, double* partials, unsigned* ticket, Fin fin) {
   if (n <= 0) {
     if constexpr (DOT) {
       // an empty reduction still has to deliver its (zero) result
@@ -102,22 +121,39 @@ void launch_rows_impl(cudaStream_t st, int max_grid, int n, int ntiles, const in
   const int grid = std::max(1, std::min({ntiles, max_grid, g_nsm * per_sm}));
   const size_t smem = tile_smem_bytes<TA>();
   counted();
-  k_tile_rows<TA, XL, EP, DOT, Fin><<<grid, kBlock, smem, st>>>(ntiles, tp, ts, rp, ci, av, xl, ep,
-                                                                partials, ticket, fin, g_err);
+#define DR_LAUNCH(F, g)                                                                          \
+  k_tile_rows<F, g, TA, XL, EP, DOT, Fin><<<grid, kBlock, smem, st>>>(ntiles, tp, ts, rp, ci, av, xl, \
+                                                                      ep, partials, ticket, fin,   \
+                                                                      g_err)
+  if (flat) {
+    DR_LAUNCH(true, 1);
+  } else {
+    switch (G) {
+      case 1: DR_LAUNCH(false, 1); break;
+      case 2: DR_LAUNCH(false, 2); break;
+      case 4: DR_LAUNCH(false, 4); break;
+      case 8: DR_LAUNCH(false, 8); break;
+      case 16: DR_LAUNCH(false, 16); break;
+      case 32: DR_LAUNCH(false, 32); break;
+      default: fail("bad lanes per row");
+    }
+  }
+#undef DR_LAUNCH
   DR_CK(cudaGetLastError());
 }
 
 template <typename TA, class XL, class EP>
 void launch_rows(cudaStream_t st, int max_grid, const DevMat& M, const TA* av, XL xl, EP ep) {
-  launch_rows_impl<TA, XL, EP, false, FinStore>(st, max_grid, M.n, M.ntiles, M.tp, M.ts, M.rp, M.ci,
-                                                av, xl, ep, nullptr, nullptr, FinStore{nullptr});
+  launch_rows_impl<TA, XL, EP, false, FinStore>(st, max_grid, M.G, M.flat, M.n, M.ntiles, M.tp, M.ts,
+                                                M.rp, M.ci, av, xl, ep, nullptr, nullptr,
+                                                FinStore{nullptr});
 }
 
 template <typename TA, class XL, class EP, class Fin>
 void launch_rows_dot(cudaStream_t st, int max_grid, const DevMat& M, const TA* av, XL xl, EP ep,
                      double* partials, unsigned* ticket, Fin fin) {
-  launch_rows_impl<TA, XL, EP, true, Fin>(st, max_grid, M.n, M.ntiles, M.tp, M.ts, M.rp, M.ci, av,
-                                          xl, ep, partials, ticket, fin);
+  launch_rows_impl<TA, XL, EP, true, Fin>(st, max_grid, M.G, M.flat, M.n, M.ntiles, M.tp, M.ts, M.rp,
+                                          M.ci, av, xl, ep, partials, ticket, fin);
 }
 
 int grid1d(long long n, int max_grid) {
@@ -190,7 +226,8 @@ DevHier::DevHier(const HostHierarchy& H, int device) {
       M.v = alloc<double>(ci.size() + 4);
       if (v) h2d(M.v, *v, st_);
       M.Ggs = pick_G(M.nnz, n);
-      std::vector<int> tiles = make_tiles(rp, n);
+      choose_row_form(rp, n, M.nnz, M.G, M.flat);
+      std::vector<int> tiles = make_tiles(rp, n, M.flat ? 1 : M.G);
       std::vector<int> tstart(tiles.size());
       for (size_t t = 0; t < tiles.size(); ++t) tstart[t] = rp[tiles[t]];
       M.ntiles = (int)tiles.size() - 1;

@@ -37,6 +37,8 @@ struct DevMat {
   int* ci = nullptr;
   double* v = nullptr;
   float* v32 = nullptr;
+  int G = 1;          // lanes per row of the row kernel's row-gather form
+  bool flat = false;  // row kernel forms products flat over each tile
   int Ggs = 8;        // lanes per row of the Gauss-Seidel colour kernel
   int ntiles = 0;     // row tiles (see k_tile_rows)
   int* tp = nullptr;  // tile row starts, ntiles+1

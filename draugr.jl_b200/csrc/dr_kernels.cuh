@@ -287,25 +287,29 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 
 // ------------------------------------------------------------ row kernel
 // Rows are packed (on the host, once per matrix) into tiles of at most
-// kBlock consecutive rows holding at most kTileCap nonzeros; tp[t] is the
+// kBlock/G consecutive rows holding at most kTileCap nonzeros; tp[t] is the
 // first row and ts[t] the first nonzero of tile t.  Each block walks the
 // tiles blockIdx.x, +gridDim.x, ... with two shared-memory stages: while it
 // works on one tile, the TMA engine copies the column and value arrays of
 // the tile after next into the other stage (cp.async.bulk completing on an
-// mbarrier), so HBM streaming never waits on the SM.  Per tile:
-//   1. products: the block walks the tile's nonzeros flat (thread t takes
-//      entries t, t+256, ...), gathers x (an L2-resident vector) for up to
-//      eight entries at once and overwrites each staged value with a_ij·x_j;
-//   2. rows: thread t sums the products of row t of the tile in column order
-//      (the reference's order, products and sums rounded separately, so
-//      every row is reproduced bit for bit) and applies the fused epilogue,
-//      whose operands were loaded before waiting for the stage.
-// The column / value arrays carry 4 padding entries so the 16-byte-rounded
-// copies stay in bounds.  A row longer than kTileCap forms a tile of its own
-// and is reduced by the whole block straight from global memory.
+// mbarrier), so HBM streaming never waits on the SM.  The row's other
+// operands (row bounds, epilogue inputs) are loaded before waiting for the
+// stage.  Two ways to form the products a_ij·x_j (x is L2-resident):
+//   row-gather (FLAT = false): G lanes per row gather their entries of the
+//     row, up to eight per lane at once (uniform rows: every lane busy);
+//   flat (FLAT = true, one row per thread): the whole block walks the tile's
+//     nonzeros flat, so a long row among short ones costs no more than its
+//     share (rows of very uneven length, e.g. the restriction Pᵀ).
+// Either way every row is then summed by one thread in column order — the
+// reference's order, with products and sums rounded separately — so all
+// rows up to kTileCap entries are reproduced bit for bit; products are
+// written over the staged values for that when needed.  The column / value
+// arrays carry 4 padding entries so the 16-byte-rounded copies stay in
+// bounds.  A row longer than kTileCap forms a tile of its own and is reduced
+// by the whole block straight from global memory (tree order).
 constexpr int kTileCap = 2000;
 constexpr int kStageEntries = 2008;  // kTileCap + alignment slack, a multiple of 4 entries
-constexpr int kProdIters = (kTileCap + kBlock - 1) / kBlock;
+constexpr int kFlatIters = (kTileCap + kBlock - 1) / kBlock;
 constexpr int kWaitLimit = 1 << 22;
 
 // Dynamic shared memory of k_tile_rows: two stages of columns and values
@@ -321,13 +325,14 @@ __device__ __forceinline__ void bind_epilogue(EP&) {}
 template <typename T>
 __device__ __forceinline__ void bind_epilogue(EpPcgDir<T>& e) { e.bind(); }
 
-template <typename TA, class XL, class EP, bool DOT, class Fin>
+template <bool FLAT, int G, typename TA, class XL, class EP, bool DOT, class Fin>
 __global__ void __launch_bounds__(kBlock)
 k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
             const int* __restrict__ rp, const int* __restrict__ ci, const TA* __restrict__ av,
             XL xl, EP ep, double* partials, unsigned* ticket, Fin fin, int* err) {
   using acc_t = typename EP::acc_t;
   static_assert(sizeof(acc_t) == sizeof(TA), "products are stored over the staged values");
+  static_assert(!FLAT || G == 1, "the flat form uses one row per thread");
   using Pre = typename EP::Pre;
   bind_loader(xl);
   bind_epilogue(ep);
@@ -338,6 +343,10 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ acc_t red[32];
   const int stride = gridDim.x;
+  const int lane = threadIdx.x & (G - 1);
+  const int grp = threadIdx.x / G;
+  const unsigned gmask =
+      (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
 
   auto issue = [&](int t, int b) {  // thread 0 only
     const int s = __ldg(ts + t), e = __ldg(ts + t + 1);
@@ -373,15 +382,14 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
     const int r0 = __ldg(tp + t), r1 = __ldg(tp + t + 1);
     const int s = __ldg(ts + t), e = __ldg(ts + t + 1);
     const int len = e - s;
-    // this thread's row: bounds and epilogue operands, before the wait
-    const int row = r0 + (int)threadIdx.x;
+    const int row = r0 + grp;
     const bool valid = (len <= kTileCap) && row < r1;
     int rs = 0, re = 0;
     Pre pr{};
     if (valid) {
       rs = __ldg(rp + row) - s;
       re = __ldg(rp + row + 1) - s;
-      pr = ep.pre(row);
+      if (lane == 0) pr = ep.pre(row);
     }
     if (!mbar_wait_bounded(bar + b, parity, kWaitLimit)) {
       if (threadIdx.x == 0) atomicExch(err, 1);
@@ -391,27 +399,68 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
       const int off = s - (s & ~3);
       TA* vs = sv0 + b * kStageEntries + off;
       const int* cs = sc0 + b * kStageEntries + off;
-      // 1. products, flat over the tile
-      acc_t p[kProdIters];
+      if constexpr (FLAT) {
+        acc_t p[kFlatIters];
 #pragma unroll
-      for (int j = 0; j < kProdIters; ++j) {
-        const int k = threadIdx.x + j * kBlock;
-        p[j] = (k < len) ? (acc_t)xl(cs[k]) : acc_t(0);
-      }
-#pragma unroll
-      for (int j = 0; j < kProdIters; ++j) {
-        const int k = threadIdx.x + j * kBlock;
-        if (k < len) vs[k] = (TA)mul_rn((acc_t)vs[k], p[j]);
-      }
-      __syncthreads();
-      // 2. rows, in column order
-      if (valid) {
-        acc_t a = ep.init(pr);
-        for (int k = rs; k < re; ++k) {
-          if constexpr (EP::kSign > 0) a = add_rn(a, (acc_t)vs[k]);
-          else a = sub_rn(a, (acc_t)vs[k]);
+        for (int j = 0; j < kFlatIters; ++j) {
+          const int k = threadIdx.x + j * kBlock;
+          p[j] = (k < len) ? (acc_t)xl(cs[k]) : acc_t(0);
         }
-        dacc += ep.apply(row, a, pr);
+#pragma unroll
+        for (int j = 0; j < kFlatIters; ++j) {
+          const int k = threadIdx.x + j * kBlock;
+          if (k < len) vs[k] = (TA)mul_rn((acc_t)vs[k], p[j]);
+        }
+        __syncthreads();
+        if (valid) {
+          acc_t a = ep.init(pr);
+          for (int k = rs; k < re; ++k) {
+            if constexpr (EP::kSign > 0) a = add_rn(a, (acc_t)vs[k]);
+            else a = sub_rn(a, (acc_t)vs[k]);
+          }
+          dacc += ep.apply(row, a, pr);
+        }
+      } else if constexpr (G == 1) {
+        if (valid) {
+          acc_t a = ep.init(pr);
+          for (int k0 = rs; k0 < re; k0 += 8) {
+            acc_t p[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+              p[j] = (k0 + j < re) ? mul_rn((acc_t)vs[k0 + j], (acc_t)xl(cs[k0 + j])) : acc_t(0);
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+              if (k0 + j < re) {
+                if constexpr (EP::kSign > 0) a = add_rn(a, p[j]);
+                else a = sub_rn(a, p[j]);
+              }
+          }
+          dacc += ep.apply(row, a, pr);
+        }
+      } else {
+        // G lanes form the products of a row, lane 0 sums them in order
+        for (int k0 = rs + lane; k0 < re; k0 += 8 * G) {
+          acc_t p[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const int k = k0 + j * G;
+            p[j] = (k < re) ? mul_rn((acc_t)vs[k], (acc_t)xl(cs[k])) : acc_t(0);
+          }
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const int k = k0 + j * G;
+            if (k < re) vs[k] = (TA)p[j];
+          }
+        }
+        __syncwarp(gmask);
+        if (valid && lane == 0) {
+          acc_t a = ep.init(pr);
+          for (int k = rs; k < re; ++k) {
+            if constexpr (EP::kSign > 0) a = add_rn(a, (acc_t)vs[k]);
+            else a = sub_rn(a, (acc_t)vs[k]);
+          }
+          dacc += ep.apply(row, a, pr);
+        }
       }
     } else {
       // a single row longer than the tile capacity, from global memory
