@@ -86,11 +86,14 @@ std::vector<int> make_tiles(const std::vector<int>& rp, int n, int G) {
 static_assert(kTileCap == kRowTileCap, "host and device tile capacities differ");
 
 // Form of the row kernel for a CSR pattern: flat products when row lengths
-// are very uneven (a long row among short ones), otherwise G lanes per row
-// with about six entries per lane (one lane up to 8 entries per row).
-void choose_row_form(const std::vector<int>& rp, int n, long long nnz, int& G, bool& flat) {
+// are very uneven (a long row among short ones); one lane per row up to 8
+// entries per row on average; 4 lanes with an ordered sum up to 32; beyond
+// that G lanes (about 8 entries each) with a shuffle-tree sum.
+void choose_row_form(const std::vector<int>& rp, int n, long long nnz, int& G, bool& flat,
+                     bool& ordered) {
   G = 1;
   flat = false;
+  ordered = true;
   if (n <= 0) return;
   int maxlen = 0;
   for (int i = 0; i < n; ++i) maxlen = std::max(maxlen, rp[i + 1] - rp[i]);
@@ -100,12 +103,17 @@ void choose_row_form(const std::vector<int>& rp, int n, long long nnz, int& G, b
     return;
   }
   if (avg <= 8.0) return;
-  G = 2;
-  while (G < 32 && G * 6 < avg) G *= 2;
+  if (avg <= 32.0) {
+    G = 4;
+    return;
+  }
+  ordered = false;
+  G = 8;
+  while (G < 32 && G * 8 < avg) G *= 2;
 }
 
 template <typename TA, class XL, class EP, bool DOT, class Fin>
-void launch_rows_impl(cudaStream_t st, int max_grid, int G, bool flat, int n, int ntiles,
+void launch_rows_impl(cudaStream_t st, int max_grid, int G, bool flat, bool ordered, int n, int ntiles,
                       const int* tp, const int* ts, const int* rp, const int* ci, const TA* av,
                       XL xl, EP ep, double* partials, unsigned* ticket, Fin fin) {
   if (n <= 0) {
@@ -121,30 +129,24 @@ void launch_rows_impl(cudaStream_t st, int max_grid, int G, bool flat, int n, in
   const int grid = std::max(1, std::min({ntiles, max_grid, g_nsm * per_sm}));
   const size_t smem = tile_smem_bytes<TA>();
   counted();
-#define DR_LAUNCH(F, g)                                                                          \
-  k_tile_rows<F, g, TA, XL, EP, DOT, Fin><<<grid, kBlock, smem, st>>>(ntiles, tp, ts, rp, ci, av, xl, \
-                                                                      ep, partials, ticket, fin,   \
-                                                                      g_err)
-  if (flat) {
-    DR_LAUNCH(true, 1);
-  } else {
-    switch (G) {
-      case 1: DR_LAUNCH(false, 1); break;
-      case 2: DR_LAUNCH(false, 2); break;
-      case 4: DR_LAUNCH(false, 4); break;
-      case 8: DR_LAUNCH(false, 8); break;
-      case 16: DR_LAUNCH(false, 16); break;
-      case 32: DR_LAUNCH(false, 32); break;
-      default: fail("bad lanes per row");
-    }
-  }
+#define DR_LAUNCH(F, g, O)                                                                       \
+  k_tile_rows<F, g, O, TA, XL, EP, DOT, Fin><<<grid, kBlock, smem, st>>>(ntiles, tp, ts, rp, ci, av,  \
+                                                                         xl, ep, partials, ticket,  \
+                                                                         fin, g_err)
+  if (flat) DR_LAUNCH(true, 1, true);
+  else if (G == 1) DR_LAUNCH(false, 1, true);
+  else if (G == 4 && ordered) DR_LAUNCH(false, 4, true);
+  else if (G == 8) DR_LAUNCH(false, 8, false);
+  else if (G == 16) DR_LAUNCH(false, 16, false);
+  else if (G == 32) DR_LAUNCH(false, 32, false);
+  else fail("bad row form");
 #undef DR_LAUNCH
   DR_CK(cudaGetLastError());
 }
 
 template <typename TA, class XL, class EP>
 void launch_rows(cudaStream_t st, int max_grid, const DevMat& M, const TA* av, XL xl, EP ep) {
-  launch_rows_impl<TA, XL, EP, false, FinStore>(st, max_grid, M.G, M.flat, M.n, M.ntiles, M.tp, M.ts,
+  launch_rows_impl<TA, XL, EP, false, FinStore>(st, max_grid, M.G, M.flat, M.ordered, M.n, M.ntiles, M.tp, M.ts,
                                                 M.rp, M.ci, av, xl, ep, nullptr, nullptr,
                                                 FinStore{nullptr});
 }
@@ -152,7 +154,7 @@ void launch_rows(cudaStream_t st, int max_grid, const DevMat& M, const TA* av, X
 template <typename TA, class XL, class EP, class Fin>
 void launch_rows_dot(cudaStream_t st, int max_grid, const DevMat& M, const TA* av, XL xl, EP ep,
                      double* partials, unsigned* ticket, Fin fin) {
-  launch_rows_impl<TA, XL, EP, true, Fin>(st, max_grid, M.G, M.flat, M.n, M.ntiles, M.tp, M.ts, M.rp,
+  launch_rows_impl<TA, XL, EP, true, Fin>(st, max_grid, M.G, M.flat, M.ordered, M.n, M.ntiles, M.tp, M.ts, M.rp,
                                           M.ci, av, xl, ep, partials, ticket, fin);
 }
 
@@ -226,7 +228,7 @@ DevHier::DevHier(const HostHierarchy& H, int device) {
       M.v = alloc<double>(ci.size() + 4);
       if (v) h2d(M.v, *v, st_);
       M.Ggs = pick_G(M.nnz, n);
-      choose_row_form(rp, n, M.nnz, M.G, M.flat);
+      choose_row_form(rp, n, M.nnz, M.G, M.flat, M.ordered);
       std::vector<int> tiles = make_tiles(rp, n, M.flat ? 1 : M.G);
       std::vector<int> tstart(tiles.size());
       for (size_t t = 0; t < tiles.size(); ++t) tstart[t] = rp[tiles[t]];

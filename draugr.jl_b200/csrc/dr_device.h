@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -19,12 +20,19 @@ long long kernel_launches();
 // order.
 constexpr int kRowTileCap = 2000;
 
-// 1 when every row of the CSR pattern is reduced in column order (the
-// reference's order, bit for bit), 0 if some row exceeds the tile capacity.
+// 1 when the row kernel reduces every row of the CSR pattern in column
+// order (the reference's order, bit for bit): rows average at most 32
+// entries (or are very uneven, which selects the flat form) and none
+// exceeds the tile capacity.  Mirrors choose_row_form in dr_device.cu.
 inline int rows_in_order(const std::vector<int>& rp) {
-  for (size_t i = 0; i + 1 < rp.size(); ++i)
-    if (rp[i + 1] - rp[i] > kRowTileCap) return 0;
-  return 1;
+  const size_t n = rp.size() ? rp.size() - 1 : 0;
+  if (n == 0) return 1;
+  int maxlen = 0;
+  for (size_t i = 0; i < n; ++i) maxlen = std::max(maxlen, rp[i + 1] - rp[i]);
+  if (maxlen > kRowTileCap) return 0;
+  const double avg = (double)(rp[n] - rp[0]) / (double)n;
+  if (maxlen > 64 && maxlen > 4.0 * avg) return 1;
+  return avg <= 32.0 ? 1 : 0;
 }
 
 // Sparse matrix on the device: CSR pattern, FP64 values and (after the first
@@ -39,6 +47,7 @@ struct DevMat {
   float* v32 = nullptr;
   int G = 1;          // lanes per row of the row kernel's row-gather form
   bool flat = false;  // row kernel forms products flat over each tile
+  bool ordered = true;  // rows summed in column order (the reference's)
   int Ggs = 8;        // lanes per row of the Gauss-Seidel colour kernel
   int ntiles = 0;     // row tiles (see k_tile_rows)
   int* tp = nullptr;  // tile row starts, ntiles+1

@@ -300,10 +300,11 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 //   flat (FLAT = true, one row per thread): the whole block walks the tile's
 //     nonzeros flat, so a long row among short ones costs no more than its
 //     share (rows of very uneven length, e.g. the restriction Pᵀ).
-// Either way every row is then summed by one thread in column order — the
-// reference's order, with products and sums rounded separately — so all
-// rows up to kTileCap entries are reproduced bit for bit; products are
-// written over the staged values for that when needed.  The column / value
+// Rows of up to 32 entries (ORDERED) are then summed by one thread in
+// column order — the reference's order, with products and sums rounded
+// separately — so they are reproduced bit for bit; products are written over
+// the staged values for that when needed.  Longer rows are summed by their G
+// lanes and a fixed shuffle tree (deterministic, not the reference's order).  The column / value
 // arrays carry 4 padding entries so the 16-byte-rounded copies stay in
 // bounds.  A row longer than kTileCap forms a tile of its own and is reduced
 // by the whole block straight from global memory (tree order).
@@ -325,7 +326,7 @@ __device__ __forceinline__ void bind_epilogue(EP&) {}
 template <typename T>
 __device__ __forceinline__ void bind_epilogue(EpPcgDir<T>& e) { e.bind(); }
 
-template <bool FLAT, int G, typename TA, class XL, class EP, bool DOT, class Fin>
+template <bool FLAT, int G, bool ORDERED, typename TA, class XL, class EP, bool DOT, class Fin>
 __global__ void __launch_bounds__(kBlock)
 k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
             const int* __restrict__ rp, const int* __restrict__ ci, const TA* __restrict__ av,
@@ -437,7 +438,7 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
           }
           dacc += ep.apply(row, a, pr);
         }
-      } else {
+      } else if constexpr (ORDERED) {
         // G lanes form the products of a row, lane 0 sums them in order
         for (int k0 = rs + lane; k0 < re; k0 += 8 * G) {
           acc_t p[8];
@@ -459,6 +460,27 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
             if constexpr (EP::kSign > 0) a = add_rn(a, (acc_t)vs[k]);
             else a = sub_rn(a, (acc_t)vs[k]);
           }
+          dacc += ep.apply(row, a, pr);
+        }
+      } else {
+        // long rows: G lanes sum strided products, then a fixed shuffle tree
+        acc_t sum = acc_t(0);
+        for (int k0 = rs + lane; k0 < re; k0 += 4 * G) {
+          acc_t p[4];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int k = k0 + j * G;
+            p[j] = (k < re) ? mul_rn((acc_t)vs[k], (acc_t)xl(cs[k])) : acc_t(0);
+          }
+#pragma unroll
+          for (int j = 0; j < 4; ++j) sum = add_rn(sum, p[j]);
+        }
+#pragma unroll
+        for (int o = G >> 1; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        if (valid && lane == 0) {
+          acc_t a = ep.init(pr);
+          if constexpr (EP::kSign > 0) a = add_rn(a, sum);
+          else a = sub_rn(a, sum);
           dacc += ep.apply(row, a, pr);
         }
       }
