@@ -129,6 +129,11 @@ int32_t guarded(const char* name, F&& f) {
 
 }  // namespace
 
+namespace dr {
+// Last-error text for entry points defined outside this file.
+void set_last_error(const std::string& msg) { set_error(msg); }
+}  // namespace dr
+
 extern "C" {
 
 void init_julia(int, char**) {}
@@ -433,6 +438,19 @@ int32_t draugr_b200_resetup_values_device(int32_t handle, int64_t nnz, const dou
     if (nnz != A0.nnz()) fail("partial resetup: nnz differs from the one given at setup");
     DevHier& D = device_of(*H);
     D.resetup_values(nzval_dev);
+    return 0;
+  });
+}
+
+int32_t draugr_b200_residual_device(int32_t handle, int32_t n, const double* x_dev, const double* b_dev,
+                                    double* r_dev, double* rnorm) {
+  return guarded("draugr_b200_residual_device", [&]() -> int32_t {
+    auto H = get_hier_only(handle);
+    if (n != n_finest(*H)) fail("DimensionMismatch");
+    if (!x_dev || !b_dev || !r_dev) fail("ArgumentError: NULL vector");
+    DevHier& D = device_of(*H);
+    const double nr = D.residual_norm(x_dev, b_dev, r_dev);
+    if (rnorm) *rnorm = nr;
     return 0;
   });
 }

@@ -569,6 +569,13 @@ int DevHier::solve(double* x, const double* b, const CycleOpts& o, double tol, i
   return maxiter;
 }
 
+double DevHier::residual_norm(const double* x, const double* b, double* r) {
+  residual<double>(0, x, b, r, scal_ + SC_TMP);
+  DR_CK(cudaMemcpyAsync(hscal_ + SC_TMP, scal_ + SC_TMP, sizeof(double), cudaMemcpyDeviceToHost, st_));
+  check_kernel_flag(st_);
+  return std::sqrt(hscal_[SC_TMP]);
+}
+
 // ------------------------------------------------------------ PCG
 // Preconditioned conjugate gradients around one AMG cycle per iteration
 // (x of the cycle zeroed, as preconditioner_apply! does,

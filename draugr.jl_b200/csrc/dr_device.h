@@ -111,6 +111,9 @@ class DevHier {
   int pcg(double* x, const double* b, const CycleOpts& o, double tol, int maxiter, bool mixed,
           double* relres, int verbose);
 
+  // r = b - A x on the finest level and ||r||_2 (device vectors).
+  double residual_norm(const double* x, const double* b, double* r);
+
   // Numeric resetup on the fixed structure; values of the finest matrix on
   // the device (nnz0 entries).
   void resetup_values(const double* v_dev);

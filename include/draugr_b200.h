@@ -58,6 +58,12 @@ int32_t draugr_b200_solve_device(int32_t handle, int32_t n, double *x_dev, const
 int32_t draugr_b200_cycle_device(int32_t handle, int32_t n, double *x_dev, const double *b_dev,
                                  int32_t config_handle);
 
+/* r = b - A x for the finest matrix of the hierarchy and ||r||_2 (device
+ * vectors of length n; rnorm is a host pointer, may be NULL).  The residual
+ * of amg_solve!'s convergence test (src/cycle.jl:138-139). */
+int32_t draugr_b200_residual_device(int32_t handle, int32_t n, const double *x_dev,
+                                    const double *b_dev, double *r_dev, double *rnorm);
+
 /* Partial resetup from new values of the finest matrix already on the
  * device (same pattern as at setup), nnz entries. */
 int32_t draugr_b200_resetup_values_device(int32_t handle, int64_t nnz, const double *nzval_dev);

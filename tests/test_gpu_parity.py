@@ -259,3 +259,29 @@ def test_cycle_bit_exact_when_all_rows_single_lane(fresh_case):
             x = start.copy()
             draugr.amg_cycle(x, b, h, c2)
             assert np.array_equal(x, O.cycle(start, b, 1, 1, w))
+
+
+def test_residual_entry_point(fresh_case):
+    """draugr_b200_residual_device: r = b - A x and ||r|| on device vectors."""
+    torch = pytest.importorskip("torch")
+    import ctypes as C
+    name, A, cfg, h, O = fresh_case
+    n = A.shape[0]
+    rng = np.random.default_rng(31)
+    x = rng.uniform(-1, 1, n)
+    b = rng.uniform(-1, 1, n)
+    xd = torch.tensor(x, dtype=torch.float64, device="cuda")
+    bd = torch.tensor(b, dtype=torch.float64, device="cuda")
+    rd = torch.zeros(n, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    rn = C.c_double(0)
+    rc = draugr.load().draugr_b200_residual_device(h.handle, n, xd.data_ptr(), bd.data_ptr(),
+                                                   rd.data_ptr(), C.byref(rn))
+    assert rc == 0, draugr.last_error()
+    d, L = _level_arrays(O, 0)
+    ref = oracle.residual(n, d["A_rp"], d["A_ci"], d["A_v"], x, b)
+    r = rd.cpu().numpy()
+    assert rel(r, ref) < TOL64
+    if _single_lane(h, 0)[0]:
+        assert np.array_equal(r, ref)
+    assert abs(rn.value - np.linalg.norm(ref)) <= 1e-12 * np.linalg.norm(ref)
