@@ -64,6 +64,28 @@ int32_t draugr_b200_cycle_device(int32_t handle, int32_t n, double *x_dev, const
 int32_t draugr_b200_residual_device(int32_t handle, int32_t n, const double *x_dev,
                                     const double *b_dev, double *r_dev, double *rnorm);
 
+/* The residual above for callers that cannot allocate device memory: hosts
+ * whose own pool hands out every byte of device memory (a framework's
+ * caching allocator, a solver that reserves all memory at start-up) and so
+ * cannot let a library call cudaMalloc.  No counterpart in the reference.
+ * All arrays belong to the caller and are device pointers: the n x n CSR
+ * matrix (0-based rowptr[n+1], colval[nnz], nzval[nnz]), x and b (length n)
+ * and the output r = b - A x (length n); rnorm (host pointer, may be NULL)
+ * receives ||r||_2.  stream: a cudaStream_t, NULL for the default stream.
+ * Nothing is allocated: the reduction's scratch is a static device array of
+ * 16386 doubles (128 KB, held by every GPU that loads the library until the
+ * process exits), so n is limited to 4,194,304 rows (16384 blocks of 256
+ * rows); larger n is rejected with an error.  The first call on a device
+ * looks up the scratch's device address (cudaGetSymbolAddress); make that
+ * first call before any stream capture.  All calls share the scratch, so
+ * calls that overlap on the GPU (different streams or threads) race; the
+ * call returns after its work on `stream` has finished.  Rows are summed in
+ * column order, as draugr_b200_residual_device does for rows of up to 32
+ * entries.  Returns 0 or -1. */
+int32_t draugr_b200_residual_noalloc(int32_t n, int32_t nnz, const int32_t *rowptr,
+                                     const int32_t *colval, const double *nzval, const double *x,
+                                     const double *b, double *r, double *rnorm, void *stream);
+
 /* Partial resetup from new values of the finest matrix already on the
  * device (same pattern as at setup), nnz entries. */
 int32_t draugr_b200_resetup_values_device(int32_t handle, int64_t nnz, const double *nzval_dev);
