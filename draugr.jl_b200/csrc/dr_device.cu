@@ -86,9 +86,9 @@ std::vector<int> make_tiles(const std::vector<int>& rp, int n, int G) {
 static_assert(kTileCap == kRowTileCap, "host and device tile capacities differ");
 
 // Form of the row kernel for a CSR pattern: flat products when row lengths
-// are very uneven (a long row among short ones); one lane per row up to 8
-// entries per row on average; 4 lanes with an ordered sum up to 32; beyond
-// that G lanes (about 8 entries each) with a shuffle-tree sum.
+// are very uneven (a long row among short ones); one lane per row (ordered
+// sum) up to 32 entries per row on average; beyond that G lanes (about 8
+// entries each) with a shuffle-tree sum.
 void choose_row_form(const std::vector<int>& rp, int n, long long nnz, int& G, bool& flat,
                      bool& ordered) {
   G = 1;
@@ -102,11 +102,7 @@ void choose_row_form(const std::vector<int>& rp, int n, long long nnz, int& G, b
     flat = true;
     return;
   }
-  if (avg <= 8.0) return;
-  if (avg <= 32.0) {
-    G = 4;
-    return;
-  }
+  if (avg <= 32.0) return;
   ordered = false;
   G = 8;
   while (G < 32 && G * 8 < avg) G *= 2;
