@@ -285,6 +285,7 @@ DevHier::DevHier(const HostHierarchy& H, int device) {
       DR_CK(cudaFuncSetAttribute(k_lu_solve<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
       DR_CK(cudaFuncSetAttribute(k_lu_solve<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
     }
+    build_tail();
     DR_CK(cudaStreamSynchronize(st_));
   } catch (...) {
     for (void* p : allocs_) cudaFree(p);
@@ -365,6 +366,57 @@ void DevHier::ensure_fp32() {
   cx32_ = alloc<float>(nc_);
   fp32_ = true;
   refresh_fp32();
+  build_tail();
+}
+
+// Levels from the first one with at most kTailRows rows (and below it only
+// such levels, all with Jacobi-type smoothers) down to the coarsest run in
+// one block; never the finest level (its iterate is the caller's buffer).
+static constexpr int kTailRows = 4096;
+
+void DevHier::build_tail() {
+  const int nl = nlevels();
+  tail_ = nl;
+  if (nc_ > 4096) return;
+  for (int l = nl - 1; l >= 1; --l) {
+    const DevLevel& d = L_[l];
+    const bool jac = d.smoother == SmootherKind::Jacobi || d.smoother == SmootherKind::L1Jacobi;
+    if (d.A.n > kTailRows || !jac) break;
+    tail_ = l;
+  }
+  if (tail_ >= nl) return;
+  const int cnt = nl - tail_;
+  auto make = [&](auto tag) {
+    using T = decltype(tag);
+    std::vector<TailLevel<T>> v(cnt);
+    for (int k = 0; k < cnt; ++k) {
+      DevLevel& d = L_[tail_ + k];
+      LevelVecs<T>& V = vecs<T>(tail_ + k);
+      TailLevel<T>& t = v[k];
+      t.n = d.A.n;
+      t.nc = d.P.m;
+      t.arp = d.A.rp;
+      t.aci = d.A.ci;
+      t.av = mval<T>(d.A);
+      t.invd = invd<T>(d);
+      t.omega = (T)d.omega;
+      t.prp = d.P.rp;
+      t.pci = d.P.ci;
+      t.pv = mval<T>(d.P);
+      t.rrp = d.R.rp;
+      t.rci = d.R.ci;
+      t.rv = mval<T>(d.R);
+      t.xa = V.xa;
+      t.xb = V.xb;
+      t.b = V.b;
+      t.r = V.r;
+    }
+    TailLevel<T>* dst = alloc<TailLevel<T>>(cnt);
+    DR_CK(cudaMemcpy(dst, v.data(), cnt * sizeof(TailLevel<T>), cudaMemcpyHostToDevice));
+    return (void*)dst;
+  };
+  tail64_ = make(double());
+  if (fp32_) tail32_ = make(float());
 }
 
 void DevHier::refresh_fp32() {
@@ -460,6 +512,16 @@ bool DevHier::fused_rz_ok(const CycleOpts& o) const {
 template <typename T>
 T* DevHier::cycle_level(int l, T* x, const T* b, bool x_zero, const CycleOpts& o, T* ext,
                         const double* rz_w, bool rz_first) {
+  if (l >= 1 && l == tail_ && x == vecs<T>(l).xa) {
+    const void* desc = sizeof(T) == 8 ? tail64_ : tail32_;
+    TailCoarse<T> C{nc_, clu_, cpiv_, coarse_b<T>(), coarse_x<T>()};
+    counted();
+    k_coarse_tail<T><<<1, 1024, (size_t)std::max(nc_, 1) * sizeof(double), st_>>>(
+        static_cast<const TailLevel<T>*>(desc), nlevels() - l, C, o.pre, o.post, o.w ? 1 : 0,
+        x_zero ? 1 : 0);
+    DR_CK(cudaGetLastError());
+    return x;
+  }
   DevLevel& L = L_[l];
   LevelVecs<T>& V = vecs<T>(l);
   const DevMat& A = L.A;

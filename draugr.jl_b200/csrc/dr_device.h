@@ -156,6 +156,12 @@ class DevHier {
 
   void ensure_fp32();
   void refresh_fp32();
+  void build_tail();
+  // Levels tail_ .. nlevels-1 run as one single-block kernel (k_coarse_tail);
+  // tail_ = nlevels() when no level qualifies.
+  int tail_ = 0;
+  void* tail64_ = nullptr;   // device TailLevel<double>[nlevels - tail_]
+  void* tail32_ = nullptr;   // device TailLevel<float>[...] once FP32 buffers exist
   void graphs_clear();
   double dot_host(const double* a, const double* b, int n);
 

@@ -644,6 +644,156 @@ __global__ void k_lu_solve(int n, const double* __restrict__ lu, const int* __re
   for (int i = threadIdx.x; i < n; i += blockDim.x) xout[i] = (T)y[i];
 }
 
+// ------------------------------------------------------------ coarse tail
+// The cycle from one small level down to the coarsest, in one block: every
+// phase (smoothing, residual, restriction, coarsest solve, prolongation) is
+// a loop over rows by the block's threads, one thread per row summing in
+// column order (the reference's order), separated by block barriers.  This
+// replaces about four kernel launches per level on levels whose work is a
+// few microseconds, where launch and drain latency would dominate.
+template <typename T>
+struct TailLevel {
+  int n, nc;
+  const int *arp, *aci;
+  const T *av, *invd;
+  T omega;
+  const int *prp, *pci;
+  const T* pv;
+  const int *rrp, *rci;
+  const T* rv;
+  T *xa, *xb, *b, *r;  // iterate pair, right-hand side, residual
+};
+
+template <typename T>
+struct TailCoarse {
+  int n;
+  const double* lu;
+  const int* piv;
+  T *b, *x;
+};
+
+template <typename T>
+__device__ void tail_jacobi(const TailLevel<T>& L, const T* x, const T* b, T* xn) {
+  for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
+    T ri = b[i];
+    for (int k = L.arp[i]; k < L.arp[i + 1]; ++k) ri = sub_rn(ri, mul_rn(L.av[k], x[L.aci[k]]));
+    xn[i] = add_rn(x[i], mul_rn(mul_rn(L.omega, L.invd[i]), ri));
+  }
+  __syncthreads();
+}
+
+template <typename T>
+__device__ void tail_lu_solve(const TailCoarse<T>& C, double* y) {
+  const int n = C.n;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = (double)C.b[i];
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int j = 0; j < n; ++j) {
+      const int p = C.piv[j];
+      if (p != j) {
+        const double t = y[j];
+        y[j] = y[p];
+        y[p] = t;
+      }
+    }
+  __syncthreads();
+  for (int j = 0; j < n; ++j) {
+    const double yj = y[j];
+    if (yj != 0.0)
+      for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x)
+        y[i] = __dsub_rn(y[i], __dmul_rn(yj, C.lu[(size_t)j * n + i]));
+    __syncthreads();
+  }
+  for (int j = n - 1; j >= 0; --j) {
+    if (threadIdx.x == 0 && y[j] != 0.0) y[j] = __ddiv_rn(y[j], C.lu[(size_t)j * n + j]);
+    __syncthreads();
+    const double yj = y[j];
+    if (yj != 0.0)
+      for (int i = threadIdx.x; i < j; i += blockDim.x)
+        y[i] = __dsub_rn(y[i], __dmul_rn(yj, C.lu[(size_t)j * n + i]));
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) C.x[i] = (T)y[i];
+  __syncthreads();
+}
+
+// One visit of level l (x_zero: the iterate starts at zero).  The result
+// ends in L.xa.  Levels l+1 .. nl-1 follow in `lv`; the coarsest system is C.
+template <typename T>
+__device__ void tail_visit(const TailLevel<T>* lv, int l, int nl, const TailCoarse<T>& C,
+                           bool x_zero, int pre, int post, int wcycle, double* y) {
+  const TailLevel<T>& L = lv[l];
+  T* x = L.xa;
+  T* t = L.xb;
+  const T* b = L.b;
+  bool have_r = false;
+  if (x_zero && pre >= 1) {
+    // first Jacobi step from zero, residual of its result
+    for (int i = threadIdx.x; i < L.n; i += blockDim.x) x[i] = mul_rn(mul_rn(L.omega, L.invd[i]), b[i]);
+    __syncthreads();
+    for (int s = 1; s < pre; ++s) {
+      tail_jacobi(L, x, b, t);
+      T* u = x; x = t; t = u;
+    }
+  } else {
+    if (x_zero) {
+      for (int i = threadIdx.x; i < L.n; i += blockDim.x) x[i] = T(0);
+      __syncthreads();
+    }
+    for (int s = 0; s < pre; ++s) {
+      tail_jacobi(L, x, b, t);
+      T* u = x; x = t; t = u;
+    }
+  }
+  if (!have_r) {
+    for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
+      T ax = T(0);
+      for (int k = L.arp[i]; k < L.arp[i + 1]; ++k) ax = add_rn(ax, mul_rn(L.av[k], x[L.aci[k]]));
+      L.r[i] = sub_rn(b[i], ax);
+    }
+    __syncthreads();
+  }
+  const bool last = (l + 1 == nl);
+  T* bn = last ? C.b : lv[l + 1].b;
+  for (int J = threadIdx.x; J < L.nc; J += blockDim.x) {
+    T acc = T(0);
+    for (int k = L.rrp[J]; k < L.rrp[J + 1]; ++k) acc = add_rn(acc, mul_rn(L.rv[k], L.r[L.rci[k]]));
+    bn[J] = acc;
+  }
+  __syncthreads();
+  const T* xc;
+  if (!last) {
+    tail_visit(lv, l + 1, nl, C, true, pre, post, wcycle, y);
+    if (wcycle) tail_visit(lv, l + 1, nl, C, false, pre, post, wcycle, y);
+    xc = lv[l + 1].xa;
+  } else {
+    tail_lu_solve(C, y);
+    xc = C.x;
+  }
+  for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
+    T xi = x[i];
+    for (int k = L.prp[i]; k < L.prp[i + 1]; ++k) xi = add_rn(xi, mul_rn(L.pv[k], xc[L.pci[k]]));
+    x[i] = xi;
+  }
+  __syncthreads();
+  for (int s = 0; s < post; ++s) {
+    tail_jacobi(L, x, b, t);
+    T* u = x; x = t; t = u;
+  }
+  if (x != L.xa) {
+    for (int i = threadIdx.x; i < L.n; i += blockDim.x) L.xa[i] = x[i];
+    __syncthreads();
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(1024)
+k_coarse_tail(const TailLevel<T>* lv, int nl, TailCoarse<T> C, int pre, int post, int wcycle,
+              int x_zero) {
+  extern __shared__ double ysh[];
+  tail_visit(lv, 0, nl, C, x_zero != 0, pre, post, wcycle, ysh);
+}
+
 // In-place unblocked LU with partial pivoting (dgetf2 order) of a
 // column-major n x n matrix in one block.  info = 0 or the 1-based index of
 // the first zero pivot (factorisation stops there).
