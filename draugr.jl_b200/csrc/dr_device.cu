@@ -19,7 +19,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
+#include <unordered_map>
 
 #include "dr_device.h"
 #include "dr_kernels.cuh"
@@ -108,6 +110,21 @@ void choose_row_form(const std::vector<int>& rp, int n, long long nnz, int& G, b
   while (G < 32 && G * 8 < avg) G *= 2;
 }
 
+// Blocks of kBlock threads with `smem` dynamic shared memory that fit on one
+// SM at once, per kernel (queried once).
+int resident_blocks(const void* f, size_t smem) {
+  static std::mutex mu;
+  static std::unordered_map<const void*, int> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(f);
+  if (it != cache.end()) return it->second;
+  int nb = 0;
+  DR_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, f, kBlock, smem));
+  nb = std::max(1, nb);
+  cache.emplace(f, nb);
+  return nb;
+}
+
 template <typename TA, class XL, class EP, bool DOT, class Fin>
 void launch_rows_impl(cudaStream_t st, int max_grid, int G, bool flat, bool ordered, int n, int ntiles,
                       const int* tp, const int* ts, const int* rp, const int* ci, const TA* av,
@@ -120,15 +137,17 @@ void launch_rows_impl(cudaStream_t st, int max_grid, int G, bool flat, bool orde
     }
     return;
   }
-  // resident blocks per SM: shared memory allows 4 (FP64 values) or 6 (FP32)
-  const int per_sm = sizeof(TA) == 8 ? 4 : 7;
-  const int grid = std::max(1, std::min({ntiles, max_grid, g_nsm * per_sm}));
   const size_t smem = tile_smem_bytes<TA>();
   counted();
-#define DR_LAUNCH(F, g, O)                                                                       \
-  k_tile_rows<F, g, O, TA, XL, EP, DOT, Fin><<<grid, kBlock, smem, st>>>(ntiles, tp, ts, rp, ci, av,  \
-                                                                         xl, ep, partials, ticket,  \
-                                                                         fin, g_err)
+  // one wave of resident blocks (registers and shared memory permitting)
+#define DR_LAUNCH(F, g, O)                                                                      \
+  do {                                                                                          \
+    auto kf = k_tile_rows<F, g, O, TA, XL, EP, DOT, Fin>;                                       \
+    const int grid = std::max(                                                                  \
+        1, std::min({ntiles, max_grid, g_nsm * resident_blocks((const void*)kf, smem)}));       \
+    kf<<<grid, kBlock, smem, st>>>(ntiles, tp, ts, rp, ci, av, xl, ep, partials, ticket, fin,   \
+                                   g_err);                                                      \
+  } while (0)
   if (flat) DR_LAUNCH(true, 1, true);
   else if (G == 1) DR_LAUNCH(false, 1, true);
   else if (G == 4 && ordered) DR_LAUNCH(false, 4, true);
@@ -372,12 +391,12 @@ void DevHier::ensure_fp32() {
 // Levels from the first one with at most kTailRows rows (and below it only
 // such levels, all with Jacobi-type smoothers) down to the coarsest run in
 // one block; never the finest level (its iterate is the caller's buffer).
-static constexpr int kTailRows = 4096;
+static constexpr int kTailRows = 512;
 
 void DevHier::build_tail() {
   const int nl = nlevels();
   tail_ = nl;
-  if (nc_ > 4096) return;
+  if ((size_t)(nc_ + 2) * (nc_ + 1) * sizeof(double) > 40 * 1024) return;  // y and LU in shared memory
   for (int l = nl - 1; l >= 1; --l) {
     const DevLevel& d = L_[l];
     const bool jac = d.smoother == SmootherKind::Jacobi || d.smoother == SmootherKind::L1Jacobi;
@@ -516,7 +535,7 @@ T* DevHier::cycle_level(int l, T* x, const T* b, bool x_zero, const CycleOpts& o
     const void* desc = sizeof(T) == 8 ? tail64_ : tail32_;
     TailCoarse<T> C{nc_, clu_, cpiv_, coarse_b<T>(), coarse_x<T>()};
     counted();
-    k_coarse_tail<T><<<1, 1024, (size_t)std::max(nc_, 1) * sizeof(double), st_>>>(
+    k_coarse_tail<T><<<1, 1024, (size_t)(((nc_ + 1) & ~1) + (size_t)nc_ * nc_) * sizeof(double), st_>>>(
         static_cast<const TailLevel<T>*>(desc), nlevels() - l, C, o.pre, o.post, o.w ? 1 : 0,
         x_zero ? 1 : 0);
     DR_CK(cudaGetLastError());

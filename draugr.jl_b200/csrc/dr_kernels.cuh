@@ -293,8 +293,8 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 // works on one tile, the TMA engine copies the column and value arrays of
 // the tile after next into the other stage (cp.async.bulk completing on an
 // mbarrier), so HBM streaming never waits on the SM.  The row's other
-// operands (row bounds, epilogue inputs) are loaded before waiting for the
-// stage.  Two ways to form the products a_ij·x_j (x is L2-resident):
+// operands (row bounds, epilogue inputs) are loaded one tile ahead into
+// registers.  Two ways to form the products a_ij·x_j (x is L2-resident):
 //   row-gather (FLAT = false): G lanes per row gather their entries of the
 //     row, up to eight per lane at once (uniform rows: every lane busy);
 //   flat (FLAT = true, one row per thread): the whole block walks the tile's
@@ -349,14 +349,37 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
   const unsigned gmask =
       (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
 
-  auto issue = [&](int t, int b) {  // thread 0 only
-    const int s = __ldg(ts + t), e = __ldg(ts + t + 1);
-    if (e - s > kTileCap) {
+  // A tile's bounds, and one thread's row bounds and epilogue operands in it.
+  struct Head {
+    int r0, r1, s, e;
+  };
+  struct Ctx {
+    int rs, re;
+    bool valid;
+    Pre pr;
+  };
+  auto head = [&](int t) -> Head {
+    if (t >= ntiles) return Head{0, 0, 0, 0};
+    return Head{__ldg(tp + t), __ldg(tp + t + 1), __ldg(ts + t), __ldg(ts + t + 1)};
+  };
+  auto ctx = [&](const Head& h) -> Ctx {
+    Ctx c{0, 0, false, Pre{}};
+    const int row = h.r0 + grp;
+    c.valid = (h.e - h.s <= kTileCap) && row < h.r1;
+    if (c.valid) {
+      c.rs = __ldg(rp + row) - h.s;
+      c.re = __ldg(rp + row + 1) - h.s;
+      if (lane == 0) c.pr = ep.pre(row);
+    }
+    return c;
+  };
+  auto issue = [&](const Head& h, int b) {  // thread 0 only
+    if (h.e - h.s > kTileCap) {
       mbar_arrive(bar + b);  // long row: nothing to stage
       return;
     }
-    const int sal = s & ~3;
-    const uint32_t cnt = (uint32_t)(e - sal);
+    const int sal = h.s & ~3;
+    const uint32_t cnt = (uint32_t)(h.e - sal);
     const uint32_t cb = (cnt * 4u + 15u) & ~15u;
     const uint32_t vb = (cnt * (uint32_t)sizeof(TA) + 15u) & ~15u;
     mbar_expect_tx(bar + b, cb + vb);
@@ -370,28 +393,31 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
     fence_mbar_init();
   }
   __syncthreads();
+  // Software pipeline: while tile t is reduced, the TMA engine streams the
+  // columns and values of tile t + stride (issued one tile earlier), this
+  // thread's row bounds and epilogue operands of tile t + stride are in
+  // flight to registers, and so are the bounds of tile t + 2 stride.  What
+  // is left on a tile's critical path is the L2 gather of x.
+  Head h0 = head(blockIdx.x), h1 = head(blockIdx.x + stride);
   if (threadIdx.x == 0) {
-    if (blockIdx.x < ntiles) issue(blockIdx.x, 0);
-    if (blockIdx.x + stride < ntiles) issue(blockIdx.x + stride, 1);
+    if (blockIdx.x < ntiles) issue(h0, 0);
+    if (blockIdx.x + stride < ntiles) issue(h1, 1);
   }
+  Ctx c0 = ctx(h0);
 
   double dacc = 0.0;
   int i = 0;
   for (int t = blockIdx.x; t < ntiles; t += stride, ++i) {
     const int b = i & 1;
     const uint32_t parity = (uint32_t)((i >> 1) & 1);
-    const int r0 = __ldg(tp + t), r1 = __ldg(tp + t + 1);
-    const int s = __ldg(ts + t), e = __ldg(ts + t + 1);
+    const Head h2 = head(t + 2 * stride);
+    const Ctx c1 = ctx(h1);
+    const int r0 = h0.r0, s = h0.s, e = h0.e;
     const int len = e - s;
     const int row = r0 + grp;
-    const bool valid = (len <= kTileCap) && row < r1;
-    int rs = 0, re = 0;
-    Pre pr{};
-    if (valid) {
-      rs = __ldg(rp + row) - s;
-      re = __ldg(rp + row + 1) - s;
-      if (lane == 0) pr = ep.pre(row);
-    }
+    const bool valid = c0.valid;
+    const int rs = c0.rs, re = c0.re;
+    const Pre& pr = c0.pr;
     if (!mbar_wait_bounded(bar + b, parity, kWaitLimit)) {
       if (threadIdx.x == 0) atomicExch(err, 1);
       mbar_wait_bounded(bar + b, parity, kWaitLimit);
@@ -509,8 +535,11 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
     __syncthreads();  // stage b fully consumed
     if (threadIdx.x == 0 && t + 2 * stride < ntiles) {
       fence_proxy_async();
-      issue(t + 2 * stride, b);
+      issue(h2, b);
     }
+    h0 = h1;
+    h1 = h2;
+    c0 = c1;
   }
   if constexpr (DOT) grid_sum_finalize(dacc, partials, ticket, fin);
 }
@@ -672,19 +701,36 @@ struct TailCoarse {
   T *b, *x;
 };
 
+// a ± Σ_k v[k]·x[c[k]] over [s, e) in column order, eight loads in flight
+template <int SIGN, typename T>
+__device__ __forceinline__ T tail_row(T a, const int* __restrict__ c, const T* __restrict__ v,
+                                      const T* x, int s, int e) {
+  for (int k0 = s; k0 < e; k0 += 8) {
+    T p[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) p[j] = (k0 + j < e) ? mul_rn(v[k0 + j], x[c[k0 + j]]) : T(0);
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      if (k0 + j < e) a = SIGN > 0 ? add_rn(a, p[j]) : sub_rn(a, p[j]);
+  }
+  return a;
+}
+
 template <typename T>
 __device__ void tail_jacobi(const TailLevel<T>& L, const T* x, const T* b, T* xn) {
   for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
-    T ri = b[i];
-    for (int k = L.arp[i]; k < L.arp[i + 1]; ++k) ri = sub_rn(ri, mul_rn(L.av[k], x[L.aci[k]]));
+    const T ri = tail_row<-1>(b[i], L.aci, L.av, x, L.arp[i], L.arp[i + 1]);
     xn[i] = add_rn(x[i], mul_rn(mul_rn(L.omega, L.invd[i]), ri));
   }
   __syncthreads();
 }
 
+// y: n doubles of shared memory, followed by room for the n x n factors
 template <typename T>
 __device__ void tail_lu_solve(const TailCoarse<T>& C, double* y) {
   const int n = C.n;
+  double* lu = y + ((n + 1) & ~1);
+  for (int t = threadIdx.x; t < n * n; t += blockDim.x) lu[t] = C.lu[t];
   for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = (double)C.b[i];
   __syncthreads();
   if (threadIdx.x == 0)
@@ -701,16 +747,16 @@ __device__ void tail_lu_solve(const TailCoarse<T>& C, double* y) {
     const double yj = y[j];
     if (yj != 0.0)
       for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x)
-        y[i] = __dsub_rn(y[i], __dmul_rn(yj, C.lu[(size_t)j * n + i]));
+        y[i] = __dsub_rn(y[i], __dmul_rn(yj, lu[(size_t)j * n + i]));
     __syncthreads();
   }
   for (int j = n - 1; j >= 0; --j) {
-    if (threadIdx.x == 0 && y[j] != 0.0) y[j] = __ddiv_rn(y[j], C.lu[(size_t)j * n + j]);
+    if (threadIdx.x == 0 && y[j] != 0.0) y[j] = __ddiv_rn(y[j], lu[(size_t)j * n + j]);
     __syncthreads();
     const double yj = y[j];
     if (yj != 0.0)
       for (int i = threadIdx.x; i < j; i += blockDim.x)
-        y[i] = __dsub_rn(y[i], __dmul_rn(yj, C.lu[(size_t)j * n + i]));
+        y[i] = __dsub_rn(y[i], __dmul_rn(yj, lu[(size_t)j * n + i]));
     __syncthreads();
   }
   for (int i = threadIdx.x; i < n; i += blockDim.x) C.x[i] = (T)y[i];
@@ -746,20 +792,14 @@ __device__ void tail_visit(const TailLevel<T>* lv, int l, int nl, const TailCoar
     }
   }
   if (!have_r) {
-    for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
-      T ax = T(0);
-      for (int k = L.arp[i]; k < L.arp[i + 1]; ++k) ax = add_rn(ax, mul_rn(L.av[k], x[L.aci[k]]));
-      L.r[i] = sub_rn(b[i], ax);
-    }
+    for (int i = threadIdx.x; i < L.n; i += blockDim.x)
+      L.r[i] = sub_rn(b[i], tail_row<1>(T(0), L.aci, L.av, x, L.arp[i], L.arp[i + 1]));
     __syncthreads();
   }
   const bool last = (l + 1 == nl);
   T* bn = last ? C.b : lv[l + 1].b;
-  for (int J = threadIdx.x; J < L.nc; J += blockDim.x) {
-    T acc = T(0);
-    for (int k = L.rrp[J]; k < L.rrp[J + 1]; ++k) acc = add_rn(acc, mul_rn(L.rv[k], L.r[L.rci[k]]));
-    bn[J] = acc;
-  }
+  for (int J = threadIdx.x; J < L.nc; J += blockDim.x)
+    bn[J] = tail_row<1>(T(0), L.rci, L.rv, L.r, L.rrp[J], L.rrp[J + 1]);
   __syncthreads();
   const T* xc;
   if (!last) {
@@ -770,11 +810,8 @@ __device__ void tail_visit(const TailLevel<T>* lv, int l, int nl, const TailCoar
     tail_lu_solve(C, y);
     xc = C.x;
   }
-  for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
-    T xi = x[i];
-    for (int k = L.prp[i]; k < L.prp[i + 1]; ++k) xi = add_rn(xi, mul_rn(L.pv[k], xc[L.pci[k]]));
-    x[i] = xi;
-  }
+  for (int i = threadIdx.x; i < L.n; i += blockDim.x)
+    x[i] = tail_row<1>(x[i], L.pci, L.pv, xc, L.prp[i], L.prp[i + 1]);
   __syncthreads();
   for (int s = 0; s < post; ++s) {
     tail_jacobi(L, x, b, t);
