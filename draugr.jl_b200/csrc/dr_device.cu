@@ -62,13 +62,12 @@ int pick_G(long long nnz, int n) {
   return G;
 }
 
-// Greedy packing of consecutive rows into tiles of at most kBlock/G rows
+// Greedy packing of consecutive rows into tiles of at most max_rows rows
 // and kTileCap nonzeros; a row longer than kTileCap is a tile of its own.
-std::vector<int> make_tiles(const std::vector<int>& rp, int n, int G) {
+std::vector<int> make_tiles(const std::vector<int>& rp, int n, int max_rows) {
   std::vector<int> tp;
-  tp.reserve(n / std::max(1, kBlock / G) + 2);
+  tp.reserve(n / std::max(1, max_rows) + 2);
   tp.push_back(0);
-  const int max_rows = kBlock / G;
   int r = 0;
   while (r < n) {
     int rows = 0, nz = 0;
@@ -87,46 +86,23 @@ std::vector<int> make_tiles(const std::vector<int>& rp, int n, int G) {
 
 static_assert(kTileCap == kRowTileCap, "host and device tile capacities differ");
 
-// Form of the row kernel for a CSR pattern: flat products when row lengths
-// are very uneven (a long row among short ones); one lane per row (ordered
-// sum) up to 32 entries per row on average; beyond that G lanes (about 8
-// entries each) with a shuffle-tree sum.
-void choose_row_form(const std::vector<int>& rp, int n, long long nnz, int& G, bool& flat,
-                     bool& ordered) {
-  G = 1;
-  flat = false;
-  ordered = true;
-  if (n <= 0) return;
-  int maxlen = 0;
-  for (int i = 0; i < n; ++i) maxlen = std::max(maxlen, rp[i + 1] - rp[i]);
-  const double avg = (double)nnz / (double)n;
-  if (maxlen > 64 && maxlen > 4.0 * avg) {
-    flat = true;
-    return;
-  }
-  if (avg <= 32.0) return;
-  ordered = false;
-  G = 8;
-  while (G < 32 && G * 8 < avg) G *= 2;
-}
-
-// Blocks of kBlock threads with `smem` dynamic shared memory that fit on one
+// Blocks of `nt` threads with `smem` dynamic shared memory that fit on one
 // SM at once, per kernel (queried once).
-int resident_blocks(const void* f, size_t smem) {
+int resident_blocks(const void* f, int nt, size_t smem) {
   static std::mutex mu;
   static std::unordered_map<const void*, int> cache;
   std::lock_guard<std::mutex> lk(mu);
   auto it = cache.find(f);
   if (it != cache.end()) return it->second;
   int nb = 0;
-  DR_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, f, kBlock, smem));
+  DR_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, f, nt, smem));
   nb = std::max(1, nb);
   cache.emplace(f, nb);
   return nb;
 }
 
 template <typename TA, class XL, class EP, bool DOT, class Fin>
-void launch_rows_impl(cudaStream_t st, int max_grid, int G, bool flat, bool ordered, int n, int ntiles,
+void launch_rows_impl(cudaStream_t st, int max_grid, const RowForm& f, int n, int ntiles,
                       const int* tp, const int* ts, const int* rp, const int* ci, const TA* av,
                       XL xl, EP ep, double* partials, unsigned* ticket, Fin fin) {
   if (n <= 0) {
@@ -140,20 +116,19 @@ void launch_rows_impl(cudaStream_t st, int max_grid, int G, bool flat, bool orde
   const size_t smem = tile_smem_bytes<TA>();
   counted();
   // one wave of resident blocks (registers and shared memory permitting)
-#define DR_LAUNCH(F, g, O)                                                                      \
-  do {                                                                                          \
-    auto kf = k_tile_rows<F, g, O, TA, XL, EP, DOT, Fin>;                                       \
-    const int grid = std::max(                                                                  \
-        1, std::min({ntiles, max_grid, g_nsm * resident_blocks((const void*)kf, smem)}));       \
-    kf<<<grid, kBlock, smem, st>>>(ntiles, tp, ts, rp, ci, av, xl, ep, partials, ticket, fin,   \
-                                   g_err);                                                      \
+#define DR_LAUNCH(F, g, O, NT, B)                                                                \
+  do {                                                                                           \
+    auto kf = k_tile_rows<F, g, O, NT, B, TA, XL, EP, DOT, Fin>;                                 \
+    const int grid = std::max(                                                                   \
+        1, std::min({ntiles, max_grid, g_nsm * resident_blocks((const void*)kf, NT, smem)}));    \
+    kf<<<grid, NT, smem, st>>>(ntiles, tp, ts, rp, ci, av, xl, ep, partials, ticket, fin, g_err); \
   } while (0)
-  if (flat) DR_LAUNCH(true, 1, true);
-  else if (G == 1) DR_LAUNCH(false, 1, true);
-  else if (G == 4 && ordered) DR_LAUNCH(false, 4, true);
-  else if (G == 8) DR_LAUNCH(false, 8, false);
-  else if (G == 16) DR_LAUNCH(false, 16, false);
-  else if (G == 32) DR_LAUNCH(false, 32, false);
+  if (f.flat) DR_LAUNCH(true, 1, true, 256, 8);
+  else if (f.G == 1 && f.nt == 128) DR_LAUNCH(false, 1, true, 128, 32);
+  else if (f.G == 1) DR_LAUNCH(false, 1, true, 256, 8);
+  else if (f.G == 8) DR_LAUNCH(false, 8, false, 256, 4);
+  else if (f.G == 16) DR_LAUNCH(false, 16, false, 256, 4);
+  else if (f.G == 32) DR_LAUNCH(false, 32, false, 256, 4);
   else fail("bad row form");
 #undef DR_LAUNCH
   DR_CK(cudaGetLastError());
@@ -161,7 +136,7 @@ void launch_rows_impl(cudaStream_t st, int max_grid, int G, bool flat, bool orde
 
 template <typename TA, class XL, class EP>
 void launch_rows(cudaStream_t st, int max_grid, const DevMat& M, const TA* av, XL xl, EP ep) {
-  launch_rows_impl<TA, XL, EP, false, FinStore>(st, max_grid, M.G, M.flat, M.ordered, M.n, M.ntiles, M.tp, M.ts,
+  launch_rows_impl<TA, XL, EP, false, FinStore>(st, max_grid, M.form, M.n, M.ntiles, M.tp, M.ts,
                                                 M.rp, M.ci, av, xl, ep, nullptr, nullptr,
                                                 FinStore{nullptr});
 }
@@ -169,7 +144,7 @@ void launch_rows(cudaStream_t st, int max_grid, const DevMat& M, const TA* av, X
 template <typename TA, class XL, class EP, class Fin>
 void launch_rows_dot(cudaStream_t st, int max_grid, const DevMat& M, const TA* av, XL xl, EP ep,
                      double* partials, unsigned* ticket, Fin fin) {
-  launch_rows_impl<TA, XL, EP, true, Fin>(st, max_grid, M.G, M.flat, M.ordered, M.n, M.ntiles, M.tp, M.ts, M.rp,
+  launch_rows_impl<TA, XL, EP, true, Fin>(st, max_grid, M.form, M.n, M.ntiles, M.tp, M.ts, M.rp,
                                           M.ci, av, xl, ep, partials, ticket, fin);
 }
 
@@ -243,8 +218,8 @@ DevHier::DevHier(const HostHierarchy& H, int device) {
       M.v = alloc<double>(ci.size() + 4);
       if (v) h2d(M.v, *v, st_);
       M.Ggs = pick_G(M.nnz, n);
-      choose_row_form(rp, n, M.nnz, M.G, M.flat, M.ordered);
-      std::vector<int> tiles = make_tiles(rp, n, M.flat ? 1 : M.G);
+      M.form = row_form(rp);
+      std::vector<int> tiles = make_tiles(rp, n, M.form.nt / M.form.G);
       std::vector<int> tstart(tiles.size());
       for (size_t t = 0; t < tiles.size(); ++t) tstart[t] = rp[tiles[t]];
       M.ntiles = (int)tiles.size() - 1;
@@ -530,7 +505,7 @@ bool DevHier::fused_rz_ok(const CycleOpts& o) const {
 
 template <typename T>
 T* DevHier::cycle_level(int l, T* x, const T* b, bool x_zero, const CycleOpts& o, T* ext,
-                        const double* rz_w, bool rz_first) {
+                        const double* rz_w, bool rz_first, bool x1_ready) {
   if (l >= 1 && l == tail_ && x == vecs<T>(l).xa) {
     const void* desc = sizeof(T) == 8 ? tail64_ : tail32_;
     TailCoarse<T> C{nc_, clu_, cpiv_, coarse_b<T>(), coarse_x<T>()};
@@ -549,7 +524,11 @@ T* DevHier::cycle_level(int l, T* x, const T* b, bool x_zero, const CycleOpts& o
   bool have_r = false;
   // pre-smoothing
   if (x_zero && jac && o.pre >= 1) {
-    if (o.pre == 1) {
+    if (o.pre == 1 && x1_ready) {
+      // x already holds the zero-guess Jacobi step (written by the restriction)
+      residual<T>(l, x, b, V.r, nullptr);
+      have_r = true;
+    } else if (o.pre == 1) {
       launch_rows(st_, max_grid_, A, mval<T>(A), XZeroJacobi<T>{b, invd<T>(L), om},
                   EpZeroJacobiResidual<T>{b, invd<T>(L), x, V.r, om});
       have_r = true;
@@ -571,12 +550,22 @@ T* DevHier::cycle_level(int l, T* x, const T* b, bool x_zero, const CycleOpts& o
   // restriction  b_{l+1} = Pᵀ r
   const bool last = (l + 1 == nlevels());
   T* bn = last ? coarse_b<T>() : vecs<T>(l + 1).b;
-  launch_rows(st_, max_grid_, L.R, mval<T>(L.R), XPlain<T>{V.r}, EpStore<T>{bn});
+  bool x1n = false;
+  if (!last && l + 1 != tail_ && o.pre == 1 &&
+      (L_[l + 1].smoother == SmootherKind::Jacobi || L_[l + 1].smoother == SmootherKind::L1Jacobi)) {
+    // the coarse level starts from zero with one Jacobi step: form it here
+    DevLevel& Ln = L_[l + 1];
+    launch_rows(st_, max_grid_, L.R, mval<T>(L.R), XPlain<T>{V.r},
+                EpStoreZeroJacobi<T>{bn, invd<T>(Ln), vecs<T>(l + 1).xa, (T)Ln.omega});
+    x1n = true;
+  } else {
+    launch_rows(st_, max_grid_, L.R, mval<T>(L.R), XPlain<T>{V.r}, EpStore<T>{bn});
+  }
   // coarse-grid correction
   T* xn;
   if (!last) {
     xn = vecs<T>(l + 1).xa;
-    xn = cycle_level<T>(l + 1, xn, bn, true, o, nullptr);
+    xn = cycle_level<T>(l + 1, xn, bn, true, o, nullptr, nullptr, false, x1n);
     if (o.w) xn = cycle_level<T>(l + 1, xn, bn, false, o, nullptr);
   } else {
     xn = coarse_x<T>();

@@ -20,19 +20,54 @@ long long kernel_launches();
 // order.
 constexpr int kRowTileCap = 2000;
 
+// Form of the row kernel (k_tile_rows) for a CSR pattern:
+//   flat    rows of very uneven length averaging at most 32 entries (a long
+//           row among short ones): products formed flat over each tile,
+//           then one thread per row sums them in column order;
+//   G = 1   one lane per row, rows summed in column order: batches of 8
+//           gathers with 256-thread blocks up to 12 entries per row on
+//           average, batches of 32 with 128-thread blocks up to 32;
+//   G > 1   longer rows: G = 8..32 lanes per row (about 8 entries each),
+//           summed in a fixed shuffle tree.
+struct RowForm {
+  int G = 1;
+  bool flat = false;
+  bool ordered = true;  // every row (up to the tile capacity) in column order
+  int nt = 256;         // threads per block
+  int batch = 8;        // gathers in flight per lane (G = 1)
+};
+
+inline RowForm row_form(const std::vector<int>& rp) {
+  RowForm f;
+  const size_t n = rp.size() ? rp.size() - 1 : 0;
+  if (n == 0) return f;
+  int maxlen = 0;
+  for (size_t i = 0; i < n; ++i) maxlen = std::max(maxlen, rp[i + 1] - rp[i]);
+  const double avg = (double)(rp[n] - rp[0]) / (double)n;
+  if (avg <= 32.0 && maxlen > 64 && maxlen > 4.0 * avg) {
+    f.flat = true;
+  } else if (avg <= 32.0) {
+    if (avg > 12.0) {
+      f.nt = 128;
+      f.batch = 32;
+    }
+  } else {
+    f.ordered = false;
+    f.G = 8;
+    while (f.G < 32 && f.G * 8 < avg) f.G *= 2;
+  }
+  return f;
+}
+
 // 1 when the row kernel reduces every row of the CSR pattern in column
-// order (the reference's order, bit for bit): rows average at most 32
-// entries (or are very uneven, which selects the flat form) and none
-// exceeds the tile capacity.  Mirrors choose_row_form in dr_device.cu.
+// order (the reference's order, bit for bit): an ordered form and no row
+// longer than the tile capacity.
 inline int rows_in_order(const std::vector<int>& rp) {
   const size_t n = rp.size() ? rp.size() - 1 : 0;
   if (n == 0) return 1;
   int maxlen = 0;
   for (size_t i = 0; i < n; ++i) maxlen = std::max(maxlen, rp[i + 1] - rp[i]);
-  if (maxlen > kRowTileCap) return 0;
-  const double avg = (double)(rp[n] - rp[0]) / (double)n;
-  if (maxlen > 64 && maxlen > 4.0 * avg) return 1;
-  return avg <= 32.0 ? 1 : 0;
+  return (maxlen <= kRowTileCap && row_form(rp).ordered) ? 1 : 0;
 }
 
 // Sparse matrix on the device: CSR pattern, FP64 values and (after the first
@@ -45,9 +80,7 @@ struct DevMat {
   int* ci = nullptr;
   double* v = nullptr;
   float* v32 = nullptr;
-  int G = 1;          // lanes per row of the row kernel's row-gather form
-  bool flat = false;  // row kernel forms products flat over each tile
-  bool ordered = true;  // rows summed in column order (the reference's)
+  RowForm form;       // form of the row kernel
   int Ggs = 8;        // lanes per row of the Gauss-Seidel colour kernel
   int ntiles = 0;     // row tiles (see k_tile_rows)
   int* tp = nullptr;  // tile row starts, ntiles+1
@@ -141,10 +174,11 @@ class DevHier {
 
   // rz_w: when set (finest level only), the last Jacobi sweep also forms
   // r·z with r = rz_w and stores it like the PCG's r·z (rz_first: first
-  // application, else shift the previous value to "old").
+  // application, else shift the previous value to "old").  x1_ready: x
+  // already holds the zero-guess Jacobi step (formed by the restriction).
   template <typename T>
   T* cycle_level(int l, T* x, const T* b, bool x_zero, const CycleOpts& o, T* ext_partner,
-                 const double* rz_w = nullptr, bool rz_first = false);
+                 const double* rz_w = nullptr, bool rz_first = false, bool x1_ready = false);
   template <typename T>
   T* smooth(int l, T* x, const T* b, int steps, T* ext_partner, const double* rz_w = nullptr,
             bool rz_first = false);

@@ -210,6 +210,28 @@ struct EpZeroJacobiResidual {  // x1 = (ω·invd)·b ; r = b - A x1
   }
 };
 
+// Restriction that also starts the coarse level's smoothing: b = Pᵀ r and
+// the first weighted-Jacobi step from a zero guess, x1 = (ω·invd)·b, so the
+// coarse level's first kernel is a plain residual r = b - A x1 with one
+// gather per entry (the same values as XZeroJacobi forms on the fly).
+template <typename T>
+struct EpStoreZeroJacobi {
+  using acc_t = T;
+  static constexpr int kSign = 1;
+  struct Pre { T d; };
+  T* __restrict__ b;
+  const T* __restrict__ invd;
+  T* __restrict__ x1;
+  T omega;
+  __device__ __forceinline__ Pre pre(int i) const { return {__ldg(invd + i)}; }
+  __device__ __forceinline__ T init(const Pre&) const { return T(0); }
+  __device__ __forceinline__ double apply(int i, T v, const Pre& p) const {
+    b[i] = v;
+    x1[i] = mul_rn(mul_rn(omega, p.d), v);
+    return 0.0;
+  }
+};
+
 template <typename T>
 struct EpAddTo {  // x += p xc, per entry                  (prolongation.jl:742-760)
   using acc_t = T;
@@ -287,7 +309,7 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 
 // ------------------------------------------------------------ row kernel
 // Rows are packed (on the host, once per matrix) into tiles of at most
-// kBlock/G consecutive rows holding at most kTileCap nonzeros; tp[t] is the
+// NT/G consecutive rows holding at most kTileCap nonzeros; tp[t] is the
 // first row and ts[t] the first nonzero of tile t.  Each block walks the
 // tiles blockIdx.x, +gridDim.x, ... with two shared-memory stages: while it
 // works on one tile, the TMA engine copies the column and value arrays of
@@ -296,7 +318,10 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 // operands (row bounds, epilogue inputs) are loaded one tile ahead into
 // registers.  Two ways to form the products a_ij·x_j (x is L2-resident):
 //   row-gather (FLAT = false): G lanes per row gather their entries of the
-//     row, up to eight per lane at once (uniform rows: every lane busy);
+//     row, B at once with one lane per row (8 for short rows; 32 with
+//     128-thread blocks for rows of 12-32 entries, so that one L2 round trip
+//     covers a row and the freed registers keep the same blocks resident),
+//     4 per lane with G > 1 (uniform rows: every lane busy);
 //   flat (FLAT = true, one row per thread): the whole block walks the tile's
 //     nonzeros flat, so a long row among short ones costs no more than its
 //     share (rows of very uneven length, e.g. the restriction Pᵀ).
@@ -310,7 +335,6 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 // by the whole block straight from global memory (tree order).
 constexpr int kTileCap = 2000;
 constexpr int kStageEntries = 2008;  // kTileCap + alignment slack, a multiple of 4 entries
-constexpr int kFlatIters = (kTileCap + kBlock - 1) / kBlock;
 constexpr int kWaitLimit = 1 << 22;
 
 // Dynamic shared memory of k_tile_rows: two stages of columns and values
@@ -326,14 +350,16 @@ __device__ __forceinline__ void bind_epilogue(EP&) {}
 template <typename T>
 __device__ __forceinline__ void bind_epilogue(EpPcgDir<T>& e) { e.bind(); }
 
-template <bool FLAT, int G, bool ORDERED, typename TA, class XL, class EP, bool DOT, class Fin>
-__global__ void __launch_bounds__(kBlock)
+template <bool FLAT, int G, bool ORDERED, int NT, int B, typename TA, class XL, class EP, bool DOT,
+          class Fin>
+__global__ void __launch_bounds__(NT)
 k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
             const int* __restrict__ rp, const int* __restrict__ ci, const TA* __restrict__ av,
             XL xl, EP ep, double* partials, unsigned* ticket, Fin fin, int* err) {
   using acc_t = typename EP::acc_t;
   static_assert(sizeof(acc_t) == sizeof(TA), "products are stored over the staged values");
   static_assert(!FLAT || G == 1, "the flat form uses one row per thread");
+  constexpr int kFlatIters = (kTileCap + NT - 1) / NT;
   using Pre = typename EP::Pre;
   bind_loader(xl);
   bind_epilogue(ep);
@@ -430,12 +456,12 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
         acc_t p[kFlatIters];
 #pragma unroll
         for (int j = 0; j < kFlatIters; ++j) {
-          const int k = threadIdx.x + j * kBlock;
+          const int k = threadIdx.x + j * NT;
           p[j] = (k < len) ? (acc_t)xl(cs[k]) : acc_t(0);
         }
 #pragma unroll
         for (int j = 0; j < kFlatIters; ++j) {
-          const int k = threadIdx.x + j * kBlock;
+          const int k = threadIdx.x + j * NT;
           if (k < len) vs[k] = (TA)mul_rn((acc_t)vs[k], p[j]);
         }
         __syncthreads();
@@ -450,13 +476,13 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
       } else if constexpr (G == 1) {
         if (valid) {
           acc_t a = ep.init(pr);
-          for (int k0 = rs; k0 < re; k0 += 8) {
-            acc_t p[8];
+          for (int k0 = rs; k0 < re; k0 += B) {
+            acc_t p[B];
 #pragma unroll
-            for (int j = 0; j < 8; ++j)
+            for (int j = 0; j < B; ++j)
               p[j] = (k0 + j < re) ? mul_rn((acc_t)vs[k0 + j], (acc_t)xl(cs[k0 + j])) : acc_t(0);
 #pragma unroll
-            for (int j = 0; j < 8; ++j)
+            for (int j = 0; j < B; ++j)
               if (k0 + j < re) {
                 if constexpr (EP::kSign > 0) a = add_rn(a, p[j]);
                 else a = sub_rn(a, p[j]);
@@ -513,14 +539,14 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
     } else {
       // a single row longer than the tile capacity, from global memory
       acc_t sum = acc_t(0);
-      for (int k = s + threadIdx.x; k < e; k += kBlock)
+      for (int k = s + threadIdx.x; k < e; k += NT)
         sum = add_rn(sum, mul_rn((acc_t)__ldg(av + k), (acc_t)xl(__ldg(ci + k))));
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
       if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sum;
       __syncthreads();
       if (threadIdx.x < 32) {
-        sum = threadIdx.x < (kBlock >> 5) ? red[threadIdx.x] : acc_t(0);
+        sum = threadIdx.x < (NT >> 5) ? red[threadIdx.x] : acc_t(0);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
         if (threadIdx.x == 0) {
