@@ -126,8 +126,8 @@ void launch_rows_impl(cudaStream_t st, int max_grid, const RowForm& f, int n, in
   if (f.flat) DR_LAUNCH(true, 1, true, 256, 8);
   else if (f.G == 1 && f.nt == 128) DR_LAUNCH(false, 1, true, 128, 32);
   else if (f.G == 1) DR_LAUNCH(false, 1, true, 256, 8);
-  else if (f.G == 8) DR_LAUNCH(false, 8, false, 256, 4);
-  else if (f.G == 16) DR_LAUNCH(false, 16, false, 256, 4);
+  else if (f.G == 8) DR_LAUNCH(false, 8, false, 256, 12);
+  else if (f.G == 16) DR_LAUNCH(false, 16, false, 256, 12);
   else if (f.G == 32) DR_LAUNCH(false, 32, false, 256, 4);
   else fail("bad row form");
 #undef DR_LAUNCH

@@ -27,8 +27,10 @@ constexpr int kRowTileCap = 2000;
 //   G = 1   one lane per row, rows summed in column order: batches of 8
 //           gathers with 256-thread blocks up to 12 entries per row on
 //           average, batches of 32 with 128-thread blocks up to 32;
-//   G > 1   longer rows: G = 8..32 lanes per row (about 8 entries each),
-//           summed in a fixed shuffle tree.
+//   G > 1   longer rows, summed by G lanes and a fixed shuffle tree: 8 or
+//           16 lanes gathering 12 entries each at once (about 27 or 13
+//           rows fill a tile), or 32 lanes with 4 each when a few rows are
+//           much longer than the rest.
 struct RowForm {
   int G = 1;
   bool flat = false;
@@ -53,8 +55,13 @@ inline RowForm row_form(const std::vector<int>& rp) {
     }
   } else {
     f.ordered = false;
-    f.G = 8;
-    while (f.G < 32 && f.G * 8 < avg) f.G *= 2;
+    if (maxlen > 4.0 * avg) {
+      f.G = 32;  // a few long rows set each tile's time: many lanes per row
+      f.batch = 4;
+    } else {
+      f.G = avg <= 100 ? 8 : 16;  // full tiles, a row in one round of gathers
+      f.batch = 12;
+    }
   }
   return f;
 }

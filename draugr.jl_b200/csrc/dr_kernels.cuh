@@ -261,6 +261,13 @@ struct EpPcgDir {  // q = A p, p_new = z + β p_old, returns p_new·q
   }
 };
 
+// Warp barrier among the lanes executing together at this point: placed
+// between a batch of independent gathers and their first use, it makes the
+// compiler issue the whole batch first (without it, gathers whose indices
+// come from shared memory are scheduled next to their uses, a few in flight
+// at a time).  Every lane of the mask reaches it (no branch in between).
+__device__ __forceinline__ void issue_fence() { __syncwarp(__activemask()); }
+
 // ------------------------------------------------------------ TMA / mbarrier
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -321,7 +328,7 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 //     row, B at once with one lane per row (8 for short rows; 32 with
 //     128-thread blocks for rows of 12-32 entries, so that one L2 round trip
 //     covers a row and the freed registers keep the same blocks resident),
-//     4 per lane with G > 1 (uniform rows: every lane busy);
+//     12 (or 4 when a few rows are much longer) per lane with G > 1;
 //   flat (FLAT = true, one row per thread): the whole block walks the tile's
 //     nonzeros flat, so a long row among short ones costs no more than its
 //     share (rows of very uneven length, e.g. the restriction Pᵀ).
@@ -477,15 +484,18 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
         if (valid) {
           acc_t a = ep.init(pr);
           for (int k0 = rs; k0 < re; k0 += B) {
-            acc_t p[B];
+            // all B gathers issued unconditionally (slots past the row end
+            // repeat its last column, in bounds), then the ordered sum
+            acc_t xv[B];
 #pragma unroll
-            for (int j = 0; j < B; ++j)
-              p[j] = (k0 + j < re) ? mul_rn((acc_t)vs[k0 + j], (acc_t)xl(cs[k0 + j])) : acc_t(0);
+            for (int j = 0; j < B; ++j) xv[j] = (acc_t)xl(cs[min(k0 + j, re - 1)]);
+            issue_fence();
 #pragma unroll
             for (int j = 0; j < B; ++j)
               if (k0 + j < re) {
-                if constexpr (EP::kSign > 0) a = add_rn(a, p[j]);
-                else a = sub_rn(a, p[j]);
+                const acc_t p = mul_rn((acc_t)vs[k0 + j], xv[j]);
+                if constexpr (EP::kSign > 0) a = add_rn(a, p);
+                else a = sub_rn(a, p);
               }
           }
           dacc += ep.apply(row, a, pr);
@@ -517,15 +527,16 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
       } else {
         // long rows: G lanes sum strided products, then a fixed shuffle tree
         acc_t sum = acc_t(0);
-        for (int k0 = rs + lane; k0 < re; k0 += 4 * G) {
-          acc_t p[4];
+        for (int k0 = rs + lane; k0 < re; k0 += B * G) {
+          acc_t xv[B];
 #pragma unroll
-          for (int j = 0; j < 4; ++j) {
+          for (int j = 0; j < B; ++j) xv[j] = (acc_t)xl(cs[min(k0 + j * G, re - 1)]);
+          issue_fence();
+#pragma unroll
+          for (int j = 0; j < B; ++j) {
             const int k = k0 + j * G;
-            p[j] = (k < re) ? mul_rn((acc_t)vs[k], (acc_t)xl(cs[k])) : acc_t(0);
+            if (k < re) sum = add_rn(sum, mul_rn((acc_t)vs[k], xv[j]));
           }
-#pragma unroll
-          for (int j = 0; j < 4; ++j) sum = add_rn(sum, p[j]);
         }
 #pragma unroll
         for (int o = G >> 1; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
