@@ -172,7 +172,9 @@ enum : int { SC_BB = 0, SC_RR = 1, SC_RZ = 2, SC_RZOLD = 3, SC_PQ = 4, SC_TMP = 
 template <typename T>
 T* DevHier::alloc(size_t n) {
   void* p = nullptr;
-  size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+  // a multiple of 16 bytes, so a 16-byte-rounded bulk copy of any prefix of
+  // the array stays inside the allocation
+  size_t bytes = (std::max<size_t>(n, 1) * sizeof(T) + 15) & ~(size_t)15;
   DR_CK(cudaMalloc(&p, bytes));
   allocs_.push_back(p);
   bytes_ += bytes;
@@ -363,32 +365,59 @@ void DevHier::ensure_fp32() {
   build_tail();
 }
 
-// Levels from the first one with at most kTailRows rows (and below it only
-// such levels, all with Jacobi-type smoothers) down to the coarsest run in
-// one block; never the finest level (its iterate is the caller's buffer).
-static constexpr int kTailRows = 512;
+// Levels whose operands fit in the tail kernel's shared memory (all of them
+// together, FP64 values, at most kTailSmem bytes), with Jacobi-type
+// smoothers, from the coarsest up, run in one block (k_coarse_tail); never
+// the finest level (its iterate is the caller's buffer).
+static constexpr size_t kTailSmem = 200 * 1024;
+
+static size_t a16(size_t b) { return (b + 15) & ~(size_t)15; }
+
+template <typename T>
+static size_t tail_level_bytes(const DevLevel& d) {
+  const size_t n = d.A.n, nc = d.P.m, an = d.A.nnz, pn = d.P.nnz;
+  return a16(4 * (n + 1)) + a16(4 * an) + a16(sizeof(T) * an) + a16(sizeof(T) * n) +
+         a16(4 * (n + 1)) + a16(4 * pn) + a16(sizeof(T) * pn) + a16(4 * (nc + 1)) + a16(4 * pn) +
+         a16(sizeof(T) * pn) + 4 * a16(sizeof(T) * n);
+}
+
+template <typename T>
+static size_t tail_coarse_bytes(int nc) {
+  return a16(8 * ((size_t)nc * nc + nc)) + a16(4 * (size_t)nc) + 2 * a16(sizeof(T) * nc);
+}
 
 void DevHier::build_tail() {
   const int nl = nlevels();
   tail_ = nl;
-  if ((size_t)(nc_ + 2) * (nc_ + 1) * sizeof(double) > 40 * 1024) return;  // y and LU in shared memory
-  for (int l = nl - 1; l >= 1; --l) {
+  size_t total = tail_coarse_bytes<double>(nc_);
+  for (int l = nl - 1; l >= 1 && nl - l <= kern::kTailMaxLevels; --l) {
     const DevLevel& d = L_[l];
     const bool jac = d.smoother == SmootherKind::Jacobi || d.smoother == SmootherKind::L1Jacobi;
-    if (d.A.n > kTailRows || !jac) break;
+    total += tail_level_bytes<double>(d);
+    if (!jac || total > kTailSmem) break;
     tail_ = l;
   }
   if (tail_ >= nl) return;
   const int cnt = nl - tail_;
   auto make = [&](auto tag) {
     using T = decltype(tag);
+    const int slot = sizeof(T) == 8 ? 0 : 1;
     std::vector<TailLevel<T>> v(cnt);
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+      const unsigned o = (unsigned)off;
+      off += a16(bytes);
+      return o;
+    };
     for (int k = 0; k < cnt; ++k) {
       DevLevel& d = L_[tail_ + k];
       LevelVecs<T>& V = vecs<T>(tail_ + k);
       TailLevel<T>& t = v[k];
+      const size_t n = d.A.n, nc = d.P.m;
       t.n = d.A.n;
       t.nc = d.P.m;
+      t.annz = (int)d.A.nnz;
+      t.pnnz = (int)d.P.nnz;
       t.arp = d.A.rp;
       t.aci = d.A.ci;
       t.av = mval<T>(d.A);
@@ -404,7 +433,27 @@ void DevHier::build_tail() {
       t.xb = V.xb;
       t.b = V.b;
       t.r = V.r;
+      t.o_arp = take(4 * (n + 1));
+      t.o_aci = take(4 * (size_t)d.A.nnz);
+      t.o_av = take(sizeof(T) * (size_t)d.A.nnz);
+      t.o_invd = take(sizeof(T) * n);
+      t.o_prp = take(4 * (n + 1));
+      t.o_pci = take(4 * (size_t)d.P.nnz);
+      t.o_pv = take(sizeof(T) * (size_t)d.P.nnz);
+      t.o_rrp = take(4 * (nc + 1));
+      t.o_rci = take(4 * (size_t)d.P.nnz);
+      t.o_rv = take(sizeof(T) * (size_t)d.P.nnz);
+      t.o_xa = take(sizeof(T) * n);
+      t.o_xb = take(sizeof(T) * n);
+      t.o_b = take(sizeof(T) * n);
+      t.o_r = take(sizeof(T) * n);
     }
+    tail_co_[slot][0] = take(8 * ((size_t)nc_ * nc_ + nc_));
+    tail_co_[slot][1] = take(4 * (size_t)nc_);
+    tail_co_[slot][2] = take(sizeof(T) * (size_t)nc_);
+    tail_co_[slot][3] = take(sizeof(T) * (size_t)nc_);
+    tail_bytes_[slot] = off;
+    DR_CK(cudaFuncSetAttribute(k_coarse_tail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)off));
     TailLevel<T>* dst = alloc<TailLevel<T>>(cnt);
     DR_CK(cudaMemcpy(dst, v.data(), cnt * sizeof(TailLevel<T>), cudaMemcpyHostToDevice));
     return (void*)dst;
@@ -508,11 +557,13 @@ T* DevHier::cycle_level(int l, T* x, const T* b, bool x_zero, const CycleOpts& o
                         const double* rz_w, bool rz_first, bool x1_ready) {
   if (l >= 1 && l == tail_ && x == vecs<T>(l).xa) {
     const void* desc = sizeof(T) == 8 ? tail64_ : tail32_;
-    TailCoarse<T> C{nc_, clu_, cpiv_, coarse_b<T>(), coarse_x<T>()};
+    const int slot = sizeof(T) == 8 ? 0 : 1;
+    TailCoarse<T> C{nc_, clu_, cpiv_, coarse_b<T>(), coarse_x<T>(), tail_co_[slot][0], tail_co_[slot][1],
+                    tail_co_[slot][2], tail_co_[slot][3]};
     counted();
-    k_coarse_tail<T><<<1, 1024, (size_t)(((nc_ + 1) & ~1) + (size_t)nc_ * nc_) * sizeof(double), st_>>>(
+    k_coarse_tail<T><<<1, kern::kTailThreads, tail_bytes_[slot], st_>>>(
         static_cast<const TailLevel<T>*>(desc), nlevels() - l, C, o.pre, o.post, o.w ? 1 : 0,
-        x_zero ? 1 : 0);
+        x_zero ? 1 : 0, g_err);
     DR_CK(cudaGetLastError());
     return x;
   }

@@ -203,6 +203,8 @@ class DevHier {
   int tail_ = 0;
   void* tail64_ = nullptr;   // device TailLevel<double>[nlevels - tail_]
   void* tail32_ = nullptr;   // device TailLevel<float>[...] once FP32 buffers exist
+  size_t tail_bytes_[2] = {0, 0};        // shared memory of the tail kernel (FP64, FP32)
+  unsigned tail_co_[2][4] = {{0}, {0}};  // its coarsest-system offsets (TailCoarse)
   void graphs_clear();
   double dot_host(const double* a, const double* b, int n);
 

@@ -711,15 +711,19 @@ __global__ void k_lu_solve(int n, const double* __restrict__ lu, const int* __re
 }
 
 // ------------------------------------------------------------ coarse tail
-// The cycle from one small level down to the coarsest, in one block: every
-// phase (smoothing, residual, restriction, coarsest solve, prolongation) is
-// a loop over rows by the block's threads, one thread per row summing in
-// column order (the reference's order), separated by block barriers.  This
-// replaces about four kernel launches per level on levels whose work is a
-// few microseconds, where launch and drain latency would dominate.
+// The cycle from one small level down to the coarsest, in one block that
+// first copies every operand of those levels (matrices, inverse diagonals,
+// P and Pᵀ, the LU factors) into shared memory and then runs every phase
+// (smoothing, residual, restriction, coarsest solve, prolongation) from
+// there: a loop over rows by the block's threads, one thread per row
+// summing in column order (the reference's order), separated by block
+// barriers.  This replaces about four launches per level on levels whose
+// work is a few microseconds, where launch and drain latency dominate.
+// Only the top level's right-hand side (and iterate, when it does not start
+// at zero) is read from global memory, and only its result is written back.
 template <typename T>
 struct TailLevel {
-  int n, nc;
+  int n, nc, annz, pnnz;
   const int *arp, *aci;
   const T *av, *invd;
   T omega;
@@ -728,6 +732,8 @@ struct TailLevel {
   const int *rrp, *rci;
   const T* rv;
   T *xa, *xb, *b, *r;  // iterate pair, right-hand side, residual
+  // byte offsets of the shared-memory copies (arrays above, in order)
+  unsigned o_arp, o_aci, o_av, o_invd, o_prp, o_pci, o_pv, o_rrp, o_rci, o_rv, o_xa, o_xb, o_b, o_r;
 };
 
 template <typename T>
@@ -736,7 +742,12 @@ struct TailCoarse {
   const double* lu;
   const int* piv;
   T *b, *x;
+  // shared-memory offsets (bytes): factors followed by n doubles of work
+  // space, pivots, right-hand side, solution
+  unsigned o_lu, o_piv, o_b, o_x;
 };
+
+constexpr int kTailMaxLevels = 8;
 
 // a ± Σ_k v[k]·x[c[k]] over [s, e) in column order, eight loads in flight
 template <int SIGN, typename T>
@@ -762,12 +773,43 @@ __device__ void tail_jacobi(const TailLevel<T>& L, const T* x, const T* b, T* xn
   __syncthreads();
 }
 
-// y: n doubles of shared memory, followed by room for the n x n factors
+// Coarsest solve with the (shared-memory) LU factors, getrs order: row
+// interchanges, then L (unit diagonal) and U substitutions by columns, a
+// column's update skipped when its solution entry is zero.  Up to 32
+// unknowns one warp holds y in registers (lane i: y_i); larger systems use
+// the block with y in shared memory after the factors.
 template <typename T>
-__device__ void tail_lu_solve(const TailCoarse<T>& C, double* y) {
+__device__ void tail_lu_solve(const TailCoarse<T>& C) {
   const int n = C.n;
-  double* lu = y + ((n + 1) & ~1);
-  for (int t = threadIdx.x; t < n * n; t += blockDim.x) lu[t] = C.lu[t];
+  const double* lu = C.lu;
+  if (n <= 32) {
+    if (threadIdx.x < 32) {
+      const int i = threadIdx.x;
+      double y = i < n ? (double)C.b[i] : 0.0;
+      for (int j = 0; j < n; ++j) {
+        const int p = C.piv[j];
+        if (p != j) {
+          const double a = __shfl_sync(0xffffffffu, y, j);
+          const double c = __shfl_sync(0xffffffffu, y, p);
+          if (i == j) y = c;
+          if (i == p) y = a;
+        }
+      }
+      for (int j = 0; j < n; ++j) {
+        const double yj = __shfl_sync(0xffffffffu, y, j);
+        if (yj != 0.0 && i > j && i < n) y = __dsub_rn(y, __dmul_rn(yj, lu[(size_t)j * n + i]));
+      }
+      for (int j = n - 1; j >= 0; --j) {
+        if (i == j && y != 0.0) y = __ddiv_rn(y, lu[(size_t)j * n + j]);
+        const double yj = __shfl_sync(0xffffffffu, y, j);
+        if (yj != 0.0 && i < j) y = __dsub_rn(y, __dmul_rn(yj, lu[(size_t)j * n + i]));
+      }
+      if (i < n) C.x[i] = (T)y;
+    }
+    __syncthreads();
+    return;
+  }
+  double* y = const_cast<double*>(lu) + (size_t)n * n;
   for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = (double)C.b[i];
   __syncthreads();
   if (threadIdx.x == 0)
@@ -804,14 +846,13 @@ __device__ void tail_lu_solve(const TailCoarse<T>& C, double* y) {
 // ends in L.xa.  Levels l+1 .. nl-1 follow in `lv`; the coarsest system is C.
 template <typename T>
 __device__ void tail_visit(const TailLevel<T>* lv, int l, int nl, const TailCoarse<T>& C,
-                           bool x_zero, int pre, int post, int wcycle, double* y) {
+                           bool x_zero, int pre, int post, int wcycle) {
   const TailLevel<T>& L = lv[l];
   T* x = L.xa;
   T* t = L.xb;
   const T* b = L.b;
-  bool have_r = false;
   if (x_zero && pre >= 1) {
-    // first Jacobi step from zero, residual of its result
+    // first Jacobi step from zero
     for (int i = threadIdx.x; i < L.n; i += blockDim.x) x[i] = mul_rn(mul_rn(L.omega, L.invd[i]), b[i]);
     __syncthreads();
     for (int s = 1; s < pre; ++s) {
@@ -828,11 +869,9 @@ __device__ void tail_visit(const TailLevel<T>* lv, int l, int nl, const TailCoar
       T* u = x; x = t; t = u;
     }
   }
-  if (!have_r) {
-    for (int i = threadIdx.x; i < L.n; i += blockDim.x)
-      L.r[i] = sub_rn(b[i], tail_row<1>(T(0), L.aci, L.av, x, L.arp[i], L.arp[i + 1]));
-    __syncthreads();
-  }
+  for (int i = threadIdx.x; i < L.n; i += blockDim.x)
+    L.r[i] = sub_rn(b[i], tail_row<1>(T(0), L.aci, L.av, x, L.arp[i], L.arp[i + 1]));
+  __syncthreads();
   const bool last = (l + 1 == nl);
   T* bn = last ? C.b : lv[l + 1].b;
   for (int J = threadIdx.x; J < L.nc; J += blockDim.x)
@@ -840,11 +879,11 @@ __device__ void tail_visit(const TailLevel<T>* lv, int l, int nl, const TailCoar
   __syncthreads();
   const T* xc;
   if (!last) {
-    tail_visit(lv, l + 1, nl, C, true, pre, post, wcycle, y);
-    if (wcycle) tail_visit(lv, l + 1, nl, C, false, pre, post, wcycle, y);
+    tail_visit(lv, l + 1, nl, C, true, pre, post, wcycle);
+    if (wcycle) tail_visit(lv, l + 1, nl, C, false, pre, post, wcycle);
     xc = lv[l + 1].xa;
   } else {
-    tail_lu_solve(C, y);
+    tail_lu_solve(C);
     xc = C.x;
   }
   for (int i = threadIdx.x; i < L.n; i += blockDim.x)
@@ -860,12 +899,96 @@ __device__ void tail_visit(const TailLevel<T>* lv, int l, int nl, const TailCoar
   }
 }
 
+constexpr int kTailThreads = 256;
+
+// lv: nl (<= kTailMaxLevels) descriptors with global pointers and the
+// shared-memory layout; dynamic shared memory holds that layout.  Every
+// source array starts an allocation whose size is a multiple of 16 bytes
+// and every destination is 16-byte aligned, so each array arrives by one
+// bulk copy (TMA) rounded up to 16 bytes, all of them on one mbarrier.  A
+// copy that does not complete within the wait limit sets *err and the block
+// returns without touching global memory.
 template <typename T>
-__global__ void __launch_bounds__(1024)
-k_coarse_tail(const TailLevel<T>* lv, int nl, TailCoarse<T> C, int pre, int post, int wcycle,
-              int x_zero) {
-  extern __shared__ double ysh[];
-  tail_visit(lv, 0, nl, C, x_zero != 0, pre, post, wcycle, ysh);
+__global__ void __launch_bounds__(kTailThreads)
+k_coarse_tail(const TailLevel<T>* __restrict__ lv, int nl, TailCoarse<T> C, int pre, int post,
+              int wcycle, int x_zero, int* err) {
+  extern __shared__ __align__(16) unsigned char tsm[];
+  __shared__ TailLevel<T> sl[kTailMaxLevels];
+  __shared__ TailCoarse<T> sc;
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int ok;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+    // every array of the tail: (shared-memory offset, source, bytes)
+    auto each = [&](auto&& f) {
+      for (int k = 0; k < nl; ++k) {
+        const TailLevel<T>& g = lv[k];
+        f(g.o_arp, g.arp, 4 * (size_t)(g.n + 1));
+        f(g.o_aci, g.aci, 4 * (size_t)g.annz);
+        f(g.o_av, g.av, sizeof(T) * (size_t)g.annz);
+        f(g.o_invd, g.invd, sizeof(T) * (size_t)g.n);
+        f(g.o_prp, g.prp, 4 * (size_t)(g.n + 1));
+        f(g.o_pci, g.pci, 4 * (size_t)g.pnnz);
+        f(g.o_pv, g.pv, sizeof(T) * (size_t)g.pnnz);
+        f(g.o_rrp, g.rrp, 4 * (size_t)(g.nc + 1));
+        f(g.o_rci, g.rci, 4 * (size_t)g.pnnz);
+        f(g.o_rv, g.rv, sizeof(T) * (size_t)g.pnnz);
+      }
+      f(C.o_lu, C.lu, 8 * (size_t)C.n * C.n);
+      f(C.o_piv, C.piv, 4 * (size_t)C.n);
+      // the top level's right-hand side (and iterate, unless it starts at zero)
+      f(lv[0].o_b, lv[0].b, sizeof(T) * (size_t)lv[0].n);
+      if (!x_zero) f(lv[0].o_xa, lv[0].xa, sizeof(T) * (size_t)lv[0].n);
+    };
+    uint32_t total = 0;
+    each([&](unsigned, const void*, size_t b) { total += (uint32_t)((b + 15) & ~(size_t)15); });
+    mbar_expect_tx(&bar, total);
+    each([&](unsigned off, const void* src, size_t b) {
+      if (b) bulk_g2s(tsm + off, src, (uint32_t)((b + 15) & ~(size_t)15), &bar);
+    });
+  }
+  if (threadIdx.x < nl) {
+    const TailLevel<T> g = lv[threadIdx.x];
+    TailLevel<T> v = g;
+    v.arp = reinterpret_cast<const int*>(tsm + g.o_arp);
+    v.aci = reinterpret_cast<const int*>(tsm + g.o_aci);
+    v.av = reinterpret_cast<const T*>(tsm + g.o_av);
+    v.invd = reinterpret_cast<const T*>(tsm + g.o_invd);
+    v.prp = reinterpret_cast<const int*>(tsm + g.o_prp);
+    v.pci = reinterpret_cast<const int*>(tsm + g.o_pci);
+    v.pv = reinterpret_cast<const T*>(tsm + g.o_pv);
+    v.rrp = reinterpret_cast<const int*>(tsm + g.o_rrp);
+    v.rci = reinterpret_cast<const int*>(tsm + g.o_rci);
+    v.rv = reinterpret_cast<const T*>(tsm + g.o_rv);
+    v.xa = reinterpret_cast<T*>(tsm + g.o_xa);
+    v.xb = reinterpret_cast<T*>(tsm + g.o_xb);
+    v.b = reinterpret_cast<T*>(tsm + g.o_b);
+    v.r = reinterpret_cast<T*>(tsm + g.o_r);
+    sl[threadIdx.x] = v;
+  }
+  if (threadIdx.x == 32) {
+    TailCoarse<T> c = C;
+    c.lu = reinterpret_cast<const double*>(tsm + C.o_lu);
+    c.piv = reinterpret_cast<const int*>(tsm + C.o_piv);
+    c.b = reinterpret_cast<T*>(tsm + C.o_b);
+    c.x = reinterpret_cast<T*>(tsm + C.o_x);
+    sc = c;
+  }
+  if (threadIdx.x == 0) ok = 1;
+  __syncthreads();  // barrier initialised, views published
+  if (!mbar_wait_bounded(&bar, 0, kWaitLimit)) ok = 0;  // every thread observes the copies
+  __syncthreads();
+  if (!ok) {
+    if (threadIdx.x == 0) {
+      atomicExch(err, 1);
+      mbar_wait_bounded(&bar, 0, kWaitLimit);  // let copies in flight land before exit
+    }
+    return;
+  }
+  tail_visit(sl, 0, nl, sc, x_zero != 0, pre, post, wcycle);
+  // the top level's result back to global memory
+  for (int i = threadIdx.x; i < lv[0].n; i += blockDim.x) lv[0].xa[i] = sl[0].xa[i];
 }
 
 // In-place unblocked LU with partial pivoting (dgetf2 order) of a
