@@ -86,6 +86,26 @@ std::vector<int> make_tiles(const std::vector<int>& rp, int n, int max_rows) {
 
 static_assert(kTileCap == kRowTileCap, "host and device tile capacities differ");
 
+// Launch with programmatic stream serialization: the kernel may begin
+// while the previous kernel in the stream drains.  Only for kernels that
+// read nothing but sparsity patterns before pdl_wait() (k_tile_rows,
+// k_coarse_tail, k_pcg_update).
+template <typename... KArgs, typename... Args>
+void launch_dependent(void (*kern)(KArgs...), int grid, int block, size_t smem, cudaStream_t st,
+                      Args&&... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  DR_CK(cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...));
+}
+
 // Blocks of `nt` threads with `smem` dynamic shared memory that fit on one
 // SM at once, per kernel (queried once).
 int resident_blocks(const void* f, int nt, size_t smem) {
@@ -121,7 +141,8 @@ void launch_rows_impl(cudaStream_t st, int max_grid, const RowForm& f, int n, in
     auto kf = k_tile_rows<F, g, O, NT, B, TA, XL, EP, DOT, Fin>;                                 \
     const int grid = std::max(                                                                   \
         1, std::min({ntiles, max_grid, g_nsm * resident_blocks((const void*)kf, NT, smem)}));    \
-    kf<<<grid, NT, smem, st>>>(ntiles, tp, ts, rp, ci, av, xl, ep, partials, ticket, fin, g_err); \
+    launch_dependent(kf, grid, NT, smem, st, ntiles, tp, ts, rp, ci, av, xl, ep, partials, ticket, \
+                     fin, g_err);                                                                \
   } while (0)
   if (f.flat) DR_LAUNCH(true, 1, true, 256, 8);
   else if (f.G == 1 && f.nt == 128) DR_LAUNCH(false, 1, true, 128, 32);
@@ -561,9 +582,9 @@ T* DevHier::cycle_level(int l, T* x, const T* b, bool x_zero, const CycleOpts& o
     TailCoarse<T> C{nc_, clu_, cpiv_, coarse_b<T>(), coarse_x<T>(), tail_co_[slot][0], tail_co_[slot][1],
                     tail_co_[slot][2], tail_co_[slot][3]};
     counted();
-    k_coarse_tail<T><<<1, kern::kTailThreads, tail_bytes_[slot], st_>>>(
-        static_cast<const TailLevel<T>*>(desc), nlevels() - l, C, o.pre, o.post, o.w ? 1 : 0,
-        x_zero ? 1 : 0, g_err);
+    launch_dependent(k_coarse_tail<T>, 1, kern::kTailThreads, tail_bytes_[slot], st_,
+                     static_cast<const TailLevel<T>*>(desc), nlevels() - l, C, o.pre, o.post,
+                     o.w ? 1 : 0, x_zero ? 1 : 0, g_err);
     DR_CK(cudaGetLastError());
     return x;
   }
@@ -806,17 +827,19 @@ int DevHier::pcg(double* x, const double* b, const CycleOpts& o, double tol, int
       launch_rows_dot(st_, max_grid_, A, A.v, dir, EpPcgDir<float>{dir, pnew, pq_}, partials_,
                       tickets_ + TK_PQ, FinStore{scal_ + SC_PQ});
       counted();
-      k_pcg_update<float><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, X, pr_, pnew, pq_, scal_ + SC_RZ,
-                                                                    scal_ + SC_PQ, pr32_, partials_,
-                                                                    tickets_ + TK_UPD, FinStore{scal_ + SC_RR});
+      launch_dependent(k_pcg_update<float>, grid1d(n, max_grid_), kBlock, 0, st_, n, X, pr_,
+                       (const double*)pnew, (const double*)pq_, (const double*)(scal_ + SC_RZ),
+                       (const double*)(scal_ + SC_PQ), pr32_, partials_, tickets_ + TK_UPD,
+                       FinStore{scal_ + SC_RR});
     } else {
       XPcgDir<double> dir{(const double*)zptr, pold, scal_ + SC_RZ, 0.0};
       launch_rows_dot(st_, max_grid_, A, A.v, dir, EpPcgDir<double>{dir, pnew, pq_}, partials_,
                       tickets_ + TK_PQ, FinStore{scal_ + SC_PQ});
       counted();
-      k_pcg_update<float><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, X, pr_, pnew, pq_, scal_ + SC_RZ,
-                                                                    scal_ + SC_PQ, nullptr, partials_,
-                                                                    tickets_ + TK_UPD, FinStore{scal_ + SC_RR});
+      launch_dependent(k_pcg_update<float>, grid1d(n, max_grid_), kBlock, 0, st_, n, X, pr_,
+                       (const double*)pnew, (const double*)pq_, (const double*)(scal_ + SC_RZ),
+                       (const double*)(scal_ + SC_PQ), (float*)nullptr, partials_, tickets_ + TK_UPD,
+                       FinStore{scal_ + SC_RR});
     }
     DR_CK(cudaGetLastError());
     DR_CK(cudaMemcpyAsync(hscal_ + SC_RR, scal_ + SC_RR, sizeof(double), cudaMemcpyDeviceToHost, st_));

@@ -268,6 +268,15 @@ struct EpPcgDir {  // q = A p, p_new = z + β p_old, returns p_new·q
 // at a time).  Every lane of the mask reaches it (no branch in between).
 __device__ __forceinline__ void issue_fence() { __syncwarp(__activemask()); }
 
+// ------------------------------------------------------------ dependent launch
+// Kernels launched with programmatic stream serialization may start while
+// the previous kernel in the stream is still running.  Before pdl_wait()
+// such a kernel touches only what no kernel writes (sparsity patterns, tile
+// bounds); pdl_wait() returns once the previous grid has completed and its
+// writes are visible.  pdl_trigger() lets the next kernel launch early.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+
 // ------------------------------------------------------------ TMA / mbarrier
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -357,9 +366,18 @@ __device__ __forceinline__ void bind_epilogue(EP&) {}
 template <typename T>
 __device__ __forceinline__ void bind_epilogue(EpPcgDir<T>& e) { e.bind(); }
 
+// Resident blocks per SM the register allocation plans for: shared memory
+// (two stages per block) admits 4 blocks with FP64 values and 7 with FP32;
+// planning for as many lets 128-thread blocks keep a whole batch of 32
+// gathers in registers without spilling.
+template <int NT, typename TA>
+constexpr int tile_min_blocks() {
+  return NT == 128 ? (sizeof(TA) == 8 ? 4 : 5) : 1;
+}
+
 template <bool FLAT, int G, bool ORDERED, int NT, int B, typename TA, class XL, class EP, bool DOT,
           class Fin>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, (tile_min_blocks<NT, TA>()))
 k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
             const int* __restrict__ rp, const int* __restrict__ ci, const TA* __restrict__ av,
             XL xl, EP ep, double* partials, unsigned* ticket, Fin fin, int* err) {
@@ -368,8 +386,6 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
   static_assert(!FLAT || G == 1, "the flat form uses one row per thread");
   constexpr int kFlatIters = (kTileCap + NT - 1) / NT;
   using Pre = typename EP::Pre;
-  bind_loader(xl);
-  bind_epilogue(ep);
   extern __shared__ __align__(128) unsigned char smem_raw[];
   // stage b: values at sv0 + b*kStageEntries, columns at sc0 + b*kStageEntries
   TA* const sv0 = reinterpret_cast<TA*>(smem_raw);
@@ -395,18 +411,25 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
     if (t >= ntiles) return Head{0, 0, 0, 0};
     return Head{__ldg(tp + t), __ldg(tp + t + 1), __ldg(ts + t), __ldg(ts + t + 1)};
   };
-  auto ctx = [&](const Head& h) -> Ctx {
+  auto ctx_rows = [&](const Head& h) -> Ctx {  // pattern only
     Ctx c{0, 0, false, Pre{}};
     const int row = h.r0 + grp;
     c.valid = (h.e - h.s <= kTileCap) && row < h.r1;
     if (c.valid) {
       c.rs = __ldg(rp + row) - h.s;
       c.re = __ldg(rp + row + 1) - h.s;
-      if (lane == 0) c.pr = ep.pre(row);
     }
     return c;
   };
-  auto issue = [&](const Head& h, int b) {  // thread 0 only
+  auto ctx = [&](const Head& h) -> Ctx {
+    Ctx c = ctx_rows(h);
+    if (c.valid && lane == 0) c.pr = ep.pre(h.r0 + grp);
+    return c;
+  };
+  // Stage a tile: the column copy (and the expected byte count of both
+  // copies) and the value copy are issued separately, so the columns can be
+  // requested before the previous kernel has finished.  Thread 0 only.
+  auto issue_cols = [&](const Head& h, int b) {
     if (h.e - h.s > kTileCap) {
       mbar_arrive(bar + b);  // long row: nothing to stage
       return;
@@ -417,7 +440,17 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
     const uint32_t vb = (cnt * (uint32_t)sizeof(TA) + 15u) & ~15u;
     mbar_expect_tx(bar + b, cb + vb);
     bulk_g2s(sc0 + b * kStageEntries, ci + sal, cb, bar + b);
+  };
+  auto issue_vals = [&](const Head& h, int b) {
+    if (h.e - h.s > kTileCap) return;
+    const int sal = h.s & ~3;
+    const uint32_t cnt = (uint32_t)(h.e - sal);
+    const uint32_t vb = (cnt * (uint32_t)sizeof(TA) + 15u) & ~15u;
     bulk_g2s(sv0 + b * kStageEntries, av + sal, vb, bar + b);
+  };
+  auto issue = [&](const Head& h, int b) {
+    issue_cols(h, b);
+    issue_vals(h, b);
   };
 
   if (threadIdx.x == 0) {
@@ -431,12 +464,22 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
   // thread's row bounds and epilogue operands of tile t + stride are in
   // flight to registers, and so are the bounds of tile t + 2 stride.  What
   // is left on a tile's critical path is the L2 gather of x.
+  // Up to pdl_wait() only the pattern is read (it never changes).
   Head h0 = head(blockIdx.x), h1 = head(blockIdx.x + stride);
   if (threadIdx.x == 0) {
-    if (blockIdx.x < ntiles) issue(h0, 0);
-    if (blockIdx.x + stride < ntiles) issue(h1, 1);
+    if (blockIdx.x < ntiles) issue_cols(h0, 0);
+    if (blockIdx.x + stride < ntiles) issue_cols(h1, 1);
   }
-  Ctx c0 = ctx(h0);
+  Ctx c0 = ctx_rows(h0);
+  pdl_trigger();
+  pdl_wait();
+  bind_loader(xl);
+  bind_epilogue(ep);
+  if (threadIdx.x == 0) {
+    if (blockIdx.x < ntiles) issue_vals(h0, 0);
+    if (blockIdx.x + stride < ntiles) issue_vals(h1, 1);
+  }
+  if (c0.valid && lane == 0) c0.pr = ep.pre(h0.r0 + grp);
 
   double dacc = 0.0;
   int i = 0;
@@ -650,6 +693,8 @@ __global__ void __launch_bounds__(kBlock)
 k_pcg_update(int n, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
              const double* __restrict__ q, const double* __restrict__ rz, const double* __restrict__ pq,
              TR32* __restrict__ r32, double* partials, unsigned* ticket, FinStore fin) {
+  pdl_trigger();
+  pdl_wait();
   const double alpha = __ldg(rz) / __ldg(pq);
   double s = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -920,34 +965,48 @@ k_coarse_tail(const TailLevel<T>* __restrict__ lv, int nl, TailCoarse<T> C, int 
   if (threadIdx.x == 0) {
     mbar_init(&bar, 1);
     fence_mbar_init();
-    // every array of the tail: (shared-memory offset, source, bytes)
-    auto each = [&](auto&& f) {
-      for (int k = 0; k < nl; ++k) {
-        const TailLevel<T>& g = lv[k];
-        f(g.o_arp, g.arp, 4 * (size_t)(g.n + 1));
-        f(g.o_aci, g.aci, 4 * (size_t)g.annz);
-        f(g.o_av, g.av, sizeof(T) * (size_t)g.annz);
-        f(g.o_invd, g.invd, sizeof(T) * (size_t)g.n);
-        f(g.o_prp, g.prp, 4 * (size_t)(g.n + 1));
-        f(g.o_pci, g.pci, 4 * (size_t)g.pnnz);
-        f(g.o_pv, g.pv, sizeof(T) * (size_t)g.pnnz);
-        f(g.o_rrp, g.rrp, 4 * (size_t)(g.nc + 1));
-        f(g.o_rci, g.rci, 4 * (size_t)g.pnnz);
-        f(g.o_rv, g.rv, sizeof(T) * (size_t)g.pnnz);
-      }
-      f(C.o_lu, C.lu, 8 * (size_t)C.n * C.n);
-      f(C.o_piv, C.piv, 4 * (size_t)C.n);
-      // the top level's right-hand side (and iterate, unless it starts at zero)
-      f(lv[0].o_b, lv[0].b, sizeof(T) * (size_t)lv[0].n);
-      if (!x_zero) f(lv[0].o_xa, lv[0].xa, sizeof(T) * (size_t)lv[0].n);
-    };
-    uint32_t total = 0;
-    each([&](unsigned, const void*, size_t b) { total += (uint32_t)((b + 15) & ~(size_t)15); });
-    mbar_expect_tx(&bar, total);
-    each([&](unsigned off, const void* src, size_t b) {
-      if (b) bulk_g2s(tsm + off, src, (uint32_t)((b + 15) & ~(size_t)15), &bar);
-    });
   }
+  // every array of the tail: (shared-memory offset, source, bytes); the
+  // patterns (never written by a kernel) and the rest (values, factors,
+  // the top level's right-hand side and iterate)
+  auto patterns = [&](auto&& f) {
+    for (int k = 0; k < nl; ++k) {
+      const TailLevel<T>& g = lv[k];
+      f(g.o_arp, g.arp, 4 * (size_t)(g.n + 1));
+      f(g.o_aci, g.aci, 4 * (size_t)g.annz);
+      f(g.o_prp, g.prp, 4 * (size_t)(g.n + 1));
+      f(g.o_pci, g.pci, 4 * (size_t)g.pnnz);
+      f(g.o_rrp, g.rrp, 4 * (size_t)(g.nc + 1));
+      f(g.o_rci, g.rci, 4 * (size_t)g.pnnz);
+    }
+  };
+  auto values = [&](auto&& f) {
+    for (int k = 0; k < nl; ++k) {
+      const TailLevel<T>& g = lv[k];
+      f(g.o_av, g.av, sizeof(T) * (size_t)g.annz);
+      f(g.o_invd, g.invd, sizeof(T) * (size_t)g.n);
+      f(g.o_pv, g.pv, sizeof(T) * (size_t)g.pnnz);
+      f(g.o_rv, g.rv, sizeof(T) * (size_t)g.pnnz);
+    }
+    f(C.o_lu, C.lu, 8 * (size_t)C.n * C.n);
+    f(C.o_piv, C.piv, 4 * (size_t)C.n);
+    f(lv[0].o_b, lv[0].b, sizeof(T) * (size_t)lv[0].n);
+    if (!x_zero) f(lv[0].o_xa, lv[0].xa, sizeof(T) * (size_t)lv[0].n);
+  };
+  auto copy = [&](unsigned off, const void* src, size_t b) {
+    if (b) bulk_g2s(tsm + off, src, (uint32_t)((b + 15) & ~(size_t)15), &bar);
+  };
+  if (threadIdx.x == 0) {
+    uint32_t total = 0;
+    auto add = [&](unsigned, const void*, size_t b) { total += (uint32_t)((b + 15) & ~(size_t)15); };
+    patterns(add);
+    values(add);
+    mbar_expect_tx(&bar, total);
+    patterns(copy);
+  }
+  pdl_trigger();
+  pdl_wait();
+  if (threadIdx.x == 0) values(copy);
   if (threadIdx.x < nl) {
     const TailLevel<T> g = lv[threadIdx.x];
     TailLevel<T> v = g;
