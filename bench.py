@@ -290,7 +290,7 @@ def run_ours(args, world, rank, local):
         kern[name] = {"bytes": int(byts), "ms": ms, "GBps": byts / (ms * 1e-3) / 1e9}
     peak, peak_kind = peaks()
     dom = kern["l1_jacobi_fp64_level1"]
-    roofline = {"bound": "hbm", "kernel": "l1_jacobi_fp64_level1 (k_csr_rows<8>, EpJacobi)",
+    roofline = {"bound": "hbm", "kernel": "l1_jacobi_fp64_level1 (k_tile_rows: one lane per row, 256 threads, EpJacobi; finest level)",
                 "achieved": round(dom["GBps"], 1), "peak": peak, "unit": "GB/s",
                 "frac": round(dom["GBps"] / peak, 3),
                 "traffic": profiled_traffic("l1_jacobi_fp64_level1"),

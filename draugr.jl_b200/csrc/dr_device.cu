@@ -1080,12 +1080,16 @@ float DevHier::time_level_op(int lvl, int op, bool fp32, int reps) {
     T* x0 = V.r;                                   // operand vectors of this level
     T* x1 = V.xb;
     T* cvec = last ? coarse_b<T>() : vecs<T>(lvl + 1).b;   // coarse-size vector
-    if (!tout_) tout_ = alloc<double>(n0_);       // scratch output (second result of op 6)
-    T* x2 = reinterpret_cast<T*>(tout_);
+    if (!tout_) tout_ = alloc<double>(n0_);       // scratch: right-hand side of op 2,
+    if (!tout2_) tout2_ = alloc<double>(n0_);     // second result of op 6
+    T* bt = reinterpret_cast<T*>(tout_);
+    T* x2 = reinterpret_cast<T*>(tout2_);
     counted();
     k_fill<T><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, T(1), x0);
     counted();
     k_fill<T><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, T(1), x1);
+    counted();
+    k_fill<T><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, T(1), bt);
     counted();
     k_fill<T><<<grid1d(nc, max_grid_), kBlock, 0, st_>>>(nc, T(1), cvec);
     const T om = (T)L.omega;
@@ -1096,7 +1100,7 @@ float DevHier::time_level_op(int lvl, int op, bool fp32, int reps) {
           break;
         case 2:
           launch_rows(st_, max_grid_, L.A, mval<T>(L.A), XPlain<T>{x0},
-                      EpJacobi<T>{x0, x0, invd<T>(L), x1, om, nullptr});
+                      EpJacobi<T>{x0, bt, invd<T>(L), x1, om, nullptr});
           break;
         case 3:
           launch_rows(st_, max_grid_, L.R, mval<T>(L.R), XPlain<T>{x0}, EpStore<T>{cvec});

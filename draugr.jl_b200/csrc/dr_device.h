@@ -236,6 +236,7 @@ class DevHier {
   double *pr_ = nullptr, *pp_[2] = {nullptr, nullptr}, *pq_ = nullptr, *pz_ = nullptr;
   float *pr32_ = nullptr, *pz32_ = nullptr;
   double *tin1_ = nullptr, *tin2_ = nullptr, *tout_ = nullptr;  // level_op staging
+  double* tout2_ = nullptr;                                      // time_level_op scratch
   size_t bytes_ = 0;
   std::vector<void*> allocs_;
   template <typename T> T* alloc(size_t n);
