@@ -62,24 +62,51 @@ int pick_G(long long nnz, int n) {
   return G;
 }
 
-// Greedy packing of consecutive rows into tiles of at most max_rows rows
-// and kTileCap nonzeros; a row longer than kTileCap is a tile of its own.
-std::vector<int> make_tiles(const std::vector<int>& rp, int n, int max_rows) {
+// Greedy packing of consecutive rows into tiles of at most max_rows rows,
+// kTileCap nonzeros and a column span below 65536 (so that a tile's columns
+// are 16-bit offsets from its smallest column).  A row longer than kTileCap,
+// or spanning 65536 columns or more by itself, is a tile of its own.
+// Returns the tile row starts; `base` receives each tile's smallest column,
+// -1 for a row too wide for offsets.
+std::vector<int> make_tiles(const std::vector<int>& rp, const std::vector<int>& ci, int n,
+                            int max_rows, std::vector<int>& base) {
   std::vector<int> tp;
   tp.reserve(n / std::max(1, max_rows) + 2);
   tp.push_back(0);
+  base.clear();
   int r = 0;
   while (r < n) {
     int rows = 0, nz = 0;
+    bool have = false;  // any column in the tile yet
+    long long lo = 0, hi = 0;
     while (r < n && rows < max_rows) {
       const int len = rp[r + 1] - rp[r];
-      if (rows > 0 && nz + len > kTileCap) break;
+      long long rlo = 0, rhi = 0;
+      if (len > 0) {
+        rlo = rhi = ci[rp[r]];
+        for (int k = rp[r] + 1; k < rp[r + 1]; ++k) {
+          rlo = std::min<long long>(rlo, ci[k]);
+          rhi = std::max<long long>(rhi, ci[k]);
+        }
+      }
+      long long nlo = lo, nhi = hi;
+      bool nhave = have;
+      if (len > 0) {
+        nlo = have ? std::min(lo, rlo) : rlo;
+        nhi = have ? std::max(hi, rhi) : rhi;
+        nhave = true;
+      }
+      if (rows > 0 && (nz + len > kTileCap || (nhave && nhi - nlo >= 65536))) break;
       nz += len;
+      lo = nlo;
+      hi = nhi;
+      have = nhave;
       ++rows;
       ++r;
-      if (len > kTileCap) break;
+      if (len > kTileCap || (len > 0 && rhi - rlo >= 65536)) break;
     }
     tp.push_back(r);
+    base.push_back(!have ? 0 : (hi - lo >= 65536 ? -1 : (int)lo));
   }
   return tp;
 }
@@ -123,8 +150,9 @@ int resident_blocks(const void* f, int nt, size_t smem) {
 
 template <typename TA, class XL, class EP, bool DOT, class Fin>
 void launch_rows_impl(cudaStream_t st, int max_grid, const RowForm& f, int n, int ntiles,
-                      const int* tp, const int* ts, const int* rp, const int* ci, const TA* av,
-                      XL xl, EP ep, double* partials, unsigned* ticket, Fin fin) {
+                      const int* tp, const int* ts, const int* tb, const int* rp, const int* ci,
+                      const uint16_t* cu, const TA* av, XL xl, EP ep, double* partials,
+                      unsigned* ticket, Fin fin) {
   if (n <= 0) {
     if constexpr (DOT) {
       // an empty reduction still has to deliver its (zero) result
@@ -133,23 +161,29 @@ void launch_rows_impl(cudaStream_t st, int max_grid, const RowForm& f, int n, in
     }
     return;
   }
-  const size_t smem = tile_smem_bytes<TA>();
   counted();
   // one wave of resident blocks (registers and shared memory permitting)
-#define DR_LAUNCH(F, g, O, NT, B)                                                                \
+#define DR_LAUNCH(F, g, O, NT, B, TC)                                                            \
   do {                                                                                           \
-    auto kf = k_tile_rows<F, g, O, NT, B, TA, XL, EP, DOT, Fin>;                                 \
+    auto kf = k_tile_rows<F, g, O, NT, B, TA, TC, XL, EP, DOT, Fin>;                             \
+    const size_t smem = tile_smem_bytes<TA, TC>();                                               \
     const int grid = std::max(                                                                   \
         1, std::min({ntiles, max_grid, g_nsm * resident_blocks((const void*)kf, NT, smem)}));    \
-    launch_dependent(kf, grid, NT, smem, st, ntiles, tp, ts, rp, ci, av, xl, ep, partials, ticket, \
-                     fin, g_err);                                                                \
+    launch_dependent(kf, grid, NT, smem, st, ntiles, tp, ts, tb, rp, ci, cu, av, xl, ep, partials, \
+                     ticket, fin, g_err);                                                        \
   } while (0)
-  if (f.flat) DR_LAUNCH(true, 1, true, 256, 8);
-  else if (f.G == 1 && f.nt == 128) DR_LAUNCH(false, 1, true, 128, 32);
-  else if (f.G == 1) DR_LAUNCH(false, 1, true, 256, 8);
-  else if (f.G == 8) DR_LAUNCH(false, 8, false, 256, 12);
-  else if (f.G == 16) DR_LAUNCH(false, 16, false, 256, 12);
-  else if (f.G == 32) DR_LAUNCH(false, 32, false, 256, 4);
+  // 16-bit column offsets where lanes read consecutive entries (flat and
+  // tree forms), and for FP32 rows of 12-32 entries, where the bytes saved
+  // outweigh the bank conflicts of 16-bit reads at a row stride; the
+  // columns themselves for the other one-lane-per-row forms (measured on the
+  // 128^3 hierarchy: both choices per form, FP64 and FP32)
+  if (f.flat) DR_LAUNCH(true, 1, true, 256, 8, uint16_t);
+  else if (f.G == 1 && f.nt == 128 && sizeof(TA) == 4) DR_LAUNCH(false, 1, true, 128, 32, uint16_t);
+  else if (f.G == 1 && f.nt == 128) DR_LAUNCH(false, 1, true, 128, 32, int);
+  else if (f.G == 1) DR_LAUNCH(false, 1, true, 256, 8, int);
+  else if (f.G == 8) DR_LAUNCH(false, 8, false, 256, 12, uint16_t);
+  else if (f.G == 16) DR_LAUNCH(false, 16, false, 256, 12, uint16_t);
+  else if (f.G == 32) DR_LAUNCH(false, 32, false, 256, 4, uint16_t);
   else fail("bad row form");
 #undef DR_LAUNCH
   DR_CK(cudaGetLastError());
@@ -158,15 +192,15 @@ void launch_rows_impl(cudaStream_t st, int max_grid, const RowForm& f, int n, in
 template <typename TA, class XL, class EP>
 void launch_rows(cudaStream_t st, int max_grid, const DevMat& M, const TA* av, XL xl, EP ep) {
   launch_rows_impl<TA, XL, EP, false, FinStore>(st, max_grid, M.form, M.n, M.ntiles, M.tp, M.ts,
-                                                M.rp, M.ci, av, xl, ep, nullptr, nullptr,
-                                                FinStore{nullptr});
+                                                M.tb, M.rp, M.ci, M.cu, av, xl, ep, nullptr,
+                                                nullptr, FinStore{nullptr});
 }
 
 template <typename TA, class XL, class EP, class Fin>
 void launch_rows_dot(cudaStream_t st, int max_grid, const DevMat& M, const TA* av, XL xl, EP ep,
                      double* partials, unsigned* ticket, Fin fin) {
-  launch_rows_impl<TA, XL, EP, true, Fin>(st, max_grid, M.form, M.n, M.ntiles, M.tp, M.ts, M.rp,
-                                          M.ci, av, xl, ep, partials, ticket, fin);
+  launch_rows_impl<TA, XL, EP, true, Fin>(st, max_grid, M.form, M.n, M.ntiles, M.tp, M.ts, M.tb,
+                                          M.rp, M.ci, M.cu, av, xl, ep, partials, ticket, fin);
 }
 
 int grid1d(long long n, int max_grid) {
@@ -242,14 +276,25 @@ DevHier::DevHier(const HostHierarchy& H, int device) {
       if (v) h2d(M.v, *v, st_);
       M.Ggs = pick_G(M.nnz, n);
       M.form = row_form(rp);
-      std::vector<int> tiles = make_tiles(rp, n, M.form.nt / M.form.G);
+      std::vector<int> base;
+      std::vector<int> tiles = make_tiles(rp, ci, n, M.form.nt / M.form.G, base);
       std::vector<int> tstart(tiles.size());
       for (size_t t = 0; t < tiles.size(); ++t) tstart[t] = rp[tiles[t]];
       M.ntiles = (int)tiles.size() - 1;
       M.tp = alloc<int>(tiles.size());
       M.ts = alloc<int>(tiles.size());
+      M.tb = alloc<int>(base.size());
       DR_CK(cudaMemcpy(M.tp, tiles.data(), tiles.size() * sizeof(int), cudaMemcpyHostToDevice));
       DR_CK(cudaMemcpy(M.ts, tstart.data(), tstart.size() * sizeof(int), cudaMemcpyHostToDevice));
+      DR_CK(cudaMemcpy(M.tb, base.data(), base.size() * sizeof(int), cudaMemcpyHostToDevice));
+      // 16-bit column offsets from each tile's smallest column (8 padding
+      // entries for the tile kernel's 16-byte-rounded copies)
+      std::vector<uint16_t> off(ci.size() + 8, 0);
+      for (int t = 0; t < M.ntiles; ++t)
+        if (base[t] >= 0)
+          for (int k = tstart[t]; k < tstart[t + 1]; ++k) off[k] = (uint16_t)(ci[k] - base[t]);
+      M.cu = alloc<uint16_t>(off.size());
+      DR_CK(cudaMemcpy(M.cu, off.data(), off.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
     };
     for (int l = 0; l < nl; ++l) {
       const HostLevel& h = H.levels[l];

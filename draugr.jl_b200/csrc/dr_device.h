@@ -92,6 +92,8 @@ struct DevMat {
   int ntiles = 0;     // row tiles (see k_tile_rows)
   int* tp = nullptr;  // tile row starts, ntiles+1
   int* ts = nullptr;  // tile nonzero starts, ntiles+1
+  int* tb = nullptr;       // tile smallest columns (-1: row too wide for offsets), ntiles
+  uint16_t* cu = nullptr;  // columns as offsets from their tile's smallest column
 };
 
 template <typename T>

@@ -325,14 +325,22 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 
 // ------------------------------------------------------------ row kernel
 // Rows are packed (on the host, once per matrix) into tiles of at most
-// NT/G consecutive rows holding at most kTileCap nonzeros; tp[t] is the
-// first row and ts[t] the first nonzero of tile t.  Each block walks the
-// tiles blockIdx.x, +gridDim.x, ... with two shared-memory stages: while it
-// works on one tile, the TMA engine copies the column and value arrays of
-// the tile after next into the other stage (cp.async.bulk completing on an
-// mbarrier), so HBM streaming never waits on the SM.  The row's other
-// operands (row bounds, epilogue inputs) are loaded one tile ahead into
-// registers.  Two ways to form the products a_ij·x_j (x is L2-resident):
+// NT/G consecutive rows holding at most kTileCap nonzeros whose columns
+// span fewer than 65536 indices; tp[t] is the first row, ts[t] the first
+// nonzero and tb[t] the smallest column of tile t.  The columns are stored
+// a second time as 16-bit offsets from their tile's smallest column (cu),
+// which is what the kernel streams: 2 bytes per entry instead of 4.  A row
+// that alone spans 65536 or more columns, or holds more than kTileCap
+// entries, forms a tile of its own (tb = -1 marks the wide case) that is
+// read from the 32-bit columns in global memory.
+//
+// Each block walks the tiles blockIdx.x, +gridDim.x, ... with two
+// shared-memory stages: while it works on one tile, the TMA engine copies
+// the column-offset and value arrays of the tile after next into the other
+// stage (cp.async.bulk completing on an mbarrier), so HBM streaming never
+// waits on the SM.  The row's other operands (row bounds, epilogue inputs)
+// are loaded one tile ahead into registers.  Two ways to form the products
+// a_ij·x_j (x is L2-resident):
 //   row-gather (FLAT = false): G lanes per row gather their entries of the
 //     row, B at once with one lane per row (8 for short rows; 32 with
 //     128-thread blocks for rows of 12-32 entries, so that one L2 round trip
@@ -341,22 +349,26 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 //   flat (FLAT = true, one row per thread): the whole block walks the tile's
 //     nonzeros flat, so a long row among short ones costs no more than its
 //     share (rows of very uneven length, e.g. the restriction Pᵀ).
-// Rows of up to 32 entries (ORDERED) are then summed by one thread in
-// column order — the reference's order, with products and sums rounded
-// separately — so they are reproduced bit for bit; products are written over
-// the staged values for that when needed.  Longer rows are summed by their G
-// lanes and a fixed shuffle tree (deterministic, not the reference's order).  The column / value
-// arrays carry 4 padding entries so the 16-byte-rounded copies stay in
-// bounds.  A row longer than kTileCap forms a tile of its own and is reduced
-// by the whole block straight from global memory (tree order).
+// With one lane per row (ORDERED) a row is summed by one thread in column
+// order — the reference's order, with products and sums rounded separately —
+// so it is reproduced bit for bit.  With G > 1 lanes a row is summed by its
+// lanes and a fixed shuffle tree (deterministic, not the reference's order).
+// Rows read from global memory are summed by one thread in column order
+// when ORDERED and no longer than kTileCap, else by the block in a fixed
+// tree.  The offset and value arrays carry padding so the 16-byte-rounded
+// copies stay in bounds.
 constexpr int kTileCap = 2000;
-constexpr int kStageEntries = 2008;  // kTileCap + alignment slack, a multiple of 4 entries
+constexpr int kStageEntries = 2008;  // kTileCap + alignment slack, a multiple of 8 entries
 constexpr int kWaitLimit = 1 << 22;
 
-// Dynamic shared memory of k_tile_rows: two stages of columns and values
-// (47 KB for FP64 values; with the kernel's static shared memory it stays
-// under the 48 KB that needs no opt-in attribute).
-template <typename TA>
+// Dynamic shared memory of k_tile_rows: two stages of columns (TC: int, or
+// uint16_t offsets) and values, 47 KB for FP64 values (under the 48 KB that
+// needs no opt-in).  Sized for int columns whatever TC is: every row kernel
+// of one value type then asks for the same shared memory, so consecutive
+// kernels run in the same L1 / shared-memory split (kernels of different
+// sizes interleaved in a cycle cost 1-3% of the solve time in SM
+// reconfiguration and lost launch overlap).
+template <typename TA, typename TC>
 constexpr size_t tile_smem_bytes() {
   return 2 * (size_t)kStageEntries * (sizeof(int) + sizeof(TA));
 }
@@ -366,41 +378,47 @@ __device__ __forceinline__ void bind_epilogue(EP&) {}
 template <typename T>
 __device__ __forceinline__ void bind_epilogue(EpPcgDir<T>& e) { e.bind(); }
 
-// Resident blocks per SM the register allocation plans for: shared memory
-// (two stages per block) admits 4 blocks with FP64 values and 7 with FP32;
-// planning for as many lets 128-thread blocks keep a whole batch of 32
-// gathers in registers without spilling.
+// Resident blocks per SM the register allocation plans for: planning for 4
+// lets 128-thread FP64 blocks keep a whole batch of 32 gathers in registers
+// without spilling.
 template <int NT, typename TA>
 constexpr int tile_min_blocks() {
   return NT == 128 ? (sizeof(TA) == 8 ? 4 : 5) : 1;
 }
 
-template <bool FLAT, int G, bool ORDERED, int NT, int B, typename TA, class XL, class EP, bool DOT,
-          class Fin>
+// TC: the staged column type — int (the columns themselves) or uint16_t
+// (offsets from the tile's smallest column, from cu).  One lane per row
+// reads its row's columns at a row stride, where 16-bit entries would
+// collide on shared-memory banks; the other forms read consecutive entries.
+template <bool FLAT, int G, bool ORDERED, int NT, int B, typename TA, typename TC, class XL, class EP,
+          bool DOT, class Fin>
 __global__ void __launch_bounds__(NT, (tile_min_blocks<NT, TA>()))
 k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
-            const int* __restrict__ rp, const int* __restrict__ ci, const TA* __restrict__ av,
-            XL xl, EP ep, double* partials, unsigned* ticket, Fin fin, int* err) {
+            const int* __restrict__ tb, const int* __restrict__ rp, const int* __restrict__ ci,
+            const uint16_t* __restrict__ cu, const TA* __restrict__ av, XL xl, EP ep,
+            double* partials, unsigned* ticket, Fin fin, int* err) {
+  constexpr bool kOff = sizeof(TC) == 2;
+  constexpr int kColAlign = 16 / (int)sizeof(TC);  // entries per 16 bytes
+  const TC* const csrc = kOff ? reinterpret_cast<const TC*>(cu) : reinterpret_cast<const TC*>(ci);
   using acc_t = typename EP::acc_t;
-  static_assert(sizeof(acc_t) == sizeof(TA), "products are stored over the staged values");
+  static_assert(sizeof(acc_t) == sizeof(TA), "flat products are stored over the staged values");
   static_assert(!FLAT || G == 1, "the flat form uses one row per thread");
+  static_assert(!ORDERED || G == 1, "ordered sums use one lane per row");
   constexpr int kFlatIters = (kTileCap + NT - 1) / NT;
   using Pre = typename EP::Pre;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   // stage b: values at sv0 + b*kStageEntries, columns at sc0 + b*kStageEntries
   TA* const sv0 = reinterpret_cast<TA*>(smem_raw);
-  int* const sc0 = reinterpret_cast<int*>(sv0 + 2 * kStageEntries);
+  TC* const sc0 = reinterpret_cast<TC*>(sv0 + 2 * kStageEntries);
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ acc_t red[32];
   const int stride = gridDim.x;
   const int lane = threadIdx.x & (G - 1);
   const int grp = threadIdx.x / G;
-  const unsigned gmask =
-      (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
 
   // A tile's bounds, and one thread's row bounds and epilogue operands in it.
   struct Head {
-    int r0, r1, s, e;
+    int r0, r1, s, e, cb;  // cb: smallest column, -1 for a tile read from global memory
   };
   struct Ctx {
     int rs, re;
@@ -408,13 +426,15 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
     Pre pr;
   };
   auto head = [&](int t) -> Head {
-    if (t >= ntiles) return Head{0, 0, 0, 0};
-    return Head{__ldg(tp + t), __ldg(tp + t + 1), __ldg(ts + t), __ldg(ts + t + 1)};
+    if (t >= ntiles) return Head{0, 0, 0, 0, 0};
+    return Head{__ldg(tp + t), __ldg(tp + t + 1), __ldg(ts + t), __ldg(ts + t + 1),
+                kOff ? __ldg(tb + t) : 0};
   };
+  auto staged = [](const Head& h) { return (!kOff || h.cb >= 0) && h.e - h.s <= kTileCap; };
   auto ctx_rows = [&](const Head& h) -> Ctx {  // pattern only
     Ctx c{0, 0, false, Pre{}};
     const int row = h.r0 + grp;
-    c.valid = (h.e - h.s <= kTileCap) && row < h.r1;
+    c.valid = staged(h) && row < h.r1;
     if (c.valid) {
       c.rs = __ldg(rp + row) - h.s;
       c.re = __ldg(rp + row + 1) - h.s;
@@ -426,27 +446,26 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
     if (c.valid && lane == 0) c.pr = ep.pre(h.r0 + grp);
     return c;
   };
-  // Stage a tile: the column copy (and the expected byte count of both
-  // copies) and the value copy are issued separately, so the columns can be
+  // Stage a tile: the offset copy (and the expected byte count of both
+  // copies) and the value copy are issued separately, so the offsets can be
   // requested before the previous kernel has finished.  Thread 0 only.
+  // Copies start on 16-byte boundaries: kColAlign columns, 4 values.
   auto issue_cols = [&](const Head& h, int b) {
-    if (h.e - h.s > kTileCap) {
-      mbar_arrive(bar + b);  // long row: nothing to stage
+    if (!staged(h)) {
+      mbar_arrive(bar + b);  // read from global memory: nothing to stage
       return;
     }
-    const int sal = h.s & ~3;
-    const uint32_t cnt = (uint32_t)(h.e - sal);
-    const uint32_t cb = (cnt * 4u + 15u) & ~15u;
-    const uint32_t vb = (cnt * (uint32_t)sizeof(TA) + 15u) & ~15u;
+    const int sc = h.s & ~(kColAlign - 1), sv = h.s & ~3;
+    const uint32_t cb = ((uint32_t)(h.e - sc) * (uint32_t)sizeof(TC) + 15u) & ~15u;
+    const uint32_t vb = ((uint32_t)(h.e - sv) * (uint32_t)sizeof(TA) + 15u) & ~15u;
     mbar_expect_tx(bar + b, cb + vb);
-    bulk_g2s(sc0 + b * kStageEntries, ci + sal, cb, bar + b);
+    bulk_g2s(sc0 + b * kStageEntries, csrc + sc, cb, bar + b);
   };
   auto issue_vals = [&](const Head& h, int b) {
-    if (h.e - h.s > kTileCap) return;
-    const int sal = h.s & ~3;
-    const uint32_t cnt = (uint32_t)(h.e - sal);
-    const uint32_t vb = (cnt * (uint32_t)sizeof(TA) + 15u) & ~15u;
-    bulk_g2s(sv0 + b * kStageEntries, av + sal, vb, bar + b);
+    if (!staged(h)) return;
+    const int sv = h.s & ~3;
+    const uint32_t vb = ((uint32_t)(h.e - sv) * (uint32_t)sizeof(TA) + 15u) & ~15u;
+    bulk_g2s(sv0 + b * kStageEntries, av + sv, vb, bar + b);
   };
   auto issue = [&](const Head& h, int b) {
     issue_cols(h, b);
@@ -460,7 +479,7 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
   }
   __syncthreads();
   // Software pipeline: while tile t is reduced, the TMA engine streams the
-  // columns and values of tile t + stride (issued one tile earlier), this
+  // offsets and values of tile t + stride (issued one tile earlier), this
   // thread's row bounds and epilogue operands of tile t + stride are in
   // flight to registers, and so are the bounds of tile t + 2 stride.  What
   // is left on a tile's critical path is the L2 gather of x.
@@ -498,21 +517,25 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
       if (threadIdx.x == 0) atomicExch(err, 1);
       mbar_wait_bounded(bar + b, parity, kWaitLimit);
     }
-    if (len <= kTileCap) {
-      const int off = s - (s & ~3);
-      TA* vs = sv0 + b * kStageEntries + off;
-      const int* cs = sc0 + b * kStageEntries + off;
+    if (staged(h0)) {
+      TA* vs = sv0 + b * kStageEntries + (s - (s & ~3));
+      const TC* cs = sc0 + b * kStageEntries + (s - (s & ~(kColAlign - 1)));
+      const int cb = h0.cb;
       if constexpr (FLAT) {
-        acc_t p[kFlatIters];
+        if (len > 0) {
+          // slots past the tile's end repeat its last entry (in bounds)
+          acc_t p[kFlatIters];
 #pragma unroll
-        for (int j = 0; j < kFlatIters; ++j) {
-          const int k = threadIdx.x + j * NT;
-          p[j] = (k < len) ? (acc_t)xl(cs[k]) : acc_t(0);
-        }
+          for (int j = 0; j < kFlatIters; ++j) {
+            const int k = min((int)threadIdx.x + j * NT, len - 1);
+            p[j] = (acc_t)xl(cb + (int)cs[k]);
+          }
+          issue_fence();
 #pragma unroll
-        for (int j = 0; j < kFlatIters; ++j) {
-          const int k = threadIdx.x + j * NT;
-          if (k < len) vs[k] = (TA)mul_rn((acc_t)vs[k], p[j]);
+          for (int j = 0; j < kFlatIters; ++j) {
+            const int k = threadIdx.x + j * NT;
+            if (k < len) vs[k] = (TA)mul_rn((acc_t)vs[k], p[j]);
+          }
         }
         __syncthreads();
         if (valid) {
@@ -531,7 +554,7 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
             // repeat its last column, in bounds), then the ordered sum
             acc_t xv[B];
 #pragma unroll
-            for (int j = 0; j < B; ++j) xv[j] = (acc_t)xl(cs[min(k0 + j, re - 1)]);
+            for (int j = 0; j < B; ++j) xv[j] = (acc_t)xl(cb + (int)cs[min(k0 + j, re - 1)]);
             issue_fence();
 #pragma unroll
             for (int j = 0; j < B; ++j)
@@ -543,37 +566,13 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
           }
           dacc += ep.apply(row, a, pr);
         }
-      } else if constexpr (ORDERED) {
-        // G lanes form the products of a row, lane 0 sums them in order
-        for (int k0 = rs + lane; k0 < re; k0 += 8 * G) {
-          acc_t p[8];
-#pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            const int k = k0 + j * G;
-            p[j] = (k < re) ? mul_rn((acc_t)vs[k], (acc_t)xl(cs[k])) : acc_t(0);
-          }
-#pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            const int k = k0 + j * G;
-            if (k < re) vs[k] = (TA)p[j];
-          }
-        }
-        __syncwarp(gmask);
-        if (valid && lane == 0) {
-          acc_t a = ep.init(pr);
-          for (int k = rs; k < re; ++k) {
-            if constexpr (EP::kSign > 0) a = add_rn(a, (acc_t)vs[k]);
-            else a = sub_rn(a, (acc_t)vs[k]);
-          }
-          dacc += ep.apply(row, a, pr);
-        }
       } else {
-        // long rows: G lanes sum strided products, then a fixed shuffle tree
+        // longer rows: G lanes sum strided products, then a fixed shuffle tree
         acc_t sum = acc_t(0);
         for (int k0 = rs + lane; k0 < re; k0 += B * G) {
           acc_t xv[B];
 #pragma unroll
-          for (int j = 0; j < B; ++j) xv[j] = (acc_t)xl(cs[min(k0 + j * G, re - 1)]);
+          for (int j = 0; j < B; ++j) xv[j] = (acc_t)xl(cb + (int)cs[min(k0 + j * G, re - 1)]);
           issue_fence();
 #pragma unroll
           for (int j = 0; j < B; ++j) {
@@ -590,8 +589,21 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
           dacc += ep.apply(row, a, pr);
         }
       }
+    } else if (ORDERED && len <= kTileCap) {
+      // a single wide row, from global memory, summed by one thread in order
+      if (threadIdx.x == 0) {
+        const Pre p0 = ep.pre(r0);
+        acc_t a = ep.init(p0);
+        for (int k = s; k < e; ++k) {
+          const acc_t p = mul_rn((acc_t)__ldg(av + k), (acc_t)xl(__ldg(ci + k)));
+          if constexpr (EP::kSign > 0) a = add_rn(a, p);
+          else a = sub_rn(a, p);
+        }
+        dacc += ep.apply(r0, a, p0);
+      }
     } else {
-      // a single row longer than the tile capacity, from global memory
+      // a single row longer than the tile capacity (or wide, in a form that
+      // sums in a tree), from global memory, reduced by the block
       acc_t sum = acc_t(0);
       for (int k = s + threadIdx.x; k < e; k += NT)
         sum = add_rn(sum, mul_rn((acc_t)__ldg(av + k), (acc_t)xl(__ldg(ci + k))));
