@@ -439,12 +439,44 @@ static constexpr size_t kTailSmem = 200 * 1024;
 
 static size_t a16(size_t b) { return (b + 15) & ~(size_t)15; }
 
+// Sliced-ELL layout of a tail level's matrix (see TailLevel): slot of
+// entry j of row 32 s + l is eoff[s] + 32 j + l; perm maps each slot to its
+// CSR position (-1 for padding).
+struct EllPattern {
+  std::vector<int> col, len, off, perm;
+};
+
+static EllPattern ell_of(const std::vector<int>& rp, const std::vector<int>& ci) {
+  EllPattern E;
+  const int n = (int)rp.size() - 1, ns = (n + 31) / 32;
+  E.len.resize(n);
+  E.off.resize(ns);
+  int total = 0;
+  for (int s = 0; s < ns; ++s) {
+    int w = 0;
+    for (int i = 32 * s; i < std::min(n, 32 * s + 32); ++i) w = std::max(w, rp[i + 1] - rp[i]);
+    E.off[s] = total;
+    total += 32 * w;
+  }
+  E.col.assign(total, 0);
+  E.perm.assign(total, -1);
+  for (int i = 0; i < n; ++i) {
+    E.len[i] = rp[i + 1] - rp[i];
+    const int base = E.off[i / 32] + (i % 32);
+    for (int j = 0; j < E.len[i]; ++j) {
+      E.col[base + 32 * j] = ci[rp[i] + j];
+      E.perm[base + 32 * j] = rp[i] + j;
+    }
+  }
+  return E;
+}
+
 template <typename T>
-static size_t tail_level_bytes(const DevLevel& d) {
-  const size_t n = d.A.n, nc = d.P.m, an = d.A.nnz, pn = d.P.nnz;
-  return a16(4 * (n + 1)) + a16(4 * an) + a16(sizeof(T) * an) + a16(sizeof(T) * n) +
-         a16(4 * (n + 1)) + a16(4 * pn) + a16(sizeof(T) * pn) + a16(4 * (nc + 1)) + a16(4 * pn) +
-         a16(sizeof(T) * pn) + 4 * a16(sizeof(T) * n);
+static size_t tail_level_bytes(const DevLevel& d, int ne) {
+  const size_t n = d.A.n, nc = d.P.m, pn = d.P.nnz, ns = (n + 31) / 32;
+  return a16(4 * (size_t)ne) + a16(4 * n) + a16(4 * ns) + a16(sizeof(T) * (size_t)ne) +
+         a16(sizeof(T) * n) + a16(4 * (n + 1)) + a16(4 * pn) + a16(sizeof(T) * pn) +
+         a16(4 * (nc + 1)) + a16(4 * pn) + a16(sizeof(T) * pn) + 4 * a16(sizeof(T) * n);
 }
 
 template <typename T>
@@ -455,16 +487,45 @@ static size_t tail_coarse_bytes(int nc) {
 void DevHier::build_tail() {
   const int nl = nlevels();
   tail_ = nl;
+  tail_ell_.clear();
   size_t total = tail_coarse_bytes<double>(nc_);
+  std::vector<EllPattern> ells;  // from the coarsest level up
   for (int l = nl - 1; l >= 1 && nl - l <= kern::kTailMaxLevels; --l) {
     const DevLevel& d = L_[l];
     const bool jac = d.smoother == SmootherKind::Jacobi || d.smoother == SmootherKind::L1Jacobi;
-    total += tail_level_bytes<double>(d);
-    if (!jac || total > kTailSmem) break;
+    if (!jac || d.A.n > 4096 || d.A.nnz > (1 << 16)) break;
+    std::vector<int> rp(d.A.n + 1), ci(d.A.nnz);
+    DR_CK(cudaMemcpy(rp.data(), d.A.rp, rp.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    if (!ci.empty()) DR_CK(cudaMemcpy(ci.data(), d.A.ci, ci.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    EllPattern E = ell_of(rp, ci);
+    total += tail_level_bytes<double>(d, (int)E.col.size());
+    if (total > kTailSmem) break;
     tail_ = l;
+    ells.push_back(std::move(E));
   }
   if (tail_ >= nl) return;
   const int cnt = nl - tail_;
+  std::reverse(ells.begin(), ells.end());  // tail_ first
+  for (int k = 0; k < cnt; ++k) {
+    const EllPattern& E = ells[k];
+    TailEll te;
+    te.level = tail_ + k;
+    te.ne = (int)E.col.size();
+    te.col = alloc<int>(E.col.size());
+    te.len = alloc<int>(E.len.size());
+    te.off = alloc<int>(E.off.size());
+    te.perm = alloc<int>(E.perm.size());
+    te.v64 = alloc<double>(E.col.size());
+    if (!E.col.empty()) {
+      DR_CK(cudaMemcpy(te.col, E.col.data(), E.col.size() * sizeof(int), cudaMemcpyHostToDevice));
+      DR_CK(cudaMemcpy(te.perm, E.perm.data(), E.perm.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    DR_CK(cudaMemcpy(te.len, E.len.data(), E.len.size() * sizeof(int), cudaMemcpyHostToDevice));
+    DR_CK(cudaMemcpy(te.off, E.off.data(), E.off.size() * sizeof(int), cudaMemcpyHostToDevice));
+    if (fp32_) te.v32 = alloc<float>(E.col.size());
+    tail_ell_.push_back(te);
+  }
+  refresh_tail();
   auto make = [&](auto tag) {
     using T = decltype(tag);
     const int slot = sizeof(T) == 8 ? 0 : 1;
@@ -478,15 +539,17 @@ void DevHier::build_tail() {
     for (int k = 0; k < cnt; ++k) {
       DevLevel& d = L_[tail_ + k];
       LevelVecs<T>& V = vecs<T>(tail_ + k);
+      const TailEll& te = tail_ell_[k];
       TailLevel<T>& t = v[k];
-      const size_t n = d.A.n, nc = d.P.m;
+      const size_t n = d.A.n, nc = d.P.m, ns = (n + 31) / 32;
       t.n = d.A.n;
       t.nc = d.P.m;
-      t.annz = (int)d.A.nnz;
+      t.ne = te.ne;
       t.pnnz = (int)d.P.nnz;
-      t.arp = d.A.rp;
-      t.aci = d.A.ci;
-      t.av = mval<T>(d.A);
+      t.ecol = te.col;
+      t.elen = te.len;
+      t.eoff = te.off;
+      t.ev = sizeof(T) == 8 ? reinterpret_cast<const T*>(te.v64) : reinterpret_cast<const T*>(te.v32);
       t.invd = invd<T>(d);
       t.omega = (T)d.omega;
       t.prp = d.P.rp;
@@ -499,9 +562,10 @@ void DevHier::build_tail() {
       t.xb = V.xb;
       t.b = V.b;
       t.r = V.r;
-      t.o_arp = take(4 * (n + 1));
-      t.o_aci = take(4 * (size_t)d.A.nnz);
-      t.o_av = take(sizeof(T) * (size_t)d.A.nnz);
+      t.o_ecol = take(4 * (size_t)te.ne);
+      t.o_elen = take(4 * n);
+      t.o_eoff = take(4 * ns);
+      t.o_ev = take(sizeof(T) * (size_t)te.ne);
       t.o_invd = take(sizeof(T) * n);
       t.o_prp = take(4 * (n + 1));
       t.o_pci = take(4 * (size_t)d.P.nnz);
@@ -519,6 +583,44 @@ void DevHier::build_tail() {
     tail_co_[slot][2] = take(sizeof(T) * (size_t)nc_);
     tail_co_[slot][3] = take(sizeof(T) * (size_t)nc_);
     tail_bytes_[slot] = off;
+    // the prologue's bulk copies: patterns, then values, factors and the
+    // top level's right-hand side (sizes rounded up to 16 bytes; every
+    // source starts an allocation rounded the same way)
+    std::vector<TailCopy> pat, val;
+    auto rec = [&](std::vector<TailCopy>& l, unsigned o, const void* src, size_t bytes) {
+      if (bytes) l.push_back(TailCopy{src, o, (unsigned)a16(bytes)});
+    };
+    for (int k = 0; k < cnt; ++k) {
+      const TailLevel<T>& t = v[k];
+      const size_t n = t.n, ns = (n + 31) / 32;
+      rec(pat, t.o_ecol, t.ecol, 4 * (size_t)t.ne);
+      rec(pat, t.o_elen, t.elen, 4 * n);
+      rec(pat, t.o_eoff, t.eoff, 4 * ns);
+      rec(pat, t.o_prp, t.prp, 4 * (n + 1));
+      rec(pat, t.o_pci, t.pci, 4 * (size_t)t.pnnz);
+      rec(pat, t.o_rrp, t.rrp, 4 * ((size_t)t.nc + 1));
+      rec(pat, t.o_rci, t.rci, 4 * (size_t)t.pnnz);
+      rec(val, t.o_ev, t.ev, sizeof(T) * (size_t)t.ne);
+      rec(val, t.o_invd, t.invd, sizeof(T) * n);
+      rec(val, t.o_pv, t.pv, sizeof(T) * (size_t)t.pnnz);
+      rec(val, t.o_rv, t.rv, sizeof(T) * (size_t)t.pnnz);
+    }
+    rec(val, tail_co_[slot][0], clu_, 8 * (size_t)nc_ * nc_);
+    rec(val, tail_co_[slot][1], cpiv_, 4 * (size_t)nc_);
+    rec(val, v[0].o_b, v[0].b, sizeof(T) * (size_t)v[0].n);
+    TailCopyList& cl = tail_cp_[slot];
+    cl.npat = (int)pat.size();
+    cl.nval = (int)val.size();
+    cl.pat_bytes = cl.val_bytes = 0;
+    for (const TailCopy& c : pat) cl.pat_bytes += c.bytes;
+    for (const TailCopy& c : val) cl.val_bytes += c.bytes;
+    cl.xsrc = v[0].xa;
+    cl.xoff = v[0].o_xa;
+    cl.xbytes = (unsigned)a16(sizeof(T) * (size_t)v[0].n);
+    pat.insert(pat.end(), val.begin(), val.end());
+    TailCopy* dl = alloc<TailCopy>(pat.size());
+    DR_CK(cudaMemcpy(dl, pat.data(), pat.size() * sizeof(TailCopy), cudaMemcpyHostToDevice));
+    cl.list = dl;
     DR_CK(cudaFuncSetAttribute(k_coarse_tail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)off));
     TailLevel<T>* dst = alloc<TailLevel<T>>(cnt);
     DR_CK(cudaMemcpy(dst, v.data(), cnt * sizeof(TailLevel<T>), cudaMemcpyHostToDevice));
@@ -526,6 +628,22 @@ void DevHier::build_tail() {
   };
   tail64_ = make(double());
   if (fp32_) tail32_ = make(float());
+}
+
+// The tail's sliced-ELL values from the current CSR values (after setup,
+// resetup and the FP32 refresh).
+void DevHier::refresh_tail() {
+  for (const TailEll& te : tail_ell_) {
+    if (te.ne == 0) continue;
+    const DevMat& A = L_[te.level].A;
+    counted();
+    k_ell_vals<double><<<grid1d(te.ne, max_grid_), kBlock, 0, st_>>>(te.ne, te.perm, A.v, te.v64);
+    if (te.v32 && A.v32) {
+      counted();
+      k_ell_vals<float><<<grid1d(te.ne, max_grid_), kBlock, 0, st_>>>(te.ne, te.perm, A.v32, te.v32);
+    }
+  }
+  DR_CK(cudaGetLastError());
 }
 
 void DevHier::refresh_fp32() {
@@ -627,8 +745,11 @@ T* DevHier::cycle_level(int l, T* x, const T* b, bool x_zero, const CycleOpts& o
     TailCoarse<T> C{nc_, clu_, cpiv_, coarse_b<T>(), coarse_x<T>(), tail_co_[slot][0], tail_co_[slot][1],
                     tail_co_[slot][2], tail_co_[slot][3]};
     counted();
+    const TailCopyList& cl = tail_cp_[slot];
+    const TailCopies cp{static_cast<const TailCopy*>(cl.list), cl.npat, cl.nval, cl.pat_bytes,
+                        cl.val_bytes, TailCopy{cl.xsrc, cl.xoff, cl.xbytes}};
     launch_dependent(k_coarse_tail<T>, 1, kern::kTailThreads, tail_bytes_[slot], st_,
-                     static_cast<const TailLevel<T>*>(desc), nlevels() - l, C, o.pre, o.post,
+                     static_cast<const TailLevel<T>*>(desc), nlevels() - l, C, cp, o.pre, o.post,
                      o.w ? 1 : 0, x_zero ? 1 : 0, g_err);
     DR_CK(cudaGetLastError());
     return x;
@@ -992,6 +1113,7 @@ void DevHier::resetup_values(const double* v_dev) {
   k_lu_factor<<<1, threads, 0, st_>>>(nc_, clu_, cpiv_, info_);
   DR_CK(cudaGetLastError());
   refresh_fp32();
+  refresh_tail();
   check_kernel_flag(st_);
   int info = 0;
   DR_CK(cudaMemcpyAsync(&info, info_, sizeof(int), cudaMemcpyDeviceToHost, st_));

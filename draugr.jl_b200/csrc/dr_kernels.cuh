@@ -688,6 +688,15 @@ __global__ void k_convert(long long n, const TS* __restrict__ s, TD* __restrict_
     d[i] = (TD)s[i];
 }
 
+// Sliced-ELL values of the coarse tail from the CSR values (pad slots: 0).
+template <typename T>
+__global__ void k_ell_vals(int ne, const int* __restrict__ perm, const T* __restrict__ v, T* __restrict__ ev) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ne; i += gridDim.x * blockDim.x) {
+    const int p = perm[i];
+    ev[i] = p >= 0 ? v[p] : T(0);
+  }
+}
+
 // dot(a, b) with deterministic finalize
 template <typename TA, typename TB, class Fin>
 __global__ void __launch_bounds__(kBlock)
@@ -778,11 +787,19 @@ __global__ void k_lu_solve(int n, const double* __restrict__ lu, const int* __re
 // work is a few microseconds, where launch and drain latency dominate.
 // Only the top level's right-hand side (and iterate, when it does not start
 // at zero) is read from global memory, and only its result is written back.
+//
+// A level's matrix is held in sliced ELL form: rows in slices of 32, entry
+// j of row 32 s + l at eoff[s] + 32 j + l (elen[i] entries in row i, in
+// column order).  One thread per row then reads consecutive words across a
+// warp (CSR rows read one per thread collide on shared-memory banks when
+// their lengths are near multiples of 32), and still sums its row in
+// column order.  Its values are gathered from the CSR values (k_ell_vals)
+// whenever those change.
 template <typename T>
 struct TailLevel {
-  int n, nc, annz, pnnz;
-  const int *arp, *aci;
-  const T *av, *invd;
+  int n, nc, ne, pnnz;  // rows, coarse rows, ELL slots, nonzeros of P
+  const int *ecol, *elen, *eoff;
+  const T *ev, *invd;
   T omega;
   const int *prp, *pci;
   const T* pv;
@@ -790,7 +807,8 @@ struct TailLevel {
   const T* rv;
   T *xa, *xb, *b, *r;  // iterate pair, right-hand side, residual
   // byte offsets of the shared-memory copies (arrays above, in order)
-  unsigned o_arp, o_aci, o_av, o_invd, o_prp, o_pci, o_pv, o_rrp, o_rci, o_rv, o_xa, o_xb, o_b, o_r;
+  unsigned o_ecol, o_elen, o_eoff, o_ev, o_invd, o_prp, o_pci, o_pv, o_rrp, o_rci, o_rv, o_xa, o_xb,
+      o_b, o_r;
 };
 
 template <typename T>
@@ -805,6 +823,23 @@ struct TailCoarse {
 };
 
 constexpr int kTailMaxLevels = 8;
+
+// One bulk copy of the tail's prologue: `bytes` (a multiple of 16) from
+// `src` to shared-memory offset `off`.
+struct TailCopy {
+  const void* src;
+  unsigned off, bytes;
+};
+
+// The tail's copies: pattern arrays first (never written by a kernel),
+// then the rest; x, the top level's iterate, is copied only when the
+// visit does not start from zero.
+struct TailCopies {
+  const TailCopy* list;
+  int npat, nval;
+  unsigned pat_bytes, val_bytes;
+  TailCopy x;
+};
 
 // a ± Σ_k v[k]·x[c[k]] over [s, e) in column order, eight loads in flight
 template <int SIGN, typename T>
@@ -821,10 +856,28 @@ __device__ __forceinline__ T tail_row(T a, const int* __restrict__ c, const T* _
   return a;
 }
 
+// a ± Σ_j A_ij x_j over row i of a sliced-ELL matrix, in column order
+template <int SIGN, typename T>
+__device__ __forceinline__ T tail_ell_row(T a, const TailLevel<T>& L, const T* x, int i) {
+  const int base = L.eoff[i >> 5] + (i & 31), len = L.elen[i];
+  for (int j0 = 0; j0 < len; j0 += 8) {
+    T p[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int k = base + 32 * (j0 + j);
+      p[j] = (j0 + j < len) ? mul_rn(L.ev[k], x[L.ecol[k]]) : T(0);
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      if (j0 + j < len) a = SIGN > 0 ? add_rn(a, p[j]) : sub_rn(a, p[j]);
+  }
+  return a;
+}
+
 template <typename T>
 __device__ void tail_jacobi(const TailLevel<T>& L, const T* x, const T* b, T* xn) {
   for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
-    const T ri = tail_row<-1>(b[i], L.aci, L.av, x, L.arp[i], L.arp[i + 1]);
+    const T ri = tail_ell_row<-1>(b[i], L, x, i);
     xn[i] = add_rn(x[i], mul_rn(mul_rn(L.omega, L.invd[i]), ri));
   }
   __syncthreads();
@@ -926,8 +979,7 @@ __device__ void tail_visit(const TailLevel<T>* lv, int l, int nl, const TailCoar
       T* u = x; x = t; t = u;
     }
   }
-  for (int i = threadIdx.x; i < L.n; i += blockDim.x)
-    L.r[i] = sub_rn(b[i], tail_row<1>(T(0), L.aci, L.av, x, L.arp[i], L.arp[i + 1]));
+  for (int i = threadIdx.x; i < L.n; i += blockDim.x) L.r[i] = sub_rn(b[i], tail_ell_row<1>(T(0), L, x, i));
   __syncthreads();
   const bool last = (l + 1 == nl);
   T* bn = last ? C.b : lv[l + 1].b;
@@ -967,64 +1019,42 @@ constexpr int kTailThreads = 256;
 // returns without touching global memory.
 template <typename T>
 __global__ void __launch_bounds__(kTailThreads)
-k_coarse_tail(const TailLevel<T>* __restrict__ lv, int nl, TailCoarse<T> C, int pre, int post,
-              int wcycle, int x_zero, int* err) {
+k_coarse_tail(const TailLevel<T>* __restrict__ lv, int nl, TailCoarse<T> C, TailCopies cp, int pre,
+              int post, int wcycle, int x_zero, int* err) {
   extern __shared__ __align__(16) unsigned char tsm[];
   __shared__ TailLevel<T> sl[kTailMaxLevels];
   __shared__ TailCoarse<T> sc;
   __shared__ __align__(8) uint64_t bar;
   __shared__ int ok;
-  if (threadIdx.x == 0) {
-    mbar_init(&bar, 1);
-    fence_mbar_init();
-  }
-  // every array of the tail: (shared-memory offset, source, bytes); the
-  // patterns (never written by a kernel) and the rest (values, factors,
-  // the top level's right-hand side and iterate)
-  auto patterns = [&](auto&& f) {
-    for (int k = 0; k < nl; ++k) {
-      const TailLevel<T>& g = lv[k];
-      f(g.o_arp, g.arp, 4 * (size_t)(g.n + 1));
-      f(g.o_aci, g.aci, 4 * (size_t)g.annz);
-      f(g.o_prp, g.prp, 4 * (size_t)(g.n + 1));
-      f(g.o_pci, g.pci, 4 * (size_t)g.pnnz);
-      f(g.o_rrp, g.rrp, 4 * (size_t)(g.nc + 1));
-      f(g.o_rci, g.rci, 4 * (size_t)g.pnnz);
+  // warp 0 issues the copies, one per lane at a time
+  if (threadIdx.x < 32) {
+    if (threadIdx.x == 0) {
+      mbar_init(&bar, 1);
+      fence_mbar_init();
+      mbar_expect_tx(&bar, cp.pat_bytes + cp.val_bytes + (x_zero ? 0u : cp.x.bytes));
     }
-  };
-  auto values = [&](auto&& f) {
-    for (int k = 0; k < nl; ++k) {
-      const TailLevel<T>& g = lv[k];
-      f(g.o_av, g.av, sizeof(T) * (size_t)g.annz);
-      f(g.o_invd, g.invd, sizeof(T) * (size_t)g.n);
-      f(g.o_pv, g.pv, sizeof(T) * (size_t)g.pnnz);
-      f(g.o_rv, g.rv, sizeof(T) * (size_t)g.pnnz);
+    __syncwarp();
+    for (int i = threadIdx.x; i < cp.npat; i += 32) {
+      const TailCopy c = cp.list[i];
+      bulk_g2s(tsm + c.off, c.src, c.bytes, &bar);
     }
-    f(C.o_lu, C.lu, 8 * (size_t)C.n * C.n);
-    f(C.o_piv, C.piv, 4 * (size_t)C.n);
-    f(lv[0].o_b, lv[0].b, sizeof(T) * (size_t)lv[0].n);
-    if (!x_zero) f(lv[0].o_xa, lv[0].xa, sizeof(T) * (size_t)lv[0].n);
-  };
-  auto copy = [&](unsigned off, const void* src, size_t b) {
-    if (b) bulk_g2s(tsm + off, src, (uint32_t)((b + 15) & ~(size_t)15), &bar);
-  };
-  if (threadIdx.x == 0) {
-    uint32_t total = 0;
-    auto add = [&](unsigned, const void*, size_t b) { total += (uint32_t)((b + 15) & ~(size_t)15); };
-    patterns(add);
-    values(add);
-    mbar_expect_tx(&bar, total);
-    patterns(copy);
   }
   pdl_trigger();
   pdl_wait();
-  if (threadIdx.x == 0) values(copy);
+  if (threadIdx.x < 32) {
+    for (int i = threadIdx.x; i < cp.nval; i += 32) {
+      const TailCopy c = cp.list[cp.npat + i];
+      bulk_g2s(tsm + c.off, c.src, c.bytes, &bar);
+    }
+    if (threadIdx.x == 0 && !x_zero && cp.x.bytes) bulk_g2s(tsm + cp.x.off, cp.x.src, cp.x.bytes, &bar);
+  }
   if (threadIdx.x < nl) {
     const TailLevel<T> g = lv[threadIdx.x];
     TailLevel<T> v = g;
-    v.arp = reinterpret_cast<const int*>(tsm + g.o_arp);
-    v.aci = reinterpret_cast<const int*>(tsm + g.o_aci);
-    v.av = reinterpret_cast<const T*>(tsm + g.o_av);
+    v.ecol = reinterpret_cast<const int*>(tsm + g.o_ecol);
+    v.elen = reinterpret_cast<const int*>(tsm + g.o_elen);
+    v.eoff = reinterpret_cast<const int*>(tsm + g.o_eoff);
+    v.ev = reinterpret_cast<const T*>(tsm + g.o_ev);
     v.invd = reinterpret_cast<const T*>(tsm + g.o_invd);
     v.prp = reinterpret_cast<const int*>(tsm + g.o_prp);
     v.pci = reinterpret_cast<const int*>(tsm + g.o_pci);
