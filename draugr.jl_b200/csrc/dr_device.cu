@@ -439,44 +439,41 @@ static constexpr size_t kTailSmem = 200 * 1024;
 
 static size_t a16(size_t b) { return (b + 15) & ~(size_t)15; }
 
-// Sliced-ELL layout of a tail level's matrix (see TailLevel): slot of
-// entry j of row 32 s + l is eoff[s] + 32 j + l; perm maps each slot to its
-// CSR position (-1 for padding).
-struct EllPattern {
-  std::vector<int> col, len, off, perm;
-};
-
-static EllPattern ell_of(const std::vector<int>& rp, const std::vector<int>& ci) {
-  EllPattern E;
-  const int n = (int)rp.size() - 1, ns = (n + 31) / 32;
-  E.len.resize(n);
-  E.off.resize(ns);
-  int total = 0;
-  for (int s = 0; s < ns; ++s) {
-    int w = 0;
-    for (int i = 32 * s; i < std::min(n, 32 * s + 32); ++i) w = std::max(w, rp[i + 1] - rp[i]);
-    E.off[s] = total;
-    total += 32 * w;
-  }
-  E.col.assign(total, 0);
-  E.perm.assign(total, -1);
-  for (int i = 0; i < n; ++i) {
-    E.len[i] = rp[i + 1] - rp[i];
-    const int base = E.off[i / 32] + (i % 32);
-    for (int j = 0; j < E.len[i]; ++j) {
-      E.col[base + 32 * j] = ci[rp[i] + j];
-      E.perm[base + 32 * j] = rp[i] + j;
+// Thread -> row order of a tail level (see TailLevel): each warp of 32
+// takes one row per starting position modulo 32 while such rows remain,
+// then rows from the fullest positions.
+static std::vector<int> bank_order(const std::vector<int>& rp) {
+  const int n = (int)rp.size() - 1;
+  std::vector<std::vector<int>> bucket(32);
+  for (int i = 0; i < n; ++i) bucket[rp[i] & 31].push_back(i);
+  std::vector<size_t> pos(32, 0);
+  std::vector<int> ord;
+  ord.reserve(n);
+  auto left = [&](int r) { return bucket[r].size() - pos[r]; };
+  while ((int)ord.size() < n) {
+    int filled = 0;
+    for (int r = 0; r < 32; ++r)
+      if (left(r) > 0) {
+        ord.push_back(bucket[r][pos[r]++]);
+        ++filled;
+      }
+    while (filled < 32 && (int)ord.size() < n) {
+      int best = 0;
+      for (int r = 1; r < 32; ++r)
+        if (left(r) > left(best)) best = r;
+      ord.push_back(bucket[best][pos[best]++]);
+      ++filled;
     }
   }
-  return E;
+  return ord;
 }
 
 template <typename T>
-static size_t tail_level_bytes(const DevLevel& d, int ne) {
-  const size_t n = d.A.n, nc = d.P.m, pn = d.P.nnz, ns = (n + 31) / 32;
-  return a16(4 * (size_t)ne) + a16(4 * n) + a16(4 * ns) + a16(sizeof(T) * (size_t)ne) +
-         a16(sizeof(T) * n) + a16(4 * (n + 1)) + a16(4 * pn) + a16(sizeof(T) * pn) +
-         a16(4 * (nc + 1)) + a16(4 * pn) + a16(sizeof(T) * pn) + 4 * a16(sizeof(T) * n);
+static size_t tail_level_bytes(const DevLevel& d) {
+  const size_t n = d.A.n, nc = d.P.m, an = d.A.nnz, pn = d.P.nnz;
+  return a16(4 * (n + 1)) + a16(4 * an) + a16(4 * n) + a16(sizeof(T) * an) + a16(sizeof(T) * n) +
+         a16(4 * (n + 1)) + a16(4 * pn) + a16(sizeof(T) * pn) + a16(4 * (nc + 1)) + a16(4 * pn) +
+         a16(sizeof(T) * pn) + 4 * a16(sizeof(T) * n);
 }
 
 template <typename T>
@@ -487,45 +484,26 @@ static size_t tail_coarse_bytes(int nc) {
 void DevHier::build_tail() {
   const int nl = nlevels();
   tail_ = nl;
-  tail_ell_.clear();
   size_t total = tail_coarse_bytes<double>(nc_);
-  std::vector<EllPattern> ells;  // from the coarsest level up
+  std::vector<std::vector<int>> ords;  // from the coarsest level up
   for (int l = nl - 1; l >= 1 && nl - l <= kern::kTailMaxLevels; --l) {
     const DevLevel& d = L_[l];
     const bool jac = d.smoother == SmootherKind::Jacobi || d.smoother == SmootherKind::L1Jacobi;
-    if (!jac || d.A.n > 4096 || d.A.nnz > (1 << 16)) break;
-    std::vector<int> rp(d.A.n + 1), ci(d.A.nnz);
+    total += tail_level_bytes<double>(d);
+    if (!jac || d.A.n > 4096 || total > kTailSmem) break;
+    std::vector<int> rp(d.A.n + 1);
     DR_CK(cudaMemcpy(rp.data(), d.A.rp, rp.size() * sizeof(int), cudaMemcpyDeviceToHost));
-    if (!ci.empty()) DR_CK(cudaMemcpy(ci.data(), d.A.ci, ci.size() * sizeof(int), cudaMemcpyDeviceToHost));
-    EllPattern E = ell_of(rp, ci);
-    total += tail_level_bytes<double>(d, (int)E.col.size());
-    if (total > kTailSmem) break;
+    ords.push_back(bank_order(rp));
     tail_ = l;
-    ells.push_back(std::move(E));
   }
   if (tail_ >= nl) return;
   const int cnt = nl - tail_;
-  std::reverse(ells.begin(), ells.end());  // tail_ first
+  std::reverse(ords.begin(), ords.end());  // tail_ first
+  std::vector<int*> ord_dev(cnt);
   for (int k = 0; k < cnt; ++k) {
-    const EllPattern& E = ells[k];
-    TailEll te;
-    te.level = tail_ + k;
-    te.ne = (int)E.col.size();
-    te.col = alloc<int>(E.col.size());
-    te.len = alloc<int>(E.len.size());
-    te.off = alloc<int>(E.off.size());
-    te.perm = alloc<int>(E.perm.size());
-    te.v64 = alloc<double>(E.col.size());
-    if (!E.col.empty()) {
-      DR_CK(cudaMemcpy(te.col, E.col.data(), E.col.size() * sizeof(int), cudaMemcpyHostToDevice));
-      DR_CK(cudaMemcpy(te.perm, E.perm.data(), E.perm.size() * sizeof(int), cudaMemcpyHostToDevice));
-    }
-    DR_CK(cudaMemcpy(te.len, E.len.data(), E.len.size() * sizeof(int), cudaMemcpyHostToDevice));
-    DR_CK(cudaMemcpy(te.off, E.off.data(), E.off.size() * sizeof(int), cudaMemcpyHostToDevice));
-    if (fp32_) te.v32 = alloc<float>(E.col.size());
-    tail_ell_.push_back(te);
+    ord_dev[k] = alloc<int>(ords[k].size());
+    DR_CK(cudaMemcpy(ord_dev[k], ords[k].data(), ords[k].size() * sizeof(int), cudaMemcpyHostToDevice));
   }
-  refresh_tail();
   auto make = [&](auto tag) {
     using T = decltype(tag);
     const int slot = sizeof(T) == 8 ? 0 : 1;
@@ -539,17 +517,16 @@ void DevHier::build_tail() {
     for (int k = 0; k < cnt; ++k) {
       DevLevel& d = L_[tail_ + k];
       LevelVecs<T>& V = vecs<T>(tail_ + k);
-      const TailEll& te = tail_ell_[k];
       TailLevel<T>& t = v[k];
-      const size_t n = d.A.n, nc = d.P.m, ns = (n + 31) / 32;
+      const size_t n = d.A.n, nc = d.P.m;
       t.n = d.A.n;
       t.nc = d.P.m;
-      t.ne = te.ne;
+      t.annz = (int)d.A.nnz;
       t.pnnz = (int)d.P.nnz;
-      t.ecol = te.col;
-      t.elen = te.len;
-      t.eoff = te.off;
-      t.ev = sizeof(T) == 8 ? reinterpret_cast<const T*>(te.v64) : reinterpret_cast<const T*>(te.v32);
+      t.arp = d.A.rp;
+      t.aci = d.A.ci;
+      t.ord = ord_dev[k];
+      t.av = mval<T>(d.A);
       t.invd = invd<T>(d);
       t.omega = (T)d.omega;
       t.prp = d.P.rp;
@@ -562,10 +539,10 @@ void DevHier::build_tail() {
       t.xb = V.xb;
       t.b = V.b;
       t.r = V.r;
-      t.o_ecol = take(4 * (size_t)te.ne);
-      t.o_elen = take(4 * n);
-      t.o_eoff = take(4 * ns);
-      t.o_ev = take(sizeof(T) * (size_t)te.ne);
+      t.o_arp = take(4 * (n + 1));
+      t.o_aci = take(4 * (size_t)d.A.nnz);
+      t.o_ord = take(4 * n);
+      t.o_av = take(sizeof(T) * (size_t)d.A.nnz);
       t.o_invd = take(sizeof(T) * n);
       t.o_prp = take(4 * (n + 1));
       t.o_pci = take(4 * (size_t)d.P.nnz);
@@ -592,15 +569,15 @@ void DevHier::build_tail() {
     };
     for (int k = 0; k < cnt; ++k) {
       const TailLevel<T>& t = v[k];
-      const size_t n = t.n, ns = (n + 31) / 32;
-      rec(pat, t.o_ecol, t.ecol, 4 * (size_t)t.ne);
-      rec(pat, t.o_elen, t.elen, 4 * n);
-      rec(pat, t.o_eoff, t.eoff, 4 * ns);
+      const size_t n = t.n;
+      rec(pat, t.o_arp, t.arp, 4 * (n + 1));
+      rec(pat, t.o_aci, t.aci, 4 * (size_t)t.annz);
+      rec(pat, t.o_ord, t.ord, 4 * n);
       rec(pat, t.o_prp, t.prp, 4 * (n + 1));
       rec(pat, t.o_pci, t.pci, 4 * (size_t)t.pnnz);
       rec(pat, t.o_rrp, t.rrp, 4 * ((size_t)t.nc + 1));
       rec(pat, t.o_rci, t.rci, 4 * (size_t)t.pnnz);
-      rec(val, t.o_ev, t.ev, sizeof(T) * (size_t)t.ne);
+      rec(val, t.o_av, t.av, sizeof(T) * (size_t)t.annz);
       rec(val, t.o_invd, t.invd, sizeof(T) * n);
       rec(val, t.o_pv, t.pv, sizeof(T) * (size_t)t.pnnz);
       rec(val, t.o_rv, t.rv, sizeof(T) * (size_t)t.pnnz);
@@ -628,22 +605,6 @@ void DevHier::build_tail() {
   };
   tail64_ = make(double());
   if (fp32_) tail32_ = make(float());
-}
-
-// The tail's sliced-ELL values from the current CSR values (after setup,
-// resetup and the FP32 refresh).
-void DevHier::refresh_tail() {
-  for (const TailEll& te : tail_ell_) {
-    if (te.ne == 0) continue;
-    const DevMat& A = L_[te.level].A;
-    counted();
-    k_ell_vals<double><<<grid1d(te.ne, max_grid_), kBlock, 0, st_>>>(te.ne, te.perm, A.v, te.v64);
-    if (te.v32 && A.v32) {
-      counted();
-      k_ell_vals<float><<<grid1d(te.ne, max_grid_), kBlock, 0, st_>>>(te.ne, te.perm, A.v32, te.v32);
-    }
-  }
-  DR_CK(cudaGetLastError());
 }
 
 void DevHier::refresh_fp32() {
@@ -1113,7 +1074,6 @@ void DevHier::resetup_values(const double* v_dev) {
   k_lu_factor<<<1, threads, 0, st_>>>(nc_, clu_, cpiv_, info_);
   DR_CK(cudaGetLastError());
   refresh_fp32();
-  refresh_tail();
   check_kernel_flag(st_);
   int info = 0;
   DR_CK(cudaMemcpyAsync(&info, info_, sizeof(int), cudaMemcpyDeviceToHost, st_));

@@ -205,15 +205,6 @@ class DevHier {
   int tail_ = 0;
   void* tail64_ = nullptr;   // device TailLevel<double>[nlevels - tail_]
   void* tail32_ = nullptr;   // device TailLevel<float>[...] once FP32 buffers exist
-  // sliced-ELL copies of the tail levels' matrices (k_coarse_tail)
-  struct TailEll {
-    int level = 0, ne = 0;
-    int *col = nullptr, *len = nullptr, *off = nullptr, *perm = nullptr;
-    double* v64 = nullptr;
-    float* v32 = nullptr;
-  };
-  std::vector<TailEll> tail_ell_;
-  void refresh_tail();
   size_t tail_bytes_[2] = {0, 0};        // shared memory of the tail kernel (FP64, FP32)
   struct TailCopyList {  // its prologue's bulk copies (kern::TailCopies)
     const void* list = nullptr;

@@ -688,15 +688,6 @@ __global__ void k_convert(long long n, const TS* __restrict__ s, TD* __restrict_
     d[i] = (TD)s[i];
 }
 
-// Sliced-ELL values of the coarse tail from the CSR values (pad slots: 0).
-template <typename T>
-__global__ void k_ell_vals(int ne, const int* __restrict__ perm, const T* __restrict__ v, T* __restrict__ ev) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ne; i += gridDim.x * blockDim.x) {
-    const int p = perm[i];
-    ev[i] = p >= 0 ? v[p] : T(0);
-  }
-}
-
 // dot(a, b) with deterministic finalize
 template <typename TA, typename TB, class Fin>
 __global__ void __launch_bounds__(kBlock)
@@ -788,18 +779,17 @@ __global__ void k_lu_solve(int n, const double* __restrict__ lu, const int* __re
 // Only the top level's right-hand side (and iterate, when it does not start
 // at zero) is read from global memory, and only its result is written back.
 //
-// A level's matrix is held in sliced ELL form: rows in slices of 32, entry
-// j of row 32 s + l at eoff[s] + 32 j + l (elen[i] entries in row i, in
-// column order).  One thread per row then reads consecutive words across a
-// warp (CSR rows read one per thread collide on shared-memory banks when
-// their lengths are near multiples of 32), and still sums its row in
-// column order.  Its values are gathered from the CSR values (k_ell_vals)
-// whenever those change.
+// Rows are handed to threads in a per-level order (ord) in which the 32
+// rows of each warp start, as far as the pattern allows, at 32 different
+// positions modulo 32: one thread per row then reads its row's columns and
+// values from shared memory without bank conflicts (rows in natural order
+// collide when their lengths are near multiples of 32), and still sums the
+// row in column order.
 template <typename T>
 struct TailLevel {
-  int n, nc, ne, pnnz;  // rows, coarse rows, ELL slots, nonzeros of P
-  const int *ecol, *elen, *eoff;
-  const T *ev, *invd;
+  int n, nc, annz, pnnz;  // rows, coarse rows, nonzeros of A and of P
+  const int *arp, *aci, *ord;
+  const T *av, *invd;
   T omega;
   const int *prp, *pci;
   const T* pv;
@@ -807,7 +797,7 @@ struct TailLevel {
   const T* rv;
   T *xa, *xb, *b, *r;  // iterate pair, right-hand side, residual
   // byte offsets of the shared-memory copies (arrays above, in order)
-  unsigned o_ecol, o_elen, o_eoff, o_ev, o_invd, o_prp, o_pci, o_pv, o_rrp, o_rci, o_rv, o_xa, o_xb,
+  unsigned o_arp, o_aci, o_ord, o_av, o_invd, o_prp, o_pci, o_pv, o_rrp, o_rci, o_rv, o_xa, o_xb,
       o_b, o_r;
 };
 
@@ -856,28 +846,11 @@ __device__ __forceinline__ T tail_row(T a, const int* __restrict__ c, const T* _
   return a;
 }
 
-// a ± Σ_j A_ij x_j over row i of a sliced-ELL matrix, in column order
-template <int SIGN, typename T>
-__device__ __forceinline__ T tail_ell_row(T a, const TailLevel<T>& L, const T* x, int i) {
-  const int base = L.eoff[i >> 5] + (i & 31), len = L.elen[i];
-  for (int j0 = 0; j0 < len; j0 += 8) {
-    T p[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const int k = base + 32 * (j0 + j);
-      p[j] = (j0 + j < len) ? mul_rn(L.ev[k], x[L.ecol[k]]) : T(0);
-    }
-#pragma unroll
-    for (int j = 0; j < 8; ++j)
-      if (j0 + j < len) a = SIGN > 0 ? add_rn(a, p[j]) : sub_rn(a, p[j]);
-  }
-  return a;
-}
-
 template <typename T>
 __device__ void tail_jacobi(const TailLevel<T>& L, const T* x, const T* b, T* xn) {
-  for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
-    const T ri = tail_ell_row<-1>(b[i], L, x, i);
+  for (int t = threadIdx.x; t < L.n; t += blockDim.x) {
+    const int i = L.ord[t];
+    const T ri = tail_row<-1>(b[i], L.aci, L.av, x, L.arp[i], L.arp[i + 1]);
     xn[i] = add_rn(x[i], mul_rn(mul_rn(L.omega, L.invd[i]), ri));
   }
   __syncthreads();
@@ -979,7 +952,10 @@ __device__ void tail_visit(const TailLevel<T>* lv, int l, int nl, const TailCoar
       T* u = x; x = t; t = u;
     }
   }
-  for (int i = threadIdx.x; i < L.n; i += blockDim.x) L.r[i] = sub_rn(b[i], tail_ell_row<1>(T(0), L, x, i));
+  for (int t = threadIdx.x; t < L.n; t += blockDim.x) {
+    const int i = L.ord[t];
+    L.r[i] = sub_rn(b[i], tail_row<1>(T(0), L.aci, L.av, x, L.arp[i], L.arp[i + 1]));
+  }
   __syncthreads();
   const bool last = (l + 1 == nl);
   T* bn = last ? C.b : lv[l + 1].b;
@@ -1051,10 +1027,10 @@ k_coarse_tail(const TailLevel<T>* __restrict__ lv, int nl, TailCoarse<T> C, Tail
   if (threadIdx.x < nl) {
     const TailLevel<T> g = lv[threadIdx.x];
     TailLevel<T> v = g;
-    v.ecol = reinterpret_cast<const int*>(tsm + g.o_ecol);
-    v.elen = reinterpret_cast<const int*>(tsm + g.o_elen);
-    v.eoff = reinterpret_cast<const int*>(tsm + g.o_eoff);
-    v.ev = reinterpret_cast<const T*>(tsm + g.o_ev);
+    v.arp = reinterpret_cast<const int*>(tsm + g.o_arp);
+    v.aci = reinterpret_cast<const int*>(tsm + g.o_aci);
+    v.ord = reinterpret_cast<const int*>(tsm + g.o_ord);
+    v.av = reinterpret_cast<const T*>(tsm + g.o_av);
     v.invd = reinterpret_cast<const T*>(tsm + g.o_invd);
     v.prp = reinterpret_cast<const int*>(tsm + g.o_prp);
     v.pci = reinterpret_cast<const int*>(tsm + g.o_pci);
