@@ -314,6 +314,7 @@ DevHier::DevHier(const HostHierarchy& H, int device) {
       }
       d.has_rap = h.has_rap_map;
       if (d.has_rap) up_csr(d.AP, h.A.n, h.P.nc, h.ap_rp, h.ap_ci, nullptr);
+
       const int n = h.A.n;
       if (l > 0) {
         d.v64.xa = alloc<double>(n);
@@ -1024,6 +1025,19 @@ int DevHier::pcg(double* x, const double* b, const CycleOpts& o, double tol, int
 }
 
 // ------------------------------------------------------------ resetup
+// One Galerkin product O = S·B (k_spgemm_warp): 8 warps per block, output
+// rows of up to 384 entries staged in shared memory (longer rows work in
+// place in global memory; a wider stage at lower occupancy measured slower
+// on the 128^3 27-point hierarchy).
+void DevHier::spgemm(DevMat& O, const DevMat& S, const DevMat& B) {
+  constexpr int W = 8, CAP = 384;
+  counted();
+  const int grid = std::max(1, std::min((O.n + W - 1) / W, max_grid_));
+  k_spgemm_warp<CAP, W><<<grid, W * 32, spgemm_smem_bytes<CAP, W>(), st_>>>(
+      O.n, O.rp, O.ci, O.v, S.rp, S.ci, S.v, B.rp, B.ci, B.v);
+  DR_CK(cudaGetLastError());
+}
+
 void DevHier::resetup_values(const double* v_dev) {
   const int nl = nlevels();
   for (int l = 0; l < nl; ++l)
@@ -1047,20 +1061,8 @@ void DevHier::resetup_values(const double* v_dev) {
   for (int l = 0; l < nl; ++l) {
     DevLevel& d = L_[l];
     DevMat& next = (l + 1 < nl) ? L_[l + 1].A : C_;
-    {
-      const int grid = std::max(1, std::min((d.A.n + (kBlock / 8) - 1) / (kBlock / 8), max_grid_));
-      counted();
-      k_spgemm_rows<8, 120><<<grid, kBlock, 0, st_>>>(d.AP.n, d.AP.rp, d.AP.ci, d.AP.v, d.A.rp, d.A.ci,
-                                                      d.A.v, d.P.rp, d.P.ci, d.P.v);
-      DR_CK(cudaGetLastError());
-    }
-    {
-      const int grid = std::max(1, std::min((next.n + (kBlock / 32) - 1) / (kBlock / 32), max_grid_));
-      counted();
-      k_spgemm_rows<32, 500><<<grid, kBlock, 0, st_>>>(next.n, next.rp, next.ci, next.v, d.R.rp, d.R.ci,
-                                                       d.R.v, d.AP.rp, d.AP.ci, d.AP.v);
-      DR_CK(cudaGetLastError());
-    }
+    spgemm(d.AP, d.A, d.P);
+    spgemm(next, d.R, d.AP);
     if (l + 1 < nl) upd_invd(L_[l + 1]);
   }
   // coarsest dense matrix and its LU

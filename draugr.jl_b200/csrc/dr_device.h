@@ -200,6 +200,7 @@ class DevHier {
   void ensure_fp32();
   void refresh_fp32();
   void build_tail();
+  void spgemm(DevMat& O, const DevMat& S, const DevMat& B);
   // Levels tail_ .. nlevels-1 run as one single-block kernel (k_coarse_tail);
   // tail_ = nlevels() when no level qualifies.
   int tail_ = 0;

@@ -1163,74 +1163,123 @@ __global__ void k_l1_invdiag(int n, const int* __restrict__ rp, const double* __
 }
 
 // ------------------------------------------------------------ Galerkin product
-// One output row per group of G lanes:  out_I = Σ_k s_Ik · B_{j_k}  on the
-// fixed sorted pattern of out_I.  Phase 1 (A·P): s = A, B = P.  Phase 2
-// (Pᵀ·(AP)): s = R = Pᵀ in transpose-map order, B = A·P.  The k loop is
-// sequential and each B row holds a column at most once, so every output
-// entry accumulates its terms in (k, B-entry) order with no two lanes
-// touching the same entry in one step: the sum is deterministic and equal to
-// a sequential CPU loop in that order (products and sums rounded
-// separately).  Output positions are found by binary search in the pattern
-// row, staged in shared memory when it fits.
-template <int G, int CAP>
-__global__ void __launch_bounds__(kBlock)
-k_spgemm_rows(int nrows, const int* __restrict__ out_rp, const int* __restrict__ out_ci,
+// Phase 1 (A·P): S = A, B = P.  Phase 2 (Pᵀ·(AP)): S = R = Pᵀ in
+// transpose-map order, B = A·P.
+//
+// Numeric sparse product O = S·B on O's fixed, sorted sparsity pattern (the
+// Galerkin products A·P and Pᵀ·(AP) of a partial resetup), one warp per
+// output row, deterministic and without atomics.
+//
+// The products of row I are numbered in the order (entry k of S's row,
+// entry t of B's row j_k).  For each run of 32 entries of S's row the warp
+// scans the lengths of the B rows they select; then, 32 products at a time,
+// every lane finds its product's entry (a shuffle search over the scan),
+// forms it and looks its column up in O's row pattern (binary search;
+// staged in shared memory when the row has at most CAP entries).  Products
+// that land on the same output entry are added by the lowest of their lanes
+// in lane order, after the entry's earlier sum: every entry accumulates its
+// products in the same order as a sequential loop over (k, t) — the order
+// of the CPU setup's numeric product, bit for bit.
+//
+// WPB warps per block; the per-warp row patterns and sums (CAP entries each)
+// live in dynamic shared memory: spgemm_smem_bytes<CAP, WPB>().
+template <int CAP, int WPB>
+constexpr size_t spgemm_smem_bytes() {
+  return (size_t)WPB * CAP * (sizeof(double) + sizeof(int)) + (size_t)WPB * 32 * sizeof(double);
+}
+
+template <int CAP, int WPB>
+__global__ void __launch_bounds__(WPB * 32)
+k_spgemm_warp(int nrows, const int* __restrict__ out_rp, const int* __restrict__ out_ci,
               double* __restrict__ out_v, const int* __restrict__ s_rp, const int* __restrict__ s_ci,
               const double* __restrict__ s_v, const int* __restrict__ b_rp,
               const int* __restrict__ b_ci, const double* __restrict__ b_v) {
-  constexpr int GPB = kBlock / G;  // groups per block
-  __shared__ int scol[GPB][CAP];
-  __shared__ double sacc[GPB][CAP];
-  const int lane = threadIdx.x & (G - 1);
-  const int gl = threadIdx.x / G;
-  const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
-  const long long ngroups = (long long)gridDim.x * GPB;
-  for (long long I0 = (long long)blockIdx.x * GPB + gl; I0 < nrows; I0 += ngroups) {
+  extern __shared__ __align__(16) unsigned char gsm[];
+  double (*sacc)[CAP] = reinterpret_cast<double (*)[CAP]>(gsm);
+  double (*sprod)[32] = reinterpret_cast<double (*)[32]>(gsm + (size_t)WPB * CAP * sizeof(double));
+  int (*scol)[CAP] = reinterpret_cast<int (*)[CAP]>(gsm + (size_t)WPB * (CAP + 32) * sizeof(double));
+  const int lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5;
+  const unsigned full = 0xffffffffu;
+  for (long long I0 = (long long)blockIdx.x * WPB + w; I0 < nrows; I0 += (long long)gridDim.x * WPB) {
     const int I = (int)I0;
     const int os = out_rp[I], oe = out_rp[I + 1];
     const int m = oe - os;
     const bool fits = m <= CAP;
-    if (fits) {
-      for (int t = lane; t < m; t += G) {
-        scol[gl][t] = out_ci[os + t];
-        sacc[gl][t] = 0.0;
-      }
-    } else {
-      for (int t = lane; t < m; t += G) out_v[os + t] = 0.0;
+    const int* pat = fits ? scol[w] : out_ci + os;
+    double* acc = fits ? sacc[w] : out_v + os;
+    for (int t = lane; t < m; t += 32) {
+      if (fits) scol[w][t] = out_ci[os + t];
+      acc[t] = 0.0;
     }
-    __syncwarp(gmask);
+    __syncwarp();
     const int ss = s_rp[I], se = s_rp[I + 1];
-    for (int k = ss; k < se; ++k) {
-      const int j = s_ci[k];
-      const double sv = s_v[k];
-      const int bs = b_rp[j], be = b_rp[j + 1];
-      for (int t = bs + lane; t < be; t += G) {
-        const int J = b_ci[t];
-        const double prod = __dmul_rn(sv, b_v[t]);
-        int lo = 0, hi = m - 1, pos = -1;
-        if (fits) {
-          while (lo <= hi) {
-            int mid = (lo + hi) >> 1;
-            int c = scol[gl][mid];
-            if (c == J) { pos = mid; break; }
-            if (c < J) lo = mid + 1; else hi = mid - 1;
-          }
-          if (pos >= 0) sacc[gl][pos] = __dadd_rn(sacc[gl][pos], prod);
-        } else {
-          while (lo <= hi) {
-            int mid = (lo + hi) >> 1;
-            int c = out_ci[os + mid];
-            if (c == J) { pos = mid; break; }
-            if (c < J) lo = mid + 1; else hi = mid - 1;
-          }
-          if (pos >= 0) out_v[os + pos] = __dadd_rn(out_v[os + pos], prod);
-        }
+    for (int k0 = ss; k0 < se; k0 += 32) {
+      const int k = k0 + lane;
+      int bs = 0, len = 0;
+      double sv = 0.0;
+      if (k < se) {
+        const int j = s_ci[k];
+        sv = s_v[k];
+        bs = b_rp[j];
+        len = b_rp[j + 1] - bs;
       }
-      __syncwarp(gmask);
+      int incl = len;  // inclusive scan of the selected B rows' lengths
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(full, incl, o);
+        if (lane >= o) incl += y;
+      }
+      const int excl = incl - len;
+      const int total = __shfl_sync(full, incl, 31);
+      for (int f0 = 0; f0 < total; f0 += 32) {
+        const int f = f0 + lane;
+        // the entry of S's row that owns product f: the largest q with excl_q <= f
+        int q = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+          const int ex = __shfl_sync(full, excl, q + step);
+          if (ex <= f) q += step;
+        }
+        const int qbs = __shfl_sync(full, bs, q);
+        const int qex = __shfl_sync(full, excl, q);
+        const double qsv = __shfl_sync(full, sv, q);
+        const bool act = f < total;
+        int pos = -1;
+        double prod = 0.0;
+        if (act) {
+          const int t = qbs + (f - qex);
+          const int J = b_ci[t];
+          prod = __dmul_rn(qsv, b_v[t]);
+          int lo = 0, hi = m - 1;
+          while (lo <= hi) {
+            const int mid = (lo + hi) >> 1;
+            const int c = pat[mid];
+            if (c == J) {
+              pos = mid;
+              break;
+            }
+            if (c < J) lo = mid + 1;
+            else hi = mid - 1;
+          }
+        }
+        sprod[w][lane] = prod;
+        const unsigned am = __ballot_sync(full, pos >= 0);
+        __syncwarp();
+        if (pos >= 0) {
+          const unsigned peers = __match_any_sync(am, pos);
+          if (lane == __ffs(peers) - 1) {
+            double a = acc[pos];
+            for (unsigned mm = peers; mm; mm &= mm - 1) a = __dadd_rn(a, sprod[w][__ffs(mm) - 1]);
+            acc[pos] = a;
+          }
+        }
+        __syncwarp();
+      }
     }
     if (fits)
-      for (int t = lane; t < m; t += G) out_v[os + t] = sacc[gl][t];
-    __syncwarp(gmask);
+      for (int t = lane; t < m; t += 32) out_v[os + t] = sacc[w][t];
+    __syncwarp();
   }
 }
 

@@ -285,3 +285,16 @@ def test_residual_entry_point(fresh_case):
     if _single_lane(h, 0)[0]:
         assert np.array_equal(r, ref)
     assert abs(rn.value - np.linalg.norm(ref)) <= 1e-12 * np.linalg.norm(ref)
+
+
+def test_resetup_reproduces_setup_values_bit_exact(fresh_case):
+    """The GPU Galerkin products accumulate every entry in the order of the
+    CPU setup's numeric product: a partial resetup with the setup's own
+    values reproduces every level (and the coarsest dense matrix) exactly."""
+    name, A, cfg, h, O = fresh_case
+    before = [h.export(l, "A_nzval").copy() for l in range(h.nlevels)]
+    dense = h.export(-1, "C_dense").copy()
+    draugr.amg_resetup(h, A, cfg, partial=True)
+    for l in range(h.nlevels):
+        assert np.array_equal(h.export(l, "A_nzval"), before[l]), (name, l)
+    assert np.array_equal(h.export(-1, "C_dense"), dense)
