@@ -262,40 +262,7 @@ DevHier::DevHier(const HostHierarchy& H, int device) {
     nnz0_ = nl ? H.levels[0].A.nnz() : H.coarse.nnz();
     L_.resize(nl);
     auto up_csr = [&](DevMat& M, int n, int m, const std::vector<int>& rp, const std::vector<int>& ci,
-                      const std::vector<double>* v) {
-      M.n = n;
-      M.m = m;
-      M.nnz = (long long)ci.size();
-      M.rp = alloc<int>(rp.size());
-      // column and value arrays carry 4 padding entries for the tile
-      // kernel's 128-bit loads
-      M.ci = alloc<int>(ci.size() + 4);
-      h2d(M.rp, rp, st_);
-      h2d(M.ci, ci, st_);
-      M.v = alloc<double>(ci.size() + 4);
-      if (v) h2d(M.v, *v, st_);
-      M.Ggs = pick_G(M.nnz, n);
-      M.form = row_form(rp);
-      std::vector<int> base;
-      std::vector<int> tiles = make_tiles(rp, ci, n, M.form.nt / M.form.G, base);
-      std::vector<int> tstart(tiles.size());
-      for (size_t t = 0; t < tiles.size(); ++t) tstart[t] = rp[tiles[t]];
-      M.ntiles = (int)tiles.size() - 1;
-      M.tp = alloc<int>(tiles.size());
-      M.ts = alloc<int>(tiles.size());
-      M.tb = alloc<int>(base.size());
-      DR_CK(cudaMemcpy(M.tp, tiles.data(), tiles.size() * sizeof(int), cudaMemcpyHostToDevice));
-      DR_CK(cudaMemcpy(M.ts, tstart.data(), tstart.size() * sizeof(int), cudaMemcpyHostToDevice));
-      DR_CK(cudaMemcpy(M.tb, base.data(), base.size() * sizeof(int), cudaMemcpyHostToDevice));
-      // 16-bit column offsets from each tile's smallest column (8 padding
-      // entries for the tile kernel's 16-byte-rounded copies)
-      std::vector<uint16_t> off(ci.size() + 8, 0);
-      for (int t = 0; t < M.ntiles; ++t)
-        if (base[t] >= 0)
-          for (int k = tstart[t]; k < tstart[t + 1]; ++k) off[k] = (uint16_t)(ci[k] - base[t]);
-      M.cu = alloc<uint16_t>(off.size());
-      DR_CK(cudaMemcpy(M.cu, off.data(), off.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
-    };
+                      const std::vector<double>* v) { upload_csr(M, n, m, rp, ci, v); };
     for (int l = 0; l < nl; ++l) {
       const HostLevel& h = H.levels[l];
       DevLevel& d = L_[l];
@@ -361,6 +328,45 @@ DevHier::DevHier(const HostHierarchy& H, int device) {
   }
 }
 
+// Upload a CSR pattern (and optionally values) with the row kernel's
+// tiling and 16-bit column offsets.  Host arrays must outlive the stream's
+// copies (callers synchronise the stream before releasing them).
+void DevHier::upload_csr(DevMat& M, int n, int m, const std::vector<int>& rp, const std::vector<int>& ci,
+                       const std::vector<double>* v) {
+  M.n = n;
+  M.m = m;
+  M.nnz = (long long)ci.size();
+  M.rp = alloc<int>(rp.size());
+  // column and value arrays carry 4 padding entries for the tile
+  // kernel's 128-bit loads
+  M.ci = alloc<int>(ci.size() + 4);
+  h2d(M.rp, rp, st_);
+  h2d(M.ci, ci, st_);
+  M.v = alloc<double>(ci.size() + 4);
+  if (v) h2d(M.v, *v, st_);
+  M.Ggs = pick_G(M.nnz, n);
+  M.form = row_form(rp);
+  std::vector<int> base;
+  std::vector<int> tiles = make_tiles(rp, ci, n, M.form.nt / M.form.G, base);
+  std::vector<int> tstart(tiles.size());
+  for (size_t t = 0; t < tiles.size(); ++t) tstart[t] = rp[tiles[t]];
+  M.ntiles = (int)tiles.size() - 1;
+  M.tp = alloc<int>(tiles.size());
+  M.ts = alloc<int>(tiles.size());
+  M.tb = alloc<int>(base.size());
+  DR_CK(cudaMemcpy(M.tp, tiles.data(), tiles.size() * sizeof(int), cudaMemcpyHostToDevice));
+  DR_CK(cudaMemcpy(M.ts, tstart.data(), tstart.size() * sizeof(int), cudaMemcpyHostToDevice));
+  DR_CK(cudaMemcpy(M.tb, base.data(), base.size() * sizeof(int), cudaMemcpyHostToDevice));
+  // 16-bit column offsets from each tile's smallest column (8 padding
+  // entries for the tile kernel's 16-byte-rounded copies)
+  std::vector<uint16_t> off(ci.size() + 8, 0);
+  for (int t = 0; t < M.ntiles; ++t)
+    if (base[t] >= 0)
+      for (int k = tstart[t]; k < tstart[t + 1]; ++k) off[k] = (uint16_t)(ci[k] - base[t]);
+  M.cu = alloc<uint16_t>(off.size());
+  DR_CK(cudaMemcpy(M.cu, off.data(), off.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
+  }
+
 DevHier::~DevHier() {
   cudaSetDevice(device_);
   if (st_) cudaStreamSynchronize(st_);
@@ -407,7 +413,7 @@ template <> double* DevHier::coarse_x<double>() { return cx64_; }
 template <> float* DevHier::coarse_x<float>() { return cx32_; }
 template <> const double* DevHier::mval<double>(const DevMat& M) const { return M.v; }
 template <> const float* DevHier::mval<float>(const DevMat& M) const { return M.v32; }
-template <> const double* DevHier::invd<double>(const DevLevel& L) const { return L.invd; }
+template <> const double* DevHier::invd<double>(const DevLevel& L) const { return tr_ ? L.invdT : L.invd; }
 template <> const float* DevHier::invd<float>(const DevLevel& L) const { return L.invd32; }
 
 // ------------------------------------------------------------ FP32 copies
@@ -628,7 +634,7 @@ template <typename T>
 T* DevHier::smooth(int l, T* x, const T* b, int steps, T* ext, const double* rz_w, bool rz_first) {
   DevLevel& L = L_[l];
   LevelVecs<T>& V = vecs<T>(l);
-  const DevMat& A = L.A;
+  const DevMat& A = tr_ ? L.At : L.A;
   const T om = (T)L.omega;
   if (L.smoother == SmootherKind::Jacobi || L.smoother == SmootherKind::L1Jacobi) {
     for (int s = 0; s < steps; ++s) {
@@ -672,7 +678,7 @@ T* DevHier::smooth(int l, T* x, const T* b, int steps, T* ext, const double* rz_
 
 template <typename T>
 void DevHier::residual(int l, const T* x, const T* b, T* r, double* rr_dst) {
-  const DevMat& A = l < nlevels() ? L_[l].A : C_;
+  const DevMat& A = l < nlevels() ? (tr_ ? L_[l].At : L_[l].A) : C_;
   if (rr_dst)
     launch_rows_dot(st_, max_grid_, A, mval<T>(A), XPlain<T>{x}, EpResidual<T>{b, r}, partials_,
                     tickets_ + TK_RES, FinStore{rr_dst});
@@ -689,6 +695,11 @@ void DevHier::coarse_solve(const T* b, T* x) {
   const size_t lbytes = (size_t)nc_ * nc_ * sizeof(double);
   const int staged = (ybytes + lbytes) <= 40 * 1024 ? 1 : 0;
   counted();
+  if (tr_) {  // A_c^T y = b with the factors of A_c (adjoint solves)
+    k_lu_solve_t<T><<<1, 32, ybytes, st_>>>(nc_, clu_, cpiv_, b, x);
+    DR_CK(cudaGetLastError());
+    return;
+  }
   k_lu_solve<T><<<1, threads, ybytes + (staged ? lbytes : 0), st_>>>(nc_, clu_, cpiv_, b, x, staged);
   DR_CK(cudaGetLastError());
 }
@@ -701,7 +712,7 @@ bool DevHier::fused_rz_ok(const CycleOpts& o) const {
 template <typename T>
 T* DevHier::cycle_level(int l, T* x, const T* b, bool x_zero, const CycleOpts& o, T* ext,
                         const double* rz_w, bool rz_first, bool x1_ready) {
-  if (l >= 1 && l == tail_ && x == vecs<T>(l).xa) {
+  if (!tr_ && l >= 1 && l == tail_ && x == vecs<T>(l).xa) {
     const void* desc = sizeof(T) == 8 ? tail64_ : tail32_;
     const int slot = sizeof(T) == 8 ? 0 : 1;
     TailCoarse<T> C{nc_, clu_, cpiv_, coarse_b<T>(), coarse_x<T>(), tail_co_[slot][0], tail_co_[slot][1],
@@ -718,7 +729,7 @@ T* DevHier::cycle_level(int l, T* x, const T* b, bool x_zero, const CycleOpts& o
   }
   DevLevel& L = L_[l];
   LevelVecs<T>& V = vecs<T>(l);
-  const DevMat& A = L.A;
+  const DevMat& A = tr_ ? L.At : L.A;
   const T om = (T)L.omega;
   const bool jac = (L.smoother == SmootherKind::Jacobi || L.smoother == SmootherKind::L1Jacobi);
   bool have_r = false;
@@ -833,6 +844,165 @@ int DevHier::solve(double* x, const double* b, const CycleOpts& o, double tol, i
   if (verbose >= 1) std::printf("AMG solve did NOT converge: %d iterations, final residual %.2e\n", maxiter, rel);
   if (relres) *relres = rel;
   return maxiter;
+}
+
+// ------------------------------------------------------------ transposed hierarchy
+// A^T of every level (pattern transposed on the host once, values gathered
+// from A's whenever those change) with the smoother diagonal of A^T, for
+// cycles on A^T: the same P and R, coarse operators P^T A^T P = (P^T A P)^T,
+// the coarsest solve with the transposed LU factors.  Jacobi-type smoothers.
+void DevHier::build_transpose() {
+  if (at_built_) return;
+  for (auto& d : L_)
+    if (d.smoother != SmootherKind::Jacobi && d.smoother != SmootherKind::L1Jacobi)
+      fail("transposed cycles need Jacobi or l1-Jacobi smoothing on every level");
+  DR_CK(cudaStreamSynchronize(st_));
+  std::vector<std::vector<int>> keep_rp, keep_ci;  // alive until the uploads finish
+  for (auto& d : L_) {
+    const int n = d.A.n;
+    std::vector<int> rp(n + 1), ci(d.A.nnz);
+    DR_CK(cudaMemcpy(rp.data(), d.A.rp, rp.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    if (!ci.empty()) DR_CK(cudaMemcpy(ci.data(), d.A.ci, ci.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    std::vector<int> trp(n + 1, 0), tci(ci.size()), perm(ci.size());
+    for (int k = 0; k < (int)ci.size(); ++k) ++trp[ci[k] + 1];
+    for (int j = 0; j < n; ++j) trp[j + 1] += trp[j];
+    std::vector<int> fill(trp.begin(), trp.end() - 1);
+    for (int i = 0; i < n; ++i)  // rows in order: each transposed row's columns ascend
+      for (int k = rp[i]; k < rp[i + 1]; ++k) {
+        const int q = fill[ci[k]]++;
+        tci[q] = i;
+        perm[q] = k;
+      }
+    upload_csr(d.At, n, n, trp, tci, nullptr);
+    d.at_perm = alloc<int>(perm.size());
+    h2d(d.at_perm, perm, st_);
+    d.invdT = alloc<double>(n);
+    keep_rp.push_back(std::move(trp));
+    keep_ci.push_back(std::move(tci));
+    keep_ci.push_back(std::move(perm));
+  }
+  DR_CK(cudaStreamSynchronize(st_));
+  at_built_ = true;
+  refresh_transpose();
+  DR_CK(cudaStreamSynchronize(st_));
+}
+
+void DevHier::refresh_transpose() {
+  for (auto& d : L_) {
+    if (d.A.nnz > 0) {
+      counted();
+      k_gather_vals<<<grid1d(d.A.nnz, max_grid_), kBlock, 0, st_>>>(d.A.nnz, d.at_perm, d.A.v, d.At.v);
+    }
+    counted();
+    if (d.smoother == SmootherKind::L1Jacobi)
+      k_l1_invdiag<<<grid1d(d.A.n, max_grid_), kBlock, 0, st_>>>(d.A.n, d.At.rp, d.At.v, d.invdT);
+    else
+      k_invdiag<<<grid1d(d.A.n, max_grid_), kBlock, 0, st_>>>(d.A.n, d.At.rp, d.At.ci, d.At.v, d.invdT);
+  }
+  DR_CK(cudaGetLastError());
+}
+
+void DevHier::lin3(int n, double a, const double* x, double b, const double* y, double c, const double* z,
+                   double* out) {
+  counted();
+  k_lin3<<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, a, x, b, y, c, z, out);
+  DR_CK(cudaGetLastError());
+}
+
+// z = M r: one cycle from a zero iterate (FP64), result copied to `out`.
+void DevHier::precond64(const double* r, double* out, const CycleOpts& o) {
+  if (L_.empty()) {
+    coarse_solve<double>(r, out);
+    return;
+  }
+  const double* z = cycle_level<double>(0, out, r, true, o, out);
+  if (z != out) DR_CK(cudaMemcpyAsync(out, z, (size_t)n0_ * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+}
+
+// Right-preconditioned BiCGStab (FP64) on A or, with `transpose`, on A^T
+// with cycles on the transposed hierarchy: x is the initial guess and the
+// solution (device memory).  Returns the iterations; relres = |b - A x|/|b|.
+int DevHier::bicgstab(double* x, const double* b, const CycleOpts& o, double tol, int maxiter,
+                      bool transpose, double* relres, int verbose) {
+  if (transpose) build_transpose();
+  struct Mode {
+    bool& f;
+    bool old;
+    ~Mode() { f = old; }
+  } mode{tr_, tr_};
+  tr_ = transpose;
+  graphs_clear();
+  const int n = n0_;
+  if (!bk_[0])
+    for (auto& p : bk_) p = alloc<double>(n);
+  double *r = bk_[0], *rh = bk_[1], *p = bk_[2], *v = bk_[3], *sv = bk_[4], *t = bk_[5], *ph = bk_[6],
+         *sh = bk_[7];
+  auto spmv = [&](const double* in, double* out) {
+    const DevMat& A = L_.empty() ? C_ : (tr_ ? L_[0].At : L_[0].A);
+    launch_rows(st_, max_grid_, A, A.v, XPlain<double>{in}, EpStore<double>{out});
+  };
+  const double bnorm = std::sqrt(dot_host(b, b, n));
+  if (bnorm == 0.0) {
+    counted();
+    k_fill<double><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, 0.0, x);
+    DR_CK(cudaStreamSynchronize(st_));
+    if (relres) *relres = 0.0;
+    return 0;
+  }
+  spmv(x, t);
+  lin3(n, 1.0, b, -1.0, t, 0.0, nullptr, r);  // r = b - A x
+  DR_CK(cudaMemcpyAsync(rh, r, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+  double rel = std::sqrt(dot_host(r, r, n)) / bnorm;
+  double rho = 1.0, alpha = 1.0, omega = 1.0;
+  counted();
+  k_fill<double><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, 0.0, p);
+  counted();
+  k_fill<double><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, 0.0, v);
+  int it = 0;
+  while (rel >= tol && it < maxiter) {
+    ++it;
+    const double rho1 = dot_host(rh, r, n);
+    if (rho1 == 0.0) break;  // breakdown: r orthogonal to the shadow residual
+    const double beta = (rho1 / rho) * (alpha / omega);
+    lin3(n, 1.0, r, beta, p, -beta * omega, v, p);  // p = r + beta (p - omega v)
+    precond64(p, ph, o);
+    spmv(ph, v);
+    alpha = rho1 / dot_host(rh, v, n);
+    lin3(n, 1.0, r, -alpha, v, 0.0, nullptr, sv);  // s = r - alpha v
+    const double snorm = std::sqrt(dot_host(sv, sv, n));
+    if (snorm / bnorm < tol) {
+      lin3(n, 1.0, x, alpha, ph, 0.0, nullptr, x);
+      DR_CK(cudaMemcpyAsync(r, sv, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+      rel = snorm / bnorm;
+      break;
+    }
+    precond64(sv, sh, o);
+    spmv(sh, t);
+    const double tt = dot_host(t, t, n);
+    omega = tt > 0.0 ? dot_host(t, sv, n) / tt : 0.0;
+    lin3(n, 1.0, x, alpha, ph, omega, sh, x);      // x += alpha p^ + omega s^
+    lin3(n, 1.0, sv, -omega, t, 0.0, nullptr, r);  // r = s - omega t
+    rel = std::sqrt(dot_host(r, r, n)) / bnorm;
+    rho = rho1;
+    if (verbose >= 2) std::printf("  BiCGStab iter %4d: relative residual %.6e\n", it, rel);
+    if (omega == 0.0) break;
+  }
+  // true residual of the result
+  spmv(x, t);
+  lin3(n, 1.0, b, -1.0, t, 0.0, nullptr, r);
+  rel = std::sqrt(dot_host(r, r, n)) / bnorm;
+  check_kernel_flag(st_);
+  if (relres) *relres = rel;
+  return it;
+}
+
+// dL/da_ij = -lambda_i x_j over the finest matrix's nonzeros (CSR order).
+void DevHier::nz_gradient(const double* x, const double* lam, double* grad) {
+  const DevMat& A = L_.empty() ? C_ : L_[0].A;
+  counted();
+  k_nz_grad<<<grid1d(A.n, max_grid_), kBlock, 0, st_>>>(A.n, A.rp, A.ci, x, lam, grad);
+  DR_CK(cudaGetLastError());
+  DR_CK(cudaStreamSynchronize(st_));
 }
 
 double DevHier::residual_norm(const double* x, const double* b, double* r) {
@@ -1076,6 +1246,7 @@ void DevHier::resetup_values(const double* v_dev) {
   k_lu_factor<<<1, threads, 0, st_>>>(nc_, clu_, cpiv_, info_);
   DR_CK(cudaGetLastError());
   refresh_fp32();
+  if (at_built_) refresh_transpose();
   check_kernel_flag(st_);
   int info = 0;
   DR_CK(cudaMemcpyAsync(&info, info_, sizeof(int), cudaMemcpyDeviceToHost, st_));

@@ -115,6 +115,9 @@ struct DevLevel {
   int* color_order = nullptr;
   bool has_rap = false;
   DevMat AP;                 // pattern and values of A·P (partial resetup)
+  DevMat At;                 // A^T (transposed cycles; built on first use)
+  int* at_perm = nullptr;    // At value k = A value at_perm[k]
+  double* invdT = nullptr;   // smoother diagonal of A^T
   LevelVecs<double> v64;
   LevelVecs<float> v32;
 };
@@ -152,6 +155,12 @@ class DevHier {
             double* relres);
   int pcg(double* x, const double* b, const CycleOpts& o, double tol, int maxiter, bool mixed,
           double* relres, int verbose);
+  // Right-preconditioned BiCGStab (FP64) on A, or on A^T with cycles on the
+  // transposed hierarchy (adjoint solves); Jacobi-type smoothers.
+  int bicgstab(double* x, const double* b, const CycleOpts& o, double tol, int maxiter, bool transpose,
+               double* relres, int verbose);
+  // dL/da_ij = -lambda_i x_j for the finest matrix's nonzeros (CSR order).
+  void nz_gradient(const double* x, const double* lam, double* grad);
 
   // r = b - A x on the finest level and ||r||_2 (device vectors).
   double residual_norm(const double* x, const double* b, double* r);
@@ -200,6 +209,17 @@ class DevHier {
   void ensure_fp32();
   void refresh_fp32();
   void build_tail();
+  // transposed hierarchy (adjoint solves)
+  bool at_built_ = false;
+  bool tr_ = false;          // cycle pieces use A^T (and the transposed coarsest solve)
+  void build_transpose();
+  void refresh_transpose();
+  double* bk_[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  void lin3(int n, double a, const double* x, double b, const double* y, double c, const double* z,
+            double* out);
+  void precond64(const double* r, double* out, const CycleOpts& o);
+  void upload_csr(DevMat& M, int n, int m, const std::vector<int>& rp, const std::vector<int>& ci,
+                  const std::vector<double>* v);
   void spgemm(DevMat& O, const DevMat& S, const DevMat& B);
   // Levels tail_ .. nlevels-1 run as one single-block kernel (k_coarse_tail);
   // tail_ = nlevels() when no level qualifies.

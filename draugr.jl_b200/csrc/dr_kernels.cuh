@@ -688,6 +688,36 @@ __global__ void k_convert(long long n, const TS* __restrict__ s, TD* __restrict_
     d[i] = (TD)s[i];
 }
 
+// out = a x + b y + c z (out may be x, y or z; z may be null when c = 0)
+__global__ void k_lin3(int n, double a, const double* x, double b, const double* y, double c,
+                       const double* z, double* out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double v = a * x[i] + b * y[i];
+    if (z) v += c * z[i];
+    out[i] = v;
+  }
+}
+
+// Gradient of a loss L(x), x = A^-1 b, with respect to the nonzeros of A,
+// given the adjoint lambda = A^-T dL/dx:  dL/da_ij = -lambda_i x_j, in CSR
+// order.
+__global__ void k_nz_grad(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                          const double* __restrict__ x, const double* __restrict__ lam,
+                          double* __restrict__ grad) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double li = lam[i];
+    for (int k = rp[i]; k < rp[i + 1]; ++k) grad[k] = -li * x[ci[k]];
+  }
+}
+
+// dst[k] = src[perm[k]] (values of a transposed matrix from the original's)
+__global__ void k_gather_vals(long long cnt, const int* __restrict__ perm, const double* __restrict__ src,
+                              double* __restrict__ dst) {
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < cnt;
+       k += (long long)gridDim.x * blockDim.x)
+    dst[k] = src[perm[k]];
+}
+
 // dot(a, b) with deterministic finalize
 template <typename TA, typename TB, class Fin>
 __global__ void __launch_bounds__(kBlock)
@@ -1066,6 +1096,36 @@ k_coarse_tail(const TailLevel<T>* __restrict__ lv, int nl, TailCoarse<T> C, Tail
   tail_visit(sl, 0, nl, sc, x_zero != 0, pre, post, wcycle);
   // the top level's result back to global memory
   for (int i = threadIdx.x; i < lv[0].n; i += blockDim.x) lv[0].xa[i] = sl[0].xa[i];
+}
+
+// Solve A^T y = b with the dgetf2 factors of A (A = P L U, column-major,
+// pivots piv): U^T z = b, L^T w = z, then the row interchanges in reverse
+// (dgetrs with trans = 'T').  One thread: used by adjoint solves only.
+template <typename T>
+__global__ void k_lu_solve_t(int n, const double* __restrict__ lu, const int* __restrict__ piv,
+                             const T* __restrict__ bin, T* __restrict__ xout) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  extern __shared__ double ys[];
+  for (int i = 0; i < n; ++i) ys[i] = (double)bin[i];
+  for (int j = 0; j < n; ++j) {  // U^T (lower triangular, non-unit)
+    double t = ys[j];
+    for (int i = 0; i < j; ++i) t -= lu[(size_t)j * n + i] * ys[i];
+    ys[j] = t / lu[(size_t)j * n + j];
+  }
+  for (int j = n - 1; j >= 0; --j) {  // L^T (upper triangular, unit)
+    double t = ys[j];
+    for (int i = j + 1; i < n; ++i) t -= lu[(size_t)j * n + i] * ys[i];
+    ys[j] = t;
+  }
+  for (int j = n - 1; j >= 0; --j) {
+    const int p = piv[j];
+    if (p != j) {
+      const double t = ys[j];
+      ys[j] = ys[p];
+      ys[p] = t;
+    }
+  }
+  for (int i = 0; i < n; ++i) xout[i] = (T)ys[i];
 }
 
 // In-place unblocked LU with partial pivoting (dgetf2 order) of a

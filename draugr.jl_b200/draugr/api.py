@@ -417,6 +417,90 @@ def pcg(x, b, h: Hierarchy, config: AMGConfig | None = None, tol: float = 1e-8,
     return x, it, rel.value
 
 
+def bicgstab(x, b, h: Hierarchy, config: AMGConfig | None = None, tol: float = 1e-8,
+             maxiter: int = 500, transpose: bool = False):
+    """BiCGStab preconditioned by one FP64 AMG cycle (nonsymmetric systems).
+    transpose=True solves A^T x = b with cycles on the transposed hierarchy
+    (the adjoint system of a gradient).  Returns (x, niter, relres)."""
+    config = config if config is not None else (h.config or AMGConfig())
+    lib = _lib.load()
+    rel = C.c_double(0.0)
+    if _is_device(x):
+        it = _lib.check(lib.draugr_b200_bicgstab_device(h.handle, x.numel(), x.data_ptr(), b.data_ptr(),
+                                                        config_handle(config), tol, maxiter,
+                                                        1 if transpose else 0, C.byref(rel)), "bicgstab")
+        return x, it, rel.value
+    _check_vec(x, b, h)
+    it = _lib.check(lib.draugr_b200_bicgstab(h.handle, len(x), _ptr(x), _ptr(b), config_handle(config),
+                                             tol, maxiter, 1 if transpose else 0, C.byref(rel)),
+                    "bicgstab")
+    return x, it, rel.value
+
+
+def nz_gradient(h: Hierarchy, x, lam):
+    """dL/da_ij = -lambda_i x_j for the finest matrix's nonzeros (CSR order),
+    with x = A^-1 b and lambda = A^-T dL/dx (CUDA tensors); returns a new
+    CUDA tensor of nnz entries."""
+    import torch
+
+    lib = _lib.load()
+    nnz = int(h.level_info(0)[1]) if h.nlevels > 0 else int(h.level_info(-1)[1])
+    grad = torch.empty(nnz, dtype=torch.float64, device=x.device)
+    _lib.check(lib.draugr_b200_nz_gradient_device(h.handle, x.numel(), x.data_ptr(), lam.data_ptr(),
+                                                  grad.data_ptr()), "nz_gradient")
+    return grad
+
+
+class _Solve:
+    """Holder of the torch.autograd.Function (built on first use, so that the
+    package imports without torch)."""
+    fn = None
+
+
+def amg_solve_diff(values, b, h: Hierarchy, config: AMGConfig | None = None, tol: float = 1e-12,
+                   maxiter: int = 1000, symmetric: bool = False):
+    """x = A(values)^-1 b as a differentiable torch operation (the role of a
+    ChainRulesCore rrule around solve).  values: CUDA tensor of the finest
+    matrix's nonzeros (the setup pattern, CSR order); b: CUDA tensor.  The
+    forward pass resets the hierarchy up with `values` and solves (PCG when
+    symmetric, else BiCGStab); the backward pass solves the adjoint system
+    A^T lambda = dL/dx on the transposed hierarchy (or with PCG when
+    symmetric), then dL/db = lambda and dL/da_ij = -lambda_i x_j.  Only x is
+    kept between the passes."""
+    import torch
+
+    if _Solve.fn is None:
+        class Fn(torch.autograd.Function):
+            @staticmethod
+            def forward(ctx, values, b, h, config, tol, maxiter, symmetric):
+                amg_resetup(h, values.detach().contiguous(), config)
+                x = torch.zeros_like(b)
+                bb = b.detach().contiguous()
+                if symmetric:
+                    _, it, rel = pcg(x, bb, h, config, tol=tol, maxiter=maxiter)
+                else:
+                    _, it, rel = bicgstab(x, bb, h, config, tol=tol, maxiter=maxiter)
+                ctx.h, ctx.config, ctx.tol, ctx.maxiter, ctx.symmetric = h, config, tol, maxiter, symmetric
+                ctx.save_for_backward(x)
+                return x
+
+            @staticmethod
+            def backward(ctx, gx):
+                (x,) = ctx.saved_tensors
+                lam = torch.zeros_like(x)
+                g = gx.contiguous()
+                if ctx.symmetric:
+                    pcg(lam, g, ctx.h, ctx.config, tol=ctx.tol, maxiter=ctx.maxiter)
+                else:
+                    bicgstab(lam, g, ctx.h, ctx.config, tol=ctx.tol, maxiter=ctx.maxiter, transpose=True)
+                gv = nz_gradient(ctx.h, x, lam)
+                return gv, lam, None, None, None, None, None
+
+        _Solve.fn = Fn
+    config = config if config is not None else (h.config or AMGConfig())
+    return _Solve.fn.apply(values, b, h, config, tol, maxiter, symmetric)
+
+
 def _check_vec(x, b, h):
     for name, a in (("x", x), ("b", b)):
         if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous):

@@ -153,6 +153,104 @@ def anisotropic_27pt(n: int, eps_z: float = 1e-3, kappa_elem: np.ndarray | None 
                         [valid[i] for i in order])
 
 
+def _csr_with_jacobian(n, v_rc, vals, d_rc, d_cell, d_vals, ncells):
+    """CSR matrix from value contributions (rows, cols, vals) and the sparse
+    Jacobian J (nnz x ncells) of its values with respect to cell
+    coefficients from derivative contributions (rows, cols, cells, dvals)."""
+    A = sp.csr_matrix((vals, v_rc), shape=(n, n))
+    A.sum_duplicates()
+    A.sort_indices()
+    rid = np.repeat(np.arange(n, dtype=np.int64), np.diff(A.indptr))
+    keys = rid * n + A.indices  # ascending: CSR order
+    dk = d_rc[0].astype(np.int64) * n + d_rc[1]
+    pos = np.searchsorted(keys, dk)
+    assert np.array_equal(keys[pos], dk)
+    J = sp.csr_matrix((d_vals, (pos, d_cell)), shape=(A.nnz, ncells))
+    J.sum_duplicates()
+    return A, J
+
+
+def _faces(shape):
+    """Interior faces (a, b) along each axis of a cell grid, and boundary
+    cells (one entry per boundary face)."""
+    idx = np.arange(int(np.prod(shape))).reshape(shape)
+    inner, bnd = [], []
+    for axis in range(len(shape)):
+        m = shape[axis]
+        a = np.take(idx, np.arange(m - 1), axis=axis).ravel()
+        b = np.take(idx, np.arange(1, m), axis=axis).ravel()
+        inner.append((axis, a, b))
+        for side in (0, m - 1):
+            bnd.append(np.take(idx, [side], axis=axis).ravel())
+    return inner, bnd
+
+
+def _fv_system(kappa, flux=None):
+    """Finite-volume operator of -div(kappa grad u) + div(w u) (upwind) with
+    Dirichlet boundary on a unit-spaced cell grid; flux[axis] gives, per
+    interior face (a, b) of that axis, the flux from a to b (None: no
+    convection).  Returns (A, J)."""
+    shape = kappa.shape
+    n = kappa.size
+    k = kappa.ravel()
+    inner, bnd = _faces(shape)
+    vr, vcol, vv, dr, dcol, dcell, dv = [], [], [], [], [], [], []
+
+    def val(r, c, x):
+        vr.append(r); vcol.append(c); vv.append(x)
+
+    def der(r, c, cell, x):
+        dr.append(r); dcol.append(c); dcell.append(cell); dv.append(x)
+
+    for axis, a, b in inner:
+        ka, kb = k[a], k[b]
+        T = 2 * ka * kb / (ka + kb)
+        dTa = 2 * kb * kb / (ka + kb) ** 2
+        dTb = 2 * ka * ka / (ka + kb) ** 2
+        F = flux[axis] if flux is not None else np.zeros(len(a))
+        out_a, out_b = np.maximum(F, 0.0), np.maximum(-F, 0.0)
+        for r, c, sgn, cv in ((a, a, 1.0, out_a), (b, b, 1.0, out_b), (a, b, -1.0, out_b), (b, a, -1.0, out_a)):
+            val(r, c, sgn * T + (cv if sgn > 0 else -cv))
+            der(r, c, a, sgn * dTa)
+            der(r, c, b, sgn * dTb)
+    for c in bnd:
+        val(c, c, 2 * k[c])
+        der(c, c, c, np.full(len(c), 2.0))
+    cat = np.concatenate
+    return _csr_with_jacobian(n, (cat(vr), cat(vcol)), cat(vv), (cat(dr), cat(dcol)), cat(dcell), cat(dv), n)
+
+
+def fv_diffusion_3d(kappa: np.ndarray):
+    """Cell-centred finite volumes for -div(kappa grad u) on the m^3 grid of
+    kappa ([z, y, x]), harmonic face transmissibilities, Dirichlet boundary
+    (boundary faces 2 kappa).  Symmetric.  Returns (A, J), J = d(values of
+    A)/d(kappa) (nnz x m^3)."""
+    return _fv_system(kappa)
+
+
+def convection_diffusion_2d(kappa: np.ndarray, peclet: float = 50.0, seed: int = 0):
+    """Upwind finite volumes for -div(kappa grad u) + div(w u) on the m^2
+    grid of kappa ([y, x]), Dirichlet boundary.  w is divergence-free, from a
+    seeded smooth stream function that vanishes on the boundary (no flow
+    through it), scaled so that the largest face flux is `peclet` (the cell
+    Peclet number at kappa = 1).  Nonsymmetric M-matrix.  Returns (A, J)."""
+    m = kappa.shape[0]
+    rng = np.random.default_rng(seed)
+    yy, xx = np.meshgrid(np.linspace(0, 1, m + 1), np.linspace(0, 1, m + 1), indexing="ij")
+    psi = np.zeros((m + 1, m + 1))
+    for _ in range(6):
+        kx, ky = rng.integers(1, 5, size=2)
+        ph = rng.uniform(0, 2 * np.pi, size=2)
+        psi += rng.normal() * np.sin(kx * np.pi * xx + ph[0]) * np.sin(ky * np.pi * yy + ph[1])
+    psi *= np.sin(np.pi * xx) * np.sin(np.pi * yy)  # zero on the boundary
+    fx = (psi[1:, 1:-1] - psi[:-1, 1:-1])  # x faces between cells (j, i) and (j, i+1): psi(top) - psi(bottom)
+    fy = -(psi[1:-1, 1:] - psi[1:-1, :-1])  # y faces between (j, i) and (j+1, i)
+    scale = peclet / max(np.abs(fx).max(), np.abs(fy).max(), 1e-300)
+    # face order of _faces: axis 0 (y) faces, then axis 1 (x) faces, each raveled [y, x]
+    flux = {0: (fy * scale).ravel(), 1: (fx * scale).ravel()}
+    return _fv_system(kappa, flux)
+
+
 def rhs(n: int, seed: int = 0) -> np.ndarray:
     """b ~ U(-1, 1), seeded."""
     return np.random.default_rng(seed).uniform(-1.0, 1.0, n)

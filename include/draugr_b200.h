@@ -104,6 +104,29 @@ int32_t draugr_b200_pcg_device(int32_t handle, int32_t n, double *x_dev, const d
                                int32_t config_handle, double tol, int32_t maxiter,
                                int32_t precision, double *relres);
 
+/* BiCGStab preconditioned (on the right) by one FP64 AMG cycle per
+ * application, until ||b - M x|| / ||b|| < tol, for nonsymmetric systems.
+ * transpose 0: M = A.  transpose 1: M = A^T, the adjoint system of a
+ * gradient computation, with cycles on the transposed hierarchy (A^T on
+ * every level, the same P and P^T, the transposed coarsest LU solve);
+ * every level must use (l1-)Jacobi smoothing.  x holds the initial guess;
+ * relres (may be NULL) receives the final true relative residual.  Returns
+ * iterations or -1.  No counterpart in the reference, which has neither a
+ * nonsymmetric Krylov solver nor adjoints. */
+int32_t draugr_b200_bicgstab(int32_t handle, int32_t n, double *x, const double *b,
+                             int32_t config_handle, double tol, int32_t maxiter,
+                             int32_t transpose, double *relres);
+int32_t draugr_b200_bicgstab_device(int32_t handle, int32_t n, double *x_dev, const double *b_dev,
+                                    int32_t config_handle, double tol, int32_t maxiter,
+                                    int32_t transpose, double *relres);
+
+/* Gradient of a loss L(x), x = A^-1 b, with respect to the nonzeros of the
+ * finest matrix: grad[k] = -lambda_i x_j for nonzero k = (i, j) in CSR
+ * order, where lambda = A^-T dL/dx (device vectors; grad has nnz entries).
+ * dL/db is lambda itself.  No counterpart in the reference. */
+int32_t draugr_b200_nz_gradient_device(int32_t handle, int32_t n, const double *x_dev,
+                                       const double *lambda_dev, double *grad_dev);
+
 /* One operation on one level, host arrays in and out (kernel-level checks).
  * op 0: y = A x (in1 = x)            op 1: r = b - A x (in1 = x, in2 = b)
  * op 2: `steps` smoother sweeps from x (in1) for rhs b (in2)
