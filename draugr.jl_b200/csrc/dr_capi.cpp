@@ -34,12 +34,12 @@ std::mutex g_mu;
 std::map<int32_t, Config> g_cfg;
 std::map<int32_t, std::shared_ptr<Hier>> g_hier;
 int32_t g_next = 1;
-std::string g_last_error;
+// The last error of the calling thread (the reference keeps one per
+// process; per thread, a host that calls from several threads reads the
+// message of its own failed call).
+thread_local std::string g_last_error;
 
-void set_error(const std::string& m) {
-  std::lock_guard<std::mutex> lk(g_mu);
-  g_last_error = m;
-}
+void set_error(const std::string& m) { g_last_error = m; }
 
 int32_t new_handle() { return g_next++; }
 

@@ -38,8 +38,29 @@ static inline void counted() { g_launches.fetch_add(1, std::memory_order_relaxed
 
 // SM count of the device in use and a device flag the row kernels set when a
 // bounded wait gives up (checked after every solve / resetup).
-static int g_nsm = 148;
-static int* g_err = nullptr;
+static std::atomic<int> g_nsm{148};  // SM count (written by every hierarchy constructor)
+// Flag a row kernel sets when a bounded wait gave up, one per device
+// (allocated once, under a lock: hierarchies may be built from several
+// host threads).  Shared by the hierarchies of a device; the host reads and
+// clears it after each solve.
+static std::mutex g_err_mu;
+static std::atomic<int*> g_err_dev[64];
+
+static int* err_flag() {
+  int dev = 0;
+  DR_CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) fail("device index out of range");
+  int* p = g_err_dev[dev].load(std::memory_order_acquire);
+  if (p) return p;
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  p = g_err_dev[dev].load(std::memory_order_relaxed);
+  if (!p) {
+    DR_CK(cudaMalloc(&p, sizeof(int)));
+    DR_CK(cudaMemset(p, 0, sizeof(int)));
+    g_err_dev[dev].store(p, std::memory_order_release);
+  }
+  return p;
+}
 
 void cuda_check(cudaError_t e, const char* what, const char* file, int line) {
   if (e != cudaSuccess) {
@@ -170,7 +191,7 @@ void launch_rows_impl(cudaStream_t st, int max_grid, const RowForm& f, int n, in
     const int grid = std::max(                                                                   \
         1, std::min({ntiles, max_grid, g_nsm * resident_blocks((const void*)kf, NT, smem)}));    \
     launch_dependent(kf, grid, NT, smem, st, ntiles, tp, ts, tb, rp, ci, cu, av, xl, ep, partials, \
-                     ticket, fin, g_err);                                                        \
+                     ticket, fin, err_flag());                                                   \
   } while (0)
   // 16-bit column offsets where lanes read consecutive entries (flat and
   // tree forms), and for FP32 rows of 12-32 entries, where the bytes saved
@@ -247,10 +268,7 @@ DevHier::DevHier(const HostHierarchy& H, int device) {
   DR_CK(cudaDeviceGetAttribute(&nsm_, cudaDevAttrMultiProcessorCount, device));
   max_grid_ = nsm_ * 8;
   g_nsm = nsm_;
-  if (!g_err) {
-    DR_CK(cudaMalloc(&g_err, sizeof(int)));
-    DR_CK(cudaMemset(g_err, 0, sizeof(int)));
-  }
+  err_flag();
   DR_CK(cudaStreamCreateWithFlags(&own_st_, cudaStreamNonBlocking));
   st_ = own_st_;
   own_stream_ = true;
@@ -382,10 +400,11 @@ DevHier::~DevHier() {
 // cleared so the hierarchy stays usable).
 static void check_kernel_flag(cudaStream_t st) {
   int e = 0;
-  DR_CK(cudaMemcpyAsync(&e, g_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  int* flag = err_flag();
+  DR_CK(cudaMemcpyAsync(&e, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
   DR_CK(cudaStreamSynchronize(st));
   if (e) {
-    DR_CK(cudaMemsetAsync(g_err, 0, sizeof(int), st));
+    DR_CK(cudaMemsetAsync(flag, 0, sizeof(int), st));
     DR_CK(cudaStreamSynchronize(st));
     fail("a row kernel timed out waiting for its tile copy (results discarded)");
   }
@@ -486,6 +505,30 @@ static size_t tail_level_bytes(const DevLevel& d) {
 template <typename T>
 static size_t tail_coarse_bytes(int nc) {
   return a16(8 * ((size_t)nc * nc + nc)) + a16(4 * (size_t)nc) + 2 * a16(sizeof(T) * nc);
+}
+
+// The tail kernel's dynamic shared-memory limit is a per-function setting
+// shared by every hierarchy of the process: raise it once per device to
+// the opt-in maximum (a limit, not an allocation), so that no hierarchy's
+// tail size lowers another's.
+template <typename T>
+static void allow_tail_smem() {
+  static std::mutex mu;
+  static bool done[64] = {false};
+  int dev = 0;
+  DR_CK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev < 0 || dev >= 64 || done[dev]) return;
+  int optin = 0;
+  DR_CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  int stat = 0;
+  {
+    cudaFuncAttributes fa{};
+    DR_CK(cudaFuncGetAttributes(&fa, k_coarse_tail<T>));
+    stat = (int)fa.sharedSizeBytes;
+  }
+  DR_CK(cudaFuncSetAttribute(k_coarse_tail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - stat));
+  done[dev] = true;
 }
 
 void DevHier::build_tail() {
@@ -605,7 +648,7 @@ void DevHier::build_tail() {
     TailCopy* dl = alloc<TailCopy>(pat.size());
     DR_CK(cudaMemcpy(dl, pat.data(), pat.size() * sizeof(TailCopy), cudaMemcpyHostToDevice));
     cl.list = dl;
-    DR_CK(cudaFuncSetAttribute(k_coarse_tail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)off));
+    allow_tail_smem<T>();
     TailLevel<T>* dst = alloc<TailLevel<T>>(cnt);
     DR_CK(cudaMemcpy(dst, v.data(), cnt * sizeof(TailLevel<T>), cudaMemcpyHostToDevice));
     return (void*)dst;
@@ -723,7 +766,7 @@ T* DevHier::cycle_level(int l, T* x, const T* b, bool x_zero, const CycleOpts& o
                         cl.val_bytes, TailCopy{cl.xsrc, cl.xoff, cl.xbytes}};
     launch_dependent(k_coarse_tail<T>, 1, kern::kTailThreads, tail_bytes_[slot], st_,
                      static_cast<const TailLevel<T>*>(desc), nlevels() - l, C, cp, o.pre, o.post,
-                     o.w ? 1 : 0, x_zero ? 1 : 0, g_err);
+                     o.w ? 1 : 0, x_zero ? 1 : 0, err_flag());
     DR_CK(cudaGetLastError());
     return x;
   }

@@ -501,6 +501,26 @@ def amg_solve_diff(values, b, h: Hierarchy, config: AMGConfig | None = None, tol
     return _Solve.fn.apply(values, b, h, config, tol, maxiter, symmetric)
 
 
+def pcg_batch(hierarchies, xs, bs, config: AMGConfig | None = None, tol: float = 1e-8,
+              maxiter: int = 500, precision: str = "mixed", workers: int = 16):
+    """PCG on many independent systems at once: each hierarchy runs on its
+    own CUDA stream, driven by one host thread of a pool of `workers`, so
+    the small kernels of many systems share the GPU.  xs / bs: per-system
+    vectors (CUDA tensors or NumPy arrays), x updated in place.  Returns a
+    list of (niter, relres, seconds) per system."""
+    import time
+    from concurrent.futures import ThreadPoolExecutor
+
+    def one(k):
+        t0 = time.perf_counter()
+        _, it, rel = pcg(xs[k], bs[k], hierarchies[k], config, tol=tol, maxiter=maxiter,
+                         precision=precision)
+        return it, rel, time.perf_counter() - t0
+
+    with ThreadPoolExecutor(max_workers=max(1, min(workers, len(hierarchies)))) as ex:
+        return list(ex.map(one, range(len(hierarchies))))
+
+
 def _check_vec(x, b, h):
     for name, a in (("x", x), ("b", b)):
         if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous):
