@@ -1,0 +1,435 @@
+// Block (multi-right-hand-side) solves: k <= 32 systems with the same
+// operator, vectors stored row-major as n x k (column c of row i at
+// i*k + c).  Every level matrix is read once per block product for all k
+// columns, which turns the bandwidth of k separate solves (k passes over
+// the matrices) into one pass plus the vector traffic.
+//
+// Kernels: one warp per row, lane c works on column c.  The warp reads 32
+// of the row's entries at a time (coalesced) and hands them to every lane
+// by shuffle; each lane gathers x[col][lane] (the k columns of a row are
+// contiguous, so the warp's gather is one contiguous span) and sums its
+// row in column order with separately rounded products and sums, as the
+// reference's loops do.  Deterministic column dot products: per-warp
+// partials reduced in a fixed order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "dr_device.h"
+
+namespace dr {
+
+namespace {
+
+constexpr int kBlock = 256;
+constexpr int kWarps = kBlock / 32;
+
+__device__ __forceinline__ double rn_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float rn_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double rn_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float rn_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double rn_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float rn_sub(float a, float b) { return __fsub_rn(a, b); }
+
+enum : int { BM_STORE = 0, BM_RESID = 1, BM_JACOBI = 2, BM_ADDTO = 3 };
+
+// Y = A X (STORE), Y = B - A X (RESID), Y = X + (omega d)(B - A X)
+// (JACOBI), Y += A X (ADDTO, A = P), for k columns.
+template <typename TA, typename T, int MODE>
+__global__ void __launch_bounds__(kBlock)
+k_spmm(int nrows, int k, const int* __restrict__ rp, const int* __restrict__ ci, const TA* __restrict__ av,
+       const T* __restrict__ X, const T* __restrict__ B, const T* __restrict__ dinv, T omega, T* Y) {
+  const int lane = threadIdx.x & 31;
+  const bool col = lane < k;
+  const long long nw = (long long)gridDim.x * kWarps;
+  for (long long r0 = (long long)blockIdx.x * kWarps + (threadIdx.x >> 5); r0 < nrows; r0 += nw) {
+    const int row = (int)r0;
+    const int rs = rp[row], re = rp[row + 1];
+    T acc = T(0);
+    if (col) {
+      if (MODE == BM_ADDTO) acc = Y[(size_t)row * k + lane];
+      if (MODE == BM_JACOBI) acc = B[(size_t)row * k + lane];
+    }
+    for (int k0 = rs; k0 < re; k0 += 32) {
+      const int my = k0 + lane;
+      const int cj = my < re ? ci[my] : 0;
+      const T vj = my < re ? (T)av[my] : T(0);
+      const int cnt = min(32, re - k0);
+      for (int j = 0; j < cnt; ++j) {
+        const int c = __shfl_sync(0xffffffffu, cj, j);
+        const T v = __shfl_sync(0xffffffffu, vj, j);
+        if (col) {
+          const T p = rn_mul(v, X[(size_t)c * k + lane]);
+          acc = (MODE == BM_JACOBI) ? rn_sub(acc, p) : rn_add(acc, p);
+        }
+      }
+    }
+    if (col) {
+      const size_t o = (size_t)row * k + lane;
+      if (MODE == BM_RESID) Y[o] = rn_sub(B[o], acc);
+      else if (MODE == BM_JACOBI) Y[o] = rn_add(X[o], rn_mul(rn_mul(omega, dinv[row]), acc));
+      else Y[o] = acc;
+    }
+  }
+}
+
+template <typename T>
+__global__ void k_bl_fill(long long n, T* __restrict__ x) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    x[i] = T(0);
+}
+
+// X = (omega d) B  (first Jacobi step from a zero iterate)
+template <typename T>
+__global__ void k_bl_jz(int n, int k, const T* __restrict__ B, const T* __restrict__ dinv, T omega,
+                        T* __restrict__ X) {
+  const long long tot = (long long)n * k;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x)
+    X[e] = rn_mul(rn_mul(omega, dinv[e / k]), B[e]);
+}
+
+// Coarsest solve for k columns with the dgetf2 factors (dgetrs order),
+// one thread per column, its vector in shared memory (n * k doubles of
+// dynamic shared memory; every thread reads the same factor entry at a
+// time, a broadcast).
+template <typename T>
+__global__ void k_bl_lu(int n, int k, const double* __restrict__ lu, const int* __restrict__ piv,
+                        const T* __restrict__ B, T* __restrict__ X) {
+  extern __shared__ double ysm[];
+  const int c = threadIdx.x;
+  if (c >= k) return;
+  double* y = ysm + (size_t)c;  // element i at y[i * k]
+  for (int i = 0; i < n; ++i) y[(size_t)i * k] = (double)B[(size_t)i * k + c];
+  for (int j = 0; j < n; ++j) {
+    const int p = piv[j];
+    if (p != j) {
+      const double t = y[(size_t)j * k];
+      y[(size_t)j * k] = y[(size_t)p * k];
+      y[(size_t)p * k] = t;
+    }
+  }
+  for (int j = 0; j < n; ++j) {
+    const double yj = y[(size_t)j * k];
+    if (yj != 0.0)
+      for (int i = j + 1; i < n; ++i)
+        y[(size_t)i * k] = __dsub_rn(y[(size_t)i * k], __dmul_rn(yj, lu[(size_t)j * n + i]));
+  }
+  for (int j = n - 1; j >= 0; --j) {
+    if (y[(size_t)j * k] != 0.0) y[(size_t)j * k] = __ddiv_rn(y[(size_t)j * k], lu[(size_t)j * n + j]);
+    const double yj = y[(size_t)j * k];
+    if (yj != 0.0)
+      for (int i = 0; i < j; ++i)
+        y[(size_t)i * k] = __dsub_rn(y[(size_t)i * k], __dmul_rn(yj, lu[(size_t)j * n + i]));
+  }
+  for (int i = 0; i < n; ++i) X[(size_t)i * k + c] = (T)y[(size_t)i * k];
+}
+
+// Column dot products a_c . b_c: per-block partials part[block][c]
+// (warps take rows, lane c accumulates column c, warps summed in order).
+__global__ void __launch_bounds__(kBlock)
+k_bl_dot_part(int n, int k, const double* __restrict__ a, const double* __restrict__ b,
+              double* __restrict__ part) {
+  __shared__ double ws[kWarps][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double s = 0.0;
+  if (lane < k)
+    for (long long r = (long long)blockIdx.x * kWarps + w; r < n; r += (long long)gridDim.x * kWarps) {
+      const size_t o = (size_t)r * k + lane;
+      s += a[o] * b[o];
+    }
+  ws[w][lane] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double t = 0.0;
+    for (int q = 0; q < kWarps; ++q) t += ws[q][threadIdx.x];
+    if (threadIdx.x < k) part[(size_t)blockIdx.x * 32 + threadIdx.x] = t;
+  }
+}
+
+// Column totals of the partials: 32 groups of blocks per column (strided),
+// then the groups in order — 1024 threads, a fixed summation order.
+__global__ void __launch_bounds__(1024)
+k_bl_dot_final(int nblocks, int k, const double* __restrict__ part, double* __restrict__ out) {
+  __shared__ double g[32][33];
+  const int c = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double t = 0.0;
+  if (c < k)
+    for (int q = w; q < nblocks; q += 32) t += part[(size_t)q * 32 + c];
+  g[w][c] = t;
+  __syncthreads();
+  if (w == 0 && c < k) {
+    double s = 0.0;
+    for (int q = 0; q < 32; ++q) s += g[q][c];
+    out[c] = s;
+  }
+}
+
+// X += alpha_c P, R -= alpha_c Q (and R32 = (float) R when given)
+__global__ void k_bl_update(int n, int k, const double* __restrict__ alpha, double* __restrict__ X,
+                            double* __restrict__ R, const double* __restrict__ P, const double* __restrict__ Q,
+                            float* __restrict__ R32) {
+  const long long tot = (long long)n * k;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    const double a = alpha[e % k];
+    X[e] += a * P[e];
+    const double r = R[e] - a * Q[e];
+    R[e] = r;
+    if (R32) R32[e] = (float)r;
+  }
+}
+
+// P = Z + beta_c P
+__global__ void k_bl_dir(int n, int k, const double* __restrict__ beta, const double* __restrict__ Z,
+                         double* __restrict__ P) {
+  const long long tot = (long long)n * k;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x)
+    P[e] = Z[e] + beta[e % k] * P[e];
+}
+
+template <typename TS, typename TD>
+__global__ void k_bl_convert(long long n, const TS* __restrict__ s, TD* __restrict__ d) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    d[i] = (TD)s[i];
+}
+
+int grid_for(long long work, int max_grid) {
+  return (int)std::max<long long>(1, std::min<long long>((work + kBlock - 1) / kBlock, max_grid));
+}
+
+int warp_grid(int rows, int max_grid) {
+  return std::max(1, std::min((rows + kWarps - 1) / kWarps, max_grid));
+}
+
+}  // namespace
+
+template <>
+DevHier::BlockVecs<float>& DevHier::bvecs<float>(int l) {
+  return blk32_[l];
+}
+template <>
+DevHier::BlockVecs<double>& DevHier::bvecs<double>(int l) {
+  return blk64_[l];
+}
+
+void DevHier::ensure_block(int k) {
+  if (k <= blk_k_) return;
+  const int nl = nlevels();
+  blk32_.assign(nl, BlockVecs<float>{});
+  blk64_.assign(nl, BlockVecs<double>{});
+  for (int l = 0; l < nl; ++l) {
+    const size_t m = (size_t)L_[l].A.n * k;
+    blk32_[l] = BlockVecs<float>{alloc<float>(m), alloc<float>(m), alloc<float>(m), alloc<float>(m)};
+    blk64_[l] = BlockVecs<double>{alloc<double>(m), alloc<double>(m), alloc<double>(m), alloc<double>(m)};
+  }
+  const size_t mc = (size_t)std::max(nc_, 1) * k;
+  bcb32_ = alloc<float>(mc);
+  bcx32_ = alloc<float>(mc);
+  bcb64_ = alloc<double>(mc);
+  bcx64_ = alloc<double>(mc);
+  const size_t m0 = (size_t)n0_ * k;
+  for (auto& p : bpcg_) p = alloc<double>(m0);
+  for (auto& p : bpcg32_) p = alloc<float>(m0);
+  bpart_ = alloc<double>((size_t)max_grid_ * 32);
+  bdev_ = alloc<double>(8 * 32);
+  if (!bhost_) DR_CK(cudaMallocHost(&bhost_, 8 * 32 * sizeof(double)));
+  blk_k_ = k;
+}
+
+void DevHier::col_dots(int n, int k, const double* a, const double* b, double* dst_dev) {
+  const int grid = warp_grid(n, max_grid_);
+  note_launch();
+  k_bl_dot_part<<<grid, kBlock, 0, st_>>>(n, k, a, b, bpart_);
+  note_launch();
+  k_bl_dot_final<<<1, 1024, 0, st_>>>(grid, k, bpart_, dst_dev);
+  DR_CK(cudaGetLastError());
+}
+
+// One cycle of level l on k columns; returns where the result ended (X or
+// the level's partner buffer).
+template <typename T>
+T* DevHier::cycle_block(int l, T* X, const T* B, bool x_zero, const CycleOpts& o, int k) {
+  DevLevel& L = L_[l];
+  BlockVecs<T>& V = bvecs<T>(l);
+  const DevMat& A = L.A;
+  const int n = A.n;
+  const T om = (T)L.omega;
+  const T* dinv = invd<T>(L);
+  const T* av = mval<T>(A);
+  const int grid = warp_grid(n, max_grid_);
+  T* x = X;
+  T* t = (X == V.x) ? V.t : V.x;
+  int pre = o.pre;
+  if (x_zero) {
+    note_launch();
+    if (pre >= 1) {
+      k_bl_jz<T><<<grid_for((long long)n * k, max_grid_), kBlock, 0, st_>>>(n, k, B, dinv, om, x);
+      --pre;
+    } else {
+      k_bl_fill<T><<<grid_for((long long)n * k, max_grid_), kBlock, 0, st_>>>((long long)n * k, x);
+    }
+  }
+  for (int s = 0; s < pre; ++s) {
+    note_launch();
+    k_spmm<T, T, BM_JACOBI><<<grid, kBlock, 0, st_>>>(n, k, A.rp, A.ci, av, x, B, dinv, om, t);
+    std::swap(x, t);
+  }
+  note_launch();
+  k_spmm<T, T, BM_RESID><<<grid, kBlock, 0, st_>>>(n, k, A.rp, A.ci, av, x, B, nullptr, T(0), V.r);
+  const bool last = (l + 1 == nlevels());
+  T* bc = last ? (sizeof(T) == 8 ? (T*)bcb64_ : (T*)bcb32_) : bvecs<T>(l + 1).b;
+  const DevMat& R = L.R;
+  note_launch();
+  k_spmm<T, T, BM_STORE><<<warp_grid(R.n, max_grid_), kBlock, 0, st_>>>(R.n, k, R.rp, R.ci, mval<T>(R), V.r,
+                                                                        nullptr, nullptr, T(0), bc);
+  T* xc;
+  if (!last) {
+    xc = cycle_block<T>(l + 1, bvecs<T>(l + 1).x, bc, true, o, k);
+    if (o.w) xc = cycle_block<T>(l + 1, xc, bc, false, o, k);
+  } else {
+    xc = sizeof(T) == 8 ? (T*)bcx64_ : (T*)bcx32_;
+    note_launch();
+    const size_t smem = (size_t)nc_ * k * sizeof(double);
+    if (smem > 48 * 1024) {
+      int optin = 0;
+      DR_CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_));
+      if (smem > (size_t)optin) fail("block solves: the coarsest system is too large for one block");
+      DR_CK(cudaFuncSetAttribute(k_bl_lu<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    k_bl_lu<T><<<1, 32, smem, st_>>>(nc_, k, clu_, cpiv_, bc, xc);
+  }
+  const DevMat& P = L.P;
+  note_launch();
+  k_spmm<T, T, BM_ADDTO><<<warp_grid(P.n, max_grid_), kBlock, 0, st_>>>(P.n, k, P.rp, P.ci, mval<T>(P), xc,
+                                                                        nullptr, nullptr, T(0), x);
+  for (int s = 0; s < o.post; ++s) {
+    note_launch();
+    k_spmm<T, T, BM_JACOBI><<<grid, kBlock, 0, st_>>>(n, k, A.rp, A.ci, av, x, B, dinv, om, t);
+    std::swap(x, t);
+  }
+  DR_CK(cudaGetLastError());
+  return x;
+}
+
+template float* DevHier::cycle_block<float>(int, float*, const float*, bool, const CycleOpts&, int);
+template double* DevHier::cycle_block<double>(int, double*, const double*, bool, const CycleOpts&, int);
+
+int DevHier::pcg_block(double* X, const double* B, int k, const CycleOpts& o, double tol, int maxiter,
+                       bool mixed, int* iters, double* relres, int verbose) {
+  if (k < 1 || k > 32) fail("pcg_block: k must be 1..32");
+  if (L_.empty()) fail("pcg_block: the hierarchy has no levels");
+  for (auto& d : L_)
+    if (d.smoother != SmootherKind::Jacobi && d.smoother != SmootherKind::L1Jacobi)
+      fail("block solves need Jacobi or l1-Jacobi smoothing on every level");
+  if (mixed) ensure_fp32();
+  ensure_block(k);
+  const int n = n0_;
+  const long long m = (long long)n * k;
+  double *R = bpcg_[0], *P = bpcg_[1], *Q = bpcg_[2], *Z = bpcg_[3];
+  float* R32 = bpcg32_[0];
+  const DevMat& A = L_[0].A;
+  const int grid = warp_grid(n, max_grid_);
+  const int vgrid = grid_for(m, max_grid_);
+  // device k-vectors: 0 bb, 1 rr, 2 rz, 3 pq, 4 alpha, 5 beta
+  double* dv = bdev_;
+  double* hv = bhost_;
+  auto fetch = [&](int slot) {
+    DR_CK(cudaMemcpyAsync(hv + slot * 32, dv + slot * 32, k * sizeof(double), cudaMemcpyDeviceToHost, st_));
+  };
+  auto precond = [&]() {  // Z = M R
+    if (mixed) {
+      note_launch();
+      k_bl_convert<double, float><<<vgrid, kBlock, 0, st_>>>(m, R, R32);
+      float* z = cycle_block<float>(0, bvecs<float>(0).x, R32, true, o, k);
+      note_launch();
+      k_bl_convert<float, double><<<vgrid, kBlock, 0, st_>>>(m, z, Z);
+    } else {
+      double* z = cycle_block<double>(0, bvecs<double>(0).x, R, true, o, k);
+      DR_CK(cudaMemcpyAsync(Z, z, (size_t)m * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+    }
+  };
+  note_launch();
+  k_spmm<double, double, BM_RESID><<<grid, kBlock, 0, st_>>>(n, k, A.rp, A.ci, A.v, X, B, nullptr, 0.0, R);
+  col_dots(n, k, B, B, dv + 0 * 32);
+  col_dots(n, k, R, R, dv + 1 * 32);
+  fetch(0);
+  fetch(1);
+  DR_CK(cudaStreamSynchronize(st_));
+  std::vector<double> bb(hv, hv + k), rr(hv + 32, hv + 32 + k);
+  std::vector<char> active(k);
+  std::vector<int> its(k, 0);
+  int nact = 0;
+  for (int c = 0; c < k; ++c) {
+    active[c] = bb[c] > 0.0 && std::sqrt(rr[c] / bb[c]) >= tol;
+    nact += active[c];
+  }
+  precond();
+  col_dots(n, k, R, Z, dv + 2 * 32);
+  fetch(2);
+  DR_CK(cudaMemcpyAsync(P, Z, (size_t)m * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+  DR_CK(cudaStreamSynchronize(st_));
+  std::vector<double> rz(hv + 64, hv + 64 + k);
+  int it = 0;
+  while (nact > 0 && it < maxiter) {
+    ++it;
+    note_launch();
+    k_spmm<double, double, BM_STORE><<<grid, kBlock, 0, st_>>>(n, k, A.rp, A.ci, A.v, P, nullptr, nullptr, 0.0,
+                                                               Q);
+    col_dots(n, k, P, Q, dv + 3 * 32);
+    fetch(3);
+    DR_CK(cudaStreamSynchronize(st_));
+    for (int c = 0; c < k; ++c) hv[4 * 32 + c] = (active[c] && hv[96 + c] != 0.0) ? rz[c] / hv[96 + c] : 0.0;
+    DR_CK(cudaMemcpyAsync(dv + 4 * 32, hv + 4 * 32, k * sizeof(double), cudaMemcpyHostToDevice, st_));
+    note_launch();
+    k_bl_update<<<vgrid, kBlock, 0, st_>>>(n, k, dv + 4 * 32, X, R, P, Q, nullptr);
+    col_dots(n, k, R, R, dv + 1 * 32);
+    fetch(1);
+    DR_CK(cudaStreamSynchronize(st_));
+    for (int c = 0; c < k; ++c)
+      if (active[c]) {
+        its[c] = it;
+        if (std::sqrt(hv[32 + c] / bb[c]) < tol) {
+          active[c] = 0;
+          --nact;
+        }
+      }
+    if (verbose >= 2) std::printf("  block PCG iter %4d: %d of %d columns active\n", it, nact, k);
+    if (nact == 0) break;
+    precond();
+    col_dots(n, k, R, Z, dv + 2 * 32);
+    fetch(2);
+    DR_CK(cudaStreamSynchronize(st_));
+    for (int c = 0; c < k; ++c) {
+      const double rzn = hv[64 + c];
+      hv[5 * 32 + c] = (active[c] && rz[c] != 0.0) ? rzn / rz[c] : 0.0;
+      rz[c] = rzn;
+    }
+    DR_CK(cudaMemcpyAsync(dv + 5 * 32, hv + 5 * 32, k * sizeof(double), cudaMemcpyHostToDevice, st_));
+    note_launch();
+    k_bl_dir<<<vgrid, kBlock, 0, st_>>>(n, k, dv + 5 * 32, Z, P);
+  }
+  // true residuals of the result
+  note_launch();
+  k_spmm<double, double, BM_RESID><<<grid, kBlock, 0, st_>>>(n, k, A.rp, A.ci, A.v, X, B, nullptr, 0.0, R);
+  col_dots(n, k, R, R, dv + 1 * 32);
+  fetch(1);
+  DR_CK(cudaStreamSynchronize(st_));
+  DR_CK(cudaGetLastError());
+  int worst = 0;
+  for (int c = 0; c < k; ++c) {
+    if (iters) iters[c] = its[c];
+    if (relres) relres[c] = bb[c] > 0.0 ? std::sqrt(hv[32 + c] / bb[c]) : 0.0;
+    worst = std::max(worst, its[c]);
+  }
+  return worst;
+}
+
+}  // namespace dr

@@ -530,6 +530,20 @@ int32_t draugr_b200_bicgstab_device(int32_t handle, int32_t n, double* x_dev, co
   });
 }
 
+int32_t draugr_b200_pcg_block_device(int32_t handle, int32_t n, int32_t k, double* X_dev, const double* B_dev,
+                                     int32_t config_handle, double tol, int32_t maxiter, int32_t precision,
+                                     int32_t* iters, double* relres) {
+  return guarded("draugr_b200_pcg_block_device", [&]() -> int32_t {
+    Config c;
+    auto H = get_hier(handle, config_handle, &c);
+    if (n != n_finest(*H)) fail("DimensionMismatch");
+    if (precision != 0 && precision != 1) fail("precision must be 0 (FP64 cycle) or 1 (FP32 cycle)");
+    if (!X_dev || !B_dev) fail("ArgumentError: NULL block");
+    return device_of(*H).pcg_block(X_dev, B_dev, k, opts_of(c), tol, maxiter, precision == 1, iters, relres,
+                                   c.verbose);
+  });
+}
+
 int32_t draugr_b200_nz_gradient_device(int32_t handle, int32_t n, const double* x_dev,
                                        const double* lambda_dev, double* grad_dev) {
   return guarded("draugr_b200_nz_gradient_device", [&]() -> int32_t {

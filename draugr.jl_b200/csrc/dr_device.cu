@@ -35,6 +35,7 @@ using namespace kern;
 static std::atomic<long long> g_launches{0};
 long long kernel_launches() { return g_launches.load(); }
 static inline void counted() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void note_launch() { counted(); }
 
 // SM count of the device in use and a device flag the row kernels set when a
 // bounded wait gives up (checked after every solve / resetup).
@@ -256,6 +257,9 @@ T* DevHier::alloc(size_t n) {
   bytes_ += bytes;
   return (T*)p;
 }
+template double* DevHier::alloc<double>(size_t);
+template float* DevHier::alloc<float>(size_t);
+template int* DevHier::alloc<int>(size_t);
 
 template <typename T>
 static void h2d(T* d, const std::vector<T>& h, cudaStream_t st) {

@@ -13,6 +13,7 @@ namespace dr {
 
 void cuda_check(cudaError_t e, const char* what, const char* file, int line);
 long long kernel_launches();
+void note_launch();  // counts one kernel launch (kernel_launches)
 #define DR_CK(x) ::dr::cuda_check((x), #x, __FILE__, __LINE__)
 
 // Nonzeros per tile of the row kernel (k_tile_rows); rows longer than this
@@ -161,6 +162,14 @@ class DevHier {
                double* relres, int verbose);
   // dL/da_ij = -lambda_i x_j for the finest matrix's nonzeros (CSR order).
   void nz_gradient(const double* x, const double* lam, double* grad);
+  // Block PCG: k <= 32 right-hand sides at once, X and B row-major n x k
+  // on the device (column c of row i at i*k + c).  One pass over each level
+  // matrix per block product serves all k columns; per-column scalars, a
+  // column stops changing once it has converged.  iters[k] and relres[k]
+  // (host, may be null) receive each column's iterations and final relative
+  // residual.  Returns the largest iteration count.
+  int pcg_block(double* X, const double* B, int k, const CycleOpts& o, double tol, int maxiter, bool mixed,
+                int* iters, double* relres, int verbose);
 
   // r = b - A x on the finest level and ||r||_2 (device vectors).
   double residual_norm(const double* x, const double* b, double* r);
@@ -209,6 +218,27 @@ class DevHier {
   void ensure_fp32();
   void refresh_fp32();
   void build_tail();
+  // block (multi-right-hand-side) solves: per-level n x k buffers
+  template <typename T>
+  struct BlockVecs {
+    T *x = nullptr, *t = nullptr, *b = nullptr, *r = nullptr;
+  };
+  std::vector<BlockVecs<float>> blk32_;
+  std::vector<BlockVecs<double>> blk64_;
+  int blk_k_ = 0;  // columns the block buffers hold
+  float *bcb32_ = nullptr, *bcx32_ = nullptr;
+  double *bcb64_ = nullptr, *bcx64_ = nullptr;
+  double* bpcg_[4] = {nullptr, nullptr, nullptr, nullptr};  // R, P, Q, Z
+  float* bpcg32_[2] = {nullptr, nullptr};                   // R, Z in FP32
+  double* bpart_ = nullptr;  // column-dot partial sums
+  double* bdev_ = nullptr;   // k-vectors on the device (dot results, alpha, beta)
+  double* bhost_ = nullptr;  // their pinned host mirror
+  void ensure_block(int k);
+  template <typename T>
+  BlockVecs<T>& bvecs(int l);
+  template <typename T>
+  T* cycle_block(int l, T* X, const T* B, bool x_zero, const CycleOpts& o, int k);
+  void col_dots(int n, int k, const double* a, const double* b, double* dst_dev);
   // transposed hierarchy (adjoint solves)
   bool at_built_ = false;
   bool tr_ = false;          // cycle pieces use A^T (and the transposed coarsest solve)
@@ -283,5 +313,11 @@ class DevHier {
 
   friend struct DevHierAccess;
 };
+
+// Value and smoother-diagonal arrays by precision (defined in dr_device.cu).
+template <> const double* DevHier::mval<double>(const DevMat& M) const;
+template <> const float* DevHier::mval<float>(const DevMat& M) const;
+template <> const double* DevHier::invd<double>(const DevLevel& L) const;
+template <> const float* DevHier::invd<float>(const DevLevel& L) const;
 
 }  // namespace dr

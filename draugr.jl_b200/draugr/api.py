@@ -501,6 +501,27 @@ def amg_solve_diff(values, b, h: Hierarchy, config: AMGConfig | None = None, tol
     return _Solve.fn.apply(values, b, h, config, tol, maxiter, symmetric)
 
 
+def pcg_multi(X, B, h: Hierarchy, config: AMGConfig | None = None, tol: float = 1e-8,
+              maxiter: int = 500, precision: str = "mixed"):
+    """PCG for up to 32 right-hand sides of one matrix at once.  X, B: CUDA
+    float64 tensors of shape (n, k), row-major (X holds the initial guesses
+    and receives the solutions).  Each product with a level matrix serves
+    all k columns in one pass over the matrix.  Returns (X, iterations per
+    column, relative residual per column)."""
+    config = config if config is not None else (h.config or AMGConfig())
+    if X.dim() != 2 or X.shape != B.shape or not X.is_contiguous() or not B.is_contiguous():
+        raise ValueError("X and B must be contiguous (n, k) tensors of the same shape")
+    n, k = int(X.shape[0]), int(X.shape[1])
+    prec = {"fp64": 0, "mixed": 1, "fp32": 1}[precision]
+    its = (C.c_int32 * k)()
+    rel = (C.c_double * k)()
+    lib = _lib.load()
+    _lib.check(lib.draugr_b200_pcg_block_device(h.handle, n, k, X.data_ptr(), B.data_ptr(),
+                                                config_handle(config), tol, maxiter, prec, its, rel),
+               "pcg_multi")
+    return X, list(its), list(rel)
+
+
 def pcg_batch(hierarchies, xs, bs, config: AMGConfig | None = None, tol: float = 1e-8,
               maxiter: int = 500, precision: str = "mixed", workers: int = 16):
     """PCG on many independent systems at once: each hierarchy runs on its

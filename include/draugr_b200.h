@@ -120,6 +120,20 @@ int32_t draugr_b200_bicgstab_device(int32_t handle, int32_t n, double *x_dev, co
                                     int32_t config_handle, double tol, int32_t maxiter,
                                     int32_t transpose, double *relres);
 
+/* Conjugate gradients for k (1..32) right-hand sides of the same matrix
+ * at once: X and B are device arrays of n x k doubles, row-major (column c
+ * of row i at i*k + c); X holds the initial guesses.  Each product with a
+ * level matrix serves all k columns in one pass over the matrix.
+ * precision as for draugr_b200_pcg; every level must use (l1-)Jacobi
+ * smoothing.  iters and relres (host arrays of k entries, may be NULL)
+ * receive each column's iterations and final true relative residual.
+ * Returns the largest iteration count or -1.  No counterpart in the
+ * reference. */
+int32_t draugr_b200_pcg_block_device(int32_t handle, int32_t n, int32_t k, double *X_dev,
+                                     const double *B_dev, int32_t config_handle, double tol,
+                                     int32_t maxiter, int32_t precision, int32_t *iters,
+                                     double *relres);
+
 /* Gradient of a loss L(x), x = A^-1 b, with respect to the nonzeros of the
  * finest matrix: grad[k] = -lambda_i x_j for nonzero k = (i, j) in CSR
  * order, where lambda = A^-T dL/dx (device vectors; grad has nnz entries).

@@ -40,3 +40,29 @@ def test_concurrent_solves_equal_sequential_ones():
             assert np.array_equal(xn, seq[k][0]), k
             bn = b.cpu().numpy()
             assert np.linalg.norm(bn - A @ xn) / np.linalg.norm(bn) < 1e-8
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("side,k", [(20, 5), (24, 32), (16, 1)])
+def test_block_pcg_matches_single_solves(side, k, precision):
+    """Many right-hand sides of one matrix (the C3 96^3 x 32 case, reduced):
+    block PCG, one pass over each level matrix for all k columns, against
+    k single-right-hand-side PCG solves."""
+    A = problems.poisson3d(side)
+    n = A.shape[0]
+    cfg = draugr.hypre_default_config(agg_trunc_factor=0.2, smoother=draugr.L1JacobiSmootherType(), seed=6)
+    h = draugr.amg_setup(A, cfg)
+    rng = np.random.default_rng(side + k)
+    Bn = rng.uniform(-1, 1, (n, k))
+    B = torch.tensor(Bn, device="cuda")
+    X = torch.zeros_like(B)
+    torch.cuda.synchronize()
+    X, its, rels = draugr.pcg_multi(X, B, h, cfg, tol=1e-8, maxiter=500, precision=precision)
+    Xn = X.cpu().numpy()
+    for c in range(k):
+        x1, it1, _ = draugr.pcg(np.zeros(n), Bn[:, c].copy(), h, cfg, tol=1e-8, maxiter=500,
+                                precision=precision)
+        assert abs(its[c] - it1) <= 1, (c, its[c], it1)
+        r = np.linalg.norm(Bn[:, c] - A @ Xn[:, c]) / np.linalg.norm(Bn[:, c])
+        assert r < 1e-8 and abs(r - rels[c]) < 1e-12
+        assert np.linalg.norm(Xn[:, c] - x1) / np.linalg.norm(x1) < 1e-6
