@@ -61,6 +61,10 @@ def parse():
                     help="the 27-point coefficient-update workload: time GPU partial resetups "
                          "(numeric Galerkin products) at --n^3 nodes, then PCG on the result")
     ap.add_argument("--updates", type=int, default=20)
+    ap.add_argument("--profile-block", action="store_true",
+                    help="run exactly one block PCG solve (3D Poisson 96^3, 32 right-hand sides, mixed)")
+    ap.add_argument("--profile-resetup", action="store_true",
+                    help="run exactly one partial resetup (27-point anisotropic diffusion on --n^3 nodes)")
     ap.add_argument("--batch", action="store_true",
                     help="the batching workload: 64 independent 3D Poisson systems (sides 16..64) "
                          "solved concurrently, and one 96^3 operator with 32 right-hand sides")
@@ -642,6 +646,46 @@ def run_batch(args):
                                     "worst_relres_fp64_verified": blk_rr}}}
 
 
+def run_profile_block(args):
+    import torch
+
+    import draugr
+    from draugr import problems
+
+    torch.cuda.set_device(0)
+    A = problems.poisson3d(96)
+    cfg = draugr.hypre_default_config(agg_trunc_factor=0.2, smoother=draugr.L1JacobiSmootherType(),
+                                      seed=args.seed)
+    h = draugr.amg_setup(A, cfg)
+    B = torch.tensor(np.random.default_rng(args.seed).uniform(-1, 1, (A.shape[0], 32)), device="cuda")
+    X = torch.zeros_like(B)
+    torch.cuda.synchronize()
+    _, its, rel = draugr.pcg_multi(X, B, h, cfg, tol=TOL, maxiter=MAXITER, precision="mixed")
+    return {"profile_block": True, "iterations": [int(min(its)), int(max(its))], "relres_max": max(rel)}
+
+
+def run_profile_resetup(args):
+    import torch
+
+    import draugr
+    from draugr import problems
+
+    torch.cuda.set_device(0)
+    m = args.n
+    rng = np.random.default_rng(args.seed)
+    kappa = np.ones((m + 1,) * 3)
+    A = problems.anisotropic_27pt(m, 1e-3, kappa)
+    cfg = draugr.hypre_default_config(agg_trunc_factor=0.2, smoother=draugr.L1JacobiSmootherType(),
+                                      seed=args.seed)
+    h = draugr.amg_setup(A, cfg)
+    kappa = kappa * np.exp(0.5 * rng.standard_normal(kappa.shape))
+    v = torch.tensor(problems.anisotropic_27pt(m, 1e-3, kappa).data, device="cuda")
+    torch.cuda.synchronize()
+    draugr.amg_resetup(h, v, cfg)
+    torch.cuda.synchronize()
+    return {"profile_resetup": True, "n": int(A.shape[0]), "nnz": int(A.nnz), "levels": h.nlevels + 1}
+
+
 def run_profile_solve(args):
     import torch
 
@@ -663,6 +707,12 @@ def main():
         return
     if args.batch:
         print(json.dumps(run_batch(args)), flush=True)
+        return
+    if args.profile_block:
+        print(json.dumps(run_profile_block(args)), flush=True)
+        return
+    if args.profile_resetup:
+        print(json.dumps(run_profile_resetup(args)), flush=True)
         return
     if args.profile_solve:
         print(json.dumps(run_profile_solve(args)), flush=True)

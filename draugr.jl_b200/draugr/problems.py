@@ -185,11 +185,18 @@ def _faces(shape):
     return inner, bnd
 
 
-def _fv_system(kappa, flux=None):
+# Position in CSR order of every value contribution of _fv_system, per cell
+# grid shape (the contributions' rows and columns depend only on the shape).
+_FV_POSITIONS = {}
+
+
+def _fv_system(kappa, flux=None, values_only=False):
     """Finite-volume operator of -div(kappa grad u) + div(w u) (upwind) with
     Dirichlet boundary on a unit-spaced cell grid; flux[axis] gives, per
     interior face (a, b) of that axis, the flux from a to b (None: no
-    convection).  Returns (A, J)."""
+    convection).  Returns (A, J), or with values_only the values of A in
+    CSR order alone (the pattern depends only on the grid shape; the
+    positions of the contributions are computed once per shape)."""
     shape = kappa.shape
     n = kappa.size
     k = kappa.ravel()
@@ -217,23 +224,32 @@ def _fv_system(kappa, flux=None):
         val(c, c, 2 * k[c])
         der(c, c, c, np.full(len(c), 2.0))
     cat = np.concatenate
+    if values_only:
+        pos = _FV_POSITIONS.get(shape)
+        if pos is None:
+            keys = cat(vr).astype(np.int64) * n + cat(vcol)
+            uniq, inv = np.unique(keys, return_inverse=True)
+            _FV_POSITIONS[shape] = pos = (inv, len(uniq))
+        return np.bincount(pos[0], weights=cat(vv), minlength=pos[1])
     return _csr_with_jacobian(n, (cat(vr), cat(vcol)), cat(vv), (cat(dr), cat(dcol)), cat(dcell), cat(dv), n)
 
 
-def fv_diffusion_3d(kappa: np.ndarray):
+def fv_diffusion_3d(kappa: np.ndarray, values_only: bool = False):
     """Cell-centred finite volumes for -div(kappa grad u) on the m^3 grid of
     kappa ([z, y, x]), harmonic face transmissibilities, Dirichlet boundary
     (boundary faces 2 kappa).  Symmetric.  Returns (A, J), J = d(values of
-    A)/d(kappa) (nnz x m^3)."""
-    return _fv_system(kappa)
+    A)/d(kappa) (nnz x m^3); with values_only, A's values in CSR order."""
+    return _fv_system(kappa, values_only=values_only)
 
 
-def convection_diffusion_2d(kappa: np.ndarray, peclet: float = 50.0, seed: int = 0):
+def convection_diffusion_2d(kappa: np.ndarray, peclet: float = 50.0, seed: int = 0,
+                            values_only: bool = False):
     """Upwind finite volumes for -div(kappa grad u) + div(w u) on the m^2
     grid of kappa ([y, x]), Dirichlet boundary.  w is divergence-free, from a
     seeded smooth stream function that vanishes on the boundary (no flow
     through it), scaled so that the largest face flux is `peclet` (the cell
-    Peclet number at kappa = 1).  Nonsymmetric M-matrix.  Returns (A, J)."""
+    Peclet number at kappa = 1).  Nonsymmetric M-matrix.  Returns (A, J);
+    with values_only, A's values in CSR order."""
     m = kappa.shape[0]
     rng = np.random.default_rng(seed)
     yy, xx = np.meshgrid(np.linspace(0, 1, m + 1), np.linspace(0, 1, m + 1), indexing="ij")
@@ -248,7 +264,7 @@ def convection_diffusion_2d(kappa: np.ndarray, peclet: float = 50.0, seed: int =
     scale = peclet / max(np.abs(fx).max(), np.abs(fy).max(), 1e-300)
     # face order of _faces: axis 0 (y) faces, then axis 1 (x) faces, each raveled [y, x]
     flux = {0: (fy * scale).ravel(), 1: (fx * scale).ravel()}
-    return _fv_system(kappa, flux)
+    return _fv_system(kappa, flux, values_only)
 
 
 def rhs(n: int, seed: int = 0) -> np.ndarray:
