@@ -77,6 +77,88 @@ k_spmm(int nrows, int k, const int* __restrict__ rp, const int* __restrict__ ci,
   }
 }
 
+// The same products with vector gathers, when each row's k columns split
+// into 16-byte pieces (k a multiple of 4 FP32 / 2 FP64 values, 16-byte
+// aligned vectors): TPR threads per row, each owning V consecutive
+// columns, 32 / TPR rows per warp.  A thread reads the row's (column,
+// value) pairs itself (the TPR threads of a row read the same address) and
+// gathers one 16-byte piece of X per entry, so an entry costs a few
+// instructions per piece instead of shuffles and a scalar gather per
+// column.  Each column is summed in column order with separately rounded
+// products and sums: the results equal k_spmm's bit for bit.
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+  using type = float4;
+  static constexpr int V = 4;
+  __device__ static void get(const type& a, float* o) { o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w; }
+  __device__ static type make(const float* o) { return make_float4(o[0], o[1], o[2], o[3]); }
+};
+template <>
+struct Vec16<double> {
+  using type = double2;
+  static constexpr int V = 2;
+  __device__ static void get(const type& a, double* o) { o[0] = a.x; o[1] = a.y; }
+  __device__ static type make(const double* o) { return make_double2(o[0], o[1]); }
+};
+
+template <typename TA, typename T, int MODE, int TPR>
+__global__ void __launch_bounds__(kBlock)
+k_spmm_vec(int nrows, int k, const int* __restrict__ rp, const int* __restrict__ ci,
+           const TA* __restrict__ av, const T* __restrict__ X, const T* __restrict__ B,
+           const T* __restrict__ dinv, T omega, T* Y) {
+  using VV = Vec16<T>;
+  using VT = typename VV::type;
+  constexpr int V = VV::V;
+  constexpr int RPW = 32 / TPR;
+  const int lane = threadIdx.x & 31;
+  const int c0 = (lane % TPR) * V;  // first column of this thread
+  if (c0 >= k) return;              // no warp-wide operations below
+  const long long w = (long long)blockIdx.x * kWarps + (threadIdx.x >> 5);
+  const long long nw = (long long)gridDim.x * kWarps;
+  for (long long r = w * RPW + lane / TPR; r < nrows; r += nw * RPW) {
+    const int row = (int)r;
+    const int rs = rp[row], re = rp[row + 1];
+    const size_t o = (size_t)row * k + c0;
+    T acc[V];
+    if (MODE == BM_ADDTO) VV::get(*reinterpret_cast<const VT*>(Y + o), acc);
+    else if (MODE == BM_JACOBI) VV::get(*reinterpret_cast<const VT*>(B + o), acc);
+    else
+#pragma unroll
+      for (int q = 0; q < V; ++q) acc[q] = T(0);
+#pragma unroll 4
+    for (int e = rs; e < re; ++e) {
+      const int c = ci[e];
+      const T v = (T)av[e];
+      T xv[V];
+      VV::get(*reinterpret_cast<const VT*>(X + (size_t)c * k + c0), xv);
+#pragma unroll
+      for (int q = 0; q < V; ++q) {
+        const T p = rn_mul(v, xv[q]);
+        acc[q] = (MODE == BM_JACOBI) ? rn_sub(acc[q], p) : rn_add(acc[q], p);
+      }
+    }
+    T out[V];
+    if (MODE == BM_RESID) {
+      T bv[V];
+      VV::get(*reinterpret_cast<const VT*>(B + o), bv);
+#pragma unroll
+      for (int q = 0; q < V; ++q) out[q] = rn_sub(bv[q], acc[q]);
+    } else if (MODE == BM_JACOBI) {
+      T xo[V];
+      VV::get(*reinterpret_cast<const VT*>(X + o), xo);
+      const T sc = rn_mul(omega, dinv[row]);
+#pragma unroll
+      for (int q = 0; q < V; ++q) out[q] = rn_add(xo[q], rn_mul(sc, acc[q]));
+    } else {
+#pragma unroll
+      for (int q = 0; q < V; ++q) out[q] = acc[q];
+    }
+    *reinterpret_cast<VT*>(Y + o) = VV::make(out);
+  }
+}
+
 template <typename T>
 __global__ void k_bl_fill(long long n, T* __restrict__ x) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -97,11 +179,21 @@ __global__ void k_bl_jz(int n, int k, const T* __restrict__ B, const T* __restri
 // Coarsest solve for k columns with the dgetf2 factors (dgetrs order),
 // one thread per column, its vector in shared memory (n * k doubles of
 // dynamic shared memory; every thread reads the same factor entry at a
-// time, a broadcast).
+// time, a broadcast).  With `stage` the factors are first copied into
+// shared memory after the vectors (n * n more doubles), so the
+// substitutions' chains of dependent steps read shared memory instead of
+// global memory.
 template <typename T>
-__global__ void k_bl_lu(int n, int k, const double* __restrict__ lu, const int* __restrict__ piv,
-                        const T* __restrict__ B, T* __restrict__ X) {
+__global__ void k_bl_lu(int n, int k, const double* __restrict__ lu_g, const int* __restrict__ piv,
+                        const T* __restrict__ B, T* __restrict__ X, int stage) {
   extern __shared__ double ysm[];
+  const double* lu = lu_g;
+  if (stage) {
+    double* ls = ysm + (size_t)n * k;
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) ls[e] = lu_g[e];
+    __syncthreads();
+    lu = ls;
+  }
   const int c = threadIdx.x;
   if (c >= k) return;
   double* y = ysm + (size_t)c;  // element i at y[i * k]
@@ -209,6 +301,30 @@ int warp_grid(int rows, int max_grid) {
   return std::max(1, std::min((rows + kWarps - 1) / kWarps, max_grid));
 }
 
+bool aligned16(const void* p) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// Block product on `nrows` rows: the vector-gather kernel when the rows'
+// k columns split into 16-byte pieces, else one warp per row.
+template <typename TA, typename T, int MODE>
+void spmm(cudaStream_t st, int max_grid, int nrows, int k, const int* rp, const int* ci, const TA* av,
+          const T* X, const T* B, const T* dinv, T omega, T* Y) {
+  constexpr int V = Vec16<T>::V;
+  if (k % V == 0 && aligned16(X) && aligned16(B) && aligned16(Y)) {
+    const int tpr = k / V <= 1 ? 1 : k / V <= 2 ? 2 : k / V <= 4 ? 4 : k / V <= 8 ? 8 : 16;
+    const int rows_per_block = kWarps * (32 / tpr);
+    const int grid = std::max(1, std::min((nrows + rows_per_block - 1) / rows_per_block, max_grid));
+    switch (tpr) {
+      case 1: k_spmm_vec<TA, T, MODE, 1><<<grid, kBlock, 0, st>>>(nrows, k, rp, ci, av, X, B, dinv, omega, Y); break;
+      case 2: k_spmm_vec<TA, T, MODE, 2><<<grid, kBlock, 0, st>>>(nrows, k, rp, ci, av, X, B, dinv, omega, Y); break;
+      case 4: k_spmm_vec<TA, T, MODE, 4><<<grid, kBlock, 0, st>>>(nrows, k, rp, ci, av, X, B, dinv, omega, Y); break;
+      case 8: k_spmm_vec<TA, T, MODE, 8><<<grid, kBlock, 0, st>>>(nrows, k, rp, ci, av, X, B, dinv, omega, Y); break;
+      default: k_spmm_vec<TA, T, MODE, 16><<<grid, kBlock, 0, st>>>(nrows, k, rp, ci, av, X, B, dinv, omega, Y); break;
+    }
+    return;
+  }
+  k_spmm<TA, T, MODE><<<warp_grid(nrows, max_grid), kBlock, 0, st>>>(nrows, k, rp, ci, av, X, B, dinv, omega, Y);
+}
+
 }  // namespace
 
 template <>
@@ -264,7 +380,6 @@ T* DevHier::cycle_block(int l, T* X, const T* B, bool x_zero, const CycleOpts& o
   const T om = (T)L.omega;
   const T* dinv = invd<T>(L);
   const T* av = mval<T>(A);
-  const int grid = warp_grid(n, max_grid_);
   T* x = X;
   T* t = (X == V.x) ? V.t : V.x;
   int pre = o.pre;
@@ -279,16 +394,16 @@ T* DevHier::cycle_block(int l, T* X, const T* B, bool x_zero, const CycleOpts& o
   }
   for (int s = 0; s < pre; ++s) {
     note_launch();
-    k_spmm<T, T, BM_JACOBI><<<grid, kBlock, 0, st_>>>(n, k, A.rp, A.ci, av, x, B, dinv, om, t);
+    spmm<T, T, BM_JACOBI>(st_, max_grid_, n, k, A.rp, A.ci, av, x, B, dinv, om, t);
     std::swap(x, t);
   }
   note_launch();
-  k_spmm<T, T, BM_RESID><<<grid, kBlock, 0, st_>>>(n, k, A.rp, A.ci, av, x, B, nullptr, T(0), V.r);
+  spmm<T, T, BM_RESID>(st_, max_grid_, n, k, A.rp, A.ci, av, x, B, nullptr, T(0), V.r);
   const bool last = (l + 1 == nlevels());
   T* bc = last ? (sizeof(T) == 8 ? (T*)bcb64_ : (T*)bcb32_) : bvecs<T>(l + 1).b;
   const DevMat& R = L.R;
   note_launch();
-  k_spmm<T, T, BM_STORE><<<warp_grid(R.n, max_grid_), kBlock, 0, st_>>>(R.n, k, R.rp, R.ci, mval<T>(R), V.r,
+  spmm<T, T, BM_STORE>(st_, max_grid_, R.n, k, R.rp, R.ci, mval<T>(R), V.r,
                                                                         nullptr, nullptr, T(0), bc);
   T* xc;
   if (!last) {
@@ -297,22 +412,25 @@ T* DevHier::cycle_block(int l, T* X, const T* B, bool x_zero, const CycleOpts& o
   } else {
     xc = sizeof(T) == 8 ? (T*)bcx64_ : (T*)bcx32_;
     note_launch();
-    const size_t smem = (size_t)nc_ * k * sizeof(double);
-    if (smem > 48 * 1024) {
-      int optin = 0;
-      DR_CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_));
-      if (smem > (size_t)optin) fail("block solves: the coarsest system is too large for one block");
+    size_t smem = (size_t)nc_ * k * sizeof(double);
+    int optin = 0;
+    DR_CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_));
+    if (smem > (size_t)optin) fail("block solves: the coarsest system is too large for one block");
+    // the factors too, when they fit beside the vectors
+    const size_t with_lu = smem + (size_t)nc_ * nc_ * sizeof(double);
+    const int stage = with_lu <= (size_t)optin ? 1 : 0;
+    if (stage) smem = with_lu;
+    if (smem > 48 * 1024)
       DR_CK(cudaFuncSetAttribute(k_bl_lu<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    }
-    k_bl_lu<T><<<1, 32, smem, st_>>>(nc_, k, clu_, cpiv_, bc, xc);
+    k_bl_lu<T><<<1, 32, smem, st_>>>(nc_, k, clu_, cpiv_, bc, xc, stage);
   }
   const DevMat& P = L.P;
   note_launch();
-  k_spmm<T, T, BM_ADDTO><<<warp_grid(P.n, max_grid_), kBlock, 0, st_>>>(P.n, k, P.rp, P.ci, mval<T>(P), xc,
+  spmm<T, T, BM_ADDTO>(st_, max_grid_, P.n, k, P.rp, P.ci, mval<T>(P), xc,
                                                                         nullptr, nullptr, T(0), x);
   for (int s = 0; s < o.post; ++s) {
     note_launch();
-    k_spmm<T, T, BM_JACOBI><<<grid, kBlock, 0, st_>>>(n, k, A.rp, A.ci, av, x, B, dinv, om, t);
+    spmm<T, T, BM_JACOBI>(st_, max_grid_, n, k, A.rp, A.ci, av, x, B, dinv, om, t);
     std::swap(x, t);
   }
   DR_CK(cudaGetLastError());
@@ -357,7 +475,7 @@ int DevHier::pcg_block(double* X, const double* B, int k, const CycleOpts& o, do
     }
   };
   note_launch();
-  k_spmm<double, double, BM_RESID><<<grid, kBlock, 0, st_>>>(n, k, A.rp, A.ci, A.v, X, B, nullptr, 0.0, R);
+  spmm<double, double, BM_RESID>(st_, max_grid_, n, k, A.rp, A.ci, A.v, X, B, nullptr, 0.0, R);
   col_dots(n, k, B, B, dv + 0 * 32);
   col_dots(n, k, R, R, dv + 1 * 32);
   fetch(0);
@@ -381,7 +499,7 @@ int DevHier::pcg_block(double* X, const double* B, int k, const CycleOpts& o, do
   while (nact > 0 && it < maxiter) {
     ++it;
     note_launch();
-    k_spmm<double, double, BM_STORE><<<grid, kBlock, 0, st_>>>(n, k, A.rp, A.ci, A.v, P, nullptr, nullptr, 0.0,
+    spmm<double, double, BM_STORE>(st_, max_grid_, n, k, A.rp, A.ci, A.v, P, nullptr, nullptr, 0.0,
                                                                Q);
     col_dots(n, k, P, Q, dv + 3 * 32);
     fetch(3);
@@ -418,7 +536,7 @@ int DevHier::pcg_block(double* X, const double* B, int k, const CycleOpts& o, do
   }
   // true residuals of the result
   note_launch();
-  k_spmm<double, double, BM_RESID><<<grid, kBlock, 0, st_>>>(n, k, A.rp, A.ci, A.v, X, B, nullptr, 0.0, R);
+  spmm<double, double, BM_RESID>(st_, max_grid_, n, k, A.rp, A.ci, A.v, X, B, nullptr, 0.0, R);
   col_dots(n, k, R, R, dv + 1 * 32);
   fetch(1);
   DR_CK(cudaStreamSynchronize(st_));
