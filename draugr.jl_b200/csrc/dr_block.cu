@@ -445,8 +445,8 @@ int DevHier::pcg_block(double* X, const double* B, int k, const CycleOpts& o, do
   if (k < 1 || k > 32) fail("pcg_block: k must be 1..32");
   if (L_.empty()) fail("pcg_block: the hierarchy has no levels");
   for (auto& d : L_)
-    if (d.smoother != SmootherKind::Jacobi && d.smoother != SmootherKind::L1Jacobi)
-      fail("block solves need Jacobi or l1-Jacobi smoothing on every level");
+    if (!jacobi_type(d.smoother))
+      fail("block solves need Jacobi, l1-Jacobi or SPAI(0) smoothing on every level");
   if (mixed) ensure_fp32();
   ensure_block(k);
   const int n = n0_;

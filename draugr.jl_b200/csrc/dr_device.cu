@@ -542,7 +542,7 @@ void DevHier::build_tail() {
   std::vector<std::vector<int>> ords;  // from the coarsest level up
   for (int l = nl - 1; l >= 1 && nl - l <= kern::kTailMaxLevels; --l) {
     const DevLevel& d = L_[l];
-    const bool jac = d.smoother == SmootherKind::Jacobi || d.smoother == SmootherKind::L1Jacobi;
+    const bool jac = jacobi_type(d.smoother);
     total += tail_level_bytes<double>(d);
     if (!jac || d.A.n > 4096 || total > kTailSmem) break;
     std::vector<int> rp(d.A.n + 1);
@@ -683,7 +683,7 @@ T* DevHier::smooth(int l, T* x, const T* b, int steps, T* ext, const double* rz_
   LevelVecs<T>& V = vecs<T>(l);
   const DevMat& A = tr_ ? L.At : L.A;
   const T om = (T)L.omega;
-  if (L.smoother == SmootherKind::Jacobi || L.smoother == SmootherKind::L1Jacobi) {
+  if (jacobi_type(L.smoother)) {
     for (int s = 0; s < steps; ++s) {
       T* dst = (l == 0) ? (x == V.xb ? ext : V.xb) : (x == V.xa ? V.xb : V.xa);
       if (rz_w && s == steps - 1) {
@@ -753,7 +753,7 @@ void DevHier::coarse_solve(const T* b, T* x) {
 
 bool DevHier::fused_rz_ok(const CycleOpts& o) const {
   return !L_.empty() && o.post >= 1 &&
-         (L_[0].smoother == SmootherKind::Jacobi || L_[0].smoother == SmootherKind::L1Jacobi);
+         jacobi_type(L_[0].smoother);
 }
 
 template <typename T>
@@ -778,7 +778,7 @@ T* DevHier::cycle_level(int l, T* x, const T* b, bool x_zero, const CycleOpts& o
   LevelVecs<T>& V = vecs<T>(l);
   const DevMat& A = tr_ ? L.At : L.A;
   const T om = (T)L.omega;
-  const bool jac = (L.smoother == SmootherKind::Jacobi || L.smoother == SmootherKind::L1Jacobi);
+  const bool jac = jacobi_type(L.smoother);
   bool have_r = false;
   // pre-smoothing
   if (x_zero && jac && o.pre >= 1) {
@@ -810,7 +810,7 @@ T* DevHier::cycle_level(int l, T* x, const T* b, bool x_zero, const CycleOpts& o
   T* bn = last ? coarse_b<T>() : vecs<T>(l + 1).b;
   bool x1n = false;
   if (!last && l + 1 != tail_ && o.pre == 1 &&
-      (L_[l + 1].smoother == SmootherKind::Jacobi || L_[l + 1].smoother == SmootherKind::L1Jacobi)) {
+      jacobi_type(L_[l + 1].smoother)) {
     // the coarse level starts from zero with one Jacobi step: form it here
     DevLevel& Ln = L_[l + 1];
     launch_rows(st_, max_grid_, L.R, mval<T>(L.R), XPlain<T>{V.r},
@@ -901,8 +901,8 @@ int DevHier::solve(double* x, const double* b, const CycleOpts& o, double tol, i
 void DevHier::build_transpose() {
   if (at_built_) return;
   for (auto& d : L_)
-    if (d.smoother != SmootherKind::Jacobi && d.smoother != SmootherKind::L1Jacobi)
-      fail("transposed cycles need Jacobi or l1-Jacobi smoothing on every level");
+    if (!jacobi_type(d.smoother))
+      fail("transposed cycles need Jacobi, l1-Jacobi or SPAI(0) smoothing on every level");
   DR_CK(cudaStreamSynchronize(st_));
   std::vector<std::vector<int>> keep_rp, keep_ci;  // alive until the uploads finish
   for (auto& d : L_) {
@@ -943,6 +943,8 @@ void DevHier::refresh_transpose() {
     counted();
     if (d.smoother == SmootherKind::L1Jacobi)
       k_l1_invdiag<<<grid1d(d.A.n, max_grid_), kBlock, 0, st_>>>(d.A.n, d.At.rp, d.At.v, d.invdT);
+    else if (d.smoother == SmootherKind::SPAI0)
+      k_spai0_diag<<<grid1d(d.A.n, max_grid_), kBlock, 0, st_>>>(d.A.n, d.At.rp, d.At.ci, d.At.v, d.invdT);
     else
       k_invdiag<<<grid1d(d.A.n, max_grid_), kBlock, 0, st_>>>(d.A.n, d.At.rp, d.At.ci, d.At.v, d.invdT);
   }
@@ -1270,6 +1272,8 @@ void DevHier::resetup_values(const double* v_dev) {
     counted();
     if (d.smoother == SmootherKind::L1Jacobi || d.smoother == SmootherKind::L1ColoredGS)
       k_l1_invdiag<<<grid1d(d.A.n, max_grid_), kBlock, 0, st_>>>(d.A.n, d.A.rp, d.A.v, d.invd);
+    else if (d.smoother == SmootherKind::SPAI0)
+      k_spai0_diag<<<grid1d(d.A.n, max_grid_), kBlock, 0, st_>>>(d.A.n, d.A.rp, d.A.ci, d.A.v, d.invd);
     else
       k_invdiag<<<grid1d(d.A.n, max_grid_), kBlock, 0, st_>>>(d.A.n, d.A.rp, d.A.ci, d.A.v, d.invd);
     DR_CK(cudaGetLastError());

@@ -232,6 +232,21 @@ void l1_inverse_diagonal(const CSR& A, std::vector<double>& invd) {
   }
 }
 
+// SPAI(0): m_i = a_ii / sum_j a_ij^2, the minimiser of ||e_i - m_i A_i,:||,
+// 0 for a zero row; products and sums rounded separately, in column order.
+void spai0_diagonal(const CSR& A, std::vector<double>& m) {
+  m.resize(A.n);
+#pragma omp parallel for schedule(static, 4096)
+  for (int i = 0; i < A.n; ++i) {
+    double d = 0.0, s = 0.0;
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+      s += A.v[k] * A.v[k];
+      if (A.ci[k] == i) d = A.v[k];
+    }
+    m[i] = s > 0.0 ? d / s : 0.0;
+  }
+}
+
 void csr_to_dense(const CSR& A, std::vector<double>& M) {
   const int n = A.n;
   M.assign((size_t)n * n, 0.0);
@@ -340,6 +355,10 @@ void build_smoother(HostLevel& L, const Config& cfg) {
     case SmootherKind::L1Jacobi:
       l1_inverse_diagonal(L.A, L.invdiag);
       break;
+    case SmootherKind::SPAI0:  // x + m (b - A x): the Jacobi sweep with omega = 1
+      spai0_diagonal(L.A, L.invdiag);
+      L.omega = 1.0;
+      break;
     case SmootherKind::ColoredGS:
       greedy_coloring(L.A, L.colors, L.num_colors);
       color_order_from(L.colors, L.num_colors, L.color_off, L.color_order);
@@ -352,8 +371,8 @@ void build_smoother(HostLevel& L, const Config& cfg) {
       break;
     default:
       fail("smoother \"" + smoother_name(cfg.smoother) +
-           "\" is not supported by the B200 build (use jacobi, l1_jacobi, colored_gs or "
-           "l1_colored_gs)");
+           "\" is not supported by the B200 build (use jacobi, l1_jacobi, spai0, colored_gs "
+           "or l1_colored_gs)");
   }
 }
 
@@ -365,12 +384,12 @@ void build_hierarchy(const CSR& A_in, const Config& cfg, bool allow_partial_rese
   if (A_in.n != A_in.m) fail("matrix must be square");
   // Check the smoother before any work, so an unsupported choice fails fast.
   switch (cfg.smoother) {
-    case SmootherKind::Jacobi: case SmootherKind::L1Jacobi:
+    case SmootherKind::Jacobi: case SmootherKind::L1Jacobi: case SmootherKind::SPAI0:
     case SmootherKind::ColoredGS: case SmootherKind::L1ColoredGS: break;
     default:
       fail("smoother \"" + smoother_name(cfg.smoother) +
-           "\" is not supported by the B200 build (use jacobi, l1_jacobi, colored_gs or "
-           "l1_colored_gs)");
+           "\" is not supported by the B200 build (use jacobi, l1_jacobi, spai0, colored_gs "
+           "or l1_colored_gs)");
   }
   H = HostHierarchy();
   H.cfg = cfg;

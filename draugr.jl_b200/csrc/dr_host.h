@@ -96,6 +96,13 @@ enum class SmootherKind : int {
   SerialILU0 = 10,
 };
 
+// Smoothers whose sweep is x + (omega d_i)(b - A x)_i with a per-row
+// factor d: Jacobi and l1-Jacobi (d = 1/a_ii, 1/sum|a_ij|) and SPAI(0)
+// (d = a_ii / sum a_ij^2, omega = 1).
+inline bool jacobi_type(SmootherKind k) {
+  return k == SmootherKind::Jacobi || k == SmootherKind::L1Jacobi || k == SmootherKind::SPAI0;
+}
+
 enum class StrengthKind : int { Absolute = 0, Signed = 1 };
 
 struct Config {
@@ -204,6 +211,7 @@ void color_order_from(const std::vector<int>& colors, int num_colors,
                       std::vector<int>& off, std::vector<int>& order);
 void inverse_diagonal(const CSR& A, std::vector<double>& invd);     // smoothers.jl:47-63
 void l1_inverse_diagonal(const CSR& A, std::vector<double>& invd);  // smoothers.jl:816-827
+void spai0_diagonal(const CSR& A, std::vector<double>& m);          // smoothers.jl:524-538
 void csr_to_dense(const CSR& A, std::vector<double>& M);            // setup.jl:495-516
 void dense_lu(int n, std::vector<double>& lu, std::vector<int>& piv);
 

@@ -1222,6 +1222,21 @@ __global__ void k_l1_invdiag(int n, const int* __restrict__ rp, const double* __
   }
 }
 
+// src/smoothers.jl:524-538: SPAI(0) m_i = a_ii / sum_j a_ij^2 (0 for a
+// zero row), products and sums rounded separately, in column order
+__global__ void k_spai0_diag(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                             const double* __restrict__ v, double* __restrict__ m) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double d = 0.0, s = 0.0;
+    for (int k = rp[i]; k < rp[i + 1]; ++k) {
+      const double a = v[k];
+      s = __dadd_rn(s, __dmul_rn(a, a));
+      if (ci[k] == i) d = a;
+    }
+    m[i] = s > 0.0 ? __ddiv_rn(d, s) : 0.0;
+  }
+}
+
 // ------------------------------------------------------------ Galerkin product
 // Phase 1 (A·P): S = A, B = P.  Phase 2 (Pᵀ·(AP)): S = R = Pᵀ in
 // transpose-map order, B = A·P.

@@ -109,7 +109,7 @@ int32_t draugr_b200_pcg_device(int32_t handle, int32_t n, double *x_dev, const d
  * transpose 0: M = A.  transpose 1: M = A^T, the adjoint system of a
  * gradient computation, with cycles on the transposed hierarchy (A^T on
  * every level, the same P and P^T, the transposed coarsest LU solve);
- * every level must use (l1-)Jacobi smoothing.  x holds the initial guess;
+ * every level must use Jacobi, l1-Jacobi or SPAI(0) smoothing.  x holds the initial guess;
  * relres (may be NULL) receives the final true relative residual.  Returns
  * iterations or -1.  No counterpart in the reference, which has neither a
  * nonsymmetric Krylov solver nor adjoints. */
@@ -124,7 +124,7 @@ int32_t draugr_b200_bicgstab_device(int32_t handle, int32_t n, double *x_dev, co
  * at once: X and B are device arrays of n x k doubles, row-major (column c
  * of row i at i*k + c); X holds the initial guesses.  Each product with a
  * level matrix serves all k columns in one pass over the matrix.
- * precision as for draugr_b200_pcg; every level must use (l1-)Jacobi
+ * precision as for draugr_b200_pcg; every level must use Jacobi, l1-Jacobi or SPAI(0)
  * smoothing.  iters and relres (host arrays of k entries, may be NULL)
  * receive each column's iterations and final true relative residual.
  * Returns the largest iteration count or -1.  No counterpart in the

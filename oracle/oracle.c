@@ -34,7 +34,7 @@ typedef struct {
   const int *P_rp, *P_ci;
   const double *P_v;
   const int *T_off, *T_rows, *T_pnz;
-  int smoother; /* 0 jacobi, 1 colored_gs, 5 l1_jacobi, 6 l1_colored_gs */
+  int smoother; /* 0 jacobi, 1 colored_gs, 3 spai0, 5 l1_jacobi, 6 l1_colored_gs */
   double omega;
   double *invd;
   int ncolors;
@@ -102,6 +102,39 @@ void orc_l1_invdiag(int n, const int *rp, const double *v, double *invd) {
     for (int k = rp[i]; k < rp[i + 1]; ++k) l1 += fabs(v[k]);
     invd[i] = l1 > 2.220446049250313e-16 ? 1.0 / l1 : 0.0;
   }
+}
+
+/* spai0_kernel!, src/smoothers.jl:524-538: m_i = a_ii / sum_j a_ij^2 (the
+ * last diagonal entry of the row, 0 for a zero row) */
+void orc_spai0(int n, const int *rp, const int *ci, const double *v, double *m) {
+#pragma omp parallel for schedule(static, CHUNK)
+  for (int i = 0; i < n; ++i) {
+    double d = 0.0, s = 0.0;
+    for (int k = rp[i]; k < rp[i + 1]; ++k) {
+      s += v[k] * v[k];
+      if (ci[k] == i) d = v[k];
+    }
+    m[i] = s > 0.0 ? d / s : 0.0;
+  }
+}
+
+/* smooth!(::SPAI0Smoother): spai0_smooth_kernel! with the tmp/x ping-pong
+ * and the copy back on odd step counts, src/smoothers.jl:546-583 */
+void orc_spai0_smooth(int n, const int *rp, const int *ci, const double *v, const double *m,
+                      double *x, const double *b, int steps, double *tmp) {
+  double *src = x, *dst = tmp;
+  for (int s = 0; s < steps; ++s) {
+#pragma omp parallel for schedule(static, CHUNK)
+    for (int i = 0; i < n; ++i) {
+      double ri = b[i];
+      for (int k = rp[i]; k < rp[i + 1]; ++k) ri -= v[k] * src[ci[k]];
+      dst[i] = src[i] + m[i] * ri;
+    }
+    double *t = src;
+    src = dst;
+    dst = t;
+  }
+  if (steps & 1) memcpy(x, tmp, (size_t)n * sizeof(double));
 }
 
 /* smooth!(::JacobiSmoother / ::L1JacobiSmoother): jacobi_kernel! with the
@@ -443,6 +476,8 @@ static void smooth(olevel *L, double *x, const double *b, int steps) {
   if (steps <= 0) return;
   if (L->smoother == 0 || L->smoother == 5)
     orc_jacobi(L->n, L->A_rp, L->A_ci, L->A_v, L->invd, L->omega, x, b, steps, L->tmp);
+  else if (L->smoother == 3)
+    orc_spai0_smooth(L->n, L->A_rp, L->A_ci, L->A_v, L->invd, x, b, steps, L->tmp);
   else
     orc_gs(L->n, L->A_rp, L->A_ci, L->A_v, L->invd, L->ncolors, L->color_off, L->color_order, x, b,
            steps);
@@ -575,6 +610,7 @@ int orc_pcg(ohier *h, double *x, const double *b, int pre, int post, int w, doub
  * Returns 0 or the LU's zero-pivot index. */
 static void upd_invd(olevel *L) {
   if (L->smoother == 5 || L->smoother == 6) orc_l1_invdiag(L->n, L->A_rp, L->A_v, L->invd);
+  else if (L->smoother == 3) orc_spai0(L->n, L->A_rp, L->A_ci, L->A_v, L->invd);
   else orc_invdiag(L->n, L->A_rp, L->A_ci, L->A_v, L->invd);
 }
 

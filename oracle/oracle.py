@@ -63,6 +63,8 @@ def _declare(lib):
         "orc_residual": (None, [i32, P, P, P, P, P, P]),
         "orc_invdiag": (None, [i32, P, P, P, P]),
         "orc_l1_invdiag": (None, [i32, P, P, P]),
+        "orc_spai0": (None, [i32, P, P, P, P]),
+        "orc_spai0_smooth": (None, [i32, P, P, P, P, P, P, i32, P]),
         "orc_jacobi": (None, [i32, P, P, P, P, f64, P, P, i32, P]),
         "orc_greedy_coloring": (i32, [i32, P, P, P]),
         "orc_color_order": (None, [i32, P, i32, P, P]),
@@ -119,6 +121,22 @@ def invdiag(n, rp, ci, v, l1=False):
     else:
         load().orc_invdiag(n, ptr(rp), ptr(ci), ptr(v), ptr(d))
     return d
+
+
+def spai0(n, rp, ci, v):
+    """SPAI(0) diagonal m_i = a_ii / sum_j a_ij^2 (spai0_kernel!)."""
+    m = np.zeros(n)
+    load().orc_spai0(n, ptr(rp), ptr(ci), ptr(v), ptr(m))
+    return m
+
+
+def spai0_smooth(n, rp, ci, v, m, x, b, steps):
+    """`steps` SPAI(0) sweeps x <- x + m (b - A x) (smooth!(::SPAI0Smoother))."""
+    x = np.array(x, dtype=np.float64)
+    tmp = np.zeros(n)
+    load().orc_spai0_smooth(n, ptr(rp), ptr(ci), ptr(v), ptr(np.ascontiguousarray(m, np.float64)), ptr(x),
+                            ptr(np.ascontiguousarray(b, np.float64)), steps, ptr(tmp))
+    return x
 
 
 def jacobi(n, rp, ci, v, invd, omega, x, b, steps):
@@ -202,7 +220,7 @@ def strength_abs(n, rp, ci, v, theta):
 
 
 # ---------------------------------------------------------------- hierarchy mirror
-SMOOTHER_KIND = {0: "jacobi", 1: "colored_gs", 5: "l1_jacobi", 6: "l1_colored_gs"}
+SMOOTHER_KIND = {0: "jacobi", 1: "colored_gs", 3: "spai0", 5: "l1_jacobi", 6: "l1_colored_gs"}
 
 
 class OracleHierarchy:

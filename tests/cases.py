@@ -15,6 +15,10 @@ CASES = {
     "pmis_direct_gs": (lambda: problems.poisson3d(10),
                        draugr.AMGConfig(coarsening=draugr.PMISCoarsening(0.25),
                                         smoother=draugr.ColoredGaussSeidelType())),
+    "pmis_standard_spai0": (lambda: problems.heterogeneous_diffusion_3d(10, seed=5),
+                            draugr.AMGConfig(coarsening=draugr.PMISCoarsening(
+                                0.25, draugr.StandardInterpolation()),
+                                smoother=draugr.SPAI0SmootherType())),
     "aniso27_hmis": (lambda: problems.anisotropic_27pt(9, 1e-3),
                      draugr.AMGConfig(coarsening=draugr.HMISCoarsening(
                          0.25, draugr.ExtendedIInterpolation(0.2)),

@@ -136,7 +136,11 @@ def test_structure_matches_oracle(host_case):
         scale = np.abs(c_v).max()
         assert np.abs(c_v - nv).max() <= 1e-12 * scale
         kind = int(info[4])
-        inv = oracle.invdiag(n, arp, aci, av, l1=kind in (5, 6))
+        if kind == 3:  # SPAI(0): m_i = a_ii / sum a_ij^2, swept with omega = 1
+            inv = oracle.spai0(n, arp, aci, av)
+            assert h.export(l, "omega")[0] == 1.0
+        else:
+            inv = oracle.invdiag(n, arp, aci, av, l1=kind in (5, 6))
         assert np.array_equal(inv, h.export(l, "invdiag"))
         if kind in (1, 6):
             colors, ncol, coff, order = oracle.greedy_coloring(n, arp, aci)

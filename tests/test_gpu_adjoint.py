@@ -150,13 +150,16 @@ def test_full_size_gradient(name):
     check_finite_differences(h, make, kappa, b, S, d, symmetric, L, gk, rng, tol=1e-15, rtol=1e-4)
 
 
-def test_transposed_bicgstab_solves_the_adjoint_system():
+@pytest.mark.parametrize("smoother", ["l1_jacobi", "spai0"])
+def test_transposed_bicgstab_solves_the_adjoint_system(smoother):
     kappa = np.exp(np.random.default_rng(2).normal(0.0, 1.0, (48, 48)))
     A, _ = problems.convection_diffusion_2d(kappa, 50.0, seed=1)
-    h = draugr.amg_setup(A, CFG)
+    cfg = CFG if smoother == "l1_jacobi" else draugr.hypre_default_config(
+        agg_trunc_factor=0.2, smoother=draugr.SPAI0SmootherType(), seed=3)
+    h = draugr.amg_setup(A, cfg)
     b = np.random.default_rng(3).uniform(-1, 1, A.shape[0])
     for transpose, M in ((False, A), (True, A.T.tocsr())):
-        x, it, rr = draugr.bicgstab(np.zeros(A.shape[0]), b, h, CFG, tol=1e-10, maxiter=500,
+        x, it, rr = draugr.bicgstab(np.zeros(A.shape[0]), b, h, cfg, tol=1e-10, maxiter=500,
                                     transpose=transpose)
         assert it < 500 and rr < 1e-10
         assert np.linalg.norm(b - M @ x) / np.linalg.norm(b) < 1e-10

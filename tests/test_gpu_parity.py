@@ -63,14 +63,17 @@ def test_level_kernels(case):
         for steps in (1, 2, 3):
             if L.smoother in (0, 5):
                 ref = oracle.jacobi(n, d["A_rp"], d["A_ci"], d["A_v"], d["invd"], L.omega, x, b, steps)
+            elif L.smoother == 3:
+                ref = oracle.spai0_smooth(n, d["A_rp"], d["A_ci"], d["A_v"], d["invd"], x, b, steps)
             else:
                 ref = oracle.gs(n, d["A_rp"], d["A_ci"], d["A_v"], d["invd"], L.ncolors,
                                 d["color_off"], d["color_order"], x, b, steps)
             assert rel(h.level_op(l, 2, x, b, steps=steps), ref) < TOL64, (l, steps)
             assert rel(h.level_op(l, 2, x, b, steps=steps, precision=1), ref) < TOL32
-        if L.smoother in (0, 5):
-            x1 = oracle.jacobi(n, d["A_rp"], d["A_ci"], d["A_v"], d["invd"], L.omega,
-                               np.zeros(n), b, 1)
+        if L.smoother in (0, 3, 5):
+            x1 = (oracle.spai0_smooth(n, d["A_rp"], d["A_ci"], d["A_v"], d["invd"], np.zeros(n), b, 1)
+                  if L.smoother == 3 else
+                  oracle.jacobi(n, d["A_rp"], d["A_ci"], d["A_v"], d["invd"], L.omega, np.zeros(n), b, 1))
             r1 = oracle.residual(n, d["A_rp"], d["A_ci"], d["A_v"], x1, b)
             out = h.level_op(l, 6, b)
             assert rel(out[:n], x1) < TOL64

@@ -114,6 +114,28 @@ def test_l1_invdiag():
     assert np.isclose(inv[4], 0.25)
 
 
+def test_spai0_diagonal_smoothing_and_solve():
+    """testsets "SPAI0 Smoother - Build / Smoothing" and "AMG Solve - SPAI0"
+    (test/runtests.jl:754-788): interior row [-1 2 -1] gives m = 2/6; 10
+    sweeps reduce the residual; amg_solve! with SPAI(0) on the 10 x 10
+    Poisson matrix reaches 1e-8 in fewer than 200 cycles."""
+    A = problems.poisson1d(10)
+    n, rp, ci, v = parts(A)
+    m = oracle.spai0(n, rp, ci, v)
+    assert len(m) == 10 and np.isclose(m[4], 2.0 / 6.0)
+    b = np.ones(n)
+    x = oracle.spai0_smooth(n, rp, ci, v, m, np.zeros(n), b, 10)
+    assert np.linalg.norm(b - A @ x) < np.linalg.norm(b)
+    A = problems.poisson2d(10)
+    b = np.random.default_rng(2).uniform(0, 1, 100)
+    cfg = draugr.AMGConfig(smoother=draugr.SPAI0SmootherType())
+    h = draugr.amg_setup(A, cfg, on_device=False)
+    O = oracle.OracleHierarchy(h)
+    x, it, rel = O.solve(np.zeros(100), b, tol=1e-8, maxiter=200)
+    assert it < 200 and rel < 1e-8
+    assert np.linalg.norm(b - A @ x) / np.linalg.norm(b) < 1e-8
+
+
 def test_coloring():
     """testsets "Graph Coloring" (:549-566) and "Colored GS Smoother" (:568-588)."""
     A = problems.poisson1d(10)
