@@ -364,11 +364,14 @@ int64_t draugr_b200_export(int32_t handle, int32_t lvl, const char* what, void* 
       else if (w == "R_nzval") dv = &L.Rv;
       else if (w == "invdiag") dv = &L.invdiag;
       else if (w == "omega") { tmpd.assign(1, L.omega); dv = &tmpd; }
+      else if (w == "cheb_coef") dv = &L.cheb_coef;
+      else if (w == "cheb_v0") dv = &L.cheb_v0;
       else if (w == "AP_nzval") {
         if (!H->dev) fail("AP_nzval lives on the device only");
         dv = &tmpd;
       }
-      if (dv && H->dev && w != "P_nzval" && w != "R_nzval" && w != "omega") {
+      if (dv && H->dev && w != "P_nzval" && w != "R_nzval" && w != "omega" && w != "cheb_v0" &&
+          !(w == "cheb_coef" && L.cheb_coef.empty())) {
         H->dev->export_values(lvl, w, tmpd);
         dv = &tmpd;
       }

@@ -311,6 +311,14 @@ DevHier::DevHier(const HostHierarchy& H, int device) {
       }
       d.v64.xb = alloc<double>(n);
       d.v64.r = alloc<double>(n);
+      if (h.smoother == SmootherKind::Chebyshev) {
+        d.cheb_degree = h.cheb_degree;
+        d.cheb_v0 = alloc<double>(n);
+        h2d(d.cheb_v0, h.cheb_v0, st_);
+        d.cheb_coef = alloc<double>(2 * (size_t)h.cheb_degree + 2);
+        h2d(d.cheb_coef, h.cheb_coef, st_);
+        d.v64.d = alloc<double>(n);
+      }
     }
     nc_ = H.nc;
     up_csr(C_, H.coarse.n, H.coarse.m, H.coarse.rp, H.coarse.ci, &H.coarse.v);
@@ -453,6 +461,7 @@ void DevHier::ensure_fp32() {
     d.v32.xb = alloc<float>(n);
     d.v32.b = alloc<float>(n);
     d.v32.r = alloc<float>(n);
+    if (d.smoother == SmootherKind::Chebyshev) d.v32.d = alloc<float>(n);
   }
   cb32_ = alloc<float>(nc_);
   cx32_ = alloc<float>(nc_);
@@ -700,6 +709,16 @@ T* DevHier::smooth(int l, T* x, const T* b, int steps, T* ext, const double* rz_
       }
       x = dst;
     }
+  } else if (L.smoother == SmootherKind::Chebyshev) {
+    // each application: `cheb_degree` fused residual-and-update steps, the
+    // iterate ping-ponging between two buffers as in the Jacobi sweeps
+    for (int s = 0; s < steps; ++s)
+      for (int j = 0; j < L.cheb_degree; ++j) {
+        T* dst = (l == 0) ? (x == V.xb ? ext : V.xb) : (x == V.xa ? V.xb : V.xa);
+        launch_rows(st_, max_grid_, A, mval<T>(A), XPlain<T>{x},
+                    EpCheby<T>{x, b, invd<T>(L), V.d, dst, L.cheb_coef, j});
+        x = dst;
+      }
   } else {
     for (int s = 0; s < steps; ++s)
       for (int c = 0; c < L.ncolors; ++c) {
@@ -1277,6 +1296,24 @@ void DevHier::resetup_values(const double* v_dev) {
     else
       k_invdiag<<<grid1d(d.A.n, max_grid_), kBlock, 0, st_>>>(d.A.n, d.A.rp, d.A.ci, d.A.v, d.invd);
     DR_CK(cudaGetLastError());
+    if (d.smoother == SmootherKind::Chebyshev) {
+      // update_smoother!(::ChebyshevSmoother): the spectral radius of D^-1 A
+      // again (10 power steps from the stored start vector, on the device),
+      // then the coefficients
+      double* v = d.v64.xb;
+      double* w = d.v64.r;
+      double* lam2 = d.cheb_coef + 2 * d.cheb_degree;
+      DR_CK(cudaMemcpyAsync(v, d.cheb_v0, (size_t)d.A.n * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+      for (int it = 0; it < 10; ++it) {
+        launch_rows_dot(st_, max_grid_, d.A, d.A.v, XPlain<double>{v}, EpPowerStep{d.invd, w}, partials_,
+                        tickets_ + TK_DOT, FinStore{lam2});
+        counted();
+        k_cheb_rescale<<<grid1d(d.A.n, max_grid_), kBlock, 0, st_>>>(d.A.n, w, lam2, v);
+      }
+      counted();
+      k_cheb_coef<<<1, 32, 0, st_>>>(lam2, d.cheb_degree, d.cheb_coef);
+      DR_CK(cudaGetLastError());
+    }
   };
   if (nl > 0) upd_invd(L_[0]);
   for (int l = 0; l < nl; ++l) {
@@ -1492,6 +1529,7 @@ void DevHier::export_values(int lvl, const std::string& what, std::vector<double
     if (what == "A_nzval") { src = d.A.v; n = d.A.nnz; }
     else if (what == "P_nzval") { src = d.P.v; n = d.P.nnz; }
     else if (what == "invdiag") { src = d.invd; n = d.A.n; }
+    else if (what == "cheb_coef" && d.cheb_coef) { src = d.cheb_coef; n = 2LL * d.cheb_degree; }
     else if (what == "AP_nzval" && d.has_rap) { src = d.AP.v; n = d.AP.nnz; }
   }
   if (!src) fail("unknown device export: " + what);

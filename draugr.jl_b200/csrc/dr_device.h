@@ -103,6 +103,7 @@ struct LevelVecs {
   T* xb = nullptr;  // ... and its Jacobi ping-pong partner (level 0: partner of the caller's x)
   T* b = nullptr;   // right-hand side (levels >= 1: written by the restriction above)
   T* r = nullptr;   // residual
+  T* d = nullptr;   // Chebyshev update direction (Chebyshev levels only)
 };
 
 struct DevLevel {
@@ -119,6 +120,12 @@ struct DevLevel {
   DevMat At;                 // A^T (transposed cycles; built on first use)
   int* at_perm = nullptr;    // At value k = A value at_perm[k]
   double* invdT = nullptr;   // smoother diagonal of A^T
+  // Chebyshev: inner steps per application, the normalised power-iteration
+  // start vector, and the coefficient table (2 * degree entries, then the
+  // squared norm of the last power step)
+  int cheb_degree = 0;
+  double* cheb_v0 = nullptr;
+  double* cheb_coef = nullptr;
   LevelVecs<double> v64;
   LevelVecs<float> v32;
 };

@@ -247,6 +247,43 @@ void spai0_diagonal(const CSR& A, std::vector<double>& m) {
   }
 }
 
+double spectral_radius_estimate(const CSR& A, const std::vector<double>& invd, std::vector<double>& v,
+                                int niter) {
+  const int n = A.n;
+  std::vector<double> w(n);
+  double lam = 1.0;
+  for (int it = 0; it < niter; ++it) {
+#pragma omp parallel for schedule(static, 4096)
+    for (int i = 0; i < n; ++i) {
+      double s = 0.0;
+      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) s += A.v[k] * v[A.ci[k]];
+      w[i] = s * invd[i];
+    }
+    double ss = 0.0;
+    for (int i = 0; i < n; ++i) ss += w[i] * w[i];
+    lam = std::sqrt(ss);
+    if (lam > kEps)
+      for (int i = 0; i < n; ++i) v[i] = w[i] / lam;
+  }
+  return lam;
+}
+
+void chebyshev_coefficients(double rho, int degree, std::vector<double>& coef) {
+  const double lmax = 1.1 * rho;
+  const double lmin = lmax / 30.0;
+  const double theta = (lmax + lmin) / 2.0;
+  const double delta = (lmax - lmin) / 2.0;
+  coef.assign(2 * (size_t)degree, 0.0);
+  coef[0] = 1.0 / theta;
+  double s_old = theta / delta;
+  for (int k = 1; k < degree; ++k) {
+    const double s_new = 1.0 / (2.0 * theta / delta - s_old);
+    coef[2 * k] = 2.0 * s_new / delta;
+    coef[2 * k + 1] = s_new * s_old;
+    s_old = s_new;
+  }
+}
+
 void csr_to_dense(const CSR& A, std::vector<double>& M) {
   const int n = A.n;
   M.assign((size_t)n * n, 0.0);
@@ -345,7 +382,25 @@ void coarsen_with_fallback(const CSR& A, const Coarsening& alg, const Config& cf
   }
 }
 
-void build_smoother(HostLevel& L, const Config& cfg) {
+// Normalised start vector of the Chebyshev power iteration: standard normal
+// entries (Box-Muller on splitmix64 uniforms), divided by their 2-norm.
+std::vector<double> chebyshev_start(int n, uint64_t seed) {
+  std::vector<double> v(n);
+  uint64_t s = seed;
+  for (int i = 0; i < n; ++i) {
+    const double u1 = 1.0 - rng_uniform(s);  // (0, 1]
+    const double u2 = rng_uniform(s);
+    v[i] = std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
+  }
+  double ss = 0.0;
+  for (int i = 0; i < n; ++i) ss += v[i] * v[i];
+  const double nv = std::sqrt(ss);
+  if (nv > 0.0)
+    for (int i = 0; i < n; ++i) v[i] /= nv;
+  return v;
+}
+
+void build_smoother(HostLevel& L, const Config& cfg, int level) {
   L.smoother = cfg.smoother;
   L.omega = cfg.jacobi_omega;
   switch (cfg.smoother) {
@@ -359,6 +414,15 @@ void build_smoother(HostLevel& L, const Config& cfg) {
       spai0_diagonal(L.A, L.invdiag);
       L.omega = 1.0;
       break;
+    case SmootherKind::Chebyshev: {  // build_chebyshev_smoother, smoothers.jl:895-910 (degree 3)
+      inverse_diagonal(L.A, L.invdiag);
+      L.cheb_degree = 3;
+      L.cheb_v0 = chebyshev_start(L.A.n, cfg.seed ^ (0xC6EB5E5ULL * (uint64_t)(level + 1)));
+      std::vector<double> v = L.cheb_v0;
+      L.cheb_rho = spectral_radius_estimate(L.A, L.invdiag, v, 10);
+      chebyshev_coefficients(L.cheb_rho, L.cheb_degree, L.cheb_coef);
+      break;
+    }
     case SmootherKind::ColoredGS:
       greedy_coloring(L.A, L.colors, L.num_colors);
       color_order_from(L.colors, L.num_colors, L.color_off, L.color_order);
@@ -371,8 +435,8 @@ void build_smoother(HostLevel& L, const Config& cfg) {
       break;
     default:
       fail("smoother \"" + smoother_name(cfg.smoother) +
-           "\" is not supported by the B200 build (use jacobi, l1_jacobi, spai0, colored_gs "
-           "or l1_colored_gs)");
+           "\" is not supported by the B200 build (use jacobi, l1_jacobi, spai0, chebyshev, "
+           "colored_gs or l1_colored_gs)");
   }
 }
 
@@ -385,11 +449,12 @@ void build_hierarchy(const CSR& A_in, const Config& cfg, bool allow_partial_rese
   // Check the smoother before any work, so an unsupported choice fails fast.
   switch (cfg.smoother) {
     case SmootherKind::Jacobi: case SmootherKind::L1Jacobi: case SmootherKind::SPAI0:
+    case SmootherKind::Chebyshev:
     case SmootherKind::ColoredGS: case SmootherKind::L1ColoredGS: break;
     default:
       fail("smoother \"" + smoother_name(cfg.smoother) +
-           "\" is not supported by the B200 build (use jacobi, l1_jacobi, spai0, colored_gs "
-           "or l1_colored_gs)");
+           "\" is not supported by the B200 build (use jacobi, l1_jacobi, spai0, chebyshev, "
+           "colored_gs or l1_colored_gs)");
   }
   H = HostHierarchy();
   H.cfg = cfg;
@@ -424,7 +489,7 @@ void build_hierarchy(const CSR& A_in, const Config& cfg, bool allow_partial_rese
     }
     L.A = std::move(cur);
     L.P = std::move(P);
-    build_smoother(L, cfg);
+    build_smoother(L, cfg, (int)H.levels.size());
     H.levels.push_back(std::move(L));
     cur = std::move(next);
   }

@@ -150,6 +150,15 @@ struct HostLevel {
   std::vector<int> colors;        // 1-based colours, per row
   std::vector<int> color_off;     // num_colors+1, 0-based offsets
   std::vector<int> color_order;   // rows sorted by colour
+  // Chebyshev (src/smoothers.jl:860-1003): the normalised start vector of
+  // the power iteration for the spectral radius of D^-1 A (seeded; the
+  // reference draws an unseeded randn), the estimate, and the coefficients
+  // of the `cheb_degree` inner steps: cheb_coef[0] = 1/theta, then
+  // (scale_r, scale_d) of steps 1.. at [2j], [2j+1].
+  int cheb_degree = 0;
+  std::vector<double> cheb_v0;
+  double cheb_rho = 0.0;
+  std::vector<double> cheb_coef;
 };
 
 struct HostHierarchy {
@@ -212,6 +221,14 @@ void color_order_from(const std::vector<int>& colors, int num_colors,
 void inverse_diagonal(const CSR& A, std::vector<double>& invd);     // smoothers.jl:47-63
 void l1_inverse_diagonal(const CSR& A, std::vector<double>& invd);  // smoothers.jl:816-827
 void spai0_diagonal(const CSR& A, std::vector<double>& m);          // smoothers.jl:524-538
+// _estimate_spectral_radius (smoothers.jl:869-887): `niter` power steps on
+// D^-1 A from the normalised v (overwritten); returns the last ||w||.
+double spectral_radius_estimate(const CSR& A, const std::vector<double>& invd, std::vector<double>& v,
+                                int niter);
+// Coefficients of one Chebyshev application of `degree` inner steps for the
+// spectral-radius estimate rho (the bounds [rho * 1.1 / 30, rho * 1.1] and
+// the recurrence of smoothers.jl:895-986); 2 * degree entries.
+void chebyshev_coefficients(double rho, int degree, std::vector<double>& coef);
 void csr_to_dense(const CSR& A, std::vector<double>& M);            // setup.jl:495-516
 void dense_lu(int n, std::vector<double>& lu, std::vector<int>& piv);
 

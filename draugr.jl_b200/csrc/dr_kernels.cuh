@@ -261,6 +261,60 @@ struct EpPcgDir {  // q = A p, p_new = z + β p_old, returns p_new·q
   }
 };
 
+// One inner step j of a Chebyshev application (src/smoothers.jl:947-986,
+// residual_kernel_smoother! :988-999): Ax = sum a x from zero, r = b - Ax,
+// then j = 0: d = (invd r) c0 with c0 = 1/theta; j > 0: d = (c0 invd) r +
+// c1 d with (c0, c1) = (scale_r, scale_d) of step j; xn = x + d.  The
+// coefficients are read from device memory once per thread (bind()), so a
+// resetup can recompute them on the device.
+template <typename T>
+struct EpCheby {
+  using acc_t = T;
+  static constexpr int kSign = 1;
+  struct Pre { T x, b, di, d; };
+  const T* __restrict__ x;
+  const T* __restrict__ b;
+  const T* __restrict__ invd;
+  T* d;
+  T* __restrict__ xn;
+  const double* __restrict__ coef;
+  int j;
+  T c0, c1;
+  __device__ __forceinline__ void bind() {
+    c0 = (T)__ldg(coef + 2 * j);
+    c1 = j ? (T)__ldg(coef + 2 * j + 1) : T(0);
+  }
+  __device__ __forceinline__ Pre pre(int i) const {
+    return {__ldg(x + i), __ldg(b + i), __ldg(invd + i), j ? d[i] : T(0)};
+  }
+  __device__ __forceinline__ T init(const Pre&) const { return T(0); }
+  __device__ __forceinline__ double apply(int i, T v, const Pre& p) const {
+    const T r = sub_rn(p.b, v);
+    const T dn = j == 0 ? mul_rn(mul_rn(p.di, r), c0)
+                        : add_rn(mul_rn(mul_rn(c0, p.di), r), mul_rn(c1, p.d));
+    d[i] = dn;
+    xn[i] = add_rn(p.x, dn);
+    return 0.0;
+  }
+};
+
+// One power step of the spectral-radius estimate of D^-1 A
+// (src/smoothers.jl:876-880): w = (A v) invd, returning w_i^2 for ||w||.
+struct EpPowerStep {
+  using acc_t = double;
+  static constexpr int kSign = 1;
+  struct Pre { double di; };
+  const double* __restrict__ invd;
+  double* __restrict__ w;
+  __device__ __forceinline__ Pre pre(int i) const { return {__ldg(invd + i)}; }
+  __device__ __forceinline__ double init(const Pre&) const { return 0.0; }
+  __device__ __forceinline__ double apply(int i, double s, const Pre& p) const {
+    const double wi = mul_rn(s, p.di);
+    w[i] = wi;
+    return mul_rn(wi, wi);
+  }
+};
+
 // Warp barrier among the lanes executing together at this point: placed
 // between a batch of independent gathers and their first use, it makes the
 // compiler issue the whole batch first (without it, gathers whose indices
@@ -377,6 +431,8 @@ template <class EP>
 __device__ __forceinline__ void bind_epilogue(EP&) {}
 template <typename T>
 __device__ __forceinline__ void bind_epilogue(EpPcgDir<T>& e) { e.bind(); }
+template <typename T>
+__device__ __forceinline__ void bind_epilogue(EpCheby<T>& e) { e.bind(); }
 
 // Resident blocks per SM the register allocation plans for: planning for 4
 // lets 128-thread FP64 blocks keep a whole batch of 32 gathers in registers
@@ -1219,6 +1275,39 @@ __global__ void k_l1_invdiag(int n, const int* __restrict__ rp, const double* __
     double l1 = 0.0;
     for (int k = rp[i]; k < rp[i + 1]; ++k) l1 = __dadd_rn(l1, fabs(v[k]));
     invd[i] = l1 > 2.220446049250313e-16 ? __drcp_rn(l1) : 0.0;
+  }
+}
+
+// Power step, continued: lambda = ||w|| = sqrt(lam2[0]); v = w / lambda when
+// lambda > eps (src/smoothers.jl:881-884).
+__global__ void k_cheb_rescale(int n, const double* __restrict__ w, const double* __restrict__ lam2,
+                               double* __restrict__ v) {
+  const double lam = sqrt(__ldg(lam2));
+  if (!(lam > 2.220446049250313e-16)) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    v[i] = __ddiv_rn(w[i], lam);
+}
+
+// Chebyshev coefficients from the spectral-radius estimate rho =
+// sqrt(lam2[0]) (build_chebyshev_smoother and smooth!, src/smoothers.jl:
+// 895-910, :947-986): lambda_max = 1.1 rho, lambda_min = lambda_max / 30,
+// coef[0] = 1/theta, then (scale_r, scale_d) of inner steps 1.. at [2k],
+// [2k+1].  One thread.
+__global__ void k_cheb_coef(const double* __restrict__ lam2, int degree, double* __restrict__ coef) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const double rho = sqrt(lam2[0]);
+  const double lmax = __dmul_rn(1.1, rho);
+  const double lmin = __ddiv_rn(lmax, 30.0);
+  const double theta = __ddiv_rn(__dadd_rn(lmax, lmin), 2.0);
+  const double delta = __ddiv_rn(__dsub_rn(lmax, lmin), 2.0);
+  coef[0] = __ddiv_rn(1.0, theta);
+  coef[1] = 0.0;
+  double s_old = __ddiv_rn(theta, delta);
+  for (int k = 1; k < degree; ++k) {
+    const double s_new = __ddiv_rn(1.0, __dsub_rn(__ddiv_rn(__dmul_rn(2.0, theta), delta), s_old));
+    coef[2 * k] = __ddiv_rn(__dmul_rn(2.0, s_new), delta);
+    coef[2 * k + 1] = __dmul_rn(s_new, s_old);
+    s_old = s_new;
   }
 }
 

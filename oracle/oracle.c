@@ -34,7 +34,7 @@ typedef struct {
   const int *P_rp, *P_ci;
   const double *P_v;
   const int *T_off, *T_rows, *T_pnz;
-  int smoother; /* 0 jacobi, 1 colored_gs, 3 spai0, 5 l1_jacobi, 6 l1_colored_gs */
+  int smoother; /* 0 jacobi, 1 colored_gs, 3 spai0, 5 l1_jacobi, 6 l1_colored_gs, 8 chebyshev */
   double omega;
   double *invd;
   int ncolors;
@@ -43,6 +43,11 @@ typedef struct {
   /* Galerkin restriction map (orc_coarse_sparsity) for the resetup */
   const int64_t *nz_off;
   const int *tpi, *tai, *tpj;
+  /* Chebyshev: inner steps, normalised power-iteration start vector,
+   * coefficient table (2 * degree), update direction */
+  int cheb_degree;
+  const double *cheb_v0;
+  double *cheb_coef, *cheb_d;
 } olevel;
 
 typedef struct {
@@ -135,6 +140,86 @@ void orc_spai0_smooth(int n, const int *rp, const int *ci, const double *v, cons
     dst = t;
   }
   if (steps & 1) memcpy(x, tmp, (size_t)n * sizeof(double));
+}
+
+/* _estimate_spectral_radius, src/smoothers.jl:869-887: `niter` power steps
+ * w = (A v) .* invdiag (csr_mul_kernel! sums from zero), lambda = ||w||,
+ * v = w / lambda when lambda > eps; v holds the normalised start vector and
+ * is overwritten, w is work.  Returns the last lambda.  (norm is a plain
+ * sum of squares here; the reference's BLAS nrm2 scales, which changes
+ * only the last bits.) */
+double orc_spectral_radius(int n, const int *rp, const int *ci, const double *a, const double *invd,
+                           double *v, int niter, double *w) {
+  double lam = 1.0;
+  for (int it = 0; it < niter; ++it) {
+#pragma omp parallel for schedule(static, CHUNK)
+    for (int i = 0; i < n; ++i) {
+      double s = 0.0;
+      for (int k = rp[i]; k < rp[i + 1]; ++k) s += a[k] * v[ci[k]];
+      w[i] = s * invd[i];
+    }
+    double ss = 0.0;
+    for (int i = 0; i < n; ++i) ss += w[i] * w[i];
+    lam = sqrt(ss);
+    if (lam > 2.220446049250313e-16)
+      for (int i = 0; i < n; ++i) v[i] = w[i] / lam;
+  }
+  return lam;
+}
+
+/* Chebyshev bounds and recurrence coefficients, build_chebyshev_smoother
+ * (src/smoothers.jl:895-910: lambda_max = 1.1 rho, lambda_min =
+ * lambda_max / 30) and smooth! (:947-986): coef[0] = 1/theta, coef[1] = 0,
+ * then scale_r, scale_d of inner step k at [2k], [2k+1]. */
+void orc_cheb_coef(double rho, int degree, double *coef) {
+  double lmax = 1.1 * rho;
+  double lmin = lmax / 30.0;
+  double theta = (lmax + lmin) / 2.0;
+  double delta = (lmax - lmin) / 2.0;
+  coef[0] = 1.0 / theta;
+  coef[1] = 0.0;
+  double s_old = theta / delta;
+  for (int k = 1; k < degree; ++k) {
+    double s_new = 1.0 / (2.0 * theta / delta - s_old);
+    coef[2 * k] = 2.0 * s_new / delta;
+    coef[2 * k + 1] = s_new * s_old;
+    s_old = s_new;
+  }
+}
+
+/* residual_kernel_smoother!, src/smoothers.jl:988-999: Ax summed from zero,
+ * then r = b - Ax */
+static void cheb_residual(int n, const int *rp, const int *ci, const double *a, const double *x,
+                          const double *b, double *r) {
+#pragma omp parallel for schedule(static, CHUNK)
+  for (int i = 0; i < n; ++i) {
+    double s = 0.0;
+    for (int k = rp[i]; k < rp[i + 1]; ++k) s += a[k] * x[ci[k]];
+    r[i] = b[i] - s;
+  }
+}
+
+/* smooth!(::ChebyshevSmoother), src/smoothers.jl:947-986, with
+ * chebyshev_init_kernel! / chebyshev_iter_kernel! (:924-940): per step, the
+ * residual of the whole vector, then d = invdiag r / theta, x += d; then
+ * degree - 1 times the residual, d = scale_r invdiag r + scale_d d, x += d. */
+void orc_chebyshev(int n, const int *rp, const int *ci, const double *a, const double *invd,
+                   const double *coef, int degree, double *x, const double *b, int steps, double *r,
+                   double *d) {
+  for (int s = 0; s < steps; ++s) {
+    cheb_residual(n, rp, ci, a, x, b, r);
+    for (int i = 0; i < n; ++i) {
+      d[i] = invd[i] * r[i] * coef[0];
+      x[i] += d[i];
+    }
+    for (int k = 1; k < degree; ++k) {
+      cheb_residual(n, rp, ci, a, x, b, r);
+      for (int i = 0; i < n; ++i) {
+        d[i] = coef[2 * k] * invd[i] * r[i] + coef[2 * k + 1] * d[i];
+        x[i] += d[i];
+      }
+    }
+  }
 }
 
 /* smooth!(::JacobiSmoother / ::L1JacobiSmoother): jacobi_kernel! with the
@@ -478,6 +563,9 @@ static void smooth(olevel *L, double *x, const double *b, int steps) {
     orc_jacobi(L->n, L->A_rp, L->A_ci, L->A_v, L->invd, L->omega, x, b, steps, L->tmp);
   else if (L->smoother == 3)
     orc_spai0_smooth(L->n, L->A_rp, L->A_ci, L->A_v, L->invd, x, b, steps, L->tmp);
+  else if (L->smoother == 8)
+    orc_chebyshev(L->n, L->A_rp, L->A_ci, L->A_v, L->invd, L->cheb_coef, L->cheb_degree, x, b, steps,
+                  L->tmp, L->cheb_d);
   else
     orc_gs(L->n, L->A_rp, L->A_ci, L->A_v, L->invd, L->ncolors, L->color_off, L->color_order, x, b,
            steps);
@@ -612,6 +700,11 @@ static void upd_invd(olevel *L) {
   if (L->smoother == 5 || L->smoother == 6) orc_l1_invdiag(L->n, L->A_rp, L->A_v, L->invd);
   else if (L->smoother == 3) orc_spai0(L->n, L->A_rp, L->A_ci, L->A_v, L->invd);
   else orc_invdiag(L->n, L->A_rp, L->A_ci, L->A_v, L->invd);
+  if (L->smoother == 8) { /* update_smoother!(::ChebyshevSmoother), src/smoothers.jl:912-922 */
+    memcpy(L->tmp, L->cheb_v0, (size_t)L->n * sizeof(double));
+    double rho = orc_spectral_radius(L->n, L->A_rp, L->A_ci, L->A_v, L->invd, L->tmp, 10, L->r);
+    orc_cheb_coef(rho, L->cheb_degree, L->cheb_coef);
+  }
 }
 
 int orc_resetup(ohier *h, const double *v0, int64_t nnz0) {

@@ -48,7 +48,8 @@ class OLevel(C.Structure):
                 ("P_ci", P), ("P_v", P), ("T_off", P), ("T_rows", P), ("T_pnz", P),
                 ("smoother", i32), ("omega", f64), ("invd", P), ("ncolors", i32),
                 ("color_off", P), ("color_order", P), ("r", P), ("xc", P), ("bc", P),
-                ("tmp", P), ("nz_off", P), ("tpi", P), ("tai", P), ("tpj", P)]
+                ("tmp", P), ("nz_off", P), ("tpi", P), ("tai", P), ("tpj", P),
+                ("cheb_degree", i32), ("cheb_v0", P), ("cheb_coef", P), ("cheb_d", P)]
 
 
 class OHier(C.Structure):
@@ -64,6 +65,9 @@ def _declare(lib):
         "orc_invdiag": (None, [i32, P, P, P, P]),
         "orc_l1_invdiag": (None, [i32, P, P, P]),
         "orc_spai0": (None, [i32, P, P, P, P]),
+        "orc_spectral_radius": (f64, [i32, P, P, P, P, P, i32, P]),
+        "orc_cheb_coef": (None, [f64, i32, P]),
+        "orc_chebyshev": (None, [i32, P, P, P, P, P, i32, P, P, i32, P, P]),
         "orc_spai0_smooth": (None, [i32, P, P, P, P, P, P, i32, P]),
         "orc_jacobi": (None, [i32, P, P, P, P, f64, P, P, i32, P]),
         "orc_greedy_coloring": (i32, [i32, P, P, P]),
@@ -136,6 +140,32 @@ def spai0_smooth(n, rp, ci, v, m, x, b, steps):
     tmp = np.zeros(n)
     load().orc_spai0_smooth(n, ptr(rp), ptr(ci), ptr(v), ptr(np.ascontiguousarray(m, np.float64)), ptr(x),
                             ptr(np.ascontiguousarray(b, np.float64)), steps, ptr(tmp))
+    return x
+
+
+def spectral_radius(n, rp, ci, v, invd, v0, niter=10):
+    """Power-iteration estimate of the spectral radius of D^-1 A from the
+    normalised start vector v0 (_estimate_spectral_radius)."""
+    w = np.zeros(n)
+    vv = np.array(v0, dtype=np.float64)
+    return load().orc_spectral_radius(n, ptr(rp), ptr(ci), ptr(v), ptr(np.ascontiguousarray(invd, np.float64)),
+                                      ptr(vv), niter, ptr(w))
+
+
+def cheb_coef(rho, degree=3):
+    """Chebyshev coefficient table (1/theta, 0, scale_r, scale_d, ...)."""
+    c = np.zeros(2 * degree)
+    load().orc_cheb_coef(float(rho), degree, ptr(c))
+    return c
+
+
+def chebyshev(n, rp, ci, v, invd, coef, x, b, steps):
+    """`steps` Chebyshev applications (smooth!(::ChebyshevSmoother))."""
+    x = np.array(x, dtype=np.float64)
+    coef = np.ascontiguousarray(coef, np.float64)
+    r, d = np.zeros(n), np.zeros(n)
+    load().orc_chebyshev(n, ptr(rp), ptr(ci), ptr(v), ptr(np.ascontiguousarray(invd, np.float64)), ptr(coef),
+                         len(coef) // 2, ptr(x), ptr(np.ascontiguousarray(b, np.float64)), steps, ptr(r), ptr(d))
     return x
 
 
@@ -220,7 +250,8 @@ def strength_abs(n, rp, ci, v, theta):
 
 
 # ---------------------------------------------------------------- hierarchy mirror
-SMOOTHER_KIND = {0: "jacobi", 1: "colored_gs", 3: "spai0", 5: "l1_jacobi", 6: "l1_colored_gs"}
+SMOOTHER_KIND = {0: "jacobi", 1: "colored_gs", 3: "spai0", 5: "l1_jacobi", 6: "l1_colored_gs",
+                 8: "chebyshev"}
 
 
 class OracleHierarchy:
@@ -255,6 +286,11 @@ class OracleHierarchy:
             omega = float(h.export(l, "omega")[0])
             L = levels[l]
             L.n, L.nc, L.smoother, L.omega = n, nc, sk, omega
+            if sk == 8:
+                d.update(cheb_v0=h.export(l, "cheb_v0"), cheb_coef=h.export(l, "cheb_coef").copy(),
+                         cheb_d=np.zeros(n))
+                L.cheb_degree = len(d["cheb_coef"]) // 2
+                L.cheb_v0, L.cheb_coef, L.cheb_d = ptr(d["cheb_v0"]), ptr(d["cheb_coef"]), ptr(d["cheb_d"])
             L.ncolors = int(info[5])
             for k in ("A_rp", "A_ci", "A_v", "P_rp", "P_ci", "P_v", "T_off", "T_rows", "T_pnz",
                       "invd", "color_off", "color_order", "r", "xc", "bc", "tmp"):

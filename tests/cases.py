@@ -19,6 +19,8 @@ CASES = {
                             draugr.AMGConfig(coarsening=draugr.PMISCoarsening(
                                 0.25, draugr.StandardInterpolation()),
                                 smoother=draugr.SPAI0SmootherType())),
+    "hmis_chebyshev": (lambda: problems.heterogeneous_diffusion_3d(10, seed=7),
+                       draugr.AMGConfig(smoother=draugr.ChebyshevSmootherType())),
     "aniso27_hmis": (lambda: problems.anisotropic_27pt(9, 1e-3),
                      draugr.AMGConfig(coarsening=draugr.HMISCoarsening(
                          0.25, draugr.ExtendedIInterpolation(0.2)),

@@ -139,6 +139,10 @@ def test_structure_matches_oracle(host_case):
         if kind == 3:  # SPAI(0): m_i = a_ii / sum a_ij^2, swept with omega = 1
             inv = oracle.spai0(n, arp, aci, av)
             assert h.export(l, "omega")[0] == 1.0
+        elif kind == 8:  # Chebyshev: Jacobi diagonal, power iteration, coefficients
+            inv = oracle.invdiag(n, arp, aci, av)
+            rho = oracle.spectral_radius(n, arp, aci, av, inv, h.export(l, "cheb_v0"))
+            assert np.array_equal(oracle.cheb_coef(rho, 3), h.export(l, "cheb_coef"))
         else:
             inv = oracle.invdiag(n, arp, aci, av, l1=kind in (5, 6))
         assert np.array_equal(inv, h.export(l, "invdiag"))

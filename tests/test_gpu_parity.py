@@ -65,6 +65,8 @@ def test_level_kernels(case):
                 ref = oracle.jacobi(n, d["A_rp"], d["A_ci"], d["A_v"], d["invd"], L.omega, x, b, steps)
             elif L.smoother == 3:
                 ref = oracle.spai0_smooth(n, d["A_rp"], d["A_ci"], d["A_v"], d["invd"], x, b, steps)
+            elif L.smoother == 8:
+                ref = oracle.chebyshev(n, d["A_rp"], d["A_ci"], d["A_v"], d["invd"], d["cheb_coef"], x, b, steps)
             else:
                 ref = oracle.gs(n, d["A_rp"], d["A_ci"], d["A_v"], d["invd"], L.ncolors,
                                 d["color_off"], d["color_order"], x, b, steps)
@@ -164,6 +166,8 @@ def test_resetup_matches_reference_galerkin(case):
         ref = O.level_values(l)
         assert rel(dev, ref) < TOL64, f"level {l}"
         assert rel(h.export(l, "invdiag"), O.levels_np[l]["invd"]) < TOL64
+        if "cheb_coef" in O.levels_np[l]:  # spectral radius and coefficients redone on the device
+            assert rel(h.export(l, "cheb_coef"), O.levels_np[l]["cheb_coef"]) < TOL64
     nc = O.nc
     assert rel(h.export(-1, "C_dense"), O.dense) < TOL64
     # the resetup hierarchy solves the new system

@@ -136,6 +136,40 @@ def test_spai0_diagonal_smoothing_and_solve():
     assert np.linalg.norm(b - A @ x) / np.linalg.norm(b) < 1e-8
 
 
+def test_chebyshev_build_smoothing_solve_and_resetup():
+    """testsets "Chebyshev Smoother - Build / Smoothing / AMG Solve" and
+    "Chebyshev - Resetup" (test/runtests.jl:1913-1966): 0 < lambda_min <
+    lambda_max and degree 3; 5 applications reduce the residual; amg_solve!
+    with V(2,2) Chebyshev reaches 1e-8 in fewer than 200 cycles, also after
+    a resetup with the values doubled."""
+    A = problems.poisson1d(10)
+    n, rp, ci, v = parts(A)
+    inv = oracle.invdiag(n, rp, ci, v)
+    v0 = np.random.default_rng(3).standard_normal(n)
+    rho = oracle.spectral_radius(n, rp, ci, v, inv, v0 / np.linalg.norm(v0))
+    lmax, lmin = 1.1 * rho, 1.1 * rho / 30.0
+    assert lmax > lmin > 0
+    coef = oracle.cheb_coef(rho, 3)
+    assert len(coef) == 2 * 3 and np.isclose(coef[0], 2.0 / (lmax + lmin))
+    b = np.ones(n)
+    x = oracle.chebyshev(n, rp, ci, v, inv, coef, np.zeros(n), b, 5)
+    assert np.linalg.norm(b - A @ x) < np.linalg.norm(b)
+    for m in (10, 8):
+        A = problems.poisson2d(m)
+        N = m * m
+        b = np.random.default_rng(m).uniform(0, 1, N)
+        cfg = draugr.AMGConfig(smoother=draugr.ChebyshevSmootherType(), pre_smoothing_steps=2,
+                               post_smoothing_steps=2, max_coarse_size=10)
+        h = draugr.amg_setup(A, cfg, on_device=False)
+        O = oracle.OracleHierarchy(h, with_rmaps=True)
+        x, it, rel = O.solve(np.zeros(N), b, 2, 2, False, 1e-8, 200)
+        assert it < 200 and np.linalg.norm(b - A @ x) / np.linalg.norm(b) < 1e-8
+        if m == 8:
+            O.resetup(2.0 * A.data)
+            x, it, rel = O.solve(np.zeros(N), b, 2, 2, False, 1e-8, 200)
+            assert it < 200 and np.linalg.norm(b - 2.0 * (A @ x)) / np.linalg.norm(b) < 1e-8
+
+
 def test_coloring():
     """testsets "Graph Coloring" (:549-566) and "Colored GS Smoother" (:568-588)."""
     A = problems.poisson1d(10)
