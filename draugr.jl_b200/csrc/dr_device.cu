@@ -376,6 +376,8 @@ void DevHier::upload_csr(DevMat& M, int n, int m, const std::vector<int>& rp, co
   if (v) h2d(M.v, *v, st_);
   M.Ggs = pick_G(M.nnz, n);
   M.form = row_form(rp);
+  M.maxlen = 0;
+  for (int i = 0; i < n; ++i) M.maxlen = std::max(M.maxlen, rp[i + 1] - rp[i]);
   std::vector<int> base;
   std::vector<int> tiles = make_tiles(rp, ci, n, M.form.nt / M.form.G, base);
   std::vector<int> tstart(tiles.size());
@@ -1267,12 +1269,21 @@ int DevHier::pcg(double* x, const double* b, const CycleOpts& o, double tol, int
 // rows of up to 384 entries staged in shared memory (longer rows work in
 // place in global memory; a wider stage at lower occupancy measured slower
 // on the 128^3 27-point hierarchy).
+// The staged pattern capacity per warp is the smallest of 128, 256 and 384
+// entries that holds the output's longest row (longer rows search global
+// memory): 128 and 256 leave room for 8 blocks of 8 warps per SM (the
+// register limit), 384 for 5.
 void DevHier::spgemm(DevMat& O, const DevMat& S, const DevMat& B) {
-  constexpr int W = 8, CAP = 384;
+  constexpr int W = 8;
   counted();
   const int grid = std::max(1, std::min((O.n + W - 1) / W, max_grid_));
-  k_spgemm_warp<CAP, W><<<grid, W * 32, spgemm_smem_bytes<CAP, W>(), st_>>>(
-      O.n, O.rp, O.ci, O.v, S.rp, S.ci, S.v, B.rp, B.ci, B.v);
+#define DR_SPGEMM(CAP)                                                                      \
+  k_spgemm_warp<CAP, W><<<grid, W * 32, spgemm_smem_bytes<CAP, W>(), st_>>>(              \
+      O.n, O.rp, O.ci, O.v, S.rp, S.ci, S.v, B.rp, B.ci, B.v)
+  if (O.maxlen <= 128) DR_SPGEMM(128);
+  else if (O.maxlen <= 256) DR_SPGEMM(256);
+  else DR_SPGEMM(384);
+#undef DR_SPGEMM
   DR_CK(cudaGetLastError());
 }
 

@@ -95,6 +95,7 @@ struct DevMat {
   int* ts = nullptr;  // tile nonzero starts, ntiles+1
   int* tb = nullptr;       // tile smallest columns (-1: row too wide for offsets), ntiles
   uint16_t* cu = nullptr;  // columns as offsets from their tile's smallest column
+  int maxlen = 0;          // longest row
 };
 
 template <typename T>
