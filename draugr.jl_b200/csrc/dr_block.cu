@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstdio>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "dr_device.h"
@@ -103,21 +104,46 @@ struct Vec16<double> {
   __device__ static type make(const double* o) { return make_double2(o[0], o[1]); }
 };
 
+// Per-block partial sums of each column of a vector-layout kernel (TPR
+// threads per row, V consecutive columns per thread): every thread's V sums
+// go to shared memory, then thread c < k adds those of the threads owning
+// column c, in thread order, into part[block * 32 + c] (deterministic for
+// a given grid; k_bl_dot_final adds the blocks).
+template <int TPR, int V>
+__device__ __forceinline__ void block_col_partials(const double (&s)[V], int k, double* __restrict__ part) {
+  __shared__ double red[kBlock * V];
+#pragma unroll
+  for (int q = 0; q < V; ++q) red[threadIdx.x * V + q] = s[q];
+  __syncthreads();
+  const int c = threadIdx.x;
+  if (c < k) {
+    const int g = c / V, q = c % V;
+    double t = 0.0;
+    for (int u = g; u < kBlock; u += TPR) t += red[u * V + q];
+    part[(size_t)blockIdx.x * 32 + c] = t;
+  }
+}
+
+// With `part` (STORE mode), also the column partials of X_row . Y_row (the
+// p . q of block CG).
 template <typename TA, typename T, int MODE, int TPR>
 __global__ void __launch_bounds__(kBlock)
 k_spmm_vec(int nrows, int k, const int* __restrict__ rp, const int* __restrict__ ci,
            const TA* __restrict__ av, const T* __restrict__ X, const T* __restrict__ B,
-           const T* __restrict__ dinv, T omega, T* Y) {
+           const T* __restrict__ dinv, T omega, T* Y, double* __restrict__ part) {
   using VV = Vec16<T>;
   using VT = typename VV::type;
   constexpr int V = VV::V;
   constexpr int RPW = 32 / TPR;
   const int lane = threadIdx.x & 31;
   const int c0 = (lane % TPR) * V;  // first column of this thread
-  if (c0 >= k) return;              // no warp-wide operations below
+  const bool act = c0 < k;
+  double dsum[V];
+#pragma unroll
+  for (int q = 0; q < V; ++q) dsum[q] = 0.0;
   const long long w = (long long)blockIdx.x * kWarps + (threadIdx.x >> 5);
   const long long nw = (long long)gridDim.x * kWarps;
-  for (long long r = w * RPW + lane / TPR; r < nrows; r += nw * RPW) {
+  for (long long r = w * RPW + lane / TPR; act && r < nrows; r += nw * RPW) {
     const int row = (int)r;
     const int rs = rp[row], re = rp[row + 1];
     const size_t o = (size_t)row * k + c0;
@@ -156,7 +182,73 @@ k_spmm_vec(int nrows, int k, const int* __restrict__ rp, const int* __restrict__
       for (int q = 0; q < V; ++q) out[q] = acc[q];
     }
     *reinterpret_cast<VT*>(Y + o) = VV::make(out);
+    if (MODE == BM_STORE && part) {
+      T xo[V];
+      VV::get(*reinterpret_cast<const VT*>(X + o), xo);
+#pragma unroll
+      for (int q = 0; q < V; ++q) dsum[q] += (double)xo[q] * (double)out[q];
+    }
   }
+  if (MODE == BM_STORE && part) block_col_partials<TPR, V>(dsum, k, part);
+}
+
+// X += alpha_c P, R -= alpha_c Q, optionally R32 = (float) R, and the
+// column partials of R . R; vector layout (TPR threads per row, 2 columns
+// per thread).
+template <int TPR>
+__global__ void __launch_bounds__(kBlock)
+k_bl_update_vec(int n, int k, const double* __restrict__ alpha, double* __restrict__ X,
+                double* __restrict__ R, const double* __restrict__ P, const double* __restrict__ Q,
+                float* __restrict__ R32, double* __restrict__ part) {
+  constexpr int RPW = 32 / TPR;
+  const int lane = threadIdx.x & 31;
+  const int c0 = (lane % TPR) * 2;
+  const bool act = c0 < k;
+  double s[2] = {0.0, 0.0};
+  const double a0 = act ? alpha[c0] : 0.0, a1 = act ? alpha[c0 + 1] : 0.0;
+  const long long w = (long long)blockIdx.x * kWarps + (threadIdx.x >> 5);
+  const long long nw = (long long)gridDim.x * kWarps;
+  for (long long r = w * RPW + lane / TPR; act && r < n; r += nw * RPW) {
+    const size_t o = (size_t)r * k + c0;
+    double2 x = *reinterpret_cast<const double2*>(X + o);
+    double2 rr = *reinterpret_cast<const double2*>(R + o);
+    const double2 p = *reinterpret_cast<const double2*>(P + o);
+    const double2 q = *reinterpret_cast<const double2*>(Q + o);
+    x.x += a0 * p.x;
+    x.y += a1 * p.y;
+    rr.x = rr.x - a0 * q.x;
+    rr.y = rr.y - a1 * q.y;
+    *reinterpret_cast<double2*>(X + o) = x;
+    *reinterpret_cast<double2*>(R + o) = rr;
+    if (R32) *reinterpret_cast<float2*>(R32 + o) = make_float2((float)rr.x, (float)rr.y);
+    s[0] += rr.x * rr.x;
+    s[1] += rr.y * rr.y;
+  }
+  block_col_partials<TPR, 2>(s, k, part);
+}
+
+// Z = (double) z and the column partials of R . Z (the preconditioned
+// residual handed back to block CG); vector layout, 2 columns per thread.
+template <typename TS, int TPR>
+__global__ void __launch_bounds__(kBlock)
+k_bl_take_z(int n, int k, const TS* __restrict__ z, const double* __restrict__ R, double* __restrict__ Z,
+            double* __restrict__ part) {
+  constexpr int RPW = 32 / TPR;
+  const int lane = threadIdx.x & 31;
+  const int c0 = (lane % TPR) * 2;
+  const bool act = c0 < k;
+  double s[2] = {0.0, 0.0};
+  const long long w = (long long)blockIdx.x * kWarps + (threadIdx.x >> 5);
+  const long long nw = (long long)gridDim.x * kWarps;
+  for (long long r = w * RPW + lane / TPR; act && r < n; r += nw * RPW) {
+    const size_t o = (size_t)r * k + c0;
+    const double z0 = (double)z[o], z1 = (double)z[o + 1];
+    const double2 rr = *reinterpret_cast<const double2*>(R + o);
+    *reinterpret_cast<double2*>(Z + o) = make_double2(z0, z1);
+    s[0] += rr.x * z0;
+    s[1] += rr.y * z1;
+  }
+  block_col_partials<TPR, 2>(s, k, part);
 }
 
 template <typename T>
@@ -303,26 +395,41 @@ int warp_grid(int rows, int max_grid) {
 
 bool aligned16(const void* p) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
+// Threads per row for `per_row` vector pieces (a power of two up to 16).
+int tpr_for(int per_row) {
+  return per_row <= 1 ? 1 : per_row <= 2 ? 2 : per_row <= 4 ? 4 : per_row <= 8 ? 8 : 16;
+}
+
+// Blocks of the vector-layout kernels: 32 / tpr rows per warp.
+int vec_grid(int nrows, int tpr, int max_grid) {
+  const int rows_per_block = kWarps * (32 / tpr);
+  return std::max(1, std::min((nrows + rows_per_block - 1) / rows_per_block, max_grid));
+}
+
 // Block product on `nrows` rows: the vector-gather kernel when the rows'
-// k columns split into 16-byte pieces, else one warp per row.
+// k columns split into 16-byte pieces, else one warp per row.  With `part`
+// (STORE mode only) the vector kernel also leaves the column partials of
+// X_row . Y_row there; returns its grid (the number of partials per
+// column), or 0 when the one-warp-per-row kernel ran (no partials).
 template <typename TA, typename T, int MODE>
-void spmm(cudaStream_t st, int max_grid, int nrows, int k, const int* rp, const int* ci, const TA* av,
-          const T* X, const T* B, const T* dinv, T omega, T* Y) {
+int spmm(cudaStream_t st, int max_grid, int nrows, int k, const int* rp, const int* ci, const TA* av,
+         const T* X, const T* B, const T* dinv, T omega, T* Y, double* part = nullptr) {
   constexpr int V = Vec16<T>::V;
   if (k % V == 0 && aligned16(X) && aligned16(B) && aligned16(Y)) {
-    const int tpr = k / V <= 1 ? 1 : k / V <= 2 ? 2 : k / V <= 4 ? 4 : k / V <= 8 ? 8 : 16;
-    const int rows_per_block = kWarps * (32 / tpr);
-    const int grid = std::max(1, std::min((nrows + rows_per_block - 1) / rows_per_block, max_grid));
+    const int tpr = tpr_for(k / V);
+    const int grid = vec_grid(nrows, tpr, max_grid);
     switch (tpr) {
-      case 1: k_spmm_vec<TA, T, MODE, 1><<<grid, kBlock, 0, st>>>(nrows, k, rp, ci, av, X, B, dinv, omega, Y); break;
-      case 2: k_spmm_vec<TA, T, MODE, 2><<<grid, kBlock, 0, st>>>(nrows, k, rp, ci, av, X, B, dinv, omega, Y); break;
-      case 4: k_spmm_vec<TA, T, MODE, 4><<<grid, kBlock, 0, st>>>(nrows, k, rp, ci, av, X, B, dinv, omega, Y); break;
-      case 8: k_spmm_vec<TA, T, MODE, 8><<<grid, kBlock, 0, st>>>(nrows, k, rp, ci, av, X, B, dinv, omega, Y); break;
-      default: k_spmm_vec<TA, T, MODE, 16><<<grid, kBlock, 0, st>>>(nrows, k, rp, ci, av, X, B, dinv, omega, Y); break;
+#define DR_SPMM_VEC(t)                                                                                     \
+  case t:                                                                                                  \
+    k_spmm_vec<TA, T, MODE, t><<<grid, kBlock, 0, st>>>(nrows, k, rp, ci, av, X, B, dinv, omega, Y, part); \
+    break;
+      DR_SPMM_VEC(1) DR_SPMM_VEC(2) DR_SPMM_VEC(4) DR_SPMM_VEC(8) DR_SPMM_VEC(16)
+#undef DR_SPMM_VEC
     }
-    return;
+    return grid;
   }
   k_spmm<TA, T, MODE><<<warp_grid(nrows, max_grid), kBlock, 0, st>>>(nrows, k, rp, ci, av, X, B, dinv, omega, Y);
+  return 0;
 }
 
 }  // namespace
@@ -462,16 +569,64 @@ int DevHier::pcg_block(double* X, const double* B, int k, const CycleOpts& o, do
   auto fetch = [&](int slot) {
     DR_CK(cudaMemcpyAsync(hv + slot * 32, dv + slot * 32, k * sizeof(double), cudaMemcpyDeviceToHost, st_));
   };
-  auto precond = [&]() {  // Z = M R
-    if (mixed) {
-      note_launch();
-      k_bl_convert<double, float><<<vgrid, kBlock, 0, st_>>>(m, R, R32);
-      float* z = cycle_block<float>(0, bvecs<float>(0).x, R32, true, o, k);
-      note_launch();
-      k_bl_convert<float, double><<<vgrid, kBlock, 0, st_>>>(m, z, Z);
+  // Fused outer iteration (even k, 16-byte aligned vectors): p.q comes with
+  // Q = A P, r.r and the FP32 copy of R with the update, r.z with taking Z
+  // from the cycle; two columns per thread, column partials per block.
+  const bool fused = (k % 2 == 0) && aligned16(X) && aligned16(B);
+  const int tpr2 = tpr_for(k / 2);
+  const int g2 = vec_grid(n, tpr2, max_grid_);
+  auto dot_final = [&](int nblocks, double* dst) {
+    note_launch();
+    k_bl_dot_final<<<1, 1024, 0, st_>>>(nblocks, k, bpart_, dst);
+  };
+  auto update = [&](bool r32) {  // X += alpha P, R -= alpha Q, r.r -> dv[1]
+    note_launch();
+    if (fused) {
+      float* r32p = r32 ? R32 : nullptr;
+      switch (tpr2) {
+#define DR_UPD(t)                                                                             \
+  case t:                                                                                     \
+    k_bl_update_vec<t><<<g2, kBlock, 0, st_>>>(n, k, dv + 4 * 32, X, R, P, Q, r32p, bpart_); \
+    break;
+        DR_UPD(1) DR_UPD(2) DR_UPD(4) DR_UPD(8) DR_UPD(16)
+#undef DR_UPD
+      }
+      dot_final(g2, dv + 1 * 32);
     } else {
-      double* z = cycle_block<double>(0, bvecs<double>(0).x, R, true, o, k);
-      DR_CK(cudaMemcpyAsync(Z, z, (size_t)m * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+      k_bl_update<<<vgrid, kBlock, 0, st_>>>(n, k, dv + 4 * 32, X, R, P, Q, nullptr);
+      col_dots(n, k, R, R, dv + 1 * 32);
+    }
+  };
+  bool r32_ready = false;  // R32 already holds (float) R
+  auto take_z = [&](const auto* z) {  // Z = z, r.z -> dv[2]
+    using TZ = std::remove_const_t<std::remove_pointer_t<decltype(z)>>;
+    note_launch();
+    if (fused) {
+      switch (tpr2) {
+#define DR_TZ(t)                                                                   \
+  case t:                                                                          \
+    k_bl_take_z<TZ, t><<<g2, kBlock, 0, st_>>>(n, k, z, R, Z, bpart_);            \
+    break;
+        DR_TZ(1) DR_TZ(2) DR_TZ(4) DR_TZ(8) DR_TZ(16)
+#undef DR_TZ
+      }
+      dot_final(g2, dv + 2 * 32);
+    } else {
+      k_bl_convert<TZ, double><<<vgrid, kBlock, 0, st_>>>(m, z, Z);
+      col_dots(n, k, R, Z, dv + 2 * 32);
+    }
+  };
+  auto precond = [&]() {  // Z = M R, then r.z -> dv[2]
+    if (mixed) {
+      if (!r32_ready) {
+        note_launch();
+        k_bl_convert<double, float><<<vgrid, kBlock, 0, st_>>>(m, R, R32);
+      }
+      const float* z = cycle_block<float>(0, bvecs<float>(0).x, R32, true, o, k);
+      take_z(z);
+    } else {
+      const double* z = cycle_block<double>(0, bvecs<double>(0).x, R, true, o, k);
+      take_z(z);
     }
   };
   note_launch();
@@ -490,7 +645,6 @@ int DevHier::pcg_block(double* X, const double* B, int k, const CycleOpts& o, do
     nact += active[c];
   }
   precond();
-  col_dots(n, k, R, Z, dv + 2 * 32);
   fetch(2);
   DR_CK(cudaMemcpyAsync(P, Z, (size_t)m * sizeof(double), cudaMemcpyDeviceToDevice, st_));
   DR_CK(cudaStreamSynchronize(st_));
@@ -499,16 +653,16 @@ int DevHier::pcg_block(double* X, const double* B, int k, const CycleOpts& o, do
   while (nact > 0 && it < maxiter) {
     ++it;
     note_launch();
-    spmm<double, double, BM_STORE>(st_, max_grid_, n, k, A.rp, A.ci, A.v, P, nullptr, nullptr, 0.0,
-                                                               Q);
-    col_dots(n, k, P, Q, dv + 3 * 32);
+    const int gq = spmm<double, double, BM_STORE>(st_, max_grid_, n, k, A.rp, A.ci, A.v, P, nullptr, nullptr,
+                                                  0.0, Q, fused ? bpart_ : nullptr);
+    if (gq > 0 && fused) dot_final(gq, dv + 3 * 32);
+    else col_dots(n, k, P, Q, dv + 3 * 32);
     fetch(3);
     DR_CK(cudaStreamSynchronize(st_));
     for (int c = 0; c < k; ++c) hv[4 * 32 + c] = (active[c] && hv[96 + c] != 0.0) ? rz[c] / hv[96 + c] : 0.0;
     DR_CK(cudaMemcpyAsync(dv + 4 * 32, hv + 4 * 32, k * sizeof(double), cudaMemcpyHostToDevice, st_));
-    note_launch();
-    k_bl_update<<<vgrid, kBlock, 0, st_>>>(n, k, dv + 4 * 32, X, R, P, Q, nullptr);
-    col_dots(n, k, R, R, dv + 1 * 32);
+    update(mixed);
+    r32_ready = mixed && fused;
     fetch(1);
     DR_CK(cudaStreamSynchronize(st_));
     for (int c = 0; c < k; ++c)
@@ -522,7 +676,6 @@ int DevHier::pcg_block(double* X, const double* B, int k, const CycleOpts& o, do
     if (verbose >= 2) std::printf("  block PCG iter %4d: %d of %d columns active\n", it, nact, k);
     if (nact == 0) break;
     precond();
-    col_dots(n, k, R, Z, dv + 2 * 32);
     fetch(2);
     DR_CK(cudaStreamSynchronize(st_));
     for (int c = 0; c < k; ++c) {
