@@ -542,6 +542,59 @@ def pcg_batch(hierarchies, xs, bs, config: AMGConfig | None = None, tol: float =
         return list(ex.map(one, range(len(hierarchies))))
 
 
+class DraugrPreconditioner:
+    """One AMG cycle from a zero guess as a preconditioner, the role of
+    Draugr.jl's DraugrPreconditioner (src/preconditioner.jl:12-102).
+
+    update(A) builds the hierarchy on first use and resets it up (partial,
+    same pattern) afterwards, like preconditioner_update!; apply(x, y) /
+    ldiv(x, y) zero x and run one cycle for right-hand side y, like
+    preconditioner_apply! / ldiv!, on NumPy arrays or CUDA tensors (x is
+    updated in place and returned); nrows is preconditioner_nrows.
+    as_linear_operator() wraps apply for SciPy's Krylov solvers
+    (scipy.sparse.linalg.cg / gmres / bicgstab take it as M), the Python
+    counterpart of the LinearSolve.jl and Krylov.jl hooks."""
+
+    def __init__(self, config: AMGConfig | None = None, **kwargs):
+        self.config = config if config is not None else AMGConfig(**kwargs)
+        self.hierarchy: Hierarchy | None = None
+        self.dim: tuple[int, int] | None = None
+
+    def update(self, A):
+        if self.hierarchy is None:
+            self.hierarchy = amg_setup(A, self.config)
+        else:
+            amg_resetup(self.hierarchy, A, self.config)
+        self.dim = tuple(A.shape)
+        return self
+
+    def apply(self, x, y):
+        if self.hierarchy is None:
+            raise _lib.DraugrError("preconditioner applied before update(A)")
+        if _is_device(x):
+            x.zero_()
+        else:
+            x[:] = 0.0
+        return amg_cycle(x, y, self.hierarchy, self.config)
+
+    ldiv = apply
+
+    @property
+    def nrows(self) -> int:
+        return 0 if self.dim is None else self.dim[0]
+
+    def as_linear_operator(self):
+        import scipy.sparse.linalg as spla
+
+        n = self.nrows
+
+        def mv(y):
+            y = np.ascontiguousarray(np.asarray(y, dtype=np.float64).reshape(-1))
+            return self.apply(np.empty(n), y)
+
+        return spla.LinearOperator((n, n), matvec=mv, dtype=np.float64)
+
+
 def _check_vec(x, b, h):
     for name, a in (("x", x), ("b", b)):
         if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous):

@@ -205,3 +205,12 @@ def test_setup_seed_determinism():
 def test_check_raises():
     with pytest.raises(draugr.DraugrError):
         check(-1, "x")
+
+
+def test_preconditioner_before_update():
+    """DraugrPreconditioner keeps the reference's lifecycle: no hierarchy
+    (nrows 0) until update(A), and applying it before then is an error."""
+    P = draugr.DraugrPreconditioner(smoother=draugr.L1JacobiSmootherType())
+    assert P.nrows == 0 and P.hierarchy is None
+    with pytest.raises(draugr.DraugrError):
+        P.apply(np.zeros(4), np.ones(4))
