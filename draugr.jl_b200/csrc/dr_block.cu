@@ -314,6 +314,62 @@ __global__ void k_bl_lu(int n, int k, const double* __restrict__ lu_g, const int
   for (int i = 0; i < n; ++i) X[(size_t)i * k + c] = (T)y[(size_t)i * k];
 }
 
+// The same solve with one warp per column for n <= 64: the factors in
+// shared memory (n * n doubles), each lane holding y_i for i = lane and
+// lane + 32 in registers; at step j the lane owning y_j hands it to the
+// others by shuffle.  Every y_i sees the same operations in the same order
+// as in k_bl_lu (bit-identical results); the n steps of each substitution
+// cost a shuffle and one update per lane instead of a sequential sweep.
+template <typename T>
+__global__ void __launch_bounds__(1024)
+k_bl_lu_warp(int n, int k, const double* __restrict__ lu_g, const int* __restrict__ piv,
+             const T* __restrict__ B, T* __restrict__ X) {
+  extern __shared__ double lsm[];  // n * n factors, then n per warp (the pivoted column)
+  double* lu = lsm;
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) lu[e] = lu_g[e];
+  __syncthreads();
+  const int c = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (c >= k) return;  // whole warps leave; no block barrier follows
+  double* ys = lsm + (size_t)n * n + (size_t)c * n;
+  for (int i = lane; i < n; i += 32) ys[i] = (double)B[(size_t)i * k + c];
+  __syncwarp();
+  if (lane == 0)
+    for (int j = 0; j < n; ++j) {
+      const int p = piv[j];
+      if (p != j) {
+        const double t = ys[j];
+        ys[j] = ys[p];
+        ys[p] = t;
+      }
+    }
+  __syncwarp();
+  double y0 = lane < n ? ys[lane] : 0.0, y1 = lane + 32 < n ? ys[lane + 32] : 0.0;
+  for (int j = 0; j < n; ++j) {  // L y = b (unit diagonal)
+    const double yj = __shfl_sync(0xffffffffu, j < 32 ? y0 : y1, j & 31);
+    if (yj != 0.0) {
+      if (lane > j && lane < n) y0 = __dsub_rn(y0, __dmul_rn(yj, lu[(size_t)j * n + lane]));
+      if (lane + 32 > j && lane + 32 < n) y1 = __dsub_rn(y1, __dmul_rn(yj, lu[(size_t)j * n + lane + 32]));
+    }
+  }
+  for (int j = n - 1; j >= 0; --j) {  // U x = y
+    const double d = lu[(size_t)j * n + j];
+    if (lane == (j & 31)) {
+      if (j < 32) {
+        if (y0 != 0.0) y0 = __ddiv_rn(y0, d);
+      } else if (y1 != 0.0) {
+        y1 = __ddiv_rn(y1, d);
+      }
+    }
+    const double yj = __shfl_sync(0xffffffffu, j < 32 ? y0 : y1, j & 31);
+    if (yj != 0.0) {
+      if (lane < j) y0 = __dsub_rn(y0, __dmul_rn(yj, lu[(size_t)j * n + lane]));
+      if (lane + 32 < j) y1 = __dsub_rn(y1, __dmul_rn(yj, lu[(size_t)j * n + lane + 32]));
+    }
+  }
+  if (lane < n) X[(size_t)lane * k + c] = (T)y0;
+  if (lane + 32 < n) X[(size_t)(lane + 32) * k + c] = (T)y1;
+}
+
 // Column dot products a_c . b_c: per-block partials part[block][c]
 // (warps take rows, lane c accumulates column c, warps summed in order).
 __global__ void __launch_bounds__(kBlock)
@@ -519,17 +575,22 @@ T* DevHier::cycle_block(int l, T* X, const T* B, bool x_zero, const CycleOpts& o
   } else {
     xc = sizeof(T) == 8 ? (T*)bcx64_ : (T*)bcx32_;
     note_launch();
-    size_t smem = (size_t)nc_ * k * sizeof(double);
-    int optin = 0;
-    DR_CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_));
-    if (smem > (size_t)optin) fail("block solves: the coarsest system is too large for one block");
-    // the factors too, when they fit beside the vectors
-    const size_t with_lu = smem + (size_t)nc_ * nc_ * sizeof(double);
-    const int stage = with_lu <= (size_t)optin ? 1 : 0;
-    if (stage) smem = with_lu;
-    if (smem > 48 * 1024)
-      DR_CK(cudaFuncSetAttribute(k_bl_lu<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_bl_lu<T><<<1, 32, smem, st_>>>(nc_, k, clu_, cpiv_, bc, xc, stage);
+    if (nc_ <= 64) {
+      const size_t wsm = ((size_t)nc_ * nc_ + (size_t)k * nc_) * sizeof(double);  // <= 48 KB
+      k_bl_lu_warp<T><<<1, 32 * k, wsm, st_>>>(nc_, k, clu_, cpiv_, bc, xc);
+    } else {
+      size_t smem = (size_t)nc_ * k * sizeof(double);
+      int optin = 0;
+      DR_CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_));
+      if (smem > (size_t)optin) fail("block solves: the coarsest system is too large for one block");
+      // the factors too, when they fit beside the vectors
+      const size_t with_lu = smem + (size_t)nc_ * nc_ * sizeof(double);
+      const int stage = with_lu <= (size_t)optin ? 1 : 0;
+      if (stage) smem = with_lu;
+      if (smem > 48 * 1024)
+        DR_CK(cudaFuncSetAttribute(k_bl_lu<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_bl_lu<T><<<1, 32, smem, st_>>>(nc_, k, clu_, cpiv_, bc, xc, stage);
+    }
   }
   const DevMat& P = L.P;
   note_launch();

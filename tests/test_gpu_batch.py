@@ -5,6 +5,8 @@ hierarchy and CUDA stream, solved concurrently from a pool of host threads
 hierarchy, so the concurrent results must equal the same solves run one
 at a time, bit for bit, and reach 1e-8 (FP64-verified)."""
 
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -43,14 +45,17 @@ def test_concurrent_solves_equal_sequential_ones():
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-@pytest.mark.parametrize("side,k", [(20, 5), (24, 32), (16, 1)])
-def test_block_pcg_matches_single_solves(side, k, precision):
+@pytest.mark.parametrize("side,k,coarse", [(20, 5, 50), (24, 32, 50), (16, 1, 50), (18, 32, 300)])
+def test_block_pcg_matches_single_solves(side, k, coarse, precision):
     """Many right-hand sides of one matrix (the C3 96^3 x 32 case, reduced):
     block PCG, one pass over each level matrix for all k columns, against
-    k single-right-hand-side PCG solves."""
+    k single-right-hand-side PCG solves.  Odd k takes the unfused outer
+    iteration and one warp per row; max_coarse_size 300 gives a coarsest
+    system of more than 64 unknowns (the one-thread-per-column solve)."""
     A = problems.poisson3d(side)
     n = A.shape[0]
     cfg = draugr.hypre_default_config(agg_trunc_factor=0.2, smoother=draugr.L1JacobiSmootherType(), seed=6)
+    cfg = dataclasses.replace(cfg, max_coarse_size=coarse)
     h = draugr.amg_setup(A, cfg)
     rng = np.random.default_rng(side + k)
     Bn = rng.uniform(-1, 1, (n, k))
