@@ -16,8 +16,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <mutex>
 #include <string>
 #include <type_traits>
+#include <unordered_map>
 #include <vector>
 
 #include "dr_device.h"
@@ -136,35 +138,59 @@ k_spmm_vec(int nrows, int k, const int* __restrict__ rp, const int* __restrict__
   constexpr int V = VV::V;
   constexpr int RPW = 32 / TPR;
   const int lane = threadIdx.x & 31;
-  const int c0 = (lane % TPR) * V;  // first column of this thread
+  const int sub = lane % TPR;
+  const int c0 = sub * V;           // first column of this thread
   const bool act = c0 < k;
+  const int cg = act ? c0 : k - V;  // lanes past k read (and drop) the last piece
+  // the TPR lanes of one row (a row's lanes always run together)
+  const unsigned gmask = TPR == 32 ? 0xffffffffu : (((1u << TPR) - 1u) << (lane & ~(TPR - 1)));
   double dsum[V];
 #pragma unroll
   for (int q = 0; q < V; ++q) dsum[q] = 0.0;
   const long long w = (long long)blockIdx.x * kWarps + (threadIdx.x >> 5);
   const long long nw = (long long)gridDim.x * kWarps;
-  for (long long r = w * RPW + lane / TPR; act && r < nrows; r += nw * RPW) {
+  for (long long r = w * RPW + lane / TPR; r < nrows; r += nw * RPW) {
     const int row = (int)r;
     const int rs = rp[row], re = rp[row + 1];
-    const size_t o = (size_t)row * k + c0;
+    const size_t o = (size_t)row * k + cg;
     T acc[V];
     if (MODE == BM_ADDTO) VV::get(*reinterpret_cast<const VT*>(Y + o), acc);
     else if (MODE == BM_JACOBI) VV::get(*reinterpret_cast<const VT*>(B + o), acc);
     else
 #pragma unroll
       for (int q = 0; q < V; ++q) acc[q] = T(0);
-#pragma unroll 4
-    for (int e = rs; e < re; ++e) {
-      const int c = ci[e];
-      const T v = (T)av[e];
-      T xv[V];
-      VV::get(*reinterpret_cast<const VT*>(X + (size_t)c * k + c0), xv);
+    // the row's lanes load up to TPR (column, value) pairs at once and pass
+    // them round; the X pieces of 4 entries are gathered before the first
+    // is used (slots past the row's end repeat its last entry)
+    for (int k0 = rs; k0 < re; k0 += TPR) {
+      const int my = k0 + sub;
+      const int cj = my < re ? ci[my] : 0;
+      const T vj = my < re ? (T)av[my] : T(0);
+      const int cnt = min(TPR, re - k0);
+      for (int j0 = 0; j0 < cnt; j0 += 4) {
+        T vv[4];
+        VT xs[4];
 #pragma unroll
-      for (int q = 0; q < V; ++q) {
-        const T p = rn_mul(v, xv[q]);
-        acc[q] = (MODE == BM_JACOBI) ? rn_sub(acc[q], p) : rn_add(acc[q], p);
+        for (int u = 0; u < 4; ++u) {
+          const int jj = min(j0 + u, cnt - 1);
+          const int c = __shfl_sync(gmask, cj, jj, TPR);
+          vv[u] = __shfl_sync(gmask, vj, jj, TPR);
+          xs[u] = *reinterpret_cast<const VT*>(X + (size_t)c * k + cg);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (j0 + u < cnt) {
+            T xv[V];
+            VV::get(xs[u], xv);
+#pragma unroll
+            for (int q = 0; q < V; ++q) {
+              const T p = rn_mul(vv[u], xv[q]);
+              acc[q] = (MODE == BM_JACOBI) ? rn_sub(acc[q], p) : rn_add(acc[q], p);
+            }
+          }
       }
     }
+    if (!act) continue;
     T out[V];
     if (MODE == BM_RESID) {
       T bv[V];
@@ -456,10 +482,28 @@ int tpr_for(int per_row) {
   return per_row <= 1 ? 1 : per_row <= 2 ? 2 : per_row <= 4 ? 4 : per_row <= 8 ? 8 : 16;
 }
 
-// Blocks of the vector-layout kernels: 32 / tpr rows per warp.
-int vec_grid(int nrows, int tpr, int max_grid) {
+// Blocks of a vector-layout kernel f (32 / tpr rows per warp): enough for
+// the rows, at most one wave of resident blocks (max_grid allows 8 blocks
+// of 256 threads per SM; registers may allow fewer, queried once per
+// kernel).
+int vec_grid(const void* f, int nrows, int tpr, int max_grid) {
+  static std::mutex mu;
+  static std::unordered_map<const void*, int> occ;
+  int nb;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = occ.find(f);
+    if (it == occ.end()) {
+      nb = 0;
+      DR_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, f, kBlock, 0));
+      nb = std::max(1, std::min(nb, 8));
+      occ.emplace(f, nb);
+    } else {
+      nb = it->second;
+    }
+  }
   const int rows_per_block = kWarps * (32 / tpr);
-  return std::max(1, std::min((nrows + rows_per_block - 1) / rows_per_block, max_grid));
+  return std::max(1, std::min((nrows + rows_per_block - 1) / rows_per_block, max_grid / 8 * nb));
 }
 
 // Block product on `nrows` rows: the vector-gather kernel when the rows'
@@ -473,12 +517,15 @@ int spmm(cudaStream_t st, int max_grid, int nrows, int k, const int* rp, const i
   constexpr int V = Vec16<T>::V;
   if (k % V == 0 && aligned16(X) && aligned16(B) && aligned16(Y)) {
     const int tpr = tpr_for(k / V);
-    const int grid = vec_grid(nrows, tpr, max_grid);
+    int grid = 1;
     switch (tpr) {
-#define DR_SPMM_VEC(t)                                                                                     \
-  case t:                                                                                                  \
-    k_spmm_vec<TA, T, MODE, t><<<grid, kBlock, 0, st>>>(nrows, k, rp, ci, av, X, B, dinv, omega, Y, part); \
-    break;
+#define DR_SPMM_VEC(t)                                                                            \
+  case t: {                                                                                       \
+    auto kf = k_spmm_vec<TA, T, MODE, t>;                                                         \
+    grid = vec_grid((const void*)kf, nrows, t, max_grid);                                         \
+    kf<<<grid, kBlock, 0, st>>>(nrows, k, rp, ci, av, X, B, dinv, omega, Y, part);                \
+    break;                                                                                        \
+  }
       DR_SPMM_VEC(1) DR_SPMM_VEC(2) DR_SPMM_VEC(4) DR_SPMM_VEC(8) DR_SPMM_VEC(16)
 #undef DR_SPMM_VEC
     }
@@ -635,7 +682,7 @@ int DevHier::pcg_block(double* X, const double* B, int k, const CycleOpts& o, do
   // from the cycle; two columns per thread, column partials per block.
   const bool fused = (k % 2 == 0) && aligned16(X) && aligned16(B);
   const int tpr2 = tpr_for(k / 2);
-  const int g2 = vec_grid(n, tpr2, max_grid_);
+  const int g2 = vec_grid((const void*)k_bl_update_vec<16>, n, tpr2, max_grid_);
   auto dot_final = [&](int nblocks, double* dst) {
     note_launch();
     k_bl_dot_final<<<1, 1024, 0, st_>>>(nblocks, k, bpart_, dst);
