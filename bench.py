@@ -195,12 +195,15 @@ def dist_init(args):
 
 
 def max_over_ranks(v, world):
+    """The largest of every rank's v (a device tensor under NCCL, a host one
+    under gloo)."""
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
