@@ -366,12 +366,19 @@ int64_t draugr_b200_export(int32_t handle, int32_t lvl, const char* what, void* 
       else if (w == "omega") { tmpd.assign(1, L.omega); dv = &tmpd; }
       else if (w == "cheb_coef") dv = &L.cheb_coef;
       else if (w == "cheb_v0") dv = &L.cheb_v0;
+      else if (w == "ilu_L") dv = &L.ilu_L;
+      else if (w == "ilu_U") dv = &L.ilu_U;
+      else if (w == "ilu_diag") iv = &L.ilu_diag;
+      else if (w == "ilu_fwd_order") iv = &L.ilu_fwd_order;
+      else if (w == "ilu_fwd_offsets") iv = &L.ilu_fwd_off;
+      else if (w == "ilu_bwd_order") iv = &L.ilu_bwd_order;
+      else if (w == "ilu_bwd_offsets") iv = &L.ilu_bwd_off;
       else if (w == "AP_nzval") {
         if (!H->dev) fail("AP_nzval lives on the device only");
         dv = &tmpd;
       }
       if (dv && H->dev && w != "P_nzval" && w != "R_nzval" && w != "omega" && w != "cheb_v0" &&
-          !(w == "cheb_coef" && L.cheb_coef.empty())) {
+          !(w == "cheb_coef" && L.cheb_coef.empty()) && !((w == "ilu_L" || w == "ilu_U") && L.ilu_L.empty())) {
         H->dev->export_values(lvl, w, tmpd);
         dv = &tmpd;
       }

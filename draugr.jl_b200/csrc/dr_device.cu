@@ -21,6 +21,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <unordered_map>
 
 #include "dr_device.h"
@@ -311,6 +312,24 @@ DevHier::DevHier(const HostHierarchy& H, int device) {
       }
       d.v64.xb = alloc<double>(n);
       d.v64.r = alloc<double>(n);
+      if (h.smoother == SmootherKind::ILU0 || h.smoother == SmootherKind::SerialILU0) {
+        d.ilu_diag = alloc<int>(n);
+        h2d(d.ilu_diag, h.ilu_diag, st_);
+        d.ilu_L = alloc<double>(h.A.v.size() + 4);
+        d.ilu_U = alloc<double>(h.A.v.size() + 4);
+        h2d(d.ilu_L, h.ilu_L, st_);
+        h2d(d.ilu_U, h.ilu_U, st_);
+        d.ilu_fwd = alloc<int>(n);
+        d.ilu_bwd = alloc<int>(n);
+        h2d(d.ilu_fwd, h.ilu_fwd_order, st_);
+        h2d(d.ilu_bwd, h.ilu_bwd_order, st_);
+        d.ilu_fwd_off = h.ilu_fwd_off;
+        d.ilu_bwd_off = h.ilu_bwd_off;
+        d.ilu_rp = h.A.rp;
+        d.ilu_ci = h.A.ci;
+        d.ilu_diag_h = h.ilu_diag;
+        d.v64.d = alloc<double>(n);
+      }
       if (h.smoother == SmootherKind::Chebyshev) {
         d.cheb_degree = h.cheb_degree;
         d.cheb_v0 = alloc<double>(n);
@@ -464,6 +483,11 @@ void DevHier::ensure_fp32() {
     d.v32.b = alloc<float>(n);
     d.v32.r = alloc<float>(n);
     if (d.smoother == SmootherKind::Chebyshev) d.v32.d = alloc<float>(n);
+    if (d.ilu_L) {
+      d.v32.d = alloc<float>(n);
+      d.ilu_L32 = alloc<float>(d.A.nnz + 4);
+      d.ilu_U32 = alloc<float>(d.A.nnz + 4);
+    }
   }
   cb32_ = alloc<float>(nc_);
   cx32_ = alloc<float>(nc_);
@@ -683,6 +707,12 @@ void DevHier::refresh_fp32() {
     k_convert<double, float><<<grid1d(d.R.nnz, max_grid_), kBlock, 0, st_>>>(d.R.nnz, d.R.v, d.R.v32);
     counted();
     k_convert<double, float><<<grid1d(d.A.n, max_grid_), kBlock, 0, st_>>>(d.A.n, d.invd, d.invd32);
+    if (d.ilu_L32) {
+      counted();
+      k_convert<double, float><<<grid1d(d.A.nnz, max_grid_), kBlock, 0, st_>>>(d.A.nnz, d.ilu_L, d.ilu_L32);
+      counted();
+      k_convert<double, float><<<grid1d(d.A.nnz, max_grid_), kBlock, 0, st_>>>(d.A.nnz, d.ilu_U, d.ilu_U32);
+    }
   }
   DR_CK(cudaGetLastError());
 }
@@ -710,6 +740,30 @@ T* DevHier::smooth(int l, T* x, const T* b, int steps, T* ext, const double* rz_
                     EpJacobi<T>{x, b, invd<T>(L), dst, om, nullptr});
       }
       x = dst;
+    }
+  } else if (L.ilu_L) {
+    // ILU(0): dx = (LU)^-1 (b - A x) by the two level schedules, x += dx
+    // (in place)
+    T* t = V.d;
+    const T* Lv = std::is_same<T, float>::value ? (const T*)L.ilu_L32 : (const T*)L.ilu_L;
+    const T* Uv = std::is_same<T, float>::value ? (const T*)L.ilu_U32 : (const T*)L.ilu_U;
+    for (int s = 0; s < steps; ++s) {
+      residual<T>(l, x, b, t, nullptr);
+      for (size_t v = 0; v + 1 < L.ilu_fwd_off.size(); ++v) {
+        const int off = L.ilu_fwd_off[v], cnt = L.ilu_fwd_off[v + 1] - off;
+        counted();
+        k_ilu_fwd<T><<<grid1d(cnt, max_grid_), kBlock, 0, st_>>>(cnt, L.ilu_fwd + off, A.rp, A.ci, L.ilu_diag,
+                                                                Lv, t);
+      }
+      for (size_t v = 0; v + 1 < L.ilu_bwd_off.size(); ++v) {
+        const int off = L.ilu_bwd_off[v], cnt = L.ilu_bwd_off[v + 1] - off;
+        counted();
+        k_ilu_bwd<T><<<grid1d(cnt, max_grid_), kBlock, 0, st_>>>(cnt, L.ilu_bwd + off, A.rp, A.ci, L.ilu_diag,
+                                                                Uv, t);
+      }
+      counted();
+      k_ilu_apply<T><<<grid1d(A.n, max_grid_), kBlock, 0, st_>>>(A.n, t, x);
+      DR_CK(cudaGetLastError());
     }
   } else if (L.smoother == SmootherKind::Chebyshev) {
     // each application: `cheb_degree` fused residual-and-update steps, the
@@ -1307,6 +1361,23 @@ void DevHier::resetup_values(const double* v_dev) {
     else
       k_invdiag<<<grid1d(d.A.n, max_grid_), kBlock, 0, st_>>>(d.A.n, d.A.rp, d.A.ci, d.A.v, d.invd);
     DR_CK(cudaGetLastError());
+    if (d.ilu_L) {
+      // update_smoother!(::ILU0Smoother / ::SerialILU0Smoother), src/
+      // smoothers.jl:1332-1337: the factorisation is sequential, so it runs
+      // on the host from the level's new values, as in the reference
+      CSR a;
+      a.n = a.m = d.A.n;
+      a.rp = d.ilu_rp;
+      a.ci = d.ilu_ci;
+      a.v.resize(d.A.nnz);
+      DR_CK(cudaMemcpyAsync(a.v.data(), d.A.v, (size_t)d.A.nnz * sizeof(double), cudaMemcpyDeviceToHost, st_));
+      DR_CK(cudaStreamSynchronize(st_));
+      std::vector<double> Lh, Uh;
+      ilu0_factorize(a, d.ilu_diag_h, Lh, Uh);
+      h2d(d.ilu_L, Lh, st_);
+      h2d(d.ilu_U, Uh, st_);
+      DR_CK(cudaStreamSynchronize(st_));  // Lh, Uh leave scope
+    }
     if (d.smoother == SmootherKind::Chebyshev) {
       // update_smoother!(::ChebyshevSmoother): the spectral radius of D^-1 A
       // again (10 power steps from the stored start vector, on the device),
@@ -1541,6 +1612,8 @@ void DevHier::export_values(int lvl, const std::string& what, std::vector<double
     else if (what == "P_nzval") { src = d.P.v; n = d.P.nnz; }
     else if (what == "invdiag") { src = d.invd; n = d.A.n; }
     else if (what == "cheb_coef" && d.cheb_coef) { src = d.cheb_coef; n = 2LL * d.cheb_degree; }
+    else if (what == "ilu_L" && d.ilu_L) { src = d.ilu_L; n = d.A.nnz; }
+    else if (what == "ilu_U" && d.ilu_U) { src = d.ilu_U; n = d.A.nnz; }
     else if (what == "AP_nzval" && d.has_rap) { src = d.AP.v; n = d.AP.nnz; }
   }
   if (!src) fail("unknown device export: " + what);

@@ -127,6 +127,15 @@ struct DevLevel {
   int cheb_degree = 0;
   double* cheb_v0 = nullptr;
   double* cheb_coef = nullptr;
+  // ILU(0): diagonal positions, factors (FP64; FP32 after the first mixed
+  // use), the substitution schedules (rows by level on the device, level
+  // offsets on the host) and the host pattern for refactorising after a
+  // resetup
+  int* ilu_diag = nullptr;
+  double *ilu_L = nullptr, *ilu_U = nullptr;
+  float *ilu_L32 = nullptr, *ilu_U32 = nullptr;
+  int *ilu_fwd = nullptr, *ilu_bwd = nullptr;
+  std::vector<int> ilu_fwd_off, ilu_bwd_off, ilu_rp, ilu_ci, ilu_diag_h;
   LevelVecs<double> v64;
   LevelVecs<float> v32;
 };

@@ -382,6 +382,100 @@ void coarsen_with_fallback(const CSR& A, const Coarsening& alg, const Config& cf
   }
 }
 
+}  // namespace
+
+void ilu0_diag_indices(const CSR& A, std::vector<int>& diag) {
+  diag.assign(A.n, -1);
+  for (int i = 0; i < A.n; ++i) {
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
+      if (A.ci[k] == i) {
+        diag[i] = k;
+        break;
+      }
+    if (diag[i] < 0) fail("ILU(0) needs a diagonal entry in every row (row " + std::to_string(i) + ")");
+  }
+}
+
+void ilu0_factorize(const CSR& A, const std::vector<int>& diag, std::vector<double>& L,
+                    std::vector<double>& U) {
+  const int n = A.n;
+  U = A.v;
+  L.assign(A.v.size(), 0.0);
+  const double kMaxFactor = 1e8;
+  std::vector<double> rn(n);
+  for (int i = 0; i < n; ++i) {
+    double s = 0.0;
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) s += std::fabs(A.v[k]);
+    rn[i] = s;
+  }
+  auto safe = [&](double scale) { return kEps * std::max(1.0, scale); };
+  for (int i = 0; i < n; ++i) {
+    const int rs = A.rp[i], re = A.rp[i + 1];
+    for (int nz = rs; nz < diag[i]; ++nz) {
+      const int k = A.ci[nz];
+      const double ukk = U[diag[k]];
+      if (std::fabs(ukk) < safe(rn[k])) {
+        L[nz] = 0.0;
+        U[nz] = 0.0;
+        continue;
+      }
+      double lik = U[nz] / ukk;
+      const double nl = std::fabs(lik);
+      if (nl > kMaxFactor) lik = lik * (kMaxFactor / nl);
+      L[nz] = lik;
+      U[nz] = 0.0;
+      for (int nk = diag[k] + 1; nk < A.rp[k + 1]; ++nk) {
+        const int j = A.ci[nk];
+        // binary search of column j in row i (_find_nz_in_row)
+        int lo = rs, hi = re - 1, at = -1;
+        while (lo <= hi) {
+          const int mid = (lo + hi) >> 1;
+          const int c = A.ci[mid];
+          if (c == j) { at = mid; break; }
+          if (c < j) lo = mid + 1;
+          else hi = mid - 1;
+        }
+        if (at >= 0) U[at] -= lik * U[nk];
+      }
+    }
+    const double thr = safe(rn[i]);
+    if (std::fabs(U[diag[i]]) < thr) U[diag[i]] = thr;
+  }
+}
+
+void ilu0_levels(const CSR& A, const std::vector<int>& diag, std::vector<int>& fwd_order,
+                 std::vector<int>& fwd_off, std::vector<int>& bwd_order, std::vector<int>& bwd_off) {
+  const int n = A.n;
+  auto order_by = [&](const std::vector<int>& level, int nlev, std::vector<int>& order,
+                      std::vector<int>& off) {
+    off.assign(nlev + 1, 0);
+    for (int i = 0; i < n; ++i) ++off[level[i]];  // levels are 1-based
+    for (int c = 0; c < nlev; ++c) off[c + 1] += off[c];
+    std::vector<int> pos(off.begin(), off.end() - 1);
+    order.resize(n);
+    for (int i = 0; i < n; ++i) order[pos[level[i] - 1]++] = i;
+  };
+  std::vector<int> lev(n);
+  int nf = 0;
+  for (int i = 0; i < n; ++i) {
+    int m = 0;
+    for (int nz = A.rp[i]; nz < diag[i]; ++nz) m = std::max(m, lev[A.ci[nz]]);
+    lev[i] = m + 1;
+    nf = std::max(nf, lev[i]);
+  }
+  order_by(lev, nf, fwd_order, fwd_off);
+  int nb = 0;
+  for (int i = n - 1; i >= 0; --i) {
+    int m = 0;
+    for (int nz = diag[i] + 1; nz < A.rp[i + 1]; ++nz) m = std::max(m, lev[A.ci[nz]]);
+    lev[i] = m + 1;
+    nb = std::max(nb, lev[i]);
+  }
+  order_by(lev, nb, bwd_order, bwd_off);
+}
+
+namespace {
+
 // Normalised start vector of the Chebyshev power iteration: standard normal
 // entries (Box-Muller on splitmix64 uniforms), divided by their 2-norm.
 std::vector<double> chebyshev_start(int n, uint64_t seed) {
@@ -414,6 +508,16 @@ void build_smoother(HostLevel& L, const Config& cfg, int level) {
       spai0_diagonal(L.A, L.invdiag);
       L.omega = 1.0;
       break;
+    case SmootherKind::ILU0:
+    case SmootherKind::SerialILU0:
+      // build_ilu0_smoother / build_serial_ilu0_smoother (smoothers.jl:1112-1126,
+      // :1309-1330): the same factors; both substitute row by row in column
+      // order, which the level schedule reproduces exactly
+      ilu0_diag_indices(L.A, L.ilu_diag);
+      ilu0_levels(L.A, L.ilu_diag, L.ilu_fwd_order, L.ilu_fwd_off, L.ilu_bwd_order, L.ilu_bwd_off);
+      ilu0_factorize(L.A, L.ilu_diag, L.ilu_L, L.ilu_U);
+      inverse_diagonal(L.A, L.invdiag);  // not used by the sweep; kept for exports
+      break;
     case SmootherKind::Chebyshev: {  // build_chebyshev_smoother, smoothers.jl:895-910 (degree 3)
       inverse_diagonal(L.A, L.invdiag);
       L.cheb_degree = 3;
@@ -436,7 +540,7 @@ void build_smoother(HostLevel& L, const Config& cfg, int level) {
     default:
       fail("smoother \"" + smoother_name(cfg.smoother) +
            "\" is not supported by the B200 build (use jacobi, l1_jacobi, spai0, chebyshev, "
-           "colored_gs or l1_colored_gs)");
+           "ilu0, serial_ilu0, colored_gs or l1_colored_gs)");
   }
 }
 
@@ -449,12 +553,12 @@ void build_hierarchy(const CSR& A_in, const Config& cfg, bool allow_partial_rese
   // Check the smoother before any work, so an unsupported choice fails fast.
   switch (cfg.smoother) {
     case SmootherKind::Jacobi: case SmootherKind::L1Jacobi: case SmootherKind::SPAI0:
-    case SmootherKind::Chebyshev:
+    case SmootherKind::Chebyshev: case SmootherKind::ILU0: case SmootherKind::SerialILU0:
     case SmootherKind::ColoredGS: case SmootherKind::L1ColoredGS: break;
     default:
       fail("smoother \"" + smoother_name(cfg.smoother) +
            "\" is not supported by the B200 build (use jacobi, l1_jacobi, spai0, chebyshev, "
-           "colored_gs or l1_colored_gs)");
+           "ilu0, serial_ilu0, colored_gs or l1_colored_gs)");
   }
   H = HostHierarchy();
   H.cfg = cfg;

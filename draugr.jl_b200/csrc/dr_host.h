@@ -159,6 +159,13 @@ struct HostLevel {
   std::vector<double> cheb_v0;
   double cheb_rho = 0.0;
   std::vector<double> cheb_coef;
+  // ILU(0) and serial ILU(0) (src/smoothers.jl:1016-1440): factors on A's
+  // pattern (ilu_L: strictly lower part of L, unit diagonal implied;
+  // ilu_U: upper part with the diagonal), the diagonal positions, and the
+  // level schedules of the two substitutions (rows by level, offsets).
+  std::vector<int> ilu_diag;
+  std::vector<double> ilu_L, ilu_U;
+  std::vector<int> ilu_fwd_order, ilu_fwd_off, ilu_bwd_order, ilu_bwd_off;
 };
 
 struct HostHierarchy {
@@ -229,6 +236,18 @@ double spectral_radius_estimate(const CSR& A, const std::vector<double>& invd, s
 // spectral-radius estimate rho (the bounds [rho * 1.1 / 30, rho * 1.1] and
 // the recurrence of smoothers.jl:895-986); 2 * degree entries.
 void chebyshev_coefficients(double rho, int degree, std::vector<double>& coef);
+// _ilu0_diag_indices (smoothers.jl:1083-1097); fails on a row without a
+// diagonal entry.
+void ilu0_diag_indices(const CSR& A, std::vector<int>& diag);
+// _ilu0_factorize! (smoothers.jl:1016-1080): sequential, with the
+// reference's zero-pivot skip, 1e8 growth clamp and diagonal safeguard.
+void ilu0_factorize(const CSR& A, const std::vector<int>& diag, std::vector<double>& L,
+                    std::vector<double>& U);
+// _compute_ilu_levels (smoothers.jl:1232-1299): rows grouped by level of
+// the forward (L) and backward (U) substitutions, in row order within a
+// level; offsets are 0-based, levels + 1 entries.
+void ilu0_levels(const CSR& A, const std::vector<int>& diag, std::vector<int>& fwd_order,
+                 std::vector<int>& fwd_off, std::vector<int>& bwd_order, std::vector<int>& bwd_off);
 void csr_to_dense(const CSR& A, std::vector<double>& M);            // setup.jl:495-516
 void dense_lu(int n, std::vector<double>& lu, std::vector<int>& piv);
 

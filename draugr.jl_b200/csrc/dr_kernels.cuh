@@ -1278,6 +1278,57 @@ __global__ void k_l1_invdiag(int n, const int* __restrict__ rp, const double* __
   }
 }
 
+// ILU(0) substitutions, one level of the schedule per launch (src/
+// smoothers.jl:1398-1423; the serial smoother's loops, :1174-1192, give the
+// same values): one thread per row, the row's products subtracted in column
+// order with separately rounded products and differences.
+// Forward: t_i -= L_ik t_k over the strictly lower part of row i.
+template <typename T>
+__global__ void k_ilu_fwd(int cnt, const int* __restrict__ order, const int* __restrict__ rp,
+                          const int* __restrict__ ci, const int* __restrict__ diag, const T* __restrict__ Lv,
+                          T* __restrict__ t) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < cnt; q += gridDim.x * blockDim.x) {
+    const int i = order[q];
+    T s = t[i];
+    for (int nz = rp[i]; nz < diag[i]; ++nz) s = sub_rn(s, mul_rn(Lv[nz], t[ci[nz]]));
+    t[i] = s;
+  }
+}
+
+__device__ __forceinline__ double div_rn(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
+template <typename T>
+__device__ __forceinline__ T eps_of();
+template <>
+__device__ __forceinline__ double eps_of<double>() { return 2.220446049250313e-16; }
+template <>
+__device__ __forceinline__ float eps_of<float>() { return 1.1920929e-07f; }
+
+// Backward: t_i -= U_ij t_j over the strictly upper part, then t_i / U_ii
+// (0 when |U_ii| <= eps).
+template <typename T>
+__global__ void k_ilu_bwd(int cnt, const int* __restrict__ order, const int* __restrict__ rp,
+                          const int* __restrict__ ci, const int* __restrict__ diag, const T* __restrict__ Uv,
+                          T* __restrict__ t) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < cnt; q += gridDim.x * blockDim.x) {
+    const int i = order[q];
+    const int di = diag[i];
+    T s = t[i];
+    for (int nz = di + 1; nz < rp[i + 1]; ++nz) s = sub_rn(s, mul_rn(Uv[nz], t[ci[nz]]));
+    const T u = Uv[di];
+    t[i] = fabs(u) > eps_of<T>() ? div_rn(s, u) : T(0);
+  }
+}
+
+// x += dx where dx is finite (src/smoothers.jl:1426-1431).
+template <typename T>
+__global__ void k_ilu_apply(int n, const T* __restrict__ dx, T* __restrict__ x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const T v = dx[i];
+    if (isfinite(v)) x[i] = add_rn(x[i], v);
+  }
+}
+
 // Power step, continued: lambda = ||w|| = sqrt(lam2[0]); v = w / lambda when
 // lambda > eps (src/smoothers.jl:881-884).
 __global__ void k_cheb_rescale(int n, const double* __restrict__ w, const double* __restrict__ lam2,

@@ -34,7 +34,8 @@ typedef struct {
   const int *P_rp, *P_ci;
   const double *P_v;
   const int *T_off, *T_rows, *T_pnz;
-  int smoother; /* 0 jacobi, 1 colored_gs, 3 spai0, 5 l1_jacobi, 6 l1_colored_gs, 8 chebyshev */
+  int smoother; /* 0 jacobi, 1 colored_gs, 3 spai0, 5 l1_jacobi, 6 l1_colored_gs, 8 chebyshev,
+                   9 ilu0, 10 serial_ilu0 */
   double omega;
   double *invd;
   int ncolors;
@@ -48,6 +49,9 @@ typedef struct {
   int cheb_degree;
   const double *cheb_v0;
   double *cheb_coef, *cheb_d;
+  /* ILU(0): diagonal positions and factors on A's pattern */
+  const int *ilu_diag;
+  double *ilu_L, *ilu_U;
 } olevel;
 
 typedef struct {
@@ -219,6 +223,78 @@ void orc_chebyshev(int n, const int *rp, const int *ci, const double *a, const d
         x[i] += d[i];
       }
     }
+  }
+}
+
+/* _ilu0_factorize!, src/smoothers.jl:1016-1080: U = A's values, L = 0; row
+ * by row, for each k < i in row i: skip (L = U = 0) when |U_kk| is below
+ * eps max(1, sum_k |a_kj|); l_ik = U_ik / U_kk clamped to magnitude 1e8;
+ * U_ij -= l_ik U_kj for j > k where (i, j) exists (_find_nz_in_row's
+ * binary search); then the diagonal safeguard U_ii = eps max(1, sum |a_ij|)
+ * when |U_ii| is below it. */
+void orc_ilu0_factor(int n, const int *rp, const int *ci, const double *a, const int *diag,
+                     double *L, double *U) {
+  const double eps = 2.220446049250313e-16;
+  int nnz = rp[n];
+  double *rn = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+  for (int k = 0; k < nnz; ++k) {
+    U[k] = a[k];
+    L[k] = 0.0;
+  }
+  for (int i = 0; i < n; ++i) {
+    double s = 0.0;
+    for (int k = rp[i]; k < rp[i + 1]; ++k) s += fabs(a[k]);
+    rn[i] = s;
+  }
+  for (int i = 0; i < n; ++i) {
+    for (int nz = rp[i]; nz < diag[i]; ++nz) {
+      int k = ci[nz];
+      double ukk = U[diag[k]];
+      if (fabs(ukk) < eps * (rn[k] > 1.0 ? rn[k] : 1.0)) {
+        L[nz] = 0.0;
+        U[nz] = 0.0;
+        continue;
+      }
+      double lik = U[nz] / ukk;
+      double nl = fabs(lik);
+      if (nl > 1e8) lik = lik * (1e8 / nl);
+      L[nz] = lik;
+      U[nz] = 0.0;
+      for (int nk = diag[k] + 1; nk < rp[k + 1]; ++nk) {
+        int j = ci[nk], lo = rp[i], hi = rp[i + 1] - 1, at = -1;
+        while (lo <= hi) {
+          int mid = (lo + hi) >> 1;
+          if (ci[mid] == j) { at = mid; break; }
+          if (ci[mid] < j) lo = mid + 1;
+          else hi = mid - 1;
+        }
+        if (at >= 0) U[at] -= lik * U[nk];
+      }
+    }
+    double thr = eps * (rn[i] > 1.0 ? rn[i] : 1.0);
+    if (fabs(U[diag[i]]) < thr) U[diag[i]] = thr;
+  }
+  free(rn);
+}
+
+/* smooth!(::SerialILU0Smoother), src/smoothers.jl:1143-1205 (the level-
+ * scheduled ILU0Smoother computes the same values): per step the residual
+ * (Ax summed from zero), forward substitution in row order, backward
+ * substitution in reverse row order with t_i / U_ii (0 when |U_ii| <=
+ * eps), then x += t where t is finite. */
+void orc_ilu0_smooth(int n, const int *rp, const int *ci, const double *a, const int *diag,
+                     const double *L, const double *U, double *x, const double *b, int steps, double *t) {
+  for (int s = 0; s < steps; ++s) {
+    cheb_residual(n, rp, ci, a, x, b, t);
+    for (int i = 0; i < n; ++i)
+      for (int nz = rp[i]; nz < diag[i]; ++nz) t[i] -= L[nz] * t[ci[nz]];
+    for (int i = n - 1; i >= 0; --i) {
+      for (int nz = diag[i] + 1; nz < rp[i + 1]; ++nz) t[i] -= U[nz] * t[ci[nz]];
+      double u = U[diag[i]];
+      t[i] = fabs(u) > 2.220446049250313e-16 ? t[i] / u : 0.0;
+    }
+    for (int i = 0; i < n; ++i)
+      if (isfinite(t[i])) x[i] += t[i];
   }
 }
 
@@ -566,6 +642,8 @@ static void smooth(olevel *L, double *x, const double *b, int steps) {
   else if (L->smoother == 8)
     orc_chebyshev(L->n, L->A_rp, L->A_ci, L->A_v, L->invd, L->cheb_coef, L->cheb_degree, x, b, steps,
                   L->tmp, L->cheb_d);
+  else if (L->smoother == 9 || L->smoother == 10)
+    orc_ilu0_smooth(L->n, L->A_rp, L->A_ci, L->A_v, L->ilu_diag, L->ilu_L, L->ilu_U, x, b, steps, L->tmp);
   else
     orc_gs(L->n, L->A_rp, L->A_ci, L->A_v, L->invd, L->ncolors, L->color_off, L->color_order, x, b,
            steps);
@@ -700,6 +778,8 @@ static void upd_invd(olevel *L) {
   if (L->smoother == 5 || L->smoother == 6) orc_l1_invdiag(L->n, L->A_rp, L->A_v, L->invd);
   else if (L->smoother == 3) orc_spai0(L->n, L->A_rp, L->A_ci, L->A_v, L->invd);
   else orc_invdiag(L->n, L->A_rp, L->A_ci, L->A_v, L->invd);
+  if (L->smoother == 9 || L->smoother == 10) /* update_smoother!, src/smoothers.jl:1332-1337 */
+    orc_ilu0_factor(L->n, L->A_rp, L->A_ci, L->A_v, L->ilu_diag, L->ilu_L, L->ilu_U);
   if (L->smoother == 8) { /* update_smoother!(::ChebyshevSmoother), src/smoothers.jl:912-922 */
     memcpy(L->tmp, L->cheb_v0, (size_t)L->n * sizeof(double));
     double rho = orc_spectral_radius(L->n, L->A_rp, L->A_ci, L->A_v, L->invd, L->tmp, 10, L->r);

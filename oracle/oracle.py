@@ -49,7 +49,8 @@ class OLevel(C.Structure):
                 ("smoother", i32), ("omega", f64), ("invd", P), ("ncolors", i32),
                 ("color_off", P), ("color_order", P), ("r", P), ("xc", P), ("bc", P),
                 ("tmp", P), ("nz_off", P), ("tpi", P), ("tai", P), ("tpj", P),
-                ("cheb_degree", i32), ("cheb_v0", P), ("cheb_coef", P), ("cheb_d", P)]
+                ("cheb_degree", i32), ("cheb_v0", P), ("cheb_coef", P), ("cheb_d", P),
+                ("ilu_diag", P), ("ilu_L", P), ("ilu_U", P)]
 
 
 class OHier(C.Structure):
@@ -67,6 +68,8 @@ def _declare(lib):
         "orc_spai0": (None, [i32, P, P, P, P]),
         "orc_spectral_radius": (f64, [i32, P, P, P, P, P, i32, P]),
         "orc_cheb_coef": (None, [f64, i32, P]),
+        "orc_ilu0_factor": (None, [i32, P, P, P, P, P, P]),
+        "orc_ilu0_smooth": (None, [i32, P, P, P, P, P, P, P, P, i32, P]),
         "orc_chebyshev": (None, [i32, P, P, P, P, P, i32, P, P, i32, P, P]),
         "orc_spai0_smooth": (None, [i32, P, P, P, P, P, P, i32, P]),
         "orc_jacobi": (None, [i32, P, P, P, P, f64, P, P, i32, P]),
@@ -157,6 +160,34 @@ def cheb_coef(rho, degree=3):
     c = np.zeros(2 * degree)
     load().orc_cheb_coef(float(rho), degree, ptr(c))
     return c
+
+
+def ilu0_diag(n, rp, ci):
+    """Position of each row's diagonal entry (_ilu0_diag_indices)."""
+    d = np.zeros(n, np.int32)
+    for i in range(n):
+        row = ci[rp[i]:rp[i + 1]]
+        d[i] = rp[i] + int(np.nonzero(row == i)[0][0])
+    return d
+
+
+def ilu0_factor(n, rp, ci, v, diag):
+    """ILU(0) factors (L strictly lower, U upper with the diagonal) on A's
+    pattern (_ilu0_factorize!)."""
+    L, U = np.zeros(len(ci)), np.zeros(len(ci))
+    load().orc_ilu0_factor(n, ptr(rp), ptr(ci), ptr(v), ptr(np.ascontiguousarray(diag, np.int32)), ptr(L),
+                           ptr(U))
+    return L, U
+
+
+def ilu0_smooth(n, rp, ci, v, diag, L, U, x, b, steps):
+    """`steps` ILU(0) smoothing steps (smooth!(::SerialILU0Smoother))."""
+    x = np.array(x, dtype=np.float64)
+    t = np.zeros(n)
+    load().orc_ilu0_smooth(n, ptr(rp), ptr(ci), ptr(v), ptr(np.ascontiguousarray(diag, np.int32)),
+                           ptr(np.ascontiguousarray(L, np.float64)), ptr(np.ascontiguousarray(U, np.float64)),
+                           ptr(x), ptr(np.ascontiguousarray(b, np.float64)), steps, ptr(t))
+    return x
 
 
 def chebyshev(n, rp, ci, v, invd, coef, x, b, steps):
@@ -251,7 +282,7 @@ def strength_abs(n, rp, ci, v, theta):
 
 # ---------------------------------------------------------------- hierarchy mirror
 SMOOTHER_KIND = {0: "jacobi", 1: "colored_gs", 3: "spai0", 5: "l1_jacobi", 6: "l1_colored_gs",
-                 8: "chebyshev"}
+                 8: "chebyshev", 9: "ilu0", 10: "serial_ilu0"}
 
 
 class OracleHierarchy:
@@ -291,6 +322,10 @@ class OracleHierarchy:
                          cheb_d=np.zeros(n))
                 L.cheb_degree = len(d["cheb_coef"]) // 2
                 L.cheb_v0, L.cheb_coef, L.cheb_d = ptr(d["cheb_v0"]), ptr(d["cheb_coef"]), ptr(d["cheb_d"])
+            if sk in (9, 10):
+                d.update(ilu_diag=h.export(l, "ilu_diag"), ilu_L=h.export(l, "ilu_L").copy(),
+                         ilu_U=h.export(l, "ilu_U").copy())
+                L.ilu_diag, L.ilu_L, L.ilu_U = ptr(d["ilu_diag"]), ptr(d["ilu_L"]), ptr(d["ilu_U"])
             L.ncolors = int(info[5])
             for k in ("A_rp", "A_ci", "A_v", "P_rp", "P_ci", "P_v", "T_off", "T_rows", "T_pnz",
                       "invd", "color_off", "color_order", "r", "xc", "bc", "tmp"):

@@ -21,6 +21,11 @@ CASES = {
                                 smoother=draugr.SPAI0SmootherType())),
     "hmis_chebyshev": (lambda: problems.heterogeneous_diffusion_3d(10, seed=7),
                        draugr.AMGConfig(smoother=draugr.ChebyshevSmootherType())),
+    "aggregation_ilu0": (lambda: problems.poisson2d(24),
+                         draugr.AMGConfig(coarsening=draugr.AggregationCoarsening(0.25),
+                                          smoother=draugr.ILU0SmootherType())),
+    "hmis_serial_ilu0": (lambda: problems.heterogeneous_diffusion_3d(10, seed=9),
+                         draugr.AMGConfig(smoother=draugr.SerialILU0SmootherType())),
     "aniso27_hmis": (lambda: problems.anisotropic_27pt(9, 1e-3),
                      draugr.AMGConfig(coarsening=draugr.HMISCoarsening(
                          0.25, draugr.ExtendedIInterpolation(0.2)),

@@ -92,7 +92,7 @@ def test_index_base_and_validation(lib):
     assert lib.draugr_b200_setup_host(n, len(ci), p(rp), p(bad), p(v), cfg, 0, 1) == -1
     assert "column index out of range" in draugr.last_error()
     # unsupported smoother fails with a clear message
-    cfg2 = draugr.config_handle(draugr.AMGConfig(smoother=draugr.ILU0SmootherType()))
+    cfg2 = draugr.config_handle(draugr.AMGConfig(smoother=draugr.SPAI1SmootherType()))
     assert lib.draugr_b200_setup_host(n, len(ci), p(rp), p(ci), p(v), cfg2, 0, 1) == -1
     assert "not supported" in draugr.last_error()
 
@@ -139,6 +139,21 @@ def test_structure_matches_oracle(host_case):
         if kind == 3:  # SPAI(0): m_i = a_ii / sum a_ij^2, swept with omega = 1
             inv = oracle.spai0(n, arp, aci, av)
             assert h.export(l, "omega")[0] == 1.0
+        elif kind in (9, 10):  # ILU(0): factors and level schedules
+            inv = oracle.invdiag(n, arp, aci, av)
+            diag = oracle.ilu0_diag(n, arp, aci)
+            assert np.array_equal(diag, h.export(l, "ilu_diag"))
+            Lf, Uf = oracle.ilu0_factor(n, arp, aci, av, diag)
+            assert np.array_equal(Lf, h.export(l, "ilu_L")) and np.array_equal(Uf, h.export(l, "ilu_U"))
+            for which, lower in (("fwd", True), ("bwd", False)):
+                order, off = h.export(l, f"ilu_{which}_order"), h.export(l, f"ilu_{which}_offsets")
+                assert np.array_equal(np.sort(order), np.arange(n)) and off[0] == 0 and off[-1] == n
+                level = np.empty(n, np.int64)
+                for v in range(len(off) - 1):
+                    level[order[off[v]:off[v + 1]]] = v
+                for i in range(n):  # every dependency sits in an earlier level
+                    deps = aci[arp[i]:diag[i]] if lower else aci[diag[i] + 1:arp[i + 1]]
+                    assert np.all(level[deps] < level[i])
         elif kind == 8:  # Chebyshev: Jacobi diagonal, power iteration, coefficients
             inv = oracle.invdiag(n, arp, aci, av)
             rho = oracle.spectral_radius(n, arp, aci, av, inv, h.export(l, "cheb_v0"))

@@ -67,6 +67,9 @@ def test_level_kernels(case):
                 ref = oracle.spai0_smooth(n, d["A_rp"], d["A_ci"], d["A_v"], d["invd"], x, b, steps)
             elif L.smoother == 8:
                 ref = oracle.chebyshev(n, d["A_rp"], d["A_ci"], d["A_v"], d["invd"], d["cheb_coef"], x, b, steps)
+            elif L.smoother in (9, 10):
+                ref = oracle.ilu0_smooth(n, d["A_rp"], d["A_ci"], d["A_v"], d["ilu_diag"], d["ilu_L"],
+                                         d["ilu_U"], x, b, steps)
             else:
                 ref = oracle.gs(n, d["A_rp"], d["A_ci"], d["A_v"], d["invd"], L.ncolors,
                                 d["color_off"], d["color_order"], x, b, steps)
@@ -168,6 +171,9 @@ def test_resetup_matches_reference_galerkin(case):
         assert rel(h.export(l, "invdiag"), O.levels_np[l]["invd"]) < TOL64
         if "cheb_coef" in O.levels_np[l]:  # spectral radius and coefficients redone on the device
             assert rel(h.export(l, "cheb_coef"), O.levels_np[l]["cheb_coef"]) < TOL64
+        if "ilu_L" in O.levels_np[l]:  # refactorised from the level's new values
+            assert rel(h.export(l, "ilu_L"), O.levels_np[l]["ilu_L"]) < TOL64
+            assert rel(h.export(l, "ilu_U"), O.levels_np[l]["ilu_U"]) < TOL64
     nc = O.nc
     assert rel(h.export(-1, "C_dense"), O.dense) < TOL64
     # the resetup hierarchy solves the new system

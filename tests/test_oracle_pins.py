@@ -5,6 +5,7 @@ testset it restates.  Hierarchy structures come from the library's CPU setup
 (host-only, no GPU), as they do for the parity tests."""
 
 import numpy as np
+import pytest
 import scipy.sparse as sp
 
 import draugr
@@ -167,6 +168,60 @@ def test_chebyshev_build_smoothing_solve_and_resetup():
         if m == 8:
             O.resetup(2.0 * A.data)
             x, it, rel = O.solve(np.zeros(N), b, 2, 2, False, 1e-8, 200)
+            assert it < 200 and np.linalg.norm(b - 2.0 * (A @ x)) / np.linalg.norm(b) < 1e-8
+
+
+def _anisotropic(nx, ny, kx=1e4, ky=1e-2):
+    """anisotropic_csr of the reference's tests (test/runtests.jl:1681-1694)."""
+    rows, cols, vals = [], [], []
+    for j in range(ny):
+        for i in range(nx):
+            idx = j * nx + i
+            nb = [(idx, 2 * kx + 2 * ky)]
+            if i > 0:
+                nb.append((idx - 1, -kx))
+            if i < nx - 1:
+                nb.append((idx + 1, -kx))
+            if j > 0:
+                nb.append((idx - nx, -ky))
+            if j < ny - 1:
+                nb.append((idx + nx, -ky))
+            for c, v in nb:
+                rows.append(idx); cols.append(c); vals.append(v)
+    A = sp.csr_matrix((vals, (rows, cols)), shape=(nx * ny, nx * ny))
+    A.sort_indices()
+    return A
+
+
+@pytest.mark.parametrize("smoother", ["ILU0SmootherType", "SerialILU0SmootherType"])
+def test_ilu0_build_smoothing_solve_and_resetup(smoother):
+    """testsets "ILU(0) Smoother - Build / Smoothing / AMG Solve / Resetup /
+    Anisotropic" and their serial counterparts (test/runtests.jl:1972-2127):
+    factors of nnz entries and at least 2 forward levels on the 1D
+    Laplacian; 3 steps reduce the residual; amg_solve! reaches 1e-8 in fewer
+    than 200 cycles on the 10 x 10 Poisson matrix, after a resetup with
+    doubled values (8 x 8), and on the 8 x 8 anisotropic matrix."""
+    A = problems.poisson1d(10)
+    n, rp, ci, v = parts(A)
+    diag = oracle.ilu0_diag(n, rp, ci)
+    Lf, Uf = oracle.ilu0_factor(n, rp, ci, v, diag)
+    assert len(Lf) == A.nnz and len(Uf) == A.nnz and len(diag) == 10
+    cfg = draugr.AMGConfig(smoother=getattr(draugr, smoother)())
+    h = draugr.amg_setup(problems.poisson2d(10), cfg, on_device=False)
+    assert len(h.export(0, "ilu_fwd_offsets")) - 1 >= 2
+    b = np.ones(n)
+    x = oracle.ilu0_smooth(n, rp, ci, v, diag, Lf, Uf, np.zeros(n), b, 3)
+    assert np.linalg.norm(b - A @ x) < np.linalg.norm(b)
+    for A, m in ((problems.poisson2d(10), 10), (problems.poisson2d(8), 8), (_anisotropic(8, 8), 8)):
+        N = A.shape[0]
+        b = np.random.default_rng(m).uniform(0, 1, N)
+        h = draugr.amg_setup(A, cfg, on_device=False)
+        O = oracle.OracleHierarchy(h, with_rmaps=True)
+        x, it, rel = O.solve(np.zeros(N), b, 1, 1, False, 1e-8, 200)
+        assert it < 200 and np.linalg.norm(b - A @ x) / np.linalg.norm(b) < 1e-8
+        if m == 8 and A.nnz == problems.poisson2d(8).nnz:
+            O.resetup(2.0 * A.data)
+            x, it, rel = O.solve(np.zeros(N), b, 1, 1, False, 1e-8, 200)
             assert it < 200 and np.linalg.norm(b - 2.0 * (A @ x)) / np.linalg.norm(b) < 1e-8
 
 
