@@ -373,6 +373,8 @@ int64_t draugr_b200_export(int32_t handle, int32_t lvl, const char* what, void* 
       else if (w == "ilu_fwd_offsets") iv = &L.ilu_fwd_off;
       else if (w == "ilu_bwd_order") iv = &L.ilu_bwd_order;
       else if (w == "ilu_bwd_offsets") iv = &L.ilu_bwd_off;
+      else if (w == "sgs_order") iv = &L.sgs_order;
+      else if (w == "sgs_offsets") iv = &L.sgs_off;
       else if (w == "AP_nzval") {
         if (!H->dev) fail("AP_nzval lives on the device only");
         dv = &tmpd;

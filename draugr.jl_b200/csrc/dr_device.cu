@@ -312,6 +312,11 @@ DevHier::DevHier(const HostHierarchy& H, int device) {
       }
       d.v64.xb = alloc<double>(n);
       d.v64.r = alloc<double>(n);
+      if (h.smoother == SmootherKind::SerialGS || h.smoother == SmootherKind::L1SerialGS) {
+        d.sgs_order = alloc<int>(n);
+        h2d(d.sgs_order, h.sgs_order, st_);
+        d.sgs_off = h.sgs_off;
+      }
       if (h.smoother == SmootherKind::ILU0 || h.smoother == SmootherKind::SerialILU0) {
         d.ilu_diag = alloc<int>(n);
         h2d(d.ilu_diag, h.ilu_diag, st_);
@@ -741,6 +746,17 @@ T* DevHier::smooth(int l, T* x, const T* b, int steps, T* ext, const double* rz_
       }
       x = dst;
     }
+  } else if (L.sgs_order) {
+    // serial (l1) Gauss-Seidel: the in-place sweep in row order, level by
+    // level of its dependencies
+    for (int s = 0; s < steps; ++s)
+      for (size_t v = 0; v + 1 < L.sgs_off.size(); ++v) {
+        const int off = L.sgs_off[v], cnt = L.sgs_off[v + 1] - off;
+        counted();
+        k_sgs_level<T><<<grid1d(cnt, max_grid_), kBlock, 0, st_>>>(cnt, L.sgs_order + off, A.rp, A.ci, mval<T>(A),
+                                                                  b, invd<T>(L), x);
+      }
+    DR_CK(cudaGetLastError());
   } else if (L.ilu_L) {
     // ILU(0): dx = (LU)^-1 (b - A x) by the two level schedules, x += dx
     // (in place)
@@ -1354,8 +1370,11 @@ void DevHier::resetup_values(const double* v_dev) {
   }
   auto upd_invd = [&](DevLevel& d) {
     counted();
-    if (d.smoother == SmootherKind::L1Jacobi || d.smoother == SmootherKind::L1ColoredGS)
+    if (d.smoother == SmootherKind::L1Jacobi || d.smoother == SmootherKind::L1ColoredGS ||
+        d.smoother == SmootherKind::L1SerialGS)
       k_l1_invdiag<<<grid1d(d.A.n, max_grid_), kBlock, 0, st_>>>(d.A.n, d.A.rp, d.A.v, d.invd);
+    else if (d.smoother == SmootherKind::SerialGS)
+      k_sgs_invdiag<<<grid1d(d.A.n, max_grid_), kBlock, 0, st_>>>(d.A.n, d.A.rp, d.A.ci, d.A.v, d.invd);
     else if (d.smoother == SmootherKind::SPAI0)
       k_spai0_diag<<<grid1d(d.A.n, max_grid_), kBlock, 0, st_>>>(d.A.n, d.A.rp, d.A.ci, d.A.v, d.invd);
     else

@@ -136,6 +136,9 @@ struct DevLevel {
   float *ilu_L32 = nullptr, *ilu_U32 = nullptr;
   int *ilu_fwd = nullptr, *ilu_bwd = nullptr;
   std::vector<int> ilu_fwd_off, ilu_bwd_off, ilu_rp, ilu_ci, ilu_diag_h;
+  // serial Gauss-Seidel: rows by level (device), level offsets (host)
+  int* sgs_order = nullptr;
+  std::vector<int> sgs_off;
   LevelVecs<double> v64;
   LevelVecs<float> v32;
 };

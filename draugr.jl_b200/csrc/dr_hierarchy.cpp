@@ -476,6 +476,47 @@ void ilu0_levels(const CSR& A, const std::vector<int>& diag, std::vector<int>& f
 
 namespace {
 
+}  // namespace
+
+void serial_gs_levels(const CSR& A, std::vector<int>& order, std::vector<int>& off) {
+  const int n = A.n;
+  std::vector<std::vector<int>> later(n);  // later[i]: rows j < i with a_ji != 0
+  for (int j = 0; j < n; ++j)
+    for (int k = A.rp[j]; k < A.rp[j + 1]; ++k)
+      if (A.ci[k] > j) later[A.ci[k]].push_back(j);
+  std::vector<int> lev(n);
+  int nl = 0;
+  for (int i = 0; i < n; ++i) {
+    int m = 0;
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
+      if (A.ci[k] < i) m = std::max(m, lev[A.ci[k]]);
+    for (int j : later[i]) m = std::max(m, lev[j]);
+    lev[i] = m + 1;
+    nl = std::max(nl, lev[i]);
+  }
+  off.assign(nl + 1, 0);
+  for (int i = 0; i < n; ++i) ++off[lev[i]];
+  for (int c = 0; c < nl; ++c) off[c + 1] += off[c];
+  std::vector<int> pos(off.begin(), off.end() - 1);
+  order.resize(n);
+  for (int i = 0; i < n; ++i) order[pos[lev[i] - 1]++] = i;
+}
+
+void serial_gs_inverse_diagonal(const CSR& A, std::vector<double>& invd) {
+  invd.resize(A.n);
+  for (int i = 0; i < A.n; ++i) {
+    double d = 0.0;
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
+      if (A.ci[k] == i) {
+        d = A.v[k];
+        break;
+      }
+    invd[i] = std::fabs(d) > kEps ? 1.0 / d : 0.0;
+  }
+}
+
+namespace {
+
 // Normalised start vector of the Chebyshev power iteration: standard normal
 // entries (Box-Muller on splitmix64 uniforms), divided by their 2-norm.
 std::vector<double> chebyshev_start(int n, uint64_t seed) {
@@ -507,6 +548,12 @@ void build_smoother(HostLevel& L, const Config& cfg, int level) {
     case SmootherKind::SPAI0:  // x + m (b - A x): the Jacobi sweep with omega = 1
       spai0_diagonal(L.A, L.invdiag);
       L.omega = 1.0;
+      break;
+    case SmootherKind::SerialGS:   // build_serial_gs_smoother, smoothers.jl:370-376
+    case SmootherKind::L1SerialGS:  // build_l1_serial_gs_smoother, :428-434
+      if (cfg.smoother == SmootherKind::SerialGS) serial_gs_inverse_diagonal(L.A, L.invdiag);
+      else l1_inverse_diagonal(L.A, L.invdiag);
+      serial_gs_levels(L.A, L.sgs_order, L.sgs_off);
       break;
     case SmootherKind::ILU0:
     case SmootherKind::SerialILU0:
@@ -540,7 +587,7 @@ void build_smoother(HostLevel& L, const Config& cfg, int level) {
     default:
       fail("smoother \"" + smoother_name(cfg.smoother) +
            "\" is not supported by the B200 build (use jacobi, l1_jacobi, spai0, chebyshev, "
-           "ilu0, serial_ilu0, colored_gs or l1_colored_gs)");
+           "ilu0, serial_ilu0, colored_gs, l1_colored_gs, serial_gs or l1_serial_gs)");
   }
 }
 
@@ -554,11 +601,12 @@ void build_hierarchy(const CSR& A_in, const Config& cfg, bool allow_partial_rese
   switch (cfg.smoother) {
     case SmootherKind::Jacobi: case SmootherKind::L1Jacobi: case SmootherKind::SPAI0:
     case SmootherKind::Chebyshev: case SmootherKind::ILU0: case SmootherKind::SerialILU0:
+    case SmootherKind::SerialGS: case SmootherKind::L1SerialGS:
     case SmootherKind::ColoredGS: case SmootherKind::L1ColoredGS: break;
     default:
       fail("smoother \"" + smoother_name(cfg.smoother) +
            "\" is not supported by the B200 build (use jacobi, l1_jacobi, spai0, chebyshev, "
-           "ilu0, serial_ilu0, colored_gs or l1_colored_gs)");
+           "ilu0, serial_ilu0, colored_gs, l1_colored_gs, serial_gs or l1_serial_gs)");
   }
   H = HostHierarchy();
   H.cfg = cfg;

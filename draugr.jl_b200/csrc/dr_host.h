@@ -166,6 +166,9 @@ struct HostLevel {
   std::vector<int> ilu_diag;
   std::vector<double> ilu_L, ilu_U;
   std::vector<int> ilu_fwd_order, ilu_fwd_off, ilu_bwd_order, ilu_bwd_off;
+  // Serial and l1 serial Gauss-Seidel (src/smoothers.jl:318-491): rows by
+  // level of the sweep's dependencies, level offsets.
+  std::vector<int> sgs_order, sgs_off;
 };
 
 struct HostHierarchy {
@@ -248,6 +251,14 @@ void ilu0_factorize(const CSR& A, const std::vector<int>& diag, std::vector<doub
 // level; offsets are 0-based, levels + 1 entries.
 void ilu0_levels(const CSR& A, const std::vector<int>& diag, std::vector<int>& fwd_order,
                  std::vector<int>& fwd_off, std::vector<int>& bwd_order, std::vector<int>& bwd_off);
+// Level schedule that reproduces the in-place forward Gauss-Seidel sweep in
+// row order: row i follows every j < i with a_ij or a_ji nonzero (it reads
+// the new x_j of its lower neighbours, and its upper neighbours must still
+// read its old x_i).
+void serial_gs_levels(const CSR& A, std::vector<int>& order, std::vector<int>& off);
+// _serial_gs_compute_invdiag! (smoothers.jl:329-340): 1/a_ii (the first
+// diagonal entry of the row), 0 when |a_ii| <= eps.
+void serial_gs_inverse_diagonal(const CSR& A, std::vector<double>& invd);
 void csr_to_dense(const CSR& A, std::vector<double>& M);            // setup.jl:495-516
 void dense_lu(int n, std::vector<double>& lu, std::vector<int>& piv);
 

@@ -1320,6 +1320,36 @@ __global__ void k_ilu_bwd(int cnt, const int* __restrict__ order, const int* __r
   }
 }
 
+// One level of the serial Gauss-Seidel sweep (src/smoothers.jl:350-362):
+// one thread per row, r = b_i - a_i1 x_1 - ... in column order, x_i +=
+// invd_i r, in place.
+template <typename T>
+__global__ void k_sgs_level(int cnt, const int* __restrict__ order, const int* __restrict__ rp,
+                            const int* __restrict__ ci, const T* __restrict__ av, const T* __restrict__ b,
+                            const T* __restrict__ invd, T* x) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < cnt; q += gridDim.x * blockDim.x) {
+    const int i = order[q];
+    T r = b[i];
+    for (int nz = rp[i]; nz < rp[i + 1]; ++nz) r = sub_rn(r, mul_rn(av[nz], x[ci[nz]]));
+    x[i] = add_rn(x[i], mul_rn(invd[i], r));
+  }
+}
+
+// _serial_gs_compute_invdiag! (src/smoothers.jl:329-340): 1/a_ii from the
+// row's first diagonal entry, 0 when |a_ii| <= eps.
+__global__ void k_sgs_invdiag(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                              const double* __restrict__ v, double* __restrict__ invd) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double d = 0.0;
+    for (int k = rp[i]; k < rp[i + 1]; ++k)
+      if (ci[k] == i) {
+        d = v[k];
+        break;
+      }
+    invd[i] = fabs(d) > 2.220446049250313e-16 ? __drcp_rn(d) : 0.0;
+  }
+}
+
 // x += dx where dx is finite (src/smoothers.jl:1426-1431).
 template <typename T>
 __global__ void k_ilu_apply(int n, const T* __restrict__ dx, T* __restrict__ x) {

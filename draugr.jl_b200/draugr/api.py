@@ -282,7 +282,8 @@ class Hierarchy:
         is_int = what in ("A_rowptr", "A_colval", "P_rowptr", "P_colval", "T_offsets", "T_rows",
                           "T_pnz", "colors", "color_order", "color_offsets", "AP_rowptr",
                           "AP_colval", "C_rowptr", "C_colval", "C_piv", "ilu_diag", "ilu_fwd_order",
-                          "ilu_fwd_offsets", "ilu_bwd_order", "ilu_bwd_offsets")
+                          "ilu_fwd_offsets", "ilu_bwd_order", "ilu_bwd_offsets", "sgs_order",
+                          "sgs_offsets")
         out = np.zeros(cnt, dtype=np.int32 if is_int else np.float64)
         _lib.check(lib.draugr_b200_export(self.handle, lvl, what.encode(), _ptr(out), cnt),
                    f"export {what}")

@@ -34,8 +34,8 @@ typedef struct {
   const int *P_rp, *P_ci;
   const double *P_v;
   const int *T_off, *T_rows, *T_pnz;
-  int smoother; /* 0 jacobi, 1 colored_gs, 3 spai0, 5 l1_jacobi, 6 l1_colored_gs, 8 chebyshev,
-                   9 ilu0, 10 serial_ilu0 */
+  int smoother; /* 0 jacobi, 1 colored_gs, 2 serial_gs, 3 spai0, 5 l1_jacobi, 6 l1_colored_gs,
+                   7 l1_serial_gs, 8 chebyshev, 9 ilu0, 10 serial_ilu0 */
   double omega;
   double *invd;
   int ncolors;
@@ -296,6 +296,32 @@ void orc_ilu0_smooth(int n, const int *rp, const int *ci, const double *a, const
     for (int i = 0; i < n; ++i)
       if (isfinite(t[i])) x[i] += t[i];
   }
+}
+
+/* _serial_gs_compute_invdiag!, src/smoothers.jl:329-340: 1/a_ii from the
+ * row's first diagonal entry, 0 when |a_ii| <= eps */
+void orc_serial_gs_invdiag(int n, const int *rp, const int *ci, const double *v, double *invd) {
+  for (int i = 0; i < n; ++i) {
+    double d = 0.0;
+    for (int k = rp[i]; k < rp[i + 1]; ++k)
+      if (ci[k] == i) {
+        d = v[k];
+        break;
+      }
+    invd[i] = fabs(d) > 2.220446049250313e-16 ? 1.0 / d : 0.0;
+  }
+}
+
+/* _serial_gs_sweep!, src/smoothers.jl:350-362: rows in order, in place:
+ * r_i = b_i - sum_j a_ij x_j (current x), x_i += invdiag_i r_i */
+void orc_serial_gs(int n, const int *rp, const int *ci, const double *v, const double *invd, double *x,
+                   const double *b, int steps) {
+  for (int s = 0; s < steps; ++s)
+    for (int i = 0; i < n; ++i) {
+      double r = b[i];
+      for (int k = rp[i]; k < rp[i + 1]; ++k) r -= v[k] * x[ci[k]];
+      x[i] += invd[i] * r;
+    }
 }
 
 /* smooth!(::JacobiSmoother / ::L1JacobiSmoother): jacobi_kernel! with the
@@ -642,6 +668,8 @@ static void smooth(olevel *L, double *x, const double *b, int steps) {
   else if (L->smoother == 8)
     orc_chebyshev(L->n, L->A_rp, L->A_ci, L->A_v, L->invd, L->cheb_coef, L->cheb_degree, x, b, steps,
                   L->tmp, L->cheb_d);
+  else if (L->smoother == 2 || L->smoother == 7)
+    orc_serial_gs(L->n, L->A_rp, L->A_ci, L->A_v, L->invd, x, b, steps);
   else if (L->smoother == 9 || L->smoother == 10)
     orc_ilu0_smooth(L->n, L->A_rp, L->A_ci, L->A_v, L->ilu_diag, L->ilu_L, L->ilu_U, x, b, steps, L->tmp);
   else
@@ -775,7 +803,8 @@ int orc_pcg(ohier *h, double *x, const double *b, int pre, int post, int w, doub
  * coarse_ci / coarse_v describe the coarsest CSR when nlevels == 0.
  * Returns 0 or the LU's zero-pivot index. */
 static void upd_invd(olevel *L) {
-  if (L->smoother == 5 || L->smoother == 6) orc_l1_invdiag(L->n, L->A_rp, L->A_v, L->invd);
+  if (L->smoother == 5 || L->smoother == 6 || L->smoother == 7) orc_l1_invdiag(L->n, L->A_rp, L->A_v, L->invd);
+  else if (L->smoother == 2) orc_serial_gs_invdiag(L->n, L->A_rp, L->A_ci, L->A_v, L->invd);
   else if (L->smoother == 3) orc_spai0(L->n, L->A_rp, L->A_ci, L->A_v, L->invd);
   else orc_invdiag(L->n, L->A_rp, L->A_ci, L->A_v, L->invd);
   if (L->smoother == 9 || L->smoother == 10) /* update_smoother!, src/smoothers.jl:1332-1337 */

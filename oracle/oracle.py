@@ -69,6 +69,8 @@ def _declare(lib):
         "orc_spectral_radius": (f64, [i32, P, P, P, P, P, i32, P]),
         "orc_cheb_coef": (None, [f64, i32, P]),
         "orc_ilu0_factor": (None, [i32, P, P, P, P, P, P]),
+        "orc_serial_gs_invdiag": (None, [i32, P, P, P, P]),
+        "orc_serial_gs": (None, [i32, P, P, P, P, P, P, i32]),
         "orc_ilu0_smooth": (None, [i32, P, P, P, P, P, P, P, P, i32, P]),
         "orc_chebyshev": (None, [i32, P, P, P, P, P, i32, P, P, i32, P, P]),
         "orc_spai0_smooth": (None, [i32, P, P, P, P, P, P, i32, P]),
@@ -160,6 +162,21 @@ def cheb_coef(rho, degree=3):
     c = np.zeros(2 * degree)
     load().orc_cheb_coef(float(rho), degree, ptr(c))
     return c
+
+
+def serial_gs_invdiag(n, rp, ci, v):
+    """1/a_ii for the serial Gauss-Seidel smoother (_serial_gs_compute_invdiag!)."""
+    d = np.zeros(n)
+    load().orc_serial_gs_invdiag(n, ptr(rp), ptr(ci), ptr(v), ptr(d))
+    return d
+
+
+def serial_gs(n, rp, ci, v, invd, x, b, steps):
+    """`steps` in-place forward Gauss-Seidel sweeps in row order (_serial_gs_sweep!)."""
+    x = np.array(x, dtype=np.float64)
+    load().orc_serial_gs(n, ptr(rp), ptr(ci), ptr(v), ptr(np.ascontiguousarray(invd, np.float64)), ptr(x),
+                         ptr(np.ascontiguousarray(b, np.float64)), steps)
+    return x
 
 
 def ilu0_diag(n, rp, ci):
@@ -281,8 +298,8 @@ def strength_abs(n, rp, ci, v, theta):
 
 
 # ---------------------------------------------------------------- hierarchy mirror
-SMOOTHER_KIND = {0: "jacobi", 1: "colored_gs", 3: "spai0", 5: "l1_jacobi", 6: "l1_colored_gs",
-                 8: "chebyshev", 9: "ilu0", 10: "serial_ilu0"}
+SMOOTHER_KIND = {0: "jacobi", 1: "colored_gs", 2: "serial_gs", 3: "spai0", 5: "l1_jacobi",
+                 6: "l1_colored_gs", 7: "l1_serial_gs", 8: "chebyshev", 9: "ilu0", 10: "serial_ilu0"}
 
 
 class OracleHierarchy:

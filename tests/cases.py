@@ -26,6 +26,11 @@ CASES = {
                                           smoother=draugr.ILU0SmootherType())),
     "hmis_serial_ilu0": (lambda: problems.heterogeneous_diffusion_3d(10, seed=9),
                          draugr.AMGConfig(smoother=draugr.SerialILU0SmootherType())),
+    "aggregation_serial_gs": (lambda: problems.poisson2d(24),
+                              draugr.AMGConfig(coarsening=draugr.AggregationCoarsening(0.25),
+                                               smoother=draugr.SerialGaussSeidelType())),
+    "hmis_l1_serial_gs": (lambda: problems.heterogeneous_diffusion_3d(10, seed=11),
+                          draugr.AMGConfig(smoother=draugr.L1SerialGaussSeidelType())),
     "aniso27_hmis": (lambda: problems.anisotropic_27pt(9, 1e-3),
                      draugr.AMGConfig(coarsening=draugr.HMISCoarsening(
                          0.25, draugr.ExtendedIInterpolation(0.2)),

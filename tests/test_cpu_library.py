@@ -139,6 +139,17 @@ def test_structure_matches_oracle(host_case):
         if kind == 3:  # SPAI(0): m_i = a_ii / sum a_ij^2, swept with omega = 1
             inv = oracle.spai0(n, arp, aci, av)
             assert h.export(l, "omega")[0] == 1.0
+        elif kind in (2, 7):  # serial (l1) Gauss-Seidel: diagonal and sweep schedule
+            inv = oracle.serial_gs_invdiag(n, arp, aci, av) if kind == 2 else oracle.invdiag(n, arp, aci, av, l1=True)
+            order, off = h.export(l, "sgs_order"), h.export(l, "sgs_offsets")
+            assert np.array_equal(np.sort(order), np.arange(n)) and off[0] == 0 and off[-1] == n
+            level = np.empty(n, np.int64)
+            for v in range(len(off) - 1):
+                level[order[off[v]:off[v + 1]]] = v
+            rr = np.repeat(np.arange(n), np.diff(arp))
+            off_diag = rr != aci
+            lo, hi = np.minimum(rr, aci)[off_diag], np.maximum(rr, aci)[off_diag]
+            assert np.all(level[lo] < level[hi])  # every coupling ordered as the row sweep
         elif kind in (9, 10):  # ILU(0): factors and level schedules
             inv = oracle.invdiag(n, arp, aci, av)
             diag = oracle.ilu0_diag(n, arp, aci)

@@ -67,6 +67,8 @@ def test_level_kernels(case):
                 ref = oracle.spai0_smooth(n, d["A_rp"], d["A_ci"], d["A_v"], d["invd"], x, b, steps)
             elif L.smoother == 8:
                 ref = oracle.chebyshev(n, d["A_rp"], d["A_ci"], d["A_v"], d["invd"], d["cheb_coef"], x, b, steps)
+            elif L.smoother in (2, 7):
+                ref = oracle.serial_gs(n, d["A_rp"], d["A_ci"], d["A_v"], d["invd"], x, b, steps)
             elif L.smoother in (9, 10):
                 ref = oracle.ilu0_smooth(n, d["A_rp"], d["A_ci"], d["A_v"], d["ilu_diag"], d["ilu_L"],
                                          d["ilu_U"], x, b, steps)

@@ -171,6 +171,31 @@ def test_chebyshev_build_smoothing_solve_and_resetup():
             assert it < 200 and np.linalg.norm(b - 2.0 * (A @ x)) / np.linalg.norm(b) < 1e-8
 
 
+@pytest.mark.parametrize("l1", [False, True])
+def test_serial_gs_build_smoothing_and_solve(l1):
+    """testsets "Serial GS Smoother" and "L1 Serial GS Smoother" (test/
+    runtests.jl:648-740): invdiag 0.5 (l1: 1/4 inside, 1/3 at the ends) on
+    the 1D Laplacian; 10 sweeps reduce the residual; amg_solve! reaches 1e-8
+    in fewer than 200 cycles on the 10 x 10 Poisson matrix."""
+    A = problems.poisson1d(10)
+    n, rp, ci, v = parts(A)
+    inv = oracle.invdiag(n, rp, ci, v, l1=True) if l1 else oracle.serial_gs_invdiag(n, rp, ci, v)
+    if l1:
+        assert np.isclose(inv[4], 0.25) and np.isclose(inv[0], 1.0 / 3.0)
+    else:
+        assert np.allclose(inv, 0.5)
+    b = np.ones(n)
+    x = oracle.serial_gs(n, rp, ci, v, inv, np.zeros(n), b, 10)
+    assert np.linalg.norm(b - A @ x) < np.linalg.norm(b)
+    A = problems.poisson2d(10)
+    b = np.random.default_rng(4).uniform(0, 1, 100)
+    cfg = draugr.AMGConfig(smoother=draugr.L1SerialGaussSeidelType() if l1 else draugr.SerialGaussSeidelType())
+    h = draugr.amg_setup(A, cfg, on_device=False)
+    O = oracle.OracleHierarchy(h)
+    x, it, rel = O.solve(np.zeros(100), b, tol=1e-8, maxiter=200)
+    assert it < 200 and np.linalg.norm(b - A @ x) / np.linalg.norm(b) < 1e-8
+
+
 def _anisotropic(nx, ny, kx=1e4, ky=1e-2):
     """anisotropic_csr of the reference's tests (test/runtests.jl:1681-1694)."""
     rows, cols, vals = [], [], []
