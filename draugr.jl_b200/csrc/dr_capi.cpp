@@ -373,6 +373,7 @@ int64_t draugr_b200_export(int32_t handle, int32_t lvl, const char* what, void* 
       else if (w == "ilu_fwd_offsets") iv = &L.ilu_fwd_off;
       else if (w == "ilu_bwd_order") iv = &L.ilu_bwd_order;
       else if (w == "ilu_bwd_offsets") iv = &L.ilu_bwd_off;
+      else if (w == "spai1_M") dv = &L.spai1_M;
       else if (w == "sgs_order") iv = &L.sgs_order;
       else if (w == "sgs_offsets") iv = &L.sgs_off;
       else if (w == "AP_nzval") {
@@ -380,7 +381,8 @@ int64_t draugr_b200_export(int32_t handle, int32_t lvl, const char* what, void* 
         dv = &tmpd;
       }
       if (dv && H->dev && w != "P_nzval" && w != "R_nzval" && w != "omega" && w != "cheb_v0" &&
-          !(w == "cheb_coef" && L.cheb_coef.empty()) && !((w == "ilu_L" || w == "ilu_U") && L.ilu_L.empty())) {
+          !(w == "cheb_coef" && L.cheb_coef.empty()) && !((w == "ilu_L" || w == "ilu_U") && L.ilu_L.empty()) &&
+          !(w == "spai1_M" && L.spai1_M.empty())) {
         H->dev->export_values(lvl, w, tmpd);
         dv = &tmpd;
       }

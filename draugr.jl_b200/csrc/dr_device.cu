@@ -312,6 +312,13 @@ DevHier::DevHier(const HostHierarchy& H, int device) {
       }
       d.v64.xb = alloc<double>(n);
       d.v64.r = alloc<double>(n);
+      if (h.smoother == SmootherKind::SPAI1) {
+        d.spai1_M = alloc<double>(h.A.v.size() + 4);
+        h2d(d.spai1_M, h.spai1_M, st_);
+        d.v64.d = alloc<double>(n);
+        d.ilu_rp = h.A.rp;  // host pattern for recomputing M after a resetup
+        d.ilu_ci = h.A.ci;
+      }
       if (h.smoother == SmootherKind::SerialGS || h.smoother == SmootherKind::L1SerialGS) {
         d.sgs_order = alloc<int>(n);
         h2d(d.sgs_order, h.sgs_order, st_);
@@ -488,6 +495,10 @@ void DevHier::ensure_fp32() {
     d.v32.b = alloc<float>(n);
     d.v32.r = alloc<float>(n);
     if (d.smoother == SmootherKind::Chebyshev) d.v32.d = alloc<float>(n);
+    if (d.spai1_M) {
+      d.v32.d = alloc<float>(n);
+      d.spai1_M32 = alloc<float>(d.A.nnz + 4);
+    }
     if (d.ilu_L) {
       d.v32.d = alloc<float>(n);
       d.ilu_L32 = alloc<float>(d.A.nnz + 4);
@@ -712,6 +723,10 @@ void DevHier::refresh_fp32() {
     k_convert<double, float><<<grid1d(d.R.nnz, max_grid_), kBlock, 0, st_>>>(d.R.nnz, d.R.v, d.R.v32);
     counted();
     k_convert<double, float><<<grid1d(d.A.n, max_grid_), kBlock, 0, st_>>>(d.A.n, d.invd, d.invd32);
+    if (d.spai1_M32) {
+      counted();
+      k_convert<double, float><<<grid1d(d.A.nnz, max_grid_), kBlock, 0, st_>>>(d.A.nnz, d.spai1_M, d.spai1_M32);
+    }
     if (d.ilu_L32) {
       counted();
       k_convert<double, float><<<grid1d(d.A.nnz, max_grid_), kBlock, 0, st_>>>(d.A.nnz, d.ilu_L, d.ilu_L32);
@@ -745,6 +760,13 @@ T* DevHier::smooth(int l, T* x, const T* b, int steps, T* ext, const double* rz_
                     EpJacobi<T>{x, b, invd<T>(L), dst, om, nullptr});
       }
       x = dst;
+    }
+  } else if (L.spai1_M) {
+    // SPAI(1): r = b - A x, then x += M r, in place
+    const T* Mv = std::is_same<T, float>::value ? (const T*)L.spai1_M32 : (const T*)L.spai1_M;
+    for (int s = 0; s < steps; ++s) {
+      launch_rows(st_, max_grid_, A, mval<T>(A), XPlain<T>{x}, EpResidualSub<T>{b, V.d});
+      launch_rows(st_, max_grid_, A, Mv, XPlain<T>{V.d}, EpAddSum<T>{x});
     }
   } else if (L.sgs_order) {
     // serial (l1) Gauss-Seidel: the in-place sweep in row order, level by
@@ -1380,6 +1402,21 @@ void DevHier::resetup_values(const double* v_dev) {
     else
       k_invdiag<<<grid1d(d.A.n, max_grid_), kBlock, 0, st_>>>(d.A.n, d.A.rp, d.A.ci, d.A.v, d.invd);
     DR_CK(cudaGetLastError());
+    if (d.spai1_M) {
+      // update_smoother!(::SPAI1Smoother), src/smoothers.jl:692-699: M again
+      // on the host from the level's new values, as in the reference
+      CSR a;
+      a.n = a.m = d.A.n;
+      a.rp = d.ilu_rp;
+      a.ci = d.ilu_ci;
+      a.v.resize(d.A.nnz);
+      DR_CK(cudaMemcpyAsync(a.v.data(), d.A.v, (size_t)d.A.nnz * sizeof(double), cudaMemcpyDeviceToHost, st_));
+      DR_CK(cudaStreamSynchronize(st_));
+      std::vector<double> Mh;
+      spai1_values(a, Mh);
+      h2d(d.spai1_M, Mh, st_);
+      DR_CK(cudaStreamSynchronize(st_));
+    }
     if (d.ilu_L) {
       // update_smoother!(::ILU0Smoother / ::SerialILU0Smoother), src/
       // smoothers.jl:1332-1337: the factorisation is sequential, so it runs
@@ -1632,6 +1669,7 @@ void DevHier::export_values(int lvl, const std::string& what, std::vector<double
     else if (what == "invdiag") { src = d.invd; n = d.A.n; }
     else if (what == "cheb_coef" && d.cheb_coef) { src = d.cheb_coef; n = 2LL * d.cheb_degree; }
     else if (what == "ilu_L" && d.ilu_L) { src = d.ilu_L; n = d.A.nnz; }
+    else if (what == "spai1_M" && d.spai1_M) { src = d.spai1_M; n = d.A.nnz; }
     else if (what == "ilu_U" && d.ilu_U) { src = d.ilu_U; n = d.A.nnz; }
     else if (what == "AP_nzval" && d.has_rap) { src = d.AP.v; n = d.AP.nnz; }
   }

@@ -129,8 +129,8 @@ struct DevLevel {
   double* cheb_coef = nullptr;
   // ILU(0): diagonal positions, factors (FP64; FP32 after the first mixed
   // use), the substitution schedules (rows by level on the device, level
-  // offsets on the host) and the host pattern for refactorising after a
-  // resetup
+  // offsets on the host); ilu_rp / ilu_ci: the host pattern for recomputing
+  // ILU(0) factors or SPAI(1)'s M after a resetup
   int* ilu_diag = nullptr;
   double *ilu_L = nullptr, *ilu_U = nullptr;
   float *ilu_L32 = nullptr, *ilu_U32 = nullptr;
@@ -139,6 +139,9 @@ struct DevLevel {
   // serial Gauss-Seidel: rows by level (device), level offsets (host)
   int* sgs_order = nullptr;
   std::vector<int> sgs_off;
+  // SPAI(1): M on A's pattern (FP64; FP32 after the first mixed use)
+  double* spai1_M = nullptr;
+  float* spai1_M32 = nullptr;
   LevelVecs<double> v64;
   LevelVecs<float> v32;
 };

@@ -517,6 +517,124 @@ void serial_gs_inverse_diagonal(const CSR& A, std::vector<double>& invd) {
 
 namespace {
 
+}  // namespace
+
+namespace {
+
+// Solve the k x k symmetric system G m = r (row-major G, overwritten) by the
+// upper Cholesky factor (G = U^T U, LAPACK potf2 order); false when a pivot
+// is not positive.
+bool cholesky_solve(int k, std::vector<double>& G, const std::vector<double>& r, std::vector<double>& m) {
+  for (int j = 0; j < k; ++j) {
+    double s = G[(size_t)j * k + j];
+    for (int t = 0; t < j; ++t) s -= G[(size_t)t * k + j] * G[(size_t)t * k + j];
+    if (!(s > 0.0)) return false;
+    const double ujj = std::sqrt(s);
+    G[(size_t)j * k + j] = ujj;
+    for (int l = j + 1; l < k; ++l) {
+      double v = G[(size_t)j * k + l];
+      for (int t = 0; t < j; ++t) v -= G[(size_t)t * k + j] * G[(size_t)t * k + l];
+      G[(size_t)j * k + l] = v / ujj;
+    }
+  }
+  m = r;
+  for (int j = 0; j < k; ++j) {  // U^T y = r
+    double v = m[j];
+    for (int t = 0; t < j; ++t) v -= G[(size_t)t * k + j] * m[t];
+    m[j] = v / G[(size_t)j * k + j];
+  }
+  for (int j = k - 1; j >= 0; --j) {  // U m = y
+    double v = m[j];
+    for (int t = j + 1; t < k; ++t) v -= G[(size_t)j * k + t] * m[t];
+    m[j] = v / G[(size_t)j * k + j];
+  }
+  return true;
+}
+
+// Partial-pivoting LU solve of the k x k system (row-major G, overwritten);
+// false on a zero pivot.
+bool lu_solve_small(int k, std::vector<double>& G, const std::vector<double>& r, std::vector<double>& m) {
+  m = r;
+  for (int j = 0; j < k; ++j) {
+    int p = j;
+    for (int i = j + 1; i < k; ++i)
+      if (std::fabs(G[(size_t)i * k + j]) > std::fabs(G[(size_t)p * k + j])) p = i;
+    if (G[(size_t)p * k + j] == 0.0) return false;
+    if (p != j) {
+      for (int c = 0; c < k; ++c) std::swap(G[(size_t)p * k + c], G[(size_t)j * k + c]);
+      std::swap(m[p], m[j]);
+    }
+    for (int i = j + 1; i < k; ++i) {
+      const double f = G[(size_t)i * k + j] / G[(size_t)j * k + j];
+      for (int c = j; c < k; ++c) G[(size_t)i * k + c] -= f * G[(size_t)j * k + c];
+      m[i] -= f * m[j];
+    }
+  }
+  for (int j = k - 1; j >= 0; --j) {
+    double v = m[j];
+    for (int c = j + 1; c < k; ++c) v -= G[(size_t)j * k + c] * m[c];
+    m[j] = v / G[(size_t)j * k + j];
+  }
+  return true;
+}
+
+}  // namespace
+
+void spai1_values(const CSR& A, std::vector<double>& M) {
+  const int n = A.n;
+  M.assign(A.v.size(), 0.0);
+  // rows of each column, ascending (the transpose pattern)
+  std::vector<int> cp(n + 1, 0), cr(A.ci.size());
+  for (int c : A.ci) ++cp[c + 1];
+  for (int j = 0; j < n; ++j) cp[j + 1] += cp[j];
+  {
+    std::vector<int> f(cp.begin(), cp.end() - 1);
+    for (int r = 0; r < n; ++r)
+      for (int k = A.rp[r]; k < A.rp[r + 1]; ++k) cr[f[A.ci[k]]++] = r;
+  }
+#pragma omp parallel
+  {
+    std::vector<int> loc(n, -1), rows;
+    std::vector<double> G, rhs, m;
+#pragma omp for schedule(dynamic, 256)
+    for (int i = 0; i < n; ++i) {
+      const int rs = A.rp[i], k = A.rp[i + 1] - rs;
+      if (k == 0) continue;
+      for (int p = 0; p < k; ++p) loc[A.ci[rs + p]] = p;
+      rows.clear();
+      for (int p = 0; p < k; ++p) {
+        const int c = A.ci[rs + p];
+        rows.insert(rows.end(), cr.begin() + cp[c], cr.begin() + cp[c + 1]);
+      }
+      std::sort(rows.begin(), rows.end());
+      rows.erase(std::unique(rows.begin(), rows.end()), rows.end());
+      G.assign((size_t)k * k, 0.0);
+      for (int r : rows) {
+        for (int a = A.rp[r]; a < A.rp[r + 1]; ++a) {
+          const int p = loc[A.ci[a]];
+          if (p < 0) continue;
+          const double vp = A.v[a];
+          for (int b = A.rp[r]; b < A.rp[r + 1]; ++b) {
+            const int q = loc[A.ci[b]];
+            if (q >= 0) G[(size_t)p * k + q] += vp * A.v[b];
+          }
+        }
+      }
+      rhs.assign(A.v.begin() + rs, A.v.begin() + rs + k);
+      for (int p = 0; p < k; ++p) {
+        double& g = G[(size_t)p * k + p];
+        g += kEps * std::max(1.0, std::fabs(g));
+      }
+      std::vector<double> G2 = G;
+      if (!cholesky_solve(k, G, rhs, m) && !lu_solve_small(k, G2, rhs, m)) m.assign(k, 0.0);
+      for (int p = 0; p < k; ++p) M[rs + p] = m[p];
+      for (int p = 0; p < k; ++p) loc[A.ci[rs + p]] = -1;
+    }
+  }
+}
+
+namespace {
+
 // Normalised start vector of the Chebyshev power iteration: standard normal
 // entries (Box-Muller on splitmix64 uniforms), divided by their 2-norm.
 std::vector<double> chebyshev_start(int n, uint64_t seed) {
@@ -548,6 +666,10 @@ void build_smoother(HostLevel& L, const Config& cfg, int level) {
     case SmootherKind::SPAI0:  // x + m (b - A x): the Jacobi sweep with omega = 1
       spai0_diagonal(L.A, L.invdiag);
       L.omega = 1.0;
+      break;
+    case SmootherKind::SPAI1:  // build_spai1_smoother, smoothers.jl:598-607
+      spai1_values(L.A, L.spai1_M);
+      inverse_diagonal(L.A, L.invdiag);  // not used by the sweep; kept for exports
       break;
     case SmootherKind::SerialGS:   // build_serial_gs_smoother, smoothers.jl:370-376
     case SmootherKind::L1SerialGS:  // build_l1_serial_gs_smoother, :428-434
@@ -586,8 +708,8 @@ void build_smoother(HostLevel& L, const Config& cfg, int level) {
       break;
     default:
       fail("smoother \"" + smoother_name(cfg.smoother) +
-           "\" is not supported by the B200 build (use jacobi, l1_jacobi, spai0, chebyshev, "
-           "ilu0, serial_ilu0, colored_gs, l1_colored_gs, serial_gs or l1_serial_gs)");
+           "\" is not supported by the B200 build (use jacobi, l1_jacobi, spai0, spai1, "
+           "chebyshev, ilu0, serial_ilu0, colored_gs, l1_colored_gs, serial_gs or l1_serial_gs)");
   }
 }
 
@@ -601,12 +723,12 @@ void build_hierarchy(const CSR& A_in, const Config& cfg, bool allow_partial_rese
   switch (cfg.smoother) {
     case SmootherKind::Jacobi: case SmootherKind::L1Jacobi: case SmootherKind::SPAI0:
     case SmootherKind::Chebyshev: case SmootherKind::ILU0: case SmootherKind::SerialILU0:
-    case SmootherKind::SerialGS: case SmootherKind::L1SerialGS:
+    case SmootherKind::SerialGS: case SmootherKind::L1SerialGS: case SmootherKind::SPAI1:
     case SmootherKind::ColoredGS: case SmootherKind::L1ColoredGS: break;
     default:
       fail("smoother \"" + smoother_name(cfg.smoother) +
-           "\" is not supported by the B200 build (use jacobi, l1_jacobi, spai0, chebyshev, "
-           "ilu0, serial_ilu0, colored_gs, l1_colored_gs, serial_gs or l1_serial_gs)");
+           "\" is not supported by the B200 build (use jacobi, l1_jacobi, spai0, spai1, "
+           "chebyshev, ilu0, serial_ilu0, colored_gs, l1_colored_gs, serial_gs or l1_serial_gs)");
   }
   H = HostHierarchy();
   H.cfg = cfg;

@@ -169,6 +169,9 @@ struct HostLevel {
   // Serial and l1 serial Gauss-Seidel (src/smoothers.jl:318-491): rows by
   // level of the sweep's dependencies, level offsets.
   std::vector<int> sgs_order, sgs_off;
+  // SPAI(1) (src/smoothers.jl:586-760): the approximate inverse M on A's
+  // pattern.
+  std::vector<double> spai1_M;
 };
 
 struct HostHierarchy {
@@ -259,6 +262,13 @@ void serial_gs_levels(const CSR& A, std::vector<int>& order, std::vector<int>& o
 // _serial_gs_compute_invdiag! (smoothers.jl:329-340): 1/a_ii (the first
 // diagonal entry of the row), 0 when |a_ii| <= eps.
 void serial_gs_inverse_diagonal(const CSR& A, std::vector<double>& invd);
+// _compute_spai1! (smoothers.jl:620-690): per row i, the Gram matrix
+// G_pq = sum_r a_r,Jp a_r,Jq over the rows r touching the row's columns J
+// (ascending r, as the reference's loop over all rows), the right-hand side
+// a_i,J, G_pp += eps max(1, |G_pp|), and G m = rhs (Cholesky, as Julia's
+// `\` factorises a symmetric positive definite matrix; partial-pivoting LU
+// if that breaks down).  The values of M on A's pattern.
+void spai1_values(const CSR& A, std::vector<double>& M);
 void csr_to_dense(const CSR& A, std::vector<double>& M);            // setup.jl:495-516
 void dense_lu(int n, std::vector<double>& lu, std::vector<int>& piv);
 

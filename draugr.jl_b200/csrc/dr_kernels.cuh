@@ -298,6 +298,32 @@ struct EpCheby {
   }
 };
 
+// The two passes of a SPAI(1) step (src/smoothers.jl:709-760): r = b -
+// a_i1 x_1 - ... (from b, in column order), then x_i += (M_i1 r_1 + ...)
+// (the sum formed from zero, then added).
+template <typename T>
+struct EpResidualSub {
+  using acc_t = T;
+  static constexpr int kSign = -1;
+  struct Pre { T b; };
+  const T* __restrict__ b;
+  T* __restrict__ r;
+  __device__ __forceinline__ Pre pre(int i) const { return {__ldg(b + i)}; }
+  __device__ __forceinline__ T init(const Pre& p) const { return p.b; }
+  __device__ __forceinline__ double apply(int i, T v, const Pre&) const { r[i] = v; return 0.0; }
+};
+
+template <typename T>
+struct EpAddSum {
+  using acc_t = T;
+  static constexpr int kSign = 1;
+  struct Pre { T x; };
+  T* __restrict__ x;
+  __device__ __forceinline__ Pre pre(int i) const { return {x[i]}; }
+  __device__ __forceinline__ T init(const Pre&) const { return T(0); }
+  __device__ __forceinline__ double apply(int i, T v, const Pre& p) const { x[i] = add_rn(p.x, v); return 0.0; }
+};
+
 // One power step of the spectral-radius estimate of D^-1 A
 // (src/smoothers.jl:876-880): w = (A v) invd, returning w_i^2 for ||w||.
 struct EpPowerStep {

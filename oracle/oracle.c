@@ -34,8 +34,8 @@ typedef struct {
   const int *P_rp, *P_ci;
   const double *P_v;
   const int *T_off, *T_rows, *T_pnz;
-  int smoother; /* 0 jacobi, 1 colored_gs, 2 serial_gs, 3 spai0, 5 l1_jacobi, 6 l1_colored_gs,
-                   7 l1_serial_gs, 8 chebyshev, 9 ilu0, 10 serial_ilu0 */
+  int smoother; /* 0 jacobi, 1 colored_gs, 2 serial_gs, 3 spai0, 4 spai1, 5 l1_jacobi,
+                   6 l1_colored_gs, 7 l1_serial_gs, 8 chebyshev, 9 ilu0, 10 serial_ilu0 */
   double omega;
   double *invd;
   int ncolors;
@@ -52,6 +52,8 @@ typedef struct {
   /* ILU(0): diagonal positions and factors on A's pattern */
   const int *ilu_diag;
   double *ilu_L, *ilu_U;
+  /* SPAI(1): M on A's pattern */
+  double *spai1_M;
 } olevel;
 
 typedef struct {
@@ -295,6 +297,126 @@ void orc_ilu0_smooth(int n, const int *rp, const int *ci, const double *a, const
     }
     for (int i = 0; i < n; ++i)
       if (isfinite(t[i])) x[i] += t[i];
+  }
+}
+
+/* G m = r for the small symmetric Gram matrix of SPAI(1) (row-major G,
+ * overwritten): upper Cholesky (potf2 order), else partial-pivoting LU,
+ * else m = 0 (the dense solve of Julia's `\` on a symmetric matrix) */
+static void spai1_solve(int k, double *G, const double *r, double *m) {
+  double *G2 = (double *)malloc(sizeof(double) * (size_t)k * k);
+  memcpy(G2, G, sizeof(double) * (size_t)k * k);
+  int ok = 1;
+  for (int j = 0; j < k && ok; ++j) {
+    double s = G[j * k + j];
+    for (int t = 0; t < j; ++t) s -= G[t * k + j] * G[t * k + j];
+    if (!(s > 0.0)) { ok = 0; break; }
+    double u = sqrt(s);
+    G[j * k + j] = u;
+    for (int l = j + 1; l < k; ++l) {
+      double v = G[j * k + l];
+      for (int t = 0; t < j; ++t) v -= G[t * k + j] * G[t * k + l];
+      G[j * k + l] = v / u;
+    }
+  }
+  if (ok) {
+    for (int j = 0; j < k; ++j) {
+      double v = r[j];
+      for (int t = 0; t < j; ++t) v -= G[t * k + j] * m[t];
+      m[j] = v / G[j * k + j];
+    }
+    for (int j = k - 1; j >= 0; --j) {
+      double v = m[j];
+      for (int t = j + 1; t < k; ++t) v -= G[j * k + t] * m[t];
+      m[j] = v / G[j * k + j];
+    }
+  } else {
+    for (int j = 0; j < k; ++j) m[j] = r[j];
+    for (int j = 0; j < k && !ok; ++j) {
+      int p = j;
+      for (int i = j + 1; i < k; ++i)
+        if (fabs(G2[i * k + j]) > fabs(G2[p * k + j])) p = i;
+      if (G2[p * k + j] == 0.0) { ok = -1; break; }
+      if (p != j) {
+        for (int c = 0; c < k; ++c) { double t = G2[p * k + c]; G2[p * k + c] = G2[j * k + c]; G2[j * k + c] = t; }
+        double t = m[p]; m[p] = m[j]; m[j] = t;
+      }
+      for (int i = j + 1; i < k; ++i) {
+        double f = G2[i * k + j] / G2[j * k + j];
+        for (int c = j; c < k; ++c) G2[i * k + c] -= f * G2[j * k + c];
+        m[i] -= f * m[j];
+      }
+    }
+    if (ok == -1) {
+      for (int j = 0; j < k; ++j) m[j] = 0.0;
+    } else {
+      for (int j = k - 1; j >= 0; --j) {
+        double v = m[j];
+        for (int c = j + 1; c < k; ++c) v -= G2[j * k + c] * m[c];
+        m[j] = v / G2[j * k + j];
+      }
+    }
+  }
+  free(G2);
+}
+
+/* position of column c in row i's columns J (k entries), or -1 (the
+ * reference's col_to_local map) */
+static int spai1_local(const int *J, int k, int c) {
+  for (int p = 0; p < k; ++p)
+    if (J[p] == c) return p;
+  return -1;
+}
+
+/* _compute_spai1!, src/smoothers.jl:620-690, loop for loop: for each row i
+ * with columns J, every row r of A (in order) adds a_rp a_rq to G_pq for
+ * its entries in J; rhs_p = a_i,Jp; G_pp += eps max(1, |G_pp|); m = G \ rhs
+ * stored on row i's entries. */
+void orc_spai1(int n, const int *rp, const int *ci, const double *a, double *M) {
+  for (int i = 0; i < n; ++i) {
+    const int rs = rp[i], k = rp[i + 1] - rs;
+    if (k == 0) continue;
+    const int *J = ci + rs;
+    double *G = (double *)calloc((size_t)k * k, sizeof(double));
+    double *rhs = (double *)malloc(sizeof(double) * (size_t)k);
+    double *m = (double *)malloc(sizeof(double) * (size_t)k);
+    for (int r = 0; r < n; ++r) /* every row, in order */
+      for (int e1 = rp[r]; e1 < rp[r + 1]; ++e1) {
+        const int p = spai1_local(J, k, ci[e1]);
+        if (p < 0) continue;
+        for (int e2 = rp[r]; e2 < rp[r + 1]; ++e2) {
+          const int q = spai1_local(J, k, ci[e2]);
+          if (q >= 0) G[p * k + q] += a[e1] * a[e2];
+        }
+      }
+    for (int p = 0; p < k; ++p) rhs[p] = a[rs + p];
+    for (int p = 0; p < k; ++p) {
+      const double g = fabs(G[p * k + p]);
+      G[p * k + p] += 2.220446049250313e-16 * (g > 1.0 ? g : 1.0);
+    }
+    spai1_solve(k, G, rhs, m);
+    for (int p = 0; p < k; ++p) M[rs + p] = m[p];
+    free(G);
+    free(rhs);
+    free(m);
+  }
+}
+
+/* smooth!(::SPAI1Smoother), src/smoothers.jl:709-760: per step r = b - A x
+ * (from b, column order), then x_i += sum_j M_ij r_j (summed from zero) */
+void orc_spai1_smooth(int n, const int *rp, const int *ci, const double *a, const double *M, double *x,
+                      const double *b, int steps, double *r) {
+  for (int s = 0; s < steps; ++s) {
+    for (int i = 0; i < n; ++i) {
+      double ri = b[i];
+      for (int nz = rp[i]; nz < rp[i + 1]; ++nz) ri -= a[nz] * x[ci[nz]];
+      r[i] = ri;
+    }
+    for (int i = 0; i < n; ++i) {
+      double v = 0.0;
+      for (int nz = rp[i]; nz < rp[i + 1]; ++nz) v += M[nz] * r[ci[nz]];
+      x[i] += v;
+    }
   }
 }
 
@@ -670,6 +792,8 @@ static void smooth(olevel *L, double *x, const double *b, int steps) {
                   L->tmp, L->cheb_d);
   else if (L->smoother == 2 || L->smoother == 7)
     orc_serial_gs(L->n, L->A_rp, L->A_ci, L->A_v, L->invd, x, b, steps);
+  else if (L->smoother == 4)
+    orc_spai1_smooth(L->n, L->A_rp, L->A_ci, L->A_v, L->spai1_M, x, b, steps, L->tmp);
   else if (L->smoother == 9 || L->smoother == 10)
     orc_ilu0_smooth(L->n, L->A_rp, L->A_ci, L->A_v, L->ilu_diag, L->ilu_L, L->ilu_U, x, b, steps, L->tmp);
   else
@@ -807,6 +931,8 @@ static void upd_invd(olevel *L) {
   else if (L->smoother == 2) orc_serial_gs_invdiag(L->n, L->A_rp, L->A_ci, L->A_v, L->invd);
   else if (L->smoother == 3) orc_spai0(L->n, L->A_rp, L->A_ci, L->A_v, L->invd);
   else orc_invdiag(L->n, L->A_rp, L->A_ci, L->A_v, L->invd);
+  if (L->smoother == 4) /* update_smoother!(::SPAI1Smoother), src/smoothers.jl:692-699 */
+    orc_spai1(L->n, L->A_rp, L->A_ci, L->A_v, L->spai1_M);
   if (L->smoother == 9 || L->smoother == 10) /* update_smoother!, src/smoothers.jl:1332-1337 */
     orc_ilu0_factor(L->n, L->A_rp, L->A_ci, L->A_v, L->ilu_diag, L->ilu_L, L->ilu_U);
   if (L->smoother == 8) { /* update_smoother!(::ChebyshevSmoother), src/smoothers.jl:912-922 */

@@ -50,7 +50,7 @@ class OLevel(C.Structure):
                 ("color_off", P), ("color_order", P), ("r", P), ("xc", P), ("bc", P),
                 ("tmp", P), ("nz_off", P), ("tpi", P), ("tai", P), ("tpj", P),
                 ("cheb_degree", i32), ("cheb_v0", P), ("cheb_coef", P), ("cheb_d", P),
-                ("ilu_diag", P), ("ilu_L", P), ("ilu_U", P)]
+                ("ilu_diag", P), ("ilu_L", P), ("ilu_U", P), ("spai1_M", P)]
 
 
 class OHier(C.Structure):
@@ -70,6 +70,8 @@ def _declare(lib):
         "orc_cheb_coef": (None, [f64, i32, P]),
         "orc_ilu0_factor": (None, [i32, P, P, P, P, P, P]),
         "orc_serial_gs_invdiag": (None, [i32, P, P, P, P]),
+        "orc_spai1": (None, [i32, P, P, P, P]),
+        "orc_spai1_smooth": (None, [i32, P, P, P, P, P, P, i32, P]),
         "orc_serial_gs": (None, [i32, P, P, P, P, P, P, i32]),
         "orc_ilu0_smooth": (None, [i32, P, P, P, P, P, P, P, P, i32, P]),
         "orc_chebyshev": (None, [i32, P, P, P, P, P, i32, P, P, i32, P, P]),
@@ -162,6 +164,23 @@ def cheb_coef(rho, degree=3):
     c = np.zeros(2 * degree)
     load().orc_cheb_coef(float(rho), degree, ptr(c))
     return c
+
+
+def spai1(n, rp, ci, v):
+    """SPAI(1) values of M on A's pattern (_compute_spai1!, the reference's
+    loop over every row for every row: small cases only)."""
+    M = np.zeros(len(ci))
+    load().orc_spai1(n, ptr(rp), ptr(ci), ptr(v), ptr(M))
+    return M
+
+
+def spai1_smooth(n, rp, ci, v, M, x, b, steps):
+    """`steps` SPAI(1) steps x <- x + M (b - A x) (smooth!(::SPAI1Smoother))."""
+    x = np.array(x, dtype=np.float64)
+    r = np.zeros(n)
+    load().orc_spai1_smooth(n, ptr(rp), ptr(ci), ptr(v), ptr(np.ascontiguousarray(M, np.float64)), ptr(x),
+                            ptr(np.ascontiguousarray(b, np.float64)), steps, ptr(r))
+    return x
 
 
 def serial_gs_invdiag(n, rp, ci, v):
@@ -298,7 +317,7 @@ def strength_abs(n, rp, ci, v, theta):
 
 
 # ---------------------------------------------------------------- hierarchy mirror
-SMOOTHER_KIND = {0: "jacobi", 1: "colored_gs", 2: "serial_gs", 3: "spai0", 5: "l1_jacobi",
+SMOOTHER_KIND = {0: "jacobi", 1: "colored_gs", 2: "serial_gs", 3: "spai0", 4: "spai1", 5: "l1_jacobi",
                  6: "l1_colored_gs", 7: "l1_serial_gs", 8: "chebyshev", 9: "ilu0", 10: "serial_ilu0"}
 
 
@@ -339,6 +358,9 @@ class OracleHierarchy:
                          cheb_d=np.zeros(n))
                 L.cheb_degree = len(d["cheb_coef"]) // 2
                 L.cheb_v0, L.cheb_coef, L.cheb_d = ptr(d["cheb_v0"]), ptr(d["cheb_coef"]), ptr(d["cheb_d"])
+            if sk == 4:
+                d.update(spai1_M=h.export(l, "spai1_M").copy())
+                L.spai1_M = ptr(d["spai1_M"])
             if sk in (9, 10):
                 d.update(ilu_diag=h.export(l, "ilu_diag"), ilu_L=h.export(l, "ilu_L").copy(),
                          ilu_U=h.export(l, "ilu_U").copy())

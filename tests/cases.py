@@ -31,6 +31,9 @@ CASES = {
                                                smoother=draugr.SerialGaussSeidelType())),
     "hmis_l1_serial_gs": (lambda: problems.heterogeneous_diffusion_3d(10, seed=11),
                           draugr.AMGConfig(smoother=draugr.L1SerialGaussSeidelType())),
+    "aggregation_spai1": (lambda: problems.poisson2d(16),
+                          draugr.AMGConfig(coarsening=draugr.AggregationCoarsening(0.25),
+                                           smoother=draugr.SPAI1SmootherType())),
     "aniso27_hmis": (lambda: problems.anisotropic_27pt(9, 1e-3),
                      draugr.AMGConfig(coarsening=draugr.HMISCoarsening(
                          0.25, draugr.ExtendedIInterpolation(0.2)),

@@ -91,8 +91,8 @@ def test_index_base_and_validation(lib):
     bad[3] = n + 5
     assert lib.draugr_b200_setup_host(n, len(ci), p(rp), p(bad), p(v), cfg, 0, 1) == -1
     assert "column index out of range" in draugr.last_error()
-    # unsupported smoother fails with a clear message
-    cfg2 = draugr.config_handle(draugr.AMGConfig(smoother=draugr.SPAI1SmootherType()))
+    # an unsupported choice (RS coarsening) fails with a clear message
+    cfg2 = draugr.config_handle(draugr.AMGConfig(coarsening=draugr.RSCoarsening()))
     assert lib.draugr_b200_setup_host(n, len(ci), p(rp), p(ci), p(v), cfg2, 0, 1) == -1
     assert "not supported" in draugr.last_error()
 
@@ -139,6 +139,9 @@ def test_structure_matches_oracle(host_case):
         if kind == 3:  # SPAI(0): m_i = a_ii / sum a_ij^2, swept with omega = 1
             inv = oracle.spai0(n, arp, aci, av)
             assert h.export(l, "omega")[0] == 1.0
+        elif kind == 4:  # SPAI(1): M on A's pattern, against the reference's loop
+            inv = oracle.invdiag(n, arp, aci, av)
+            assert np.array_equal(oracle.spai1(n, arp, aci, av), h.export(l, "spai1_M"))
         elif kind in (2, 7):  # serial (l1) Gauss-Seidel: diagonal and sweep schedule
             inv = oracle.serial_gs_invdiag(n, arp, aci, av) if kind == 2 else oracle.invdiag(n, arp, aci, av, l1=True)
             order, off = h.export(l, "sgs_order"), h.export(l, "sgs_offsets")

@@ -67,6 +67,8 @@ def test_level_kernels(case):
                 ref = oracle.spai0_smooth(n, d["A_rp"], d["A_ci"], d["A_v"], d["invd"], x, b, steps)
             elif L.smoother == 8:
                 ref = oracle.chebyshev(n, d["A_rp"], d["A_ci"], d["A_v"], d["invd"], d["cheb_coef"], x, b, steps)
+            elif L.smoother == 4:
+                ref = oracle.spai1_smooth(n, d["A_rp"], d["A_ci"], d["A_v"], d["spai1_M"], x, b, steps)
             elif L.smoother in (2, 7):
                 ref = oracle.serial_gs(n, d["A_rp"], d["A_ci"], d["A_v"], d["invd"], x, b, steps)
             elif L.smoother in (9, 10):
@@ -173,6 +175,8 @@ def test_resetup_matches_reference_galerkin(case):
         assert rel(h.export(l, "invdiag"), O.levels_np[l]["invd"]) < TOL64
         if "cheb_coef" in O.levels_np[l]:  # spectral radius and coefficients redone on the device
             assert rel(h.export(l, "cheb_coef"), O.levels_np[l]["cheb_coef"]) < TOL64
+        if "spai1_M" in O.levels_np[l]:  # M recomputed from the level's new values
+            assert rel(h.export(l, "spai1_M"), O.levels_np[l]["spai1_M"]) < TOL64
         if "ilu_L" in O.levels_np[l]:  # refactorised from the level's new values
             assert rel(h.export(l, "ilu_L"), O.levels_np[l]["ilu_L"]) < TOL64
             assert rel(h.export(l, "ilu_U"), O.levels_np[l]["ilu_U"]) < TOL64

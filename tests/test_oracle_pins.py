@@ -171,6 +171,29 @@ def test_chebyshev_build_smoothing_solve_and_resetup():
             assert it < 200 and np.linalg.norm(b - 2.0 * (A @ x)) / np.linalg.norm(b) < 1e-8
 
 
+def test_spai1_build_smoothing_and_solve():
+    """testsets "SPAI1 Smoother - Build / Smoothing" and "AMG Solve - SPAI1"
+    (test/runtests.jl:793-823): M has nnz(A) entries; 10 steps reduce the
+    residual; amg_solve! with V(2,2) SPAI(1) reaches 1e-8 in fewer than 300
+    cycles on the 10 x 10 Poisson matrix."""
+    A = problems.poisson1d(5)
+    n, rp, ci, v = parts(A)
+    assert len(oracle.spai1(n, rp, ci, v)) == A.nnz
+    A = problems.poisson1d(10)
+    n, rp, ci, v = parts(A)
+    M = oracle.spai1(n, rp, ci, v)
+    b = np.ones(n)
+    x = oracle.spai1_smooth(n, rp, ci, v, M, np.zeros(n), b, 10)
+    assert np.linalg.norm(b - A @ x) < np.linalg.norm(b)
+    A = problems.poisson2d(10)
+    b = np.random.default_rng(6).uniform(0, 1, 100)
+    cfg = draugr.AMGConfig(smoother=draugr.SPAI1SmootherType(), pre_smoothing_steps=2, post_smoothing_steps=2)
+    h = draugr.amg_setup(A, cfg, on_device=False)
+    O = oracle.OracleHierarchy(h)
+    x, it, rel = O.solve(np.zeros(100), b, 2, 2, False, 1e-8, 300)
+    assert it < 300 and np.linalg.norm(b - A @ x) / np.linalg.norm(b) < 1e-8
+
+
 @pytest.mark.parametrize("l1", [False, True])
 def test_serial_gs_build_smoothing_and_solve(l1):
     """testsets "Serial GS Smoother" and "L1 Serial GS Smoother" (test/
