@@ -375,6 +375,7 @@ int64_t draugr_b200_export(int32_t handle, int32_t lvl, const char* what, void* 
       else if (w == "ilu_bwd_offsets") iv = &L.ilu_bwd_off;
       else if (w == "spai1_M") dv = &L.spai1_M;
       else if (w == "sgs_order") iv = &L.sgs_order;
+      else if (w == "cf") iv = &L.cf;
       else if (w == "sgs_offsets") iv = &L.sgs_off;
       else if (w == "AP_nzval") {
         if (!H->dev) fail("AP_nzval lives on the device only");

@@ -473,6 +473,75 @@ static void ensure_fine_have_coarse_neighbor(std::vector<int>& cf, const CSR& A,
   }
 }
 
+void coarsen_rs(const CSR& A, double theta, std::vector<int>& cf, std::vector<int>& cmap, int& nc) {
+  const int n = A.n;
+  if (n <= 1) {
+    cf.assign(n, 1);
+    build_cmap(cf, cmap, nc);
+    return;
+  }
+  const std::vector<uint8_t> st = strength_absolute(A, theta);
+  std::vector<int> lam = strong_transpose_count(A, st);
+  std::vector<int> off, src;
+  strong_transpose_adj(A, st, off, src);
+  cf.assign(n, 0);  // 0 undecided, 1 C, -1 F
+  for (int i = 0; i < n; ++i)
+    if (!has_strong_nbr(A, st, i) && lam[i] == 0) cf[i] = 1;  // isolated
+  // buckets of undecided points by lambda: doubly linked lists, new members
+  // at the head
+  int top = 0;
+  for (int v : lam) top = std::max(top, v);
+  std::vector<int> head(std::max(top + 1, n), -1), next(n, -1), prev(n, -1);
+  auto push = [&](int i) {
+    const int k = lam[i];
+    if (k >= (int)head.size()) head.resize(k + 1, -1);
+    next[i] = head[k];
+    prev[i] = -1;
+    if (head[k] >= 0) prev[head[k]] = i;
+    head[k] = i;
+  };
+  auto remove = [&](int i) {
+    const int k = lam[i];
+    if (prev[i] >= 0) next[prev[i]] = next[i];
+    else head[k] = next[i];
+    if (next[i] >= 0) prev[next[i]] = prev[i];
+    next[i] = prev[i] = -1;
+  };
+  auto update = [&](int i, int v) {
+    remove(i);
+    lam[i] = v;
+    push(i);
+  };
+  for (int i = 0; i < n; ++i)
+    if (cf[i] == 0) push(i);
+  while (true) {
+    while (top >= 0 && head[top] < 0) --top;
+    if (top < 0) break;
+    const int best = head[top];
+    remove(best);
+    cf[best] = 1;
+    for (int q = off[best]; q < off[best + 1]; ++q) {  // points depending on best become F
+      const int j = src[q];
+      if (cf[j] != 0) continue;
+      remove(j);
+      cf[j] = -1;
+      for (int k = A.rp[j]; k < A.rp[j + 1]; ++k) {  // their strong influences gain weight
+        const int c = A.ci[k];
+        if (c != j && st[k] && cf[c] == 0) {
+          update(c, lam[c] + 1);
+          top = std::max(top, lam[c]);
+        }
+      }
+    }
+    for (int k = A.rp[best]; k < A.rp[best + 1]; ++k) {  // best's strong influences lose weight
+      const int c = A.ci[k];
+      if (c != best && st[k] && cf[c] == 0) update(c, std::max(0, lam[c] - 1));
+    }
+  }
+  ensure_fine_have_coarse_neighbor(cf, A, st);
+  build_cmap(cf, cmap, nc);
+}
+
 void coarsen_aggressive_cf(const CSR& A_in, double theta, bool base_hmis, const Config& cfg,
                            uint64_t& rng, std::vector<int>& cf, std::vector<int>& cmap,
                            int& nc) {

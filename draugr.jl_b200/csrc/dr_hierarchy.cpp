@@ -323,28 +323,25 @@ void dense_lu(int n, std::vector<double>& a, std::vector<int>& piv) {
 // ------------------------------------------------------------ level loop
 namespace {
 
-bool uses_cf(CoarsenKind k) {
-  return k == CoarsenKind::PMIS || k == CoarsenKind::HMIS || k == CoarsenKind::RS;
-}
-
+// cf receives the C/F splitting (empty for aggregation).
 void coarsen_and_build_p(const CSR& A, const Coarsening& alg, const Config& cfg, uint64_t& rng,
-                         Prolong& P, int& nc) {
-  std::vector<int> cf, cmap;
+                         Prolong& P, int& nc, std::vector<int>& cf) {
+  std::vector<int> cmap;
+  cf.clear();
   switch (alg.kind) {
     case CoarsenKind::PMIS:
-    case CoarsenKind::HMIS: {
+    case CoarsenKind::HMIS:
+    case CoarsenKind::RS: {  // coarsen_cf (coarsening.jl:1157-1187)
       CSR Aw;
       const CSR* Ap = &A;
       if (cfg.max_row_sum < 1.0) { Aw = apply_max_row_sum(A, cfg.max_row_sum); Ap = &Aw; }
       if (alg.kind == CoarsenKind::PMIS) coarsen_pmis(*Ap, alg.theta, rng, cf, cmap, nc);
-      else coarsen_hmis(*Ap, alg.theta, rng, cf, cmap, nc);
+      else if (alg.kind == CoarsenKind::HMIS) coarsen_hmis(*Ap, alg.theta, rng, cf, cmap, nc);
+      else coarsen_rs(*Ap, alg.theta, cf, cmap, nc);
       P = build_interpolation(A, cf, cmap, nc, alg.interp, alg.theta);
       if (alg.interp.trunc_factor > 0) P = truncate_interpolation(P, alg.interp.trunc_factor);
       return;
     }
-    case CoarsenKind::RS:
-      fail("RS coarsening is not supported by the B200 build (use hmis, pmis, aggressive_hmis, "
-           "aggressive_pmis, aggregation or smoothed_aggregation)");
     case CoarsenKind::AggressivePMIS:
     case CoarsenKind::AggressiveHMIS: {
       coarsen_aggressive_cf(A, alg.theta, alg.kind == CoarsenKind::AggressiveHMIS, cfg, rng, cf,
@@ -367,17 +364,18 @@ void coarsen_and_build_p(const CSR& A, const Coarsening& alg, const Config& cfg,
 }
 
 void coarsen_with_fallback(const CSR& A, const Coarsening& alg, const Config& cfg, uint64_t& rng,
-                           Prolong& P, int& nc) {
+                           Prolong& P, int& nc, std::vector<int>& cf) {
   const int n = A.n;
-  coarsen_and_build_p(A, alg, cfg, rng, P, nc);
+  coarsen_and_build_p(A, alg, cfg, rng, P, nc, cf);
   if (nc < 0.8 * n || n <= cfg.max_coarse_size) return;
   for (int attempt = 1; attempt <= 3; ++attempt) {
     Coarsening red = alg;
     red.theta = alg.theta * std::pow(0.5, attempt);
     Prolong P2;
     int nc2 = 0;
-    coarsen_and_build_p(A, red, cfg, rng, P2, nc2);
-    if (nc2 < nc) { P = std::move(P2); nc = nc2; }
+    std::vector<int> cf2;
+    coarsen_and_build_p(A, red, cfg, rng, P2, nc2, cf2);
+    if (nc2 < nc) { P = std::move(P2); nc = nc2; cf = std::move(cf2); }
     if (nc < 0.8 * n) break;
   }
 }
@@ -741,10 +739,12 @@ void build_hierarchy(const CSR& A_in, const Config& cfg, bool allow_partial_rese
     const Coarsening& alg = lvl <= cfg.initial_coarsening_levels ? cfg.initial_coarsening : cfg.coarsening;
     Prolong P;
     int nc = 0;
-    coarsen_with_fallback(cur, alg, cfg, rng, P, nc);
+    std::vector<int> cf;
+    coarsen_with_fallback(cur, alg, cfg, rng, P, nc, cf);
     if (nc >= n) break;
     if (nc == 0) break;
     HostLevel L;
+    L.cf = std::move(cf);
     L.T = build_transpose_map(P);
     L.Rv.resize(P.nnz());
     for (size_t k = 0; k < L.T.pnz.size(); ++k) L.Rv[k] = P.v[L.T.pnz[k]];

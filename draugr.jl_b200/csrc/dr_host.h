@@ -172,6 +172,9 @@ struct HostLevel {
   // SPAI(1) (src/smoothers.jl:586-760): the approximate inverse M on A's
   // pattern.
   std::vector<double> spai1_M;
+  // C/F splitting of the level (1 coarse, -1 fine) for splitting-based
+  // coarsening; empty for aggregation.
+  std::vector<int> cf;
 };
 
 struct HostHierarchy {
@@ -198,6 +201,12 @@ void coarsen_pmis(const CSR& A, double theta, uint64_t& rng, std::vector<int>& c
                   std::vector<int>& cmap, int& nc);
 void coarsen_hmis(const CSR& A, double theta, uint64_t& rng, std::vector<int>& cf,
                   std::vector<int>& cmap, int& nc);
+// coarsen_rs (coarsening.jl:660-810): classical Ruge-Stueben splitting --
+// isolated points coarse, then the greedy first pass over buckets of the
+// measure lambda (points strongly depending on each point; the most
+// recently bucketed point of the highest bucket first), then every F-point
+// given a strong C-neighbour.  Deterministic.
+void coarsen_rs(const CSR& A, double theta, std::vector<int>& cf, std::vector<int>& cmap, int& nc);
 void coarsen_aggressive_cf(const CSR& A, double theta, bool base_hmis, const Config& cfg,
                            uint64_t& rng, std::vector<int>& cf, std::vector<int>& cmap,
                            int& nc);

@@ -283,7 +283,7 @@ class Hierarchy:
                           "T_pnz", "colors", "color_order", "color_offsets", "AP_rowptr",
                           "AP_colval", "C_rowptr", "C_colval", "C_piv", "ilu_diag", "ilu_fwd_order",
                           "ilu_fwd_offsets", "ilu_bwd_order", "ilu_bwd_offsets", "sgs_order",
-                          "sgs_offsets")
+                          "sgs_offsets", "cf")
         out = np.zeros(cnt, dtype=np.int32 if is_int else np.float64)
         _lib.check(lib.draugr_b200_export(self.handle, lvl, what.encode(), _ptr(out), cnt),
                    f"export {what}")

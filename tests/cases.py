@@ -34,6 +34,9 @@ CASES = {
     "aggregation_spai1": (lambda: problems.poisson2d(16),
                           draugr.AMGConfig(coarsening=draugr.AggregationCoarsening(0.25),
                                            smoother=draugr.SPAI1SmootherType())),
+    "rs_direct_l1jacobi": (lambda: problems.heterogeneous_diffusion_3d(10, seed=13),
+                           draugr.AMGConfig(coarsening=draugr.RSCoarsening(0.25, draugr.DirectInterpolation()),
+                                            smoother=draugr.L1JacobiSmootherType())),
     "aniso27_hmis": (lambda: problems.anisotropic_27pt(9, 1e-3),
                      draugr.AMGConfig(coarsening=draugr.HMISCoarsening(
                          0.25, draugr.ExtendedIInterpolation(0.2)),

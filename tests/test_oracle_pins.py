@@ -171,6 +171,47 @@ def test_chebyshev_build_smoothing_solve_and_resetup():
             assert it < 200 and np.linalg.norm(b - 2.0 * (A @ x)) / np.linalg.norm(b) < 1e-8
 
 
+def _check_rs_splitting(A, cf, nc):
+    """Every point C or F, nc = number of C-points, 0 < nc < n, and every
+    F-point with a strong C-neighbour (the checks of the reference's RS
+    testsets)."""
+    n, rp, ci, v = parts(A)
+    assert len(cf) == n and np.all(np.abs(cf) == 1)
+    assert 0 < nc < n and int(np.sum(cf == 1)) == nc
+    st = oracle.strength_abs(n, rp, ci, v, 0.25)
+    for i in range(n):
+        if cf[i] == -1:
+            row = range(rp[i], rp[i + 1])
+            assert any(ci[k] != i and st[k] and cf[ci[k]] == 1 for k in row), i
+
+
+def test_rs_coarsening():
+    """testsets "RS Coarsening - Basic / 2D / larger system / Solve /
+    Standard Interpolation / Good coarsening ratios" (test/runtests.jl:
+    1254-1334, :2567-2590): valid splittings of the 1D (20) and 2D (10 x 10,
+    30 x 30) Laplacians; amg_solve! with V(2,2) reaches 1e-8 in fewer than
+    200 cycles with direct and standard interpolation; every level of the
+    30 x 30 hierarchy is smaller than the one above."""
+    for A in (problems.poisson1d(20), problems.poisson2d(10), problems.poisson2d(30)):
+        cfg = draugr.AMGConfig(coarsening=draugr.RSCoarsening(0.25), max_coarse_size=2)
+        h = draugr.amg_setup(A, cfg, on_device=False)
+        _check_rs_splitting(A, h.export(0, "cf"), int(h.level_info(0)[2]))
+    A = problems.poisson2d(10)
+    b = np.random.default_rng(7).uniform(0, 1, 100)
+    for interp in (draugr.DirectInterpolation(), draugr.StandardInterpolation()):
+        cfg = draugr.AMGConfig(coarsening=draugr.RSCoarsening(0.25, interp), pre_smoothing_steps=2,
+                               post_smoothing_steps=2)
+        h = draugr.amg_setup(A, cfg, on_device=False)
+        assert h.nlevels >= 1
+        O = oracle.OracleHierarchy(h)
+        x, it, rel = O.solve(np.zeros(100), b, 2, 2, False, 1e-8, 200)
+        assert it < 200 and np.linalg.norm(b - A @ x) / np.linalg.norm(b) < 1e-8
+    h = draugr.amg_setup(problems.poisson2d(30), draugr.AMGConfig(coarsening=draugr.RSCoarsening(0.25)),
+                         on_device=False)
+    sizes = [int(h.level_info(l)[0]) for l in range(h.nlevels)] + [int(h.level_info(-1)[0])]
+    assert all(b < a for a, b in zip(sizes, sizes[1:]))
+
+
 def test_spai1_build_smoothing_and_solve():
     """testsets "SPAI1 Smoother - Build / Smoothing" and "AMG Solve - SPAI1"
     (test/runtests.jl:793-823): M has nnz(A) entries; 10 steps reduce the
