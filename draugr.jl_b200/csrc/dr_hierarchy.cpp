@@ -789,7 +789,9 @@ std::string hierarchy_summary(const HostHierarchy& H, int n_finest) {
   o << "  Levels:          " << nl + 1 << " (" << nl << " AMG + 1 coarse direct)\n";
   o << "  Cycle type:      " << (c.cycle_w ? "W" : "V") << "-cycle\n";
   o << "  Backend:         CUDA (sm_100a)\n";
-  o << "  Coarse solve:    " << (c.coarse_solve_on_cpu ? "CPU (forced)" : "default") << "\n";
+  o << "  Coarse solve:    "
+    << (c.coarse_solve_on_cpu ? "GPU (coarse_solve_on_cpu requested; same LU solve, same values)" : "GPU")
+    << "\n";
   o << "  Strength:        " << (c.strength == StrengthKind::Absolute ? "AbsoluteStrength" : "SignedStrength") << "\n";
   o << "  Coarsening:      " << coarsening_name(c.coarsening) << "\n";
   if (c.initial_coarsening_levels > 0)
