@@ -14,6 +14,8 @@
 // with values in transpose-map order, so no index indirection is needed.
 #include <cuda_runtime.h>
 
+#include <cub/device/device_scan.cuh>
+
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -261,6 +263,7 @@ T* DevHier::alloc(size_t n) {
 template double* DevHier::alloc<double>(size_t);
 template float* DevHier::alloc<float>(size_t);
 template int* DevHier::alloc<int>(size_t);
+template long long* DevHier::alloc<long long>(size_t);
 
 template <typename T>
 static void h2d(T* d, const std::vector<T>& h, cudaStream_t st) {
@@ -1365,7 +1368,69 @@ int DevHier::pcg(double* x, const double* b, const CycleOpts& o, double tol, int
 // entries that holds the output's longest row (longer rows search global
 // memory): 128 and 256 leave room for 8 blocks of 8 warps per SM (the
 // register limit), 384 for 5.
-void DevHier::spgemm(DevMat& O, const DevMat& S, const DevMat& B) {
+// Record the product lists of O = S B (k_spgemm_sym: counts, an exclusive
+// scan into offsets, then the pairs).  They cost 8 bytes per product and
+// are kept only when that is under half of the free device memory; false
+// when they are not built (the warp kernel then stays in use).
+bool DevHier::build_spgemm_list(const DevMat& O, const DevMat& S, const DevMat& B, SpgemmList& L) {
+  L.tried = true;
+  const long long nout = O.nnz;
+  if (nout <= 0 || O.n <= 0) return false;
+  constexpr int W = 8, CAP = 256;
+  const int grid = std::max(1, std::min((O.n + W - 1) / W, max_grid_));
+  int* cnt = nullptr;
+  long long* cnt64 = nullptr;
+  void* tmp = nullptr;
+  size_t tmp_bytes = 0;
+  bool ok = false;
+  DR_CK(cudaMalloc(&cnt, (size_t)nout * sizeof(int)));
+  DR_CK(cudaMalloc(&cnt64, (size_t)(nout + 1) * sizeof(long long)));
+  long long* off = alloc<long long>(nout + 1);
+  DR_CK(cudaMemsetAsync(cnt, 0, (size_t)nout * sizeof(int), st_));
+  counted();
+  k_spgemm_sym<CAP, W, false><<<grid, W * 32, 0, st_>>>(O.n, O.rp, O.ci, S.rp, S.ci, B.rp, B.ci, cnt, nullptr,
+                                                         nullptr, nullptr);
+  DR_CK(cudaGetLastError());
+  // widen the counts (the last one 0) and scan them into the offsets
+  DR_CK(cudaMemsetAsync(cnt64, 0, (size_t)(nout + 1) * sizeof(long long), st_));
+  counted();
+  k_convert<int, long long><<<grid1d(nout, max_grid_), kBlock, 0, st_>>>(nout, cnt, cnt64);
+  DR_CK(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, cnt64, off, nout + 1, st_));
+  DR_CK(cudaMalloc(&tmp, std::max<size_t>(tmp_bytes, 16)));
+  DR_CK(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, cnt64, off, nout + 1, st_));
+  long long total = 0;
+  DR_CK(cudaMemcpyAsync(&total, off + nout, sizeof(long long), cudaMemcpyDeviceToHost, st_));
+  DR_CK(cudaStreamSynchronize(st_));
+  size_t free_b = 0, total_b = 0;
+  DR_CK(cudaMemGetInfo(&free_b, &total_b));
+  if (total > 0 && (size_t)total * 8 < free_b / 2) {
+    L.ls = alloc<int>((size_t)total);
+    L.lb = alloc<int>((size_t)total);
+    DR_CK(cudaMemsetAsync(cnt, 0, (size_t)nout * sizeof(int), st_));
+    counted();
+    k_spgemm_sym<CAP, W, true><<<grid, W * 32, 0, st_>>>(O.n, O.rp, O.ci, S.rp, S.ci, B.rp, B.ci, cnt, off,
+                                                          L.ls, L.lb);
+    DR_CK(cudaGetLastError());
+    L.off = off;
+    L.total = total;
+    ok = true;
+  }
+  DR_CK(cudaStreamSynchronize(st_));
+  DR_CK(cudaFree(tmp));
+  DR_CK(cudaFree(cnt64));
+  DR_CK(cudaFree(cnt));
+  return ok;
+}
+
+void DevHier::spgemm(DevMat& O, const DevMat& S, const DevMat& B, SpgemmList* list) {
+  if (list && !list->tried) build_spgemm_list(O, S, B, *list);
+  if (list && list->off) {
+    counted();
+    k_spgemm_apply<<<grid1d(O.nnz, max_grid_), kBlock, 0, st_>>>(O.nnz, list->off, list->ls, list->lb, S.v, B.v,
+                                                                 O.v);
+    DR_CK(cudaGetLastError());
+    return;
+  }
   constexpr int W = 8;
   counted();
   const int grid = std::max(1, std::min((O.n + W - 1) / W, max_grid_));
@@ -1457,8 +1522,8 @@ void DevHier::resetup_values(const double* v_dev) {
   for (int l = 0; l < nl; ++l) {
     DevLevel& d = L_[l];
     DevMat& next = (l + 1 < nl) ? L_[l + 1].A : C_;
-    spgemm(d.AP, d.A, d.P);
-    spgemm(next, d.R, d.AP);
+    spgemm(d.AP, d.A, d.P, &d.ap_list);
+    spgemm(next, d.R, d.AP, &d.rap_list);
     if (l + 1 < nl) upd_invd(L_[l + 1]);
   }
   // coarsest dense matrix and its LU

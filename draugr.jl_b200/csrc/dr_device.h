@@ -107,6 +107,16 @@ struct LevelVecs {
   T* d = nullptr;   // Chebyshev update direction (Chebyshev levels only)
 };
 
+// Product lists of one numeric Galerkin product on fixed patterns (see
+// k_spgemm_sym): per output entry its (S entry, B entry) pairs.
+struct SpgemmList {
+  long long* off = nullptr;  // nout + 1
+  int* ls = nullptr;         // total pairs
+  int* lb = nullptr;
+  long long total = 0;
+  bool tried = false;        // a build was attempted (memory may have been short)
+};
+
 struct DevLevel {
   DevMat A, P, R;            // R = Pᵀ stored as the transpose map with values
   SmootherKind smoother = SmootherKind::Jacobi;
@@ -118,6 +128,7 @@ struct DevLevel {
   int* color_order = nullptr;
   bool has_rap = false;
   DevMat AP;                 // pattern and values of A·P (partial resetup)
+  SpgemmList ap_list, rap_list;  // product lists of A·P and Pᵀ·(AP), built on the first resetup
   DevMat At;                 // A^T (transposed cycles; built on first use)
   int* at_perm = nullptr;    // At value k = A value at_perm[k]
   double* invdT = nullptr;   // smoother diagonal of A^T
@@ -273,7 +284,8 @@ class DevHier {
   void precond64(const double* r, double* out, const CycleOpts& o);
   void upload_csr(DevMat& M, int n, int m, const std::vector<int>& rp, const std::vector<int>& ci,
                   const std::vector<double>* v);
-  void spgemm(DevMat& O, const DevMat& S, const DevMat& B);
+  void spgemm(DevMat& O, const DevMat& S, const DevMat& B, SpgemmList* list = nullptr);
+  bool build_spgemm_list(const DevMat& O, const DevMat& S, const DevMat& B, SpgemmList& list);
   // Levels tail_ .. nlevels-1 run as one single-block kernel (k_coarse_tail);
   // tail_ = nlevels() when no level qualifies.
   int tail_ = 0;

@@ -1304,6 +1304,122 @@ __global__ void k_l1_invdiag(int n, const int* __restrict__ rp, const double* __
   }
 }
 
+// ------------------------------------------------------------ Galerkin product lists
+// The numeric Galerkin product O = S B on fixed patterns as a list of
+// product pairs per output entry: entry e of O is the sum, in list order,
+// of s_v[ls[p]] * b_v[lb[p]] for p in [off[e], off[e + 1]).  The lists are
+// recorded once by k_spgemm_sym (COUNT, then FILL after an exclusive scan
+// of the counts) walking the products exactly as k_spgemm_warp does -- in
+// the order (entry k of S's row, entry t of B's row j_k), grouped by output
+// entry in lane order -- so k_spgemm_apply adds every entry's products in
+// the same order and gives the same values bit for bit, with a few
+// instructions and 24 bytes of traffic per product.
+template <int CAP, int WPB, bool FILL>
+__global__ void __launch_bounds__(WPB * 32)
+k_spgemm_sym(int nrows, const int* __restrict__ out_rp, const int* __restrict__ out_ci,
+             const int* __restrict__ s_rp, const int* __restrict__ s_ci, const int* __restrict__ b_rp,
+             const int* __restrict__ b_ci, int* cnt, const long long* __restrict__ off,
+             int* __restrict__ ls, int* __restrict__ lb) {
+  __shared__ int scol[WPB][CAP];
+  __shared__ int sk[WPB][32], st[WPB][32];
+  const int lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5;
+  const unsigned full = 0xffffffffu;
+  for (long long I0 = (long long)blockIdx.x * WPB + w; I0 < nrows; I0 += (long long)gridDim.x * WPB) {
+    const int I = (int)I0;
+    const int os = out_rp[I], oe = out_rp[I + 1];
+    const int m = oe - os;
+    const bool fits = m <= CAP;
+    const int* pat = fits ? scol[w] : out_ci + os;
+    if (fits)
+      for (int t = lane; t < m; t += 32) scol[w][t] = out_ci[os + t];
+    __syncwarp();
+    const int ss = s_rp[I], se = s_rp[I + 1];
+    for (int k0 = ss; k0 < se; k0 += 32) {
+      const int k = k0 + lane;
+      int bs = 0, len = 0;
+      if (k < se) {
+        const int j = s_ci[k];
+        bs = b_rp[j];
+        len = b_rp[j + 1] - bs;
+      }
+      int incl = len;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(full, incl, o);
+        if (lane >= o) incl += y;
+      }
+      const int excl = incl - len;
+      const int total = __shfl_sync(full, incl, 31);
+      for (int f0 = 0; f0 < total; f0 += 32) {
+        const int f = f0 + lane;
+        int q = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+          const int ex = __shfl_sync(full, excl, q + step);
+          if (ex <= f) q += step;
+        }
+        const int qbs = __shfl_sync(full, bs, q);
+        const int qex = __shfl_sync(full, excl, q);
+        const bool act = f < total;
+        int pos = -1, t = 0;
+        if (act) {
+          t = qbs + (f - qex);
+          const int J = b_ci[t];
+          int lo = 0, hi = m - 1;
+          while (lo <= hi) {
+            const int mid = (lo + hi) >> 1;
+            const int c = pat[mid];
+            if (c == J) {
+              pos = mid;
+              break;
+            }
+            if (c < J) lo = mid + 1;
+            else hi = mid - 1;
+          }
+        }
+        if (FILL) {
+          sk[w][lane] = k0 + q;
+          st[w][lane] = t;
+        }
+        const unsigned am = __ballot_sync(full, pos >= 0);
+        __syncwarp();
+        if (pos >= 0) {
+          const unsigned peers = __match_any_sync(am, pos);
+          if (lane == __ffs(peers) - 1) {
+            const int e = os + pos;
+            if (FILL) {
+              long long slot = off[e] + cnt[e];
+              for (unsigned mm = peers; mm; mm &= mm - 1) {
+                const int src = __ffs(mm) - 1;
+                ls[slot] = sk[w][src];
+                lb[slot] = st[w][src];
+                ++slot;
+              }
+            }
+            cnt[e] += __popc(peers);
+          }
+        }
+        __syncwarp();
+      }
+    }
+  }
+}
+
+// O's values from the product lists (see k_spgemm_sym): one thread per
+// output entry, products multiplied and added in list order, separately
+// rounded.
+__global__ void k_spgemm_apply(long long nout, const long long* __restrict__ off, const int* __restrict__ ls,
+                               const int* __restrict__ lb, const double* __restrict__ s_v,
+                               const double* __restrict__ b_v, double* __restrict__ out_v) {
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nout;
+       e += (long long)gridDim.x * blockDim.x) {
+    double a = 0.0;
+    for (long long p = off[e]; p < off[e + 1]; ++p) a = __dadd_rn(a, __dmul_rn(s_v[ls[p]], b_v[lb[p]]));
+    out_v[e] = a;
+  }
+}
+
 // ILU(0) substitutions, one level of the schedule per launch (src/
 // smoothers.jl:1398-1423; the serial smoother's loops, :1174-1192, give the
 // same values): one thread per row, the row's products subtracted in column
