@@ -106,6 +106,18 @@ def test_jacobi_invdiag_and_smoothing():
     assert np.linalg.norm(b - A @ x) < np.linalg.norm(b)
 
 
+def test_safe_inverse_diagonal():
+    """testset "Safe Diagonal - Zero diagonal row" (test/runtests.jl:1784-1796):
+    a row whose diagonal is 1e-20 gets a finite (zero) inverse.  (The
+    library's diagonals equal the oracle's bit for bit in
+    test_cpu_library.py::test_structure_matches_oracle.)"""
+    A = sp.csr_matrix(np.array([[2.0, -1.0, 0.0], [-1.0, 1e-20, -1.0], [0.0, -1.0, 2.0]]))
+    A.sort_indices()
+    n, rp, ci, v = parts(A)
+    inv = oracle.invdiag(n, rp, ci, v)
+    assert np.all(np.isfinite(inv)) and inv[1] == 0.0
+
+
 def test_l1_invdiag():
     """testset "L1 Colored GS Smoother - Build" (:607-617): interior row l1
     norm 4 -> invdiag 0.25."""
