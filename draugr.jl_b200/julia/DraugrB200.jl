@@ -19,6 +19,7 @@ using SparseArrays
 
 export AMGConfig, hypre_default_config, AMGHierarchy
 export amg_setup, amg_solve!, amg_cycle!, amg_resetup!, amg_pcg!
+export amg_bicgstab!, amg_pcg_block!, nz_gradient!
 export DraugrB200Preconditioner
 
 const libdraugr = get(ENV, "DRAUGR_B200_LIB", joinpath(@__DIR__, "..", "libdraugr_b200.so"))
@@ -68,6 +69,11 @@ struct HMISCoarsening <: CoarseningAlgorithm
     θ::Float64
     interpolation::InterpolationType
 end
+struct RSCoarsening <: CoarseningAlgorithm
+    θ::Float64
+    interpolation::InterpolationType
+end
+RSCoarsening(θ::Real=0.25) = RSCoarsening(θ, DirectInterpolation())
 HMISCoarsening(θ::Real=0.25) = HMISCoarsening(θ, DirectInterpolation())
 struct AggressiveCoarsening <: CoarseningAlgorithm
     θ::Float64
@@ -94,7 +100,7 @@ for (T, name) in ((:JacobiSmootherType, "jacobi"), (:L1JacobiSmootherType, "l1_j
         export $T
     end
 end
-export AggregationCoarsening, PMISCoarsening, HMISCoarsening, AggressiveCoarsening,
+export AggregationCoarsening, PMISCoarsening, HMISCoarsening, RSCoarsening, AggressiveCoarsening,
        SmoothedAggregationCoarsening, DirectInterpolation, StandardInterpolation,
        ExtendedIInterpolation
 
@@ -113,6 +119,7 @@ coarsening_json(c::AggregationCoarsening) = ("aggregation", c.θ, nothing,
 coarsening_json(c::SmoothedAggregationCoarsening) = ("smoothed_aggregation", c.θ, nothing, ",\"sa_omega\":$(c.ω)")
 coarsening_json(c::PMISCoarsening) = ("pmis", c.θ, c.interpolation, "")
 coarsening_json(c::HMISCoarsening) = ("hmis", c.θ, c.interpolation, "")
+coarsening_json(c::RSCoarsening) = ("rs", c.θ, c.interpolation, "")
 coarsening_json(c::AggressiveCoarsening) = ("aggressive_" * String(c.base), c.θ, c.interpolation, "")
 
 """
@@ -262,13 +269,81 @@ function amg_pcg!(x::AbstractVector{Float64}, b::AbstractVector{Float64}, h::AMG
                   precision::Symbol=:fp64)
     prec = precision === :mixed ? Int32(1) : Int32(0)
     rel = Ref{Float64}(0.0)
-    fn = isdevice(x) ? :draugr_b200_pcg_device : :draugr_b200_pcg
-    px, pb = isdevice(x) ? (rawptr(x), rawptr(b)) : (pointer(x), pointer(b))
-    it = GC.@preserve x b ccall((fn, libdraugr), Int32,
-                                (Int32, Int32, Ptr{Float64}, Ptr{Float64}, Int32, Float64, Int32,
-                                 Int32, Ref{Float64}),
-                                h.handle, length(x), px, pb, config.handle, tol, maxiter, prec, rel)
+    it = GC.@preserve x b if isdevice(x)
+        ccall((:draugr_b200_pcg_device, libdraugr), Int32,
+              (Int32, Int32, Ptr{Float64}, Ptr{Float64}, Int32, Float64, Int32, Int32, Ref{Float64}),
+              h.handle, length(x), rawptr(x), rawptr(b), config.handle, tol, maxiter, prec, rel)
+    else
+        ccall((:draugr_b200_pcg, libdraugr), Int32,
+              (Int32, Int32, Ptr{Float64}, Ptr{Float64}, Int32, Float64, Int32, Int32, Ref{Float64}),
+              h.handle, length(x), pointer(x), pointer(b), config.handle, tol, maxiter, prec, rel)
+    end
     return x, Int(check(it, "amg_pcg!")), rel[]
+end
+
+"""
+    amg_bicgstab!(x, b, h, config; tol=1e-8, maxiter=500, transpose=false) -> (x, niter, relres)
+
+BiCGStab preconditioned (on the right) by one FP64 cycle, for nonsymmetric
+systems; `transpose=true` solves Aᵀx = b on the transposed hierarchy (the
+adjoint solve of a gradient).  Every level must use Jacobi, l1-Jacobi or
+SPAI(0) smoothing for the transposed cycle.
+"""
+function amg_bicgstab!(x::AbstractVector{Float64}, b::AbstractVector{Float64}, h::AMGHierarchy,
+                       config::AMGConfig=AMGConfig(); tol::Real=1e-8, maxiter::Int=500,
+                       transpose::Bool=false)
+    rel = Ref{Float64}(0.0)
+    tr = Int32(transpose)
+    it = GC.@preserve x b if isdevice(x)
+        ccall((:draugr_b200_bicgstab_device, libdraugr), Int32,
+              (Int32, Int32, Ptr{Float64}, Ptr{Float64}, Int32, Float64, Int32, Int32, Ref{Float64}),
+              h.handle, length(x), rawptr(x), rawptr(b), config.handle, tol, maxiter, tr, rel)
+    else
+        ccall((:draugr_b200_bicgstab, libdraugr), Int32,
+              (Int32, Int32, Ptr{Float64}, Ptr{Float64}, Int32, Float64, Int32, Int32, Ref{Float64}),
+              h.handle, length(x), pointer(x), pointer(b), config.handle, tol, maxiter, tr, rel)
+    end
+    return x, Int(check(it, "amg_bicgstab!")), rel[]
+end
+
+"""
+    amg_pcg_block!(X, B, h, config; tol=1e-8, maxiter=500, precision=:mixed) -> (X, iters, relres)
+
+CG for k ≤ 32 right-hand sides of one matrix at once, each product with a
+level matrix serving all k.  `X` and `B` are device matrices of size
+(k, n): column i holds row i's k entries (the library's n × k row-major
+layout).  Returns per-column iteration counts and relative residuals.
+"""
+function amg_pcg_block!(X::AbstractMatrix{Float64}, B::AbstractMatrix{Float64}, h::AMGHierarchy,
+                        config::AMGConfig=AMGConfig(); tol::Real=1e-8, maxiter::Int=500,
+                        precision::Symbol=:mixed)
+    k, n = size(X)
+    size(B) == (k, n) || throw(DimensionMismatch("X and B must have the same size"))
+    its = zeros(Int32, k)
+    rel = zeros(Float64, k)
+    prec = precision === :mixed ? Int32(1) : Int32(0)
+    rc = GC.@preserve X B ccall((:draugr_b200_pcg_block_device, libdraugr), Int32,
+                                (Int32, Int32, Int32, Ptr{Float64}, Ptr{Float64}, Int32, Float64, Int32,
+                                 Int32, Ptr{Int32}, Ptr{Float64}),
+                                h.handle, n, k, rawptr(X), rawptr(B), config.handle, tol, maxiter, prec,
+                                its, rel)
+    check(rc, "amg_pcg_block!")
+    return X, Int.(its), rel
+end
+
+"""
+    nz_gradient!(grad, h, x, λ) -> grad
+
+dL/da_ij = -λ_i x_j for the finest matrix's nonzeros, in CSR order (device
+vectors; grad has nnz entries), with x = A⁻¹b and λ = A⁻ᵀ dL/dx.
+"""
+function nz_gradient!(grad::AbstractVector{Float64}, h::AMGHierarchy, x::AbstractVector{Float64},
+                      λ::AbstractVector{Float64})
+    rc = GC.@preserve grad x λ ccall((:draugr_b200_nz_gradient_device, libdraugr), Int32,
+                                     (Int32, Int32, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
+                                     h.handle, length(x), rawptr(x), rawptr(λ), rawptr(grad))
+    check(rc, "nz_gradient!")
+    return grad
 end
 
 """
