@@ -81,29 +81,35 @@ k_spmm(int nrows, int k, const int* __restrict__ rp, const int* __restrict__ ci,
 }
 
 // The same products with vector gathers, when each row's k columns split
-// into 16-byte pieces (k a multiple of 4 FP32 / 2 FP64 values, 16-byte
-// aligned vectors): TPR threads per row, each owning V consecutive
-// columns, 32 / TPR rows per warp.  A thread reads the row's (column,
-// value) pairs itself (the TPR threads of a row read the same address) and
-// gathers one 16-byte piece of X per entry, so an entry costs a few
-// instructions per piece instead of shuffles and a scalar gather per
-// column.  Each column is summed in column order with separately rounded
-// products and sums: the results equal k_spmm's bit for bit.
+// into pieces of V = 4 consecutive columns (k a multiple of 4, 16-byte
+// aligned vectors; a piece is one 16-byte load in FP32, two in FP64): TPR
+// threads per row, each owning one piece, 32 / TPR rows per warp.  A row's
+// threads pass its (column, value) pairs round and gather one piece of X
+// per entry, so an entry costs a few instructions per piece instead of
+// shuffles and a scalar gather per column (four FP64 columns per thread
+// rather than two took the 96^3 x 32 FP64 block solve from 97 to 90 ms).
+// Each column is summed in column order with separately rounded products
+// and sums: the results equal k_spmm's bit for bit.
 template <typename T>
-struct Vec16;
+struct VecPiece;
 template <>
-struct Vec16<float> {
+struct VecPiece<float> {
   using type = float4;
   static constexpr int V = 4;
   __device__ static void get(const type& a, float* o) { o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w; }
   __device__ static type make(const float* o) { return make_float4(o[0], o[1], o[2], o[3]); }
 };
+struct __align__(16) double2x2 {
+  double2 lo, hi;
+};
 template <>
-struct Vec16<double> {
-  using type = double2;
-  static constexpr int V = 2;
-  __device__ static void get(const type& a, double* o) { o[0] = a.x; o[1] = a.y; }
-  __device__ static type make(const double* o) { return make_double2(o[0], o[1]); }
+struct VecPiece<double> {  // four FP64 columns: two 16-byte loads
+  using type = double2x2;
+  static constexpr int V = 4;
+  __device__ static void get(const type& a, double* o) { o[0] = a.lo.x; o[1] = a.lo.y; o[2] = a.hi.x; o[3] = a.hi.y; }
+  __device__ static type make(const double* o) {
+    return double2x2{make_double2(o[0], o[1]), make_double2(o[2], o[3])};
+  }
 };
 
 // Per-block partial sums of each column of a vector-layout kernel (TPR
@@ -133,7 +139,7 @@ __global__ void __launch_bounds__(kBlock)
 k_spmm_vec(int nrows, int k, const int* __restrict__ rp, const int* __restrict__ ci,
            const TA* __restrict__ av, const T* __restrict__ X, const T* __restrict__ B,
            const T* __restrict__ dinv, T omega, T* Y, double* __restrict__ part) {
-  using VV = Vec16<T>;
+  using VV = VecPiece<T>;
   using VT = typename VV::type;
   constexpr int V = VV::V;
   constexpr int RPW = 32 / TPR;
@@ -507,14 +513,14 @@ int vec_grid(const void* f, int nrows, int tpr, int max_grid) {
 }
 
 // Block product on `nrows` rows: the vector-gather kernel when the rows'
-// k columns split into 16-byte pieces, else one warp per row.  With `part`
+// k columns split into pieces of 4, else one warp per row.  With `part`
 // (STORE mode only) the vector kernel also leaves the column partials of
 // X_row . Y_row there; returns its grid (the number of partials per
 // column), or 0 when the one-warp-per-row kernel ran (no partials).
 template <typename TA, typename T, int MODE>
 int spmm(cudaStream_t st, int max_grid, int nrows, int k, const int* rp, const int* ci, const TA* av,
          const T* X, const T* B, const T* dinv, T omega, T* Y, double* part = nullptr) {
-  constexpr int V = Vec16<T>::V;
+  constexpr int V = VecPiece<T>::V;
   if (k % V == 0 && aligned16(X) && aligned16(B) && aligned16(Y)) {
     const int tpr = tpr_for(k / V);
     int grid = 1;

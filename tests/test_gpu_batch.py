@@ -45,13 +45,15 @@ def test_concurrent_solves_equal_sequential_ones():
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-@pytest.mark.parametrize("side,k,coarse", [(20, 5, 50), (24, 32, 50), (16, 1, 50), (18, 32, 300)])
+@pytest.mark.parametrize("side,k,coarse", [(20, 5, 50), (24, 32, 50), (16, 1, 50), (18, 32, 300), (17, 6, 50)])
 def test_block_pcg_matches_single_solves(side, k, coarse, precision):
     """Many right-hand sides of one matrix (the C3 96^3 x 32 case, reduced):
     block PCG, one pass over each level matrix for all k columns, against
     k single-right-hand-side PCG solves.  Odd k takes the unfused outer
-    iteration and one warp per row; max_coarse_size 300 gives a coarsest
-    system of more than 64 unknowns (the one-thread-per-column solve)."""
+    iteration and one warp per row; k = 6 the fused outer iteration with one
+    warp per row (6 columns do not split into pieces of 4); max_coarse_size
+    300 gives a coarsest system of more than 64 unknowns (the
+    one-thread-per-column solve)."""
     A = problems.poisson3d(side)
     n = A.shape[0]
     cfg = draugr.hypre_default_config(agg_trunc_factor=0.2, smoother=draugr.L1JacobiSmootherType(), seed=6)
