@@ -87,7 +87,13 @@ int32_t draugr_b200_residual_noalloc(int32_t n, int32_t nnz, const int32_t *rowp
                                      const double *b, double *r, double *rnorm, void *stream);
 
 /* Partial resetup from new values of the finest matrix already on the
- * device (same pattern as at setup), nnz entries. */
+ * device (same pattern as at setup), nnz entries.  The first partial
+ * resetup of a hierarchy also records its Galerkin product lists (8 bytes
+ * per product, kept while under half of the free device memory), which
+ * make later resetups faster.  A resetup synchronises its stream and may
+ * allocate: do not capture it in a CUDA graph.  Replaces the device-side
+ * part of amg_resetup! (src/resetup.jl:20-45); the reference copies the
+ * values to the host first (ext/DraugrCUDAExt.jl:49). */
 int32_t draugr_b200_resetup_values_device(int32_t handle, int64_t nnz, const double *nzval_dev);
 
 /* Conjugate gradients preconditioned by one AMG cycle per iteration, until
