@@ -321,6 +321,36 @@ def run_ours(args, world, rank, local):
                 "kernels": {k: {kk: (round(vv, 4) if isinstance(vv, float) else vv)
                                 for kk, vv in v.items()} for k, v in kern.items()}}
 
+    # the whole V-cycle: algorithmic bytes of the kernels one FP64 V(1,1)
+    # cycle launches, per level, against the cycle's event-timed duration
+    vc_bytes = 0
+    for l in range(h.nlevels):
+        info = h.level_info(l)
+        ln, lnnz, lnc, lnnzp = int(info[0]), int(info[1]), int(info[2]), int(info[3])
+        resid = lnnz * 12 + 4 * (ln + 1) + 3 * ln * 8
+        vc_bytes += resid + op_bytes(3, 0, ln, lnnz, lnc, lnnzp) + op_bytes(4, 0, ln, lnnz, lnc, lnnzp)
+        vc_bytes += op_bytes(2, 0, ln, lnnz, lnc, lnnzp) * (2 if l == 0 else 1)
+    xc = torch.zeros(n, dtype=torch.float64, device=dev)
+    for _ in range(3):
+        draugr.amg_cycle(xc, bd, h, cfg)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    ncyc = 20
+    e0.record(stream)
+    for _ in range(ncyc):
+        draugr.amg_cycle(xc, bd, h, cfg)
+    e1.record(stream)
+    e1.synchronize()
+    vc_ms = e0.elapsed_time(e1) / ncyc
+    vcycle = {"precision": "fp64", "ms": round(vc_ms, 4), "algorithmic_bytes": int(vc_bytes),
+              "GBps": round(vc_bytes / (vc_ms * 1e-3) / 1e9, 1),
+              "frac": round(vc_bytes / (vc_ms * 1e-3) / 1e9 / peak, 3),
+              "note": "V(1,1) through draugr_b200_cycle_device, 20 cycles after 3 warm-up; bytes: "
+                      "per level the residual (12 nnz + 4 (n+1) + 24 n), restriction, prolongation and "
+                      "the Jacobi sweep formulas (two sweeps on the finest level, whose pre-smoothing "
+                      "starts from a given x; the coarser levels' first sweep is formed in the "
+                      "restriction), shared-memory tail levels included at their global-memory size"}
+
     out = {"metric": METRIC, "value": res["mixed"]["time_s"], "unit": "s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": res["mixed"]["time_s"] * 1e3, "higher_is_better": False,
@@ -331,7 +361,8 @@ def run_ours(args, world, rank, local):
                           parallelism=f"replicas x{world}" if world > 1 else "1 GPU"),
            "fp64": res["fp64"], "mixed": res["mixed"],
            "speedup_mixed_vs_fp64": res["fp64"]["time_s"] / res["mixed"]["time_s"],
-           "e2e": e2e, "roofline": roofline, "clocks": clocks, "gpu_launches": int(launches)}
+           "e2e": e2e, "roofline": roofline, "vcycle": vcycle, "clocks": clocks,
+           "gpu_launches": int(launches)}
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(h, b, cfg)
