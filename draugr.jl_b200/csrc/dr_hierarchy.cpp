@@ -478,17 +478,26 @@ namespace {
 
 void serial_gs_levels(const CSR& A, std::vector<int>& order, std::vector<int>& off) {
   const int n = A.n;
-  std::vector<std::vector<int>> later(n);  // later[i]: rows j < i with a_ji != 0
+  // rows j < i with a_ji != 0, per row i (CSR: lo_off / lo_src)
+  std::vector<int> lo_off(n + 1, 0);
   for (int j = 0; j < n; ++j)
     for (int k = A.rp[j]; k < A.rp[j + 1]; ++k)
-      if (A.ci[k] > j) later[A.ci[k]].push_back(j);
+      if (A.ci[k] > j) ++lo_off[A.ci[k] + 1];
+  for (int i = 0; i < n; ++i) lo_off[i + 1] += lo_off[i];
+  std::vector<int> lo_src(lo_off[n]);
+  {
+    std::vector<int> pos(lo_off.begin(), lo_off.end() - 1);
+    for (int j = 0; j < n; ++j)
+      for (int k = A.rp[j]; k < A.rp[j + 1]; ++k)
+        if (A.ci[k] > j) lo_src[pos[A.ci[k]]++] = j;
+  }
   std::vector<int> lev(n);
   int nl = 0;
   for (int i = 0; i < n; ++i) {
     int m = 0;
     for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
       if (A.ci[k] < i) m = std::max(m, lev[A.ci[k]]);
-    for (int j : later[i]) m = std::max(m, lev[j]);
+    for (int q = lo_off[i]; q < lo_off[i + 1]; ++q) m = std::max(m, lev[lo_src[q]]);
     lev[i] = m + 1;
     nl = std::max(nl, lev[i]);
   }
