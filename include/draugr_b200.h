@@ -36,11 +36,16 @@ int32_t draugr_b200_level_info(int32_t handle, int32_t lvl, int64_t *info);
 
 /* Copy one array of level lvl (0-based indices) into out.  Integer arrays
  * (int32): A_rowptr A_colval P_rowptr P_colval T_offsets T_rows T_pnz
- * colors color_order color_offsets AP_rowptr AP_colval, and for lvl = -1
- * C_rowptr C_colval C_piv.  Double arrays: A_nzval P_nzval R_nzval invdiag
- * AP_nzval, and for lvl = -1 C_nzval C_dense C_lu.  Values come from the
- * device when the hierarchy lives there (so they reflect resetups).
- * out = NULL returns the element count.  Returns the element count. */
+ * colors color_order color_offsets AP_rowptr AP_colval cf (the C/F
+ * splitting, 1 / -1, of splitting-based coarsening), ilu_diag
+ * ilu_fwd_order ilu_fwd_offsets ilu_bwd_order ilu_bwd_offsets (ILU(0)
+ * levels), sgs_order sgs_offsets (serial Gauss-Seidel schedule), and for
+ * lvl = -1 C_rowptr C_colval C_piv.  Double arrays: A_nzval P_nzval
+ * R_nzval invdiag omega AP_nzval, cheb_coef cheb_v0 (Chebyshev), ilu_L
+ * ilu_U (ILU(0) factors), spai1_M (SPAI(1)), and for lvl = -1 C_nzval
+ * C_dense C_lu.  Values come from the device when the hierarchy lives there
+ * (so they reflect resetups).  out = NULL returns the element count.
+ * Returns the element count. */
 int64_t draugr_b200_export(int32_t handle, int32_t lvl, const char *what, void *out,
                            int64_t capacity_elems);
 
