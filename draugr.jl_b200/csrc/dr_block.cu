@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <mutex>
 #include <string>
 #include <type_traits>
@@ -491,8 +492,8 @@ int tpr_for(int per_row) {
 // Blocks of a vector-layout kernel f (32 / tpr rows per warp): enough for
 // the rows, at most one wave of resident blocks (max_grid allows 8 blocks
 // of 256 threads per SM; registers may allow fewer, queried once per
-// kernel).
-int vec_grid(const void* f, int nrows, int tpr, int max_grid) {
+// kernel), or nb_cap blocks per SM when that is smaller (0: no cap).
+int vec_grid(const void* f, int nrows, int tpr, int max_grid, int nb_cap = 0) {
   static std::mutex mu;
   static std::unordered_map<const void*, int> occ;
   int nb;
@@ -508,6 +509,7 @@ int vec_grid(const void* f, int nrows, int tpr, int max_grid) {
       nb = it->second;
     }
   }
+  if (nb_cap > 0) nb = std::min(nb, nb_cap);
   const int rows_per_block = kWarps * (32 / tpr);
   return std::max(1, std::min((nrows + rows_per_block - 1) / rows_per_block, max_grid / 8 * nb));
 }
@@ -517,18 +519,24 @@ int vec_grid(const void* f, int nrows, int tpr, int max_grid) {
 // (STORE mode only) the vector kernel also leaves the column partials of
 // X_row . Y_row there; returns its grid (the number of partials per
 // column), or 0 when the one-warp-per-row kernel ran (no partials).
+// `sh` overrides the vector kernel's threads per row (a power of two from
+// the default up to 16; the extra threads help load a row's entries and
+// drop their sums) and caps its blocks per SM.  Every shape gives the same
+// values: each column of a row is summed by one thread in column order.
 template <typename TA, typename T, int MODE>
 int spmm(cudaStream_t st, int max_grid, int nrows, int k, const int* rp, const int* ci, const TA* av,
-         const T* X, const T* B, const T* dinv, T omega, T* Y, double* part = nullptr) {
+         const T* X, const T* B, const T* dinv, T omega, T* Y, double* part = nullptr,
+         BlockShape sh = {}) {
   constexpr int V = VecPiece<T>::V;
   if (k % V == 0 && aligned16(X) && aligned16(B) && aligned16(Y)) {
-    const int tpr = tpr_for(k / V);
+    const int t0 = tpr_for(k / V);
+    const int tpr = (sh.tpr >= t0 && sh.tpr <= 16 && (sh.tpr & (sh.tpr - 1)) == 0) ? sh.tpr : t0;
     int grid = 1;
     switch (tpr) {
 #define DR_SPMM_VEC(t)                                                                            \
   case t: {                                                                                       \
     auto kf = k_spmm_vec<TA, T, MODE, t>;                                                         \
-    grid = vec_grid((const void*)kf, nrows, t, max_grid);                                         \
+    grid = vec_grid((const void*)kf, nrows, t, max_grid, sh.nb);                                  \
     kf<<<grid, kBlock, 0, st>>>(nrows, k, rp, ci, av, X, B, dinv, omega, Y, part);                \
     break;                                                                                        \
   }
@@ -576,6 +584,120 @@ void DevHier::ensure_block(int k) {
   blk_k_ = k;
 }
 
+BlockShape DevHier::shape_of(const void* rp, int mode, int bytes, int k) const {
+  if (!btune_on_) return BlockShape{};
+  if (bforce_tpr_) return BlockShape{bforce_tpr_, 0};
+  auto it = bshape_.find(ShapeKey{rp, mode, bytes, k});
+  return it == bshape_.end() ? BlockShape{} : it->second;
+}
+
+// Picks the launch shape of each product of the block cycle (threads per
+// row: 32 / tpr rows per warp, and blocks per SM) by timing the candidates
+// on this hierarchy's own matrices, once per k and precision.  A candidate
+// replaces the default only when it is at least 3% faster.  The candidates
+// run on the block buffers, zeroed first, before a solve uses them, and
+// every shape gives the same values, so tuning changes no result.  The
+// FP64 product with A that also forms p.q keeps the default shape, so that
+// the partial sums, and with them every dot product, do not depend on the
+// timing.  The environment variable DRAUGR_B200_BLOCK_TUNE, read at each
+// block solve, set to 0 keeps the default shapes and set to 2, 4, 8 or 16
+// forces that many threads per row (at least the default) on every product
+// of the cycle, without timing.
+template <typename T>
+void DevHier::tune_block(int k, int verbose) {
+  btune_on_ = true;
+  bforce_tpr_ = 0;
+  if (const char* env = std::getenv("DRAUGR_B200_BLOCK_TUNE"); env && *env) {
+    const int v = std::atoi(env);
+    if (v == 0) {
+      btune_on_ = false;
+      return;
+    }
+    if (v == 2 || v == 4 || v == 8 || v == 16) {
+      bforce_tpr_ = v;
+      return;
+    }
+  }
+  constexpr int V = VecPiece<T>::V;
+  if (k % V != 0) return;  // the one-warp-per-row kernel has no shape to pick
+  if (!btuned_.insert({k, (int)sizeof(T)}).second) return;
+  const int t0 = tpr_for(k / V);
+  std::vector<BlockShape> cand;
+  for (int t = t0; t <= 16; t *= 2)
+    for (int nb = 0; nb <= 2; nb += 2) cand.push_back(BlockShape{t, nb});
+  constexpr int kReps = 3;
+  cudaEvent_t e0, e1;
+  DR_CK(cudaEventCreate(&e0));
+  DR_CK(cudaEventCreate(&e1));
+  static const char* kOpName[4] = {"A x (Jacobi)", "b - A x", "P^T r", "x + P x_c"};
+  static const int kOpMode[4] = {BM_JACOBI, BM_RESID, BM_STORE, BM_ADDTO};
+  const int nl = nlevels();
+  for (int l = 0; l < nl; ++l) {
+    DevLevel& L = L_[l];
+    BlockVecs<T>& W = bvecs<T>(l);
+    const size_t m = (size_t)L.A.n * k;
+    T* const bufs[4] = {W.x, W.t, W.b, W.r};
+    for (T* p : bufs) DR_CK(cudaMemsetAsync(p, 0, m * sizeof(T), st_));
+    const bool last = (l + 1 == nl);
+    T* bc = last ? (sizeof(T) == 8 ? (T*)bcb64_ : (T*)bcb32_) : bvecs<T>(l + 1).b;
+    T* xc = last ? (sizeof(T) == 8 ? (T*)bcx64_ : (T*)bcx32_) : bvecs<T>(l + 1).x;
+    const size_t mc = (size_t)std::max(last ? nc_ : L_[l + 1].A.n, 1) * k;
+    DR_CK(cudaMemsetAsync(bc, 0, mc * sizeof(T), st_));
+    DR_CK(cudaMemsetAsync(xc, 0, mc * sizeof(T), st_));
+    const T* dinv = invd<T>(L);
+    const T om = (T)L.omega;
+    const DevMat &A = L.A, &R = L.R, &P = L.P;
+    auto launch = [&](int op, BlockShape sh) {
+      note_launch();
+      switch (op) {
+        case 0:
+          spmm<T, T, BM_JACOBI>(st_, max_grid_, A.n, k, A.rp, A.ci, mval<T>(A), W.x, W.b, dinv, om, W.t, nullptr, sh);
+          break;
+        case 1:
+          spmm<T, T, BM_RESID>(st_, max_grid_, A.n, k, A.rp, A.ci, mval<T>(A), W.x, W.b, nullptr, T(0), W.r,
+                               nullptr, sh);
+          break;
+        case 2:
+          spmm<T, T, BM_STORE>(st_, max_grid_, R.n, k, R.rp, R.ci, mval<T>(R), W.r, nullptr, nullptr, T(0), bc,
+                               nullptr, sh);
+          break;
+        default:  // x += P x_c with x_c = 0 leaves x at zero
+          spmm<T, T, BM_ADDTO>(st_, max_grid_, P.n, k, P.rp, P.ci, mval<T>(P), xc, nullptr, nullptr, T(0), W.x,
+                               nullptr, sh);
+      }
+    };
+    const void* rps[4] = {A.rp, A.rp, R.rp, P.rp};
+    for (int op = 0; op < 4; ++op) {
+      float best = 0.f, def = 0.f;
+      BlockShape pick{};
+      for (size_t c = 0; c < cand.size(); ++c) {
+        launch(op, cand[c]);  // warm-up
+        DR_CK(cudaEventRecord(e0, st_));
+        for (int r = 0; r < kReps; ++r) launch(op, cand[c]);
+        DR_CK(cudaEventRecord(e1, st_));
+        DR_CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        DR_CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (c == 0) {
+          def = best = ms;
+        } else if (ms < best && ms < 0.97f * def) {
+          best = ms;
+          pick = cand[c];
+        }
+      }
+      if (pick.tpr) bshape_[ShapeKey{rps[op], kOpMode[op], (int)sizeof(T), k}] = pick;
+      if (verbose >= 1)
+        std::printf("block tuning (k = %d, FP%d) level %d %-12s: %2d threads per row, %s blocks per SM, "
+                    "%.1f us (default %.1f us)\n",
+                    k, 8 * (int)sizeof(T), l, kOpName[op], pick.tpr ? pick.tpr : t0,
+                    pick.nb ? "2" : "all resident", 1e3 * best / kReps, 1e3 * def / kReps);
+    }
+  }
+  DR_CK(cudaEventDestroy(e0));
+  DR_CK(cudaEventDestroy(e1));
+  DR_CK(cudaGetLastError());
+}
+
 void DevHier::col_dots(int n, int k, const double* a, const double* b, double* dst_dev) {
   const int grid = warp_grid(n, max_grid_);
   note_launch();
@@ -598,6 +720,7 @@ T* DevHier::cycle_block(int l, T* X, const T* B, bool x_zero, const CycleOpts& o
   const T* av = mval<T>(A);
   T* x = X;
   T* t = (X == V.x) ? V.t : V.x;
+  const BlockShape sj = shape_of(A.rp, BM_JACOBI, sizeof(T), k);
   int pre = o.pre;
   if (x_zero) {
     note_launch();
@@ -610,17 +733,18 @@ T* DevHier::cycle_block(int l, T* X, const T* B, bool x_zero, const CycleOpts& o
   }
   for (int s = 0; s < pre; ++s) {
     note_launch();
-    spmm<T, T, BM_JACOBI>(st_, max_grid_, n, k, A.rp, A.ci, av, x, B, dinv, om, t);
+    spmm<T, T, BM_JACOBI>(st_, max_grid_, n, k, A.rp, A.ci, av, x, B, dinv, om, t, nullptr, sj);
     std::swap(x, t);
   }
   note_launch();
-  spmm<T, T, BM_RESID>(st_, max_grid_, n, k, A.rp, A.ci, av, x, B, nullptr, T(0), V.r);
+  spmm<T, T, BM_RESID>(st_, max_grid_, n, k, A.rp, A.ci, av, x, B, nullptr, T(0), V.r, nullptr,
+                       shape_of(A.rp, BM_RESID, sizeof(T), k));
   const bool last = (l + 1 == nlevels());
   T* bc = last ? (sizeof(T) == 8 ? (T*)bcb64_ : (T*)bcb32_) : bvecs<T>(l + 1).b;
   const DevMat& R = L.R;
   note_launch();
-  spmm<T, T, BM_STORE>(st_, max_grid_, R.n, k, R.rp, R.ci, mval<T>(R), V.r,
-                                                                        nullptr, nullptr, T(0), bc);
+  spmm<T, T, BM_STORE>(st_, max_grid_, R.n, k, R.rp, R.ci, mval<T>(R), V.r, nullptr, nullptr, T(0), bc, nullptr,
+                       shape_of(R.rp, BM_STORE, sizeof(T), k));
   T* xc;
   if (!last) {
     xc = cycle_block<T>(l + 1, bvecs<T>(l + 1).x, bc, true, o, k);
@@ -647,11 +771,11 @@ T* DevHier::cycle_block(int l, T* X, const T* B, bool x_zero, const CycleOpts& o
   }
   const DevMat& P = L.P;
   note_launch();
-  spmm<T, T, BM_ADDTO>(st_, max_grid_, P.n, k, P.rp, P.ci, mval<T>(P), xc,
-                                                                        nullptr, nullptr, T(0), x);
+  spmm<T, T, BM_ADDTO>(st_, max_grid_, P.n, k, P.rp, P.ci, mval<T>(P), xc, nullptr, nullptr, T(0), x, nullptr,
+                       shape_of(P.rp, BM_ADDTO, sizeof(T), k));
   for (int s = 0; s < o.post; ++s) {
     note_launch();
-    spmm<T, T, BM_JACOBI>(st_, max_grid_, n, k, A.rp, A.ci, av, x, B, dinv, om, t);
+    spmm<T, T, BM_JACOBI>(st_, max_grid_, n, k, A.rp, A.ci, av, x, B, dinv, om, t, nullptr, sj);
     std::swap(x, t);
   }
   DR_CK(cudaGetLastError());
@@ -670,6 +794,8 @@ int DevHier::pcg_block(double* X, const double* B, int k, const CycleOpts& o, do
       fail("block solves need Jacobi, l1-Jacobi or SPAI(0) smoothing on every level");
   if (mixed) ensure_fp32();
   ensure_block(k);
+  if (mixed) tune_block<float>(k, verbose);
+  else tune_block<double>(k, verbose);
   const int n = n0_;
   const long long m = (long long)n * k;
   double *R = bpcg_[0], *P = bpcg_[1], *Q = bpcg_[2], *Z = bpcg_[3];

@@ -4,7 +4,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
+#include <set>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "dr_host.h"
@@ -163,6 +166,12 @@ struct CycleOpts {
   bool w = false;
 };
 
+// Launch shape of a block (multi-right-hand-side) product: threads per row
+// (32 / tpr rows per warp) and resident blocks per SM; 0 takes the default.
+struct BlockShape {
+  int tpr = 0, nb = 0;
+};
+
 // Per-launch timing of the dominant kernels, filled when enabled.
 struct KernelClock {
   bool enabled = false;
@@ -268,6 +277,22 @@ class DevHier {
   double* bdev_ = nullptr;   // k-vectors on the device (dot results, alpha, beta)
   double* bhost_ = nullptr;  // their pinned host mirror
   void ensure_block(int k);
+  // Launch shapes of the block products, picked by timing (tune_block) per
+  // matrix, product mode, precision and k.
+  struct ShapeKey {
+    const void* rp;
+    int mode, bytes, k;
+    bool operator<(const ShapeKey& o) const {
+      return rp != o.rp ? rp < o.rp : mode != o.mode ? mode < o.mode : bytes != o.bytes ? bytes < o.bytes : k < o.k;
+    }
+  };
+  std::map<ShapeKey, BlockShape> bshape_;
+  std::set<std::pair<int, int>> btuned_;  // (k, bytes of the cycle's type) already tuned
+  bool btune_on_ = true;                  // DRAUGR_B200_BLOCK_TUNE=0 at a solve: default shapes
+  int bforce_tpr_ = 0;                    // DRAUGR_B200_BLOCK_TUNE=2/4/8/16: threads per row forced
+  BlockShape shape_of(const void* rp, int mode, int bytes, int k) const;
+  template <typename T>
+  void tune_block(int k, int verbose);
   template <typename T>
   BlockVecs<T>& bvecs(int l);
   template <typename T>

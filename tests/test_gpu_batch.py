@@ -73,3 +73,31 @@ def test_block_pcg_matches_single_solves(side, k, coarse, precision):
         r = np.linalg.norm(Bn[:, c] - A @ Xn[:, c]) / np.linalg.norm(Bn[:, c])
         assert r < 1e-8 and abs(r - rels[c]) < 1e-12
         assert np.linalg.norm(Xn[:, c] - x1) / np.linalg.norm(x1) < 1e-6
+
+
+@pytest.mark.parametrize("k,precision", [(8, "mixed"), (8, "fp64"), (32, "mixed")])
+def test_block_launch_shapes_change_no_value(k, precision, monkeypatch):
+    """The launch shapes of the block cycle's products (threads per row,
+    blocks per SM) are picked by timing.  Every shape sums each column of a
+    row in one thread in column order, so the default shapes, each forced
+    number of threads per row (DRAUGR_B200_BLOCK_TUNE=4/8/16, up to four
+    times the threads a row's columns need) and the timed pick give the same
+    solve bit for bit."""
+    A = problems.poisson3d(22)
+    n = A.shape[0]
+    cfg = draugr.hypre_default_config(agg_trunc_factor=0.2, smoother=draugr.L1JacobiSmootherType(), seed=4)
+    h = draugr.amg_setup(A, cfg)
+    B = torch.tensor(np.random.default_rng(k).uniform(-1, 1, (n, k)), device="cuda")
+    runs = {}
+    for setting in ["0", "4", "8", "16", ""]:
+        monkeypatch.setenv("DRAUGR_B200_BLOCK_TUNE", setting)
+        X = torch.zeros_like(B)
+        torch.cuda.synchronize()
+        X, its, rels = draugr.pcg_multi(X, B, h, cfg, tol=1e-8, maxiter=500, precision=precision)
+        runs[setting] = (X.cpu().numpy(), list(its), list(rels))
+    X0, its0, rels0 = runs["0"]
+    assert max(its0) > 0
+    for setting, (X, its, rels) in runs.items():
+        assert its == its0, setting
+        assert rels == rels0, setting
+        assert np.array_equal(X, X0), setting
