@@ -138,7 +138,12 @@ int32_t draugr_b200_bicgstab_device(int32_t handle, int32_t n, double *x_dev, co
  * precision as for draugr_b200_pcg; every level must use Jacobi, l1-Jacobi or SPAI(0)
  * smoothing.  iters and relres (host arrays of k entries, may be NULL)
  * receive each column's iterations and final true relative residual.
- * Returns the largest iteration count or -1.  No counterpart in the
+ * Returns the largest iteration count or -1.  The first call for a given k
+ * and precision on a hierarchy times the launch shapes of the cycle's
+ * products (threads per row, blocks per SM) and keeps the fastest; results
+ * do not depend on the shapes.  The environment variable
+ * DRAUGR_B200_BLOCK_TUNE, read at each call: 0 keeps the default shapes,
+ * 2/4/8/16 forces that many threads per row.  No counterpart in the
  * reference. */
 int32_t draugr_b200_pcg_block_device(int32_t handle, int32_t n, int32_t k, double *X_dev,
                                      const double *B_dev, int32_t config_handle, double tol,
