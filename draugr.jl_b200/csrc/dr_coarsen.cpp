@@ -248,6 +248,51 @@ static void strong_transpose_adj(const CSR& A, const std::vector<uint8_t>& st,
       if (A.ci[k] != i && st[k]) src[pos[A.ci[k]]++] = i;
 }
 
+// Strong off-diagonal couplings of every row as a compact CSR: row i's
+// entries k with ci[k] != i and st[k], in row order.  The sequential
+// splitting loops walk these lists instead of A's rows and the strength
+// flags (same entries, same order).
+namespace {
+struct StrongRows {
+  std::vector<int> off, col;
+  int begin(int i) const { return off[i]; }
+  int end(int i) const { return off[i + 1]; }
+};
+}  // namespace
+
+static StrongRows strong_rows(const CSR& A, const std::vector<uint8_t>& st) {
+  const int n = A.n;
+  StrongRows S;
+  S.off.assign(n + 1, 0);
+#pragma omp parallel for schedule(static, 4096)
+  for (int i = 0; i < n; ++i) {
+    int c = 0;
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) c += (A.ci[k] != i && st[k]);
+    S.off[i + 1] = c;
+  }
+  for (int i = 0; i < n; ++i) S.off[i + 1] += S.off[i];
+  S.col.resize(S.off[n]);
+#pragma omp parallel for schedule(static, 4096)
+  for (int i = 0; i < n; ++i) {
+    int w = S.off[i];
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
+      if (A.ci[k] != i && st[k]) S.col[w++] = A.ci[k];
+  }
+  return S;
+}
+
+// Transpose of the strong couplings: for every j, the rows i that depend
+// strongly on j, ascending (the lists of strong_transpose_adj).
+static void strong_transpose(const StrongRows& S, int n, std::vector<int>& off, std::vector<int>& src) {
+  off.assign(n + 1, 0);
+  for (int j : S.col) off[j + 1]++;
+  for (int j = 0; j < n; ++j) off[j + 1] += off[j];
+  src.resize(off[n]);
+  std::vector<int> pos(off.begin(), off.end() - 1);
+  for (int i = 0; i < n; ++i)
+    for (int t = S.begin(i); t < S.end(i); ++t) src[pos[S.col[t]]++] = i;
+}
+
 static bool has_strong_nbr(const CSR& A, const std::vector<uint8_t>& st, int i) {
   for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
     if (A.ci[k] != i && st[k]) return true;
@@ -336,22 +381,22 @@ struct Buckets {
 };
 }  // namespace
 
-static std::vector<int> rs_first_pass(const CSR& A, const std::vector<uint8_t>& st, bool use_zpt) {
-  const int n = A.n;
+static std::vector<int> rs_first_pass(const StrongRows& S, int n, bool use_zpt) {
   const int f_pnt = use_zpt ? -2 : -1;
-  std::vector<int> lam = strong_transpose_count(A, st);
   std::vector<int> st_off, st_src;
-  strong_transpose_adj(A, st, st_off, st_src);
+  strong_transpose(S, n, st_off, st_src);
+  std::vector<int> lam(n);
+  for (int i = 0; i < n; ++i) lam[i] = st_off[i + 1] - st_off[i];
   std::vector<int> cf(n, 0);
   for (int i = 0; i < n; ++i)
-    if (!has_strong_nbr(A, st, i) && lam[i] == 0) cf[i] = 1;
+    if (S.begin(i) == S.end(i) && lam[i] == 0) cf[i] = 1;
   for (int i = 0; i < n; ++i) {
     if (cf[i] != 0) continue;
     if (lam[i] == 0) {
       cf[i] = f_pnt;
-      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
-        int j = A.ci[k];
-        if (j != i && st[k] && cf[j] == 0) lam[j]++;
+      for (int t = S.begin(i); t < S.end(i); ++t) {
+        const int j = S.col[t];
+        if (cf[j] == 0) lam[j]++;
       }
     }
   }
@@ -370,31 +415,31 @@ static std::vector<int> rs_first_pass(const CSR& A, const std::vector<uint8_t>& 
     B.remove(best);
     cf[best] = 1;
     for (int idx = st_off[best]; idx < st_off[best + 1]; ++idx) {
-      int j = st_src[idx];
+      const int j = st_src[idx];
       if (cf[j] != 0) continue;
       B.remove(j);
       cf[j] = -1;
-      for (int k2 = A.rp[j]; k2 < A.rp[j + 1]; ++k2) {
-        int q = A.ci[k2];
-        if (q != j && st[k2] && cf[q] == 0) {
-          int nv = lam[q] + 1;
+      for (int t = S.begin(j); t < S.end(j); ++t) {
+        const int q = S.col[t];
+        if (cf[q] == 0) {
+          const int nv = lam[q] + 1;
           B.update(q, nv);
           if (nv > top) top = nv;
         }
       }
     }
-    for (int k = A.rp[best]; k < A.rp[best + 1]; ++k) {
-      int j = A.ci[k];
-      if (j != best && st[k] && cf[j] == 0) {
-        int nv = std::max(0, lam[j] - 1);
+    for (int t = S.begin(best); t < S.end(best); ++t) {
+      const int j = S.col[t];
+      if (cf[j] == 0) {
+        const int nv = std::max(0, lam[j] - 1);
         B.update(j, nv);
         if (nv == 0) {
           B.remove(j);
           cf[j] = f_pnt;
-          for (int k2 = A.rp[j]; k2 < A.rp[j + 1]; ++k2) {
-            int q = A.ci[k2];
-            if (q != j && st[k2] && cf[q] == 0) {
-              int nv2 = lam[q] + 1;
+          for (int t2 = S.begin(j); t2 < S.end(j); ++t2) {
+            const int q = S.col[t2];
+            if (cf[q] == 0) {
+              const int nv2 = lam[q] + 1;
               B.update(q, nv2);
               if (nv2 > top) top = nv2;
             }
@@ -406,9 +451,8 @@ static std::vector<int> rs_first_pass(const CSR& A, const std::vector<uint8_t>& 
   return cf;
 }
 
-static void pmis_on_undecided(std::vector<int>& cf, const CSR& A, const std::vector<uint8_t>& st,
-                              const std::vector<double>& meas) {
-  const int n = A.n;
+static void pmis_on_undecided(std::vector<int>& cf, const StrongRows& S, const std::vector<double>& meas) {
+  const int n = (int)cf.size();
   for (int it = 0; it <= n; ++it) {
     bool all_decided = true;
     for (int i = 0; i < n; ++i) {
@@ -416,16 +460,16 @@ static void pmis_on_undecided(std::vector<int>& cf, const CSR& A, const std::vec
       all_decided = false;
       if (meas[i] < 1.0) { cf[i] = -1; continue; }
       bool is_max = true;
-      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
-        int j = A.ci[k];
-        if (j != i && st[k] && cf[j] != -1 && meas[j] > meas[i]) { is_max = false; break; }
+      for (int t = S.begin(i); t < S.end(i); ++t) {
+        const int j = S.col[t];
+        if (cf[j] != -1 && meas[j] > meas[i]) { is_max = false; break; }
       }
       if (is_max) cf[i] = 1;
     }
     for (int i = 0; i < n; ++i) {
       if (cf[i] != 0) continue;
-      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
-        if (st[k] && cf[A.ci[k]] == 1) { cf[i] = -1; break; }
+      for (int t = S.begin(i); t < S.end(i); ++t)
+        if (cf[S.col[t]] == 1) { cf[i] = -1; break; }
     }
     if (all_decided) break;
   }
@@ -441,18 +485,19 @@ void coarsen_hmis(const CSR& A, double theta, uint64_t& rng, std::vector<int>& c
     build_cmap(cf, cmap, nc);
     return;
   }
-  std::vector<uint8_t> st = strength_absolute(A, theta);
-  cf = rs_first_pass(A, st, true);
-  std::vector<int> stc = strong_transpose_count(A, st);
+  const StrongRows S = strong_rows(A, strength_absolute(A, theta));
+  cf = rs_first_pass(S, n, true);
+  std::vector<int> stc(n, 0);
+  for (int j : S.col) stc[j]++;
   std::vector<double> meas(n);
   for (int i = 0; i < n; ++i) meas[i] = (double)stc[i] + rng_uniform(rng);
   for (int i = 0; i < n; ++i) {
     if (cf[i] == -2) {
-      if (meas[i] >= 1.0 || has_strong_nbr(A, st, i)) cf[i] = 0;
+      if (meas[i] >= 1.0 || S.begin(i) != S.end(i)) cf[i] = 0;
       else cf[i] = -1;
     }
   }
-  pmis_on_undecided(cf, A, st, meas);
+  pmis_on_undecided(cf, S, meas);
   build_cmap(cf, cmap, nc);
 }
 
