@@ -427,9 +427,9 @@ OPS = {0: "spmv", 2: "jacobi", 3: "restrict", 4: "prolong", 6: "zero_jacobi_resi
 
 
 def op_bytes(op, prec, n, nnz, nc, nnzp):
-    """Algorithmic bytes of one level kernel (each operand once, int32
-    indices; the formulas of the survey's measurement table, with V = 8 for
-    FP64 and 4 for FP32 values and vectors)."""
+    """Algorithmic bytes of one level kernel: every operand counted once,
+    the x gather once per vector entry (ideal reuse), int32 indices, and
+    V = 8 bytes per value and vector entry in FP64, 4 in FP32."""
     V = 8 if prec == 0 else 4
     if op == 0:
         return nnz * (4 + V) + 4 * (n + 1) + 2 * n * V

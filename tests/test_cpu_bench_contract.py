@@ -1,6 +1,6 @@
 """The JSON line of bench.py's reference arm (the oracle's PCG on the host
-cores), run at a small size on the CPU: one line with the keys the driver
-reads, the same metric and units as the product arm, and the e2e and
+cores), run at a small size on the CPU: one JSON line with the benchmark
+keys, the same metric and units as the product arm, and the e2e and
 cpu_baseline objects it has to carry."""
 
 import json
