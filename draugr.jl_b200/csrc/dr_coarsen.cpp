@@ -299,6 +299,60 @@ static bool has_strong_nbr(const CSR& A, const std::vector<uint8_t>& st, int i) 
   return false;
 }
 
+// PMIS sweeps over an adjacency (off, col), until no point is undecided
+// (0): every undecided point that no neighbour outside F beats by measure
+// becomes C, then every undecided point with a C neighbour becomes F.  With
+// f_below_one (HMIS) an undecided point of measure below one becomes F
+// instead of being tested.  Within a sweep no decision changes the outcome
+// of another: C and undecided both count as "outside F", and a point made F
+// for its measure could not beat any point that is tested.  So every sweep
+// decides its points in parallel from the state before it, and gives the
+// same states as deciding them one after another in row order.
+static void pmis_sweeps(std::vector<int>& cf, const std::vector<int>& off, const std::vector<int>& col,
+                        const std::vector<double>& meas, bool f_below_one) {
+  const int n = (int)cf.size();
+  std::vector<int8_t> nxt(n, 0);
+  for (;;) {
+    int undecided = 0;
+#pragma omp parallel for schedule(static, 4096) reduction(+ : undecided)
+    for (int i = 0; i < n; ++i) {
+      nxt[i] = 0;
+      if (cf[i] != 0) continue;
+      ++undecided;
+      if (f_below_one && meas[i] < 1.0) {
+        nxt[i] = -1;
+        continue;
+      }
+      bool is_max = true;
+      for (int t = off[i]; t < off[i + 1]; ++t) {
+        const int j = col[t];
+        if (cf[j] != -1 && meas[j] > meas[i]) {
+          is_max = false;
+          break;
+        }
+      }
+      if (is_max) nxt[i] = 1;
+    }
+    if (undecided == 0) break;
+#pragma omp parallel for schedule(static, 4096)
+    for (int i = 0; i < n; ++i)
+      if (nxt[i]) cf[i] = nxt[i];
+#pragma omp parallel for schedule(static, 4096)
+    for (int i = 0; i < n; ++i) {
+      nxt[i] = 0;
+      if (cf[i] != 0) continue;
+      for (int t = off[i]; t < off[i + 1]; ++t)
+        if (cf[col[t]] == 1) {
+          nxt[i] = -1;
+          break;
+        }
+    }
+#pragma omp parallel for schedule(static, 4096)
+    for (int i = 0; i < n; ++i)
+      if (nxt[i]) cf[i] = nxt[i];
+  }
+}
+
 static void build_cmap(const std::vector<int>& cf, std::vector<int>& cmap, int& nc) {
   const int n = (int)cf.size();
   cmap.assign(n, -1);
@@ -316,34 +370,15 @@ void coarsen_pmis(const CSR& A, double theta, uint64_t& rng, std::vector<int>& c
     build_cmap(cf, cmap, nc);
     return;
   }
-  std::vector<uint8_t> st = strength_absolute(A, theta);
-  std::vector<int> stc = strong_transpose_count(A, st);
+  const StrongRows S = strong_rows(A, strength_absolute(A, theta));
+  std::vector<int> stc(n, 0);
+  for (int j : S.col) stc[j]++;
   std::vector<double> meas(n);
   for (int i = 0; i < n; ++i) meas[i] = (double)stc[i] + rng_uniform(rng);
   cf.assign(n, 0);
   for (int i = 0; i < n; ++i)
-    if (!has_strong_nbr(A, st, i) && stc[i] == 0) cf[i] = 1;
-  for (int it = 0; it <= n; ++it) {
-    bool all_decided = true;
-    for (int i = 0; i < n; ++i) {
-      if (cf[i] != 0) continue;
-      all_decided = false;
-      bool is_max = true;
-      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
-        int j = A.ci[k];
-        if (st[k] && j != i && cf[j] != -1 && meas[j] > meas[i]) { is_max = false; break; }
-      }
-      if (is_max) cf[i] = 1;
-    }
-    for (int i = 0; i < n; ++i) {
-      if (cf[i] != 0) continue;
-      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
-        if (st[k] && cf[A.ci[k]] == 1) { cf[i] = -1; break; }
-    }
-    if (all_decided) break;
-  }
-  for (int i = 0; i < n; ++i)
-    if (cf[i] == 0) cf[i] = 1;
+    if (S.begin(i) == S.end(i) && stc[i] == 0) cf[i] = 1;
+  pmis_sweeps(cf, S.off, S.col, meas, false);
   build_cmap(cf, cmap, nc);
 }
 
@@ -452,29 +487,7 @@ static std::vector<int> rs_first_pass(const StrongRows& S, int n, bool use_zpt) 
 }
 
 static void pmis_on_undecided(std::vector<int>& cf, const StrongRows& S, const std::vector<double>& meas) {
-  const int n = (int)cf.size();
-  for (int it = 0; it <= n; ++it) {
-    bool all_decided = true;
-    for (int i = 0; i < n; ++i) {
-      if (cf[i] != 0) continue;
-      all_decided = false;
-      if (meas[i] < 1.0) { cf[i] = -1; continue; }
-      bool is_max = true;
-      for (int t = S.begin(i); t < S.end(i); ++t) {
-        const int j = S.col[t];
-        if (cf[j] != -1 && meas[j] > meas[i]) { is_max = false; break; }
-      }
-      if (is_max) cf[i] = 1;
-    }
-    for (int i = 0; i < n; ++i) {
-      if (cf[i] != 0) continue;
-      for (int t = S.begin(i); t < S.end(i); ++t)
-        if (cf[S.col[t]] == 1) { cf[i] = -1; break; }
-    }
-    if (all_decided) break;
-  }
-  for (int i = 0; i < n; ++i)
-    if (cf[i] == 0) cf[i] = -1;
+  pmis_sweeps(cf, S.off, S.col, meas, true);
 }
 
 void coarsen_hmis(const CSR& A, double theta, uint64_t& rng, std::vector<int>& cf,
@@ -621,68 +634,58 @@ void coarsen_aggressive_cf(const CSR& A_in, double theta, bool base_hmis, const 
   std::vector<int> st_off, st_src;
   strong_transpose_adj(A, st, st_off, st_src);
   std::vector<int> noff(m + 1, 0);
-  std::vector<std::vector<int>> nbr_chunks;
-  std::vector<int> ncount(m, 0);
   std::vector<int> nflat;
   {
-    // two passes (count, fill) over a, each with a per-thread marker array
-    std::vector<std::vector<int>> rows(m);
+    // the neighbours of a, in visiting order, each once (count, then fill)
+    auto walk = [&](int a, std::vector<int>& mark, auto&& emit) {
+      const int node = cidx[a];
+      auto add = [&](int b) {
+        if (b != a && mark[b] != a) {
+          mark[b] = a;
+          emit(b);
+        }
+      };
+      // cn(node): strong C neighbours of node(a) (a -> them via "i is C")
+      for (int k = A.rp[node]; k < A.rp[node + 1]; ++k) {
+        const int j = A.ci[k];
+        if (j != node && st[k] && cf1[j] == 1) add(clocal[j]);
+      }
+      // every i that has node(a) as a strong neighbour
+      for (int t = st_off[node]; t < st_off[node + 1]; ++t) {
+        const int i = st_src[t];
+        if (cf1[i] == 1) add(clocal[i]);
+        for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+          const int j = A.ci[k];
+          if (j != i && st[k] && cf1[j] == 1) add(clocal[j]);
+        }
+      }
+    };
 #pragma omp parallel
     {
       std::vector<int> mark(m, -1);
-      std::vector<int> buf;
 #pragma omp for schedule(dynamic, 256)
       for (int a = 0; a < m; ++a) {
-        buf.clear();
-        int node = cidx[a];
-        auto add = [&](int b) {
-          if (b != a && mark[b] != a) { mark[b] = a; buf.push_back(b); }
-        };
-        // cn(node): strong C neighbours of node(a) (a -> them via "i is C")
-        for (int k = A.rp[node]; k < A.rp[node + 1]; ++k) {
-          int j = A.ci[k];
-          if (j != node && st[k] && cf1[j] == 1) add(clocal[j]);
-        }
-        // every i that has node(a) as a strong neighbour
-        for (int t = st_off[node]; t < st_off[node + 1]; ++t) {
-          int i = st_src[t];
-          if (cf1[i] == 1) add(clocal[i]);
-          for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
-            int j = A.ci[k];
-            if (j != i && st[k] && cf1[j] == 1) add(clocal[j]);
-          }
-        }
-        rows[a] = buf;
+        int cnt = 0;
+        walk(a, mark, [&](int) { ++cnt; });
+        noff[a + 1] = cnt;
       }
     }
-    for (int a = 0; a < m; ++a) noff[a + 1] = noff[a] + (int)rows[a].size();
+    for (int a = 0; a < m; ++a) noff[a + 1] += noff[a];
     nflat.resize(noff[m]);
-    for (int a = 0; a < m; ++a) std::copy(rows[a].begin(), rows[a].end(), nflat.begin() + noff[a]);
+#pragma omp parallel
+    {
+      std::vector<int> mark(m, -1);
+#pragma omp for schedule(dynamic, 256)
+      for (int a = 0; a < m; ++a) {
+        int w = noff[a];
+        walk(a, mark, [&](int b) { nflat[w++] = b; });
+      }
+    }
   }
   std::vector<double> cmeas(m);
   for (int a = 0; a < m; ++a) cmeas[a] = (double)(noff[a + 1] - noff[a]) + rng_uniform(rng);
   std::vector<int> cf2(m, 0);
-  for (int it = 0; it <= m; ++it) {
-    bool all_decided = true;
-    for (int a = 0; a < m; ++a) {
-      if (cf2[a] != 0) continue;
-      all_decided = false;
-      bool is_max = true;
-      for (int t = noff[a]; t < noff[a + 1]; ++t) {
-        int b = nflat[t];
-        if (cf2[b] != -1 && cmeas[b] > cmeas[a]) { is_max = false; break; }
-      }
-      if (is_max) cf2[a] = 1;
-    }
-    for (int a = 0; a < m; ++a) {
-      if (cf2[a] != 0) continue;
-      for (int t = noff[a]; t < noff[a + 1]; ++t)
-        if (cf2[nflat[t]] == 1) { cf2[a] = -1; break; }
-    }
-    if (all_decided) break;
-  }
-  for (int a = 0; a < m; ++a)
-    if (cf2[a] == 0) cf2[a] = 1;
+  pmis_sweeps(cf2, noff, nflat, cmeas, false);
   cf = cf1;
   for (int a = 0; a < m; ++a)
     if (cf2[a] == -1) cf[cidx[a]] = -1;
