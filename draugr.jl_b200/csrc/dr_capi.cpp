@@ -401,6 +401,16 @@ int64_t draugr_b200_export(int32_t handle, int32_t lvl, const char* what, void* 
   return result;
 }
 
+const char* draugr_b200_config_json(int32_t config_handle) {
+  static thread_local std::string s;
+  s.clear();
+  const int32_t rc = guarded("draugr_b200_config_json", [&]() -> int32_t {
+    s = config_to_json(get_cfg(config_handle));
+    return 0;
+  });
+  return rc < 0 ? nullptr : s.c_str();
+}
+
 const char* draugr_b200_summary(int32_t handle) {
   static thread_local std::string s;
   s.clear();

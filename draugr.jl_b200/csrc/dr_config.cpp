@@ -397,4 +397,51 @@ std::string coarsening_name(const Coarsening& c) {
   return o.str();
 }
 
+namespace {
+const char* coarsen_key(CoarsenKind k) {
+  switch (k) {
+    case CoarsenKind::Aggregation: return "aggregation";
+    case CoarsenKind::PMIS: return "pmis";
+    case CoarsenKind::HMIS: return "hmis";
+    case CoarsenKind::RS: return "rs";
+    case CoarsenKind::AggressivePMIS: return "aggressive_pmis";
+    case CoarsenKind::AggressiveHMIS: return "aggressive_hmis";
+    case CoarsenKind::SmoothedAggregation: return "smoothed_aggregation";
+  }
+  return "?";
+}
+
+const char* interp_key(InterpKind k) {
+  return k == InterpKind::Direct ? "direct" : k == InterpKind::Standard ? "standard" : "extended_i";
+}
+
+void coarsening_json(std::ostringstream& o, const Coarsening& c) {
+  o << "{\"type\": \"" << coarsen_key(c.kind) << "\", \"theta\": " << c.theta
+    << ", \"interpolation\": {\"type\": \"" << interp_key(c.interp.kind)
+    << "\", \"trunc_factor\": " << c.interp.trunc_factor << ", \"max_elements\": " << c.interp.max_elements
+    << ", \"norm_p\": " << c.interp.norm_p << ", \"rescale\": " << (c.interp.rescale ? "true" : "false")
+    << "}, \"filtering\": " << (c.filtering ? "true" : "false") << ", \"filter_tol\": " << c.filter_tol
+    << ", \"omega\": " << c.sa_omega << "}";
+}
+}  // namespace
+
+std::string config_to_json(const Config& c) {
+  std::ostringstream o;
+  o.precision(17);
+  o << "{\"coarsening\": ";
+  coarsening_json(o, c.coarsening);
+  o << ", \"initial_coarsening\": ";
+  coarsening_json(o, c.initial_coarsening);
+  o << ", \"initial_coarsening_levels\": " << c.initial_coarsening_levels << ", \"smoother\": \""
+    << smoother_name(c.smoother) << "\", \"jacobi_omega\": " << c.jacobi_omega
+    << ", \"max_levels\": " << c.max_levels << ", \"max_coarse_size\": " << c.max_coarse_size
+    << ", \"pre_smoothing_steps\": " << c.pre_smoothing_steps
+    << ", \"post_smoothing_steps\": " << c.post_smoothing_steps << ", \"verbose\": " << c.verbose
+    << ", \"max_row_sum\": " << c.max_row_sum << ", \"cycle\": \"" << (c.cycle_w ? "w" : "v")
+    << "\", \"strength\": \"" << (c.strength == StrengthKind::Signed ? "signed" : "absolute")
+    << "\", \"coarse_solve_on_cpu\": " << (c.coarse_solve_on_cpu ? "true" : "false")
+    << ", \"seed\": " << c.seed << "}";
+  return o.str();
+}
+
 }  // namespace dr

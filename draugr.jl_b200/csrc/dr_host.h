@@ -128,6 +128,9 @@ Config config_from_json(const char* json);   // src/cfunction_interface.jl:178-2
 Config hypre_default_config(double agg_trunc_factor);
 std::string smoother_name(SmootherKind k);
 std::string coarsening_name(const Coarsening& c);
+// Every field of a parsed configuration as JSON (lower-case type names as
+// the parser accepts them; coarsening and initial coarsening as objects).
+std::string config_to_json(const Config& c);
 
 // ---------------------------------------------------------------------------
 // Hierarchy (host side).  One HostLevel per AMG level (src/types.jl:431-440)

@@ -33,6 +33,7 @@ SIGNATURES = {
     "draugr_b200_level_info": (i32, [i32, i32, P]),
     "draugr_b200_export": (i64, [i32, i32, C.c_char_p, P, i64]),
     "draugr_b200_summary": (C.c_char_p, [i32]),
+    "draugr_b200_config_json": (C.c_char_p, [i32]),
     "draugr_b200_device_bytes": (i64, [i32]),
     "draugr_b200_solve_device": (i32, [i32, i32, P, P, i32, f64, i32]),
     "draugr_b200_cycle_device": (i32, [i32, i32, P, P, i32]),

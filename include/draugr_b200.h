@@ -53,6 +53,17 @@ int64_t draugr_b200_export(int32_t handle, int32_t lvl, const char *what, void *
  * (src/setup.jl:405-473).  Valid until the next call. */
 const char *draugr_b200_summary(int32_t handle);
 
+/* Every field of a parsed configuration as JSON, for inspection: the
+ * coarsening and initial coarsening as objects (type, theta, interpolation
+ * with its options, aggregation filtering, smoothed-aggregation omega),
+ * then smoother, jacobi_omega, level and step counts, verbose,
+ * max_row_sum, cycle ("v" or "w"), strength, coarse_solve_on_cpu and seed.
+ * Type names are the lower-case names draugr_amg_config_from_json accepts.
+ * The reference's Julia callers read the same fields from the config object
+ * behind the handle (src/cfunction_interface.jl:165-221).  Valid until the
+ * next call on this thread; NULL on an invalid handle. */
+const char *draugr_b200_config_json(int32_t config_handle);
+
 /* Device memory held by the hierarchy, in bytes (0 if host-only). */
 int64_t draugr_b200_device_bytes(int32_t handle);
 
