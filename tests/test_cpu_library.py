@@ -7,6 +7,7 @@ import re
 
 import numpy as np
 import pytest
+import scipy.sparse as sp
 
 import draugr
 import oracle
@@ -245,3 +246,37 @@ def test_preconditioner_before_update():
     assert P.nrows == 0 and P.hierarchy is None
     with pytest.raises(draugr.DraugrError):
         P.apply(np.zeros(4), np.ones(4))
+
+
+def test_csr_from_raw_testsets(lib):
+    """testset "csr_from_raw" (test/runtests.jl:3157-3224), through the C
+    ABI: the same 3 x 3 matrix given one-based and zero-based arrives as
+    the same CSR (read back as the coarsest matrix, 0-based) with A * 1 =
+    (1, 0, 1); a zero-based 50 x 50 tridiagonal solves to 1e-6 with the
+    default configuration; index_base 2 is rejected."""
+    p = lambda a: a.ctypes.data_as(draugr._lib.C.c_void_p)
+    cfg = draugr.config_handle(draugr.AMGConfig())
+    v = np.array([2.0, -1.0, -1.0, 2.0, -1.0, -1.0, 2.0])
+    got = []
+    for base, rp, ci in ((1, [1, 3, 6, 8], [1, 2, 1, 2, 3, 2, 3]), (0, [0, 2, 5, 7], [0, 1, 0, 1, 2, 1, 2])):
+        rp, ci = np.array(rp, np.int32), np.array(ci, np.int32)
+        h = lib.draugr_b200_setup_host(3, 7, p(rp), p(ci), p(v), cfg, base, 1)
+        assert h > 0, draugr.last_error()
+        H = draugr.Hierarchy(h, 3, None)
+        assert H.nlevels == 0
+        A = sp.csr_matrix((H.export(-1, "C_nzval"), H.export(-1, "C_colval"), H.export(-1, "C_rowptr")),
+                          shape=(3, 3))
+        assert (A[0, 0], A[0, 1], A[1, 0], A[1, 1], A[2, 2]) == (2.0, -1.0, -1.0, 2.0, 2.0)
+        assert np.array_equal(A @ np.ones(3), [1.0, 0.0, 1.0])
+        got.append(A)
+        H.free()
+    assert (got[0] != got[1]).nnz == 0
+    n = 50
+    T = sp.diags([np.full(n - 1, -1.0), np.full(n, 2.0), np.full(n - 1, -1.0)], [-1, 0, 1], format="csr")
+    h = draugr.amg_setup(T, draugr.AMGConfig(), on_device=False)
+    O = oracle.OracleHierarchy(h)
+    x, _, _ = O.solve(np.zeros(n), np.ones(n), tol=1e-6, maxiter=100)
+    assert np.linalg.norm(np.ones(n) - T @ x) / np.sqrt(n) < 1e-6
+    rp, ci = np.array([1, 3, 5], np.int32), np.array([1, 2, 1, 2], np.int32)
+    assert lib.draugr_b200_setup_host(2, 4, p(rp), p(ci), p(np.array([1.0, 2.0, 3.0, 4.0])), cfg, 2, 1) == -1
+    assert "index_base" in draugr.last_error()
