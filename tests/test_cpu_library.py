@@ -280,3 +280,44 @@ def test_csr_from_raw_testsets(lib):
     rp, ci = np.array([1, 3, 5], np.int32), np.array([1, 2, 1, 2], np.int32)
     assert lib.draugr_b200_setup_host(2, 4, p(rp), p(ci), p(np.array([1.0, 2.0, 3.0, 4.0])), cfg, 2, 1) == -1
     assert "index_base" in draugr.last_error()
+
+
+def test_full_resetup_and_direct_solve_testsets():
+    """testsets "AMG Resetup - partial=false", "... with
+    allow_partial_resetup", "... partial=false, allow_partial_resetup=false"
+    and "Small System Direct Solve" (test/runtests.jl:467-547), on host-only
+    hierarchies: a full resetup rebuilds the hierarchy from the new values
+    (the solve then meets 1e-8 on 2A and differs from the first), keeps or
+    drops the Galerkin maps as allow_partial_resetup says, and a system no
+    larger than max_coarse_size has no levels and is solved directly to
+    1e-10.  (The partial resetup that follows in the second testset runs on
+    the GPU and is covered there.)"""
+    A = problems.poisson2d(10)
+    cfg = draugr.AMGConfig(coarsening=draugr.AggregationCoarsening())
+    b = np.random.default_rng(21).uniform(0, 1, 100)
+
+    def solve(h, M):
+        x, _, _ = oracle.OracleHierarchy(h).solve(np.zeros(100), b, tol=1e-8, maxiter=200)
+        assert np.linalg.norm(b - M @ x) / np.linalg.norm(b) < 1e-8
+        return x
+
+    h = draugr.amg_setup(A, cfg, on_device=False)
+    x1 = solve(h, A)
+    A2 = A.copy()
+    A2.data = A2.data * 2.0
+    draugr.amg_resetup(h, A2, cfg, partial=False)
+    x2 = solve(h, A2)
+    assert not np.allclose(x1, x2, atol=1e-6)
+    h = draugr.amg_setup(A, cfg, allow_partial_resetup=False, on_device=False)
+    assert all(h.level_info(l)[6] == -1 for l in range(h.nlevels))
+    draugr.amg_resetup(h, A, cfg, partial=False, allow_partial_resetup=True)
+    assert h.nlevels > 0 and all(h.level_info(l)[6] >= 0 for l in range(h.nlevels))
+    h = draugr.amg_setup(A, cfg, on_device=False)
+    draugr.amg_resetup(h, A, cfg, partial=False, allow_partial_resetup=False)
+    assert all(h.level_info(l)[6] == -1 for l in range(h.nlevels))
+    solve(h, A)
+    A5 = problems.poisson1d(5)
+    h = draugr.amg_setup(A5, draugr.AMGConfig(max_coarse_size=10), on_device=False)
+    assert h.nlevels == 0
+    x, _, _ = oracle.OracleHierarchy(h).solve(np.zeros(5), np.ones(5), tol=1e-10)
+    assert np.linalg.norm(np.ones(5) - A5 @ x) < 1e-10
