@@ -28,8 +28,23 @@ def agg_hierarchy(A, **kw):
     return draugr.amg_setup(A, cfg, on_device=False)
 
 
+def test_strength_and_aggregation_coarsening():
+    """testsets "Strength of Connection" and "Aggregation Coarsening"
+    (:96-116): every off-diagonal entry of the 1D Laplacian (10) is strong
+    at theta 0.25 (18 of them); aggregation of the 1D Laplacian (20) gives
+    0 < nc < 20 aggregates covering every point, none of them empty."""
+    n, rp, ci, v = parts(problems.poisson1d(10))
+    assert int(np.sum(oracle.strength_abs(n, rp, ci, v, 0.25))) == 18
+    h = agg_hierarchy(problems.poisson1d(20))
+    P = explicit_P(h, 0)
+    nc = P.shape[1]
+    assert P.shape[0] == 20 and 0 < nc < 20
+    assert np.all(np.diff(P.indptr) == 1)
+    assert set(P.indices.tolist()) == set(range(nc))
+
+
 def test_prolongation_and_restriction():
-    """testset "Prolongation" (:71-124): aggregation P has one unit entry per
+    """testset "Prolongation" (:138-179): aggregation P has one unit entry per
     row, P*ones = ones, restriction preserves the sum, the transpose map has
     nc+1 offsets ending at nnz(P)+1, and restrict! equals the explicit Pᵀr
     (atol 1e-12)."""
@@ -72,7 +87,7 @@ def _galerkin_check(A, scale):
 
 
 def test_galerkin_product():
-    """testsets "Galerkin Product" (:214-241), "contention-free kernel"
+    """testsets "Galerkin Product" (:215-241), "contention-free kernel"
     (:181-212) and "In-place Galerkin Resetup" (:243-270)."""
     _galerkin_check(problems.poisson1d(10), 2.0)
     _galerkin_check(problems.poisson1d(20), 3.0)
