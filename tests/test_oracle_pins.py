@@ -417,3 +417,55 @@ def test_lu_matches_numpy():
     S = M.copy()
     S[:, 3] = 0.0
     assert oracle.lu_factor(S)[2] == 4  # SingularException(4)
+
+
+def test_l1_jacobi_lu_refactorization_and_cpu_coarse_solve():
+    """testsets "l1-Jacobi Smoother - Build / Smoothing / AMG Solve /
+    Resetup" (:1857-1908), "In-place LU Refactorization" (:1103-1129), "AMG
+    Solve - coarse_solve_on_cpu" (:374-390), "AMG Setup - Aggregation" and
+    "AMG Cycle Convergence - Aggregation" (:286-330): the l1 inverse
+    diagonal of an interior row of the 1D Laplacian is 1/4 and ten sweeps
+    reduce the residual; l1-Jacobi and coarse_solve_on_cpu hierarchies solve
+    10 x 10 to 1e-8 in fewer than 200 cycles; after a resetup with doubled
+    values (which refactorises the coarsest LU) the solve again meets 1e-8;
+    five V(2,2) cycles of an aggregation hierarchy on 20 x 20 reduce the
+    residual of b = 1."""
+    n, rp, ci, v = parts(problems.poisson1d(10))
+    invd = oracle.invdiag(n, rp, ci, v, l1=True)
+    assert len(invd) == 10 and invd[4] == pytest.approx(0.25)
+    b = np.ones(10)
+    x = oracle.jacobi(n, rp, ci, v, invd, 2.0 / 3.0, np.zeros(10), b, 10)
+    A1 = problems.poisson1d(10)
+    assert np.linalg.norm(b - A1 @ x) < np.linalg.norm(b)
+    A = problems.poisson2d(10)
+    b = np.random.default_rng(31).uniform(0, 1, 100)
+    for cfg in (draugr.AMGConfig(smoother=draugr.L1JacobiSmootherType()),
+                draugr.AMGConfig(coarse_solve_on_cpu=True)):
+        h = draugr.amg_setup(A, cfg, on_device=False)
+        x, it, _ = oracle.OracleHierarchy(h).solve(np.zeros(100), b, tol=1e-8, maxiter=200)
+        assert it < 200 and np.linalg.norm(b - A @ x) / np.linalg.norm(b) < 1e-8
+    A8 = problems.poisson2d(8)
+    b8 = np.random.default_rng(32).uniform(0, 1, 64)
+    for cfg in (draugr.AMGConfig(smoother=draugr.L1JacobiSmootherType()),
+                draugr.AMGConfig(coarsening=draugr.AggregationCoarsening())):
+        h = draugr.amg_setup(A8, cfg, on_device=False)
+        O = oracle.OracleHierarchy(h)
+        x1, _, _ = O.solve(np.zeros(64), b8, tol=1e-8, maxiter=200)
+        assert np.linalg.norm(b8 - A8 @ x1) / np.linalg.norm(b8) < 1e-8
+        O.resetup(A8.data * 2.0)
+        x2, _, _ = O.solve(np.zeros(64), b8, tol=1e-8, maxiter=200)
+        assert np.linalg.norm(b8 - 2.0 * (A8 @ x2)) / np.linalg.norm(b8) < 1e-8
+    h = draugr.amg_setup(A, draugr.AMGConfig(coarsening=draugr.AggregationCoarsening()), on_device=False)
+    assert h.nlevels > 0
+    assert all(h.level_info(l)[2] < h.level_info(l)[0] for l in range(h.nlevels))
+    A20 = problems.poisson2d(20)
+    cfg = draugr.AMGConfig(coarsening=draugr.AggregationCoarsening(), pre_smoothing_steps=2,
+                           post_smoothing_steps=2)
+    h = draugr.amg_setup(A20, cfg, on_device=False)
+    assert h.nlevels > 0
+    O = oracle.OracleHierarchy(h)
+    b = np.ones(400)
+    x = np.zeros(400)
+    for _ in range(5):
+        x = O.cycle(x, b, 2, 2)
+    assert np.linalg.norm(b - A20 @ x) < np.linalg.norm(b)
