@@ -469,3 +469,45 @@ def test_l1_jacobi_lu_refactorization_and_cpu_coarse_solve():
     for _ in range(5):
         x = O.cycle(x, b, 2, 2)
     assert np.linalg.norm(b - A20 @ x) < np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("smoother", ["jacobi", "spai0", "l1_jacobi", "colored_gs", "l1_colored_gs", "ilu0",
+                                      "chebyshev", "spai1", "serial_gs", "serial_ilu0", "l1_serial_gs"])
+def test_every_smoother_type_smooths(smoother):
+    """testsets "Standalone Smoother API - build_smoother / smooth! /
+    update_smoother! / all types smooth correctly" (:2490-2562): on the 1D
+    Laplacian (10), the smoother the library builds for each type (Jacobi's
+    inverse diagonal is 0.5 throughout) takes ten sweeps of the oracle's
+    smoother from zero to a smaller residual than b = 1."""
+    A = problems.poisson1d(10)
+    cls = {k.name: k for k in (draugr.JacobiSmootherType, draugr.SPAI0SmootherType, draugr.L1JacobiSmootherType,
+                               draugr.ColoredGaussSeidelType, draugr.L1ColoredGaussSeidelType,
+                               draugr.ILU0SmootherType, draugr.ChebyshevSmootherType, draugr.SPAI1SmootherType,
+                               draugr.SerialGaussSeidelType, draugr.SerialILU0SmootherType,
+                               draugr.L1SerialGaussSeidelType)}[smoother]
+    h = draugr.amg_setup(A, draugr.AMGConfig(coarsening=draugr.AggregationCoarsening(), smoother=cls(),
+                                             max_coarse_size=2), on_device=False)
+    n, rp, ci, v = parts(A)
+    b = np.ones(n)
+    x0 = np.zeros(n)
+    invd = h.export(0, "invdiag")
+    omega = float(h.export(0, "omega")[0])
+    if smoother in ("jacobi", "l1_jacobi"):
+        if smoother == "jacobi":
+            assert np.all(invd == 0.5)
+        x = oracle.jacobi(n, rp, ci, v, invd, omega, x0, b, 10)
+    elif smoother == "spai0":
+        x = oracle.spai0_smooth(n, rp, ci, v, oracle.spai0(n, rp, ci, v), x0, b, 10)
+    elif smoother in ("colored_gs", "l1_colored_gs"):
+        off, order = h.export(0, "color_offsets"), h.export(0, "color_order")
+        x = oracle.gs(n, rp, ci, v, invd, len(off) - 1, off, order, x0, b, 10)
+    elif smoother in ("ilu0", "serial_ilu0"):
+        x = oracle.ilu0_smooth(n, rp, ci, v, h.export(0, "ilu_diag"), h.export(0, "ilu_L"), h.export(0, "ilu_U"),
+                               x0, b, 10)
+    elif smoother == "chebyshev":
+        x = oracle.chebyshev(n, rp, ci, v, invd, h.export(0, "cheb_coef"), x0, b, 10)
+    elif smoother == "spai1":
+        x = oracle.spai1_smooth(n, rp, ci, v, h.export(0, "spai1_M"), x0, b, 10)
+    else:
+        x = oracle.serial_gs(n, rp, ci, v, invd, x0, b, 10)
+    assert np.linalg.norm(b - A @ x) < np.linalg.norm(b)
