@@ -17,6 +17,7 @@
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
+#include <chrono>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -973,6 +974,8 @@ double DevHier::dot_host(const double* a, const double* b, int n) {
 
 int DevHier::solve(double* x, const double* b, const CycleOpts& o, double tol, int maxiter, int verbose,
                    double* relres) {
+  const auto t_solve = std::chrono::steady_clock::now();
+  auto secs = [&]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t_solve).count(); };
   const double bnorm = std::sqrt(dot_host(b, b, n0_));
   if (bnorm == 0.0) {
     counted();
@@ -999,12 +1002,14 @@ int DevHier::solve(double* x, const double* b, const CycleOpts& o, double tol, i
     if (verbose >= 2) std::printf("  AMG iter %4d: residual norm = %.6e, relative = %.6e\n", it, rnorm, rel);
     if (rel < tol || it == maxiter) check_kernel_flag(st_);
     if (rel < tol) {
-      if (verbose >= 1) std::printf("AMG solve converged: %d iterations, final residual %.2e\n", it, rel);
+      if (verbose >= 1)
+        std::printf("AMG solve converged: %d iterations, %.4f s, final residual %.2e\n", it, secs(), rel);
       if (relres) *relres = rel;
       return it;
     }
   }
-  if (verbose >= 1) std::printf("AMG solve did NOT converge: %d iterations, final residual %.2e\n", maxiter, rel);
+  if (verbose >= 1)
+    std::printf("AMG solve did NOT converge: %d iterations, %.4f s, final residual %.2e\n", maxiter, secs(), rel);
   if (relres) *relres = rel;
   return maxiter;
 }

@@ -785,6 +785,44 @@ void build_hierarchy(const CSR& A_in, const Config& cfg, bool allow_partial_rese
       std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
+namespace {
+// The smoother's configuration type name and its per-level display name, as
+// the reference's verbose setup print shows them (src/setup.jl:426, :478-488).
+const char* smoother_type_name(SmootherKind k) {
+  switch (k) {
+    case SmootherKind::Jacobi: return "JacobiSmootherType";
+    case SmootherKind::ColoredGS: return "ColoredGaussSeidelType";
+    case SmootherKind::SerialGS: return "SerialGaussSeidelType";
+    case SmootherKind::SPAI0: return "SPAI0SmootherType";
+    case SmootherKind::SPAI1: return "SPAI1SmootherType";
+    case SmootherKind::L1Jacobi: return "L1JacobiSmootherType";
+    case SmootherKind::L1ColoredGS: return "L1ColoredGaussSeidelType";
+    case SmootherKind::L1SerialGS: return "L1SerialGaussSeidelType";
+    case SmootherKind::Chebyshev: return "ChebyshevSmootherType";
+    case SmootherKind::ILU0: return "ILU0SmootherType";
+    case SmootherKind::SerialILU0: return "SerialILU0SmootherType";
+  }
+  return "?";
+}
+
+const char* smoother_display_name(SmootherKind k) {
+  switch (k) {
+    case SmootherKind::Jacobi: return "Jacobi";
+    case SmootherKind::ColoredGS: return "Colored GS";
+    case SmootherKind::SerialGS: return "Serial GS";
+    case SmootherKind::SPAI0: return "SPAI(0)";
+    case SmootherKind::SPAI1: return "SPAI(1)";
+    case SmootherKind::L1Jacobi: return "l1-Jacobi";
+    case SmootherKind::L1ColoredGS: return "l1-Colored GS";
+    case SmootherKind::L1SerialGS: return "l1-Serial GS";
+    case SmootherKind::Chebyshev: return "Chebyshev";
+    case SmootherKind::ILU0: return "ILU(0)";
+    case SmootherKind::SerialILU0: return "Serial ILU(0)";
+  }
+  return "?";
+}
+}  // namespace
+
 std::string hierarchy_summary(const HostHierarchy& H, int n_finest) {
   // Layout of _print_hierarchy_info, src/setup.jl:405-473.
   std::ostringstream o;
@@ -798,6 +836,7 @@ std::string hierarchy_summary(const HostHierarchy& H, int n_finest) {
   o << "  Levels:          " << nl + 1 << " (" << nl << " AMG + 1 coarse direct)\n";
   o << "  Cycle type:      " << (c.cycle_w ? "W" : "V") << "-cycle\n";
   o << "  Backend:         CUDA (sm_100a)\n";
+  o << "  Block size:      256 (row kernels on rows of 12-32 entries: 128)\n";
   o << "  Coarse solve:    "
     << (c.coarse_solve_on_cpu ? "GPU (coarse_solve_on_cpu requested; same LU solve, same values)" : "GPU")
     << "\n";
@@ -806,12 +845,15 @@ std::string hierarchy_summary(const HostHierarchy& H, int n_finest) {
   if (c.initial_coarsening_levels > 0)
     o << "  Initial coars.:  " << coarsening_name(c.initial_coarsening) << " (first "
       << c.initial_coarsening_levels << " levels)\n";
-  o << "  Smoother:        " << smoother_name(c.smoother) << "\n";
+  o << "  Smoother:        " << smoother_type_name(c.smoother) << "\n";
   if (c.smoother == SmootherKind::Jacobi || c.smoother == SmootherKind::L1Jacobi) {
     std::snprintf(buf, sizeof buf, "    omega = %.3f\n", c.jacobi_omega); o << buf;
   }
   std::snprintf(buf, sizeof buf, "  Pre-smooth:      %d steps, Post-smooth: %d steps\n",
                 c.pre_smoothing_steps, c.post_smoothing_steps); o << buf;
+  if (c.max_row_sum < 1.0) {
+    std::snprintf(buf, sizeof buf, "  Max row sum:     %.2f\n", c.max_row_sum); o << buf;
+  }
   o << "+-------+----------+-----------+---------+------------------------------------+\n";
   o << "  Level     Rows        NNZ      Ratio    Smoother                              \n";
   o << "+-------+----------+-----------+---------+------------------------------------+\n";
@@ -822,11 +864,11 @@ std::string hierarchy_summary(const HostHierarchy& H, int n_finest) {
     tot_rows += L.A.n;
     if (i == 0)
       std::snprintf(buf, sizeof buf, "  %5d   %7d    %8lld        -   %s\n", i + 1, L.A.n,
-                    (long long)L.A.nnz(), smoother_name(L.smoother).c_str());
+                    (long long)L.A.nnz(), smoother_display_name(L.smoother));
     else
       std::snprintf(buf, sizeof buf, "  %5d   %7d    %8lld    %5.3f   %s\n", i + 1, L.A.n,
                     (long long)L.A.nnz(), (double)L.A.n / H.levels[i - 1].A.n,
-                    smoother_name(L.smoother).c_str());
+                    smoother_display_name(L.smoother));
     o << buf;
   }
   int64_t cnz = 0;

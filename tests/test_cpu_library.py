@@ -211,9 +211,15 @@ def test_prolongation_properties(host_case):
 
 
 def test_hierarchy_summary(host_case):
+    """testset "Verbose Output" (test/runtests.jl:830-856), the setup part:
+    the summary carries the hierarchy header, the backend and block size,
+    and the operator complexity; the level table names the smoothers as the
+    reference's setup print does (src/setup.jl:478-488)."""
     name, A, cfg, h = host_case
     s = h.summary()
-    assert "AMG Hierarchy Summary" in s and "Operator complexity" in s
+    for key in ("AMG Hierarchy Summary", "Operator complexity", "Backend", "Block size", "Direct (LU)"):
+        assert key in s, key
+    assert type(cfg.smoother).__name__ in s
 
 
 def test_allow_partial_resetup_false_has_no_maps():
