@@ -217,6 +217,16 @@ def hypre_default_config(theta: float = 0.5, agg_num_levels: int = 1,
                      initial_coarsening_levels=agg_num_levels, **kwargs)
 
 
+def config_fields(config: AMGConfig | str | None) -> dict:
+    """Every field of the configuration as the library parsed it
+    (draugr_b200_config_json): coarsening and initial coarsening as dicts,
+    smoother, omega, level and step counts, cycle, strength and seed."""
+    text = _lib.load().draugr_b200_config_json(config_handle(config))
+    if text is None:
+        raise _lib.DraugrError(f"config_fields: {_lib.last_error()}")
+    return json.loads(text)
+
+
 _cfg_cache: dict[str, int] = {}
 
 

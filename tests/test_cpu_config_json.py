@@ -125,6 +125,20 @@ def test_invalid_input_and_handle_lifecycle(lib):
     assert c["coarsening"]["type"] == "hmis" and c["smoother"] == "l1_colored_gs" and c["cycle"] == "v"
 
 
+def test_python_mirror_round_trip():
+    """The Python mirror's AMGConfig goes through the same parser: its
+    fields read back unchanged (draugr.config_fields)."""
+    cfg = draugr.AMGConfig(coarsening=draugr.PMISCoarsening(0.3, draugr.StandardInterpolation(0.1)),
+                           smoother=draugr.ChebyshevSmootherType(), max_levels=7, cycle_type="W",
+                           strength_type=draugr.SignedStrength(), seed=9)
+    c = draugr.config_fields(cfg)
+    assert c["coarsening"]["type"] == "pmis" and c["coarsening"]["theta"] == pytest.approx(0.3)
+    assert c["coarsening"]["interpolation"]["type"] == "standard"
+    assert c["coarsening"]["interpolation"]["trunc_factor"] == pytest.approx(0.1)
+    assert (c["smoother"], c["max_levels"], c["cycle"], c["strength"], c["seed"]) == (
+        "chebyshev", 7, "w", "signed", 9)
+
+
 def test_full_realistic_config(lib):
     """"full realistic config" (:3474-3510)."""
     c = parse(lib, """{"coarsening": "hmis",
