@@ -332,6 +332,7 @@ class OracleHierarchy:
 
     def __init__(self, h, with_rmaps: bool = False):
         self._keep = []
+        self.with_rmaps = with_rmaps
         nl = h.nlevels
         self.nlevels = nl
         levels = (OLevel * max(nl, 1))()
@@ -432,6 +433,8 @@ class OracleHierarchy:
         return x, it, rel.value
 
     def resetup(self, new_values):
+        if self.nlevels > 1 and not self.with_rmaps:
+            raise ValueError("resetup of a hierarchy with more than one level needs with_rmaps=True")
         v = np.ascontiguousarray(new_values, np.float64)
         info = load().orc_resetup(C.byref(self.H), ptr(v), len(v))
         if info:

@@ -182,7 +182,7 @@ def test_smoothed_aggregation():
     # resetup with doubled values (P frozen) still solves to 1e-8
     cfg = draugr.AMGConfig(coarsening=alg, **V22)
     h = draugr.amg_setup(A, cfg, on_device=False)
-    O = oracle.OracleHierarchy(h)
+    O = oracle.OracleHierarchy(h, with_rmaps=True)
     _, it1, _ = O.solve(np.zeros(100), b, 2, 2, False, 1e-8, 200)
     assert it1 < 200
     A2 = A.copy()

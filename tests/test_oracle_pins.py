@@ -449,7 +449,7 @@ def test_l1_jacobi_lu_refactorization_and_cpu_coarse_solve():
     for cfg in (draugr.AMGConfig(smoother=draugr.L1JacobiSmootherType()),
                 draugr.AMGConfig(coarsening=draugr.AggregationCoarsening())):
         h = draugr.amg_setup(A8, cfg, on_device=False)
-        O = oracle.OracleHierarchy(h)
+        O = oracle.OracleHierarchy(h, with_rmaps=True)
         x1, _, _ = O.solve(np.zeros(64), b8, tol=1e-8, maxiter=200)
         assert np.linalg.norm(b8 - A8 @ x1) / np.linalg.norm(b8) < 1e-8
         O.resetup(A8.data * 2.0)
