@@ -350,3 +350,82 @@ def test_sparse_csc_input():
     O.resetup((2.0 * T).tocsr().data)
     x, it, _ = O.solve(np.zeros(n), b, tol=1e-6, maxiter=100)
     assert it < 100 and np.linalg.norm(b - 2.0 * (T @ x)) / np.linalg.norm(b) < 1e-6
+
+
+def _split_top(s):
+    """Split s at commas outside (), {} and []."""
+    out, depth, cur = [], 0, ""
+    for ch in s:
+        if ch in "({[":
+            depth += 1
+        elif ch in ")}]":
+            depth -= 1
+        if ch == "," and depth == 0:
+            out.append(cur.strip())
+            cur = ""
+        else:
+            cur += ch
+    if cur.strip():
+        out.append(cur.strip())
+    return out
+
+
+def _c_params():
+    """name -> (return type, [parameter types]) of every declared function."""
+    decls = {}
+    for h in HEADERS:
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        for m in re.finditer(r"([A-Za-z_][A-Za-z0-9_ \*]*?)\b(draugr_[A-Za-z0-9_]+|init_julia|shutdown_julia)"
+                             r"\s*\(([^)]*)\)\s*;", text):
+            params = [p.strip() for p in m.group(3).split(",") if p.strip() and p.strip() != "void"]
+            decls[m.group(2)] = (m.group(1).strip(), params)
+    return decls
+
+
+def test_julia_bindings_match_the_c_header():
+    """The Julia module cannot run here (no Julia in the image), so its
+    ccall signatures are checked against include/*.h: every symbol is
+    declared, with the same number of arguments, each of a matching kind
+    (Int32 / Int64 / Float64 / pointer / string), and a matching return."""
+    jl = (ROOT / "draugr.jl_b200" / "julia" / "DraugrB200.jl").read_text()
+    decls = _c_params()
+
+    def kind_c(t):
+        t = t.replace("const", "").strip()
+        if "char" in t and "*" in t:
+            return "str"
+        if "*" in t:
+            return "ptr"
+        base = t.split()[0]
+        return {"int32_t": "i32", "int64_t": "i64", "double": "f64", "float": "f32", "void": "void"}[base]
+
+    def kind_jl(t):
+        if t.startswith(("Ptr", "CuPtr", "Ref")):
+            return "ptr"
+        if t == "Cstring":
+            return "str"
+        return {"Int32": "i32", "Int64": "i64", "Float64": "f64", "Float32": "f32", "Cvoid": "void",
+                "Nothing": "void"}[t]
+
+    seen = 0
+    for m in re.finditer(r"ccall\(", jl):
+        depth, i = 0, m.end() - 1
+        while True:
+            depth += {"(": 1, ")": -1}.get(jl[i], 0)
+            if depth == 0:
+                break
+            i += 1
+        args = _split_top(jl[m.end():i])
+        name = re.match(r"\(:([A-Za-z0-9_]+)", args[0]).group(1)
+        ret, types = args[1], args[2].strip()
+        assert types.startswith("(") and types.endswith(")"), name
+        jtypes = _split_top(types[1:-1])
+        assert name in decls, name
+        cret, cparams = decls[name]
+        assert len(jtypes) == len(cparams), (name, jtypes, cparams)
+        for jt, ct in zip(jtypes, cparams):
+            ctype = re.sub(r"\b[A-Za-z_][A-Za-z0-9_]*$", "", ct).strip() or ct
+            assert kind_jl(jt) == kind_c(ctype), (name, jt, ct)
+        assert kind_jl(ret) == kind_c(cret), (name, ret, cret)
+        seen += 1
+    assert seen >= 15
