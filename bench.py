@@ -9,16 +9,20 @@ of 1e-8, checked in FP64):
   Hierarchy: hypre_default_config(agg_trunc_factor=0.2) with l1-Jacobi
   (HMIS θ=0.5, aggressive HMIS on level 1, extended+i interpolation),
   V(1,1).  Solver: conjugate gradients preconditioned by one AMG cycle.
-  `value` = mean time of the mixed-precision solve (FP32 hierarchy and
-  cycle, FP64 outer residual / products / dots / updates); the FP64-cycle
-  solve is timed beside it.  Inputs stay in HBM; the finest matrix alone
-  (175 MB) exceeds the 126 MB L2, so no L2 flush is needed between steps.
+  `value` = mean time of the FP64 solve (FP64 hierarchy, cycle and outer
+  CG: the reference's arithmetic); the mixed-precision solve (FP32
+  hierarchy and cycle, FP64 outer residual / products / dots / updates) is
+  timed beside it ("mixed", "speedup_mixed_vs_fp64").  Inputs stay in HBM;
+  the finest matrix alone (175 MB) exceeds the 126 MB L2, so no L2 flush is
+  needed between steps.  `e2e` is the FP64 solve through the C ABI
+  (draugr_b200_pcg) with pinned host x and b.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 --impl reference times the reference's CPU solve (the oracle restatement of
 Draugr.jl's cycle inside a textbook PCG, all host cores) on the same
-system and hierarchy structure.
+system and hierarchy structure; the structure is built by a child process
+(--write-structure) so that the timed process loads only the oracle.
 """
 
 from __future__ import annotations
@@ -72,6 +76,9 @@ def parse():
     ap.add_argument("--workers", type=int, default=16)
     ap.add_argument("--profile-solve", choices=["fp64", "mixed"], default=None,
                     help="run exactly one PCG solve in this precision (for profiling)")
+    ap.add_argument("--write-structure", default=None, metavar="PATH",
+                    help="build the workload's hierarchy structure on the host (no GPU) and write "
+                         "it with the right-hand side to PATH (.npz) for the reference arm")
     return ap.parse_args()
 
 
@@ -86,11 +93,11 @@ def workload(n, seed):
     return A, b, cfg
 
 
-def workload_config(n, A, h=None, setup_s=None):
+def workload_config(n, rows, nnz, h=None):
     d = {"workload": f"3D 7-point heterogeneous diffusion {n}^3 (kappa=exp(g), sigma=3, "
                      "corr. length 8), hypre_default_config(agg_trunc_factor=0.2) + l1-Jacobi "
                      "V(1,1), AMG-PCG to 1e-8 from x0=0",
-         "n": int(A.shape[0]), "nnz": int(A.nnz), "tol": TOL,
+         "n": int(rows), "nnz": int(nnz), "tol": TOL,
          "l2": "inputs larger than L2 (finest matrix alone 175 MB > 126 MB); no flush"}
     if h is not None:
         nl = h.nlevels
@@ -99,8 +106,6 @@ def workload_config(n, A, h=None, setup_s=None):
         d.update(levels=nl + 1, level_rows=rows, level_nnz=nnzs,
                  level_nnzP=[int(h.level_info(l)[3]) for l in range(nl)],
                  operator_complexity=round(sum(nnzs) / nnzs[0], 3) if nnzs else None)
-    if setup_s is not None:
-        d["setup_s_cpu"] = round(setup_s, 3)
     return d
 
 
@@ -208,6 +213,17 @@ def max_over_ranks(v, world):
     return float(t.item())
 
 
+def repo_libraries():
+    """Shared objects under this repository mapped into this process."""
+    try:
+        maps = pathlib.Path("/proc/self/maps").read_text().splitlines()
+    except OSError:
+        return None
+    root = str(ROOT)
+    return sorted({ln.split()[-1][len(root) + 1:] for ln in maps
+                   if ln.split()[-1].startswith(root) and ".so" in ln.split()[-1]})
+
+
 def barrier(world):
     if world > 1:
         import torch.distributed as dist
@@ -259,7 +275,7 @@ def run_ours(args, world, rank, local):
         torch.cuda.synchronize()
         barrier(world)
         torch.cuda.synchronize()
-        if mode == "mixed":
+        if mode == "fp64":  # the headline value: the reference's arithmetic, FP64 throughout
             launches0 = draugr.load().draugr_b200_kernel_launches()
             with ClockSampler(local) as cs:
                 times, its = timed(mode, args.steps)
@@ -282,20 +298,28 @@ def run_ours(args, world, rank, local):
     xh = torch.zeros(n, dtype=torch.float64, pin_memory=True).numpy()
     bh = torch.zeros(n, dtype=torch.float64, pin_memory=True).numpy()
     bh[:] = b
-    e2e_times = []
-    for k in range(args.warmup + args.steps):
-        xh[:] = 0.0
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        draugr.pcg(xh, bh, h, cfg, tol=TOL, maxiter=MAXITER, precision="mixed")
-        e1.record(stream)
-        e1.synchronize()
-        if k >= args.warmup:
-            e2e_times.append(e0.elapsed_time(e1) / 1e3)
-    e2e = {"value": max_over_ranks(float(np.mean(e2e_times)), world), "unit": "s",
+
+    def e2e_time(mode):
+        ts = []
+        for k in range(args.warmup + args.steps):
+            xh[:] = 0.0
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            draugr.pcg(xh, bh, h, cfg, tol=TOL, maxiter=MAXITER, precision=mode)
+            e1.record(stream)
+            e1.synchronize()
+            if k >= args.warmup:
+                ts.append(e0.elapsed_time(e1) / 1e3)
+        rr = float(np.linalg.norm(b - A @ xh) / bnorm)
+        if rr >= TOL:
+            raise SystemExit(f"{mode} solve through the C ABI did not reach {TOL}: {rr}")
+        return max_over_ranks(float(np.mean(ts)), world)
+
+    e2e = {"value": e2e_time("fp64"), "unit": "s",
            "h2d_bytes_per_step": 2 * n * 8, "d2h_bytes_per_step": n * 8,
-           "path": "draugr_b200_pcg (C ABI, pinned host x/b)"}
+           "path": "draugr_b200_pcg, precision 0 (C ABI, pinned host x and b, FP64 cycle)",
+           "mixed": e2e_time("mixed")}
 
     # roofline of the dominant kernels: finest-level Jacobi sweep and SpMV
     nnz = A.nnz
@@ -351,17 +375,20 @@ def run_ours(args, world, rank, local):
                       "starts from a given x; the coarser levels' first sweep is formed in the "
                       "restriction), shared-memory tail levels included at their global-memory size"}
 
-    out = {"metric": METRIC, "value": res["mixed"]["time_s"], "unit": "s", "n_gpus": world,
+    out = {"metric": METRIC, "value": res["fp64"]["time_s"], "unit": "s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup,
-           "ms_per_step": res["mixed"]["time_s"] * 1e3, "higher_is_better": False,
+           "ms_per_step": res["fp64"]["time_s"] * 1e3, "higher_is_better": False,
            "scaling": "weak", "vs_baseline": None,
-           "dtype": "f32 (hierarchy, cycle) + f64 (outer residual, A-products, dots, updates)",
+           "dtype": "f64 (value, e2e: FP64 cycle and outer CG); 'mixed': f32 hierarchy and cycle "
+                    "inside f64 CG",
            "data": "synthetic (seeded log-normal permeability field, b ~ U(-1,1))",
-           "config": dict(workload_config(args.n, A, h, setup_s),
+           "config": dict(workload_config(args.n, n, A.nnz, h),
                           parallelism=f"replicas x{world}" if world > 1 else "1 GPU"),
+           "setup_s_cpu": round(setup_s, 3),
            "fp64": res["fp64"], "mixed": res["mixed"],
            "speedup_mixed_vs_fp64": res["fp64"]["time_s"] / res["mixed"]["time_s"],
            "e2e": e2e, "roofline": roofline, "vcycle": vcycle, "clocks": clocks,
+           "loaded_repo_libraries": repo_libraries(),
            "gpu_launches": int(launches)}
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -396,19 +423,55 @@ def cpu_baseline(h, b, cfg):
 
 
 # --------------------------------------------------------------- reference
-def run_reference(args, world, rank):
+def write_structure(args):
+    """--write-structure: the workload's hierarchy structure, built on the
+    host by the library's setup (no GPU is touched), written with b for
+    the reference arm, which then loads only the oracle."""
     import draugr
 
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+
+    A, b, cfg = workload(args.n, args.seed)
+    t0 = time.time()
+    h = draugr.amg_setup(A, cfg, on_device=False)
+    oracle.save_structure(h, args.write_structure, b=b, setup_s=time.time() - t0,
+                          pre=cfg.pre_smoothing_steps, post=cfg.post_smoothing_steps,
+                          w=int(cfg.cycle_type == "W"))
+    h.free()
+
+
+def run_reference(args, world, rank):
+    """The reference's CPU solve phase (the oracle's restatement of
+    Draugr.jl's kernels, OpenMP on all host threads) on the same hierarchy
+    structure.  The structure is built in a child process (the input, not
+    the timed path); this process loads nothing but the oracle."""
     if rank != 0:
         return None
-    A, b, cfg = workload(args.n, args.seed)
-    h = draugr.amg_setup(A, cfg, on_device=False)   # structure only (shared input)
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+
+    path = pathlib.Path(f"/tmp/draugr_structure_n{args.n}_s{args.seed}_{os.getpid()}.npz")
+    subprocess.run([sys.executable, str(ROOT / "bench.py"), "--write-structure", str(path),
+                    "--n", str(args.n), "--seed", str(args.seed)], check=True)
+    try:
+        S = oracle.StructureFile(path)
+    finally:
+        path.unlink(missing_ok=True)
+    b = S.extra("b")
+    pre, post, w = int(S.extra("pre")), int(S.extra("post")), bool(int(S.extra("w")))
+    O = oracle.OracleHierarchy(S)
+    nrows = len(b)
     times = []
     its = 0
+    x = None
     for k in range(args.warmup + args.steps):
-        t, its = cpu_solve_time(h, b, cfg)
+        t0 = time.perf_counter()
+        x, its, rel = O.pcg(np.zeros(nrows), b, pre, post, w, TOL, MAXITER)
         if k >= args.warmup:
-            times.append(t)
+            times.append(time.perf_counter() - t0)
+    rp, ci, av = S.export(0, "A_rowptr"), S.export(0, "A_colval"), S.export(0, "A_nzval")
+    rr = float(np.linalg.norm(oracle.residual(nrows, rp, ci, av, x, b)) / np.linalg.norm(b))
     v = float(np.mean(times))
     sample = ("full AMG-PCG solve per step (FP64 cycle), oracle restatement of Draugr.jl's "
               "CPU kernels (Julia is not available), OpenMP on all host threads")
@@ -416,8 +479,13 @@ def run_reference(args, world, rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded log-normal permeability field, b ~ U(-1,1))",
-            "config": dict(workload_config(args.n, A, h), parallelism="CPU"),
-            "iterations": its,
+            "config": dict(workload_config(args.n, nrows, len(ci), S),
+                           parallelism=f"replicas x{world}" if world > 1 else "1 GPU"),
+            "setup_s_cpu": round(float(S.extra("setup_s")), 3),
+            "iterations": its, "relres_fp64_verified": rr,
+            "structure": "hierarchy structure built by the library's host setup in a child "
+                         "process (bench.py --write-structure); this process loads only the oracle",
+            "loaded_repo_libraries": repo_libraries(),
             "cpu_baseline": {"value": v, "unit": "s", "cores": os.cpu_count(), "kind": "port",
                              "sample": sample},
             "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -754,6 +822,9 @@ def main():
         return
     if args.kernel_only:
         print(json.dumps(run_kernel_only(args)), flush=True)
+        return
+    if args.write_structure:
+        write_structure(args)
         return
     world, rank, local = dist_init(args)
     if args.impl == "reference":

@@ -257,7 +257,7 @@ int32_t draugr_amg_cycle(int32_t handle, int32_t n, double* x, const double* b, 
     DR_CK(cudaMemcpyAsync(D.bbuf(), b, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, D.stream()));
     D.cycle(D.xbuf(), D.bbuf(), opts_of(c));
     DR_CK(cudaMemcpyAsync(x, D.xbuf(), (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, D.stream()));
-    DR_CK(cudaStreamSynchronize(D.stream()));
+    D.check_errors();
     return 0;
   });
 }
@@ -451,7 +451,7 @@ int32_t draugr_b200_cycle_device(int32_t handle, int32_t n, double* x_dev, const
     if (n != n_finest(*H)) fail("DimensionMismatch");
     DevHier& D = device_of(*H);
     D.cycle(x_dev, b_dev, opts_of(c));
-    DR_CK(cudaStreamSynchronize(D.stream()));
+    D.check_errors();
     return 0;
   });
 }
@@ -634,6 +634,8 @@ int32_t draugr_b200_time_level_op(int32_t handle, int32_t lvl, int32_t op, int32
 }
 
 int64_t draugr_b200_kernel_launches(void) { return kernel_launches(); }
+
+void draugr_b200_set_tile_wait_limit(int32_t polls) { set_tile_wait_limit(polls); }
 
 int32_t draugr_b200_set_stream(int32_t handle, void* stream) {
   return guarded("draugr_b200_set_stream", [&]() -> int32_t {

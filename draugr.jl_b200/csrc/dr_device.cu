@@ -67,6 +67,13 @@ static int* err_flag() {
   return p;
 }
 
+// Polls a row kernel makes on a tile's copy before it gives up.  Only the
+// test hook draugr_b200_set_tile_wait_limit lowers it (0 makes every row
+// kernel give up at once and report the timeout).
+static std::atomic<int> g_tile_wait_limit{kern::kWaitLimit};
+static int tile_wait_limit() { return g_tile_wait_limit.load(std::memory_order_relaxed); }
+void set_tile_wait_limit(int polls) { g_tile_wait_limit.store(polls < 0 ? kern::kWaitLimit : polls); }
+
 void cuda_check(cudaError_t e, const char* what, const char* file, int line) {
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -196,7 +203,7 @@ void launch_rows_impl(cudaStream_t st, int max_grid, const RowForm& f, int n, in
     const int grid = std::max(                                                                   \
         1, std::min({ntiles, max_grid, g_nsm * resident_blocks((const void*)kf, NT, smem)}));    \
     launch_dependent(kf, grid, NT, smem, st, ntiles, tp, ts, tb, rp, ci, cu, av, xl, ep, partials, \
-                     ticket, fin, err_flag());                                                   \
+                     ticket, fin, err_flag(), tile_wait_limit());                                \
   } while (0)
   // 16-bit column offsets where lanes read consecutive entries (flat and
   // tree forms), and for FP32 rows of 12-32 entries, where the bytes saved
@@ -458,6 +465,8 @@ static void check_kernel_flag(cudaStream_t st) {
     fail("a row kernel timed out waiting for its tile copy (results discarded)");
   }
 }
+
+void DevHier::check_errors() { check_kernel_flag(st_); }
 
 void DevHier::set_stream(cudaStream_t s) {
   DR_CK(cudaStreamSynchronize(st_));

@@ -17,6 +17,9 @@ namespace dr {
 void cuda_check(cudaError_t e, const char* what, const char* file, int line);
 long long kernel_launches();
 void note_launch();  // counts one kernel launch (kernel_launches)
+// Polls a row kernel makes on a tile copy before it reports a timeout
+// (negative: the default).  A test hook.
+void set_tile_wait_limit(int polls);
 #define DR_CK(x) ::dr::cuda_check((x), #x, __FILE__, __LINE__)
 
 // Nonzeros per tile of the row kernel (k_tile_rows); rows longer than this
@@ -192,6 +195,10 @@ class DevHier {
   // Run on the caller's stream (nullptr: back to the library's own stream).
   void set_stream(cudaStream_t s);
   size_t device_bytes() const { return bytes_; }
+
+  // Raise if a kernel of this device reported a bounded wait that gave up
+  // (synchronises the stream; clears the flag).
+  void check_errors();
 
   // Solve phase (device pointers, length n0).
   void cycle(double* x, const double* b, const CycleOpts& o);

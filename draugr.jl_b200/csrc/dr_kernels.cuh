@@ -478,7 +478,7 @@ __global__ void __launch_bounds__(NT, (tile_min_blocks<NT, TA>()))
 k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
             const int* __restrict__ tb, const int* __restrict__ rp, const int* __restrict__ ci,
             const uint16_t* __restrict__ cu, const TA* __restrict__ av, XL xl, EP ep,
-            double* partials, unsigned* ticket, Fin fin, int* err) {
+            double* partials, unsigned* ticket, Fin fin, int* err, int wait_limit) {
   constexpr bool kOff = sizeof(TC) == 2;
   constexpr int kColAlign = 16 / (int)sizeof(TC);  // entries per 16 bytes
   const TC* const csrc = kOff ? reinterpret_cast<const TC*>(cu) : reinterpret_cast<const TC*>(ci);
@@ -595,16 +595,16 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
     const bool valid = c0.valid;
     const int rs = c0.rs, re = c0.re;
     const Pre& pr = c0.pr;
-    if (!mbar_wait_bounded(bar + b, parity, kWaitLimit)) {
-      if (threadIdx.x == 0) atomicExch(err, 1);
-      mbar_wait_bounded(bar + b, parity, kWaitLimit);
-    }
+    // A thread whose wait for the stage gives up reads nothing from it (its
+    // rows are skipped); the block leaves the loop together at the barrier
+    // that ends the tile.
+    const bool ok = mbar_wait_bounded(bar + b, parity, wait_limit);
     if (staged(h0)) {
       TA* vs = sv0 + b * kStageEntries + (s - (s & ~3));
       const TC* cs = sc0 + b * kStageEntries + (s - (s & ~(kColAlign - 1)));
       const int cb = h0.cb;
       if constexpr (FLAT) {
-        if (len > 0) {
+        if (ok && len > 0) {
           // slots past the tile's end repeat its last entry (in bounds)
           acc_t p[kFlatIters];
 #pragma unroll
@@ -620,7 +620,7 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
           }
         }
         __syncthreads();
-        if (valid) {
+        if (valid && ok) {
           acc_t a = ep.init(pr);
           for (int k = rs; k < re; ++k) {
             if constexpr (EP::kSign > 0) a = add_rn(a, (acc_t)vs[k]);
@@ -629,7 +629,7 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
           dacc += ep.apply(row, a, pr);
         }
       } else if constexpr (G == 1) {
-        if (valid) {
+        if (valid && ok) {
           acc_t a = ep.init(pr);
           for (int k0 = rs; k0 < re; k0 += B) {
             // all B gathers issued unconditionally (slots past the row end
@@ -651,7 +651,8 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
       } else {
         // longer rows: G lanes sum strided products, then a fixed shuffle tree
         acc_t sum = acc_t(0);
-        for (int k0 = rs + lane; k0 < re; k0 += B * G) {
+        const int rend = ok ? re : rs;
+        for (int k0 = rs + lane; k0 < rend; k0 += B * G) {
           acc_t xv[B];
 #pragma unroll
           for (int j = 0; j < B; ++j) xv[j] = (acc_t)xl(cb + (int)cs[min(k0 + j * G, re - 1)]);
@@ -664,7 +665,7 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
         }
 #pragma unroll
         for (int o = G >> 1; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-        if (valid && lane == 0) {
+        if (valid && ok && lane == 0) {
           acc_t a = ep.init(pr);
           if constexpr (EP::kSign > 0) a = add_rn(a, sum);
           else a = sub_rn(a, sum);
@@ -706,7 +707,19 @@ k_tile_rows(int ntiles, const int* __restrict__ tp, const int* __restrict__ ts,
         }
       }
     }
-    __syncthreads();  // stage b fully consumed
+    // stage b fully consumed; block-uniform abort if any thread gave up
+    if (__syncthreads_or(!ok)) {
+      // Flag the error, let the copies in flight land (stage b, and stage
+      // 1-b if the next tile was issued) with bounded waits, and leave the
+      // loop; the reduction below still completes, so its ticket is reset.
+      if (threadIdx.x == 0) {
+        atomicExch(err, 1);
+        mbar_wait_bounded(bar + b, parity, kWaitLimit);
+        if (t + stride < ntiles) mbar_wait_bounded(bar + (b ^ 1), (uint32_t)(((i + 1) >> 1) & 1), kWaitLimit);
+      }
+      __syncthreads();
+      break;
+    }
     if (threadIdx.x == 0 && t + 2 * stride < ntiles) {
       fence_proxy_async();
       issue(h2, b);

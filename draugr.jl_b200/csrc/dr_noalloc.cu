@@ -54,7 +54,7 @@ k_residual_noalloc(int n, const int* __restrict__ rp, const int* __restrict__ ci
     for (int k = rp[i]; k < rp[i + 1]; ++k) ax = __dadd_rn(ax, __dmul_rn(v[k], x[ci[k]]));
     const double ri = __dsub_rn(b[i], ax);
     r[i] = ri;
-    rr = ri * ri;
+    rr = __dmul_rn(ri, ri);
   }
   for (int o = 16; o > 0; o >>= 1) rr += __shfl_xor_sync(0xffffffffu, rr, o);
   if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = rr;

@@ -50,6 +50,7 @@ SIGNATURES = {
     "draugr_b200_time_level_op": (i32, [i32, i32, i32, i32, i32, P]),
     "draugr_b200_kernel_launches": (i64, []),
     "draugr_b200_set_stream": (i32, [i32, P]),
+    "draugr_b200_set_tile_wait_limit": (None, [i32]),
 }
 
 _lib = None

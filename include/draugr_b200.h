@@ -94,10 +94,11 @@ int32_t draugr_b200_residual_device(int32_t handle, int32_t n, const double *x_d
  * rows); larger n is rejected with an error.  The first call on a device
  * looks up the scratch's device address (cudaGetSymbolAddress); make that
  * first call before any stream capture.  All calls share the scratch, so
- * calls that overlap on the GPU (different streams or threads) race; the
- * call returns after its work on `stream` has finished.  Rows are summed in
- * column order, as draugr_b200_residual_device does for rows of up to 32
- * entries.  Returns 0 or -1. */
+ * calls that overlap on the GPU (different streams or threads) race.  Every
+ * call copies ||r||_2 back to the host and synchronises `stream` before it
+ * returns.  Rows are summed in column order with separately rounded
+ * products and sums, as the reference's residual_kernel! does, so r equals
+ * that kernel's result bit for bit.  Returns 0 or -1. */
 int32_t draugr_b200_residual_noalloc(int32_t n, int32_t nnz, const int32_t *rowptr,
                                      const int32_t *colval, const double *nzval, const double *x,
                                      const double *b, double *r, double *rnorm, void *stream);
@@ -192,6 +193,14 @@ int32_t draugr_b200_set_stream(int32_t handle, void *stream);
 /* Number of CUDA kernels this library has launched in the process so far
  * (each launch of a captured CUDA graph adds the kernels it contains). */
 int64_t draugr_b200_kernel_launches(void);
+
+/* Test hook, no counterpart in the reference: the number of polls a row
+ * kernel makes on a tile's copy (an mbarrier wait) before it gives up,
+ * flags the timeout and returns; the entry point that launched it then
+ * returns -1 with "timed out" in draugr_amg_last_error.  A negative value
+ * restores the default (2^22).  0 makes every row kernel give up at once,
+ * which is how the timeout path is tested without a stuck copy. */
+void draugr_b200_set_tile_wait_limit(int32_t polls);
 
 #ifdef __cplusplus
 }

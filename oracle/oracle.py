@@ -316,6 +316,53 @@ def strength_abs(n, rp, ci, v, theta):
     return s
 
 
+# ---------------------------------------------------------------- structure files
+# The arrays OracleHierarchy reads from a hierarchy, per level and for the
+# coarsest level, so that the structure can be written by one process and
+# the reference's solve phase run on it in another that loads nothing but
+# the oracle.
+_LEVEL_ARRAYS = ("A_rowptr", "A_colval", "A_nzval", "P_rowptr", "P_colval", "P_nzval", "T_offsets",
+                 "T_rows", "T_pnz", "invdiag", "color_offsets", "color_order", "omega")
+_SMOOTHER_ARRAYS = {8: ("cheb_v0", "cheb_coef"), 4: ("spai1_M",), 9: ("ilu_diag", "ilu_L", "ilu_U"),
+                    10: ("ilu_diag", "ilu_L", "ilu_U")}
+_COARSE_ARRAYS = ("C_rowptr", "C_colval", "C_nzval")
+
+
+def save_structure(h, path, **extra):
+    """Write the hierarchy structure `h` exposes (nlevels, level_info,
+    export) to an uncompressed .npz at `path`, with any extra arrays given
+    as keyword arguments (e.g. the right-hand side)."""
+    d = {"nlevels": np.array([h.nlevels], np.int64)}
+    for l in list(range(h.nlevels)) + [-1]:
+        info = np.asarray(h.level_info(l), np.int64)
+        d[f"L{l}_info"] = info
+        names = _COARSE_ARRAYS if l < 0 else _LEVEL_ARRAYS + _SMOOTHER_ARRAYS.get(int(info[4]), ())
+        for nm in names:
+            d[f"L{l}_{nm}"] = h.export(l, nm)
+    for k, v in extra.items():
+        d[f"extra_{k}"] = np.asarray(v)
+    np.savez(path, **d)
+
+
+class StructureFile:
+    """A hierarchy structure read back from save_structure's file, with the
+    nlevels / level_info / export interface OracleHierarchy takes."""
+
+    def __init__(self, path):
+        z = np.load(path)
+        self._d = {k: z[k] for k in z.files}
+        self.nlevels = int(self._d["nlevels"][0])
+
+    def level_info(self, lvl):
+        return self._d[f"L{lvl}_info"]
+
+    def export(self, lvl, what):
+        return self._d[f"L{lvl}_{what}"]
+
+    def extra(self, name):
+        return self._d[f"extra_{name}"]
+
+
 # ---------------------------------------------------------------- hierarchy mirror
 SMOOTHER_KIND = {0: "jacobi", 1: "colored_gs", 2: "serial_gs", 3: "spai0", 4: "spai1", 5: "l1_jacobi",
                  6: "l1_colored_gs", 7: "l1_serial_gs", 8: "chebyshev", 9: "ilu0", 10: "serial_ilu0"}

@@ -1,7 +1,8 @@
 """The JSON line of bench.py's reference arm (the oracle's PCG on the host
 cores), run at a small size on the CPU: one JSON line with the benchmark
 keys, the same metric and units as the product arm, and the e2e and
-cpu_baseline objects it has to carry."""
+cpu_baseline objects it has to carry, and a process that mapped none of
+the product's libraries."""
 
 import json
 import subprocess
@@ -27,3 +28,7 @@ def test_reference_arm_json_line():
     assert d["e2e"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0
     assert d["cpu_baseline"]["value"] == d["value"] and d["cpu_baseline"]["kind"] in ("port", "reference")
     assert d["config"]["workload"].startswith("3D 7-point heterogeneous diffusion 12^3")
+    assert d["relres_fp64_verified"] < 1e-8
+    # the timed process ran the oracle only: the product library is not mapped
+    libs = d["loaded_repo_libraries"]
+    assert "oracle/liboracle.so" in libs and not any("libdraugr_b200" in x for x in libs), libs

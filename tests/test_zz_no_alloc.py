@@ -1,10 +1,13 @@
 """draugr_b200_residual_noalloc: the residual entry point for callers that
 cannot allocate device memory (their own pool owns every byte, so the
 library may not call cudaMalloc for them).  It works on the caller's CSR
-arrays and vectors with a static scratch array, and must give what the
+arrays and vectors with a static scratch array.  It must give what the
 allocating entry point draugr_b200_residual_device gives for the same
-matrix and vectors, call after call.  Collected last (file name) so a run
-that stops at the first failure has run every other test before it."""
+matrix and vectors, call after call, and, since it sums every row in
+column order with separately rounded products and sums, the oracle's
+residual (the reference's residual_kernel!) bit for bit.  Collected last
+(file name) so a run that stops at the first failure has run every other
+test before it."""
 
 import ctypes as C
 
@@ -12,6 +15,7 @@ import numpy as np
 import pytest
 
 import draugr
+import oracle
 from draugr import problems
 
 pytestmark = pytest.mark.gpu
@@ -27,13 +31,17 @@ def test_noalloc_residual_matches_allocating_entry_point():
     h = draugr.amg_setup(A, cfg)
     lib = draugr.load()
     dev = torch.device("cuda")
-    rp = torch.tensor(A.indptr, dtype=torch.int32, device=dev)
-    ci = torch.tensor(A.indices, dtype=torch.int32, device=dev)
-    v = torch.tensor(A.data, dtype=torch.float64, device=dev)
+    rp_h = np.ascontiguousarray(A.indptr, np.int32)
+    ci_h = np.ascontiguousarray(A.indices, np.int32)
+    v_h = np.ascontiguousarray(A.data, np.float64)
+    rp = torch.tensor(rp_h, device=dev)
+    ci = torch.tensor(ci_h, device=dev)
+    v = torch.tensor(v_h, device=dev)
     rng = np.random.default_rng(12)
     for call in range(2):
-        x = torch.tensor(rng.uniform(-1, 1, n), dtype=torch.float64, device=dev)
-        b = torch.tensor(rng.uniform(-1, 1, n), dtype=torch.float64, device=dev)
+        x_h, b_h = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)
+        x = torch.tensor(x_h, dtype=torch.float64, device=dev)
+        b = torch.tensor(b_h, dtype=torch.float64, device=dev)
         r_ref = torch.zeros(n, dtype=torch.float64, device=dev)
         r_na = torch.full((n,), float("nan"), dtype=torch.float64, device=dev)
         torch.cuda.synchronize()
@@ -48,6 +56,7 @@ def test_noalloc_residual_matches_allocating_entry_point():
         assert np.all(np.isfinite(got))
         assert np.max(np.abs(got - ref)) <= TOL * np.max(np.abs(ref)), f"call {call}"
         assert abs(rn_na.value - rn_ref.value) <= TOL * rn_ref.value, f"call {call}"
+        assert np.array_equal(got, oracle.residual(n, rp_h, ci_h, v_h, x_h, b_h)), f"call {call}"
     h.free()
 
 
