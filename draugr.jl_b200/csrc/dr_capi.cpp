@@ -467,6 +467,27 @@ int32_t draugr_b200_resetup_values_device(int32_t handle, int64_t nnz, const dou
   });
 }
 
+int32_t draugr_b200_galerkin_host(int32_t handle, int32_t lvl, int64_t nnz_in, const double* a_vals,
+                                  int64_t nnz_out, double* ac_vals) {
+  return guarded("draugr_b200_galerkin_host", [&]() -> int32_t {
+    auto H = get_hier_only(handle);
+    if (lvl < 0 || lvl >= (int)H->host.levels.size()) fail("level index out of range");
+    const HostLevel& L = H->host.levels[lvl];
+    if (!L.has_rap_map) fail("the level keeps no A*P pattern (set up with allow_partial_resetup=1)");
+    const CSR& next = lvl + 1 < (int)H->host.levels.size() ? H->host.levels[lvl + 1].A : H->host.coarse;
+    if (nnz_in != L.A.nnz()) fail("nnz_in differs from the level's nonzeros");
+    if (nnz_out != next.nnz()) fail("nnz_out differs from the next level's nonzeros");
+    if ((nnz_in > 0 && !a_vals) || (nnz_out > 0 && !ac_vals)) fail("ArgumentError: NULL array");
+    CSR A = L.A;
+    A.v.assign(a_vals, a_vals + nnz_in);
+    std::vector<double> ap_v, c_v;
+    numeric_ap(A, L.P, L.ap_rp, L.ap_ci, ap_v);
+    numeric_ptap(L.T, L.Rv, L.ap_rp, L.ap_ci, ap_v, next.rp, next.ci, c_v);
+    std::copy(c_v.begin(), c_v.end(), ac_vals);
+    return 0;
+  });
+}
+
 int32_t draugr_b200_residual_device(int32_t handle, int32_t n, const double* x_dev, const double* b_dev,
                                     double* r_dev, double* rnorm) {
   return guarded("draugr_b200_residual_device", [&]() -> int32_t {

@@ -299,6 +299,17 @@ class Hierarchy:
                    f"export {what}")
         return out
 
+    def galerkin_host(self, lvl: int, values) -> np.ndarray:
+        """The next level's values from new values of level lvl, by the
+        setup's numeric product on the host (draugr_b200_galerkin_host)."""
+        lib = _lib.load()
+        v = np.ascontiguousarray(values, np.float64)
+        nnz_next = int(self.level_info(lvl + 1)[1] if lvl + 1 < self.nlevels else self.level_info(-1)[1])
+        out = np.zeros(nnz_next)
+        _lib.check(lib.draugr_b200_galerkin_host(self.handle, lvl, len(v), _ptr(v), nnz_next, _ptr(out)),
+                   "galerkin_host")
+        return out
+
     def summary(self) -> str:
         s = _lib.load().draugr_b200_summary(self.handle)
         return s.decode() if s else ""

@@ -113,6 +113,18 @@ int32_t draugr_b200_residual_noalloc(int32_t n, int32_t nnz, const int32_t *rowp
  * values to the host first (ext/DraugrCUDAExt.jl:49). */
 int32_t draugr_b200_resetup_values_device(int32_t handle, int64_t nnz, const double *nzval_dev);
 
+/* The Galerkin product of level lvl computed on the host by the setup's
+ * numeric product (A*P, then Pᵀ(AP), each entry accumulated in the same
+ * order as the device's partial resetup): a_vals holds new values of level
+ * lvl's matrix (nnz_in, its pattern), ac_vals receives the next level's
+ * values (nnz_out, its pattern).  Needs a hierarchy set up with
+ * allow_partial_resetup = 1.  For checking device resetups; the reference's
+ * counterpart is galerkin_product! on the CPU backend
+ * (src/galerkin.jl:194-222), which sums the same products per entry in its
+ * triple map's order. */
+int32_t draugr_b200_galerkin_host(int32_t handle, int32_t lvl, int64_t nnz_in, const double *a_vals,
+                                  int64_t nnz_out, double *ac_vals);
+
 /* Conjugate gradients preconditioned by one AMG cycle per iteration, until
  * ||b - A x|| / ||b|| < tol.  precision 0: FP64 cycle.  precision 1: cycle
  * on FP32 copies of the hierarchy with FP64 outer residual, products with A,

@@ -222,6 +222,20 @@ def test_hierarchy_summary(host_case):
     assert type(cfg.smoother).__name__ in s
 
 
+def test_host_galerkin_reproduces_the_setup_product(host_case):
+    """draugr_b200_galerkin_host with a level's own values gives the next
+    level's values bit for bit (the same numeric product as the setup), and
+    is linear in the values (2A gives twice the product exactly)."""
+    name, A, cfg, h = host_case
+    for l in range(h.nlevels):
+        v = h.export(l, "A_nzval")
+        nxt = h.export(l + 1, "A_nzval") if l + 1 < h.nlevels else h.export(-1, "C_nzval")
+        assert np.array_equal(h.galerkin_host(l, v), nxt), (name, l)
+        assert np.array_equal(h.galerkin_host(l, 2.0 * v), 2.0 * nxt), (name, l)
+    with pytest.raises(draugr.DraugrError):
+        h.galerkin_host(h.nlevels, np.zeros(1))
+
+
 def test_allow_partial_resetup_false_has_no_maps():
     A = problems.poisson2d(16)
     h = draugr.amg_setup(A, draugr.AMGConfig(coarsening=draugr.AggregationCoarsening()),

@@ -1,0 +1,150 @@
+"""Parity at the benchmark's own sizes, through the C ABI, against the
+oracle (the CPU restatement of Draugr.jl's arithmetic) on the same
+hierarchy structure.
+
+* The 128^3 heterogeneous-diffusion system of the headline benchmark
+  (2,097,152 unknowns; hypre_default_config(agg_trunc_factor=0.2) with
+  l1-Jacobi): one V and one W cycle against the oracle's amg_cycle!
+  (src/cycle.jl:12-28) at 1e-12; the FP64 AMG-PCG against the oracle's PCG
+  (same iteration count +-1, iterate within 1e-7); the mixed-precision
+  PCG (FP32 cycle) reaches 1e-8 as verified by an FP64 residual, and its
+  distance from the FP64 oracle solution is checked and reported.  At this
+  size the hierarchy uses the one-lane and the multi-lane (shuffle-tree)
+  row forms, 16-bit column offsets, the flat restriction and the
+  shared-memory coarse tail.
+* The 27-point anisotropic coefficient-update system: a partial resetup
+  (numeric Galerkin products on the GPU, src/resetup.jl:27-45) against the
+  reference's triple-map product at 64^3 nodes (the largest size whose
+  triple map, about 2 GB at the finest level, is built here in seconds),
+  and at the full 128^3 nodes against the setup's host numeric product bit
+  for bit, level by level.
+"""
+
+import numpy as np
+import pytest
+
+import draugr
+import oracle
+from draugr import problems
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / (nb if nb > 0 else 1.0)
+
+
+@pytest.fixture(scope="module")
+def c2():
+    A = problems.heterogeneous_diffusion_3d(128, sigma=3.0, corr_len=8.0, seed=2024)
+    cfg = draugr.hypre_default_config(agg_trunc_factor=0.2, smoother=draugr.L1JacobiSmootherType(),
+                                      seed=2024)
+    h = draugr.amg_setup(A, cfg)
+    O = oracle.OracleHierarchy(h)
+    b = problems.rhs(A.shape[0], 2025)
+    yield A, cfg, h, O, b
+    h.free()
+
+
+def test_c2_128cubed_has_ordered_and_tree_summed_levels(c2):
+    """level_info[7] is 1 when every row of the level's matrix is summed by
+    one lane in column order and 0 when some rows are summed by several
+    lanes and a shuffle tree: both kinds occur at this size."""
+    A, cfg, h, O, b = c2
+    assert A.shape[0] == 128 ** 3
+    ordered = {int(h.level_info(l)[7]) for l in range(h.nlevels)}
+    assert ordered == {0, 1}, ordered
+
+
+@pytest.mark.parametrize("wcycle", [False, True])
+def test_c2_128cubed_cycle(c2, wcycle):
+    A, cfg, h, O, b = c2
+    n = A.shape[0]
+    c = draugr.hypre_default_config(agg_trunc_factor=0.2, smoother=draugr.L1JacobiSmootherType(),
+                                    seed=2024, cycle_type="W" if wcycle else "V")
+    x = np.zeros(n)
+    draugr.amg_cycle(x, b, h, c)
+    ref = O.cycle(np.zeros(n), b, 1, 1, wcycle)
+    assert rel(x, ref) < 1e-12
+    # a second cycle from a nonzero iterate (pre-smoothing from a given x)
+    draugr.amg_cycle(x, b, h, c)
+    ref = O.cycle(ref, b, 1, 1, wcycle)
+    assert rel(x, ref) < 1e-12
+
+
+def test_c2_128cubed_pcg_fp64_and_mixed(c2):
+    A, cfg, h, O, b = c2
+    n = A.shape[0]
+    xo, ito, relo = O.pcg(np.zeros(n), b, 1, 1, False, 1e-8, 500)
+    x, it, rr = draugr.pcg(np.zeros(n), b, h, cfg, tol=1e-8, maxiter=500, precision="fp64")
+    assert abs(it - ito) <= 1, (it, ito)
+    assert rel(x, xo) < 1e-7
+    assert np.linalg.norm(b - A @ x) / np.linalg.norm(b) < 1e-8
+    xm, itm, rm = draugr.pcg(np.zeros(n), b, h, cfg, tol=1e-8, maxiter=500, precision="mixed")
+    rm64 = np.linalg.norm(b - A @ xm) / np.linalg.norm(b)
+    err = rel(xm, xo)
+    print(f"\nC2 128^3: FP64 PCG {it} iterations (oracle {ito}), |x - x_oracle|/|x_oracle| = "
+          f"{rel(x, xo):.2e}; mixed PCG {itm} iterations, FP64 residual {rm64:.2e}, "
+          f"|x_mixed - x_oracle|/|x_oracle| = {err:.2e}")
+    assert rm64 < 1e-8
+    assert err < 1e-5
+    assert itm <= int(1.25 * it) + 2
+
+
+def _aniso27(m, kappa):
+    return problems.anisotropic_27pt(m, 1e-3, kappa)
+
+
+def test_c4_64cubed_resetup_against_the_triple_map():
+    m = 64
+    rng = np.random.default_rng(2024)
+    kappa = np.ones((m + 1,) * 3)
+    A = _aniso27(m, kappa)
+    cfg = draugr.hypre_default_config(agg_trunc_factor=0.2, smoother=draugr.L1JacobiSmootherType(),
+                                      seed=2024)
+    h = draugr.amg_setup(A, cfg)
+    O = oracle.OracleHierarchy(h, with_rmaps=True)
+    n = A.shape[0]
+    b = problems.rhs(n, 7)
+    for update in range(2):
+        kappa = kappa * np.exp(0.5 * rng.standard_normal(kappa.shape))
+        A2 = _aniso27(m, kappa)
+        draugr.amg_resetup(h, A2, cfg, partial=True)
+        O.resetup(A2.data)
+        for l in range(h.nlevels):
+            assert rel(h.export(l, "A_nzval"), O.level_values(l)) < 1e-12, (update, l)
+            assert rel(h.export(l, "invdiag"), O.levels_np[l]["invd"]) < 1e-12, (update, l)
+        assert rel(h.export(-1, "C_dense"), O.dense) < 1e-12
+    xo, ito, _ = O.pcg(np.zeros(n), b, 1, 1, False, 1e-8, 500)
+    x, it, _ = draugr.pcg(np.zeros(n), b, h, cfg, tol=1e-8, maxiter=500, precision="fp64")
+    assert abs(it - ito) <= 1, (it, ito)
+    assert np.linalg.norm(b - A2 @ x) / np.linalg.norm(b) < 1e-8
+    h.free()
+
+
+def test_c4_128cubed_resetup_bit_exact_against_the_host_product():
+    torch = pytest.importorskip("torch")
+    m = 128
+    rng = np.random.default_rng(2024)
+    kappa = np.ones((m + 1,) * 3)
+    A = _aniso27(m, kappa)
+    cfg = draugr.hypre_default_config(agg_trunc_factor=0.2, smoother=draugr.L1JacobiSmootherType(),
+                                      seed=2024)
+    h = draugr.amg_setup(A, cfg)
+    kappa = kappa * np.exp(0.5 * rng.standard_normal(kappa.shape))
+    A2 = _aniso27(m, kappa)
+    v = torch.tensor(A2.data, device="cuda")
+    for _ in range(2):  # the second resetup runs in the steady state
+        draugr.amg_resetup(h, v, cfg)
+    vals = A2.data
+    for l in range(h.nlevels):
+        nxt = h.export(l + 1, "A_nzval") if l + 1 < h.nlevels else h.export(-1, "C_nzval")
+        want = h.galerkin_host(l, vals)
+        assert np.array_equal(nxt, want), (l, rel(nxt, want))
+        vals = nxt
+    n = A.shape[0]
+    b = problems.rhs(n, 8)
+    x, it, _ = draugr.pcg(np.zeros(n), b, h, cfg, tol=1e-8, maxiter=500, precision="fp64")
+    assert np.linalg.norm(b - A2 @ x) / np.linalg.norm(b) < 1e-8
+    h.free()
