@@ -576,6 +576,95 @@ int32_t draugr_b200_bicgstab_device(int32_t handle, int32_t n, double* x_dev, co
   });
 }
 
+static int32_t fgmres_impl(int32_t handle, int32_t n, double* x, const double* b, int32_t config_handle,
+                           double tol, int32_t maxiter, int32_t restart, int32_t precision, double* relres,
+                           bool host) {
+  Config c;
+  auto H = get_hier(handle, config_handle, &c);
+  if (n != n_finest(*H)) fail("DimensionMismatch");
+  if (!x || !b) fail("ArgumentError: NULL vector");
+  if (precision != 0 && precision != 1) fail("precision must be 0 (FP64 cycle) or 1 (FP32 cycle)");
+  if (restart < 1 || restart > 63) fail("restart must be between 1 and 63");
+  DevHier& D = device_of(*H);
+  double rr = 0;
+  int it;
+  if (host) {
+    DR_CK(cudaMemcpyAsync(D.xbuf(), x, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, D.stream()));
+    DR_CK(cudaMemcpyAsync(D.bbuf(), b, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, D.stream()));
+    it = D.fgmres(D.xbuf(), D.bbuf(), opts_of(c), tol, maxiter, restart, precision == 1, &rr, c.verbose);
+    DR_CK(cudaMemcpyAsync(x, D.xbuf(), (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, D.stream()));
+    DR_CK(cudaStreamSynchronize(D.stream()));
+  } else {
+    it = D.fgmres(x, b, opts_of(c), tol, maxiter, restart, precision == 1, &rr, c.verbose);
+  }
+  if (relres) *relres = rr;
+  return it;
+}
+
+int32_t draugr_b200_fgmres(int32_t handle, int32_t n, double* x, const double* b, int32_t config_handle,
+                           double tol, int32_t maxiter, int32_t restart, int32_t precision, double* relres) {
+  return guarded("draugr_b200_fgmres", [&]() {
+    return fgmres_impl(handle, n, x, b, config_handle, tol, maxiter, restart, precision, relres, true);
+  });
+}
+
+int32_t draugr_b200_fgmres_device(int32_t handle, int32_t n, double* x_dev, const double* b_dev,
+                                  int32_t config_handle, double tol, int32_t maxiter, int32_t restart,
+                                  int32_t precision, double* relres) {
+  return guarded("draugr_b200_fgmres_device", [&]() {
+    return fgmres_impl(handle, n, x_dev, b_dev, config_handle, tol, maxiter, restart, precision, relres, false);
+  });
+}
+
+static int32_t refine_impl(int32_t handle, int32_t n, double* x, const double* b, int32_t config_handle,
+                           double tol, int32_t max_outer, double inner_tol, int32_t inner_maxiter,
+                           int32_t inner_method, int32_t precision, double* relres, int32_t* inner_iters,
+                           bool host) {
+  Config c;
+  auto H = get_hier(handle, config_handle, &c);
+  if (n != n_finest(*H)) fail("DimensionMismatch");
+  if (!x || !b) fail("ArgumentError: NULL vector");
+  if (precision != 0 && precision != 1) fail("precision must be 0 (FP64 cycle) or 1 (FP32 cycle)");
+  if (inner_method != 0 && inner_method != 1) fail("inner_method must be 0 (PCG) or 1 (FGMRES)");
+  if (!(inner_tol > 0.0 && inner_tol < 1.0)) fail("inner_tol must lie in (0, 1)");
+  DevHier& D = device_of(*H);
+  double rr = 0;
+  int inner = 0, steps;
+  if (host) {
+    DR_CK(cudaMemcpyAsync(D.xbuf(), x, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, D.stream()));
+    DR_CK(cudaMemcpyAsync(D.bbuf(), b, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, D.stream()));
+    steps = D.refine(D.xbuf(), D.bbuf(), opts_of(c), tol, max_outer, inner_tol, inner_maxiter, inner_method,
+                     precision == 1, &rr, &inner, c.verbose);
+    DR_CK(cudaMemcpyAsync(x, D.xbuf(), (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, D.stream()));
+    DR_CK(cudaStreamSynchronize(D.stream()));
+  } else {
+    steps = D.refine(x, b, opts_of(c), tol, max_outer, inner_tol, inner_maxiter, inner_method, precision == 1,
+                     &rr, &inner, c.verbose);
+  }
+  if (relres) *relres = rr;
+  if (inner_iters) *inner_iters = inner;
+  return steps;
+}
+
+int32_t draugr_b200_refine(int32_t handle, int32_t n, double* x, const double* b, int32_t config_handle,
+                           double tol, int32_t max_outer, double inner_tol, int32_t inner_maxiter,
+                           int32_t inner_method, int32_t precision, double* relres, int32_t* inner_iters) {
+  return guarded("draugr_b200_refine", [&]() {
+    return refine_impl(handle, n, x, b, config_handle, tol, max_outer, inner_tol, inner_maxiter, inner_method,
+                       precision, relres, inner_iters, true);
+  });
+}
+
+int32_t draugr_b200_refine_device(int32_t handle, int32_t n, double* x_dev, const double* b_dev,
+                                  int32_t config_handle, double tol, int32_t max_outer, double inner_tol,
+                                  int32_t inner_maxiter, int32_t inner_method, int32_t precision,
+                                  double* relres, int32_t* inner_iters) {
+  return guarded("draugr_b200_refine_device", [&]() {
+    return refine_impl(handle, n, x_dev, b_dev, config_handle, tol, max_outer, inner_tol, inner_maxiter,
+                       inner_method, precision, relres, inner_iters, false);
+  });
+}
+
 int32_t draugr_b200_pcg_block_device(int32_t handle, int32_t n, int32_t k, double* X_dev, const double* B_dev,
                                      int32_t config_handle, double tol, int32_t maxiter, int32_t precision,
                                      int32_t* iters, double* relres) {

@@ -1175,6 +1175,197 @@ int DevHier::bicgstab(double* x, const double* b, const CycleOpts& o, double tol
   return it;
 }
 
+// One FP32 AMG cycle from a zero guess on an FP64 right-hand side, the
+// result returned in FP64 (the preconditioner of the mixed FGMRES).
+void DevHier::precond32(const double* r, double* out, const CycleOpts& o) {
+  ensure_fp32();
+  const int n = n0_;
+  if (!pr32_) {
+    pr32_ = alloc<float>(n);
+    pz32_ = alloc<float>(n);
+  }
+  counted();
+  k_convert<double, float><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, r, pr32_);
+  const float* z = pz32_;
+  if (L_.empty()) coarse_solve<float>(pr32_, pz32_);
+  else z = cycle_level<float>(0, pz32_, pr32_, true, o, pz32_);
+  counted();
+  k_convert<float, double><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, z, out);
+  DR_CK(cudaGetLastError());
+}
+
+// Flexible GMRES(m) with right preconditioning (Saad's FGMRES): the
+// preconditioned vectors z_j are kept, since the preconditioner (an FP32
+// cycle rounds differently for every input) need not be a fixed linear map.
+// Arnoldi in FP64 with classical Gram-Schmidt applied twice: h = Vᵀw and
+// w -= V h by k_mdot / k_maxpy (deterministic reductions), then ||w||; the
+// Hessenberg column, its Givens rotations and the least-squares update stay
+// on the host (one device-to-host copy per iteration).  Restarts from the
+// true residual; stops when the rotated residual estimate, and then the true
+// residual, is below tol·||b||.
+int DevHier::fgmres(double* x, const double* b, const CycleOpts& o, double tol, int maxiter, int restart,
+                    bool mixed, double* relres, int verbose) {
+  const int n = n0_;
+  const int m = std::max(1, std::min(restart, 63));
+  graphs_clear();
+  const int gx = grid1d(n, max_grid_);
+  if (gm_m_ < m) {
+    // reallocation at a larger restart length (the old arrays stay with the
+    // hierarchy until it is freed)
+    gm_V_ = alloc<double>((size_t)(m + 1) * n);
+    gm_Z_ = alloc<double>((size_t)m * n);
+    gm_w_ = alloc<double>(n);
+    gm_h_ = alloc<double>(2 * 64 + 2);
+    gm_part_ = alloc<double>((size_t)65 * max_grid_);
+    gm_tk_ = alloc<unsigned>(65);
+    DR_CK(cudaMemsetAsync(gm_tk_, 0, 65 * sizeof(unsigned), st_));
+    gm_m_ = m;
+  }
+  double *V = gm_V_, *Z = gm_Z_, *w = gm_w_;
+  const DevMat& A = L_.empty() ? C_ : L_[0].A;
+  auto spmv = [&](const double* in, double* out) {
+    launch_rows(st_, max_grid_, A, A.v, XPlain<double>{in}, EpStore<double>{out});
+  };
+  auto mdot = [&](int k, const double* vw, double* h) {
+    counted();
+    k_mdot<<<dim3(gx, k), kBlock, 0, st_>>>(n, V, (long long)n, vw, gm_part_, gm_tk_, h);
+  };
+  auto maxpy = [&](int k, const double* Mv, const double* h, double sign, double* out) {
+    counted();
+    k_maxpy<<<gx, kBlock, 0, st_>>>(n, k, Mv, (long long)n, h, sign, out);
+  };
+  const double bnorm = std::sqrt(dot_host(b, b, n));
+  if (bnorm == 0.0) {
+    counted();
+    k_fill<double><<<gx, kBlock, 0, st_>>>(n, 0.0, x);
+    DR_CK(cudaStreamSynchronize(st_));
+    if (relres) *relres = 0.0;
+    return 0;
+  }
+  std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m), hh(2 * 64 + 2);
+  int it = 0;
+  double rel = 1.0;
+  while (true) {
+    spmv(x, w);
+    lin3(n, 1.0, b, -1.0, w, 0.0, nullptr, w);  // w = b - A x
+    const double beta = std::sqrt(dot_host(w, w, n));
+    rel = beta / bnorm;
+    if (verbose >= 2) std::printf("  FGMRES restart at iter %4d: relative residual %.6e\n", it, rel);
+    if (rel < tol || it >= maxiter) break;
+    lin3(n, 1.0 / beta, w, 0.0, w, 0.0, nullptr, V);  // V_0 = w / beta
+    std::fill(g.begin(), g.end(), 0.0);
+    g[0] = beta;
+    int jn = 0;  // columns in this cycle
+    for (int j = 0; j < m && it < maxiter; ++j) {
+      ++it;
+      double* vj = V + (size_t)j * n;
+      double* zj = Z + (size_t)j * n;
+      if (mixed) precond32(vj, zj, o);
+      else precond64(vj, zj, o);
+      spmv(zj, w);
+      // classical Gram-Schmidt, twice
+      mdot(j + 1, w, gm_h_);
+      maxpy(j + 1, V, gm_h_, -1.0, w);
+      mdot(j + 1, w, gm_h_ + 64);
+      maxpy(j + 1, V, gm_h_ + 64, -1.0, w);
+      counted();
+      k_dot<double, double, FinStore><<<gx, kBlock, 0, st_>>>(n, w, w, partials_, tickets_ + TK_DOT,
+                                                             FinStore{gm_h_ + 128});
+      DR_CK(cudaGetLastError());
+      DR_CK(cudaMemcpyAsync(hh.data(), gm_h_, hh.size() * sizeof(double), cudaMemcpyDeviceToHost, st_));
+      DR_CK(cudaStreamSynchronize(st_));
+      const double hn = std::sqrt(hh[128]);
+      double* col = &H[(size_t)j * (m + 1)];
+      for (int i = 0; i <= j; ++i) col[i] = hh[i] + hh[64 + i];
+      col[j + 1] = hn;
+      if (hn > 0.0) lin3(n, 1.0 / hn, w, 0.0, w, 0.0, nullptr, V + (size_t)(j + 1) * n);
+      // previous rotations, then a new one zeroing col[j+1]
+      for (int i = 0; i < j; ++i) {
+        const double t = cs[i] * col[i] + sn[i] * col[i + 1];
+        col[i + 1] = -sn[i] * col[i] + cs[i] * col[i + 1];
+        col[i] = t;
+      }
+      const double den = std::hypot(col[j], col[j + 1]);
+      cs[j] = den > 0.0 ? col[j] / den : 1.0;
+      sn[j] = den > 0.0 ? col[j + 1] / den : 0.0;
+      col[j] = den;
+      col[j + 1] = 0.0;
+      g[j + 1] = -sn[j] * g[j];
+      g[j] = cs[j] * g[j];
+      jn = j + 1;
+      const double est = std::fabs(g[j + 1]) / bnorm;
+      if (verbose >= 2) std::printf("  FGMRES iter %4d: estimated relative residual %.6e\n", it, est);
+      if (est < tol || hn == 0.0) break;
+    }
+    // y = H⁻¹ g (upper triangular), x += Z y
+    for (int i = jn - 1; i >= 0; --i) {
+      double t = g[i];
+      for (int k = i + 1; k < jn; ++k) t -= H[(size_t)k * (m + 1) + i] * y[k];
+      const double d = H[(size_t)i * (m + 1) + i];
+      y[i] = d != 0.0 ? t / d : 0.0;
+    }
+    DR_CK(cudaMemcpyAsync(gm_h_, y.data(), (size_t)jn * sizeof(double), cudaMemcpyHostToDevice, st_));
+    maxpy(jn, Z, gm_h_, 1.0, x);
+    DR_CK(cudaStreamSynchronize(st_));  // y leaves scope only after the copy
+  }
+  check_kernel_flag(st_);
+  if (verbose >= 1)
+    std::printf("FGMRES (%s cycle) %s: %d iterations, final residual %.2e\n", mixed ? "FP32" : "FP64",
+                rel < tol ? "converged" : "did NOT converge", it, rel);
+  if (relres) *relres = rel;
+  return it;
+}
+
+int DevHier::refine(double* x, const double* b, const CycleOpts& o, double tol, int max_outer,
+                    double inner_tol, int inner_maxiter, int inner, bool mixed, double* relres,
+                    int* inner_total, int verbose) {
+  const int n = n0_;
+  if (!ir_r_) {
+    ir_r_ = alloc<double>(n);
+    ir_d_ = alloc<double>(n);
+    ir_x_ = alloc<double>(n);
+  }
+  const DevMat& A = L_.empty() ? C_ : L_[0].A;
+  const double bnorm = std::sqrt(dot_host(b, b, n));
+  int total = 0, outer = 0;
+  double rel = 0.0;
+  if (bnorm == 0.0) {
+    counted();
+    k_fill<double><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, 0.0, x);
+    DR_CK(cudaStreamSynchronize(st_));
+  } else {
+    // the iterate lives in a buffer of its own: the inner PCG works in the
+    // hierarchy's iterate buffer, which may be the caller's x (host entry)
+    double* const xout = x;
+    DR_CK(cudaMemcpyAsync(ir_x_, xout, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+    x = ir_x_;
+    while (true) {
+      launch_rows(st_, max_grid_, A, A.v, XPlain<double>{x}, EpStore<double>{ir_r_});
+      lin3(n, 1.0, b, -1.0, ir_r_, 0.0, nullptr, ir_r_);  // r = b - A x (FP64)
+      rel = std::sqrt(dot_host(ir_r_, ir_r_, n)) / bnorm;
+      if (verbose >= 2) std::printf("  refinement step %3d: relative residual %.6e\n", outer, rel);
+      if (rel < tol || outer >= max_outer) break;
+      ++outer;
+      counted();
+      k_fill<double><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, 0.0, ir_d_);
+      double rr = 0.0;
+      const int its = inner == 1 ? fgmres(ir_d_, ir_r_, o, inner_tol, inner_maxiter, 30, mixed, &rr, 0)
+                                 : pcg(ir_d_, ir_r_, o, inner_tol, inner_maxiter, mixed, &rr, 0);
+      total += its;
+      lin3(n, 1.0, x, 1.0, ir_d_, 0.0, nullptr, x);  // x += d
+      if (its == 0) break;  // the inner solver made no progress
+    }
+    DR_CK(cudaMemcpyAsync(xout, ir_x_, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+  }
+  check_kernel_flag(st_);
+  if (verbose >= 1)
+    std::printf("iterative refinement (%s inner, %s cycle): %d steps, %d inner iterations, residual %.2e\n",
+                inner == 1 ? "FGMRES" : "PCG", mixed ? "FP32" : "FP64", outer, total, rel);
+  if (relres) *relres = rel;
+  if (inner_total) *inner_total = total;
+  return outer;
+}
+
 // dL/da_ij = -lambda_i x_j over the finest matrix's nonzeros (CSR order).
 void DevHier::nz_gradient(const double* x, const double* lam, double* grad) {
   const DevMat& A = L_.empty() ? C_ : L_[0].A;

@@ -210,6 +210,17 @@ class DevHier {
   // transposed hierarchy (adjoint solves); Jacobi-type smoothers.
   int bicgstab(double* x, const double* b, const CycleOpts& o, double tol, int maxiter, bool transpose,
                double* relres, int verbose);
+  // Flexible GMRES(restart), right-preconditioned by one AMG cycle per
+  // iteration (FP64, or with `mixed` the FP32 cycle), FP64 Arnoldi
+  // (classical Gram-Schmidt, twice), until ||b - A x|| / ||b|| < tol.
+  int fgmres(double* x, const double* b, const CycleOpts& o, double tol, int maxiter, int restart,
+             bool mixed, double* relres, int verbose);
+  // Iterative refinement: r = b - A x in FP64, A d = r solved to inner_tol
+  // (relative to ||r||) by AMG-PCG (inner 0) or FGMRES (inner 1), x += d,
+  // until ||b - A x|| / ||b|| < tol.  Returns the outer steps; inner_total
+  // receives the inner iterations.
+  int refine(double* x, const double* b, const CycleOpts& o, double tol, int max_outer, double inner_tol,
+             int inner_maxiter, int inner, bool mixed, double* relres, int* inner_total, int verbose);
   // dL/da_ij = -lambda_i x_j for the finest matrix's nonzeros (CSR order).
   void nz_gradient(const double* x, const double* lam, double* grad);
   // Block PCG: k <= 32 right-hand sides at once, X and B row-major n x k
@@ -314,6 +325,13 @@ class DevHier {
   void lin3(int n, double a, const double* x, double b, const double* y, double c, const double* z,
             double* out);
   void precond64(const double* r, double* out, const CycleOpts& o);
+  void precond32(const double* r, double* out, const CycleOpts& o);  // FP32 cycle, FP64 in and out
+  // FGMRES workspace: (restart + 1) basis vectors, restart preconditioned
+  // vectors, one work vector, reduction partials and tickets per column.
+  int gm_m_ = 0;
+  double *gm_V_ = nullptr, *gm_Z_ = nullptr, *gm_w_ = nullptr, *gm_h_ = nullptr, *gm_part_ = nullptr;
+  unsigned* gm_tk_ = nullptr;
+  double *ir_r_ = nullptr, *ir_d_ = nullptr, *ir_x_ = nullptr;  // iterative refinement: residual, correction, iterate
   void upload_csr(DevMat& M, int n, int m, const std::vector<int>& rp, const std::vector<int>& ci,
                   const std::vector<double>* v);
   void spgemm(DevMat& O, const DevMat& S, const DevMat& B, SpgemmList* list = nullptr);

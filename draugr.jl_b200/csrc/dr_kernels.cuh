@@ -824,6 +824,35 @@ k_dot(int n, const TA* __restrict__ a, const TB* __restrict__ b, double* partial
   grid_sum_finalize(s, partials, ticket, fin);
 }
 
+// Krylov basis products for FGMRES (columns of V at stride ld):
+//   k_mdot:  h_j = v_j · w for j < k; blockIdx.y = j, per-block partials,
+//            the last block of column j sums them in block order
+//            (deterministic);
+//   k_maxpy: w += sign · Σ_j h_j v_j, the coefficients read once per block.
+__global__ void __launch_bounds__(kBlock)
+k_mdot(int n, const double* __restrict__ V, long long ld, const double* __restrict__ w, double* partials,
+       unsigned* tickets, double* h) {
+  const int j = blockIdx.y;
+  const double* __restrict__ v = V + (long long)j * ld;
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    s = fma(v[i], w[i], s);
+  grid_sum_finalize(s, partials + (size_t)j * gridDim.x, tickets + j, FinStore{h + j});
+}
+
+__global__ void __launch_bounds__(kBlock)
+k_maxpy(int n, int k, const double* __restrict__ V, long long ld, const double* __restrict__ h, double sign,
+        double* __restrict__ w) {
+  __shared__ double hs[64];
+  for (int j = threadIdx.x; j < k; j += blockDim.x) hs[j] = sign * h[j];
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double s = w[i];
+    for (int j = 0; j < k; ++j) s = fma(hs[j], V[(long long)j * ld + i], s);
+    w[i] = s;
+  }
+}
+
 // x += α p ; r -= α q ; rr = r·r ; optional r32 copy.  α = rz / pq.
 template <typename TR32>
 __global__ void __launch_bounds__(kBlock)

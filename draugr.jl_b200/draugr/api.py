@@ -460,6 +460,53 @@ def bicgstab(x, b, h: Hierarchy, config: AMGConfig | None = None, tol: float = 1
     return x, it, rel.value
 
 
+def fgmres(x, b, h: Hierarchy, config: AMGConfig | None = None, tol: float = 1e-8, maxiter: int = 500,
+           restart: int = 30, precision: str = "fp64"):
+    """Flexible GMRES(restart) right-preconditioned by one AMG cycle (FP64,
+    or precision="mixed": the FP32 cycle with FP64 Arnoldi), for symmetric
+    and nonsymmetric systems.  x (numpy or CUDA tensor) holds the initial
+    guess and is updated in place.  Returns (x, niter, relres)."""
+    config = config if config is not None else (h.config or AMGConfig())
+    prec = {"fp64": 0, "mixed": 1}[precision]
+    lib = _lib.load()
+    rel = C.c_double(0.0)
+    if _is_device(x):
+        it = _lib.check(lib.draugr_b200_fgmres_device(h.handle, x.numel(), x.data_ptr(), b.data_ptr(),
+                                                      config_handle(config), tol, maxiter, restart, prec,
+                                                      C.byref(rel)), "fgmres")
+        return x, it, rel.value
+    _check_vec(x, b, h)
+    it = _lib.check(lib.draugr_b200_fgmres(h.handle, len(x), _ptr(x), _ptr(b), config_handle(config), tol,
+                                           maxiter, restart, prec, C.byref(rel)), "fgmres")
+    return x, it, rel.value
+
+
+def refine(x, b, h: Hierarchy, config: AMGConfig | None = None, tol: float = 1e-8, max_outer: int = 20,
+           inner_tol: float = 1e-4, inner_maxiter: int = 500, inner: str = "pcg", precision: str = "mixed"):
+    """Iterative refinement: FP64 residual r = b - A x, the correction A d = r
+    solved to inner_tol by AMG-PCG (inner="pcg") or FGMRES (inner="fgmres")
+    with an FP64 or FP32 (precision="mixed") cycle, x += d, until the FP64
+    relative residual is below tol.  Returns (x, steps, inner_iterations,
+    relres)."""
+    config = config if config is not None else (h.config or AMGConfig())
+    prec = {"fp64": 0, "mixed": 1}[precision]
+    meth = {"pcg": 0, "fgmres": 1}[inner]
+    lib = _lib.load()
+    rel = C.c_double(0.0)
+    its = C.c_int32(0)
+    if _is_device(x):
+        st = _lib.check(lib.draugr_b200_refine_device(h.handle, x.numel(), x.data_ptr(), b.data_ptr(),
+                                                      config_handle(config), tol, max_outer, inner_tol,
+                                                      inner_maxiter, meth, prec, C.byref(rel), C.byref(its)),
+                        "refine")
+        return x, st, its.value, rel.value
+    _check_vec(x, b, h)
+    st = _lib.check(lib.draugr_b200_refine(h.handle, len(x), _ptr(x), _ptr(b), config_handle(config), tol,
+                                           max_outer, inner_tol, inner_maxiter, meth, prec, C.byref(rel),
+                                           C.byref(its)), "refine")
+    return x, st, its.value, rel.value
+
+
 def nz_gradient(h: Hierarchy, x, lam):
     """dL/da_ij = -lambda_i x_j for the finest matrix's nonzeros (CSR order),
     with x = A^-1 b and lambda = A^-T dL/dx (CUDA tensors); returns a new

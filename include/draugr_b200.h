@@ -139,6 +139,38 @@ int32_t draugr_b200_pcg_device(int32_t handle, int32_t n, double *x_dev, const d
                                int32_t config_handle, double tol, int32_t maxiter,
                                int32_t precision, double *relres);
 
+/* Flexible GMRES(restart), right-preconditioned by one AMG cycle per
+ * iteration, until ||b - A x|| / ||b|| < tol, for symmetric and
+ * nonsymmetric systems.  precision 0: FP64 cycle; precision 1: FP32 cycle
+ * (FP32 copies of the hierarchy) with the Arnoldi basis, Gram-Schmidt
+ * products, least-squares update and residuals in FP64.  restart: 1 to 63
+ * basis vectors before a restart from the true residual.  x holds the
+ * initial guess; relres (may be NULL) receives the final true relative
+ * residual.  Returns iterations or -1.  The reference hands amg_cycle! to
+ * LinearSolve.jl's Krylov methods as a preconditioner instead
+ * (ext/DraugrLinearSolveExt.jl:35-37, src/preconditioner.jl:76-102). */
+int32_t draugr_b200_fgmres(int32_t handle, int32_t n, double *x, const double *b, int32_t config_handle,
+                           double tol, int32_t maxiter, int32_t restart, int32_t precision, double *relres);
+int32_t draugr_b200_fgmres_device(int32_t handle, int32_t n, double *x_dev, const double *b_dev,
+                                  int32_t config_handle, double tol, int32_t maxiter, int32_t restart,
+                                  int32_t precision, double *relres);
+
+/* Iterative refinement: the residual r = b - A x is formed in FP64, the
+ * correction equation A d = r is solved to inner_tol (relative to ||r||) by
+ * AMG-PCG (inner_method 0) or FGMRES(30) (inner_method 1) with an FP64
+ * (precision 0) or FP32 (precision 1) cycle, and x += d, until
+ * ||b - A x|| / ||b|| < tol or max_outer steps.  relres (may be NULL): the
+ * final FP64 relative residual; inner_iters (may be NULL): the inner
+ * iterations in all.  Returns the refinement steps or -1.  No counterpart
+ * in the reference (see draugr_b200_fgmres). */
+int32_t draugr_b200_refine(int32_t handle, int32_t n, double *x, const double *b, int32_t config_handle,
+                           double tol, int32_t max_outer, double inner_tol, int32_t inner_maxiter,
+                           int32_t inner_method, int32_t precision, double *relres, int32_t *inner_iters);
+int32_t draugr_b200_refine_device(int32_t handle, int32_t n, double *x_dev, const double *b_dev,
+                                  int32_t config_handle, double tol, int32_t max_outer, double inner_tol,
+                                  int32_t inner_maxiter, int32_t inner_method, int32_t precision,
+                                  double *relres, int32_t *inner_iters);
+
 /* BiCGStab preconditioned (on the right) by one FP64 AMG cycle per
  * application, until ||b - M x|| / ||b|| < tol, for nonsymmetric systems.
  * transpose 0: M = A.  transpose 1: M = A^T, the adjoint system of a
