@@ -540,39 +540,43 @@ int32_t draugr_b200_pcg_device(int32_t handle, int32_t n, double* x_dev, const d
 }
 
 static int32_t bicgstab_impl(int32_t handle, int32_t n, double* x, const double* b, int32_t config_handle,
-                             double tol, int32_t maxiter, int32_t transpose, double* relres, bool host) {
+                             double tol, int32_t maxiter, int32_t transpose, int32_t precision, double* relres,
+                             bool host) {
   Config c;
   auto H = get_hier(handle, config_handle, &c);
   if (n != n_finest(*H)) fail("DimensionMismatch");
   if (!x || !b) fail("ArgumentError: NULL vector");
+  if (precision != 0 && precision != 1) fail("precision must be 0 (FP64 cycle) or 1 (FP32 cycle)");
+  const bool mixed = precision == 1;
   DevHier& D = device_of(*H);
   double rr = 0;
   int it;
   if (host) {
     DR_CK(cudaMemcpyAsync(D.xbuf(), x, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, D.stream()));
     DR_CK(cudaMemcpyAsync(D.bbuf(), b, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, D.stream()));
-    it = D.bicgstab(D.xbuf(), D.bbuf(), opts_of(c), tol, maxiter, transpose != 0, &rr, c.verbose);
+    it = D.bicgstab(D.xbuf(), D.bbuf(), opts_of(c), tol, maxiter, transpose != 0, &rr, c.verbose, mixed);
     DR_CK(cudaMemcpyAsync(x, D.xbuf(), (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, D.stream()));
     DR_CK(cudaStreamSynchronize(D.stream()));
   } else {
-    it = D.bicgstab(x, b, opts_of(c), tol, maxiter, transpose != 0, &rr, c.verbose);
+    it = D.bicgstab(x, b, opts_of(c), tol, maxiter, transpose != 0, &rr, c.verbose, mixed);
   }
   if (relres) *relres = rr;
   return it;
 }
 
 int32_t draugr_b200_bicgstab(int32_t handle, int32_t n, double* x, const double* b, int32_t config_handle,
-                             double tol, int32_t maxiter, int32_t transpose, double* relres) {
+                             double tol, int32_t maxiter, int32_t transpose, int32_t precision, double* relres) {
   return guarded("draugr_b200_bicgstab", [&]() {
-    return bicgstab_impl(handle, n, x, b, config_handle, tol, maxiter, transpose, relres, true);
+    return bicgstab_impl(handle, n, x, b, config_handle, tol, maxiter, transpose, precision, relres, true);
   });
 }
 
 int32_t draugr_b200_bicgstab_device(int32_t handle, int32_t n, double* x_dev, const double* b_dev,
                                     int32_t config_handle, double tol, int32_t maxiter, int32_t transpose,
-                                    double* relres) {
+                                    int32_t precision, double* relres) {
   return guarded("draugr_b200_bicgstab_device", [&]() {
-    return bicgstab_impl(handle, n, x_dev, b_dev, config_handle, tol, maxiter, transpose, relres, false);
+    return bicgstab_impl(handle, n, x_dev, b_dev, config_handle, tol, maxiter, transpose, precision, relres,
+                         false);
   });
 }
 

@@ -491,7 +491,7 @@ template <> float* DevHier::coarse_x<float>() { return cx32_; }
 template <> const double* DevHier::mval<double>(const DevMat& M) const { return M.v; }
 template <> const float* DevHier::mval<float>(const DevMat& M) const { return M.v32; }
 template <> const double* DevHier::invd<double>(const DevLevel& L) const { return tr_ ? L.invdT : L.invd; }
-template <> const float* DevHier::invd<float>(const DevLevel& L) const { return L.invd32; }
+template <> const float* DevHier::invd<float>(const DevLevel& L) const { return tr_ ? L.invdT32 : L.invd32; }
 
 // ------------------------------------------------------------ FP32 copies
 void DevHier::ensure_fp32() {
@@ -521,8 +521,17 @@ void DevHier::ensure_fp32() {
   cb32_ = alloc<float>(nc_);
   cx32_ = alloc<float>(nc_);
   fp32_ = true;
+  if (at_built_) alloc_transpose_fp32();
   refresh_fp32();
   build_tail();
+}
+
+// FP32 copies of the transposed levels' values and smoother diagonals.
+void DevHier::alloc_transpose_fp32() {
+  for (auto& d : L_) {
+    if (!d.At.v32) d.At.v32 = alloc<float>(d.At.nnz + 4);
+    if (!d.invdT32) d.invdT32 = alloc<float>(d.A.n);
+  }
 }
 
 // Levels whose operands fit in the tail kernel's shared memory (all of them
@@ -745,6 +754,12 @@ void DevHier::refresh_fp32() {
       k_convert<double, float><<<grid1d(d.A.nnz, max_grid_), kBlock, 0, st_>>>(d.A.nnz, d.ilu_L, d.ilu_L32);
       counted();
       k_convert<double, float><<<grid1d(d.A.nnz, max_grid_), kBlock, 0, st_>>>(d.A.nnz, d.ilu_U, d.ilu_U32);
+    }
+    if (d.At.v32) {  // transposed copies (FP32 transposed cycles)
+      counted();
+      k_convert<double, float><<<grid1d(d.At.nnz, max_grid_), kBlock, 0, st_>>>(d.At.nnz, d.At.v, d.At.v32);
+      counted();
+      k_convert<double, float><<<grid1d(d.A.n, max_grid_), kBlock, 0, st_>>>(d.A.n, d.invdT, d.invdT32);
     }
   }
   DR_CK(cudaGetLastError());
@@ -1061,6 +1076,10 @@ void DevHier::build_transpose() {
   DR_CK(cudaStreamSynchronize(st_));
   at_built_ = true;
   refresh_transpose();
+  if (fp32_) {
+    alloc_transpose_fp32();
+    refresh_fp32();
+  }
   DR_CK(cudaStreamSynchronize(st_));
 }
 
@@ -1102,8 +1121,9 @@ void DevHier::precond64(const double* r, double* out, const CycleOpts& o) {
 // with cycles on the transposed hierarchy: x is the initial guess and the
 // solution (device memory).  Returns the iterations; relres = |b - A x|/|b|.
 int DevHier::bicgstab(double* x, const double* b, const CycleOpts& o, double tol, int maxiter,
-                      bool transpose, double* relres, int verbose) {
+                      bool transpose, double* relres, int verbose, bool mixed) {
   if (transpose) build_transpose();
+  if (mixed) ensure_fp32();
   struct Mode {
     bool& f;
     bool old;
@@ -1144,7 +1164,8 @@ int DevHier::bicgstab(double* x, const double* b, const CycleOpts& o, double tol
     if (rho1 == 0.0) break;  // breakdown: r orthogonal to the shadow residual
     const double beta = (rho1 / rho) * (alpha / omega);
     lin3(n, 1.0, r, beta, p, -beta * omega, v, p);  // p = r + beta (p - omega v)
-    precond64(p, ph, o);
+    if (mixed) precond32(p, ph, o);
+    else precond64(p, ph, o);
     spmv(ph, v);
     alpha = rho1 / dot_host(rh, v, n);
     lin3(n, 1.0, r, -alpha, v, 0.0, nullptr, sv);  // s = r - alpha v
@@ -1155,7 +1176,8 @@ int DevHier::bicgstab(double* x, const double* b, const CycleOpts& o, double tol
       rel = snorm / bnorm;
       break;
     }
-    precond64(sv, sh, o);
+    if (mixed) precond32(sv, sh, o);
+    else precond64(sv, sh, o);
     spmv(sh, t);
     const double tt = dot_host(t, t, n);
     omega = tt > 0.0 ? dot_host(t, sv, n) / tt : 0.0;
@@ -1741,8 +1763,8 @@ void DevHier::resetup_values(const double* v_dev) {
   counted();
   k_lu_factor<<<1, threads, 0, st_>>>(nc_, clu_, cpiv_, info_);
   DR_CK(cudaGetLastError());
+  if (at_built_) refresh_transpose();  // before the FP32 copies, which include the transposed ones
   refresh_fp32();
-  if (at_built_) refresh_transpose();
   check_kernel_flag(st_);
   int info = 0;
   DR_CK(cudaMemcpyAsync(&info, info_, sizeof(int), cudaMemcpyDeviceToHost, st_));

@@ -138,6 +138,7 @@ struct DevLevel {
   DevMat At;                 // A^T (transposed cycles; built on first use)
   int* at_perm = nullptr;    // At value k = A value at_perm[k]
   double* invdT = nullptr;   // smoother diagonal of A^T
+  float* invdT32 = nullptr;  // its FP32 copy (FP32 transposed cycles)
   // Chebyshev: inner steps per application, the normalised power-iteration
   // start vector, and the coefficient table (2 * degree entries, then the
   // squared norm of the last power step)
@@ -209,7 +210,7 @@ class DevHier {
   // Right-preconditioned BiCGStab (FP64) on A, or on A^T with cycles on the
   // transposed hierarchy (adjoint solves); Jacobi-type smoothers.
   int bicgstab(double* x, const double* b, const CycleOpts& o, double tol, int maxiter, bool transpose,
-               double* relres, int verbose);
+               double* relres, int verbose, bool mixed = false);
   // Flexible GMRES(restart), right-preconditioned by one AMG cycle per
   // iteration (FP64, or with `mixed` the FP32 cycle), FP64 Arnoldi
   // (classical Gram-Schmidt, twice), until ||b - A x|| / ||b|| < tol.
@@ -326,6 +327,7 @@ class DevHier {
             double* out);
   void precond64(const double* r, double* out, const CycleOpts& o);
   void precond32(const double* r, double* out, const CycleOpts& o);  // FP32 cycle, FP64 in and out
+  void alloc_transpose_fp32();
   // FGMRES workspace: (restart + 1) basis vectors, restart preconditioned
   // vectors, one work vector, reduction partials and tickets per column.
   int gm_m_ = 0;

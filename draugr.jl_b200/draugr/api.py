@@ -441,21 +441,24 @@ def pcg(x, b, h: Hierarchy, config: AMGConfig | None = None, tol: float = 1e-8,
 
 
 def bicgstab(x, b, h: Hierarchy, config: AMGConfig | None = None, tol: float = 1e-8,
-             maxiter: int = 500, transpose: bool = False):
-    """BiCGStab preconditioned by one FP64 AMG cycle (nonsymmetric systems).
-    transpose=True solves A^T x = b with cycles on the transposed hierarchy
-    (the adjoint system of a gradient).  Returns (x, niter, relres)."""
+             maxiter: int = 500, transpose: bool = False, precision: str = "fp64"):
+    """BiCGStab preconditioned by one AMG cycle (nonsymmetric systems):
+    precision="fp64" (FP64 cycle) or "mixed" (FP32 cycle, FP64 vectors,
+    products and dots).  transpose=True solves A^T x = b with cycles on the
+    transposed hierarchy (the adjoint system of a gradient).  Returns
+    (x, niter, relres)."""
     config = config if config is not None else (h.config or AMGConfig())
+    prec = {"fp64": 0, "mixed": 1}[precision]
     lib = _lib.load()
     rel = C.c_double(0.0)
     if _is_device(x):
         it = _lib.check(lib.draugr_b200_bicgstab_device(h.handle, x.numel(), x.data_ptr(), b.data_ptr(),
                                                         config_handle(config), tol, maxiter,
-                                                        1 if transpose else 0, C.byref(rel)), "bicgstab")
+                                                        1 if transpose else 0, prec, C.byref(rel)), "bicgstab")
         return x, it, rel.value
     _check_vec(x, b, h)
     it = _lib.check(lib.draugr_b200_bicgstab(h.handle, len(x), _ptr(x), _ptr(b), config_handle(config),
-                                             tol, maxiter, 1 if transpose else 0, C.byref(rel)),
+                                             tol, maxiter, 1 if transpose else 0, prec, C.byref(rel)),
                     "bicgstab")
     return x, it, rel.value
 
@@ -528,7 +531,7 @@ class _Solve:
 
 
 def amg_solve_diff(values, b, h: Hierarchy, config: AMGConfig | None = None, tol: float = 1e-12,
-                   maxiter: int = 1000, symmetric: bool = False):
+                   maxiter: int = 1000, symmetric: bool = False, precision: str = "fp64"):
     """x = A(values)^-1 b as a differentiable torch operation (the role of a
     ChainRulesCore rrule around solve).  values: CUDA tensor of the finest
     matrix's nonzeros (the setup pattern, CSR order); b: CUDA tensor.  The
@@ -536,21 +539,24 @@ def amg_solve_diff(values, b, h: Hierarchy, config: AMGConfig | None = None, tol
     symmetric, else BiCGStab); the backward pass solves the adjoint system
     A^T lambda = dL/dx on the transposed hierarchy (or with PCG when
     symmetric), then dL/db = lambda and dL/da_ij = -lambda_i x_j.  Only x is
-    kept between the passes."""
+    kept between the passes.  precision="mixed" runs both solves with the
+    FP32 cycle (FP32 copies of the hierarchy and of its transpose) inside
+    the FP64 Krylov iteration."""
     import torch
 
     if _Solve.fn is None:
         class Fn(torch.autograd.Function):
             @staticmethod
-            def forward(ctx, values, b, h, config, tol, maxiter, symmetric):
+            def forward(ctx, values, b, h, config, tol, maxiter, symmetric, precision):
                 amg_resetup(h, values.detach().contiguous(), config)
                 x = torch.zeros_like(b)
                 bb = b.detach().contiguous()
                 if symmetric:
-                    _, it, rel = pcg(x, bb, h, config, tol=tol, maxiter=maxiter)
+                    _, it, rel = pcg(x, bb, h, config, tol=tol, maxiter=maxiter, precision=precision)
                 else:
-                    _, it, rel = bicgstab(x, bb, h, config, tol=tol, maxiter=maxiter)
+                    _, it, rel = bicgstab(x, bb, h, config, tol=tol, maxiter=maxiter, precision=precision)
                 ctx.h, ctx.config, ctx.tol, ctx.maxiter, ctx.symmetric = h, config, tol, maxiter, symmetric
+                ctx.precision = precision
                 ctx.save_for_backward(x)
                 return x
 
@@ -560,15 +566,18 @@ def amg_solve_diff(values, b, h: Hierarchy, config: AMGConfig | None = None, tol
                 lam = torch.zeros_like(x)
                 g = gx.contiguous()
                 if ctx.symmetric:
-                    pcg(lam, g, ctx.h, ctx.config, tol=ctx.tol, maxiter=ctx.maxiter)
+                    pcg(lam, g, ctx.h, ctx.config, tol=ctx.tol, maxiter=ctx.maxiter, precision=ctx.precision)
                 else:
-                    bicgstab(lam, g, ctx.h, ctx.config, tol=ctx.tol, maxiter=ctx.maxiter, transpose=True)
+                    bicgstab(lam, g, ctx.h, ctx.config, tol=ctx.tol, maxiter=ctx.maxiter, transpose=True,
+                             precision=ctx.precision)
                 gv = nz_gradient(ctx.h, x, lam)
-                return gv, lam, None, None, None, None, None
+                return gv, lam, None, None, None, None, None, None
 
         _Solve.fn = Fn
     config = config if config is not None else (h.config or AMGConfig())
-    return _Solve.fn.apply(values, b, h, config, tol, maxiter, symmetric)
+    if precision not in ("fp64", "mixed"):
+        raise ValueError("precision must be 'fp64' or 'mixed'")
+    return _Solve.fn.apply(values, b, h, config, tol, maxiter, symmetric, precision)
 
 
 def pcg_multi(X, B, h: Hierarchy, config: AMGConfig | None = None, tol: float = 1e-8,

@@ -19,10 +19,11 @@ using SparseArrays
 
 export AMGConfig, hypre_default_config, AMGHierarchy
 export amg_setup, amg_solve!, amg_cycle!, amg_resetup!, amg_pcg!
-export amg_bicgstab!, amg_pcg_block!, nz_gradient!
+export amg_bicgstab!, amg_fgmres!, amg_refine!, amg_pcg_block!, nz_gradient!
+export amg_solve_diff, amg_solve_adjoint, amg_resetup_values!
 export DraugrB200Preconditioner
 
-const libdraugr = get(ENV, "DRAUGR_B200_LIB", joinpath(@__DIR__, "..", "libdraugr_b200.so"))
+const libdraugr = get(ENV, "DRAUGR_B200_LIB", joinpath(@__DIR__, "..", "..", "libdraugr_b200.so"))
 
 struct DraugrError <: Exception
     msg::String
@@ -282,28 +283,88 @@ function amg_pcg!(x::AbstractVector{Float64}, b::AbstractVector{Float64}, h::AMG
 end
 
 """
-    amg_bicgstab!(x, b, h, config; tol=1e-8, maxiter=500, transpose=false) -> (x, niter, relres)
+    amg_bicgstab!(x, b, h, config; tol=1e-8, maxiter=500, transpose=false, precision=:fp64) -> (x, niter, relres)
 
-BiCGStab preconditioned (on the right) by one FP64 cycle, for nonsymmetric
+BiCGStab preconditioned (on the right) by one cycle, for nonsymmetric
 systems; `transpose=true` solves Aᵀx = b on the transposed hierarchy (the
 adjoint solve of a gradient).  Every level must use Jacobi, l1-Jacobi or
-SPAI(0) smoothing for the transposed cycle.
+SPAI(0) smoothing for the transposed cycle.  `precision=:mixed` runs the
+cycle on FP32 copies (of the hierarchy or its transpose) with the BiCGStab
+vectors, products and dots in FP64.
 """
 function amg_bicgstab!(x::AbstractVector{Float64}, b::AbstractVector{Float64}, h::AMGHierarchy,
                        config::AMGConfig=AMGConfig(); tol::Real=1e-8, maxiter::Int=500,
-                       transpose::Bool=false)
+                       transpose::Bool=false, precision::Symbol=:fp64)
     rel = Ref{Float64}(0.0)
     tr = Int32(transpose)
+    prec = precision === :mixed ? Int32(1) : Int32(0)
     it = GC.@preserve x b if isdevice(x)
         ccall((:draugr_b200_bicgstab_device, libdraugr), Int32,
-              (Int32, Int32, Ptr{Float64}, Ptr{Float64}, Int32, Float64, Int32, Int32, Ref{Float64}),
-              h.handle, length(x), rawptr(x), rawptr(b), config.handle, tol, maxiter, tr, rel)
+              (Int32, Int32, Ptr{Float64}, Ptr{Float64}, Int32, Float64, Int32, Int32, Int32, Ref{Float64}),
+              h.handle, length(x), rawptr(x), rawptr(b), config.handle, tol, maxiter, tr, prec, rel)
     else
         ccall((:draugr_b200_bicgstab, libdraugr), Int32,
-              (Int32, Int32, Ptr{Float64}, Ptr{Float64}, Int32, Float64, Int32, Int32, Ref{Float64}),
-              h.handle, length(x), pointer(x), pointer(b), config.handle, tol, maxiter, tr, rel)
+              (Int32, Int32, Ptr{Float64}, Ptr{Float64}, Int32, Float64, Int32, Int32, Int32, Ref{Float64}),
+              h.handle, length(x), pointer(x), pointer(b), config.handle, tol, maxiter, tr, prec, rel)
     end
     return x, Int(check(it, "amg_bicgstab!")), rel[]
+end
+
+"""
+    amg_fgmres!(x, b, h, config; tol=1e-8, maxiter=500, restart=30, precision=:fp64) -> (x, niter, relres)
+
+Flexible GMRES(restart), right-preconditioned by one cycle per iteration
+(FP64, or the FP32 cycle with `precision=:mixed`), FP64 Arnoldi.  For
+symmetric and nonsymmetric systems.
+"""
+function amg_fgmres!(x::AbstractVector{Float64}, b::AbstractVector{Float64}, h::AMGHierarchy,
+                     config::AMGConfig=AMGConfig(); tol::Real=1e-8, maxiter::Int=500, restart::Int=30,
+                     precision::Symbol=:fp64)
+    rel = Ref{Float64}(0.0)
+    prec = precision === :mixed ? Int32(1) : Int32(0)
+    it = GC.@preserve x b if isdevice(x)
+        ccall((:draugr_b200_fgmres_device, libdraugr), Int32,
+              (Int32, Int32, Ptr{Float64}, Ptr{Float64}, Int32, Float64, Int32, Int32, Int32, Ref{Float64}),
+              h.handle, length(x), rawptr(x), rawptr(b), config.handle, tol, maxiter, restart, prec, rel)
+    else
+        ccall((:draugr_b200_fgmres, libdraugr), Int32,
+              (Int32, Int32, Ptr{Float64}, Ptr{Float64}, Int32, Float64, Int32, Int32, Int32, Ref{Float64}),
+              h.handle, length(x), pointer(x), pointer(b), config.handle, tol, maxiter, restart, prec, rel)
+    end
+    return x, Int(check(it, "amg_fgmres!")), rel[]
+end
+
+"""
+    amg_refine!(x, b, h, config; tol=1e-8, max_outer=20, inner_tol=1e-4, inner_maxiter=500,
+                inner=:pcg, precision=:mixed) -> (x, steps, inner_iterations, relres)
+
+Iterative refinement: FP64 residual r = b - A x, the correction A d = r
+solved to `inner_tol` by AMG-PCG (`inner=:pcg`) or FGMRES (`inner=:fgmres`)
+with the FP32 (`:mixed`) or FP64 cycle, x += d, until the FP64 relative
+residual is below `tol`.
+"""
+function amg_refine!(x::AbstractVector{Float64}, b::AbstractVector{Float64}, h::AMGHierarchy,
+                     config::AMGConfig=AMGConfig(); tol::Real=1e-8, max_outer::Int=20,
+                     inner_tol::Real=1e-4, inner_maxiter::Int=500, inner::Symbol=:pcg,
+                     precision::Symbol=:mixed)
+    rel = Ref{Float64}(0.0)
+    its = Ref{Int32}(0)
+    prec = precision === :mixed ? Int32(1) : Int32(0)
+    meth = inner === :fgmres ? Int32(1) : Int32(0)
+    st = GC.@preserve x b if isdevice(x)
+        ccall((:draugr_b200_refine_device, libdraugr), Int32,
+              (Int32, Int32, Ptr{Float64}, Ptr{Float64}, Int32, Float64, Int32, Float64, Int32, Int32, Int32,
+               Ref{Float64}, Ref{Int32}),
+              h.handle, length(x), rawptr(x), rawptr(b), config.handle, tol, max_outer, inner_tol,
+              inner_maxiter, meth, prec, rel, its)
+    else
+        ccall((:draugr_b200_refine, libdraugr), Int32,
+              (Int32, Int32, Ptr{Float64}, Ptr{Float64}, Int32, Float64, Int32, Float64, Int32, Int32, Int32,
+               Ref{Float64}, Ref{Int32}),
+              h.handle, length(x), pointer(x), pointer(b), config.handle, tol, max_outer, inner_tol,
+              inner_maxiter, meth, prec, rel, its)
+    end
+    return x, Int(check(st, "amg_refine!")), Int(its[]), rel[]
 end
 
 """
@@ -344,6 +405,74 @@ function nz_gradient!(grad::AbstractVector{Float64}, h::AMGHierarchy, x::Abstrac
                                      h.handle, length(x), rawptr(x), rawptr(λ), rawptr(grad))
     check(rc, "nz_gradient!")
     return grad
+end
+
+"""
+    amg_resetup_values!(h, nzval) -> h
+
+Partial resetup from new values of the finest matrix in CSR order (the
+setup's pattern), on the device (`nzval` a device array) or copied there.
+"""
+function amg_resetup_values!(h::AMGHierarchy, nzval::AbstractVector{Float64})
+    GC.@preserve nzval begin
+        if isdevice(nzval)
+            check(ccall((:draugr_b200_resetup_values_device, libdraugr), Int32, (Int32, Int64, Ptr{Float64}),
+                        h.handle, length(nzval), rawptr(nzval)), "amg_resetup_values!")
+        else
+            throw(ArgumentError("amg_resetup_values! takes device values; use amg_resetup! for a host matrix"))
+        end
+    end
+    return h
+end
+
+"""
+    amg_solve_diff(nzval, b, h, config; tol=1e-12, maxiter=1000, symmetric=false, precision=:fp64) -> x
+
+x = A(nzval)⁻¹ b, where nzval are the finest matrix's nonzeros in CSR order
+(the setup pattern): a partial resetup with `nzval`, then AMG-PCG
+(`symmetric`) or AMG-BiCGStab.  Differentiable: the package extension for
+ChainRulesCore defines its `rrule`, whose pullback solves Aᵀλ = x̄ on the
+transposed hierarchy and returns (nzval̄ = -λᵢxⱼ per nonzero, b̄ = λ).
+`nzval`, `b` and the result are device arrays (e.g. CuArray{Float64}).
+"""
+function amg_solve_diff(nzval::AbstractVector{Float64}, b::AbstractVector{Float64}, h::AMGHierarchy,
+                        config::AMGConfig=AMGConfig(); tol::Real=1e-12, maxiter::Int=1000,
+                        symmetric::Bool=false, precision::Symbol=:fp64)
+    amg_resetup_values!(h, nzval)
+    x = similar(b)
+    fill!(x, 0.0)
+    if symmetric
+        amg_pcg!(x, b, h, config; tol=tol, maxiter=maxiter, precision=precision)
+    else
+        amg_bicgstab!(x, b, h, config; tol=tol, maxiter=maxiter, precision=precision)
+    end
+    return x
+end
+
+"""
+    amg_solve_adjoint(x̄, x, h, config; tol, maxiter, symmetric, precision) -> (nzval̄, b̄)
+
+The pullback of `amg_solve_diff` at its result x: λ = A⁻ᵀ x̄ (PCG when
+symmetric, else BiCGStab on the transposed hierarchy), b̄ = λ and
+nzval̄ᵢⱼ = -λᵢ xⱼ over the nonzeros (draugr_b200_nz_gradient_device).  Only
+x is needed from the forward pass.
+"""
+function amg_solve_adjoint(x̄::AbstractVector{Float64}, x::AbstractVector{Float64}, h::AMGHierarchy,
+                           config::AMGConfig=AMGConfig(); tol::Real=1e-12, maxiter::Int=1000,
+                           symmetric::Bool=false, precision::Symbol=:fp64)
+    λ = similar(x)
+    fill!(λ, 0.0)
+    if symmetric
+        amg_pcg!(λ, x̄, h, config; tol=tol, maxiter=maxiter, precision=precision)
+    else
+        amg_bicgstab!(λ, x̄, h, config; tol=tol, maxiter=maxiter, transpose=true, precision=precision)
+    end
+    info = zeros(Int64, 10)
+    check(ccall((:draugr_b200_level_info, libdraugr), Int32, (Int32, Int32, Ptr{Int64}), h.handle, 0, info),
+          "amg_solve_adjoint")
+    grad = similar(x, Int(info[2]))
+    nz_gradient!(grad, h, x, λ)
+    return grad, λ
 end
 
 """

@@ -171,21 +171,24 @@ int32_t draugr_b200_refine_device(int32_t handle, int32_t n, double *x_dev, cons
                                   int32_t inner_maxiter, int32_t inner_method, int32_t precision,
                                   double *relres, int32_t *inner_iters);
 
-/* BiCGStab preconditioned (on the right) by one FP64 AMG cycle per
+/* BiCGStab preconditioned (on the right) by one AMG cycle per
  * application, until ||b - M x|| / ||b|| < tol, for nonsymmetric systems.
  * transpose 0: M = A.  transpose 1: M = A^T, the adjoint system of a
  * gradient computation, with cycles on the transposed hierarchy (A^T on
  * every level, the same P and P^T, the transposed coarsest LU solve);
- * every level must use Jacobi, l1-Jacobi or SPAI(0) smoothing.  x holds the initial guess;
+ * every level must use Jacobi, l1-Jacobi or SPAI(0) smoothing.
+ * precision 0: FP64 cycle; precision 1: FP32 cycle (FP32 copies of the
+ * hierarchy, or of the transposed hierarchy) with the BiCGStab vectors,
+ * products with M and dot products in FP64.  x holds the initial guess;
  * relres (may be NULL) receives the final true relative residual.  Returns
  * iterations or -1.  No counterpart in the reference, which has neither a
  * nonsymmetric Krylov solver nor adjoints. */
 int32_t draugr_b200_bicgstab(int32_t handle, int32_t n, double *x, const double *b,
                              int32_t config_handle, double tol, int32_t maxiter,
-                             int32_t transpose, double *relres);
+                             int32_t transpose, int32_t precision, double *relres);
 int32_t draugr_b200_bicgstab_device(int32_t handle, int32_t n, double *x_dev, const double *b_dev,
                                     int32_t config_handle, double tol, int32_t maxiter,
-                                    int32_t transpose, double *relres);
+                                    int32_t transpose, int32_t precision, double *relres);
 
 /* Conjugate gradients for k (1..32) right-hand sides of the same matrix
  * at once: X and B are device arrays of n x k doubles, row-major (column c

@@ -401,7 +401,7 @@ def test_julia_bindings_match_the_c_header():
     ccall signatures are checked against include/*.h: every symbol is
     declared, with the same number of arguments, each of a matching kind
     (Int32 / Int64 / Float64 / pointer / string), and a matching return."""
-    jl = (ROOT / "draugr.jl_b200" / "julia" / "DraugrB200.jl").read_text()
+    jl = "\n".join(f.read_text() for f in sorted((ROOT / "draugr.jl_b200" / "julia").rglob("*.jl")))
     decls = _c_params()
 
     def kind_c(t):
@@ -443,3 +443,19 @@ def test_julia_bindings_match_the_c_header():
         assert kind_jl(ret) == kind_c(cret), (name, ret, cret)
         seen += 1
     assert seen >= 15
+
+
+def test_julia_rrule_extension_is_declared():
+    """The ChainRulesCore rrule for amg_solve_diff lives in a package
+    extension (loaded with ChainRulesCore): Project.toml declares it, the
+    extension defines the rrule and its pullback calls the device adjoint."""
+    jdir = ROOT / "draugr.jl_b200" / "julia"
+    proj = (jdir / "Project.toml").read_text()
+    assert 'DraugrB200ChainRulesCoreExt = "ChainRulesCore"' in proj and "[weakdeps]" in proj
+    ext = (jdir / "ext" / "DraugrB200ChainRulesCoreExt.jl").read_text()
+    assert "ChainRulesCore.rrule(::typeof(DraugrB200.amg_solve_diff)" in ext
+    assert "DraugrB200.amg_solve_adjoint(" in ext
+    src = (jdir / "src" / "DraugrB200.jl").read_text()
+    for fn in ("function amg_solve_diff(", "function amg_solve_adjoint(", "function amg_fgmres!(",
+               "function amg_refine!("):
+        assert fn in src, fn

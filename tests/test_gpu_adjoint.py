@@ -42,29 +42,30 @@ def cpu_adjoint(A, J, b, S, d):
     return J.T @ gvals, lam
 
 
-def gpu_grad(make, kappa, b, S, d, symmetric, h=None, tol=1e-13):
+def gpu_grad(make, kappa, b, S, d, symmetric, h=None, tol=1e-13, precision="fp64"):
     A, J = make(kappa)
     if h is None:
         h = draugr.amg_setup(A, CFG)
     vals = torch.tensor(A.data, device="cuda", requires_grad=True)
     bt = torch.tensor(b, device="cuda", requires_grad=True)
-    x = draugr.amg_solve_diff(vals, bt, h, CFG, tol=tol, maxiter=2000, symmetric=symmetric)
+    x = draugr.amg_solve_diff(vals, bt, h, CFG, tol=tol, maxiter=2000, symmetric=symmetric,
+                              precision=precision)
     St = torch.tensor(S, device="cuda")
     L = ((x[St] - torch.tensor(d, device="cuda")) ** 2).sum()
     L.backward()
     return h, float(L.detach()), J.T @ vals.grad.cpu().numpy(), bt.grad.cpu().numpy()
 
 
-def gpu_loss(h, make, kappa, b, S, d, symmetric, tol=1e-13):
+def gpu_loss(h, make, kappa, b, S, d, symmetric, tol=1e-13, precision="fp64"):
     v = make(kappa, values_only=True)
     with torch.no_grad():
         x = draugr.amg_solve_diff(torch.tensor(v, device="cuda"), torch.tensor(b, device="cuda"), h,
-                                  CFG, tol=tol, maxiter=3000, symmetric=symmetric)
+                                  CFG, tol=tol, maxiter=3000, symmetric=symmetric, precision=precision)
     return float(((x.cpu().numpy()[S] - d) ** 2).sum())
 
 
 def check_finite_differences(h, make, kappa, b, S, d, symmetric, L, gk, rng, ndir=20, tol=1e-13,
-                             rtol=1e-5):
+                             rtol=1e-5, precision="fp64"):
     """Central differences of the GPU forward solve's loss (h = 1e-6,
     relative step) along `ndir` seeded directions, against gk . delta
     (relative error `rtol`); the forward solves stop at relative residual
@@ -73,8 +74,8 @@ def check_finite_differences(h, make, kappa, b, S, d, symmetric, L, gk, rng, ndi
     shape = kappa.shape
     for t in range(ndir):
         delta = rng.normal(size=shape) * kappa
-        lp = gpu_loss(h, make, kappa + eps * delta, b, S, d, symmetric, tol)
-        lm = gpu_loss(h, make, kappa - eps * delta, b, S, d, symmetric, tol)
+        lp = gpu_loss(h, make, kappa + eps * delta, b, S, d, symmetric, tol, precision)
+        lm = gpu_loss(h, make, kappa - eps * delta, b, S, d, symmetric, tol, precision)
         fd = (lp - lm) / (2 * eps)
         ad = float(gk @ delta.ravel())
         assert abs(fd - ad) <= rtol * max(abs(ad), 1e-3 * abs(L)), (t, fd, ad)
@@ -163,3 +164,45 @@ def test_transposed_bicgstab_solves_the_adjoint_system(smoother):
                                     transpose=transpose)
         assert it < 500 and rr < 1e-10
         assert np.linalg.norm(b - M @ x) / np.linalg.norm(b) < 1e-10
+
+
+@pytest.mark.parametrize("name", sorted(CASES) + sorted(FULL))
+def test_fp32_cycle_gradient(name):
+    """The precision the C5 configuration names: both solves of the
+    gradient (forward, and the adjoint on the transposed hierarchy) with the
+    FP32 cycle (FP32 copies of the hierarchy and of its transpose) inside
+    the FP64 Krylov iteration, to 1e-13.  Checked against the FP64 CPU
+    adjoint (direct solves; for the 96^3 diffusion operator the oracle's
+    FP64 AMG-PCG to 1e-15) at 1e-10 normwise relative, and against central
+    differences on 20 seeded directions (h = 1e-6): of the FP32-cycle
+    forward solve at the small sizes (1e-5 relative), of the FP64 forward
+    solve at the full sizes (1e-4 relative), where the differences need the
+    forward solves to stop near 1e-15 and BiCGStab with the FP32 cycle
+    stalls a little above that."""
+    full = name in FULL
+    make, shape, symmetric = FULL[name] if full else CASES[name]
+    rng = np.random.default_rng(29)
+    kappa = np.exp(rng.normal(0.0, 1.0, shape))
+    n = kappa.size
+    b = rng.uniform(-1, 1, n)
+    S = np.sort(rng.choice(n, size=max(1, n // 100), replace=False))
+    d = rng.uniform(-0.1, 0.1, len(S))
+    A, J = make(kappa)
+    h, L, gk, gb = gpu_grad(make, kappa, b, S, d, symmetric, tol=1e-13, precision="mixed")
+    if full and symmetric:
+        O = oracle.OracleHierarchy(h)
+        x, _, _ = O.pcg(np.zeros(n), b, tol=1e-15, maxiter=3000)
+        gx = np.zeros(n)
+        gx[S] = 2 * (x[S] - d)
+        lam, _, _ = O.pcg(np.zeros(n), gx, tol=1e-15, maxiter=3000)
+        rows = np.repeat(np.arange(n), np.diff(A.indptr))
+        ref_k, ref_b = J.T @ (-lam[rows] * x[A.indices]), lam
+    else:
+        ref_k, ref_b = cpu_adjoint(A, J, b, S, d)
+    ek, eb = rel(gk, ref_k), rel(gb, ref_b)
+    print(f"{name}, FP32 cycle: gradient vs FP64 CPU adjoint: kappa {ek:.2e}, b {eb:.2e}")
+    assert ek < 1e-10 and eb < 1e-10, (ek, eb)
+    if full:
+        check_finite_differences(h, make, kappa, b, S, d, symmetric, L, gk, rng, tol=1e-15, rtol=1e-4)
+    else:
+        check_finite_differences(h, make, kappa, b, S, d, symmetric, L, gk, rng, precision="mixed")
