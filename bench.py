@@ -685,6 +685,43 @@ def run_batch(args):
     for A, b, x in zip(mats, bs, xs):
         bn = b.cpu().numpy()
         worst = max(worst, float(np.linalg.norm(bn - A @ x.cpu().numpy()) / np.linalg.norm(bn)))
+    # the same systems merged into one batch: one launch per cycle stage for all
+    t0 = time.time()
+    batch = draugr.batch_setup(hs, cfg)
+    merge_s = time.time() - t0
+    bcat = torch.cat(bs)
+    xcat = torch.zeros_like(bcat)
+    for _ in range(args.warmup):
+        xcat.zero_()
+        draugr.pcg_batched(xcat, bcat, batch, cfg, tol=TOL, maxiter=MAXITER, precision="mixed")
+    seg_t, seg_lat = [], []
+    for _ in range(args.steps):
+        xcat.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _, sits, srel = draugr.pcg_batched(xcat, bcat, batch, cfg, tol=TOL, maxiter=MAXITER, precision="mixed")
+        e1.record()
+        e1.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        seg_t.append(t)
+        # a system's latency: the iterations it needed at the batch's time per iteration
+        seg_lat += [t * int(k) / max(1, int(sits.max())) for k in sits]
+    xh = xcat.cpu().numpy()
+    seg_worst = 0.0
+    for k, (A, b) in enumerate(zip(mats, bs)):
+        lo, hi = int(batch.offsets[k]), int(batch.offsets[k + 1])
+        bn = b.cpu().numpy()
+        seg_worst = max(seg_worst, float(np.linalg.norm(bn - A @ xh[lo:hi]) / np.linalg.norm(bn)))
+    segmented = {"path": "draugr_b200_batch_pcg_device (hierarchies merged level by level; one launch per "
+                         "cycle stage, dot product and update for all systems; one iteration per CUDA graph)",
+                 "solves_per_s": args.systems / float(np.mean(seg_t)), "ms_per_batch": 1e3 * float(np.mean(seg_t)),
+                 "latency_s": {"p50": float(np.percentile(seg_lat, 50)), "p99": float(np.percentile(seg_lat, 99))},
+                 "iterations": [int(sits.min()), int(sits.max())], "worst_relres_fp64_verified": seg_worst,
+                 "merge_s_cpu": round(merge_s, 2),
+                 "timing": "CUDA events around each batched solve (device-resident vectors)"}
+    batch.free()
     # one operator, many right-hand sides
     A96 = problems.poisson3d(96)
     h96 = draugr.amg_setup(A96, cfg)
@@ -734,6 +771,7 @@ def run_batch(args):
             "sequential_solves_per_s": args.systems / seq_wall,
             "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
             "worst_relres_fp64_verified": worst, "setup_s_cpu": round(setup_s, 2),
+            "segmented": segmented,
             "timing": "host wall clock around each batch (device synchronised on both sides); "
                       "latency = each solve's call from a pool thread",
             "multi_rhs": {"workload": "3D 7-point Poisson 96^3, 32 right-hand sides, mixed PCG to 1e-8, "

@@ -28,6 +28,7 @@ struct Hier {
   std::unique_ptr<DevHier> dev;
   int device = 0;
   std::string summary;
+  std::unique_ptr<BatchLayout> batch;  // set for a batch of merged systems
 };
 
 std::mutex g_mu;
@@ -99,7 +100,7 @@ DevHier& device_of(Hier& H) {
     int dev = 0;
     DR_CK(cudaGetDevice(&dev));
     H.device = dev;
-    H.dev.reset(new DevHier(H.host, dev));
+    H.dev.reset(new DevHier(H.host, dev, H.batch.get()));
   }
   DR_CK(cudaSetDevice(H.device));
   return *H.dev;
@@ -666,6 +667,56 @@ int32_t draugr_b200_refine_device(int32_t handle, int32_t n, double* x_dev, cons
   return guarded("draugr_b200_refine_device", [&]() {
     return refine_impl(handle, n, x_dev, b_dev, config_handle, tol, max_outer, inner_tol, inner_maxiter,
                        inner_method, precision, relres, inner_iters, false);
+  });
+}
+
+int32_t draugr_b200_batch_setup(int32_t nsys, const int32_t* handles) {
+  return guarded("draugr_b200_batch_setup", [&]() -> int32_t {
+    if (nsys < 1 || !handles) fail("ArgumentError: a batch needs at least one hierarchy handle");
+    std::vector<std::shared_ptr<Hier>> keep;
+    std::vector<const HostHierarchy*> hs;
+    for (int32_t s = 0; s < nsys; ++s) {
+      keep.push_back(get_hier_only(handles[s]));
+      if (keep.back()->batch) fail("a batch cannot contain another batch");
+      hs.push_back(&keep.back()->host);
+    }
+    auto B = std::make_shared<Hier>();
+    B->batch = std::make_unique<BatchLayout>();
+    B->host = merge_batch(hs, *B->batch);
+    device_of(*B);
+    std::lock_guard<std::mutex> lk(g_mu);
+    int32_t h = new_handle();
+    g_hier[h] = B;
+    return h;
+  });
+}
+
+int32_t draugr_b200_batch_offsets(int32_t handle, int64_t* offsets) {
+  return guarded("draugr_b200_batch_offsets", [&]() -> int32_t {
+    auto H = get_hier_only(handle);
+    if (!H->batch) fail("not a batch handle");
+    const BatchLayout& L = *H->batch;
+    if (offsets) {
+      for (int s = 0; s < L.nsys; ++s) offsets[s] = L.off[0][s];
+      offsets[L.nsys] = L.ntotal[0];
+    }
+    return L.nsys;
+  });
+}
+
+int32_t draugr_b200_batch_pcg_device(int32_t handle, int32_t n, double* x_dev, const double* b_dev,
+                                     int32_t config_handle, double tol, int32_t maxiter, int32_t precision,
+                                     int32_t* iters, double* relres) {
+  return guarded("draugr_b200_batch_pcg_device", [&]() -> int32_t {
+    Config c;
+    auto H = get_hier(handle, config_handle, &c);
+    if (!H->batch) fail("not a batch handle");
+    if (n != H->batch->ntotal[0]) fail("DimensionMismatch: n must be the batch's total rows");
+    if (precision != 0 && precision != 1) fail("precision must be 0 (FP64 cycle) or 1 (FP32 cycle)");
+    if (!x_dev || !b_dev) fail("ArgumentError: NULL vector");
+    if (c.cycle_w) fail("batched solves run V-cycles");
+    return device_of(*H).pcg_batch_seg(x_dev, b_dev, opts_of(c), tol, maxiter, precision == 1, iters, relres,
+                                       c.verbose);
   });
 }
 

@@ -278,8 +278,9 @@ static void h2d(T* d, const std::vector<T>& h, cudaStream_t st) {
   if (!h.empty()) DR_CK(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st));
 }
 
-DevHier::DevHier(const HostHierarchy& H, int device) {
+DevHier::DevHier(const HostHierarchy& H, int device, const BatchLayout* batch) {
   device_ = device;
+  if (batch) batch_ = std::make_unique<BatchLayout>(*batch);
   DR_CK(cudaSetDevice(device));
   DR_CK(cudaDeviceGetAttribute(&nsm_, cudaDevAttrMultiProcessorCount, device));
   max_grid_ = nsm_ * 8;
@@ -305,7 +306,9 @@ DevHier::DevHier(const HostHierarchy& H, int device) {
       up_csr(d.R, h.P.nc, h.P.nf, h.T.off, h.T.rows, &h.Rv);
       d.smoother = h.smoother;
       d.omega = h.omega;
-      d.invd = alloc<double>(h.A.n);
+      d.nv = batch ? batch->ntotal[l] : h.A.n;
+      d.invd = alloc<double>(d.nv);
+      if (d.nv > h.A.n) DR_CK(cudaMemsetAsync(d.invd, 0, (size_t)d.nv * sizeof(double), st_));
       h2d(d.invd, h.invdiag, st_);
       d.ncolors = h.num_colors;
       d.color_off = h.color_off;
@@ -316,7 +319,7 @@ DevHier::DevHier(const HostHierarchy& H, int device) {
       d.has_rap = h.has_rap_map;
       if (d.has_rap) up_csr(d.AP, h.A.n, h.P.nc, h.ap_rp, h.ap_ci, nullptr);
 
-      const int n = h.A.n;
+      const int n = d.nv;
       if (l > 0) {
         d.v64.xa = alloc<double>(n);
         d.v64.b = alloc<double>(n);
@@ -364,13 +367,48 @@ DevHier::DevHier(const HostHierarchy& H, int device) {
     }
     nc_ = H.nc;
     up_csr(C_, H.coarse.n, H.coarse.m, H.coarse.rp, H.coarse.ci, &H.coarse.v);
-    cdense_ = alloc<double>((size_t)nc_ * nc_);
-    clu_ = alloc<double>((size_t)nc_ * nc_);
-    cpiv_ = alloc<int>(nc_);
     info_ = alloc<int>(1);
-    h2d(cdense_, H.coarse_dense, st_);
-    h2d(clu_, H.coarse_lu, st_);
-    h2d(cpiv_, H.coarse_piv, st_);
+    if (!batch) {
+      cdense_ = alloc<double>((size_t)nc_ * nc_);
+      clu_ = alloc<double>((size_t)nc_ * nc_);
+      cpiv_ = alloc<int>(nc_);
+      h2d(cdense_, H.coarse_dense, st_);
+      h2d(clu_, H.coarse_lu, st_);
+      h2d(cpiv_, H.coarse_piv, st_);
+    } else {
+      // the coarsest systems of the batch, per merged level
+      blu_ = alloc<double>(batch->lu.size());
+      bpiv_ = alloc<int>(batch->piv.size());
+      h2d(blu_, batch->lu, st_);
+      h2d(bpiv_, batch->piv, st_);
+      batch_dev_.resize(batch->coarse.size());
+      for (size_t l = 0; l < batch->coarse.size(); ++l) {
+        const BatchLayout::Coarse& c = batch->coarse[l];
+        BatchDev& b = batch_dev_[l];
+        b.nblk = (int)c.off.size();
+        b.maxn = c.maxn;
+        if (!b.nblk) continue;
+        b.off = alloc<int>(c.off.size());
+        b.nb = alloc<int>(c.nb.size());
+        b.poff = alloc<int>(c.poff.size());
+        b.luoff = alloc<long long>(c.luoff.size());
+        h2d(b.off, c.off, st_);
+        h2d(b.nb, c.nb, st_);
+        h2d(b.poff, c.poff, st_);
+        h2d(b.luoff, c.luoff, st_);
+      }
+      // finest-level segments: system s occupies rows off[0][s] .. off[0][s + 1] - 1
+      std::vector<int> so(batch->nsys + 1, 0), sid(n0_);
+      for (int q = 0; q < batch->nsys; ++q) so[q] = batch->off[0][q];
+      so[batch->nsys] = n0_;
+      for (int q = 0; q < batch->nsys; ++q)
+        for (int i = so[q]; i < so[q + 1]; ++i) sid[i] = q;
+      seg_off_ = alloc<int>(so.size());
+      seg_id_ = alloc<int>(sid.size());
+      h2d(seg_off_, so, st_);
+      h2d(seg_id_, sid, st_);
+      DR_CK(cudaStreamSynchronize(st_));
+    }
     cb64_ = alloc<double>(nc_);
     cx64_ = alloc<double>(nc_);
     partials_ = alloc<double>(max_grid_ + 32);
@@ -381,13 +419,14 @@ DevHier::DevHier(const HostHierarchy& H, int device) {
     DR_CK(cudaMallocHost(&hscal_, SC_N * sizeof(double)));
     xd_ = alloc<double>(n0_);
     bd_ = alloc<double>(n0_);
-    if ((size_t)nc_ * sizeof(double) > 48 * 1024) {
+    if (!batch && (size_t)nc_ * sizeof(double) > 48 * 1024) {
       size_t need = (size_t)nc_ * sizeof(double);
       if (need > 200 * 1024) fail("coarsest level too large for the on-chip LU solve (n_c = " + std::to_string(nc_) + ")");
       DR_CK(cudaFuncSetAttribute(k_lu_solve<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
       DR_CK(cudaFuncSetAttribute(k_lu_solve<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
     }
-    build_tail();
+    if (batch) tail_ = nl;  // no shared-memory tail: every level runs as its own launches
+    else build_tail();
     DR_CK(cudaStreamSynchronize(st_));
   } catch (...) {
     for (void* p : allocs_) cudaFree(p);
@@ -445,6 +484,7 @@ DevHier::~DevHier() {
   cudaSetDevice(device_);
   if (st_) cudaStreamSynchronize(st_);
   graphs_clear();
+  if (seg_graph_) cudaGraphExecDestroy(seg_graph_);
   for (void* p : allocs_) cudaFree(p);
   if (hscal_) cudaFreeHost(hscal_);
   cudaEventDestroy(ev_[0]);
@@ -501,8 +541,8 @@ void DevHier::ensure_fp32() {
     d.A.v32 = alloc<float>(d.A.nnz + 4);
     d.P.v32 = alloc<float>(d.P.nnz + 4);
     d.R.v32 = alloc<float>(d.R.nnz + 4);
-    d.invd32 = alloc<float>(d.A.n);
-    const int n = d.A.n;
+    d.invd32 = alloc<float>(d.nv);
+    const int n = d.nv;
     d.v32.xa = alloc<float>(n);
     d.v32.xb = alloc<float>(n);
     d.v32.b = alloc<float>(n);
@@ -523,7 +563,7 @@ void DevHier::ensure_fp32() {
   fp32_ = true;
   if (at_built_) alloc_transpose_fp32();
   refresh_fp32();
-  build_tail();
+  if (!batch_) build_tail();
 }
 
 // FP32 copies of the transposed levels' values and smoother diagonals.
@@ -744,7 +784,7 @@ void DevHier::refresh_fp32() {
     counted();
     k_convert<double, float><<<grid1d(d.R.nnz, max_grid_), kBlock, 0, st_>>>(d.R.nnz, d.R.v, d.R.v32);
     counted();
-    k_convert<double, float><<<grid1d(d.A.n, max_grid_), kBlock, 0, st_>>>(d.A.n, d.invd, d.invd32);
+    k_convert<double, float><<<grid1d(d.nv, max_grid_), kBlock, 0, st_>>>(d.nv, d.invd, d.invd32);
     if (d.spai1_M32) {
       counted();
       k_convert<double, float><<<grid1d(d.A.nnz, max_grid_), kBlock, 0, st_>>>(d.A.nnz, d.spai1_M, d.spai1_M32);
@@ -966,9 +1006,11 @@ T* DevHier::cycle_level(int l, T* x, const T* b, bool x_zero, const CycleOpts& o
     xn = vecs<T>(l + 1).xa;
     xn = cycle_level<T>(l + 1, xn, bn, true, o, nullptr, nullptr, false, x1n);
     if (o.w) xn = cycle_level<T>(l + 1, xn, bn, false, o, nullptr);
+    if (batch_) batch_coarse<T>(l + 1, bn, xn);  // the systems whose coarsest level is l + 1
   } else {
     xn = coarse_x<T>();
-    coarse_solve<T>(bn, xn);
+    if (batch_) batch_coarse<T>(l + 1, bn, xn);
+    else coarse_solve<T>(bn, xn);
   }
   // prolongation and correction  x += P xc
   launch_rows(st_, max_grid_, L.P, mval<T>(L.P), XPlain<T>{xn}, EpAddTo<T>{x});
@@ -1386,6 +1428,192 @@ int DevHier::refine(double* x, const double* b, const CycleOpts& o, double tol, 
   if (relres) *relres = rel;
   if (inner_total) *inner_total = total;
   return outer;
+}
+
+// ------------------------------------------------------------ batch
+// The coarsest solves of the systems whose coarsest level is merged level l
+// (rows at the end of that level's vectors), one block per system.
+template <typename T>
+void DevHier::batch_coarse(int l, const T* b, T* x) {
+  if (l >= (int)batch_dev_.size()) return;
+  const BatchDev& c = batch_dev_[l];
+  if (c.nblk == 0) return;
+  int threads = 32;
+  while (threads < c.maxn && threads < 256) threads *= 2;
+  counted();
+  k_lu_solve_batch<T><<<c.nblk, threads, (size_t)std::max(c.maxn, 1) * sizeof(double), st_>>>(
+      c.off, c.nb, c.luoff, c.poff, blu_, bpiv_, b, x);
+  DR_CK(cudaGetLastError());
+}
+template void DevHier::batch_coarse<double>(int, const double*, double*);
+template void DevHier::batch_coarse<float>(int, const float*, float*);
+
+// Conjugate gradients on every system of a batch at once.  Each iteration
+// (one CUDA graph) runs every stage once for all systems: q = A p (one
+// launch over the block-diagonal finest matrix), the per-system dot
+// products (k_seg_dot_part / k_seg_dot_final, deterministic), the step
+// sizes (k_seg_alpha), the updates (k_seg_update), the preconditioner (one
+// cycle of the merged hierarchy: one launch per stage and level, the
+// systems' coarsest solves one launch per level), r·z and the new
+// directions (k_seg_beta, k_seg_dir).  A system stops changing once its
+// relative residual is below tol (its step sizes become 0); the host reads
+// the count of converged systems after every iteration.
+int DevHier::pcg_batch_seg(double* x, const double* b, const CycleOpts& o, double tol, int maxiter, bool mixed,
+                           int* iters, double* relres, int verbose) {
+  if (!batch_) fail("not a batch of systems");
+  const int n = n0_, ns = batch_->nsys;
+  if (mixed) ensure_fp32();
+  if (!sx_) {
+    sx_ = alloc<double>(n);
+    sr_ = alloc<double>(n);
+    sp_ = alloc<double>(n);
+    sq_ = alloc<double>(n);
+    sz_ = alloc<double>(n);
+    seg_buf_ = alloc<double>(7 * (size_t)ns);
+    seg_int_ = alloc<int>(2 * (size_t)ns + 1);
+  }
+  if (mixed && !pr32_) {
+    pr32_ = alloc<float>(n);
+    pz32_ = alloc<float>(n);
+  }
+  int maxlen = 0;
+  for (int q = 0; q < ns; ++q)
+    maxlen = std::max(maxlen, (q + 1 < ns ? batch_->off[0][q + 1] : n) - batch_->off[0][q]);
+  const int PB = std::max(1, std::min(64, (maxlen + kBlock * 4 - 1) / (kBlock * 4)));
+  if (!seg_part_) seg_part_ = alloc<double>((size_t)ns * 64);
+  double* buf = seg_buf_;
+  SegScal sc{buf, buf + ns, buf + 2 * ns, buf + 3 * ns, buf + 4 * ns, buf + 5 * ns, buf + 6 * ns, seg_int_,
+             seg_int_ + ns};
+  int* ndone = seg_int_ + 2 * ns;
+  const DevMat& A = L_[0].A;
+  auto segdot = [&](const double* a, const void* bb, bool bf32, double* out) {
+    counted();
+    if (bf32)
+      k_seg_dot_part<double, float><<<dim3(PB, ns), kBlock, 0, st_>>>(seg_off_, a, (const float*)bb, seg_part_);
+    else
+      k_seg_dot_part<double, double><<<dim3(PB, ns), kBlock, 0, st_>>>(seg_off_, a, (const double*)bb,
+                                                                         seg_part_);
+    counted();
+    k_seg_dot_final<<<(ns + 7) / 8, 256, 0, st_>>>(ns, PB, seg_part_, out);
+    DR_CK(cudaGetLastError());
+  };
+  const void* zptr = nullptr;
+  auto precond = [&]() {
+    if (mixed) zptr = cycle_level<float>(0, pz32_, pr32_, true, o, pz32_);
+    else zptr = cycle_level<double>(0, sz_, sr_, true, o, sz_);
+  };
+  // r = b - A x, |b|^2, |r|^2
+  DR_CK(cudaMemcpyAsync(sx_, x, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+  launch_rows(st_, max_grid_, A, A.v, XPlain<double>{sx_}, EpResidual<double>{b, sr_});
+  segdot(b, b, false, sc.bb);
+  segdot(sr_, sr_, false, sc.rr);
+  std::vector<double> hb(2 * (size_t)ns);
+  DR_CK(cudaMemcpyAsync(hb.data(), sc.rr, 2 * (size_t)ns * sizeof(double), cudaMemcpyDeviceToHost, st_));
+  DR_CK(cudaStreamSynchronize(st_));
+  std::vector<int> hint(2 * (size_t)ns + 1, 0);
+  for (int q = 0; q < ns; ++q) {
+    const double rr = hb[q], bb = hb[ns + q];
+    if (bb == 0.0 || rr < tol * tol * bb) {  // nothing to do (b = 0: x = 0)
+      hint[q] = 1;
+      hint[2 * ns] += 1;
+    }
+  }
+  for (int q = 0; q < ns; ++q)
+    if (hb[ns + q] == 0.0)
+      DR_CK(cudaMemsetAsync(sx_ + batch_->off[0][q], 0,
+                            (size_t)((q + 1 < ns ? batch_->off[0][q + 1] : n) - batch_->off[0][q]) * sizeof(double),
+                            st_));
+  DR_CK(cudaMemcpyAsync(seg_int_, hint.data(), hint.size() * sizeof(int), cudaMemcpyHostToDevice, st_));
+  if (mixed) {
+    counted();
+    k_convert<double, float><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, sr_, pr32_);
+  }
+  precond();
+  segdot(sr_, zptr, mixed, sc.rz);
+  DR_CK(cudaMemsetAsync(sp_, 0, (size_t)n * sizeof(double), st_));
+  DR_CK(cudaMemsetAsync(sc.beta, 0, (size_t)ns * sizeof(double), st_));
+  auto dir = [&]() {
+    counted();
+    if (mixed)
+      k_seg_dir<float><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, seg_id_, (const float*)zptr, sc.beta, sp_);
+    else
+      k_seg_dir<double><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, seg_id_, (const double*)zptr, sc.beta, sp_);
+    DR_CK(cudaGetLastError());
+  };
+  dir();  // p = z
+  const int gs = (ns + 127) / 128;
+  auto iteration = [&]() {
+    launch_rows(st_, max_grid_, A, A.v, XPlain<double>{sp_}, EpStore<double>{sq_});
+    segdot(sp_, sq_, false, sc.pq);
+    counted();
+    k_seg_alpha<<<gs, 128, 0, st_>>>(ns, sc);
+    counted();
+    if (mixed)
+      k_seg_update<float><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, seg_id_, sc.alpha, sp_, sq_, sx_, sr_, pr32_);
+    else
+      k_seg_update<float><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, seg_id_, sc.alpha, sp_, sq_, sx_, sr_,
+                                                                   (float*)nullptr);
+    DR_CK(cudaGetLastError());
+    segdot(sr_, sr_, false, sc.rr);
+    precond();
+    DR_CK(cudaMemcpyAsync(sc.rzold, sc.rz, (size_t)ns * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+    segdot(sr_, zptr, mixed, sc.rz);
+    counted();
+    k_seg_beta<<<gs, 128, 0, st_>>>(ns, sc, tol * tol, ndone);
+    DR_CK(cudaGetLastError());
+    dir();
+  };
+  // one iteration as a CUDA graph (recaptured when the options change)
+  if (seg_graph_ && (seg_graph_mixed_ != mixed || seg_graph_o_.pre != o.pre || seg_graph_o_.post != o.post ||
+                     seg_graph_o_.w != o.w)) {
+    cudaGraphExecDestroy(seg_graph_);
+    seg_graph_ = nullptr;
+  }
+  if (!seg_graph_) {
+    cudaGraph_t g;
+    const long long c0 = g_launches.load();
+    DR_CK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+    iteration();
+    DR_CK(cudaStreamEndCapture(st_, &g));
+    const long long per_iter = g_launches.load() - c0;
+    g_launches.fetch_sub(per_iter);
+    DR_CK(cudaGraphInstantiate(&seg_graph_, g, 0));
+    DR_CK(cudaGraphDestroy(g));
+    seg_graph_mixed_ = mixed;
+    seg_graph_o_ = o;
+    seg_launches_ = per_iter;
+  }
+  int* hdone = reinterpret_cast<int*>(hscal_ + SC_N - 1);
+  int it = 0;
+  int done = hint[2 * ns];
+  while (done < ns && it < maxiter) {
+    DR_CK(cudaGraphLaunch(seg_graph_, st_));
+    g_launches.fetch_add(seg_launches_);
+    ++it;
+    DR_CK(cudaMemcpyAsync(hdone, ndone, sizeof(int), cudaMemcpyDeviceToHost, st_));
+    DR_CK(cudaStreamSynchronize(st_));
+    done = *hdone;
+    if (verbose >= 2) std::printf("  batch PCG iter %4d: %d of %d systems converged\n", it, done, ns);
+  }
+  // true residuals
+  launch_rows(st_, max_grid_, A, A.v, XPlain<double>{sx_}, EpResidual<double>{b, sr_});
+  segdot(sr_, sr_, false, sc.rr);
+  DR_CK(cudaMemcpyAsync(x, sx_, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+  std::vector<int> hit(ns);
+  DR_CK(cudaMemcpyAsync(hb.data(), sc.rr, 2 * (size_t)ns * sizeof(double), cudaMemcpyDeviceToHost, st_));
+  DR_CK(cudaMemcpyAsync(hit.data(), sc.iters, (size_t)ns * sizeof(int), cudaMemcpyDeviceToHost, st_));
+  DR_CK(cudaStreamSynchronize(st_));
+  check_kernel_flag(st_);
+  int maxit = 0;
+  for (int q = 0; q < ns; ++q) {
+    if (iters) iters[q] = hit[q];
+    if (relres) relres[q] = hb[ns + q] > 0.0 ? std::sqrt(hb[q] / hb[ns + q]) : 0.0;
+    maxit = std::max(maxit, hit[q]);
+  }
+  if (verbose >= 1)
+    std::printf("batch AMG-PCG (%s cycle): %d systems, %d of them converged, %d iterations at most\n",
+                mixed ? "FP32" : "FP64", ns, done, maxit);
+  return maxit;
 }
 
 // dL/da_ij = -lambda_i x_j over the finest matrix's nonzeros (CSR order).

@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <map>
+#include <memory>
 #include <set>
 #include <string>
 #include <utility>
@@ -125,6 +126,7 @@ struct SpgemmList {
 
 struct DevLevel {
   DevMat A, P, R;            // R = Pᵀ stored as the transpose map with values
+  int nv = 0;                // length of the level's vectors (A.n, more in a batch)
   SmootherKind smoother = SmootherKind::Jacobi;
   double omega = 2.0 / 3.0;
   double* invd = nullptr;
@@ -170,6 +172,30 @@ struct CycleOpts {
   bool w = false;
 };
 
+// Independent systems merged level by level (a batch).  Merged level l
+// holds, in system order, the rows of the systems that still smooth there
+// (the block-diagonal A, P and Pᵀ act on these), then the rows of the
+// systems whose coarsest level it is (solved by their own dense LU).
+struct BatchLayout {
+  int nsys = 0;
+  std::vector<int> depth;             // AMG levels of each system
+  std::vector<int> nsmooth, ntotal;   // per merged level 0..Lmax
+  std::vector<std::vector<int>> off;  // off[l][s]: first row of system s at level l (-1: absent)
+  struct Coarse {
+    std::vector<int> off, nb, poff;   // per system ending at the level: rows, size, pivot offset
+    std::vector<long long> luoff;     // offset of its factors
+    int maxn = 0;
+  };
+  std::vector<Coarse> coarse;         // per merged level
+  std::vector<double> lu;             // all coarsest factors (column-major each)
+  std::vector<int> piv;               // all pivots (0-based)
+};
+
+// Merge the hierarchies of independent systems into one (CPU); every
+// level of every system must use a Jacobi-type smoother, and systems that
+// share a level the same smoother and weight.
+HostHierarchy merge_batch(const std::vector<const HostHierarchy*>& hs, BatchLayout& lay);
+
 // Launch shape of a block (multi-right-hand-side) product: threads per row
 // (32 / tpr rows per warp) and resident blocks per SM; 0 takes the default.
 struct BlockShape {
@@ -185,7 +211,7 @@ struct KernelClock {
 
 class DevHier {
  public:
-  DevHier(const HostHierarchy& H, int device);
+  DevHier(const HostHierarchy& H, int device, const BatchLayout* batch = nullptr);
   ~DevHier();
   DevHier(const DevHier&) = delete;
   DevHier& operator=(const DevHier&) = delete;
@@ -211,6 +237,16 @@ class DevHier {
   // transposed hierarchy (adjoint solves); Jacobi-type smoothers.
   int bicgstab(double* x, const double* b, const CycleOpts& o, double tol, int maxiter, bool transpose,
                double* relres, int verbose, bool mixed = false);
+  // Batch (a hierarchy built from merge_batch): conjugate gradients on every
+  // system at once, each with its own step sizes and convergence test, one
+  // launch per cycle stage for all systems; one iteration is captured in a
+  // CUDA graph.  x, b: all systems' vectors, concatenated.  iters, relres:
+  // per system.  Returns the largest iteration count.
+  int pcg_batch_seg(double* x, const double* b, const CycleOpts& o, double tol, int maxiter, bool mixed,
+                    int* iters, double* relres, int verbose);
+  bool is_batch() const { return batch_ != nullptr; }
+  int batch_systems() const { return batch_ ? batch_->nsys : 0; }
+  const BatchLayout* batch_layout() const { return batch_.get(); }
   // Flexible GMRES(restart), right-preconditioned by one AMG cycle per
   // iteration (FP64, or with `mixed` the FP32 cycle), FP64 Arnoldi
   // (classical Gram-Schmidt, twice), until ||b - A x|| / ||b|| < tol.
@@ -327,6 +363,28 @@ class DevHier {
             double* out);
   void precond64(const double* r, double* out, const CycleOpts& o);
   void precond32(const double* r, double* out, const CycleOpts& o);  // FP32 cycle, FP64 in and out
+  // batch: layout, its device arrays per merged level (coarse blocks), the
+  // finest level's segment offsets and row -> segment map
+  std::unique_ptr<BatchLayout> batch_;
+  struct BatchDev {
+    int nblk = 0, maxn = 0;
+    int *off = nullptr, *nb = nullptr, *poff = nullptr;
+    long long* luoff = nullptr;
+  };
+  std::vector<BatchDev> batch_dev_;
+  double* blu_ = nullptr;
+  int* bpiv_ = nullptr;
+  int *seg_off_ = nullptr, *seg_id_ = nullptr;
+  double* seg_buf_ = nullptr;    // per segment: rz, rzold, pq, rr, bb, alpha, beta
+  double* seg_part_ = nullptr;   // dot partials
+  int* seg_int_ = nullptr;       // per segment: done, iters; then the count of converged segments
+  double *sx_ = nullptr, *sr_ = nullptr, *sp_ = nullptr, *sq_ = nullptr, *sz_ = nullptr;
+  cudaGraphExec_t seg_graph_ = nullptr;
+  long long seg_launches_ = 0;   // kernels in one captured batch iteration
+  bool seg_graph_mixed_ = false;
+  CycleOpts seg_graph_o_;
+  template <typename T>
+  void batch_coarse(int l, const T* b, T* x);
   void alloc_transpose_fp32();
   // FGMRES workspace: (restart + 1) basis vectors, restart preconditioned
   // vectors, one work vector, reduction partials and tickets per column.

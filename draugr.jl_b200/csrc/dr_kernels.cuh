@@ -1712,5 +1712,142 @@ k_spgemm_warp(int nrows, const int* __restrict__ out_rp, const int* __restrict__
   }
 }
 
+// ------------------------------------------------------------ batched systems
+// Many independent systems merged level by level into block-diagonal
+// matrices (a "batch"): the vectors of a merged level hold the rows of the
+// systems still smoothing there, then the rows of the systems whose
+// coarsest level it is.  Segment s of the finest level is system s.
+
+// Coarsest solves of the systems that end at one merged level: block k
+// solves its system's dense LU (column-major factors at lu + luoff[k],
+// 0-based pivots at piv + poff[k]) for rows off[k] .. off[k] + nb[k] - 1 of
+// b into x, in the operation order of k_lu_solve (so each system's coarse
+// solve gives what its own hierarchy's gives).
+template <typename T>
+__global__ void k_lu_solve_batch(const int* __restrict__ off, const int* __restrict__ nb,
+                                 const long long* __restrict__ luoff, const int* __restrict__ poff,
+                                 const double* __restrict__ lu_all, const int* __restrict__ piv_all,
+                                 const T* __restrict__ bin, T* __restrict__ xout) {
+  extern __shared__ double shb[];
+  const int k = blockIdx.x;
+  const int n = nb[k];
+  const double* __restrict__ a = lu_all + luoff[k];
+  const int* __restrict__ piv = piv_all + poff[k];
+  const T* __restrict__ b = bin + off[k];
+  T* __restrict__ x = xout + off[k];
+  double* y = shb;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = (double)b[i];
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int j = 0; j < n; ++j) {
+      const int p = piv[j];
+      if (p != j) {
+        const double t = y[j];
+        y[j] = y[p];
+        y[p] = t;
+      }
+    }
+  __syncthreads();
+  for (int j = 0; j < n; ++j) {
+    const double yj = y[j];
+    if (yj != 0.0)
+      for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x)
+        y[i] = __dsub_rn(y[i], __dmul_rn(yj, a[(size_t)j * n + i]));
+    __syncthreads();
+  }
+  for (int j = n - 1; j >= 0; --j) {
+    if (threadIdx.x == 0 && y[j] != 0.0) y[j] = __ddiv_rn(y[j], a[(size_t)j * n + j]);
+    __syncthreads();
+    const double yj = y[j];
+    if (yj != 0.0)
+      for (int i = threadIdx.x; i < j; i += blockDim.x)
+        y[i] = __dsub_rn(y[i], __dmul_rn(yj, a[(size_t)j * n + i]));
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = (T)y[i];
+}
+
+// Per-segment dot products, deterministic: blockIdx.y = segment, blocks
+// along x stride its rows; partials[s * gridDim.x + bx]; then
+// k_seg_dot_final sums each segment's partials in block order (one warp per
+// segment) into out[s].
+template <typename TA, typename TB>
+__global__ void __launch_bounds__(kBlock)
+k_seg_dot_part(const int* __restrict__ seg_off, const TA* __restrict__ a, const TB* __restrict__ b,
+               double* __restrict__ partials) {
+  const int s = blockIdx.y;
+  const int lo = seg_off[s], hi = seg_off[s + 1];
+  double v = 0.0;
+  for (int i = lo + blockIdx.x * blockDim.x + threadIdx.x; i < hi; i += gridDim.x * blockDim.x)
+    v = fma((double)a[i], (double)b[i], v);
+  v = block_sum(v);
+  if (threadIdx.x == 0) partials[(size_t)s * gridDim.x + blockIdx.x] = v;
+}
+
+__global__ void k_seg_dot_final(int nseg, int nparts, const double* __restrict__ partials,
+                                double* __restrict__ out) {
+  const int s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (s >= nseg) return;
+  double v = 0.0;
+  for (int k = lane; k < nparts; k += 32) v += partials[(size_t)s * nparts + k];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if (lane == 0) out[s] = v;
+}
+
+// Segmented PCG scalars (one thread per segment), from the dot products
+// in `dots` (per segment: [rz, rz_old, pq, rr, bb]) and the convergence
+// flags: alpha (0 once converged), beta, and, at the update step, the
+// convergence test rr < tol^2 bb with the iteration count.
+struct SegScal {
+  double* rz;
+  double* rzold;
+  double* pq;
+  double* rr;
+  double* bb;
+  double* alpha;
+  double* beta;
+  int* done;   // 1 once the segment has converged
+  int* iters;  // iterations of each segment
+};
+__global__ void k_seg_alpha(int nseg, SegScal sc) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nseg) return;
+  sc.alpha[s] = (sc.done[s] || sc.pq[s] == 0.0) ? 0.0 : sc.rz[s] / sc.pq[s];
+}
+__global__ void k_seg_beta(int nseg, SegScal sc, double tol2, int* ndone) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nseg) return;
+  if (!sc.done[s]) {
+    sc.iters[s] += 1;
+    if (sc.rr[s] < tol2 * sc.bb[s]) {
+      sc.done[s] = 1;
+      atomicAdd(ndone, 1);
+    }
+  }
+  sc.beta[s] = (sc.done[s] || sc.rzold[s] == 0.0) ? 0.0 : sc.rz[s] / sc.rzold[s];
+}
+
+// p = z + beta_s p (z of the cycle's type), per row's segment.
+template <typename TZ>
+__global__ void k_seg_dir(int n, const int* __restrict__ seg, const TZ* __restrict__ z,
+                          const double* __restrict__ beta, double* __restrict__ p) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    p[i] = (double)z[i] + beta[seg[i]] * p[i];
+}
+// x += alpha_s p; r -= alpha_s q; optional FP32 copy of r.
+template <typename TR32>
+__global__ void k_seg_update(int n, const int* __restrict__ seg, const double* __restrict__ alpha,
+                             const double* __restrict__ p, const double* __restrict__ q,
+                             double* __restrict__ x, double* __restrict__ r, TR32* __restrict__ r32) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double a = alpha[seg[i]];
+    x[i] = fma(a, p[i], x[i]);
+    const double ri = fma(-a, q[i], r[i]);
+    r[i] = ri;
+    if (r32) r32[i] = (TR32)ri;
+  }
+}
+
 }  // namespace kern
 }  // namespace dr

@@ -47,6 +47,9 @@ SIGNATURES = {
     "draugr_b200_fgmres_device": (i32, [i32, i32, P, P, i32, f64, i32, i32, i32, P]),
     "draugr_b200_refine": (i32, [i32, i32, P, P, i32, f64, i32, f64, i32, i32, i32, P, P]),
     "draugr_b200_refine_device": (i32, [i32, i32, P, P, i32, f64, i32, f64, i32, i32, i32, P, P]),
+    "draugr_b200_batch_setup": (i32, [i32, P]),
+    "draugr_b200_batch_offsets": (i32, [i32, P]),
+    "draugr_b200_batch_pcg_device": (i32, [i32, i32, P, P, i32, f64, i32, i32, P, P]),
     "draugr_b200_bicgstab": (i32, [i32, i32, P, P, i32, f64, i32, i32, i32, P]),
     "draugr_b200_bicgstab_device": (i32, [i32, i32, P, P, i32, f64, i32, i32, i32, P]),
     "draugr_b200_nz_gradient_device": (i32, [i32, i32, P, P, P]),

@@ -621,6 +621,48 @@ def pcg_batch(hierarchies, xs, bs, config: AMGConfig | None = None, tol: float =
         return list(ex.map(one, range(len(hierarchies))))
 
 
+class BatchHierarchy(Hierarchy):
+    """Independent systems merged level by level (draugr_b200_batch_setup);
+    `offsets[s]:offsets[s + 1]` are system s's rows in the batch's vectors."""
+
+    def __init__(self, handle: int, offsets: np.ndarray, config: AMGConfig | None):
+        super().__init__(handle, int(offsets[-1]), config)
+        self.offsets = offsets
+
+    @property
+    def nsystems(self) -> int:
+        return len(self.offsets) - 1
+
+
+def batch_setup(hierarchies, config: AMGConfig | None = None) -> BatchHierarchy:
+    """Merge the hierarchies of independent systems into one batch (one
+    launch per cycle stage for all of them).  The hierarchies stay usable."""
+    lib = _lib.load()
+    hs = np.ascontiguousarray([h.handle for h in hierarchies], np.int32)
+    b = _lib.check(lib.draugr_b200_batch_setup(len(hs), _ptr(hs)), "batch_setup")
+    ns = _lib.check(lib.draugr_b200_batch_offsets(b, None), "batch_offsets")
+    off = np.zeros(ns + 1, np.int64)
+    _lib.check(lib.draugr_b200_batch_offsets(b, _ptr(off)), "batch_offsets")
+    return BatchHierarchy(b, off, config if config is not None else hierarchies[0].config)
+
+
+def pcg_batched(x, b, batch: BatchHierarchy, config: AMGConfig | None = None, tol: float = 1e-8,
+                maxiter: int = 500, precision: str = "mixed"):
+    """AMG-PCG on every system of a batch at once.  x, b: CUDA float64
+    tensors holding all systems' vectors (batch.offsets); x holds the
+    initial guesses.  Returns (x, iterations per system, relative residuals
+    per system)."""
+    config = config if config is not None else (batch.config or AMGConfig())
+    prec = {"fp64": 0, "mixed": 1}[precision]
+    ns = batch.nsystems
+    its = np.zeros(ns, np.int32)
+    rel = np.zeros(ns)
+    _lib.check(_lib.load().draugr_b200_batch_pcg_device(batch.handle, x.numel(), x.data_ptr(), b.data_ptr(),
+                                                        config_handle(config), tol, maxiter, prec, _ptr(its),
+                                                        _ptr(rel)), "pcg_batched")
+    return x, its, rel
+
+
 class DraugrPreconditioner:
     """One AMG cycle from a zero guess as a preconditioner, the role of
     Draugr.jl's DraugrPreconditioner (src/preconditioner.jl:12-102).

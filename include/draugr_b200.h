@@ -171,6 +171,30 @@ int32_t draugr_b200_refine_device(int32_t handle, int32_t n, double *x_dev, cons
                                   int32_t inner_maxiter, int32_t inner_method, int32_t precision,
                                   double *relres, int32_t *inner_iters);
 
+/* Many independent systems solved as one batch.  batch_setup merges the
+ * hierarchies of `nsys` systems (handles from draugr_amg_setup, each with at
+ * least one AMG level, Jacobi, l1-Jacobi or SPAI(0) smoothing on every
+ * level, the same smoother and weight where they share a level) level by
+ * level into block-diagonal matrices, on the current device, and returns a
+ * new hierarchy handle (free it with draugr_amg_free; the systems' own
+ * handles stay valid).  The batch's vectors hold the systems' vectors one
+ * after the other; batch_offsets writes the nsys + 1 row offsets (may be
+ * NULL) and returns nsys.  batch_pcg_device runs conjugate gradients on
+ * every system at once with the AMG V-cycle of the merged hierarchy as
+ * preconditioner (precision 0: FP64, 1: FP32 cycle in the FP64 iteration):
+ * each cycle stage, dot product and update is one launch for all systems,
+ * every system keeps its own step sizes and stops changing once
+ * ||b_s - A_s x_s|| < tol ||b_s||, and one iteration runs as a CUDA graph.
+ * iters, relres (nsys entries each, may be NULL): per-system iterations and
+ * final FP64 relative residuals.  Returns the largest iteration count, or
+ * -1.  The reference solves one system per call; a caller loops over them
+ * (src/cycle.jl:110-160). */
+int32_t draugr_b200_batch_setup(int32_t nsys, const int32_t *handles);
+int32_t draugr_b200_batch_offsets(int32_t handle, int64_t *offsets);
+int32_t draugr_b200_batch_pcg_device(int32_t handle, int32_t n, double *x_dev, const double *b_dev,
+                                     int32_t config_handle, double tol, int32_t maxiter, int32_t precision,
+                                     int32_t *iters, double *relres);
+
 /* BiCGStab preconditioned (on the right) by one AMG cycle per
  * application, until ||b - M x|| / ||b|| < tol, for nonsymmetric systems.
  * transpose 0: M = A.  transpose 1: M = A^T, the adjoint system of a
