@@ -316,6 +316,32 @@ def run_ours(args, world, rank, local):
             raise SystemExit(f"{mode} solve through the C ABI did not reach {TOL}: {rr}")
         return max_over_ranks(float(np.mean(ts)), world)
 
+    # the other Krylov forms on the same system: FGMRES(30) with the FP32
+    # cycle, and iterative refinement (FP64 residual, mixed PCG to 1e-4 inside)
+    def other(fn, key):
+        for _ in range(2):
+            xd.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            r = fn()
+            e1.record(stream)
+            e1.synchronize()
+        x = xd.cpu().numpy()
+        d = {"time_s": e0.elapsed_time(e1) / 1e3, "relres_fp64_verified": float(np.linalg.norm(b - A @ x) / bnorm)}
+        d.update(key(r))
+        return d
+
+    krylov = {
+        "fgmres_mixed": other(lambda: draugr.fgmres(xd, bd, h, cfg, tol=TOL, maxiter=MAXITER, restart=30,
+                                                    precision="mixed"),
+                              lambda r: {"iterations": int(r[1])}),
+        "refine_mixed_pcg": other(lambda: draugr.refine(xd, bd, h, cfg, tol=TOL, inner_tol=1e-4,
+                                                        inner="pcg", precision="mixed"),
+                                  lambda r: {"steps": int(r[1]), "inner_iterations": int(r[2])}),
+    }
+
     e2e = {"value": e2e_time("fp64"), "unit": "s",
            "h2d_bytes_per_step": 2 * n * 8, "d2h_bytes_per_step": n * 8,
            "path": "draugr_b200_pcg, precision 0 (C ABI, pinned host x and b, FP64 cycle)",
@@ -387,6 +413,7 @@ def run_ours(args, world, rank, local):
            "setup_s_cpu": round(setup_s, 3),
            "fp64": res["fp64"], "mixed": res["mixed"],
            "speedup_mixed_vs_fp64": res["fp64"]["time_s"] / res["mixed"]["time_s"],
+           "krylov": krylov,
            "e2e": e2e, "roofline": roofline, "vcycle": vcycle, "clocks": clocks,
            "loaded_repo_libraries": repo_libraries(),
            "gpu_launches": int(launches)}

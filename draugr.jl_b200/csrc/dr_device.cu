@@ -213,6 +213,7 @@ void launch_rows_impl(cudaStream_t st, int max_grid, const RowForm& f, int n, in
   if (f.flat) DR_LAUNCH(true, 1, true, 256, 8, uint16_t);
   else if (f.G == 1 && f.nt == 128 && sizeof(TA) == 4) DR_LAUNCH(false, 1, true, 128, 32, uint16_t);
   else if (f.G == 1 && f.nt == 128) DR_LAUNCH(false, 1, true, 128, 32, int);
+  else if (f.G == 1 && f.nt == 512) DR_LAUNCH(false, 1, true, 512, 4, int);
   else if (f.G == 1) DR_LAUNCH(false, 1, true, 256, 8, int);
   else if (f.G == 8) DR_LAUNCH(false, 8, false, 256, 12, uint16_t);
   else if (f.G == 16) DR_LAUNCH(false, 16, false, 256, 12, uint16_t);

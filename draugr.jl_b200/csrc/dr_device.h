@@ -32,9 +32,11 @@ constexpr int kRowTileCap = 2000;
 //   flat    rows of very uneven length averaging at most 32 entries (a long
 //           row among short ones): products formed flat over each tile,
 //           then one thread per row sums them in column order;
-//   G = 1   one lane per row, rows summed in column order: batches of 8
-//           gathers with 256-thread blocks up to 12 entries per row on
-//           average, batches of 32 with 128-thread blocks up to 32;
+//   G = 1   one lane per row, rows summed in column order: batches of 4
+//           gathers with 512-thread blocks up to 5 entries per row on
+//           average (interpolation rows: 512 rows fill a tile), batches of
+//           8 with 256-thread blocks up to 12, batches of 32 with
+//           128-thread blocks up to 32;
 //   G > 1   longer rows, summed by G lanes and a fixed shuffle tree: 8 or
 //           16 lanes gathering 12 entries each at once (about 27 or 13
 //           rows fill a tile), or 32 lanes with 4 each when a few rows are
@@ -60,6 +62,9 @@ inline RowForm row_form(const std::vector<int>& rp) {
     if (avg > 12.0) {
       f.nt = 128;
       f.batch = 32;
+    } else if (avg <= 5.0) {
+      f.nt = 512;  // very short rows (interpolation): 512 rows fill a tile
+      f.batch = 4;
     }
   } else {
     f.ordered = false;

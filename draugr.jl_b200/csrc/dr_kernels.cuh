@@ -462,10 +462,10 @@ __device__ __forceinline__ void bind_epilogue(EpCheby<T>& e) { e.bind(); }
 
 // Resident blocks per SM the register allocation plans for: planning for 4
 // lets 128-thread FP64 blocks keep a whole batch of 32 gathers in registers
-// without spilling.
+// without spilling; 2 blocks of 512 threads (short rows, batches of 4).
 template <int NT, typename TA>
 constexpr int tile_min_blocks() {
-  return NT == 128 ? (sizeof(TA) == 8 ? 4 : 5) : 1;
+  return NT == 128 ? (sizeof(TA) == 8 ? 4 : 5) : NT == 512 ? 2 : 1;
 }
 
 // TC: the staged column type — int (the columns themselves) or uint16_t

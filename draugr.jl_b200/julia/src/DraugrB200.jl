@@ -21,6 +21,7 @@ export AMGConfig, hypre_default_config, AMGHierarchy
 export amg_setup, amg_solve!, amg_cycle!, amg_resetup!, amg_pcg!
 export amg_bicgstab!, amg_fgmres!, amg_refine!, amg_pcg_block!, nz_gradient!
 export amg_solve_diff, amg_solve_adjoint, amg_resetup_values!
+export amg_batch_setup, amg_pcg_batched!
 export DraugrB200Preconditioner
 
 const libdraugr = get(ENV, "DRAUGR_B200_LIB", joinpath(@__DIR__, "..", "..", "libdraugr_b200.so"))
@@ -473,6 +474,48 @@ function amg_solve_adjoint(x̄::AbstractVector{Float64}, x::AbstractVector{Float
     grad = similar(x, Int(info[2]))
     nz_gradient!(grad, h, x, λ)
     return grad, λ
+end
+
+"""
+    amg_batch_setup(hs::Vector{AMGHierarchy}) -> (batch::AMGHierarchy, offsets::Vector{Int})
+
+Merge independent systems' hierarchies level by level into one batch on the
+current device; system s occupies rows offsets[s]+1 : offsets[s+1] of the
+batch's vectors.  The systems' own hierarchies stay usable.
+"""
+function amg_batch_setup(hs::Vector{AMGHierarchy})
+    handles = Int32[h.handle for h in hs]
+    b = check(ccall((:draugr_b200_batch_setup, libdraugr), Int32, (Int32, Ptr{Int32}),
+                    length(handles), handles), "amg_batch_setup")
+    offs = zeros(Int64, length(hs) + 1)
+    check(ccall((:draugr_b200_batch_offsets, libdraugr), Int32, (Int32, Ptr{Int64}), b, offs),
+          "amg_batch_setup")
+    return AMGHierarchy(b, Int(offs[end])), Int.(offs)
+end
+
+"""
+    amg_pcg_batched!(x, b, batch, config; tol=1e-8, maxiter=500, precision=:mixed) -> (x, iters, relres)
+
+AMG-PCG on every system of a batch at once (device vectors holding all
+systems' rows): one launch per cycle stage for all systems, per-system step
+sizes and convergence.  Returns per-system iterations and relative
+residuals.
+"""
+function amg_pcg_batched!(x::AbstractVector{Float64}, b::AbstractVector{Float64}, batch::AMGHierarchy,
+                          config::AMGConfig=AMGConfig(); tol::Real=1e-8, maxiter::Int=500,
+                          precision::Symbol=:mixed)
+    ns = check(ccall((:draugr_b200_batch_offsets, libdraugr), Int32, (Int32, Ptr{Int64}), batch.handle,
+                     C_NULL), "amg_pcg_batched!")
+    its = zeros(Int32, ns)
+    rel = zeros(Float64, ns)
+    prec = precision === :mixed ? Int32(1) : Int32(0)
+    rc = GC.@preserve x b ccall((:draugr_b200_batch_pcg_device, libdraugr), Int32,
+                                (Int32, Int32, Ptr{Float64}, Ptr{Float64}, Int32, Float64, Int32, Int32,
+                                 Ptr{Int32}, Ptr{Float64}),
+                                batch.handle, length(x), rawptr(x), rawptr(b), config.handle, tol, maxiter,
+                                prec, its, rel)
+    check(rc, "amg_pcg_batched!")
+    return x, Int.(its), rel
 end
 
 """
