@@ -468,6 +468,14 @@ int32_t draugr_b200_resetup_values_device(int32_t handle, int64_t nnz, const dou
   });
 }
 
+int32_t draugr_b200_set_resetup_precision(int32_t handle, int32_t fp64_levels) {
+  return guarded("draugr_b200_set_resetup_precision", [&]() -> int32_t {
+    auto H = get_hier_only(handle);
+    device_of(*H).set_resetup_fp64_levels(fp64_levels);
+    return 0;
+  });
+}
+
 int32_t draugr_b200_galerkin_host(int32_t handle, int32_t lvl, int64_t nnz_in, const double* a_vals,
                                   int64_t nnz_out, double* ac_vals) {
   return guarded("draugr_b200_galerkin_host", [&]() -> int32_t {

@@ -1878,12 +1878,14 @@ bool DevHier::build_spgemm_list(const DevMat& O, const DevMat& S, const DevMat& 
   return ok;
 }
 
-void DevHier::spgemm(DevMat& O, const DevMat& S, const DevMat& B, SpgemmList* list) {
+template <typename T>
+void DevHier::spgemm(DevMat& O, const DevMat& S, const DevMat& B, T* ov, const T* sv, const T* bv,
+                     SpgemmList* list) {
   if (list && !list->tried) build_spgemm_list(O, S, B, *list);
   if (list && list->off) {
     counted();
-    k_spgemm_apply<<<grid1d(O.nnz, max_grid_), kBlock, 0, st_>>>(O.nnz, list->off, list->ls, list->lb, S.v, B.v,
-                                                                 O.v);
+    k_spgemm_apply<T><<<grid1d(O.nnz, max_grid_), kBlock, 0, st_>>>(O.nnz, list->off, list->ls, list->lb, sv, bv,
+                                                                    ov);
     DR_CK(cudaGetLastError());
     return;
   }
@@ -1891,13 +1893,17 @@ void DevHier::spgemm(DevMat& O, const DevMat& S, const DevMat& B, SpgemmList* li
   counted();
   const int grid = std::max(1, std::min((O.n + W - 1) / W, max_grid_));
 #define DR_SPGEMM(CAP)                                                                      \
-  k_spgemm_warp<CAP, W><<<grid, W * 32, spgemm_smem_bytes<CAP, W>(), st_>>>(              \
-      O.n, O.rp, O.ci, O.v, S.rp, S.ci, S.v, B.rp, B.ci, B.v)
+  k_spgemm_warp<T, CAP, W><<<grid, W * 32, spgemm_smem_bytes<T, CAP, W>(), st_>>>(        \
+      O.n, O.rp, O.ci, ov, S.rp, S.ci, sv, B.rp, B.ci, bv)
   if (O.maxlen <= 128) DR_SPGEMM(128);
   else if (O.maxlen <= 256) DR_SPGEMM(256);
   else DR_SPGEMM(384);
 #undef DR_SPGEMM
   DR_CK(cudaGetLastError());
+}
+
+void DevHier::set_resetup_fp64_levels(int n) {
+  resetup_fp64_ = n;
 }
 
 void DevHier::resetup_values(const double* v_dev) {
@@ -1975,11 +1981,30 @@ void DevHier::resetup_values(const double* v_dev) {
     }
   };
   if (nl > 0) upd_invd(L_[0]);
+  // Galerkin products 0 .. f64-1 in FP64, the rest in FP32 (on the FP32
+  // copies of A, P and Pᵀ; the FP64 copy of each FP32-computed level is its
+  // FP32 values widened, so both copies agree)
+  const int f64 = resetup_fp64_ < 0 ? nl : std::min(resetup_fp64_, nl);
+  if (f64 < nl) ensure_fp32();
   for (int l = 0; l < nl; ++l) {
     DevLevel& d = L_[l];
     DevMat& next = (l + 1 < nl) ? L_[l + 1].A : C_;
-    spgemm(d.AP, d.A, d.P, &d.ap_list);
-    spgemm(next, d.R, d.AP, &d.rap_list);
+    if (l < f64) {
+      spgemm<double>(d.AP, d.A, d.P, d.AP.v, d.A.v, d.P.v, &d.ap_list);
+      spgemm<double>(next, d.R, d.AP, next.v, d.R.v, d.AP.v, &d.rap_list);
+    } else {
+      if (l == f64) {  // this level's values came from FP64 (a product above, or the input)
+        counted();
+        k_convert<double, float><<<grid1d(d.A.nnz, max_grid_), kBlock, 0, st_>>>(d.A.nnz, d.A.v, d.A.v32);
+      }
+      if (!d.AP.v32) d.AP.v32 = alloc<float>(d.AP.nnz + 4);
+      if (!next.v32) next.v32 = alloc<float>(next.nnz + 4);
+      spgemm<float>(d.AP, d.A, d.P, d.AP.v32, d.A.v32, d.P.v32, &d.ap_list);
+      spgemm<float>(next, d.R, d.AP, next.v32, d.R.v32, d.AP.v32, &d.rap_list);
+      counted();
+      k_convert<float, double><<<grid1d(next.nnz, max_grid_), kBlock, 0, st_>>>(next.nnz, next.v32, next.v);
+      DR_CK(cudaGetLastError());
+    }
     if (l + 1 < nl) upd_invd(L_[l + 1]);
   }
   // coarsest dense matrix and its LU

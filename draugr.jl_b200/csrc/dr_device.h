@@ -232,6 +232,11 @@ class DevHier {
   // (synchronises the stream; clears the flag).
   void check_errors();
 
+  // Galerkin products of a partial resetup computed in FP64 from the top:
+  // n of them (the rest in FP32 on the FP32 copies); negative: all FP64.
+  void set_resetup_fp64_levels(int n);
+  int resetup_fp64_levels() const { return resetup_fp64_; }
+
   // Solve phase (device pointers, length n0).
   void cycle(double* x, const double* b, const CycleOpts& o);
   int solve(double* x, const double* b, const CycleOpts& o, double tol, int maxiter, int verbose,
@@ -399,11 +404,14 @@ class DevHier {
   double *ir_r_ = nullptr, *ir_d_ = nullptr, *ir_x_ = nullptr;  // iterative refinement: residual, correction, iterate
   void upload_csr(DevMat& M, int n, int m, const std::vector<int>& rp, const std::vector<int>& ci,
                   const std::vector<double>* v);
-  void spgemm(DevMat& O, const DevMat& S, const DevMat& B, SpgemmList* list = nullptr);
+  template <typename T>
+  void spgemm(DevMat& O, const DevMat& S, const DevMat& B, T* ov, const T* sv, const T* bv,
+              SpgemmList* list = nullptr);
   bool build_spgemm_list(const DevMat& O, const DevMat& S, const DevMat& B, SpgemmList& list);
   // Levels tail_ .. nlevels-1 run as one single-block kernel (k_coarse_tail);
   // tail_ = nlevels() when no level qualifies.
   int tail_ = 0;
+  int resetup_fp64_ = -1;  // see set_resetup_fp64_levels
   void* tail64_ = nullptr;   // device TailLevel<double>[nlevels - tail_]
   void* tail32_ = nullptr;   // device TailLevel<float>[...] once FP32 buffers exist
   size_t tail_bytes_[2] = {0, 0};        // shared memory of the tail kernel (FP64, FP32)

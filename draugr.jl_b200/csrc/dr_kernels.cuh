@@ -1451,13 +1451,14 @@ k_spgemm_sym(int nrows, const int* __restrict__ out_rp, const int* __restrict__ 
 // O's values from the product lists (see k_spgemm_sym): one thread per
 // output entry, products multiplied and added in list order, separately
 // rounded.
+template <typename T>
 __global__ void k_spgemm_apply(long long nout, const long long* __restrict__ off, const int* __restrict__ ls,
-                               const int* __restrict__ lb, const double* __restrict__ s_v,
-                               const double* __restrict__ b_v, double* __restrict__ out_v) {
+                               const int* __restrict__ lb, const T* __restrict__ s_v,
+                               const T* __restrict__ b_v, T* __restrict__ out_v) {
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nout;
        e += (long long)gridDim.x * blockDim.x) {
-    double a = 0.0;
-    for (long long p = off[e]; p < off[e + 1]; ++p) a = __dadd_rn(a, __dmul_rn(s_v[ls[p]], b_v[lb[p]]));
+    T a = T(0);
+    for (long long p = off[e]; p < off[e + 1]; ++p) a = add_rn(a, mul_rn(s_v[ls[p]], b_v[lb[p]]));
     out_v[e] = a;
   }
 }
@@ -1612,21 +1613,21 @@ __global__ void k_spai0_diag(int n, const int* __restrict__ rp, const int* __res
 //
 // WPB warps per block; the per-warp row patterns and sums (CAP entries each)
 // live in dynamic shared memory: spgemm_smem_bytes<CAP, WPB>().
-template <int CAP, int WPB>
+template <typename T, int CAP, int WPB>
 constexpr size_t spgemm_smem_bytes() {
-  return (size_t)WPB * CAP * (sizeof(double) + sizeof(int)) + (size_t)WPB * 32 * sizeof(double);
+  return (size_t)WPB * CAP * (sizeof(T) + sizeof(int)) + (size_t)WPB * 32 * sizeof(T);
 }
 
-template <int CAP, int WPB>
+template <typename T, int CAP, int WPB>
 __global__ void __launch_bounds__(WPB * 32)
 k_spgemm_warp(int nrows, const int* __restrict__ out_rp, const int* __restrict__ out_ci,
-              double* __restrict__ out_v, const int* __restrict__ s_rp, const int* __restrict__ s_ci,
-              const double* __restrict__ s_v, const int* __restrict__ b_rp,
-              const int* __restrict__ b_ci, const double* __restrict__ b_v) {
+              T* __restrict__ out_v, const int* __restrict__ s_rp, const int* __restrict__ s_ci,
+              const T* __restrict__ s_v, const int* __restrict__ b_rp,
+              const int* __restrict__ b_ci, const T* __restrict__ b_v) {
   extern __shared__ __align__(16) unsigned char gsm[];
-  double (*sacc)[CAP] = reinterpret_cast<double (*)[CAP]>(gsm);
-  double (*sprod)[32] = reinterpret_cast<double (*)[32]>(gsm + (size_t)WPB * CAP * sizeof(double));
-  int (*scol)[CAP] = reinterpret_cast<int (*)[CAP]>(gsm + (size_t)WPB * (CAP + 32) * sizeof(double));
+  T (*sacc)[CAP] = reinterpret_cast<T (*)[CAP]>(gsm);
+  T (*sprod)[32] = reinterpret_cast<T (*)[32]>(gsm + (size_t)WPB * CAP * sizeof(T));
+  int (*scol)[CAP] = reinterpret_cast<int (*)[CAP]>(gsm + (size_t)WPB * (CAP + 32) * sizeof(T));
   const int lane = threadIdx.x & 31;
   const int w = threadIdx.x >> 5;
   const unsigned full = 0xffffffffu;
@@ -1636,17 +1637,17 @@ k_spgemm_warp(int nrows, const int* __restrict__ out_rp, const int* __restrict__
     const int m = oe - os;
     const bool fits = m <= CAP;
     const int* pat = fits ? scol[w] : out_ci + os;
-    double* acc = fits ? sacc[w] : out_v + os;
+    T* acc = fits ? sacc[w] : out_v + os;
     for (int t = lane; t < m; t += 32) {
       if (fits) scol[w][t] = out_ci[os + t];
-      acc[t] = 0.0;
+      acc[t] = T(0);
     }
     __syncwarp();
     const int ss = s_rp[I], se = s_rp[I + 1];
     for (int k0 = ss; k0 < se; k0 += 32) {
       const int k = k0 + lane;
       int bs = 0, len = 0;
-      double sv = 0.0;
+      T sv = T(0);
       if (k < se) {
         const int j = s_ci[k];
         sv = s_v[k];
@@ -1672,14 +1673,14 @@ k_spgemm_warp(int nrows, const int* __restrict__ out_rp, const int* __restrict__
         }
         const int qbs = __shfl_sync(full, bs, q);
         const int qex = __shfl_sync(full, excl, q);
-        const double qsv = __shfl_sync(full, sv, q);
+        const T qsv = __shfl_sync(full, sv, q);
         const bool act = f < total;
         int pos = -1;
-        double prod = 0.0;
+        T prod = T(0);
         if (act) {
           const int t = qbs + (f - qex);
           const int J = b_ci[t];
-          prod = __dmul_rn(qsv, b_v[t]);
+          prod = mul_rn(qsv, b_v[t]);
           int lo = 0, hi = m - 1;
           while (lo <= hi) {
             const int mid = (lo + hi) >> 1;
@@ -1698,8 +1699,8 @@ k_spgemm_warp(int nrows, const int* __restrict__ out_rp, const int* __restrict__
         if (pos >= 0) {
           const unsigned peers = __match_any_sync(am, pos);
           if (lane == __ffs(peers) - 1) {
-            double a = acc[pos];
-            for (unsigned mm = peers; mm; mm &= mm - 1) a = __dadd_rn(a, sprod[w][__ffs(mm) - 1]);
+            T a = acc[pos];
+            for (unsigned mm = peers; mm; mm &= mm - 1) a = add_rn(a, sprod[w][__ffs(mm) - 1]);
             acc[pos] = a;
           }
         }

@@ -40,6 +40,7 @@ SIGNATURES = {
     "draugr_b200_resetup_values_device": (i32, [i32, i64, P]),
     "draugr_b200_residual_device": (i32, [i32, i32, P, P, P, P]),
     "draugr_b200_galerkin_host": (i32, [i32, i32, i64, P, i64, P]),
+    "draugr_b200_set_resetup_precision": (i32, [i32, i32]),
     "draugr_b200_residual_noalloc": (i32, [i32, i32, P, P, P, P, P, P, P, P]),
     "draugr_b200_pcg": (i32, [i32, i32, P, P, i32, f64, i32, i32, P]),
     "draugr_b200_pcg_device": (i32, [i32, i32, P, P, i32, f64, i32, i32, P]),

@@ -299,6 +299,13 @@ class Hierarchy:
                    f"export {what}")
         return out
 
+    def set_resetup_precision(self, fp64_levels: int) -> None:
+        """Galerkin products of later partial resetups: the first
+        `fp64_levels` from the top in FP64, the rest in FP32 (negative: all
+        FP64, the default)."""
+        _lib.check(_lib.load().draugr_b200_set_resetup_precision(self.handle, fp64_levels),
+                   "set_resetup_precision")
+
     def galerkin_host(self, lvl: int, values) -> np.ndarray:
         """The next level's values from new values of level lvl, by the
         setup's numeric product on the host (draugr_b200_galerkin_host)."""

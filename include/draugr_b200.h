@@ -113,6 +113,16 @@ int32_t draugr_b200_residual_noalloc(int32_t n, int32_t nnz, const int32_t *rowp
  * values to the host first (ext/DraugrCUDAExt.jl:49). */
 int32_t draugr_b200_resetup_values_device(int32_t handle, int64_t nnz, const double *nzval_dev);
 
+/* Precision of the Galerkin products of later partial resetups: the first
+ * fp64_levels products from the top (the ones that form levels 2 ..
+ * fp64_levels + 1) in FP64, the rest in FP32 on the FP32 copies of A, P and
+ * Pᵀ, each FP32-computed level's FP64 copy being its FP32 values widened.
+ * Negative (the default): every product in FP64, as the reference.  The
+ * smoother diagonals and the coarsest LU are always formed in FP64.  The
+ * reference's resetup computes every level in the matrix's own precision
+ * (src/resetup.jl:36-41). */
+int32_t draugr_b200_set_resetup_precision(int32_t handle, int32_t fp64_levels);
+
 /* The Galerkin product of level lvl computed on the host by the setup's
  * numeric product (A*P, then Pᵀ(AP), each entry accumulated in the same
  * order as the device's partial resetup): a_vals holds new values of level

@@ -148,3 +148,34 @@ def test_c4_128cubed_resetup_bit_exact_against_the_host_product():
     x, it, _ = draugr.pcg(np.zeros(n), b, h, cfg, tol=1e-8, maxiter=500, precision="fp64")
     assert np.linalg.norm(b - A2 @ x) / np.linalg.norm(b) < 1e-8
     h.free()
+
+
+def test_c4_64cubed_resetup_fp64_top_two_levels_fp32_below():
+    """The coefficient-update configuration's precision split: the Galerkin
+    products of the top two levels in FP64 (1e-12 against the reference's
+    triple map), those below in FP32 (1e-5); the solves still reach 1e-8
+    in FP64."""
+    m = 64
+    rng = np.random.default_rng(31)
+    kappa = np.ones((m + 1,) * 3)
+    A = _aniso27(m, kappa)
+    cfg = draugr.hypre_default_config(agg_trunc_factor=0.2, smoother=draugr.L1JacobiSmootherType(),
+                                      seed=2024)
+    h = draugr.amg_setup(A, cfg)
+    assert h.nlevels >= 4
+    h.set_resetup_precision(2)
+    O = oracle.OracleHierarchy(h, with_rmaps=True)
+    kappa = kappa * np.exp(0.5 * rng.standard_normal(kappa.shape))
+    A2 = _aniso27(m, kappa)
+    draugr.amg_resetup(h, A2, cfg, partial=True)
+    O.resetup(A2.data)
+    errs = [rel(h.export(l, "A_nzval"), O.level_values(l)) for l in range(h.nlevels)]
+    print("\nper-level error, FP64 top two products, FP32 below:", ["%.1e" % e for e in errs])
+    for l, e in enumerate(errs):
+        assert e < (1e-12 if l <= 2 else 1e-5), (l, e)
+    assert rel(h.export(-1, "C_dense"), O.dense) < 1e-5
+    b = problems.rhs(A.shape[0], 9)
+    for precision in ("fp64", "mixed"):
+        x, it, _ = draugr.pcg(np.zeros(A.shape[0]), b, h, cfg, tol=1e-8, maxiter=500, precision=precision)
+        assert np.linalg.norm(b - A2 @ x) / np.linalg.norm(b) < 1e-8
+    h.free()
