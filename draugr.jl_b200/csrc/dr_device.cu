@@ -1883,9 +1883,12 @@ void DevHier::spgemm(DevMat& O, const DevMat& S, const DevMat& B, T* ov, const T
                      SpgemmList* list) {
   if (list && !list->tried) build_spgemm_list(O, S, B, *list);
   if (list && list->off) {
+    constexpr int WA = 8, CAPW = 768;  // 48 KB of staged pairs per block
+    auto kf = k_spgemm_apply_staged<T, WA, CAPW>;
+    const int grid = (int)std::max<long long>(
+        1, std::min<long long>((O.nnz + 32 * WA - 1) / (32 * WA), (long long)g_nsm * resident_blocks((const void*)kf, WA * 32, 0)));
     counted();
-    k_spgemm_apply<T><<<grid1d(O.nnz, max_grid_), kBlock, 0, st_>>>(O.nnz, list->off, list->ls, list->lb, sv, bv,
-                                                                    ov);
+    kf<<<grid, WA * 32, 0, st_>>>(O.nnz, list->off, list->ls, list->lb, sv, bv, ov);
     DR_CK(cudaGetLastError());
     return;
   }

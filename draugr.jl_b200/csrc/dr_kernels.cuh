@@ -1451,6 +1451,43 @@ k_spgemm_sym(int nrows, const int* __restrict__ out_rp, const int* __restrict__ 
 // O's values from the product lists (see k_spgemm_sym): one thread per
 // output entry, products multiplied and added in list order, separately
 // rounded.
+// The same products with each warp's lists staged first: a warp takes 32
+// consecutive output entries, whose lists are contiguous, copies their
+// (S entry, B entry) pairs into shared memory with coalesced loads when
+// they number at most CAPW, and each lane then adds its entry's products
+// in list order from there (the same values as k_spgemm_apply, bit for
+// bit).  Spans longer than CAPW are read from global memory.
+template <typename T, int WPB, int CAPW>
+__global__ void __launch_bounds__(WPB * 32)
+k_spgemm_apply_staged(long long nout, const long long* __restrict__ off, const int* __restrict__ ls,
+                      const int* __restrict__ lb, const T* __restrict__ s_v, const T* __restrict__ b_v,
+                      T* __restrict__ out_v) {
+  __shared__ int2 stage[WPB][CAPW];
+  const int lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5;
+  for (long long e0 = ((long long)blockIdx.x * WPB + w) * 32; e0 < nout; e0 += (long long)gridDim.x * WPB * 32) {
+    const long long e = e0 + lane;
+    const long long p0 = __ldg(off + e0);
+    const long long p1 = __ldg(off + min(e0 + 32, nout));
+    const long long my0 = e < nout ? __ldg(off + e) : p1;
+    const long long my1 = e < nout ? __ldg(off + e + 1) : p1;
+    T a = T(0);
+    if (p1 - p0 <= CAPW) {
+      for (long long q = p0 + lane; q < p1; q += 32) stage[w][q - p0] = make_int2(__ldg(ls + q), __ldg(lb + q));
+      __syncwarp();
+#pragma unroll 4
+      for (long long q = my0; q < my1; ++q) {
+        const int2 pr = stage[w][q - p0];
+        a = add_rn(a, mul_rn(__ldg(s_v + pr.x), __ldg(b_v + pr.y)));
+      }
+      __syncwarp();
+    } else {
+      for (long long q = my0; q < my1; ++q) a = add_rn(a, mul_rn(__ldg(s_v + __ldg(ls + q)), __ldg(b_v + __ldg(lb + q))));
+    }
+    if (e < nout) out_v[e] = a;
+  }
+}
+
 template <typename T>
 __global__ void k_spgemm_apply(long long nout, const long long* __restrict__ off, const int* __restrict__ ls,
                                const int* __restrict__ lb, const T* __restrict__ s_v,
