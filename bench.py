@@ -241,6 +241,16 @@ def run_ours(args, world, rank, local):
     torch.cuda.set_device(dev)
     A, b, cfg = workload(args.n, args.seed)
     n = A.shape[0]
+    # setup for the device, its Galerkin products on the CPU and then on the
+    # GPU (the offload), after a small setup has loaded the kernels
+    from draugr import problems as _pb
+    draugr.amg_setup(_pb.poisson3d(16), cfg).free()
+    os.environ["DRAUGR_B200_GPU_SETUP"] = "0"
+    t0 = time.time()
+    hh = draugr.amg_setup(A, cfg)
+    setup_host_s = time.time() - t0
+    hh.free()
+    os.environ.pop("DRAUGR_B200_GPU_SETUP", None)
     t0 = time.time()
     h = draugr.amg_setup(A, cfg)
     setup_s = time.time() - t0
@@ -410,7 +420,7 @@ def run_ours(args, world, rank, local):
            "data": "synthetic (seeded log-normal permeability field, b ~ U(-1,1))",
            "config": dict(workload_config(args.n, n, A.nnz, h),
                           parallelism=f"replicas x{world}" if world > 1 else "1 GPU"),
-           "setup_s_cpu": round(setup_s, 3),
+           "setup_s": round(setup_s, 3), "setup_s_galerkin_on_cpu": round(setup_host_s, 3),
            "fp64": res["fp64"], "mixed": res["mixed"],
            "speedup_mixed_vs_fp64": res["fp64"]["time_s"] / res["mixed"]["time_s"],
            "krylov": krylov,

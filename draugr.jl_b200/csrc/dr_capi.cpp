@@ -161,7 +161,10 @@ static int32_t setup_impl(int32_t n, int32_t nnz, const int32_t* rowptr, const i
   CSR A = csr_from_raw(n, nnz, rowptr, colval, nzval, index_base);
   Config c = get_cfg(config_handle);
   auto H = std::make_shared<Hier>();
-  build_hierarchy(A, c, allow_partial_resetup != 0, H->host);
+  // a setup for the device computes its Galerkin products there (same
+  // hierarchy, bit for bit); a host-only setup stays on the CPU
+  std::unique_ptr<GalerkinDevice> gdev = to_device ? make_galerkin_device() : nullptr;
+  build_hierarchy(A, c, allow_partial_resetup != 0, H->host, gdev.get());
   if (to_device) device_of(*H);
   if (c.verbose >= 1) print_summary(*H);
   std::lock_guard<std::mutex> lk(g_mu);
@@ -216,7 +219,8 @@ int32_t draugr_amg_resetup(int32_t handle, int32_t n, int32_t nnz, const int32_t
       else H->host.levels[0].A.v = A.v;
     } else {
       auto NH = std::make_shared<Hier>();
-      build_hierarchy(A, c, allow_partial_resetup != 0, NH->host);
+      std::unique_ptr<GalerkinDevice> gdev = H->dev ? make_galerkin_device() : nullptr;
+      build_hierarchy(A, c, allow_partial_resetup != 0, NH->host, gdev.get());
       if (H->dev) {
         H->dev.reset();
         device_of(*NH);

@@ -1909,6 +1909,25 @@ void DevHier::set_resetup_fp64_levels(int n) {
   resetup_fp64_ = n;
 }
 
+// The numeric product O = S·B on O's pattern with the warp kernel, on raw
+// device arrays (the setup's device Galerkin products).
+void galerkin_numeric_raw(cudaStream_t st, int n, int maxlen, const int* o_rp, const int* o_ci, double* o_v,
+                          const int* s_rp, const int* s_ci, const double* s_v, const int* b_rp,
+                          const int* b_ci, const double* b_v, int max_grid) {
+  if (n <= 0) return;
+  constexpr int W = 8;
+  const int grid = std::max(1, std::min((n + W - 1) / W, max_grid));
+  counted();
+#define DR_SPGEMM(CAP)                                                                      \
+  k_spgemm_warp<double, CAP, W><<<grid, W * 32, spgemm_smem_bytes<double, CAP, W>(), st>>>( \
+      n, o_rp, o_ci, o_v, s_rp, s_ci, s_v, b_rp, b_ci, b_v)
+  if (maxlen <= 128) DR_SPGEMM(128);
+  else if (maxlen <= 256) DR_SPGEMM(256);
+  else DR_SPGEMM(384);
+#undef DR_SPGEMM
+  DR_CK(cudaGetLastError());
+}
+
 void DevHier::resetup_values(const double* v_dev) {
   const int nl = nlevels();
   for (int l = 0; l < nl; ++l)

@@ -196,6 +196,15 @@ struct BatchLayout {
   std::vector<int> piv;               // all pivots (0-based)
 };
 
+// Numeric product O = S·B on O's fixed pattern (k_spgemm_warp), raw device
+// arrays, on stream st; maxlen: O's longest row.
+void galerkin_numeric_raw(cudaStream_t st, int n, int maxlen, const int* o_rp, const int* o_ci, double* o_v,
+                          const int* s_rp, const int* s_ci, const double* s_v, const int* b_rp,
+                          const int* b_ci, const double* b_v, int max_grid);
+// A device implementation of the setup's Galerkin products on the current
+// device (nullptr when no device is usable or DRAUGR_B200_GPU_SETUP=0).
+std::unique_ptr<GalerkinDevice> make_galerkin_device();
+
 // Merge the hierarchies of independent systems into one (CPU); every
 // level of every system must use a Jacobi-type smoother, and systems that
 // share a level the same smoother and weight.

@@ -722,7 +722,8 @@ void build_smoother(HostLevel& L, const Config& cfg, int level) {
 
 }  // namespace
 
-void build_hierarchy(const CSR& A_in, const Config& cfg, bool allow_partial_resetup, HostHierarchy& H) {
+void build_hierarchy(const CSR& A_in, const Config& cfg, bool allow_partial_resetup, HostHierarchy& H,
+                     GalerkinDevice* gdev) {
   auto t0 = std::chrono::steady_clock::now();
   validate_csr(A_in, "matrix");
   if (A_in.n != A_in.m) fail("matrix must be square");
@@ -758,13 +759,15 @@ void build_hierarchy(const CSR& A_in, const Config& cfg, bool allow_partial_rese
     L.Rv.resize(P.nnz());
     for (size_t k = 0; k < L.T.pnz.size(); ++k) L.Rv[k] = P.v[L.T.pnz[k]];
     std::vector<int> ap_rp, ap_ci;
-    symbolic_ap(cur, P, ap_rp, ap_ci);
     std::vector<double> ap_v;
-    numeric_ap(cur, P, ap_rp, ap_ci, ap_v);
     CSR next;
     next.n = next.m = nc;
-    symbolic_ptap(L.T, nc, ap_rp, ap_ci, next.rp, next.ci);
-    numeric_ptap(L.T, L.Rv, ap_rp, ap_ci, ap_v, next.rp, next.ci, next.v);
+    if (!gdev || !gdev->galerkin(cur, P, L.T, L.Rv, ap_rp, ap_ci, ap_v, next)) {
+      symbolic_ap(cur, P, ap_rp, ap_ci);
+      numeric_ap(cur, P, ap_rp, ap_ci, ap_v);
+      symbolic_ptap(L.T, nc, ap_rp, ap_ci, next.rp, next.ci);
+      numeric_ptap(L.T, L.Rv, ap_rp, ap_ci, ap_v, next.rp, next.ci, next.v);
+    }
     if (allow_partial_resetup) {
       L.has_rap_map = true;
       L.ap_rp = std::move(ap_rp);

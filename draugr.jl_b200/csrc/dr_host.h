@@ -284,8 +284,18 @@ void spai1_values(const CSR& A, std::vector<double>& M);
 void csr_to_dense(const CSR& A, std::vector<double>& M);            // setup.jl:495-516
 void dense_lu(int n, std::vector<double>& lu, std::vector<int>& piv);
 
-void build_hierarchy(const CSR& A, const Config& cfg, bool allow_partial_resetup,
-                     HostHierarchy& H);
+// Optional device implementation of one level's Galerkin products during
+// setup: the pattern and values of A·P (ap_*) and of Pᵀ(AP) (next),
+// identical to symbolic_ap / numeric_ap / symbolic_ptap / numeric_ptap.
+// Returns false to leave them to the host.
+struct GalerkinDevice {
+  virtual bool galerkin(const CSR& A, const Prolong& P, const TransposeMap& T, const std::vector<double>& Rv,
+                        std::vector<int>& ap_rp, std::vector<int>& ap_ci, std::vector<double>& ap_v,
+                        CSR& next) = 0;
+  virtual ~GalerkinDevice() = default;
+};
+void build_hierarchy(const CSR& A, const Config& cfg, bool allow_partial_resetup, HostHierarchy& H,
+                     GalerkinDevice* gdev = nullptr);
 std::string hierarchy_summary(const HostHierarchy& H, int n_finest);
 
 // Random measures: splitmix64-seeded xoshiro-like generator in [0,1).
