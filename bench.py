@@ -76,6 +76,8 @@ def parse():
     ap.add_argument("--workers", type=int, default=16)
     ap.add_argument("--profile-solve", choices=["fp64", "mixed"], default=None,
                     help="run exactly one PCG solve in this precision (for profiling)")
+    ap.add_argument("--profile-batch", action="store_true",
+                    help="run exactly one segmented batched solve of the batching workload's 64 systems")
     ap.add_argument("--write-structure", default=None, metavar="PATH",
                     help="build the workload's hierarchy structure on the host (no GPU) and write "
                          "it with the right-hand side to PATH (.npz) for the reference arm")
@@ -875,6 +877,28 @@ def run_profile_resetup(args):
     return {"profile_resetup": True, "n": int(A.shape[0]), "nnz": int(A.nnz), "levels": h.nlevels + 1}
 
 
+def run_profile_batch(args):
+    import torch
+
+    import draugr
+    from draugr import problems
+
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(args.seed)
+    cfg = draugr.hypre_default_config(agg_trunc_factor=0.2, smoother=draugr.L1JacobiSmootherType(),
+                                      seed=args.seed)
+    sides = rng.integers(16, 65, size=args.systems)
+    mats = [problems.poisson3d(int(s)) for s in sides]
+    hs = [draugr.amg_setup(A, cfg) for A in mats]
+    batch = draugr.batch_setup(hs, cfg)
+    b = torch.tensor(np.concatenate([rng.uniform(-1, 1, A.shape[0]) for A in mats]), device="cuda")
+    x = torch.zeros_like(b)
+    torch.cuda.synchronize()
+    _, its, rel = draugr.pcg_batched(x, b, batch, cfg, tol=TOL, maxiter=MAXITER, precision="mixed")
+    return {"profile_batch": True, "systems": int(args.systems), "rows": int(b.numel()),
+            "iterations": [int(its.min()), int(its.max())], "relres_max": float(rel.max())}
+
+
 def run_profile_solve(args):
     import torch
 
@@ -905,6 +929,9 @@ def main():
         return
     if args.profile_solve:
         print(json.dumps(run_profile_solve(args)), flush=True)
+        return
+    if args.profile_batch:
+        print(json.dumps(run_profile_batch(args)), flush=True)
         return
     if args.kernel_only:
         print(json.dumps(run_kernel_only(args)), flush=True)

@@ -1439,11 +1439,17 @@ void DevHier::batch_coarse(int l, const T* b, T* x) {
   if (l >= (int)batch_dev_.size()) return;
   const BatchDev& c = batch_dev_[l];
   if (c.nblk == 0) return;
-  int threads = 32;
-  while (threads < c.maxn && threads < 256) threads *= 2;
   counted();
-  k_lu_solve_batch<T><<<c.nblk, threads, (size_t)std::max(c.maxn, 1) * sizeof(double), st_>>>(
-      c.off, c.nb, c.luoff, c.poff, blu_, bpiv_, b, x);
+  if (c.maxn <= kern::kLuWarpMax) {  // one warp per system
+    constexpr int WPB = 4;
+    k_lu_solve_batch_warp<T, WPB><<<(c.nblk + WPB - 1) / WPB, WPB * 32, 0, st_>>>(
+        c.nblk, c.off, c.nb, c.luoff, c.poff, blu_, bpiv_, b, x);
+  } else {
+    int threads = 32;
+    while (threads < c.maxn && threads < 256) threads *= 2;
+    k_lu_solve_batch<T><<<c.nblk, threads, (size_t)std::max(c.maxn, 1) * sizeof(double), st_>>>(
+        c.off, c.nb, c.luoff, c.poff, blu_, bpiv_, b, x);
+  }
   DR_CK(cudaGetLastError());
 }
 template void DevHier::batch_coarse<double>(int, const double*, double*);

@@ -1805,6 +1805,56 @@ __global__ void k_lu_solve_batch(const int* __restrict__ off, const int* __restr
   for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = (T)y[i];
 }
 
+// The same coarsest solves with one warp per system (systems of at most
+// kLuWarpMax unknowns), warp barriers between the substitution steps in
+// place of block barriers; the operation order is k_lu_solve's.
+constexpr int kLuWarpMax = 256;
+template <typename T, int WPB>
+__global__ void __launch_bounds__(WPB * 32)
+k_lu_solve_batch_warp(int nblk, const int* __restrict__ off, const int* __restrict__ nb,
+                      const long long* __restrict__ luoff, const int* __restrict__ poff,
+                      const double* __restrict__ lu_all, const int* __restrict__ piv_all,
+                      const T* __restrict__ bin, T* __restrict__ xout) {
+  __shared__ double ys[WPB][kLuWarpMax];
+  const int lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5;
+  const int k = blockIdx.x * WPB + w;
+  if (k >= nblk) return;  // whole warps leave together
+  const int n = nb[k];
+  const double* __restrict__ a = lu_all + luoff[k];
+  const int* __restrict__ piv = piv_all + poff[k];
+  const T* __restrict__ b = bin + off[k];
+  T* __restrict__ x = xout + off[k];
+  double* y = ys[w];
+  for (int i = lane; i < n; i += 32) y[i] = (double)b[i];
+  __syncwarp();
+  if (lane == 0)
+    for (int j = 0; j < n; ++j) {
+      const int p = piv[j];
+      if (p != j) {
+        const double t = y[j];
+        y[j] = y[p];
+        y[p] = t;
+      }
+    }
+  __syncwarp();
+  for (int j = 0; j < n; ++j) {
+    const double yj = y[j];
+    if (yj != 0.0)
+      for (int i = j + 1 + lane; i < n; i += 32) y[i] = __dsub_rn(y[i], __dmul_rn(yj, a[(size_t)j * n + i]));
+    __syncwarp();
+  }
+  for (int j = n - 1; j >= 0; --j) {
+    if (lane == 0 && y[j] != 0.0) y[j] = __ddiv_rn(y[j], a[(size_t)j * n + j]);
+    __syncwarp();
+    const double yj = y[j];
+    if (yj != 0.0)
+      for (int i = lane; i < j; i += 32) y[i] = __dsub_rn(y[i], __dmul_rn(yj, a[(size_t)j * n + i]));
+    __syncwarp();
+  }
+  for (int i = lane; i < n; i += 32) x[i] = (T)y[i];
+}
+
 // Per-segment dot products, deterministic: blockIdx.y = segment, blocks
 // along x stride its rows; partials[s * gridDim.x + bx]; then
 // k_seg_dot_final sums each segment's partials in block order (one warp per
