@@ -1353,7 +1353,7 @@ __global__ void k_l1_invdiag(int n, const int* __restrict__ rp, const double* __
 // recorded once by k_spgemm_sym (COUNT, then FILL after an exclusive scan
 // of the counts) walking the products exactly as k_spgemm_warp does -- in
 // the order (entry k of S's row, entry t of B's row j_k), grouped by output
-// entry in lane order -- so k_spgemm_apply adds every entry's products in
+// entry in lane order -- so k_spgemm_apply_staged adds every entry's products in
 // the same order and gives the same values bit for bit, with a few
 // instructions and 24 bytes of traffic per product.
 template <int CAP, int WPB, bool FILL>
@@ -1448,15 +1448,13 @@ k_spgemm_sym(int nrows, const int* __restrict__ out_rp, const int* __restrict__ 
   }
 }
 
-// O's values from the product lists (see k_spgemm_sym): one thread per
-// output entry, products multiplied and added in list order, separately
-// rounded.
-// The same products with each warp's lists staged first: a warp takes 32
+// O's values from the product lists (see k_spgemm_sym): a warp takes 32
 // consecutive output entries, whose lists are contiguous, copies their
 // (S entry, B entry) pairs into shared memory with coalesced loads when
 // they number at most CAPW, and each lane then adds its entry's products
-// in list order from there (the same values as k_spgemm_apply, bit for
-// bit).  Spans longer than CAPW are read from global memory.
+// in list order from there, multiplied and added with separate rounding
+// (the warp kernel's values, bit for bit).  Spans longer than CAPW are read
+// from global memory.
 template <typename T, int WPB, int CAPW>
 __global__ void __launch_bounds__(WPB * 32)
 k_spgemm_apply_staged(long long nout, const long long* __restrict__ off, const int* __restrict__ ls,
@@ -1485,18 +1483,6 @@ k_spgemm_apply_staged(long long nout, const long long* __restrict__ off, const i
       for (long long q = my0; q < my1; ++q) a = add_rn(a, mul_rn(__ldg(s_v + __ldg(ls + q)), __ldg(b_v + __ldg(lb + q))));
     }
     if (e < nout) out_v[e] = a;
-  }
-}
-
-template <typename T>
-__global__ void k_spgemm_apply(long long nout, const long long* __restrict__ off, const int* __restrict__ ls,
-                               const int* __restrict__ lb, const T* __restrict__ s_v,
-                               const T* __restrict__ b_v, T* __restrict__ out_v) {
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nout;
-       e += (long long)gridDim.x * blockDim.x) {
-    T a = T(0);
-    for (long long p = off[e]; p < off[e + 1]; ++p) a = add_rn(a, mul_rn(s_v[ls[p]], b_v[lb[p]]));
-    out_v[e] = a;
   }
 }
 
