@@ -1440,10 +1440,9 @@ void DevHier::batch_coarse(int l, const T* b, T* x) {
   const BatchDev& c = batch_dev_[l];
   if (c.nblk == 0) return;
   counted();
-  if (c.maxn <= kern::kLuWarpMax) {  // one warp per system
-    constexpr int WPB = 4;
-    k_lu_solve_batch_warp<T, WPB><<<(c.nblk + WPB - 1) / WPB, WPB * 32, 0, st_>>>(
-        c.nblk, c.off, c.nb, c.luoff, c.poff, blu_, bpiv_, b, x);
+  const size_t wsm = (size_t)(c.maxn + (size_t)c.maxn * c.maxn) * sizeof(double);
+  if (wsm <= 48 * 1024) {  // one warp per system, its factors staged in shared memory
+    k_lu_solve_batch_warp<T><<<c.nblk, 32, wsm, st_>>>(c.off, c.nb, c.luoff, c.poff, blu_, bpiv_, b, x, c.maxn);
   } else {
     int threads = 32;
     while (threads < c.maxn && threads < 256) threads *= 2;

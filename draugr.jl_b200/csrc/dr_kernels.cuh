@@ -1791,27 +1791,28 @@ __global__ void k_lu_solve_batch(const int* __restrict__ off, const int* __restr
   for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = (T)y[i];
 }
 
-// The same coarsest solves with one warp per system (systems of at most
-// kLuWarpMax unknowns), warp barriers between the substitution steps in
-// place of block barriers; the operation order is k_lu_solve's.
-constexpr int kLuWarpMax = 256;
-template <typename T, int WPB>
-__global__ void __launch_bounds__(WPB * 32)
-k_lu_solve_batch_warp(int nblk, const int* __restrict__ off, const int* __restrict__ nb,
-                      const long long* __restrict__ luoff, const int* __restrict__ poff,
-                      const double* __restrict__ lu_all, const int* __restrict__ piv_all,
-                      const T* __restrict__ bin, T* __restrict__ xout) {
-  __shared__ double ys[WPB][kLuWarpMax];
-  const int lane = threadIdx.x & 31;
-  const int w = threadIdx.x >> 5;
-  const int k = blockIdx.x * WPB + w;
-  if (k >= nblk) return;  // whole warps leave together
+// The same coarsest solves with one warp per system (one warp per block),
+// warp barriers between the substitution steps in place of block barriers,
+// and the system's factors first copied into shared memory (coalesced), so
+// that the 2n dependent steps read them there rather than from L2; the
+// operation order is k_lu_solve's.  Dynamic shared memory: (maxn + maxn²)
+// doubles.
+template <typename T>
+__global__ void __launch_bounds__(32)
+k_lu_solve_batch_warp(const int* __restrict__ off, const int* __restrict__ nb, const long long* __restrict__ luoff,
+                      const int* __restrict__ poff, const double* __restrict__ lu_all,
+                      const int* __restrict__ piv_all, const T* __restrict__ bin, T* __restrict__ xout, int maxn) {
+  extern __shared__ double shw[];
+  const int lane = threadIdx.x;
+  const int k = blockIdx.x;
   const int n = nb[k];
-  const double* __restrict__ a = lu_all + luoff[k];
+  const double* __restrict__ ag = lu_all + luoff[k];
   const int* __restrict__ piv = piv_all + poff[k];
   const T* __restrict__ b = bin + off[k];
   T* __restrict__ x = xout + off[k];
-  double* y = ys[w];
+  double* y = shw;
+  double* a = shw + maxn;
+  for (int t = lane; t < n * n; t += 32) a[t] = ag[t];
   for (int i = lane; i < n; i += 32) y[i] = (double)b[i];
   __syncwarp();
   if (lane == 0)
