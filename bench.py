@@ -575,7 +575,13 @@ def run_kernel_only(args):
     A, b, cfg = workload(args.n, args.seed)
     h = draugr.amg_setup(A, cfg)
     if args.level < 0:
-        return {"kernel_only": True, "levels": level_table(h, reps=max(args.reps, 10))}
+        reps = max(args.reps, 10)
+        # the V(1,1) cycle from each level down (coarse tail included): the
+        # differences between consecutive starts are each level's share
+        cyc = [{"from_level": l + 1, "prec": "fp64" if prec == 0 else "fp32",
+                "us": round(h.time_level_op(l, 8, prec, reps=reps) * 1e3, 2)}
+               for prec in (0, 1) for l in range(1, h.nlevels)]
+        return {"kernel_only": True, "levels": level_table(h, reps=reps), "cycles": cyc}
     ms = h.time_level_op(args.level, args.op, args.precision, reps=args.reps)
     info = h.level_info(args.level)
     return {"kernel_only": True, "level": args.level, "op": args.op, "precision": args.precision,

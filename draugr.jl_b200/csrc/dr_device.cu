@@ -182,10 +182,12 @@ int resident_blocks(const void* f, int nt, size_t smem) {
 }
 
 template <typename TA, class XL, class EP, bool DOT, class Fin>
-void launch_rows_impl(cudaStream_t st, int max_grid, const RowForm& f, int n, int ntiles,
-                      const int* tp, const int* ts, const int* tb, const int* rp, const int* ci,
-                      const uint16_t* cu, const TA* av, XL xl, EP ep, double* partials,
-                      unsigned* ticket, Fin fin) {
+void launch_rows_impl(cudaStream_t st, int max_grid, const DevMat& M, const TA* av, XL xl, EP ep,
+                      double* partials, unsigned* ticket, Fin fin) {
+  const RowForm& f = M.form;
+  const int n = M.n, ntiles = M.ntiles;
+  const int *tp = M.tp, *ts = M.ts, *tb = M.tb, *rp = M.rp, *ci = M.ci;
+  const uint16_t* cu = M.cu;
   if (n <= 0) {
     if constexpr (DOT) {
       // an empty reduction still has to deliver its (zero) result
@@ -225,16 +227,14 @@ void launch_rows_impl(cudaStream_t st, int max_grid, const RowForm& f, int n, in
 
 template <typename TA, class XL, class EP>
 void launch_rows(cudaStream_t st, int max_grid, const DevMat& M, const TA* av, XL xl, EP ep) {
-  launch_rows_impl<TA, XL, EP, false, FinStore>(st, max_grid, M.form, M.n, M.ntiles, M.tp, M.ts,
-                                                M.tb, M.rp, M.ci, M.cu, av, xl, ep, nullptr,
-                                                nullptr, FinStore{nullptr});
+  launch_rows_impl<TA, XL, EP, false, FinStore>(st, max_grid, M, av, xl, ep, nullptr, nullptr,
+                                                FinStore{nullptr});
 }
 
 template <typename TA, class XL, class EP, class Fin>
 void launch_rows_dot(cudaStream_t st, int max_grid, const DevMat& M, const TA* av, XL xl, EP ep,
                      double* partials, unsigned* ticket, Fin fin) {
-  launch_rows_impl<TA, XL, EP, true, Fin>(st, max_grid, M.form, M.n, M.ntiles, M.tp, M.ts, M.tb,
-                                          M.rp, M.ci, M.cu, av, xl, ep, partials, ticket, fin);
+  launch_rows_impl<TA, XL, EP, true, Fin>(st, max_grid, M, av, xl, ep, partials, ticket, fin);
 }
 
 int grid1d(long long n, int max_grid) {
@@ -612,12 +612,17 @@ static std::vector<int> bank_order(const std::vector<int>& rp) {
   return ord;
 }
 
+// Tail levels whose longest row exceeds this form their products flat
+// (TailLevel::p), in a shared-memory scratch of one value per nonzero.
+static constexpr int kTailFlatRow = 48;
+
 template <typename T>
 static size_t tail_level_bytes(const DevLevel& d) {
   const size_t n = d.A.n, nc = d.P.m, an = d.A.nnz, pn = d.P.nnz;
   return a16(4 * (n + 1)) + a16(4 * an) + a16(4 * n) + a16(sizeof(T) * an) + a16(sizeof(T) * n) +
          a16(4 * (n + 1)) + a16(4 * pn) + a16(sizeof(T) * pn) + a16(4 * (nc + 1)) + a16(4 * pn) +
-         a16(sizeof(T) * pn) + 4 * a16(sizeof(T) * n);
+         a16(sizeof(T) * pn) + 4 * a16(sizeof(T) * n) +
+         (d.A.maxlen > kTailFlatRow ? a16(sizeof(T) * an) : 0);
 }
 
 template <typename T>
@@ -722,6 +727,11 @@ void DevHier::build_tail() {
       t.o_xb = take(sizeof(T) * n);
       t.o_b = take(sizeof(T) * n);
       t.o_r = take(sizeof(T) * n);
+      // the product scratch has no global source: p only marks it (the
+      // kernel points p at shared memory)
+      const bool flat = d.A.maxlen > kTailFlatRow;
+      t.o_p = flat ? take(sizeof(T) * (size_t)d.A.nnz) : 0;
+      t.p = flat ? reinterpret_cast<T*>(V.r) : nullptr;
     }
     tail_co_[slot][0] = take(8 * ((size_t)nc_ * nc_ + nc_));
     tail_co_[slot][1] = take(4 * (size_t)nc_);
@@ -2164,7 +2174,9 @@ void DevHier::level_op(int lvl, int op, bool fp32, const double* in1, const doub
 
 float DevHier::time_level_op(int lvl, int op, bool fp32, int reps) {
   if (lvl < 0 || lvl >= nlevels()) fail("level index out of range");
-  if (op != 0 && op != 2 && op != 3 && op != 4 && op != 6) fail("time_level_op: op must be 0, 2, 3, 4 or 6");
+  if (op != 0 && op != 2 && op != 3 && op != 4 && op != 6 && op != 8)
+    fail("time_level_op: op must be 0, 2, 3, 4, 6 or 8");
+  if (op == 8 && (lvl < 1 || batch_)) fail("time_level_op: op 8 times a cycle from a level >= 1");
   if (fp32) ensure_fp32();
   cudaEvent_t e0, e1;
   DR_CK(cudaEventCreate(&e0));
@@ -2191,6 +2203,10 @@ float DevHier::time_level_op(int lvl, int op, bool fp32, int reps) {
     k_fill<T><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, T(1), bt);
     counted();
     k_fill<T><<<grid1d(nc, max_grid_), kBlock, 0, st_>>>(nc, T(1), cvec);
+    if (op == 8) {
+      counted();
+      k_fill<T><<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, T(1), V.b);
+    }
     const T om = (T)L.omega;
     auto once = [&]() {
       switch (op) {
@@ -2210,6 +2226,9 @@ float DevHier::time_level_op(int lvl, int op, bool fp32, int reps) {
         case 6:
           launch_rows(st_, max_grid_, L.A, mval<T>(L.A), XZeroJacobi<T>{x0, invd<T>(L), om},
                       EpZeroJacobiResidual<T>{x0, invd<T>(L), x1, x2, om});
+          break;
+        case 8:  // the V(1,1) cycle from level lvl down, from zero (the coarse tail included)
+          cycle_level<T>(lvl, V.xa, V.b, true, CycleOpts{}, nullptr, nullptr, false, false);
           break;
       }
     };

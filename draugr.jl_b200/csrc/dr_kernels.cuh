@@ -938,7 +938,11 @@ __global__ void k_lu_solve(int n, const double* __restrict__ lu, const int* __re
 // positions modulo 32: one thread per row then reads its row's columns and
 // values from shared memory without bank conflicts (rows in natural order
 // collide when their lengths are near multiples of 32), and still sums the
-// row in column order.
+// row in column order.  On levels with long rows the products are first
+// formed flat over the block (TailLevel::p), so the longest row's thread
+// only adds.  The descriptor's pointers are the global sources of the
+// copies; the kernel addresses the copies by their offsets from its
+// shared-memory base.
 template <typename T>
 struct TailLevel {
   int n, nc, annz, pnnz;  // rows, coarse rows, nonzeros of A and of P
@@ -950,9 +954,11 @@ struct TailLevel {
   const int *rrp, *rci;
   const T* rv;
   T *xa, *xb, *b, *r;  // iterate pair, right-hand side, residual
-  // byte offsets of the shared-memory copies (arrays above, in order)
+  T* p;                // products a_ij x_j of A, flat (levels with long rows; else null)
+  // byte offsets of the shared-memory copies (arrays above, in order; o_p:
+  // the product scratch, 0 when p is null)
   unsigned o_arp, o_aci, o_ord, o_av, o_invd, o_prp, o_pci, o_pv, o_rrp, o_rci, o_rv, o_xa, o_xb,
-      o_b, o_r;
+      o_b, o_r, o_p;
 };
 
 template <typename T>
@@ -967,6 +973,16 @@ struct TailCoarse {
 };
 
 constexpr int kTailMaxLevels = 8;
+constexpr int kTailThreads = 256;
+
+// The tail kernel's dynamic shared memory.  Arrays addressed from it by
+// offset (tail_sh) compile to shared-memory loads; pointers read back from
+// the level descriptors are generic.
+extern __shared__ __align__(16) unsigned char tail_smem[];
+template <typename U>
+__device__ __forceinline__ U* tail_sh(unsigned off) {
+  return reinterpret_cast<U*>(tail_smem + off);
+}
 
 // One bulk copy of the tail's prologue: `bytes` (a multiple of 16) from
 // `src` to shared-memory offset `off`.
@@ -985,27 +1001,96 @@ struct TailCopies {
   TailCopy x;
 };
 
-// a ± Σ_k v[k]·x[c[k]] over [s, e) in column order, eight loads in flight
+// a ± Σ_k v[k]·x[c[k]] over [s, e) in column order.  Eight entries at a
+// time: their columns and values are loaded unconditionally (slots past the
+// row end repeat its last entry), then the eight x reads, then the ordered
+// sum, so each batch costs two shared-memory round trips instead of two per
+// entry.
 template <int SIGN, typename T>
 __device__ __forceinline__ T tail_row(T a, const int* __restrict__ c, const T* __restrict__ v,
                                       const T* x, int s, int e) {
   for (int k0 = s; k0 < e; k0 += 8) {
-    T p[8];
+    int cc[8];
+    T vv[8], xv[8];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) p[j] = (k0 + j < e) ? mul_rn(v[k0 + j], x[c[k0 + j]]) : T(0);
+    for (int j = 0; j < 8; ++j) {
+      const int k = min(k0 + j, e - 1);
+      cc[j] = c[k];
+      vv[j] = v[k];
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) xv[j] = x[cc[j]];
 #pragma unroll
     for (int j = 0; j < 8; ++j)
-      if (k0 + j < e) a = SIGN > 0 ? add_rn(a, p[j]) : sub_rn(a, p[j]);
+      if (k0 + j < e) {
+        const T p = mul_rn(vv[j], xv[j]);
+        a = SIGN > 0 ? add_rn(a, p) : sub_rn(a, p);
+      }
   }
   return a;
 }
 
+// a ± p[s] ± p[s+1] ... in order, eight products loaded at a time.
+template <int SIGN, typename T>
+__device__ __forceinline__ T tail_sum(T a, const T* __restrict__ p, int s, int e) {
+  for (int k0 = s; k0 < e; k0 += 8) {
+    T pv[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) pv[j] = p[min(k0 + j, e - 1)];
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      if (k0 + j < e) a = SIGN > 0 ? add_rn(a, pv[j]) : sub_rn(a, pv[j]);
+  }
+  return a;
+}
+
+// Levels with long rows (L.p set) form the products a_ij·x_j of A flat over
+// the whole block first, so a long row no longer holds one thread for all
+// of its gathers; each row then sums its products in column order (the
+// same rounded products and sums as tail_row).
 template <typename T>
-__device__ void tail_jacobi(const TailLevel<T>& L, const T* x, const T* b, T* xn) {
+__device__ __forceinline__ void tail_products(const TailLevel<T>& L, const T* x) {
+  if (!L.p) return;
+  T* __restrict__ p = tail_sh<T>(L.o_p);
+  const int* __restrict__ c = tail_sh<const int>(L.o_aci);
+  const T* __restrict__ v = tail_sh<const T>(L.o_av);
+  const int nnz = L.annz;
+  for (int k0 = threadIdx.x; k0 < nnz; k0 += 4 * kTailThreads) {
+    int cc[4];
+    T vv[4], xv[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int k = min(k0 + j * kTailThreads, nnz - 1);
+      cc[j] = c[k];
+      vv[j] = v[k];
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) xv[j] = x[cc[j]];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (k0 + j * kTailThreads < nnz) p[k0 + j * kTailThreads] = mul_rn(vv[j], xv[j]);
+  }
+  __syncthreads();
+}
+
+// a ± Σ_k a_ik x_k over row i of A, in column order.
+template <int SIGN, typename T>
+__device__ __forceinline__ T tail_arow(const TailLevel<T>& L, T a, const T* x, int i) {
+  const int* rp = tail_sh<const int>(L.o_arp);
+  return L.p ? tail_sum<SIGN>(a, tail_sh<const T>(L.o_p), rp[i], rp[i + 1])
+             : tail_row<SIGN>(a, tail_sh<const int>(L.o_aci), tail_sh<const T>(L.o_av), x, rp[i],
+                              rp[i + 1]);
+}
+
+template <typename T>
+__device__ __forceinline__ void tail_jacobi(const TailLevel<T>& L, const T* x, const T* b, T* xn) {
+  tail_products(L, x);
+  const int* ord = tail_sh<const int>(L.o_ord);
+  const T* invd = tail_sh<const T>(L.o_invd);
   for (int t = threadIdx.x; t < L.n; t += blockDim.x) {
-    const int i = L.ord[t];
-    const T ri = tail_row<-1>(b[i], L.aci, L.av, x, L.arp[i], L.arp[i + 1]);
-    xn[i] = add_rn(x[i], mul_rn(mul_rn(L.omega, L.invd[i]), ri));
+    const int i = ord[t];
+    const T ri = tail_arow<-1>(L, b[i], x, i);
+    xn[i] = add_rn(x[i], mul_rn(mul_rn(L.omega, invd[i]), ri));
   }
   __syncthreads();
 }
@@ -1016,15 +1101,18 @@ __device__ void tail_jacobi(const TailLevel<T>& L, const T* x, const T* b, T* xn
 // unknowns one warp holds y in registers (lane i: y_i); larger systems use
 // the block with y in shared memory after the factors.
 template <typename T>
-__device__ void tail_lu_solve(const TailCoarse<T>& C) {
+__device__ __forceinline__ void tail_lu_solve(const TailCoarse<T>& C) {
   const int n = C.n;
-  const double* lu = C.lu;
+  const double* lu = tail_sh<const double>(C.o_lu);
+  const int* piv = tail_sh<const int>(C.o_piv);
+  const T* cb = tail_sh<const T>(C.o_b);
+  T* cx = tail_sh<T>(C.o_x);
   if (n <= 32) {
     if (threadIdx.x < 32) {
       const int i = threadIdx.x;
-      double y = i < n ? (double)C.b[i] : 0.0;
+      double y = i < n ? (double)cb[i] : 0.0;
       for (int j = 0; j < n; ++j) {
-        const int p = C.piv[j];
+        const int p = piv[j];
         if (p != j) {
           const double a = __shfl_sync(0xffffffffu, y, j);
           const double c = __shfl_sync(0xffffffffu, y, p);
@@ -1034,24 +1122,24 @@ __device__ void tail_lu_solve(const TailCoarse<T>& C) {
       }
       for (int j = 0; j < n; ++j) {
         const double yj = __shfl_sync(0xffffffffu, y, j);
-        if (yj != 0.0 && i > j && i < n) y = __dsub_rn(y, __dmul_rn(yj, lu[(size_t)j * n + i]));
+        if (yj != 0.0 && i > j && i < n) y = __dsub_rn(y, __dmul_rn(yj, lu[j * n + i]));
       }
       for (int j = n - 1; j >= 0; --j) {
-        if (i == j && y != 0.0) y = __ddiv_rn(y, lu[(size_t)j * n + j]);
+        if (i == j && y != 0.0) y = __ddiv_rn(y, lu[j * n + j]);
         const double yj = __shfl_sync(0xffffffffu, y, j);
-        if (yj != 0.0 && i < j) y = __dsub_rn(y, __dmul_rn(yj, lu[(size_t)j * n + i]));
+        if (yj != 0.0 && i < j) y = __dsub_rn(y, __dmul_rn(yj, lu[j * n + i]));
       }
-      if (i < n) C.x[i] = (T)y;
+      if (i < n) cx[i] = (T)y;
     }
     __syncthreads();
     return;
   }
-  double* y = const_cast<double*>(lu) + (size_t)n * n;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = (double)C.b[i];
+  double* y = tail_sh<double>(C.o_lu) + n * n;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = (double)cb[i];
   __syncthreads();
   if (threadIdx.x == 0)
     for (int j = 0; j < n; ++j) {
-      const int p = C.piv[j];
+      const int p = piv[j];
       if (p != j) {
         const double t = y[j];
         y[j] = y[p];
@@ -1063,34 +1151,42 @@ __device__ void tail_lu_solve(const TailCoarse<T>& C) {
     const double yj = y[j];
     if (yj != 0.0)
       for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x)
-        y[i] = __dsub_rn(y[i], __dmul_rn(yj, lu[(size_t)j * n + i]));
+        y[i] = __dsub_rn(y[i], __dmul_rn(yj, lu[j * n + i]));
     __syncthreads();
   }
   for (int j = n - 1; j >= 0; --j) {
-    if (threadIdx.x == 0 && y[j] != 0.0) y[j] = __ddiv_rn(y[j], lu[(size_t)j * n + j]);
+    if (threadIdx.x == 0 && y[j] != 0.0) y[j] = __ddiv_rn(y[j], lu[j * n + j]);
     __syncthreads();
     const double yj = y[j];
     if (yj != 0.0)
       for (int i = threadIdx.x; i < j; i += blockDim.x)
-        y[i] = __dsub_rn(y[i], __dmul_rn(yj, lu[(size_t)j * n + i]));
+        y[i] = __dsub_rn(y[i], __dmul_rn(yj, lu[j * n + i]));
     __syncthreads();
   }
-  for (int i = threadIdx.x; i < n; i += blockDim.x) C.x[i] = (T)y[i];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) cx[i] = (T)y[i];
   __syncthreads();
 }
 
-// One visit of level l (x_zero: the iterate starts at zero).  The result
-// ends in L.xa.  Levels l+1 .. nl-1 follow in `lv`; the coarsest system is C.
-template <typename T>
-__device__ void tail_visit(const TailLevel<T>* lv, int l, int nl, const TailCoarse<T>& C,
-                           bool x_zero, int pre, int post, int wcycle) {
+// One visit of level l = D (x_zero: the iterate starts at zero).  The
+// result ends in the level's xa.  Levels l+1 .. nl-1 follow in `lv`; the
+// coarsest system is C.  The level index is a template parameter so that
+// the visits of all levels inline into the kernel (a recursive device
+// function keeps a stack frame and spills around each call), and every
+// array is addressed from the shared-memory base by its offset.
+template <int D, typename T>
+__device__ __forceinline__ void tail_visit(const TailLevel<T>* lv, int nl, const TailCoarse<T>& C,
+                                           bool x_zero, int pre, int post, int wcycle) {
+  constexpr int l = D;
   const TailLevel<T>& L = lv[l];
-  T* x = L.xa;
-  T* t = L.xb;
-  const T* b = L.b;
+  const int n = L.n;
+  T* const xa = tail_sh<T>(L.o_xa);
+  T* x = xa;
+  T* t = tail_sh<T>(L.o_xb);
+  const T* b = tail_sh<const T>(L.o_b);
+  const T* invd = tail_sh<const T>(L.o_invd);
   if (x_zero && pre >= 1) {
     // first Jacobi step from zero
-    for (int i = threadIdx.x; i < L.n; i += blockDim.x) x[i] = mul_rn(mul_rn(L.omega, L.invd[i]), b[i]);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = mul_rn(mul_rn(L.omega, invd[i]), b[i]);
     __syncthreads();
     for (int s = 1; s < pre; ++s) {
       tail_jacobi(L, x, b, t);
@@ -1098,7 +1194,7 @@ __device__ void tail_visit(const TailLevel<T>* lv, int l, int nl, const TailCoar
     }
   } else {
     if (x_zero) {
-      for (int i = threadIdx.x; i < L.n; i += blockDim.x) x[i] = T(0);
+      for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = T(0);
       __syncthreads();
     }
     for (int s = 0; s < pre; ++s) {
@@ -1106,39 +1202,53 @@ __device__ void tail_visit(const TailLevel<T>* lv, int l, int nl, const TailCoar
       T* u = x; x = t; t = u;
     }
   }
-  for (int t = threadIdx.x; t < L.n; t += blockDim.x) {
-    const int i = L.ord[t];
-    L.r[i] = sub_rn(b[i], tail_row<1>(T(0), L.aci, L.av, x, L.arp[i], L.arp[i + 1]));
+  {
+    T* r = tail_sh<T>(L.o_r);
+    const int* ord = tail_sh<const int>(L.o_ord);
+    tail_products(L, x);
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+      const int i = ord[k];
+      r[i] = sub_rn(b[i], tail_arow<1>(L, T(0), x, i));
+    }
+    __syncthreads();
+    const bool last = (l + 1 == nl);
+    T* bn = last ? tail_sh<T>(C.o_b) : tail_sh<T>(lv[l + 1].o_b);
+    const int* rrp = tail_sh<const int>(L.o_rrp);
+    const int* rci = tail_sh<const int>(L.o_rci);
+    const T* rv = tail_sh<const T>(L.o_rv);
+    for (int J = threadIdx.x; J < L.nc; J += blockDim.x)
+      bn[J] = tail_row<1>(T(0), rci, rv, r, rrp[J], rrp[J + 1]);
+    __syncthreads();
   }
-  __syncthreads();
-  const bool last = (l + 1 == nl);
-  T* bn = last ? C.b : lv[l + 1].b;
-  for (int J = threadIdx.x; J < L.nc; J += blockDim.x)
-    bn[J] = tail_row<1>(T(0), L.rci, L.rv, L.r, L.rrp[J], L.rrp[J + 1]);
-  __syncthreads();
   const T* xc;
-  if (!last) {
-    tail_visit(lv, l + 1, nl, C, true, pre, post, wcycle);
-    if (wcycle) tail_visit(lv, l + 1, nl, C, false, pre, post, wcycle);
-    xc = lv[l + 1].xa;
+  if (l + 1 < nl) {
+    if constexpr (D + 1 < kTailMaxLevels) {
+      for (int rep = 0; rep < (wcycle ? 2 : 1); ++rep)
+        tail_visit<D + 1>(lv, nl, C, rep == 0, pre, post, wcycle);
+    }
+    xc = tail_sh<const T>(lv[l + 1].o_xa);
   } else {
     tail_lu_solve(C);
-    xc = C.x;
+    xc = tail_sh<const T>(C.o_x);
   }
-  for (int i = threadIdx.x; i < L.n; i += blockDim.x)
-    x[i] = tail_row<1>(x[i], L.pci, L.pv, xc, L.prp[i], L.prp[i + 1]);
-  __syncthreads();
+  {
+    const int* prp = tail_sh<const int>(L.o_prp);
+    const int* pci = tail_sh<const int>(L.o_pci);
+    const T* pv = tail_sh<const T>(L.o_pv);
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+      x[i] = tail_row<1>(x[i], pci, pv, xc, prp[i], prp[i + 1]);
+    __syncthreads();
+  }
   for (int s = 0; s < post; ++s) {
     tail_jacobi(L, x, b, t);
     T* u = x; x = t; t = u;
   }
-  if (x != L.xa) {
-    for (int i = threadIdx.x; i < L.n; i += blockDim.x) L.xa[i] = x[i];
+  if (x != xa) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) xa[i] = x[i];
     __syncthreads();
   }
 }
 
-constexpr int kTailThreads = 256;
 
 // lv: nl (<= kTailMaxLevels) descriptors with global pointers and the
 // shared-memory layout; dynamic shared memory holds that layout.  Every
@@ -1148,10 +1258,10 @@ constexpr int kTailThreads = 256;
 // copy that does not complete within the wait limit sets *err and the block
 // returns without touching global memory.
 template <typename T>
-__global__ void __launch_bounds__(kTailThreads)
+__global__ void __launch_bounds__(kTailThreads, 1)
 k_coarse_tail(const TailLevel<T>* __restrict__ lv, int nl, TailCoarse<T> C, TailCopies cp, int pre,
               int post, int wcycle, int x_zero, int* err) {
-  extern __shared__ __align__(16) unsigned char tsm[];
+  unsigned char* const tsm = tail_smem;
   __shared__ TailLevel<T> sl[kTailMaxLevels];
   __shared__ TailCoarse<T> sc;
   __shared__ __align__(8) uint64_t bar;
@@ -1178,36 +1288,11 @@ k_coarse_tail(const TailLevel<T>* __restrict__ lv, int nl, TailCoarse<T> C, Tail
     }
     if (threadIdx.x == 0 && !x_zero && cp.x.bytes) bulk_g2s(tsm + cp.x.off, cp.x.src, cp.x.bytes, &bar);
   }
-  if (threadIdx.x < nl) {
-    const TailLevel<T> g = lv[threadIdx.x];
-    TailLevel<T> v = g;
-    v.arp = reinterpret_cast<const int*>(tsm + g.o_arp);
-    v.aci = reinterpret_cast<const int*>(tsm + g.o_aci);
-    v.ord = reinterpret_cast<const int*>(tsm + g.o_ord);
-    v.av = reinterpret_cast<const T*>(tsm + g.o_av);
-    v.invd = reinterpret_cast<const T*>(tsm + g.o_invd);
-    v.prp = reinterpret_cast<const int*>(tsm + g.o_prp);
-    v.pci = reinterpret_cast<const int*>(tsm + g.o_pci);
-    v.pv = reinterpret_cast<const T*>(tsm + g.o_pv);
-    v.rrp = reinterpret_cast<const int*>(tsm + g.o_rrp);
-    v.rci = reinterpret_cast<const int*>(tsm + g.o_rci);
-    v.rv = reinterpret_cast<const T*>(tsm + g.o_rv);
-    v.xa = reinterpret_cast<T*>(tsm + g.o_xa);
-    v.xb = reinterpret_cast<T*>(tsm + g.o_xb);
-    v.b = reinterpret_cast<T*>(tsm + g.o_b);
-    v.r = reinterpret_cast<T*>(tsm + g.o_r);
-    sl[threadIdx.x] = v;
-  }
-  if (threadIdx.x == 32) {
-    TailCoarse<T> c = C;
-    c.lu = reinterpret_cast<const double*>(tsm + C.o_lu);
-    c.piv = reinterpret_cast<const int*>(tsm + C.o_piv);
-    c.b = reinterpret_cast<T*>(tsm + C.o_b);
-    c.x = reinterpret_cast<T*>(tsm + C.o_x);
-    sc = c;
-  }
+  // the descriptors (sizes, ω, shared-memory offsets) into shared memory
+  if (threadIdx.x < nl) sl[threadIdx.x] = lv[threadIdx.x];
+  if (threadIdx.x == 32) sc = C;
   if (threadIdx.x == 0) ok = 1;
-  __syncthreads();  // barrier initialised, views published
+  __syncthreads();  // barrier initialised, descriptors published
   if (!mbar_wait_bounded(&bar, 0, kWaitLimit)) ok = 0;  // every thread observes the copies
   __syncthreads();
   if (!ok) {
@@ -1217,9 +1302,10 @@ k_coarse_tail(const TailLevel<T>* __restrict__ lv, int nl, TailCoarse<T> C, Tail
     }
     return;
   }
-  tail_visit(sl, 0, nl, sc, x_zero != 0, pre, post, wcycle);
+  tail_visit<0>(sl, nl, sc, x_zero != 0, pre, post, wcycle);
   // the top level's result back to global memory
-  for (int i = threadIdx.x; i < lv[0].n; i += blockDim.x) lv[0].xa[i] = sl[0].xa[i];
+  const T* xa0 = tail_sh<const T>(sl[0].o_xa);
+  for (int i = threadIdx.x; i < sl[0].n; i += blockDim.x) lv[0].xa[i] = xa0[i];
 }
 
 // Solve A^T y = b with the dgetf2 factors of A (A = P L U, column-major,

@@ -262,7 +262,10 @@ int32_t draugr_b200_level_op(int32_t handle, int32_t lvl, int32_t op, int32_t pr
                              const double *in1, const double *in2, double *out, int32_t steps);
 
 /* Mean device time of `reps` launches of a level kernel (op 2: one Jacobi
- * sweep, op 0: SpMV), measured with CUDA events on the hierarchy's stream. */
+ * sweep, op 0: SpMV, 3: restriction, 4: prolongation, 6: first sweep from
+ * zero fused with the residual), or of the V(1,1) cycle from level lvl >= 1
+ * down from a zero guess (op 8, the coarse tail included), measured with
+ * CUDA events on the hierarchy's stream. */
 int32_t draugr_b200_time_level_op(int32_t handle, int32_t lvl, int32_t op, int32_t precision,
                                   int32_t reps, float *ms_per_launch);
 
