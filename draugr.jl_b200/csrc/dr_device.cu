@@ -21,6 +21,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -613,16 +614,22 @@ static std::vector<int> bank_order(const std::vector<int>& rp) {
 }
 
 // Tail levels whose longest row exceeds this form their products flat
-// (TailLevel::p), in a shared-memory scratch of one value per nonzero.
+// (TailLevel::p), in a shared-memory scratch of one value per nonzero.  The
+// environment variable DRAUGR_B200_TAIL_FLAT_ROW overrides it (read at each
+// setup; a test hook: the results are the same either way).
 static constexpr int kTailFlatRow = 48;
+static int tail_flat_row() {
+  const char* e = std::getenv("DRAUGR_B200_TAIL_FLAT_ROW");
+  return e ? std::atoi(e) : kTailFlatRow;
+}
 
 template <typename T>
-static size_t tail_level_bytes(const DevLevel& d) {
+static size_t tail_level_bytes(const DevLevel& d, int flat_row) {
   const size_t n = d.A.n, nc = d.P.m, an = d.A.nnz, pn = d.P.nnz;
   return a16(4 * (n + 1)) + a16(4 * an) + a16(4 * n) + a16(sizeof(T) * an) + a16(sizeof(T) * n) +
          a16(4 * (n + 1)) + a16(4 * pn) + a16(sizeof(T) * pn) + a16(4 * (nc + 1)) + a16(4 * pn) +
          a16(sizeof(T) * pn) + 4 * a16(sizeof(T) * n) +
-         (d.A.maxlen > kTailFlatRow ? a16(sizeof(T) * an) : 0);
+         (d.A.maxlen > flat_row ? a16(sizeof(T) * an) : 0);
 }
 
 template <typename T>
@@ -656,13 +663,14 @@ static void allow_tail_smem() {
 
 void DevHier::build_tail() {
   const int nl = nlevels();
+  const int flat_row = tail_flat_row();
   tail_ = nl;
   size_t total = tail_coarse_bytes<double>(nc_);
   std::vector<std::vector<int>> ords;  // from the coarsest level up
   for (int l = nl - 1; l >= 1 && nl - l <= kern::kTailMaxLevels; --l) {
     const DevLevel& d = L_[l];
     const bool jac = jacobi_type(d.smoother);
-    total += tail_level_bytes<double>(d);
+    total += tail_level_bytes<double>(d, flat_row);
     if (!jac || d.A.n > 4096 || total > kTailSmem) break;
     std::vector<int> rp(d.A.n + 1);
     DR_CK(cudaMemcpy(rp.data(), d.A.rp, rp.size() * sizeof(int), cudaMemcpyDeviceToHost));
@@ -729,7 +737,7 @@ void DevHier::build_tail() {
       t.o_r = take(sizeof(T) * n);
       // the product scratch has no global source: p only marks it (the
       // kernel points p at shared memory)
-      const bool flat = d.A.maxlen > kTailFlatRow;
+      const bool flat = d.A.maxlen > flat_row;
       t.o_p = flat ? take(sizeof(T) * (size_t)d.A.nnz) : 0;
       t.p = flat ? reinterpret_cast<T*>(V.r) : nullptr;
     }

@@ -280,6 +280,45 @@ def test_cycle_bit_exact_when_all_rows_single_lane(fresh_case):
             assert np.array_equal(x, O.cycle(start, b, 1, 1, w))
 
 
+def test_tail_flat_products_bit_exact(monkeypatch):
+    """The coarse tail forms the products of levels with long rows flat over
+    the block and then sums each row in column order: the same rounded
+    products and sums, so the cycle still equals the oracle's bit for bit.
+    DRAUGR_B200_TAIL_FLAT_ROW=0 makes every tail level take that path."""
+    monkeypatch.setenv("DRAUGR_B200_TAIL_FLAT_ROW", "0")
+    checked = 0
+    for name in sorted(CASES):
+        make, cfg = CASES[name]
+        A = make()
+        h = draugr.amg_setup(A, cfg)
+        jac = all(int(h.level_info(l)[4]) in (0, 5) for l in range(h.nlevels))
+        single = all(all(_single_lane(h, l)) for l in range(h.nlevels))
+        if jac and single and h.nlevels >= 2:
+            O = oracle.OracleHierarchy(h)
+            n = A.shape[0]
+            b = np.random.default_rng(12).uniform(-1, 1, n)
+            for start in (np.zeros(n), np.random.default_rng(13).uniform(-1, 1, n)):
+                x = start.copy()
+                draugr.amg_cycle(x, b, h, cfg)
+                assert np.array_equal(x, O.cycle(start, b, 1, 1, False)), name
+            checked += 1
+        h.free()
+    assert checked >= 1
+
+
+def test_cycle_from_level_timing(case):
+    """draugr_b200_time_level_op op 8 times the V(1,1) cycle from a level
+    >= 1 down (the coarse tail included) and rejects the finest level."""
+    name, A, cfg, h, O = case
+    if h.nlevels < 2 or any(int(h.level_info(l)[4]) not in (0, 3, 5) for l in range(h.nlevels)):
+        pytest.skip("needs two levels with Jacobi-type smoothers")
+    for l in range(1, h.nlevels):
+        assert h.time_level_op(l, 8, 0, reps=2) > 0.0
+        assert h.time_level_op(l, 8, 1, reps=2) > 0.0
+    with pytest.raises(draugr.DraugrError, match="op 8"):
+        h.time_level_op(0, 8, 0, reps=2)
+
+
 def test_residual_entry_point(fresh_case):
     """draugr_b200_residual_device: r = b - A x and ||r|| on device vectors."""
     torch = pytest.importorskip("torch")
