@@ -428,7 +428,10 @@ DevHier::DevHier(const HostHierarchy& H, int device, const BatchLayout* batch) {
       DR_CK(cudaFuncSetAttribute(k_lu_solve<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
     }
     if (batch) tail_ = nl;  // no shared-memory tail: every level runs as its own launches
-    else build_tail();
+    else {
+      build_tail();
+      build_fused(H);
+    }
     DR_CK(cudaStreamSynchronize(st_));
   } catch (...) {
     for (void* p : allocs_) cudaFree(p);
@@ -532,6 +535,8 @@ template <> double* DevHier::coarse_x<double>() { return cx64_; }
 template <> float* DevHier::coarse_x<float>() { return cx32_; }
 template <> const double* DevHier::mval<double>(const DevMat& M) const { return M.v; }
 template <> const float* DevHier::mval<float>(const DevMat& M) const { return M.v32; }
+template <> const double* DevHier::qval<double>(const DevLevel& d) const { return d.q; }
+template <> const float* DevHier::qval<float>(const DevLevel& d) const { return d.q32; }
 template <> const double* DevHier::invd<double>(const DevLevel& L) const { return tr_ ? L.invdT : L.invd; }
 template <> const float* DevHier::invd<float>(const DevLevel& L) const { return tr_ ? L.invdT32 : L.invd32; }
 
@@ -559,6 +564,7 @@ void DevHier::ensure_fp32() {
       d.ilu_L32 = alloc<float>(d.A.nnz + 4);
       d.ilu_U32 = alloc<float>(d.A.nnz + 4);
     }
+    if (d.fuse_up) d.q32 = alloc<float>(d.AP.nnz + 4);
   }
   cb32_ = alloc<float>(nc_);
   cx32_ = alloc<float>(nc_);
@@ -793,6 +799,58 @@ void DevHier::build_tail() {
   if (fp32_) tail32_ = make(float());
 }
 
+// Levels that run the correction and the first post-smoothing step as one
+// pass over Q = P - ω·D⁻¹·(A P) (EpCorrectJacobi): below the finest level
+// and above the shared-memory tail, Jacobi-type smoothing, A's rows summed
+// in a tree (not the reference's column order, so no bit-exact level loses
+// it), and A·P no larger than A and P together.  A·P's values come from the
+// Galerkin product on the device (refreshed by every partial resetup).
+void DevHier::build_fused(const HostHierarchy& H) {
+  const int nl = nlevels();
+  for (int l = 1; l < std::min(nl, tail_); ++l) {
+    DevLevel& d = L_[l];
+    const HostLevel& h = H.levels[l];
+    if (!d.has_rap || !jacobi_type(d.smoother) || d.A.form.ordered) continue;
+    if (d.AP.nnz > d.A.nnz + d.P.nnz) continue;
+    // each P entry's position in AP's row (both rows sorted; P's pattern is
+    // inside AP's when A's diagonal is stored)
+    std::vector<int> pos(h.P.ci.size());
+    bool ok = true;
+    for (int i = 0; i < h.A.n && ok; ++i) {
+      int k = h.ap_rp[i];
+      const int ke = h.ap_rp[i + 1];
+      for (int t = h.P.rp[i]; t < h.P.rp[i + 1]; ++t) {
+        while (k < ke && h.ap_ci[k] < h.P.ci[t]) ++k;
+        if (k == ke || h.ap_ci[k] != h.P.ci[t]) {
+          ok = false;
+          break;
+        }
+        pos[t] = k;
+      }
+    }
+    if (!ok) continue;
+    d.pq_pos = alloc<int>(pos.size());
+    DR_CK(cudaMemcpy(d.pq_pos, pos.data(), pos.size() * sizeof(int), cudaMemcpyHostToDevice));
+    d.q = alloc<double>(d.AP.nnz + 4);
+    spgemm<double>(d.AP, d.A, d.P, d.AP.v, d.A.v, d.P.v, nullptr);
+    d.fuse_up = true;
+    build_q(d);
+  }
+}
+
+void DevHier::build_q(DevLevel& d) {
+  counted();
+  k_build_q<<<grid1d(d.A.n, max_grid_), kBlock, 0, st_>>>(d.A.n, d.AP.rp, d.AP.v, d.invd, d.omega, d.P.rp,
+                                                           d.P.v, d.pq_pos, d.q);
+  DR_CK(cudaGetLastError());
+  if (fp32_) {
+    if (!d.q32) d.q32 = alloc<float>(d.AP.nnz + 4);
+    counted();
+    k_convert<double, float><<<grid1d(d.AP.nnz, max_grid_), kBlock, 0, st_>>>(d.AP.nnz, d.q, d.q32);
+    DR_CK(cudaGetLastError());
+  }
+}
+
 void DevHier::refresh_fp32() {
   if (!fp32_) return;
   for (auto& d : L_) {
@@ -813,6 +871,10 @@ void DevHier::refresh_fp32() {
       k_convert<double, float><<<grid1d(d.A.nnz, max_grid_), kBlock, 0, st_>>>(d.A.nnz, d.ilu_L, d.ilu_L32);
       counted();
       k_convert<double, float><<<grid1d(d.A.nnz, max_grid_), kBlock, 0, st_>>>(d.A.nnz, d.ilu_U, d.ilu_U32);
+    }
+    if (d.fuse_up && d.q32) {
+      counted();
+      k_convert<double, float><<<grid1d(d.AP.nnz, max_grid_), kBlock, 0, st_>>>(d.AP.nnz, d.q, d.q32);
     }
     if (d.At.v32) {  // transposed copies (FP32 transposed cycles)
       counted();
@@ -1030,6 +1092,14 @@ T* DevHier::cycle_level(int l, T* x, const T* b, bool x_zero, const CycleOpts& o
     xn = coarse_x<T>();
     if (batch_) batch_coarse<T>(l + 1, bn, xn);
     else coarse_solve<T>(bn, xn);
+  }
+  if (L.fuse_up && !tr_ && o.post >= 1 && !rz_w) {
+    // correction and the first post-smoothing step in one pass over Q
+    // (EpCorrectJacobi; V.r holds b - A x from the way down)
+    launch_rows(st_, max_grid_, L.AP, qval<T>(L), XPlain<T>{xn},
+                EpCorrectJacobi<T>{x, V.r, invd<T>(L), om});
+    x = smooth<T>(l, x, b, o.post - 1, ext, rz_w, rz_first);
+    return x;
   }
   // prolongation and correction  x += P xc
   launch_rows(st_, max_grid_, L.P, mval<T>(L.P), XPlain<T>{xn}, EpAddTo<T>{x});
@@ -2049,6 +2119,15 @@ void DevHier::resetup_values(const double* v_dev) {
       counted();
       k_convert<float, double><<<grid1d(next.nnz, max_grid_), kBlock, 0, st_>>>(next.nnz, next.v32, next.v);
       DR_CK(cudaGetLastError());
+    }
+    if (d.fuse_up) {
+      // Q from this level's new A·P (widened when formed in FP32) and the
+      // inverse diagonal refreshed with the level's values above
+      if (l >= f64) {
+        counted();
+        k_convert<float, double><<<grid1d(d.AP.nnz, max_grid_), kBlock, 0, st_>>>(d.AP.nnz, d.AP.v32, d.AP.v);
+      }
+      build_q(d);
     }
     if (l + 1 < nl) upd_invd(L_[l + 1]);
   }

@@ -142,6 +142,14 @@ struct DevLevel {
   bool has_rap = false;
   DevMat AP;                 // pattern and values of A·P (partial resetup)
   SpgemmList ap_list, rap_list;  // product lists of A·P and Pᵀ·(AP), built on the first resetup
+  // Fused correction and first post-smoothing step (EpCorrectJacobi): Q =
+  // P - ω·D⁻¹·(A P) on AP's pattern, on levels where A·P has fewer entries
+  // than A and P together and A's rows are summed in a tree; pq_pos: each P
+  // entry's position in AP's row
+  bool fuse_up = false;
+  double* q = nullptr;
+  float* q32 = nullptr;
+  int* pq_pos = nullptr;
   DevMat At;                 // A^T (transposed cycles; built on first use)
   int* at_perm = nullptr;    // At value k = A value at_perm[k]
   double* invdT = nullptr;   // smoother diagonal of A^T
@@ -314,6 +322,7 @@ class DevHier {
   template <typename T> T* coarse_b();
   template <typename T> T* coarse_x();
   template <typename T> const T* mval(const DevMat& M) const;
+  template <typename T> const T* qval(const DevLevel& d) const;
   template <typename T> const T* invd(const DevLevel& L) const;
 
   // rz_w: when set (finest level only), the last Jacobi sweep also forms
@@ -335,6 +344,8 @@ class DevHier {
   void ensure_fp32();
   void refresh_fp32();
   void build_tail();
+  void build_fused(const HostHierarchy& H);
+  void build_q(DevLevel& d);  // Q from d.AP.v, d.P.v and d.invd (and its FP32 copy)
   // block (multi-right-hand-side) solves: per-level n x k buffers
   template <typename T>
   struct BlockVecs {
@@ -484,6 +495,8 @@ class DevHier {
 // Value and smoother-diagonal arrays by precision (defined in dr_device.cu).
 template <> const double* DevHier::mval<double>(const DevMat& M) const;
 template <> const float* DevHier::mval<float>(const DevMat& M) const;
+template <> const double* DevHier::qval<double>(const DevLevel& d) const;
+template <> const float* DevHier::qval<float>(const DevLevel& d) const;
 template <> const double* DevHier::invd<double>(const DevLevel& L) const;
 template <> const float* DevHier::invd<float>(const DevLevel& L) const;
 

@@ -243,6 +243,30 @@ struct EpAddTo {  // x += p xc, per entry                  (prolongation.jl:742-
   __device__ __forceinline__ double apply(int i, T v, const Pre&) const { x[i] = v; return 0.0; }
 };
 
+// Prolongation, correction and the first weighted-Jacobi post-smoothing
+// step in one pass.  With r = b - A x the residual of the iterate before the
+// correction (formed on the way down), the reference's two steps
+//   x' = x + P xc,  x_new = x' + (ω·invd)·(b - A x')
+// equal  x_new = x + (ω·invd)·r + Q xc  with  Q = P - ω·D⁻¹·(A P)
+// (src/prolongation.jl:742-760 then src/smoothers.jl:78-94, regrouped), so
+// the row kernel runs over Q (the pattern of A·P) and gathers only the
+// coarse vector.  x is updated in place: row i reads and writes only x_i.
+template <typename T>
+struct EpCorrectJacobi {
+  using acc_t = T;
+  static constexpr int kSign = 1;
+  struct Pre { T base; };
+  T* __restrict__ x;
+  const T* __restrict__ r;
+  const T* __restrict__ invd;
+  T omega;
+  __device__ __forceinline__ Pre pre(int i) const {
+    return {add_rn(x[i], mul_rn(mul_rn(omega, __ldg(invd + i)), __ldg(r + i)))};
+  }
+  __device__ __forceinline__ T init(const Pre& p) const { return p.base; }
+  __device__ __forceinline__ double apply(int i, T v, const Pre&) const { x[i] = v; return 0.0; }
+};
+
 template <typename T>
 struct EpPcgDir {  // q = A p, p_new = z + β p_old, returns p_new·q
   using acc_t = double;
@@ -796,6 +820,20 @@ __global__ void k_lin3(int n, double a, const double* x, double b, const double*
 // Gradient of a loss L(x), x = A^-1 b, with respect to the nonzeros of A,
 // given the adjoint lambda = A^-T dL/dx:  dL/da_ij = -lambda_i x_j, in CSR
 // order.
+// Q = P - (ω·invd_i)·(A P) on the pattern of A P (see EpCorrectJacobi):
+// q_k = -(ω·invd_i)·ap_k over row i, then each P entry added at its
+// position pos[p] in that row: q = p - (ω·invd)·ap, rounded once each.
+__global__ void k_build_q(int n, const int* __restrict__ ap_rp, const double* __restrict__ ap_v,
+                          const double* __restrict__ invd, double omega, const int* __restrict__ p_rp,
+                          const double* __restrict__ p_v, const int* __restrict__ pos,
+                          double* __restrict__ q) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double w = __dmul_rn(omega, invd[i]);
+    for (int k = ap_rp[i]; k < ap_rp[i + 1]; ++k) q[k] = -__dmul_rn(w, ap_v[k]);
+    for (int t = p_rp[i]; t < p_rp[i + 1]; ++t) q[pos[t]] = __dadd_rn(q[pos[t]], p_v[t]);
+  }
+}
+
 __global__ void k_nz_grad(int n, const int* __restrict__ rp, const int* __restrict__ ci,
                           const double* __restrict__ x, const double* __restrict__ lam,
                           double* __restrict__ grad) {
