@@ -840,8 +840,8 @@ void DevHier::build_fused(const HostHierarchy& H) {
 
 void DevHier::build_q(DevLevel& d) {
   counted();
-  k_build_q<<<grid1d(d.A.n, max_grid_), kBlock, 0, st_>>>(d.A.n, d.AP.rp, d.AP.v, d.invd, d.omega, d.P.rp,
-                                                           d.P.v, d.pq_pos, d.q);
+  k_build_q<<<grid1d(32LL * d.A.n, max_grid_), kBlock, 0, st_>>>(d.A.n, d.AP.rp, d.AP.v, d.invd, d.omega,
+                                                                 d.P.rp, d.P.v, d.pq_pos, d.q);
   DR_CK(cudaGetLastError());
   if (fp32_) {
     if (!d.q32) d.q32 = alloc<float>(d.AP.nnz + 4);

@@ -823,14 +823,20 @@ __global__ void k_lin3(int n, double a, const double* x, double b, const double*
 // Q = P - (ω·invd_i)·(A P) on the pattern of A P (see EpCorrectJacobi):
 // q_k = -(ω·invd_i)·ap_k over row i, then each P entry added at its
 // position pos[p] in that row: q = p - (ω·invd)·ap, rounded once each.
-__global__ void k_build_q(int n, const int* __restrict__ ap_rp, const double* __restrict__ ap_v,
-                          const double* __restrict__ invd, double omega, const int* __restrict__ p_rp,
-                          const double* __restrict__ p_v, const int* __restrict__ pos,
-                          double* __restrict__ q) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+// One warp per row (the row's P entries have distinct positions).
+__global__ void __launch_bounds__(kBlock)
+k_build_q(int n, const int* __restrict__ ap_rp, const double* __restrict__ ap_v,
+          const double* __restrict__ invd, double omega, const int* __restrict__ p_rp,
+          const double* __restrict__ p_v, const int* __restrict__ pos, double* __restrict__ q) {
+  const int lane = threadIdx.x & 31;
+  const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long i = w0; i < n; i += nw) {
     const double w = __dmul_rn(omega, invd[i]);
-    for (int k = ap_rp[i]; k < ap_rp[i + 1]; ++k) q[k] = -__dmul_rn(w, ap_v[k]);
-    for (int t = p_rp[i]; t < p_rp[i + 1]; ++t) q[pos[t]] = __dadd_rn(q[pos[t]], p_v[t]);
+    for (int k = ap_rp[i] + lane; k < ap_rp[i + 1]; k += 32) q[k] = -__dmul_rn(w, ap_v[k]);
+    __syncwarp();
+    for (int t = p_rp[i] + lane; t < p_rp[i + 1]; t += 32) q[pos[t]] = __dadd_rn(q[pos[t]], p_v[t]);
+    __syncwarp();
   }
 }
 
