@@ -101,7 +101,25 @@ HostHierarchy merge_batch(const std::vector<const HostHierarchy*>& hs, BatchLayo
     L.T = build_transpose_map(L.P);
     L.Rv.resize(L.P.nnz());
     for (size_t k = 0; k < L.T.pnz.size(); ++k) L.Rv[k] = L.P.v[L.T.pnz[k]];
+    // the pattern of A·P, block-diagonal like P, when every system keeps
+    // its own: it carries the fused correction on the way up (a batch has
+    // no partial resetup, so has_rap_map stays false)
     L.has_rap_map = false;
+    bool all_ap = true;
+    for (int s = 0; s < ns; ++s)
+      if (lay.depth[s] > l && !hs[s]->levels[l].has_rap_map) all_ap = false;
+    if (all_ap) {
+      L.ap_rp.assign(1, 0);
+      for (int s = 0; s < ns; ++s) {
+        if (lay.depth[s] <= l) continue;
+        const HostLevel& h = hs[s]->levels[l];
+        const int co = lay.off[l + 1][s];
+        for (int i = 0; i < h.A.n; ++i) {
+          for (int k = h.ap_rp[i]; k < h.ap_rp[i + 1]; ++k) L.ap_ci.push_back(h.ap_ci[k] + co);
+          L.ap_rp.push_back((int)L.ap_ci.size());
+        }
+      }
+    }
   }
   M.nc = lay.ntotal[lmax];
   M.coarse.n = M.coarse.m = M.nc;

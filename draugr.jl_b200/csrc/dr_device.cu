@@ -319,7 +319,7 @@ DevHier::DevHier(const HostHierarchy& H, int device, const BatchLayout* batch) {
         h2d(d.color_order, h.color_order, st_);
       }
       d.has_rap = h.has_rap_map;
-      if (d.has_rap) up_csr(d.AP, h.A.n, h.P.nc, h.ap_rp, h.ap_ci, nullptr);
+      if (d.has_rap || !h.ap_rp.empty()) up_csr(d.AP, h.A.n, h.P.nc, h.ap_rp, h.ap_ci, nullptr);
 
       const int n = d.nv;
       if (l > 0) {
@@ -428,10 +428,8 @@ DevHier::DevHier(const HostHierarchy& H, int device, const BatchLayout* batch) {
       DR_CK(cudaFuncSetAttribute(k_lu_solve<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
     }
     if (batch) tail_ = nl;  // no shared-memory tail: every level runs as its own launches
-    else {
-      build_tail();
-      build_fused(H);
-    }
+    else build_tail();
+    build_fused(H);
     DR_CK(cudaStreamSynchronize(st_));
   } catch (...) {
     for (void* p : allocs_) cudaFree(p);
@@ -804,13 +802,14 @@ void DevHier::build_tail() {
 // and above the shared-memory tail, Jacobi-type smoothing, A's rows summed
 // in a tree (not the reference's column order, so no bit-exact level loses
 // it), and A·P no larger than A and P together.  A·P's values come from the
-// Galerkin product on the device (refreshed by every partial resetup).
+// Galerkin product on the device (refreshed by every partial resetup); a
+// batch's A·P is the systems' patterns merged block-diagonally.
 void DevHier::build_fused(const HostHierarchy& H) {
   const int nl = nlevels();
   for (int l = 1; l < std::min(nl, tail_); ++l) {
     DevLevel& d = L_[l];
     const HostLevel& h = H.levels[l];
-    if (!d.has_rap || !jacobi_type(d.smoother) || d.A.form.ordered) continue;
+    if (d.AP.n == 0 || !jacobi_type(d.smoother) || d.A.form.ordered) continue;
     if (d.AP.nnz > d.A.nnz + d.P.nnz) continue;
     // each P entry's position in AP's row (both rows sorted; P's pattern is
     // inside AP's when A's diagonal is stored)
