@@ -39,10 +39,13 @@ __device__ __forceinline__ float rn_add(float a, float b) { return __fadd_rn(a, 
 __device__ __forceinline__ double rn_sub(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ float rn_sub(float a, float b) { return __fsub_rn(a, b); }
 
-enum : int { BM_STORE = 0, BM_RESID = 1, BM_JACOBI = 2, BM_ADDTO = 3 };
+enum : int { BM_STORE = 0, BM_RESID = 1, BM_JACOBI = 2, BM_ADDTO = 3, BM_CORRECT = 4 };
 
 // Y = A X (STORE), Y = B - A X (RESID), Y = X + (omega d)(B - A X)
-// (JACOBI), Y += A X (ADDTO, A = P), for k columns.
+// (JACOBI), Y += A X (ADDTO, A = P), Y = Y + (omega d) B + A X (CORRECT:
+// A = Q = P - omega D^-1 (A P), B = the residual of Y formed on the way
+// down, X = the coarse correction; the fused correction and first
+// post-smoothing step), for k columns.
 template <typename TA, typename T, int MODE>
 __global__ void __launch_bounds__(kBlock)
 k_spmm(int nrows, int k, const int* __restrict__ rp, const int* __restrict__ ci, const TA* __restrict__ av,
@@ -57,6 +60,8 @@ k_spmm(int nrows, int k, const int* __restrict__ rp, const int* __restrict__ ci,
     if (col) {
       if (MODE == BM_ADDTO) acc = Y[(size_t)row * k + lane];
       if (MODE == BM_JACOBI) acc = B[(size_t)row * k + lane];
+      if (MODE == BM_CORRECT)
+        acc = rn_add(Y[(size_t)row * k + lane], rn_mul(rn_mul(omega, dinv[row]), B[(size_t)row * k + lane]));
     }
     for (int k0 = rs; k0 < re; k0 += 32) {
       const int my = k0 + lane;
@@ -163,7 +168,14 @@ k_spmm_vec(int nrows, int k, const int* __restrict__ rp, const int* __restrict__
     T acc[V];
     if (MODE == BM_ADDTO) VV::get(*reinterpret_cast<const VT*>(Y + o), acc);
     else if (MODE == BM_JACOBI) VV::get(*reinterpret_cast<const VT*>(B + o), acc);
-    else
+    else if (MODE == BM_CORRECT) {
+      T yv[V], bv[V];
+      VV::get(*reinterpret_cast<const VT*>(Y + o), yv);
+      VV::get(*reinterpret_cast<const VT*>(B + o), bv);
+      const T sc = rn_mul(omega, dinv[row]);
+#pragma unroll
+      for (int q = 0; q < V; ++q) acc[q] = rn_add(yv[q], rn_mul(sc, bv[q]));
+    } else
 #pragma unroll
       for (int q = 0; q < V; ++q) acc[q] = T(0);
     // the row's lanes load up to TPR (column, value) pairs at once and pass
@@ -629,8 +641,8 @@ void DevHier::tune_block(int k, int verbose) {
   cudaEvent_t e0, e1;
   DR_CK(cudaEventCreate(&e0));
   DR_CK(cudaEventCreate(&e1));
-  static const char* kOpName[4] = {"A x (Jacobi)", "b - A x", "P^T r", "x + P x_c"};
-  static const int kOpMode[4] = {BM_JACOBI, BM_RESID, BM_STORE, BM_ADDTO};
+  static const char* kOpName[5] = {"A x (Jacobi)", "b - A x", "P^T r", "x + P x_c", "x + Q x_c"};
+  static const int kOpMode[5] = {BM_JACOBI, BM_RESID, BM_STORE, BM_ADDTO, BM_CORRECT};
   const int nl = nlevels();
   for (int l = 0; l < nl; ++l) {
     DevLevel& L = L_[l];
@@ -661,13 +673,17 @@ void DevHier::tune_block(int k, int verbose) {
           spmm<T, T, BM_STORE>(st_, max_grid_, R.n, k, R.rp, R.ci, mval<T>(R), W.r, nullptr, nullptr, T(0), bc,
                                nullptr, sh);
           break;
-        default:  // x += P x_c with x_c = 0 leaves x at zero
+        case 3:  // x += P x_c with x_c = 0 leaves x at zero
           spmm<T, T, BM_ADDTO>(st_, max_grid_, P.n, k, P.rp, P.ci, mval<T>(P), xc, nullptr, nullptr, T(0), W.x,
                                nullptr, sh);
+          break;
+        default:  // the fused correction, with r = 0 and x_c = 0 (x stays zero)
+          spmm<T, T, BM_CORRECT>(st_, max_grid_, L.AP.n, k, L.AP.rp, L.AP.ci, qval<T>(L), xc, W.r, dinv, om,
+                                 W.x, nullptr, sh);
       }
     };
-    const void* rps[4] = {A.rp, A.rp, R.rp, P.rp};
-    for (int op = 0; op < 4; ++op) {
+    const void* rps[5] = {A.rp, A.rp, R.rp, P.rp, L.AP.rp};
+    for (int op = 0; op < (L.fuse_up ? 5 : 4); ++op) {
       float best = 0.f, def = 0.f;
       BlockShape pick{};
       for (size_t c = 0; c < cand.size(); ++c) {
@@ -770,10 +786,19 @@ T* DevHier::cycle_block(int l, T* X, const T* B, bool x_zero, const CycleOpts& o
     }
   }
   const DevMat& P = L.P;
+  int post0 = 0;
   note_launch();
-  spmm<T, T, BM_ADDTO>(st_, max_grid_, P.n, k, P.rp, P.ci, mval<T>(P), xc, nullptr, nullptr, T(0), x, nullptr,
-                       shape_of(P.rp, BM_ADDTO, sizeof(T), k));
-  for (int s = 0; s < o.post; ++s) {
+  if (L.fuse_up && o.post >= 1) {
+    // correction and the first post-smoothing step in one pass over Q (see
+    // EpCorrectJacobi; V.r holds B - A x from the way down)
+    spmm<T, T, BM_CORRECT>(st_, max_grid_, L.AP.n, k, L.AP.rp, L.AP.ci, qval<T>(L), xc, V.r, dinv, om, x,
+                           nullptr, shape_of(L.AP.rp, BM_CORRECT, sizeof(T), k));
+    post0 = 1;
+  } else {
+    spmm<T, T, BM_ADDTO>(st_, max_grid_, P.n, k, P.rp, P.ci, mval<T>(P), xc, nullptr, nullptr, T(0), x, nullptr,
+                         shape_of(P.rp, BM_ADDTO, sizeof(T), k));
+  }
+  for (int s = post0; s < o.post; ++s) {
     note_launch();
     spmm<T, T, BM_JACOBI>(st_, max_grid_, n, k, A.rp, A.ci, av, x, B, dinv, om, t, nullptr, sj);
     std::swap(x, t);
