@@ -385,13 +385,7 @@ def run_ours(args, world, rank, local):
 
     # the whole V-cycle: algorithmic bytes of the kernels one FP64 V(1,1)
     # cycle launches, per level, against the cycle's event-timed duration
-    vc_bytes = 0
-    for l in range(h.nlevels):
-        info = h.level_info(l)
-        ln, lnnz, lnc, lnnzp = int(info[0]), int(info[1]), int(info[2]), int(info[3])
-        resid = lnnz * 12 + 4 * (ln + 1) + 3 * ln * 8
-        vc_bytes += resid + op_bytes(3, 0, ln, lnnz, lnc, lnnzp) + op_bytes(4, 0, ln, lnnz, lnc, lnnzp)
-        vc_bytes += op_bytes(2, 0, ln, lnnz, lnc, lnnzp) * (2 if l == 0 else 1)
+    vc_bytes = vcycle_bytes(h)
     xc = torch.zeros(n, dtype=torch.float64, device=dev)
     for _ in range(3):
         draugr.amg_cycle(xc, bd, h, cfg)
@@ -436,6 +430,36 @@ def run_ours(args, world, rank, local):
     return out
 
 
+def vcycle_bytes(h):
+    """Algorithmic bytes of one FP64 V(1,1) cycle (the reference's passes):
+    per level the residual (12 nnz + 4 (n+1) + 24 n), restriction,
+    prolongation and Jacobi sweep formulas, two sweeps on the finest level."""
+    total = 0
+    for l in range(h.nlevels):
+        info = h.level_info(l)
+        ln, lnnz, lnc, lnnzp = int(info[0]), int(info[1]), int(info[2]), int(info[3])
+        resid = lnnz * 12 + 4 * (ln + 1) + 3 * ln * 8
+        total += resid + op_bytes(3, 0, ln, lnnz, lnc, lnnzp) + op_bytes(4, 0, ln, lnnz, lnc, lnnzp)
+        total += op_bytes(2, 0, ln, lnnz, lnc, lnnzp) * (2 if l == 0 else 1)
+    return total
+
+
+def cpu_vcycle(h, b, cfg, reps=3):
+    """The oracle's FP64 V(1,1) cycle on the host cores: mean seconds per
+    cycle (one warm-up) and the same algorithmic GB/s as the GPU cycle."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+
+    O = oracle.OracleHierarchy(h)
+    x0 = np.random.default_rng(7).uniform(-1, 1, len(b))
+    O.cycle(x0, b, cfg.pre_smoothing_steps, cfg.post_smoothing_steps, cfg.cycle_type == "W")
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        O.cycle(x0, b, cfg.pre_smoothing_steps, cfg.post_smoothing_steps, cfg.cycle_type == "W")
+    t = (time.perf_counter() - t0) / reps
+    return t, vcycle_bytes(h) / t / 1e9
+
+
 def cpu_solve_time(h, b, cfg, reps=1):
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle
@@ -454,8 +478,9 @@ def cpu_solve_time(h, b, cfg, reps=1):
 
 def cpu_baseline(h, b, cfg):
     t, its = cpu_solve_time(h, b, cfg)
+    vt, vg = cpu_vcycle(h, b, cfg)
     return {"value": t, "unit": "s", "cores": os.cpu_count(), "kind": "port",
-            "iterations": its,
+            "iterations": its, "vcycle_ms": round(vt * 1e3, 2), "vcycle_GBps": round(vg, 1),
             "sample": "one full AMG-PCG solve (FP64 cycle) of the same system and hierarchy "
                       "to 1e-8, oracle restatement of the reference's CPU kernels, OpenMP "
                       "static/64-row chunks on all host threads"}
@@ -512,6 +537,13 @@ def run_reference(args, world, rank):
     rp, ci, av = S.export(0, "A_rowptr"), S.export(0, "A_colval"), S.export(0, "A_nzval")
     rr = float(np.linalg.norm(oracle.residual(nrows, rp, ci, av, x, b)) / np.linalg.norm(b))
     v = float(np.mean(times))
+    # one V-cycle on the host cores, with the GPU cycle's algorithmic bytes
+    x0 = np.random.default_rng(7).uniform(-1, 1, nrows)
+    O.cycle(x0, b, pre, post, w)
+    t0 = time.perf_counter()
+    for _ in range(3):
+        O.cycle(x0, b, pre, post, w)
+    vt = (time.perf_counter() - t0) / 3
     sample = ("full AMG-PCG solve per step (FP64 cycle), oracle restatement of Draugr.jl's "
               "CPU kernels (Julia is not available), OpenMP on all host threads")
     return {"metric": METRIC, "impl": "reference", "value": v, "unit": "s", "n_gpus": world,
@@ -526,7 +558,8 @@ def run_reference(args, world, rank):
                          "process (bench.py --write-structure); this process loads only the oracle",
             "loaded_repo_libraries": repo_libraries(),
             "cpu_baseline": {"value": v, "unit": "s", "cores": os.cpu_count(), "kind": "port",
-                             "sample": sample},
+                             "sample": sample, "vcycle_ms": round(vt * 1e3, 2),
+                             "vcycle_GBps": round(vcycle_bytes(S) / vt / 1e9, 1)},
             "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
