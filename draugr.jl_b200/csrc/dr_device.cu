@@ -255,7 +255,7 @@ struct FinStore2 {
 // ticket slots
 enum : int { TK_DOT = 0, TK_RES = 1, TK_PQ = 2, TK_UPD = 3, TK_RZ = 4, TK_N = 8 };
 // scalar slots
-enum : int { SC_BB = 0, SC_RR = 1, SC_RZ = 2, SC_RZOLD = 3, SC_PQ = 4, SC_TMP = 5, SC_N = 8 };
+enum : int { SC_BB = 0, SC_RR = 1, SC_RZ = 2, SC_RZOLD = 3, SC_PQ = 4, SC_TMP = 5, SC_ALPHA = 6, SC_N = 8 };
 
 }  // namespace
 
@@ -293,6 +293,9 @@ DevHier::DevHier(const HostHierarchy& H, int device, const BatchLayout* batch) {
   own_stream_ = true;
   DR_CK(cudaEventCreateWithFlags(&ev_[0], cudaEventDisableTiming));
   DR_CK(cudaEventCreateWithFlags(&ev_[1], cudaEventDisableTiming));
+  DR_CK(cudaStreamCreateWithFlags(&side_st_, cudaStreamNonBlocking));
+  DR_CK(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
+  DR_CK(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
   try {
     const int nl = (int)H.levels.size();
     n0_ = nl ? H.levels[0].A.n : H.nc;
@@ -437,6 +440,9 @@ DevHier::DevHier(const HostHierarchy& H, int device, const BatchLayout* batch) {
     if (hscal_) cudaFreeHost(hscal_);
     cudaEventDestroy(ev_[0]);
     cudaEventDestroy(ev_[1]);
+    cudaEventDestroy(ev_fork_);
+    cudaEventDestroy(ev_join_);
+    cudaStreamDestroy(side_st_);
     cudaStreamDestroy(own_st_);
     throw;
   }
@@ -492,6 +498,9 @@ DevHier::~DevHier() {
   if (hscal_) cudaFreeHost(hscal_);
   cudaEventDestroy(ev_[0]);
   cudaEventDestroy(ev_[1]);
+  if (ev_fork_) cudaEventDestroy(ev_fork_);
+  if (ev_join_) cudaEventDestroy(ev_join_);
+  if (side_st_) cudaStreamDestroy(side_st_);
   if (own_stream_ && own_st_) cudaStreamDestroy(own_st_);
 }
 
@@ -520,7 +529,8 @@ void DevHier::set_stream(cudaStream_t s) {
 void DevHier::graphs_clear() {
   for (int i = 0; i < 2; ++i)
     if (pg_.g1[i]) { cudaGraphExecDestroy(pg_.g1[i]); pg_.g1[i] = nullptr; }
-  if (pg_.g2) { cudaGraphExecDestroy(pg_.g2); pg_.g2 = nullptr; }
+  for (int i = 0; i < 2; ++i)
+    if (pg_.g2[i]) { cudaGraphExecDestroy(pg_.g2[i]); pg_.g2[i] = nullptr; }
   pg_.valid = false;
 }
 
@@ -1732,11 +1742,15 @@ double DevHier::residual_norm(const double* x, const double* b, double* r) {
 // products are FP64; with `mixed` the cycle runs on FP32 copies of the
 // hierarchy values and vectors.  Per iteration:
 //   K1  q = A p,  p = z + β p_old (on the fly),  p·q       (one pass over A)
-//   K2  x += α p, r -= α q, r·r (and the FP32 copy of r)    (one vector pass)
+//   K2  r -= α q, r·r (and the FP32 copy of r), α stored    (one vector pass)
 //   M   z = M r                                              (the cycle)
-//   D   r·z                                                  (one vector pass)
-// K1+K2 and M+D are captured once as CUDA graphs; the host reads r·r of
-// iteration k while the preconditioner of iteration k runs.
+//   D   r·z                                                  (fused into M's last sweep)
+//   X   x += α p                                             (beside M)
+// K1+K2 and M+D+X are captured once as CUDA graphs (two of each, for the
+// alternating direction buffers); X is a forked branch of the second, so
+// the iterate's update runs while the cycle's latency-bound coarse levels
+// leave bandwidth free.  The host reads r·r of iteration k while the
+// preconditioner of iteration k runs.
 int DevHier::pcg(double* x, const double* b, const CycleOpts& o, double tol, int maxiter, bool mixed,
                  double* relres, int verbose) {
   if (mixed) ensure_fp32();
@@ -1838,19 +1852,19 @@ int DevHier::pcg(double* x, const double* b, const CycleOpts& o, double tol, int
       launch_rows_dot(st_, max_grid_, A, A.v, dir, EpPcgDir<float>{dir, pnew, pq_}, partials_,
                       tickets_ + TK_PQ, FinStore{scal_ + SC_PQ});
       counted();
-      launch_dependent(k_pcg_update<float>, grid1d(n, max_grid_), kBlock, 0, st_, n, X, pr_,
+      launch_dependent(k_pcg_update<float>, grid1d(n, max_grid_), kBlock, 0, st_, n, (double*)nullptr, pr_,
                        (const double*)pnew, (const double*)pq_, (const double*)(scal_ + SC_RZ),
-                       (const double*)(scal_ + SC_PQ), pr32_, partials_, tickets_ + TK_UPD,
-                       FinStore{scal_ + SC_RR});
+                       (const double*)(scal_ + SC_PQ), pr32_, scal_ + SC_ALPHA, partials_,
+                       tickets_ + TK_UPD, FinStore{scal_ + SC_RR});
     } else {
       XPcgDir<double> dir{(const double*)zptr, pold, scal_ + SC_RZ, 0.0};
       launch_rows_dot(st_, max_grid_, A, A.v, dir, EpPcgDir<double>{dir, pnew, pq_}, partials_,
                       tickets_ + TK_PQ, FinStore{scal_ + SC_PQ});
       counted();
-      launch_dependent(k_pcg_update<float>, grid1d(n, max_grid_), kBlock, 0, st_, n, X, pr_,
+      launch_dependent(k_pcg_update<float>, grid1d(n, max_grid_), kBlock, 0, st_, n, (double*)nullptr, pr_,
                        (const double*)pnew, (const double*)pq_, (const double*)(scal_ + SC_RZ),
-                       (const double*)(scal_ + SC_PQ), (float*)nullptr, partials_, tickets_ + TK_UPD,
-                       FinStore{scal_ + SC_RR});
+                       (const double*)(scal_ + SC_PQ), (float*)nullptr, scal_ + SC_ALPHA, partials_,
+                       tickets_ + TK_UPD, FinStore{scal_ + SC_RR});
     }
     DR_CK(cudaGetLastError());
     DR_CK(cudaMemcpyAsync(hscal_ + SC_RR, scal_ + SC_RR, sizeof(double), cudaMemcpyDeviceToHost, st_));
@@ -1868,15 +1882,26 @@ int DevHier::pcg(double* x, const double* b, const CycleOpts& o, double tol, int
       DR_CK(cudaGraphInstantiate(&pg_.g1[par], g, 0));
       cudaGraphDestroy(g);
     }
-    cudaGraph_t g;
-    const long long c0 = g_launches.load();
-    DR_CK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
-    precond(false);
-    DR_CK(cudaStreamEndCapture(st_, &g));
-    pg_.n2 = g_launches.load() - c0;
-    g_launches.fetch_sub(pg_.n2);
-    DR_CK(cudaGraphInstantiate(&pg_.g2, g, 0));
-    cudaGraphDestroy(g);
+    for (int par = 0; par < 2; ++par) {
+      // the preconditioner, and beside it (a forked branch) x += α p with
+      // the direction of the iteration just finished
+      cudaGraph_t g;
+      const long long c0 = g_launches.load();
+      DR_CK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+      DR_CK(cudaEventRecord(ev_fork_, st_));
+      DR_CK(cudaStreamWaitEvent(side_st_, ev_fork_, 0));
+      counted();
+      k_pcg_x<<<grid1d(n, max_grid_), kBlock, 0, side_st_>>>(n, X, pp_[par ^ 1], scal_ + SC_ALPHA);
+      DR_CK(cudaGetLastError());
+      DR_CK(cudaEventRecord(ev_join_, side_st_));
+      precond(false);
+      DR_CK(cudaStreamWaitEvent(st_, ev_join_, 0));
+      DR_CK(cudaStreamEndCapture(st_, &g));
+      pg_.n2[par] = g_launches.load() - c0;
+      g_launches.fetch_sub(pg_.n2[par]);
+      DR_CK(cudaGraphInstantiate(&pg_.g2[par], g, 0));
+      cudaGraphDestroy(g);
+    }
     pg_.valid = true;
     pg_.mixed = mixed;
     pg_.o = o;
@@ -1889,8 +1914,12 @@ int DevHier::pcg(double* x, const double* b, const CycleOpts& o, double tol, int
     DR_CK(cudaEventRecord(ev_[par], st_));
     const bool more = it < maxiter;
     if (more) {
-      DR_CK(cudaGraphLaunch(pg_.g2, st_));
-      g_launches.fetch_add(pg_.n2);
+      DR_CK(cudaGraphLaunch(pg_.g2[par], st_));  // also x += α p of this iteration
+      g_launches.fetch_add(pg_.n2[par]);
+    } else {
+      counted();
+      k_pcg_x<<<grid1d(n, max_grid_), kBlock, 0, st_>>>(n, X, pp_[par ^ 1], scal_ + SC_ALPHA);
+      DR_CK(cudaGetLastError());
     }
     DR_CK(cudaEventSynchronize(ev_[par]));
     rel = std::sqrt(hscal_[SC_RR]) / bnorm;

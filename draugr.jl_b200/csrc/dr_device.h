@@ -483,11 +483,15 @@ class DevHier {
     bool valid = false;
     bool mixed = false;
     CycleOpts o;
-    cudaGraphExec_t g1[2] = {nullptr, nullptr};  // direction + update
-    cudaGraphExec_t g2 = nullptr;                // preconditioner + r·z
-    long long n1[2] = {0, 0}, n2 = 0;            // kernels per graph
+    cudaGraphExec_t g1[2] = {nullptr, nullptr};  // direction + update of r
+    cudaGraphExec_t g2[2] = {nullptr, nullptr};  // preconditioner + r·z, beside it x += α p
+    long long n1[2] = {0, 0}, n2[2] = {0, 0};    // kernels per graph
   } pg_;
   cudaEvent_t ev_[2] = {nullptr, nullptr};
+  // a second stream and two events, to fork and join a branch of a graph
+  // capture (the PCG iterate update beside the preconditioner)
+  cudaStream_t side_st_ = nullptr;
+  cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
 
   friend struct DevHierAccess;
 };

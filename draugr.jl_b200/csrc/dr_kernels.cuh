@@ -897,24 +897,37 @@ k_maxpy(int n, int k, const double* __restrict__ V, long long ld, const double* 
   }
 }
 
-// x += α p ; r -= α q ; rr = r·r ; optional r32 copy.  α = rz / pq.
+// r -= α q ; rr = r·r ; optional r32 copy; α = rz / pq, also stored at
+// alpha_out for k_pcg_x.  With x set it also updates x += α p (one pass);
+// with x null the iterate is left to k_pcg_x, which the PCG graph runs
+// beside the preconditioner (x is not on the iteration's critical path).
 template <typename TR32>
 __global__ void __launch_bounds__(kBlock)
 k_pcg_update(int n, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
              const double* __restrict__ q, const double* __restrict__ rz, const double* __restrict__ pq,
-             TR32* __restrict__ r32, double* partials, unsigned* ticket, FinStore fin) {
+             TR32* __restrict__ r32, double* alpha_out, double* partials, unsigned* ticket, FinStore fin) {
   pdl_trigger();
   pdl_wait();
   const double alpha = __ldg(rz) / __ldg(pq);
+  if (alpha_out && blockIdx.x == 0 && threadIdx.x == 0) *alpha_out = alpha;
   double s = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    x[i] += alpha * p[i];
+    if (x) x[i] += alpha * p[i];
     double ri = r[i] - alpha * q[i];
     r[i] = ri;
     if (r32) r32[i] = (TR32)ri;
     s += ri * ri;
   }
   grid_sum_finalize(s, partials, ticket, fin);
+}
+
+// x += α p with α from k_pcg_update (the same expression, so the same
+// values as the one-pass update).
+__global__ void __launch_bounds__(kBlock)
+k_pcg_x(int n, double* __restrict__ x, const double* __restrict__ p, const double* __restrict__ alpha_p) {
+  const double alpha = __ldg(alpha_p);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    x[i] += alpha * p[i];
 }
 
 // ------------------------------------------------------------ coarsest level
