@@ -692,6 +692,12 @@ void DevHier::build_tail() {
     tail_ = l;
   }
   if (tail_ >= nl) return;
+  {
+    bool any_tree = false;
+    for (int l = 0; l < nl; ++l) any_tree = any_tree || !L_[l].A.form.ordered;
+    tail_inv_ = any_tree && nc_ >= 1 && nc_ <= 32;
+    if (tail_inv_) build_cinv();
+  }
   const int cnt = nl - tail_;
   std::reverse(ords.begin(), ords.end());  // tail_ first
   std::vector<int*> ord_dev(cnt);
@@ -782,7 +788,7 @@ void DevHier::build_tail() {
       rec(val, t.o_pv, t.pv, sizeof(T) * (size_t)t.pnnz);
       rec(val, t.o_rv, t.rv, sizeof(T) * (size_t)t.pnnz);
     }
-    rec(val, tail_co_[slot][0], clu_, 8 * (size_t)nc_ * nc_);
+    rec(val, tail_co_[slot][0], tail_inv_ ? cinv_ : clu_, 8 * (size_t)nc_ * nc_);
     rec(val, tail_co_[slot][1], cpiv_, 4 * (size_t)nc_);
     rec(val, v[0].o_b, v[0].b, sizeof(T) * (size_t)v[0].n);
     TailCopyList& cl = tail_cp_[slot];
@@ -858,6 +864,13 @@ void DevHier::build_q(DevLevel& d) {
     k_convert<double, float><<<grid1d(d.AP.nnz, max_grid_), kBlock, 0, st_>>>(d.AP.nnz, d.q, d.q32);
     DR_CK(cudaGetLastError());
   }
+}
+
+void DevHier::build_cinv() {
+  if (!cinv_) cinv_ = alloc<double>((size_t)nc_ * nc_);
+  counted();
+  k_lu_inverse<<<1, 32, 0, st_>>>(nc_, clu_, cpiv_, cinv_);
+  DR_CK(cudaGetLastError());
 }
 
 void DevHier::refresh_fp32() {
@@ -1034,7 +1047,7 @@ T* DevHier::cycle_level(int l, T* x, const T* b, bool x_zero, const CycleOpts& o
     const void* desc = sizeof(T) == 8 ? tail64_ : tail32_;
     const int slot = sizeof(T) == 8 ? 0 : 1;
     TailCoarse<T> C{nc_, clu_, cpiv_, coarse_b<T>(), coarse_x<T>(), tail_co_[slot][0], tail_co_[slot][1],
-                    tail_co_[slot][2], tail_co_[slot][3]};
+                    tail_co_[slot][2], tail_co_[slot][3], tail_inv_ ? 1 : 0};
     counted();
     const TailCopyList& cl = tail_cp_[slot];
     const TailCopies cp{static_cast<const TailCopy*>(cl.list), cl.npat, cl.nval, cl.pat_bytes,
@@ -2169,6 +2182,7 @@ void DevHier::resetup_values(const double* v_dev) {
   counted();
   k_lu_factor<<<1, threads, 0, st_>>>(nc_, clu_, cpiv_, info_);
   DR_CK(cudaGetLastError());
+  if (tail_inv_) build_cinv();
   if (at_built_) refresh_transpose();  // before the FP32 copies, which include the transposed ones
   refresh_fp32();
   check_kernel_flag(st_);

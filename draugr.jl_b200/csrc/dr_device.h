@@ -460,6 +460,12 @@ class DevHier {
   double* cdense_ = nullptr;
   double* clu_ = nullptr;
   int* cpiv_ = nullptr;
+  // the coarsest system's explicit inverse, which the shared-memory tail
+  // applies instead of the substitutions when the cycle is not bit-exact
+  // anyway (some level sums its rows in a tree) and n_c <= 32
+  double* cinv_ = nullptr;
+  bool tail_inv_ = false;
+  void build_cinv();
   int* info_ = nullptr;
   double *cb64_ = nullptr, *cx64_ = nullptr;
   float *cb32_ = nullptr, *cx32_ = nullptr;

@@ -1027,6 +1027,7 @@ struct TailCoarse {
   // shared-memory offsets (bytes): factors followed by n doubles of work
   // space, pivots, right-hand side, solution
   unsigned o_lu, o_piv, o_b, o_x;
+  int inv;  // 1: o_lu holds the explicit inverse (column-major), not the factors
 };
 
 constexpr int kTailMaxLevels = 8;
@@ -1164,6 +1165,19 @@ __device__ __forceinline__ void tail_lu_solve(const TailCoarse<T>& C) {
   const int* piv = tail_sh<const int>(C.o_piv);
   const T* cb = tail_sh<const T>(C.o_b);
   T* cx = tail_sh<T>(C.o_x);
+  if (C.inv && n <= 32) {
+    // x = A_c^-1 b, one row of the inverse per lane, summed in column order
+    if (threadIdx.x < 32) {
+      const int i = threadIdx.x;
+      if (i < n) {
+        double y = 0.0;
+        for (int j = 0; j < n; ++j) y = __dadd_rn(y, __dmul_rn(lu[j * n + i], (double)cb[j]));
+        cx[i] = (T)y;
+      }
+    }
+    __syncthreads();
+    return;
+  }
   if (n <= 32) {
     if (threadIdx.x < 32) {
       const int i = threadIdx.x;
@@ -1455,6 +1469,34 @@ __global__ void k_lu_factor(int n, double* __restrict__ a, int* __restrict__ piv
     }
     __syncthreads();
   }
+}
+
+// Explicit inverse of A from its getrf factors (column-major, 0-based
+// pivots), column j by thread j: A x = e_j solved in getrs order (row
+// interchanges, unit-lower then upper substitution).  n <= 32.
+__global__ void k_lu_inverse(int n, const double* __restrict__ lu, const int* __restrict__ piv,
+                             double* __restrict__ inv) {
+  const int j = threadIdx.x;
+  if (j >= n) return;
+  double y[32];
+  for (int i = 0; i < n; ++i) y[i] = i == j ? 1.0 : 0.0;
+  for (int k = 0; k < n; ++k) {
+    const int p = piv[k];
+    if (p != k) {
+      const double t = y[k];
+      y[k] = y[p];
+      y[p] = t;
+    }
+  }
+  for (int k = 0; k < n; ++k)
+    if (y[k] != 0.0)
+      for (int i = k + 1; i < n; ++i) y[i] = __dsub_rn(y[i], __dmul_rn(y[k], lu[k * n + i]));
+  for (int k = n - 1; k >= 0; --k) {
+    if (y[k] != 0.0) y[k] = __ddiv_rn(y[k], lu[k * n + k]);
+    if (y[k] != 0.0)
+      for (int i = 0; i < k; ++i) y[i] = __dsub_rn(y[i], __dmul_rn(y[k], lu[k * n + i]));
+  }
+  for (int i = 0; i < n; ++i) inv[j * n + i] = y[i];
 }
 
 // Scatter CSR values into a zeroed column-major dense matrix.
