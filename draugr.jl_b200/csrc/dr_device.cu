@@ -401,6 +401,15 @@ DevHier::DevHier(const HostHierarchy& H, int device, const BatchLayout* batch) {
         h2d(b.nb, c.nb, st_);
         h2d(b.poff, c.poff, st_);
         h2d(b.luoff, c.luoff, st_);
+        if (b.maxn <= kern::kInvMax) {
+          // the merged cycle is not bit-exact against the systems' own
+          // anyway: apply each coarsest system's explicit inverse
+          if (!binv_) binv_ = alloc<double>(std::max<size_t>(batch->lu.size(), 1));
+          counted();
+          k_lu_inverse_batch<<<b.nblk, kern::kInvMax, 0, st_>>>(b.nb, b.luoff, b.poff, blu_, bpiv_, binv_);
+          DR_CK(cudaGetLastError());
+          b.inv = true;
+        }
       }
       // finest-level segments: system s occupies rows off[0][s] .. off[0][s + 1] - 1
       std::vector<int> so(batch->nsys + 1, 0), sid(n0_);
@@ -1551,7 +1560,9 @@ void DevHier::batch_coarse(int l, const T* b, T* x) {
   if (c.nblk == 0) return;
   counted();
   const size_t wsm = (size_t)(c.maxn + (size_t)c.maxn * c.maxn) * sizeof(double);
-  if (wsm <= 48 * 1024) {  // one warp per system, its factors staged in shared memory
+  if (c.inv) {  // one block per system, x = A^-1 b
+    k_inv_apply_batch<T><<<c.nblk, kern::kInvMax, 0, st_>>>(c.off, c.nb, c.luoff, binv_, b, x);
+  } else if (wsm <= 48 * 1024) {  // one warp per system, its factors staged in shared memory
     k_lu_solve_batch_warp<T><<<c.nblk, 32, wsm, st_>>>(c.off, c.nb, c.luoff, c.poff, blu_, bpiv_, b, x, c.maxn);
   } else {
     int threads = 32;

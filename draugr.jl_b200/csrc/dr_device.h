@@ -400,9 +400,11 @@ class DevHier {
     int nblk = 0, maxn = 0;
     int *off = nullptr, *nb = nullptr, *poff = nullptr;
     long long* luoff = nullptr;
+    bool inv = false;  // solved with the explicit inverses (binv_), every n <= 64
   };
   std::vector<BatchDev> batch_dev_;
   double* blu_ = nullptr;
+  double* binv_ = nullptr;  // the systems' coarsest inverses, laid out like blu_
   int* bpiv_ = nullptr;
   int *seg_off_ = nullptr, *seg_id_ = nullptr;
   double* seg_buf_ = nullptr;    // per segment: rz, rzold, pq, rr, bb, alpha, beta

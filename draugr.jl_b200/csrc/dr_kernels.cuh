@@ -1473,12 +1473,14 @@ __global__ void k_lu_factor(int n, double* __restrict__ a, int* __restrict__ piv
 
 // Explicit inverse of A from its getrf factors (column-major, 0-based
 // pivots), column j by thread j: A x = e_j solved in getrs order (row
-// interchanges, unit-lower then upper substitution).  n <= 32.
-__global__ void k_lu_inverse(int n, const double* __restrict__ lu, const int* __restrict__ piv,
-                             double* __restrict__ inv) {
-  const int j = threadIdx.x;
-  if (j >= n) return;
-  double y[32];
+// interchanges, unit-lower then upper substitution).  n <= kInvMax.  Used
+// where the coarsest solve need not be the reference's substitutions bit for
+// bit.
+constexpr int kInvMax = 64;
+__device__ __forceinline__ void lu_inverse_column(int n, const double* __restrict__ lu,
+                                                  const int* __restrict__ piv, double* __restrict__ inv,
+                                                  int j) {
+  double y[kInvMax];
   for (int i = 0; i < n; ++i) y[i] = i == j ? 1.0 : 0.0;
   for (int k = 0; k < n; ++k) {
     const int p = piv[k];
@@ -1497,6 +1499,10 @@ __global__ void k_lu_inverse(int n, const double* __restrict__ lu, const int* __
       for (int i = 0; i < k; ++i) y[i] = __dsub_rn(y[i], __dmul_rn(y[k], lu[k * n + i]));
   }
   for (int i = 0; i < n; ++i) inv[j * n + i] = y[i];
+}
+__global__ void k_lu_inverse(int n, const double* __restrict__ lu, const int* __restrict__ piv,
+                             double* __restrict__ inv) {
+  if ((int)threadIdx.x < n) lu_inverse_column(n, lu, piv, inv, threadIdx.x);
 }
 
 // Scatter CSR values into a zeroed column-major dense matrix.
@@ -1932,6 +1938,35 @@ k_spgemm_warp(int nrows, const int* __restrict__ out_rp, const int* __restrict__
 // 0-based pivots at piv + poff[k]) for rows off[k] .. off[k] + nb[k] - 1 of
 // b into x, in the operation order of k_lu_solve (so each system's coarse
 // solve gives what its own hierarchy's gives).
+// The explicit inverses of the coarsest systems of a batch (block k: system
+// k, thread j: column j; inverse stored where the factors are;
+// n <= kInvMax),
+// and their application x = A^-1 b, one block of kInvMax threads per
+// system, each row of the inverse summed in column order.
+__global__ void k_lu_inverse_batch(const int* __restrict__ nb, const long long* __restrict__ luoff,
+                                   const int* __restrict__ poff, const double* __restrict__ lu_all,
+                                   const int* __restrict__ piv_all, double* __restrict__ inv_all) {
+  const int k = blockIdx.x;
+  const int n = nb[k];
+  if ((int)threadIdx.x < n)
+    lu_inverse_column(n, lu_all + luoff[k], piv_all + poff[k], inv_all + luoff[k], threadIdx.x);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kInvMax)
+k_inv_apply_batch(const int* __restrict__ off, const int* __restrict__ nb, const long long* __restrict__ luoff,
+                  const double* __restrict__ inv_all, const T* __restrict__ bin, T* __restrict__ xout) {
+  const int k = blockIdx.x;
+  const int n = nb[k], o = off[k];
+  const double* inv = inv_all + luoff[k];
+  const int i = threadIdx.x;
+  if (i < n) {
+    double y = 0.0;
+    for (int j = 0; j < n; ++j) y = __dadd_rn(y, __dmul_rn(inv[j * n + i], (double)bin[o + j]));
+    xout[o + i] = (T)y;
+  }
+}
+
 template <typename T>
 __global__ void k_lu_solve_batch(const int* __restrict__ off, const int* __restrict__ nb,
                                  const long long* __restrict__ luoff, const int* __restrict__ poff,
