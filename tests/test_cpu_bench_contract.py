@@ -27,6 +27,8 @@ def test_reference_arm_json_line():
     assert d["steps"] == 2 and d["warmup"] == 1 and d["value"] > 0
     assert d["e2e"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0
     assert d["cpu_baseline"]["value"] == d["value"] and d["cpu_baseline"]["kind"] in ("port", "reference")
+    # one host V-cycle, against the same algorithmic bytes as the GPU cycle
+    assert d["cpu_baseline"]["vcycle_ms"] > 0 and d["cpu_baseline"]["vcycle_GBps"] > 0
     assert d["config"]["workload"].startswith("3D 7-point heterogeneous diffusion 12^3")
     assert d["relres_fp64_verified"] < 1e-8
     # the timed process ran the oracle only: the product library is not mapped
