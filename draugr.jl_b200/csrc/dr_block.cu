@@ -296,6 +296,19 @@ k_bl_take_z(int n, int k, const TS* __restrict__ z, const double* __restrict__ R
   block_col_partials<TPR, 2>(s, k, part);
 }
 
+// X = A_c^-1 B for k columns (n x k row-major), A_c^-1 column-major: one
+// thread per entry, its row of the inverse summed in column order.
+template <typename T>
+__global__ void __launch_bounds__(kBlock)
+k_bl_inv(int n, int k, const double* __restrict__ inv, const T* __restrict__ B, T* __restrict__ X) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n * k) return;
+  const int i = e / k, c = e % k;
+  double y = 0.0;
+  for (int j = 0; j < n; ++j) y = __dadd_rn(y, __dmul_rn(inv[j * n + i], (double)B[(size_t)j * k + c]));
+  X[e] = (T)y;
+}
+
 template <typename T>
 __global__ void k_bl_fill(long long n, T* __restrict__ x) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -768,7 +781,9 @@ T* DevHier::cycle_block(int l, T* X, const T* B, bool x_zero, const CycleOpts& o
   } else {
     xc = sizeof(T) == 8 ? (T*)bcx64_ : (T*)bcx32_;
     note_launch();
-    if (nc_ <= 64) {
+    if (cinv_ok_) {  // the explicit inverse (a hierarchy with tree-summed levels)
+      k_bl_inv<T><<<grid_for((long long)nc_ * k, max_grid_), kBlock, 0, st_>>>(nc_, k, cinv_, bc, xc);
+    } else if (nc_ <= 64) {
       const size_t wsm = ((size_t)nc_ * nc_ + (size_t)k * nc_) * sizeof(double);  // <= 48 KB
       k_bl_lu_warp<T><<<1, 32 * k, wsm, st_>>>(nc_, k, clu_, cpiv_, bc, xc);
     } else {

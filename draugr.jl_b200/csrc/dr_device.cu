@@ -439,6 +439,14 @@ DevHier::DevHier(const HostHierarchy& H, int device, const BatchLayout* batch) {
       DR_CK(cudaFuncSetAttribute(k_lu_solve<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
       DR_CK(cudaFuncSetAttribute(k_lu_solve<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
     }
+    if (!batch) {
+      // the coarsest inverse, for hierarchies whose cycle is not bit-exact
+      // anyway (some level sums its rows in a tree)
+      bool any_tree = false;
+      for (int l = 0; l < nl; ++l) any_tree = any_tree || !L_[l].A.form.ordered;
+      cinv_ok_ = any_tree && nc_ >= 1 && nc_ <= kern::kInvMax;
+      if (cinv_ok_) build_cinv();
+    }
     if (batch) tail_ = nl;  // no shared-memory tail: every level runs as its own launches
     else build_tail();
     build_fused(H);
@@ -701,12 +709,7 @@ void DevHier::build_tail() {
     tail_ = l;
   }
   if (tail_ >= nl) return;
-  {
-    bool any_tree = false;
-    for (int l = 0; l < nl; ++l) any_tree = any_tree || !L_[l].A.form.ordered;
-    tail_inv_ = any_tree && nc_ >= 1 && nc_ <= 32;
-    if (tail_inv_) build_cinv();
-  }
+  tail_inv_ = cinv_ok_ && nc_ <= 32;
   const int cnt = nl - tail_;
   std::reverse(ords.begin(), ords.end());  // tail_ first
   std::vector<int*> ord_dev(cnt);
@@ -878,7 +881,7 @@ void DevHier::build_q(DevLevel& d) {
 void DevHier::build_cinv() {
   if (!cinv_) cinv_ = alloc<double>((size_t)nc_ * nc_);
   counted();
-  k_lu_inverse<<<1, 32, 0, st_>>>(nc_, clu_, cpiv_, cinv_);
+  k_lu_inverse<<<1, kern::kInvMax, 0, st_>>>(nc_, clu_, cpiv_, cinv_);
   DR_CK(cudaGetLastError());
 }
 
@@ -2193,7 +2196,7 @@ void DevHier::resetup_values(const double* v_dev) {
   counted();
   k_lu_factor<<<1, threads, 0, st_>>>(nc_, clu_, cpiv_, info_);
   DR_CK(cudaGetLastError());
-  if (tail_inv_) build_cinv();
+  if (cinv_ok_) build_cinv();
   if (at_built_) refresh_transpose();  // before the FP32 copies, which include the transposed ones
   refresh_fp32();
   check_kernel_flag(st_);

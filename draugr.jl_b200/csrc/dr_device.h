@@ -463,10 +463,11 @@ class DevHier {
   double* clu_ = nullptr;
   int* cpiv_ = nullptr;
   // the coarsest system's explicit inverse, which the shared-memory tail
-  // applies instead of the substitutions when the cycle is not bit-exact
-  // anyway (some level sums its rows in a tree) and n_c <= 32
+  // and the block cycle apply instead of the substitutions when the cycle
+  // is not bit-exact anyway (some level sums its rows in a tree)
   double* cinv_ = nullptr;
-  bool tail_inv_ = false;
+  bool cinv_ok_ = false;   // cinv_ is kept (such a hierarchy, n_c <= 64)
+  bool tail_inv_ = false;  // the tail applies it (n_c <= 32)
   void build_cinv();
   int* info_ = nullptr;
   double *cb64_ = nullptr, *cx64_ = nullptr;
